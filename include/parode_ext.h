@@ -1,0 +1,92 @@
+/*
+ * parode_ext.h -- entry points of libParODEShared.so beyond the reference ABI.
+ *
+ * These are additive: the reference (apatriciu/ParODE) has no counterpart
+ * for the FP64 arrays, precision forms, device residency, batching or the
+ * serving queue below, so each comment says which reference behaviour it
+ * extends.  All functions are extern "C", take plain pointers and sizes and
+ * report errors through nErr[0] (ParODEEnums.h values plus the extra codes
+ * below), exactly as the reference ABI does.
+ */
+#ifndef PARODE_EXT_H_
+#define PARODE_EXT_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Error codes beyond ParODEEnums.h (-1..-7). */
+#define ParODE_InvalidInput     (-8)  /* uIndex names no registered input               */
+#define ParODE_InvalidArgument  (-9)  /* a size, pointer or option value is out of range */
+#define ParODE_DeviceError      (-10) /* a CUDA call failed or a device wait gave up     */
+
+/* Precision forms of the scan. */
+#define PARODE_PRECISION_FP64   0  /* plain: every sweep, the carry and the outputs in FP64  */
+#define PARODE_PRECISION_MIXED  1  /* leaf sweeps in 3xTF32 on tcgen05 with FP32 accumulation;
+                                      Phi, the power table, the upper levels and the carry in FP64 */
+
+/* Options (ParODE_SetOption / ParODE_GetOption). */
+#define PARODE_OPT_PRECISION    1  /* PARODE_PRECISION_* used by SimulateODE (default FP64) */
+#define PARODE_OPT_PATH         2  /* 0 auto, 1 level-synchronous sweeps, 2 blocked fused sweeps */
+#define PARODE_OPT_LOG          3  /* non-zero: one line per solve on stderr */
+
+void ParODE_SetOption(int option, long long value, int nErr[]);
+long long ParODE_GetOption(int option, int nErr[]);
+
+/* Number of outputs SimulateODE produces for (solver, tStart, tEnd, tStep):
+ * RK4 floor((tEnd-tStart)/tStep)+1 (reference Sources/RungeKutta4thOrder.cpp:20),
+ * ABM that count from tStart+3 tStep, plus 3 (Sources/AdamsMoulton.cpp:356-358).
+ * Returns -1 for an empty horizon. */
+long long ParODE_NumOutputs(int solver, double tStart, double tEnd, double tStep);
+
+/* Registers the built-in input u_i(t) = sum_k amp[i*K+k] sin(2 pi freq[i*K+k] t + phase[i*K+k])
+ * (K = nTerms) and returns its index in the same index space as RegisterInput.
+ * Evaluated on the device in FP64 time; the scan kernels can generate it on chip. */
+void ParODE_RegisterSinusoidInput(int nInputs, int nTerms, const double* amp, const double* freq,
+                                  const double* phase, int uIndex[], int nErr[]);
+
+/* FP64 form of SimulateODE: same arguments and layouts as the C ABI
+ * (by value instead of by pointer), FP64 arrays, an explicit precision form,
+ * and 64-bit step counts.  tVect may be NULL.  yVect receives
+ * nSteps[0] x nOutputs values (time-major). */
+void ParODE_SimulateODE_d(const double* A, const double* B, const double* C, const double* D,
+                          int nInputs, int nStates, int nOutputs, int ZeroB, int ZeroC, int ZeroD,
+                          int uIndex, double tStart, double tEnd, double tStep, const double* x0,
+                          int solver, int precision, double* tVect, double* yVect,
+                          long long nSteps[], int nErr[]);
+
+/* ---- device-resident plans ------------------------------------------------
+ * A plan holds one discretised system on the device (Phi, Bbar, C, D, the
+ * initial scan state and every scan buffer), so repeated executions do no
+ * host work and no allocation.  PlanCreate performs the host FP64
+ * discretisation (and the ABM start-up) and the uploads; PlanExecute only
+ * enqueues device work on `stream` (a cudaStream_t; NULL = the library's
+ * stream) and returns without synchronising. */
+typedef struct ParODE_Plan ParODE_Plan;
+
+ParODE_Plan* ParODE_PlanCreate(const double* A, const double* B, const double* C, const double* D,
+                               int nInputs, int nStates, int nOutputs, int ZeroB, int ZeroC, int ZeroD,
+                               int uIndex, double tStart, double tEnd, double tStep, const double* x0,
+                               int solver, int precision, int nErr[]);
+/* Enqueue one solve.  yDev: device buffer of NumOutputs x nOutputs doubles,
+ * or NULL to keep the result in the plan. */
+void ParODE_PlanExecute(ParODE_Plan* plan, double* yDev, void* stream, int nErr[]);
+/* Copy the last result to host memory (synchronises the plan's stream). */
+void ParODE_PlanGetOutput(ParODE_Plan* plan, double* tVect, double* yVect, int nErr[]);
+long long ParODE_PlanNumOutputs(const ParODE_Plan* plan);
+int ParODE_PlanNumOutputChannels(const ParODE_Plan* plan);
+/* Device kernel launches one PlanExecute enqueues (for launch accounting). */
+int ParODE_PlanLaunchCount(const ParODE_Plan* plan);
+void ParODE_PlanDestroy(ParODE_Plan* plan);
+/* Stage timing: when enabled, PlanExecute records CUDA events between its
+ * stages on the execution stream.  PlanStageTimes synchronises on the last
+ * event and returns the number of stages; ms[i] receives stage i's
+ * milliseconds (up to cap) and names its '\n'-separated names. */
+void ParODE_PlanSetProfiling(ParODE_Plan* plan, int enable, int nErr[]);
+int ParODE_PlanStageTimes(ParODE_Plan* plan, float* ms, int cap, char* names, int names_cap, int nErr[]);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PARODE_EXT_H_ */

@@ -1,0 +1,297 @@
+"""parode_b200 -- Python host API over libParODEShared.so (B200 build of ParODE).
+
+The drop-in surface is the C ABI (include/ParODECInterface.h) and the
+`ParODE` extension module built next to this file; this package is a thin
+ctypes layer for Python callers, tests and benchmarks:
+
+    import parode_b200 as pb
+    pb.init()                                  # InitializeAllGPUs
+    u = pb.register_sinusoid(a, f, phi)        # or pb.register_input(src)
+    t, y = pb.simulate(A, B, C, D, x0, u, t0, t_end, h, solver=pb.RK4)
+
+Every call goes to the CUDA library.  There is no CPU fallback: importing the
+package fails if libParODEShared.so is missing, and solves report ParODE
+error codes as exceptions.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from typing import Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libParODEShared.so")
+
+RK4 = 0
+ABM = 1
+FP64 = 0
+MIXED = 1
+
+OPT_PRECISION = 1
+OPT_PATH = 2
+OPT_LOG = 3
+
+PATH_AUTO = 0
+PATH_LEVEL = 1
+PATH_BLOCKED = 2
+
+ERRORS = {
+    0: "OK", -1: "NoGPU", -2: "NotInitialized", -3: "CouldNotCreateGPUKernels", -4: "NotEnoughResources",
+    -5: "InvalidDeviceId", -6: "InvalidSystem", -7: "InvalidSolverType", -8: "InvalidInput",
+    -9: "InvalidArgument", -10: "DeviceError",
+}
+
+
+class ParODEError(RuntimeError):
+    def __init__(self, code: int, where: str = ""):
+        self.code = int(code)
+        super().__init__(f"{where}: ParODE error {code} ({ERRORS.get(int(code), '?')})")
+
+
+def build() -> None:
+    """Compile libParODEShared.so and the ParODE module (nvcc, sm_100a)."""
+    subprocess.run(["make", "-s", "-C", _HERE, "-j8"], check=True)
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: run parode_b200.build() (make -C parode_b200)")
+    L = C.CDLL(LIB_PATH)
+    dp = C.POINTER(C.c_double)
+    ip = C.POINTER(C.c_int)
+    L.GetErrorDescription.argtypes = [ip, C.c_char_p]
+    L.InitializeAllGPUs.argtypes = [C.c_char_p, C.c_char_p, ip]
+    L.GetAvailableGPUs.argtypes = [ip, ip, ip]
+    L.GetDeviceName.argtypes = [ip, C.c_char_p, ip]
+    L.InitializeSelectedGPUs.argtypes = [ip, ip, C.c_char_p, C.c_char_p, ip]
+    fp = C.POINTER(C.c_float)
+    L.SimulateODE.argtypes = [fp, fp, fp, fp, ip, ip, ip, ip, ip, ip, ip, dp, dp, dp, fp, ip, fp, fp, ip, ip]
+    L.RegisterInput.argtypes = [C.c_char_p, ip, ip]
+    L.CloseGPUC.argtypes = []
+    L.StartTimer.argtypes = [ip]
+    L.StopTimer.argtypes = [fp, ip]
+    L.ParODE_SetOption.argtypes = [C.c_int, C.c_longlong, ip]
+    L.ParODE_GetOption.argtypes = [C.c_int, ip]
+    L.ParODE_GetOption.restype = C.c_longlong
+    L.ParODE_NumOutputs.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double]
+    L.ParODE_NumOutputs.restype = C.c_longlong
+    L.ParODE_RegisterSinusoidInput.argtypes = [C.c_int, C.c_int, dp, dp, dp, ip, ip]
+    L.ParODE_SimulateODE_d.argtypes = [dp, dp, dp, dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                       C.c_int, C.c_double, C.c_double, C.c_double, dp, C.c_int, C.c_int, dp, dp,
+                                       C.POINTER(C.c_longlong), ip]
+    L.ParODE_PlanCreate.argtypes = [dp, dp, dp, dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                    C.c_double, C.c_double, C.c_double, dp, C.c_int, C.c_int, ip]
+    L.ParODE_PlanCreate.restype = C.c_void_p
+    L.ParODE_PlanExecute.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, ip]
+    L.ParODE_PlanGetOutput.argtypes = [C.c_void_p, dp, dp, ip]
+    L.ParODE_PlanNumOutputs.argtypes = [C.c_void_p]
+    L.ParODE_PlanNumOutputs.restype = C.c_longlong
+    L.ParODE_PlanNumOutputChannels.argtypes = [C.c_void_p]
+    L.ParODE_PlanLaunchCount.argtypes = [C.c_void_p]
+    L.ParODE_PlanDestroy.argtypes = [C.c_void_p]
+    L.ParODE_PlanSetProfiling.argtypes = [C.c_void_p, C.c_int, ip]
+    L.ParODE_PlanStageTimes.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_int, C.c_char_p, C.c_int, ip]
+    L.ParODE_PlanStageTimes.restype = C.c_int
+    return L
+
+
+lib = _load()
+
+
+def _dp(a: Optional[np.ndarray]):
+    return C.POINTER(C.c_double)() if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _check(err: C.c_int, where: str) -> None:
+    if err.value != 0:
+        raise ParODEError(err.value, where)
+
+
+def error_description(code: int) -> str:
+    buf = C.create_string_buffer(256)
+    c = C.c_int(code)
+    lib.GetErrorDescription(C.byref(c), buf)
+    return buf.value.decode()
+
+
+def available_gpus():
+    n = C.c_int(0)
+    ids = (C.c_int * 64)()
+    e = C.c_int(0)
+    lib.GetAvailableGPUs(C.byref(n), ids, C.byref(e))
+    _check(e, "GetAvailableGPUs")
+    return [ids[i] for i in range(n.value)]
+
+
+def init(device_ids=None) -> None:
+    """InitializeAllGPUs, or GetAvailableGPUs + InitializeSelectedGPUs."""
+    e = C.c_int(0)
+    if device_ids is None:
+        lib.InitializeAllGPUs(b"", b"", C.byref(e))
+        _check(e, "InitializeAllGPUs")
+        return
+    available_gpus()
+    ids = (C.c_int * len(device_ids))(*device_ids)
+    n = C.c_int(len(device_ids))
+    lib.InitializeSelectedGPUs(C.byref(n), ids, b"", b"", C.byref(e))
+    _check(e, "InitializeSelectedGPUs")
+
+
+def close() -> None:
+    lib.CloseGPUC()
+
+
+def set_option(option: int, value: int) -> None:
+    e = C.c_int(0)
+    lib.ParODE_SetOption(option, value, C.byref(e))
+    _check(e, "ParODE_SetOption")
+
+
+def get_option(option: int) -> int:
+    e = C.c_int(0)
+    v = lib.ParODE_GetOption(option, C.byref(e))
+    _check(e, "ParODE_GetOption")
+    return int(v)
+
+
+def num_outputs(solver: int, t0: float, t_end: float, h: float) -> int:
+    return int(lib.ParODE_NumOutputs(solver, t0, t_end, h))
+
+
+def register_input(source: str) -> int:
+    """RegisterInput: `fType UFunc(fType t, int nInputIndex)` in CUDA C++ (NVRTC)."""
+    idx = C.c_int(-1)
+    e = C.c_int(0)
+    lib.RegisterInput(source.encode(), C.byref(idx), C.byref(e))
+    _check(e, "RegisterInput")
+    return idx.value
+
+
+def register_sinusoid(a, f, phi) -> int:
+    """Built-in input u_i(t) = sum_k a[i,k] sin(2 pi f[i,k] t + phi[i,k])."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    f = np.ascontiguousarray(f, dtype=np.float64)
+    phi = np.ascontiguousarray(phi, dtype=np.float64)
+    m, K = a.shape
+    idx = C.c_int(-1)
+    e = C.c_int(0)
+    lib.ParODE_RegisterSinusoidInput(m, K, _dp(a), _dp(f), _dp(phi), C.byref(idx), C.byref(e))
+    _check(e, "ParODE_RegisterSinusoidInput")
+    return idx.value
+
+
+def _sys_arrays(A, B, Cm, D, x0):
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    n = A.shape[0]
+    B = None if B is None or np.size(B) == 0 else np.ascontiguousarray(B, dtype=np.float64)
+    Cm = None if Cm is None or np.size(Cm) == 0 else np.ascontiguousarray(Cm, dtype=np.float64)
+    D = None if D is None or np.size(D) == 0 else np.ascontiguousarray(D, dtype=np.float64)
+    x0 = np.ascontiguousarray(np.zeros(n) if x0 is None else x0, dtype=np.float64)
+    m = B.shape[1] if B is not None else (D.shape[1] if D is not None else 0)
+    p = Cm.shape[0] if Cm is not None else (D.shape[0] if D is not None else 0)
+    return A, B, Cm, D, x0, n, m, p
+
+
+def simulate(A, B, Cm, D, x0, u_index: int, t0: float, t_end: float, h: float, solver: int = RK4,
+             precision: int = FP64):
+    """ParODE_SimulateODE_d: returns (t, y) with y of shape (T, outputs)."""
+    A, B, Cm, D, x0, n, m, p = _sys_arrays(A, B, Cm, D, x0)
+    T = num_outputs(solver, t0, t_end, h)
+    if T <= 0:
+        raise ParODEError(-6, "simulate")
+    q = n if (Cm is None and D is None) else p
+    t = np.zeros(T)
+    y = np.zeros((T, q))
+    ns = C.c_longlong(0)
+    e = C.c_int(0)
+    lib.ParODE_SimulateODE_d(_dp(A), _dp(B), _dp(Cm), _dp(D), m, n, p, int(B is None), int(Cm is None),
+                             int(D is None), u_index, t0, t_end, h, _dp(x0), solver, precision, _dp(t), _dp(y),
+                             C.byref(ns), C.byref(e))
+    _check(e, "ParODE_SimulateODE_d")
+    return t[:ns.value], y[:ns.value]
+
+
+def simulate_f32(A, B, Cm, D, x0, u_index: int, t0: float, t_end: float, h: float, solver: int = RK4):
+    """The reference C ABI SimulateODE (float arrays).  Returns (t, y, err)."""
+    A32 = np.ascontiguousarray(A, dtype=np.float32)
+    n = A32.shape[0]
+    zB, zC, zD = int(B is None or np.size(B) == 0), int(Cm is None or np.size(Cm) == 0), int(D is None or np.size(D) == 0)
+    B32 = np.ascontiguousarray(B if not zB else np.zeros(1), dtype=np.float32)
+    C32 = np.ascontiguousarray(Cm if not zC else np.zeros(1), dtype=np.float32)
+    D32 = np.ascontiguousarray(D if not zD else np.zeros(1), dtype=np.float32)
+    x32 = np.ascontiguousarray(x0, dtype=np.float32)
+    m = B32.shape[1] if not zB else (D32.shape[1] if not zD else 0)
+    p = C32.shape[0] if not zC else (D32.shape[0] if not zD else n)
+    T = max(num_outputs(solver, t0, t_end, h), 1)
+    t = np.zeros(T, dtype=np.float32)
+    y = np.zeros((T, p), dtype=np.float32)
+    fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+    args_i = [C.c_int(v) for v in (m, n, p, zB, zC, zD, u_index)]
+    ts, te, hs = C.c_double(t0), C.c_double(t_end), C.c_double(h)
+    sv = C.c_int(solver)
+    nsteps = C.c_int(0)
+    e = C.c_int(0)
+    lib.SimulateODE(fp(A32), fp(B32), fp(C32), fp(D32), *[C.byref(v) for v in args_i], C.byref(ts), C.byref(te),
+                    C.byref(hs), fp(x32), C.byref(sv), fp(t), fp(y), C.byref(nsteps), C.byref(e))
+    return t[:nsteps.value], y[:nsteps.value], e.value
+
+
+class Plan:
+    """Device-resident solve (ParODE_PlanCreate / Execute / GetOutput)."""
+
+    def __init__(self, A, B, Cm, D, x0, u_index: int, t0: float, t_end: float, h: float, solver: int = RK4,
+                 precision: int = FP64):
+        A, B, Cm, D, x0, n, m, p = _sys_arrays(A, B, Cm, D, x0)
+        e = C.c_int(0)
+        self._h = lib.ParODE_PlanCreate(_dp(A), _dp(B), _dp(Cm), _dp(D), m, n, p, int(B is None), int(Cm is None),
+                                        int(D is None), u_index, t0, t_end, h, _dp(x0), solver, precision,
+                                        C.byref(e))
+        _check(e, "ParODE_PlanCreate")
+        self.num_outputs = int(lib.ParODE_PlanNumOutputs(self._h))
+        self.channels = int(lib.ParODE_PlanNumOutputChannels(self._h))
+
+    def execute(self, y_dev_ptr: int = 0, stream: int = 0) -> None:
+        e = C.c_int(0)
+        lib.ParODE_PlanExecute(self._h, C.c_void_p(y_dev_ptr or None), C.c_void_p(stream or None), C.byref(e))
+        _check(e, "ParODE_PlanExecute")
+
+    def output(self):
+        t = np.zeros(self.num_outputs)
+        y = np.zeros((self.num_outputs, self.channels))
+        e = C.c_int(0)
+        lib.ParODE_PlanGetOutput(self._h, _dp(t), _dp(y), C.byref(e))
+        _check(e, "ParODE_PlanGetOutput")
+        return t, y
+
+    def set_profiling(self, on: bool = True) -> None:
+        e = C.c_int(0)
+        lib.ParODE_PlanSetProfiling(self._h, int(on), C.byref(e))
+        _check(e, "ParODE_PlanSetProfiling")
+
+    def stage_times(self):
+        """[(stage, ms)] of the last profiled execute (synchronises)."""
+        ms = (C.c_float * 64)()
+        names = C.create_string_buffer(4096)
+        e = C.c_int(0)
+        n = lib.ParODE_PlanStageTimes(self._h, ms, 64, names, 4096, C.byref(e))
+        _check(e, "ParODE_PlanStageTimes")
+        labels = names.value.decode().split("\n")
+        return [(labels[i], float(ms[i])) for i in range(min(n, 64))]
+
+    @property
+    def launch_count(self) -> int:
+        return int(lib.ParODE_PlanLaunchCount(self._h))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib.ParODE_PlanDestroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

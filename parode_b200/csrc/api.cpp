@@ -1,0 +1,515 @@
+// api.cpp -- the exported C ABI of libParODEShared.so and its library state.
+//
+// Mirrors the reference's extern "C" layer and ParODE singleton
+// (Sources/ParODE.cpp:23-174 and :244-572): initialisation states
+// NOT / PARTIAL / FULL, the input registry, error codes in nErr[0], no
+// exception crossing the ABI.  Differences, all additive: a mutex serialises
+// calls; invalid device ids and input indices are reported instead of being
+// undefined behaviour; GetErrorDescription knows every code.
+#include "common.h"
+#include "host_math.h"
+#include "inputs.h"
+#include "solver.h"
+
+#include "FTypeDef.h"
+#include "ParODECInterface.h"
+#include "parode_ext.h"
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+using namespace parode;
+
+namespace {
+
+enum InitState { kNot = 0, kPartial = 1, kFull = 2 };
+
+struct Library {
+    std::recursive_mutex mu;
+    InitState state = kNot;
+    std::vector<int> available;  // device ordinals of compute capability 10.x
+    std::vector<int> selected;
+    InputRegistry inputs;
+    int precision = kFP64;
+    int path = kPathAuto;
+    int log = 0;
+    cudaEvent_t t_start = nullptr, t_stop = nullptr;
+    bool timer_running = false;
+
+    void clean()
+    {
+        if (!selected.empty()) {
+            cudaSetDevice(selected[0]);
+            cudaDeviceSynchronize();
+        }
+        inputs.clear();
+        if (t_start) cudaEventDestroy(t_start);
+        if (t_stop) cudaEventDestroy(t_stop);
+        t_start = t_stop = nullptr;
+        timer_running = false;
+        selected.clear();
+        available.clear();
+        state = kNot;
+    }
+
+    void enumerate()
+    {
+        available.clear();
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess) {
+            cudaGetLastError();
+            count = 0;
+        }
+        for (int d = 0; d < count; ++d) {
+            cudaDeviceProp prop;
+            if (cudaGetDeviceProperties(&prop, d) != cudaSuccess) continue;
+            if (prop.major == 10) available.push_back(d);  // kernels are built for sm_100a only
+        }
+    }
+
+    int init_devices(const std::vector<int>& ids)
+    {
+        for (int d : ids) {
+            if (cudaSetDevice(d) != cudaSuccess || cudaFree(nullptr) != cudaSuccess) {
+                cudaGetLastError();
+                return kCouldNotCreateGPUKernels;
+            }
+        }
+        selected = ids;
+        cudaSetDevice(selected[0]);
+        if (cudaEventCreate(&t_start) != cudaSuccess || cudaEventCreate(&t_stop) != cudaSuccess) {
+            cudaGetLastError();
+            return kNotEnoughResources;
+        }
+        state = kFull;
+        return kOK;
+    }
+};
+
+Library& lib()
+{
+    static Library* L = new Library();  // never destroyed: CUDA may be torn down first at exit
+    return *L;
+}
+
+const char* describe(int code)
+{
+    switch (code) {
+    case kOK: return "No Error";
+    case kNoGPU: return "Sorry, no GPU available. Please make sure that a CUDA device of compute capability 10.x (B200) and its driver are installed.";
+    case kNotInitialized: return "ParODE not initialized. Please call InitializeAllGPUs or InitializeSelectedGPUs.";
+    case kCouldNotCreateGPUKernels: return "Could not create GPU kernels; the device could not be initialised or the input function does not compile.";
+    case kNotEnoughResources: return "Not enough resources: a device allocation or transfer failed.";
+    case kInvalidDeviceId: return "Invalid device id.";
+    case kInvalidSystem: return "Invalid system: empty state, inconsistent matrix sizes or an empty time horizon.";
+    case kInvalidSolverType: return "Invalid solver type (0 = Runge-Kutta 4, 1 = Adams-Bashforth-Moulton).";
+    case kInvalidInput: return "Invalid input index: register the input function first.";
+    case kInvalidArgument: return "Invalid argument.";
+    case kDeviceError: return "A CUDA call failed.";
+    default: return "Unknown Error";
+    }
+}
+
+// Builds a SystemDesc from caller arrays.  `T` is float (C ABI) or double.
+template <class T>
+SystemDesc make_system(const T* A, const T* B, const T* C, const T* D, int nInputs, int nStates, int nOutputs,
+                       int ZeroB, int ZeroC, int ZeroD, const T* x0)
+{
+    SystemDesc s;
+    if (nStates <= 0 || !A || !x0) throw Error(kInvalidSystem, "the system has no states");
+    s.n = nStates;
+    s.m = nInputs > 0 ? nInputs : 0;
+    s.p = nOutputs > 0 ? nOutputs : 0;
+    s.zeroB = ZeroB == 1 || s.m == 0;
+    s.zeroC = ZeroC == 1;
+    s.zeroD = ZeroD == 1 || s.m == 0;
+    if ((!s.zeroB && !B) || (!s.zeroC && (!C || s.p == 0)) || (!s.zeroD && (!D || s.p == 0)))
+        throw Error(kInvalidSystem, "a matrix flagged present is missing");
+    s.A.assign(A, A + (size_t)s.n * s.n);
+    if (!s.zeroB) s.B.assign(B, B + (size_t)s.n * s.m);
+    if (!s.zeroC) s.C.assign(C, C + (size_t)s.p * s.n);
+    if (!s.zeroD) s.D.assign(D, D + (size_t)s.p * s.m);
+    s.x0.assign(x0, x0 + s.n);
+    return s;
+}
+
+int current_device_locked(Library& L)
+{
+    if (L.state != kFull || L.selected.empty()) throw Error(kNotInitialized, "ParODE not initialized");
+    return L.selected[0];
+}
+
+template <class F>
+int guarded(F&& f)
+{
+    try {
+        f();
+        return kOK;
+    } catch (const Error& e) {
+        if (lib().log) std::fprintf(stderr, "ParODE: %s\n", e.what());
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        return kNotEnoughResources;
+    } catch (...) {
+        return kDeviceError;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+void GetErrorDescription(int* ErrNo, char strErrDescription[])
+{
+    if (!strErrDescription) return;
+    const char* d = describe(ErrNo ? *ErrNo : 1);
+    std::snprintf(strErrDescription, 256, "%s", d);
+}
+
+void InitializeAllGPUs(char* pszKernelFolder, char* pszIncludeFolder, int nErr[])
+{
+    (void)pszKernelFolder;
+    (void)pszIncludeFolder;
+    Library& L = lib();
+    std::lock_guard<std::recursive_mutex> g(L.mu);
+    int rc = guarded([&] {
+        L.clean();
+        L.enumerate();
+        if (L.available.empty()) throw Error(kNoGPU, "no compute capability 10.x device");
+        int r = L.init_devices(L.available);
+        if (r != kOK) {
+            L.clean();
+            throw Error(r, "device initialisation failed");
+        }
+    });
+    if (nErr) nErr[0] = rc;
+}
+
+void GetAvailableGPUs(int nGPUs[], int GPUIds[], int nErr[])
+{
+    Library& L = lib();
+    std::lock_guard<std::recursive_mutex> g(L.mu);
+    int rc = guarded([&] {
+        L.clean();
+        L.enumerate();
+        L.state = kPartial;
+    });
+    int n = rc == kOK ? (int)L.available.size() : 0;
+    if (nGPUs) nGPUs[0] = n;
+    if (GPUIds)
+        for (int i = 0; i < n; ++i) GPUIds[i] = L.available[i];
+    if (nErr) nErr[0] = rc;
+}
+
+void GetDeviceName(int* DeviceId, char strDeviceName[], int nErr[])
+{
+    Library& L = lib();
+    std::lock_guard<std::recursive_mutex> g(L.mu);
+    int rc = kOK;
+    if (strDeviceName) strDeviceName[0] = 0;
+    if (L.state == kNot) {
+        rc = kNotInitialized;
+    } else {
+        int id = DeviceId ? *DeviceId : -1;
+        bool known = false;
+        for (int d : L.available) known = known || d == id;
+        cudaDeviceProp prop;
+        if (!known || cudaGetDeviceProperties(&prop, id) != cudaSuccess) {
+            cudaGetLastError();
+            rc = kInvalidDeviceId;
+        } else if (strDeviceName) {
+            std::snprintf(strDeviceName, 256, "%s", prop.name);
+        }
+    }
+    if (nErr) nErr[0] = rc;
+}
+
+void InitializeSelectedGPUs(int* nGPUs, int GPUIds[], char* pszKernelFolder, char* pszIncludeFolder, int nErr[])
+{
+    (void)pszKernelFolder;
+    (void)pszIncludeFolder;
+    Library& L = lib();
+    std::lock_guard<std::recursive_mutex> g(L.mu);
+    int rc = guarded([&] {
+        if (L.state != kPartial) throw Error(kNotInitialized, "call GetAvailableGPUs first");
+        int n = nGPUs ? *nGPUs : 0;
+        if (n <= 0 || !GPUIds) throw Error(kNoGPU, "no device selected");
+        std::vector<int> ids;
+        for (int i = 0; i < n; ++i) {
+            bool known = false;
+            for (int d : L.available) known = known || d == GPUIds[i];
+            if (!known) throw Error(kInvalidDeviceId, "device id not in GetAvailableGPUs");
+            ids.push_back(GPUIds[i]);
+        }
+        int r = L.init_devices(ids);
+        if (r != kOK) {
+            L.clean();
+            throw Error(r, "device initialisation failed");
+        }
+    });
+    if (nErr) nErr[0] = rc;
+}
+
+void SimulateODE(fType A[], fType B[], fType C[], fType D[], int* nInputs, int* nStates, int* nOutputs, int* ZeroB,
+                 int* ZeroC, int* ZeroD, int* uIndex, double* tStart, double* tEnd, double* tStep, fType x0[],
+                 int* solver, fType tVect[], fType xVect[], int* nSteps, int nErr[])
+{
+    Library& L = lib();
+    std::lock_guard<std::recursive_mutex> g(L.mu);
+    if (nSteps) nSteps[0] = 0;
+    int rc = guarded([&] {
+        int dev = current_device_locked(L);
+        if (!nInputs || !nStates || !nOutputs || !ZeroB || !ZeroC || !ZeroD || !uIndex || !tStart || !tEnd ||
+            !tStep || !solver)
+            throw Error(kInvalidArgument, "null argument");
+        if (*solver != kRK4 && *solver != kABM) throw Error(kInvalidSolverType, "unknown solver");
+        SystemDesc s = make_system<fType>(A, B, C, D, *nInputs, *nStates, *nOutputs, *ZeroB, *ZeroC, *ZeroD, x0);
+        PlanOptions opt;
+        opt.precision = L.precision;
+        opt.path = L.path;
+        opt.input_double = false;  // UFunc(fType t, ...) with fType = float, as the reference ABI
+        Plan plan(dev, s, &L.inputs, *uIndex, *solver, *tStart, *tEnd, *tStep, opt);
+        plan.execute(nullptr, nullptr);
+        long T = plan.num_outputs();
+        int p = plan.channels();
+        std::vector<double> t((size_t)T), y((size_t)T * p);
+        plan.get_output(t.data(), y.data());
+        if (tVect)
+            for (long k = 0; k < T; ++k) tVect[k] = (fType)t[(size_t)k];
+        if (xVect)
+            for (long q = 0; q < T * p; ++q) xVect[q] = (fType)y[(size_t)q];
+        if (nSteps) nSteps[0] = (int)T;
+        if (L.log)
+            std::fprintf(stderr, "ParODE: SimulateODE solver=%d n=%d T=%ld path=%d launches=%d\n", *solver, s.n, T,
+                         plan.path(), plan.launch_count());
+    });
+    if (nErr) nErr[0] = rc;
+}
+
+void RegisterInput(char uFunc[], int uIndex[], int nErr[])
+{
+    Library& L = lib();
+    std::lock_guard<std::recursive_mutex> g(L.mu);
+    int idx = -1;
+    int rc = guarded([&] {
+        if (L.state != kFull) throw Error(kNotInitialized, "ParODE not initialized");
+        if (!uFunc) throw Error(kCouldNotCreateGPUKernels, "no source");
+        cudaSetDevice(L.selected[0]);
+        idx = L.inputs.add_user(std::string(uFunc));
+    });
+    if (uIndex) uIndex[0] = rc == kOK ? idx : rc;
+    if (nErr) nErr[0] = rc;
+}
+
+void CloseGPUC()
+{
+    Library& L = lib();
+    std::lock_guard<std::recursive_mutex> g(L.mu);
+    L.clean();
+}
+
+void StartTimer(int nErr[])
+{
+    Library& L = lib();
+    std::lock_guard<std::recursive_mutex> g(L.mu);
+    int rc = guarded([&] {
+        current_device_locked(L);
+        cudaSetDevice(L.selected[0]);
+        PARODE_CUDA(cudaDeviceSynchronize());
+        PARODE_CUDA(cudaEventRecord(L.t_start, 0));
+        PARODE_CUDA(cudaEventSynchronize(L.t_start));
+        L.timer_running = true;
+    });
+    if (nErr) nErr[0] = rc;
+}
+
+void StopTimer(float fTime[], int nErr[])
+{
+    Library& L = lib();
+    std::lock_guard<std::recursive_mutex> g(L.mu);
+    int rc = guarded([&] {
+        current_device_locked(L);
+        cudaSetDevice(L.selected[0]);
+        PARODE_CUDA(cudaDeviceSynchronize());
+        PARODE_CUDA(cudaEventRecord(L.t_stop, 0));
+        PARODE_CUDA(cudaEventSynchronize(L.t_stop));
+        float ms = 0.f;
+        if (L.timer_running) PARODE_CUDA(cudaEventElapsedTime(&ms, L.t_start, L.t_stop));
+        if (fTime) fTime[0] = ms;
+    });
+    if (nErr) nErr[0] = rc;
+}
+
+// ---------------------------------------------------------------------------
+// extensions (parode_ext.h)
+// ---------------------------------------------------------------------------
+
+void ParODE_SetOption(int option, long long value, int nErr[])
+{
+    Library& L = lib();
+    std::lock_guard<std::recursive_mutex> g(L.mu);
+    int rc = kOK;
+    switch (option) {
+    case PARODE_OPT_PRECISION:
+        if (value != PARODE_PRECISION_FP64 && value != PARODE_PRECISION_MIXED) rc = kInvalidArgument;
+        else L.precision = (int)value;
+        break;
+    case PARODE_OPT_PATH:
+        if (value < 0 || value > 2) rc = kInvalidArgument;
+        else L.path = (int)value;
+        break;
+    case PARODE_OPT_LOG: L.log = (int)value; break;
+    default: rc = kInvalidArgument;
+    }
+    if (nErr) nErr[0] = rc;
+}
+
+long long ParODE_GetOption(int option, int nErr[])
+{
+    Library& L = lib();
+    std::lock_guard<std::recursive_mutex> g(L.mu);
+    if (nErr) nErr[0] = kOK;
+    switch (option) {
+    case PARODE_OPT_PRECISION: return L.precision;
+    case PARODE_OPT_PATH: return L.path;
+    case PARODE_OPT_LOG: return L.log;
+    default:
+        if (nErr) nErr[0] = kInvalidArgument;
+        return -1;
+    }
+}
+
+long long ParODE_NumOutputs(int solver, double tStart, double tEnd, double tStep)
+{
+    long ns = 0;
+    return num_outputs(solver, tStart, tEnd, tStep, &ns);
+}
+
+void ParODE_RegisterSinusoidInput(int nInputs, int nTerms, const double* amp, const double* freq,
+                                  const double* phase, int uIndex[], int nErr[])
+{
+    Library& L = lib();
+    std::lock_guard<std::recursive_mutex> g(L.mu);
+    int idx = -1;
+    int rc = guarded([&] {
+        if (L.state != kFull) throw Error(kNotInitialized, "ParODE not initialized");
+        idx = L.inputs.add_sinusoid(nInputs, nTerms, amp, freq, phase);
+    });
+    if (uIndex) uIndex[0] = rc == kOK ? idx : rc;
+    if (nErr) nErr[0] = rc;
+}
+
+void ParODE_SimulateODE_d(const double* A, const double* B, const double* C, const double* D, int nInputs,
+                          int nStates, int nOutputs, int ZeroB, int ZeroC, int ZeroD, int uIndex, double tStart,
+                          double tEnd, double tStep, const double* x0, int solver, int precision, double* tVect,
+                          double* yVect, long long nSteps[], int nErr[])
+{
+    Library& L = lib();
+    std::lock_guard<std::recursive_mutex> g(L.mu);
+    if (nSteps) nSteps[0] = 0;
+    int rc = guarded([&] {
+        int dev = current_device_locked(L);
+        if (precision != PARODE_PRECISION_FP64 && precision != PARODE_PRECISION_MIXED)
+            throw Error(kInvalidArgument, "unknown precision");
+        SystemDesc s = make_system<double>(A, B, C, D, nInputs, nStates, nOutputs, ZeroB, ZeroC, ZeroD, x0);
+        PlanOptions opt;
+        opt.precision = precision;
+        opt.path = L.path;
+        opt.input_double = true;
+        Plan plan(dev, s, &L.inputs, uIndex, solver, tStart, tEnd, tStep, opt);
+        plan.execute(nullptr, nullptr);
+        plan.get_output(tVect, yVect);
+        if (nSteps) nSteps[0] = plan.num_outputs();
+    });
+    if (nErr) nErr[0] = rc;
+}
+
+struct ParODE_Plan {
+    std::unique_ptr<Plan> plan;
+};
+
+ParODE_Plan* ParODE_PlanCreate(const double* A, const double* B, const double* C, const double* D, int nInputs,
+                               int nStates, int nOutputs, int ZeroB, int ZeroC, int ZeroD, int uIndex,
+                               double tStart, double tEnd, double tStep, const double* x0, int solver, int precision,
+                               int nErr[])
+{
+    Library& L = lib();
+    std::lock_guard<std::recursive_mutex> g(L.mu);
+    ParODE_Plan* out = nullptr;
+    int rc = guarded([&] {
+        int dev = current_device_locked(L);
+        if (precision != PARODE_PRECISION_FP64 && precision != PARODE_PRECISION_MIXED)
+            throw Error(kInvalidArgument, "unknown precision");
+        SystemDesc s = make_system<double>(A, B, C, D, nInputs, nStates, nOutputs, ZeroB, ZeroC, ZeroD, x0);
+        PlanOptions opt;
+        opt.precision = precision;
+        opt.path = L.path;
+        opt.input_double = true;
+        auto h = std::make_unique<ParODE_Plan>();
+        h->plan = std::make_unique<Plan>(dev, s, &L.inputs, uIndex, solver, tStart, tEnd, tStep, opt);
+        out = h.release();
+    });
+    if (nErr) nErr[0] = rc;
+    return out;
+}
+
+void ParODE_PlanExecute(ParODE_Plan* plan, double* yDev, void* stream, int nErr[])
+{
+    int rc = guarded([&] {
+        if (!plan || !plan->plan) throw Error(kInvalidArgument, "null plan");
+        plan->plan->execute(yDev, (cudaStream_t)stream);
+    });
+    if (nErr) nErr[0] = rc;
+}
+
+void ParODE_PlanGetOutput(ParODE_Plan* plan, double* tVect, double* yVect, int nErr[])
+{
+    int rc = guarded([&] {
+        if (!plan || !plan->plan) throw Error(kInvalidArgument, "null plan");
+        plan->plan->get_output(tVect, yVect);
+    });
+    if (nErr) nErr[0] = rc;
+}
+
+long long ParODE_PlanNumOutputs(const ParODE_Plan* plan) { return plan && plan->plan ? plan->plan->num_outputs() : -1; }
+
+int ParODE_PlanNumOutputChannels(const ParODE_Plan* plan) { return plan && plan->plan ? plan->plan->channels() : -1; }
+
+int ParODE_PlanLaunchCount(const ParODE_Plan* plan) { return plan && plan->plan ? plan->plan->launch_count() : 0; }
+
+void ParODE_PlanDestroy(ParODE_Plan* plan) { delete plan; }
+
+void ParODE_PlanSetProfiling(ParODE_Plan* plan, int enable, int nErr[])
+{
+    int rc = guarded([&] {
+        if (!plan || !plan->plan) throw Error(kInvalidArgument, "null plan");
+        plan->plan->set_profiling(enable != 0);
+    });
+    if (nErr) nErr[0] = rc;
+}
+
+int ParODE_PlanStageTimes(ParODE_Plan* plan, float* ms, int cap, char* names, int names_cap, int nErr[])
+{
+    int count = 0;
+    int rc = guarded([&] {
+        if (!plan || !plan->plan) throw Error(kInvalidArgument, "null plan");
+        auto st = plan->plan->stage_times();
+        std::string joined;
+        for (auto& kv : st) {
+            if (count < cap && ms) ms[count] = kv.second;
+            joined += kv.first;
+            joined += '\n';
+            ++count;
+        }
+        if (names && names_cap > 0) std::snprintf(names, (size_t)names_cap, "%s", joined.c_str());
+    });
+    if (nErr) nErr[0] = rc;
+    return count;
+}
+
+}  // extern "C"

@@ -1,0 +1,62 @@
+// common.h -- shared definitions of the ParODE B200 library (host and device).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+#include <cuda_runtime.h>
+
+namespace parode {
+
+// Error codes: ParODEEnums.h (-1..-7) and parode_ext.h (-8..-10).
+enum Err : int {
+    kOK = 0,
+    kNoGPU = -1,
+    kNotInitialized = -2,
+    kCouldNotCreateGPUKernels = -3,
+    kNotEnoughResources = -4,
+    kInvalidDeviceId = -5,
+    kInvalidSystem = -6,
+    kInvalidSolverType = -7,
+    kInvalidInput = -8,
+    kInvalidArgument = -9,
+    kDeviceError = -10,
+};
+
+// Exception carrying an API error code; never crosses the C ABI.
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& what) : std::runtime_error(what), code(c) {}
+};
+
+#define PARODE_CUDA(call)                                                                          \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) {                                                                   \
+            if (e_ == cudaErrorMemoryAllocation)                                                   \
+                throw ::parode::Error(::parode::kNotEnoughResources,                               \
+                                      std::string(#call ": ") + cudaGetErrorString(e_));           \
+            throw ::parode::Error(::parode::kDeviceError, std::string(#call ": ") + cudaGetErrorString(e_)); \
+        }                                                                                          \
+    } while (0)
+
+enum Solver : int { kRK4 = 0, kABM = 1 };
+enum Precision : int { kFP64 = 0, kMixed = 1 };
+
+inline long round_up(long v, long q) { return (v + q - 1) / q * q; }
+inline long next_pow2(long v)
+{
+    long p = 1;
+    while (p < v) p <<= 1;
+    return p;
+}
+inline int ilog2(long v)
+{
+    int l = 0;
+    while ((1L << l) < v) ++l;
+    return l;
+}
+
+}  // namespace parode

@@ -1,0 +1,154 @@
+// host_math.cpp -- host FP64 set-up of a solve (see host_math.h).
+#include "host_math.h"
+
+#include <cmath>
+#include <cstring>
+
+namespace parode {
+
+namespace {
+
+// Z (r x c) = X (r x k) * Y (k x c), row-major.
+void gemm(int r, int k, int c, const double* X, const double* Y, double* Z)
+{
+    for (int i = 0; i < r; ++i) {
+        double* z = Z + (long)i * c;
+        for (int j = 0; j < c; ++j) z[j] = 0.0;
+        for (int q = 0; q < k; ++q) {
+            double x = X[(long)i * k + q];
+            const double* y = Y + (long)q * c;
+            for (int j = 0; j < c; ++j) z[j] += x * y[j];
+        }
+    }
+}
+
+void derivative(const SystemDesc& s, const double* x, const double* u, double* dx)
+{
+    for (int r = 0; r < s.n; ++r) {
+        double v = 0.0;
+        for (int c = 0; c < s.n; ++c) v += s.A[(long)r * s.n + c] * x[c];
+        if (!s.zeroB)
+            for (int c = 0; c < s.m; ++c) v += s.B[(long)r * s.m + c] * u[c];
+        dx[r] = v;
+    }
+}
+
+}  // namespace
+
+long num_outputs(int solver, double t0, double tEnd, double h, long* n_scan)
+{
+    if (!(h > 0.0)) return -1;
+    double ts = (solver == 1) ? t0 + 3.0 * h : t0;
+    double q = (tEnd - ts) / h;
+    if (!(q > -1.0) || q > 4.0e18) return -1;
+    long ns = (long)q + 1;
+    if (n_scan) *n_scan = ns;
+    return solver == 1 ? ns + 3 : ns;
+}
+
+void time_vector(int solver, double t0, double tEnd, double h, double* tv)
+{
+    long ns = 0;
+    long nt = num_outputs(solver, t0, tEnd, h, &ns);
+    if (nt <= 0) return;
+    long pre = nt - ns;
+    double ts = (solver == 1) ? t0 + 3.0 * h : t0;
+    float prev = (float)ts;
+    for (long i = 0; i < pre; ++i) tv[i] = (double)(float)(ts - (double)(pre - i) * h);
+    tv[pre] = (double)prev;
+    for (long i = 1; i < ns; ++i) {
+        prev = (float)((double)prev + h);
+        tv[pre + i] = (double)prev;
+    }
+}
+
+void discretise_rk4(int n, int m, const double* A, const double* B, double h, double* Phi, double* Bbar)
+{
+    // Abar = I + hA + h^2/2 A^2 + h^3/6 A^3 + h^4/24 A^4 and
+    // Bbar = [B1 B2 B3] with the coefficients of the reference
+    // (Sources/RungeKutta4thOrder.cpp:42-57).
+    std::vector<double> A2((size_t)n * n), A3((size_t)n * n), A4((size_t)n * n);
+    gemm(n, n, n, A, A, A2.data());
+    gemm(n, n, n, A2.data(), A, A3.data());
+    gemm(n, n, n, A, A3.data(), A4.data());
+    const double h2 = h * h, h3 = h * h * h, h4 = h * h * h * h;
+    for (long q = 0; q < (long)n * n; ++q) {
+        int i = (int)(q / n), j = (int)(q % n);
+        Phi[q] = (i == j ? 1.0 : 0.0) + h * A[q] + 0.5 * h2 * A2[q] + (1.0 / 6.0) * h3 * A3[q] +
+                 (1.0 / 24.0) * h4 * A4[q];
+    }
+    if (m <= 0) return;
+    std::vector<double> AB((size_t)n * m), A2B((size_t)n * m), A3B((size_t)n * m);
+    gemm(n, n, m, A, B, AB.data());
+    gemm(n, n, m, A2.data(), B, A2B.data());
+    gemm(n, n, m, A3.data(), B, A3B.data());
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < m; ++j) {
+            long q = (long)i * m + j;
+            double* row = Bbar + (long)i * 3 * m;
+            row[j] = (1.0 / 6.0) * (h * B[q] + h2 * AB[q] + 0.5 * h3 * A2B[q] + 0.25 * h4 * A3B[q]);
+            row[m + j] = (1.0 / 6.0) * (4.0 * h * B[q] + 2.0 * h2 * AB[q] + 0.5 * h3 * A2B[q]);
+            row[2 * m + j] = (1.0 / 6.0) * h * B[q];
+        }
+}
+
+void discretise_abm(int n, int m, const double* A, const double* B, double h, double* Phi, double* Bbar)
+{
+    // Companion map of the linear AB4-predictor / AM4-corrector step
+    // (reference Sources/AdamsMoulton.cpp:253-316).
+    const int N = 4 * n;
+    std::vector<double> A2((size_t)n * n);
+    gemm(n, n, n, A, A, A2.data());
+    const double h2 = h * h;
+    std::memset(Phi, 0, sizeof(double) * (size_t)N * N);
+    for (int r = 0; r < n; ++r) {
+        double* last = Phi + (long)(3 * n + r) * N;
+        for (int c = 0; c < n; ++c) {
+            long q = (long)r * n + c;
+            last[c] = (-81.0 * h2 / 576.0) * A2[q];
+            last[n + c] = (1.0 * h / 24.0) * A[q] + (333.0 * h2 / 576.0) * A2[q];
+            last[2 * n + c] = (-5.0 * h / 24.0) * A[q] + (-531.0 * h2 / 576.0) * A2[q];
+            last[3 * n + c] = (r == c ? 1.0 : 0.0) + (28.0 * h / 24.0) * A[q] + (495.0 * h2 / 576.0) * A2[q];
+        }
+        Phi[(long)r * N + n + r] = 1.0;
+        Phi[(long)(n + r) * N + 2 * n + r] = 1.0;
+        Phi[(long)(2 * n + r) * N + 3 * n + r] = 1.0;
+    }
+    if (m <= 0) return;
+    std::vector<double> AB((size_t)n * m);
+    gemm(n, n, m, A, B, AB.data());
+    for (int r = 0; r < n; ++r)
+        for (int c = 0; c < m; ++c) {
+            long q = (long)r * m + c;
+            double* row = Bbar + (long)r * 5 * m;
+            row[c] = (-81.0 * h2 / 576.0) * AB[q];
+            row[m + c] = (h / 24.0) * B[q] + (333.0 * h2 / 576.0) * AB[q];
+            row[2 * m + c] = (-5.0 * h / 24.0) * B[q] + (-531.0 * h2 / 576.0) * AB[q];
+            row[3 * m + c] = (19.0 * h / 24.0) * B[q] + (495.0 * h2 / 576.0) * AB[q];
+            row[4 * m + c] = (9.0 * h / 24.0) * B[q];
+        }
+}
+
+void abm_startup(const SystemDesc& s, const double* U9, double h, double* X0)
+{
+    const int n = s.n, m = s.m;
+    std::vector<double> x(s.x0), k1(n), k2(n), k3(n), k4(n), xt(n);
+    for (int r = 0; r < n; ++r) X0[r] = x[r];
+    for (int st = 1; st < 4; ++st) {
+        const double* u0 = U9 + (long)(2 * st - 2) * m;
+        const double* uh = U9 + (long)(2 * st - 1) * m;
+        const double* u1 = U9 + (long)(2 * st) * m;
+        derivative(s, x.data(), u0, k1.data());
+        for (int i = 0; i < n; ++i) xt[i] = x[i] + 0.5 * h * k1[i];
+        derivative(s, xt.data(), uh, k2.data());
+        for (int i = 0; i < n; ++i) xt[i] = x[i] + 0.5 * h * k2[i];
+        derivative(s, xt.data(), uh, k3.data());
+        for (int i = 0; i < n; ++i) xt[i] = x[i] + h * k3[i];
+        derivative(s, xt.data(), u1, k4.data());
+        for (int i = 0; i < n; ++i)
+            x[i] = x[i] + (h / 6.0) * k1[i] + (h / 3.0) * k2[i] + (h / 3.0) * k3[i] + (h / 6.0) * k4[i];
+        for (int r = 0; r < n; ++r) X0[(long)st * n + r] = x[r];
+    }
+}
+
+}  // namespace parode

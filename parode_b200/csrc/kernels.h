@@ -1,0 +1,49 @@
+// kernels.h -- host launchers of the device kernels (FP64 path).
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace parode {
+
+// Column addressing of the batched affine-level contraction:
+//   result(g, i) = sum_k P[i][k] * src(g, k) (+ acc(g, i))
+// src(g,k) = src[g*src_gs + k*src_ks], acc/dst/cpy likewise with (g, i).
+struct LevelArgs {
+    const double* P = nullptr;
+    long ldp = 0;
+    int Np = 0;          // rows of P == contraction length (multiple of 8)
+    long ncols = 0;
+    const double* src = nullptr;
+    long src_gs = 0, src_ks = 1;
+    const double* acc = nullptr;  // may be null (no accumulate)
+    long acc_gs = 0, acc_is = 1;
+    double* dst = nullptr;
+    long dst_gs = 0, dst_is = 1;
+    double* cpy = nullptr;  // down-sweep: cpy(g,i) <- old src(g,i)
+    long cpy_gs = 0, cpy_is = 1;
+};
+
+// One Blelloch level over all columns (up-sweep, down-sweep or P*P).
+void launch_affine_level(const LevelArgs& a, cudaStream_t s);
+
+// U[j*m + i] = sum_k a sin(2 pi f t_j + phi), t_j = base + dt*j, j < count.
+void launch_sinusoid_samples(double* U, int m, int K, const double* a, const double* f, const double* phi,
+                             double base, double dt, long count, cudaStream_t s);
+
+// Scan-vector initialisation with the forcing term Gamma_k (zero padding
+// for k >= T and for the components the solver leaves empty).
+void launch_forcing(double* V, int Np, int n, int m, int solver, const double* Bbar, const double* U, long T,
+                    long Tp, cudaStream_t s);
+
+// y[(ybase + k)*p + o] = C x_k + D u_k for k < count (x_k = V[k*Np + xoff ..]).
+void launch_output(double* Y, const double* V, int Np, int xoff, int n, int m, int p, const double* C,
+                   const double* D, int zeroC, int zeroD, const double* U, int ustride, int uoff, long count,
+                   long ybase, cudaStream_t s);
+
+// dst[0..N) = src[0..N)
+void launch_copy(double* dst, const double* src, long N, cudaStream_t s);
+
+// Kernel launches made by the last call of each launcher (for accounting).
+int launches_per_level();
+
+}  // namespace parode

@@ -1,0 +1,286 @@
+// solver.cpp -- plan set-up and execution (see solver.h).
+#include "solver.h"
+
+#include "common.h"
+#include "kernels.h"
+
+#include <algorithm>
+#include <cstring>
+
+namespace parode {
+
+Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex, int solver, double t0,
+           double tEnd, double h, const PlanOptions& opt)
+    : device_(device), sys_(sys), inputs_(inputs), opt_(opt), solver_(solver), t0_(t0), tEnd_(tEnd), h_(h)
+{
+    if (solver != kRK4 && solver != kABM) throw Error(kInvalidSolverType, "unknown solver type");
+    if (sys.n <= 0) throw Error(kInvalidSystem, "the system has no states");
+    if ((long)sys.A.size() < (long)sys.n * sys.n || (long)sys.x0.size() < sys.n)
+        throw Error(kInvalidSystem, "A or x0 too small");
+    if (!sys.zeroB && (sys.m <= 0 || (long)sys.B.size() < (long)sys.n * sys.m))
+        throw Error(kInvalidSystem, "B has the wrong size");
+    if (!sys.zeroC && (sys.p <= 0 || (long)sys.C.size() < (long)sys.p * sys.n))
+        throw Error(kInvalidSystem, "C has the wrong size");
+    if (!sys.zeroD && (sys.p <= 0 || sys.m <= 0 || (long)sys.D.size() < (long)sys.p * sys.m))
+        throw Error(kInvalidSystem, "D has the wrong size");
+    nOut_ = parode::num_outputs(solver, t0, tEnd, h, &nScan_);
+    if (nOut_ <= 0 || nScan_ <= 0) throw Error(kInvalidSystem, "empty time horizon");
+    p_ = sys.out_size();
+    // inputs are sampled whenever B or D is present (reference Kernels/u.cl)
+    mu_ = (!sys.zeroB || !sys.zeroD) ? sys.m : 0;
+    if (mu_ > 0) {
+        input_ = inputs ? inputs->get(uIndex) : nullptr;
+        if (!input_) throw Error(kInvalidInput, "uIndex does not name a registered input");
+    }
+    Ns_ = solver == kRK4 ? sys.n : 4 * sys.n;
+    Np_ = (int)round_up(Ns_, 8);
+    if (Np_ > 1024) throw Error(kInvalidSystem, "scan dimension above 1024 is not supported");
+    Tp_ = next_pow2(nScan_);
+    levels_ = ilog2(Tp_);
+    path_ = kPathLevel;
+
+    PARODE_CUDA(cudaSetDevice(device_));
+    PARODE_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+
+    // ---- host FP64 discretisation --------------------------------------
+    const int n = sys.n, mB = sys.zeroB ? 0 : sys.m;
+    const int W = solver == kRK4 ? 3 : 5;
+    std::vector<double> Phi((size_t)Ns_ * Ns_), Bbar((size_t)n * W * std::max(mB, 1), 0.0);
+    if (solver == kRK4)
+        discretise_rk4(n, mB, sys.A.data(), mB ? sys.B.data() : nullptr, h, Phi.data(), Bbar.data());
+    else
+        discretise_abm(n, mB, sys.A.data(), mB ? sys.B.data() : nullptr, h, Phi.data(), Bbar.data());
+    std::vector<double> PhiP((size_t)Np_ * Np_, 0.0), X0((size_t)Np_, 0.0);
+    for (int r = 0; r < Ns_; ++r)
+        std::memcpy(&PhiP[(size_t)r * Np_], &Phi[(size_t)r * Ns_], sizeof(double) * Ns_);
+
+    // ---- device buffers ---------------------------------------------------
+    long npow = std::max(levels_, 1);
+    alloc(&dPow_, npow * (long)Np_ * Np_);
+    alloc(&dBbar_, (long)Bbar.size());
+    alloc(&dC_, std::max<long>(1, (long)p_ * n));
+    alloc(&dD_, std::max<long>(1, (long)p_ * std::max(sys.m, 1)));
+    alloc(&dX0_, Np_);
+    alloc(&dV_, Tp_ * (long)Np_);
+    alloc(&dY_, nOut_ * (long)p_);
+    if (solver == kRK4) {
+        nU_ = 2 * nScan_ + 1;
+        u_base_ = t0;
+        u_dt_ = 0.5 * h;
+    } else {
+        // ABM scan inputs on the grid (t0 + 3h) - 3h + j h
+        // (reference Sources/AdamsMoulton.cpp:426-432 with FP64 time)
+        nU_ = nScan_ + 4;
+        u_base_ = (t0 + 3.0 * h) - 3.0 * h;
+        u_dt_ = h;
+    }
+    if (mu_ > 0) alloc(&dU_, nU_ * (long)mu_);
+    PARODE_CUDA(cudaMemcpyAsync(dPow_, PhiP.data(), sizeof(double) * PhiP.size(), cudaMemcpyHostToDevice, stream_));
+    PARODE_CUDA(cudaMemcpyAsync(dBbar_, Bbar.data(), sizeof(double) * Bbar.size(), cudaMemcpyHostToDevice, stream_));
+    if (!sys.zeroC)
+        PARODE_CUDA(cudaMemcpyAsync(dC_, sys.C.data(), sizeof(double) * (size_t)p_ * n, cudaMemcpyHostToDevice,
+                                    stream_));
+    if (!sys.zeroD)
+        PARODE_CUDA(cudaMemcpyAsync(dD_, sys.D.data(), sizeof(double) * (size_t)p_ * sys.m,
+                                    cudaMemcpyHostToDevice, stream_));
+
+    // ---- initial scan state -------------------------------------------------
+    if (solver == kRK4) {
+        for (int r = 0; r < n; ++r) X0[r] = sys.x0[r];
+    } else {
+        // start-up inputs u(t0 + j h/2), j = 0..8, evaluated on the device
+        // as the reference does (Sources/AdamsMoulton.cpp:51-88)
+        std::vector<double> U9((size_t)9 * std::max(sys.m, 1), 0.0);
+        if (mu_ > 0) {
+            double* dU9 = nullptr;
+            alloc(&dU9, 9L * mu_);
+            inputs_->fill(input_, device_, dU9, mu_, t0, 0.5 * h, 9, opt_.input_double, stream_);
+            PARODE_CUDA(cudaMemcpyAsync(U9.data(), dU9, sizeof(double) * 9 * mu_, cudaMemcpyDeviceToHost, stream_));
+            PARODE_CUDA(cudaStreamSynchronize(stream_));
+        }
+        SystemDesc s0 = sys;
+        if (s0.zeroB) s0.m = 0;
+        std::vector<double> Xs((size_t)4 * n);
+        abm_startup(s0, U9.data(), h, Xs.data());
+        for (int r = 0; r < 4 * n; ++r) X0[r] = Xs[r];
+        // outputs 0..2 from the start-up states (Sources/GPUFixedStepIterative.cpp:150-172)
+        ypre_.assign((size_t)3 * p_, 0.0);
+        for (int i = 0; i < 3; ++i) {
+            const double* x = &Xs[(size_t)i * n];
+            const double* u = &U9[(size_t)(2 * i) * std::max(sys.m, 1)];
+            for (int o = 0; o < p_; ++o) {
+                double v = 0.0;
+                if (sys.zeroC && sys.zeroD) {
+                    v = x[o];
+                } else {
+                    if (!sys.zeroC)
+                        for (int c = 0; c < n; ++c) v += sys.C[(size_t)o * n + c] * x[c];
+                    if (!sys.zeroD)
+                        for (int c = 0; c < sys.m; ++c) v += sys.D[(size_t)o * sys.m + c] * u[c];
+                }
+                ypre_[(size_t)i * p_ + o] = v;
+            }
+        }
+        alloc(&dYpre_, 3L * p_);
+        PARODE_CUDA(cudaMemcpyAsync(dYpre_, ypre_.data(), sizeof(double) * ypre_.size(), cudaMemcpyHostToDevice,
+                                    stream_));
+    }
+    PARODE_CUDA(cudaMemcpyAsync(dX0_, X0.data(), sizeof(double) * Np_, cudaMemcpyHostToDevice, stream_));
+    PARODE_CUDA(cudaStreamSynchronize(stream_));
+}
+
+Plan::~Plan()
+{
+    cudaSetDevice(device_);
+    if (stream_) cudaStreamSynchronize(stream_);
+    for (cudaEvent_t e : events_) cudaEventDestroy(e);
+    for (double* p : bufs_) cudaFree(p);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Plan::alloc(double** p, long n)
+{
+    *p = nullptr;
+    cudaError_t e = cudaMalloc((void**)p, sizeof(double) * (size_t)std::max<long>(n, 1));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Error(kNotEnoughResources, "device allocation failed");
+    }
+    bufs_.push_back(*p);
+}
+
+void Plan::set_profiling(bool on) { profiling_ = on; }
+
+void Plan::mark(const char* stage, cudaStream_t s)
+{
+    if (!profiling_) return;
+    size_t k = marks_.size();
+    if (events_.size() <= k) {
+        cudaEvent_t e;
+        PARODE_CUDA(cudaEventCreate(&e));
+        events_.push_back(e);
+    }
+    marks_.push_back(stage);
+    PARODE_CUDA(cudaEventRecord(events_[k], s));
+}
+
+std::vector<std::pair<std::string, float>> Plan::stage_times()
+{
+    std::vector<std::pair<std::string, float>> out;
+    if (marks_.size() < 2) return out;
+    PARODE_CUDA(cudaEventSynchronize(events_[marks_.size() - 1]));
+    for (size_t k = 1; k < marks_.size(); ++k) {
+        float ms = 0.f;
+        PARODE_CUDA(cudaEventElapsedTime(&ms, events_[k - 1], events_[k]));
+        out.emplace_back(marks_[k], ms);
+    }
+    return out;
+}
+
+void Plan::fill_inputs(cudaStream_t s)
+{
+    if (mu_ > 0) inputs_->fill(input_, device_, dU_, mu_, u_base_, u_dt_, nU_, opt_.input_double, s);
+}
+
+void Plan::execute(double* y, cudaStream_t s)
+{
+    PARODE_CUDA(cudaSetDevice(device_));
+    if (!s) s = stream_;
+    double* Y = y ? y : dY_;
+    const long Np = Np_;
+    const int n = sys_.n;
+    int launches = 0;
+    marks_.clear();
+    mark("start", s);
+
+    fill_inputs(s);
+    launches += mu_ > 0 ? 1 : 0;
+    mark("inputs", s);
+    launch_forcing(dV_, Np_, n, sys_.zeroB ? 0 : sys_.m, solver_, dBbar_, dU_, nScan_, Tp_, s);
+    ++launches;
+    mark("forcing", s);
+
+    // power table P_l = Phi^(2^l): the up-sweep matrix of every node at level
+    // l (reference Kernels/MMKernelScanUpsweep.cl:24-53 computes these per node)
+    for (int l = 1; l < levels_; ++l) {
+        LevelArgs a;
+        a.P = dPow_ + (long)(l - 1) * Np * Np;
+        a.ldp = Np;
+        a.Np = Np_;
+        a.ncols = Np;
+        a.src = a.P;
+        a.src_gs = 1;
+        a.src_ks = Np;
+        a.dst = dPow_ + (long)l * Np * Np;
+        a.dst_gs = 1;
+        a.dst_is = Np;
+        launch_affine_level(a, s);
+        ++launches;
+    }
+    mark("power_table", s);
+    // up-sweep: v[k] = P_l v[k-d] + v[k] (reference Kernels/MVVKernelScanUpsweep.cl:25-48)
+    for (int l = 0; l < levels_; ++l) {
+        long d = 1L << l;
+        LevelArgs a;
+        a.P = dPow_ + (long)l * Np * Np;
+        a.ldp = Np;
+        a.Np = Np_;
+        a.ncols = Tp_ / (2 * d);
+        a.src = dV_ + (d - 1) * Np;
+        a.src_gs = 2 * d * Np;
+        a.acc = dV_ + (2 * d - 1) * Np;
+        a.acc_gs = 2 * d * Np;
+        a.dst = dV_ + (2 * d - 1) * Np;
+        a.dst_gs = 2 * d * Np;
+        launch_affine_level(a, s);
+        ++launches;
+    }
+    // exclusive scan seeded with the initial state at the root (the
+    // reference's carry (I, x0), Sources/GPUFixedStepIterative.cpp:191-198,327-330)
+    launch_copy(dV_ + (Tp_ - 1) * Np, dX0_, Np, s);
+    ++launches;
+    // down-sweep: v[k] <- P_l v[k] + v[k-d], v[k-d] <- v[k]
+    // (reference Kernels/MVVKernelScanDownsweep.cl:25-48 and RootCopyKernelScanDownsweep.cl:11-19)
+    for (int l = levels_ - 1; l >= 0; --l) {
+        long d = 1L << l;
+        LevelArgs a;
+        a.P = dPow_ + (long)l * Np * Np;
+        a.ldp = Np;
+        a.Np = Np_;
+        a.ncols = Tp_ / (2 * d);
+        a.src = dV_ + (2 * d - 1) * Np;
+        a.src_gs = 2 * d * Np;
+        a.acc = dV_ + (d - 1) * Np;
+        a.acc_gs = 2 * d * Np;
+        a.dst = dV_ + (2 * d - 1) * Np;
+        a.dst_gs = 2 * d * Np;
+        a.cpy = dV_ + (d - 1) * Np;
+        a.cpy_gs = 2 * d * Np;
+        launch_affine_level(a, s);
+        ++launches;
+    }
+    mark("sweeps", s);
+    // outputs (reference Kernels/SystemOutput.cl with strides (1,0)/(2,0) for
+    // RK4 and (4,3)/(1,3) for ABM, Sources/RungeKutta4thOrder.cpp:209,
+    // Sources/AdamsMoulton.cpp:398)
+    if (solver_ == kRK4) {
+        launch_output(Y, dV_, Np_, 0, n, mu_, p_, dC_, dD_, sys_.zeroC, sys_.zeroD, dU_, 2, 0, nScan_, 0, s);
+    } else {
+        launch_output(Y, dV_, Np_, 3 * n, n, mu_, p_, dC_, dD_, sys_.zeroC, sys_.zeroD, dU_, 1, 3, nScan_, 3, s);
+        PARODE_CUDA(cudaMemcpyAsync(Y, dYpre_, sizeof(double) * 3 * p_, cudaMemcpyDeviceToDevice, s));
+    }
+    ++launches;
+    mark("output", s);
+    launches_ = launches;
+    last_y_ = Y;
+}
+
+void Plan::get_output(double* t, double* y)
+{
+    PARODE_CUDA(cudaSetDevice(device_));
+    PARODE_CUDA(cudaDeviceSynchronize());
+    if (y) PARODE_CUDA(cudaMemcpy(y, last_y_ ? last_y_ : dY_, sizeof(double) * nOut_ * p_, cudaMemcpyDeviceToHost));
+    if (t) time_vector(solver_, t0_, tEnd_, h_, t);
+}
+
+}  // namespace parode

@@ -1,0 +1,83 @@
+// solver.h -- a device-resident solve of one LTI system (a "plan").
+//
+// Replaces the reference's solver objects (GPUODESolverFixedStepIterative and
+// its RungeKutta4thOrder / AdamsMoulton subclasses,
+// Sources/GPUFixedStepIterative.cpp:131-466): set-up on the host in FP64,
+// every per-step stage on the device, no host round trip inside a solve.
+#pragma once
+
+#include "host_math.h"
+#include "inputs.h"
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <utility>
+#include <vector>
+
+namespace parode {
+
+enum Path : int { kPathAuto = 0, kPathLevel = 1, kPathBlocked = 2 };
+
+struct PlanOptions {
+    int precision = 0;  // Precision
+    int path = kPathAuto;
+    bool input_double = true;  // fType of a user input function: double (true) or float
+};
+
+class Plan {
+public:
+    Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex, int solver, double t0, double tEnd,
+         double h, const PlanOptions& opt);
+    ~Plan();
+    Plan(const Plan&) = delete;
+    Plan& operator=(const Plan&) = delete;
+
+    // Enqueue one solve on `s` (nullptr = the plan's stream); y (device,
+    // num_outputs() x channels() doubles) or nullptr for the plan's buffer.
+    void execute(double* y, cudaStream_t s);
+    // Synchronise and copy the last result (and the time vector) to the host.
+    void get_output(double* t, double* y);
+
+    long num_outputs() const { return nOut_; }
+    int channels() const { return p_; }
+    int launch_count() const { return launches_; }
+    int device() const { return device_; }
+    cudaStream_t stream() const { return stream_; }
+    const double* device_output() const { return dY_; }
+    int path() const { return path_; }
+
+    // Optional stage timing with CUDA events on the execution stream.
+    void set_profiling(bool on);
+    // Stage names and milliseconds of the last profiled execute (synchronises).
+    std::vector<std::pair<std::string, float>> stage_times();
+
+private:
+    void alloc(double** p, long n);
+    void mark(const char* stage, cudaStream_t s);
+    void fill_inputs(cudaStream_t s);
+
+    int device_ = 0;
+    cudaStream_t stream_ = nullptr;
+    SystemDesc sys_;
+    InputRegistry* inputs_ = nullptr;
+    InputEntry* input_ = nullptr;
+    PlanOptions opt_;
+    int solver_ = 0;
+    double t0_ = 0, tEnd_ = 0, h_ = 0;
+    long nOut_ = 0, nScan_ = 0, Tp_ = 1, nU_ = 0;
+    int Ns_ = 0, Np_ = 0, p_ = 0, mu_ = 0, levels_ = 0;
+    int path_ = kPathLevel;
+    int launches_ = 0;
+    double u_base_ = 0, u_dt_ = 0;
+    std::vector<double> ypre_;  // ABM: outputs 0..2 computed on the host
+    std::vector<double*> bufs_;
+    double *dPow_ = nullptr, *dBbar_ = nullptr, *dC_ = nullptr, *dD_ = nullptr, *dX0_ = nullptr;
+    double *dU_ = nullptr, *dV_ = nullptr, *dY_ = nullptr, *dYpre_ = nullptr;
+    double* last_y_ = nullptr;
+    bool profiling_ = false;
+    std::vector<cudaEvent_t> events_;
+    std::vector<std::string> marks_;
+};
+
+}  // namespace parode
