@@ -110,6 +110,23 @@ int InputRegistry::add_sinusoid(int m, int K, const double* a, const double* f, 
     return (int)entries_.size() - 1;
 }
 
+const double* InputRegistry::sinusoid_device(InputEntry* e, int device)
+{
+    if ((int)e->dparams.size() <= device) e->dparams.resize(device + 1, nullptr);
+    if (!e->dparams[device]) {
+        long q = (long)e->m * e->K;
+        double* d = nullptr;
+        PARODE_CUDA(cudaMalloc(&d, sizeof(double) * 3 * q));
+        std::vector<double> h(3 * q);
+        std::memcpy(h.data(), e->a.data(), sizeof(double) * q);
+        std::memcpy(h.data() + q, e->f.data(), sizeof(double) * q);
+        std::memcpy(h.data() + 2 * q, e->phi.data(), sizeof(double) * q);
+        PARODE_CUDA(cudaMemcpy(d, h.data(), sizeof(double) * 3 * q, cudaMemcpyHostToDevice));
+        e->dparams[device] = d;
+    }
+    return e->dparams[device];
+}
+
 InputEntry* InputRegistry::get(int idx)
 {
     if (idx < 0 || idx >= (int)entries_.size()) return nullptr;
@@ -122,20 +139,8 @@ void InputRegistry::fill(InputEntry* e, int device, double* U, int m, double bas
     if (m <= 0 || count <= 0) return;
     if (e->kind == InputEntry::kSinusoid) {
         if (e->m < m) throw Error(kInvalidInput, "sinusoid input has fewer channels than the system");
-        if ((int)e->dparams.size() <= device) e->dparams.resize(device + 1, nullptr);
-        if (!e->dparams[device]) {
-            long q = (long)e->m * e->K;
-            double* d = nullptr;
-            PARODE_CUDA(cudaMalloc(&d, sizeof(double) * 3 * q));
-            std::vector<double> h(3 * q);
-            std::memcpy(h.data(), e->a.data(), sizeof(double) * q);
-            std::memcpy(h.data() + q, e->f.data(), sizeof(double) * q);
-            std::memcpy(h.data() + 2 * q, e->phi.data(), sizeof(double) * q);
-            PARODE_CUDA(cudaMemcpy(d, h.data(), sizeof(double) * 3 * q, cudaMemcpyHostToDevice));
-            e->dparams[device] = d;
-        }
         long q = (long)e->m * e->K;
-        const double* d = e->dparams[device];
+        const double* d = sinusoid_device(e, device);
         // the kernel indexes parameters as i*K + k for i < m, so a sinusoid
         // input wider than the system is read from its first m channels
         launch_sinusoid_samples(U, m, e->K, d, d + q, d + 2 * q, base, dt, count, s);

@@ -43,6 +43,8 @@ public:
     // `double_type` selects the fType = double variant of a user function.
     void fill(InputEntry* e, int device, double* U, int m, double base, double dt, long count, bool double_type,
               cudaStream_t s);
+    // Device copy of a sinusoid input's parameters: a | f | phi, m*K each.
+    const double* sinusoid_device(InputEntry* e, int device);
 
 private:
     void compile(InputEntry* e, int variant);

@@ -38,9 +38,35 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
     Tp_ = next_pow2(nScan_);
     levels_ = ilog2(Tp_);
     path_ = kPathLevel;
+    {
+        const bool can_block = blocked_shape(Ns_, mu_, solver, &shape_);
+        if (opt.path == kPathBlocked && !can_block)
+            throw Error(kInvalidArgument, "the blocked path supports scan dimensions up to 64");
+        if (opt.path != kPathLevel && can_block) path_ = kPathBlocked;
+    }
+    if (path_ == kPathBlocked) {
+        Np_ = shape_.NP;
+        ntiles_ = (nScan_ + shape_.S - 1) / shape_.S;
+        nblocks_ = ntiles_ * (shape_.S / shape_.B);
+        long c = nblocks_;
+        int lev = shape_.R;
+        while (c > shape_.S_items) {
+            c = (c + shape_.B - 1) / shape_.B;
+            lev += shape_.R;
+        }
+        levels_ = std::max(lev + ilog2(next_pow2(c)), shape_.R);
+        // input samples are produced by their own wide kernel, overlapped
+        // with the power-table kernel, rather than inside the leaf (where the
+        // FP64 sin evaluations would compete with the scan for issue slots)
+        gen_ = false;
+        stage_bytes_ = blocked_leaf_stage_bytes(shape_, sys.n, mu_, p_, solver);
+    }
+    PARODE_CUDA(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_));
 
     PARODE_CUDA(cudaSetDevice(device_));
     PARODE_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    PARODE_CUDA(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
+    for (auto& e : fork_) PARODE_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
 
     // ---- host FP64 discretisation --------------------------------------
     const int n = sys.n, mB = sys.zeroB ? 0 : sys.m;
@@ -61,7 +87,27 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
     alloc(&dC_, std::max<long>(1, (long)p_ * n));
     alloc(&dD_, std::max<long>(1, (long)p_ * std::max(sys.m, 1)));
     alloc(&dX0_, Np_);
-    alloc(&dV_, Tp_ * (long)Np_);
+    if (path_ == kPathLevel) {
+        alloc(&dV_, Tp_ * (long)Np_);
+    } else {
+        alloc(&dG_, nblocks_ * (long)Np_);
+        alloc(&dWork_, blocked_items_scratch(shape_, nblocks_) * (long)Np_);
+        alloc(&dCP_, (long)shape_.B * p_ * Np_);
+        alloc(&dCext_, (long)p_ * Np_);
+        // output rows of the scan state: C at the state block (the last n of
+        // the ABM companion state), or the state itself when C and D are absent
+        std::vector<double> Cext((size_t)p_ * Np_, 0.0);
+        const int xoff = solver == kRK4 ? 0 : 3 * n;
+        for (int o = 0; o < p_; ++o)
+            for (int c = 0; c < n; ++c) {
+                double v = 0.0;
+                if (!sys.zeroC) v = sys.C[(size_t)o * n + c];
+                else if (sys.zeroD) v = (o == c) ? 1.0 : 0.0;
+                Cext[(size_t)o * Np_ + xoff + c] = v;
+            }
+        PARODE_CUDA(cudaMemcpyAsync(dCext_, Cext.data(), sizeof(double) * Cext.size(), cudaMemcpyHostToDevice,
+                                    stream_));
+    }
     alloc(&dY_, nOut_ * (long)p_);
     if (solver == kRK4) {
         nU_ = 2 * nScan_ + 1;
@@ -74,7 +120,7 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
         u_base_ = (t0 + 3.0 * h) - 3.0 * h;
         u_dt_ = h;
     }
-    if (mu_ > 0) alloc(&dU_, nU_ * (long)mu_);
+    if (mu_ > 0 && !gen_) alloc(&dU_, nU_ * (long)mu_);
     PARODE_CUDA(cudaMemcpyAsync(dPow_, PhiP.data(), sizeof(double) * PhiP.size(), cudaMemcpyHostToDevice, stream_));
     PARODE_CUDA(cudaMemcpyAsync(dBbar_, Bbar.data(), sizeof(double) * Bbar.size(), cudaMemcpyHostToDevice, stream_));
     if (!sys.zeroC)
@@ -134,6 +180,10 @@ Plan::~Plan()
     cudaSetDevice(device_);
     if (stream_) cudaStreamSynchronize(stream_);
     for (cudaEvent_t e : events_) cudaEventDestroy(e);
+    if (side_) cudaStreamSynchronize(side_);
+    for (cudaEvent_t e : fork_)
+        if (e) cudaEventDestroy(e);
+    if (side_) cudaStreamDestroy(side_);
     for (double* p : bufs_) cudaFree(p);
     if (stream_) cudaStreamDestroy(stream_);
 }
@@ -186,6 +236,10 @@ void Plan::execute(double* y, cudaStream_t s)
 {
     PARODE_CUDA(cudaSetDevice(device_));
     if (!s) s = stream_;
+    if (path_ == kPathBlocked) {
+        execute_blocked(y ? y : dY_, s);
+        return;
+    }
     double* Y = y ? y : dY_;
     const long Np = Np_;
     const int n = sys_.n;
@@ -271,6 +325,83 @@ void Plan::execute(double* y, cudaStream_t s)
     }
     ++launches;
     mark("output", s);
+    launches_ = launches;
+    last_y_ = Y;
+}
+
+void Plan::execute_blocked(double* Y, cudaStream_t s)
+{
+    int launches = 0;
+    marks_.clear();
+    mark("start", s);
+    // Two streams: the side stream produces the input samples while the
+    // main stream squares the leaf's powers P_1..P_{R-1} (one CTA), then
+    // squares the carry's powers P_R.. (one CTA) while the leaf runs on the
+    // other SMs.  Events fork from and join back into the caller's stream.
+    PARODE_CUDA(cudaEventRecord(fork_[0], s));
+    PARODE_CUDA(cudaStreamWaitEvent(side_, fork_[0], 0));
+    if (mu_ > 0 && !gen_) {
+        fill_inputs(side_);
+        ++launches;
+    }
+    PARODE_CUDA(cudaEventRecord(fork_[1], side_));
+    launch_blocked_tables(shape_, dPow_, 1, shape_.R, dCP_, dCext_, p_, s);
+    ++launches;
+    PARODE_CUDA(cudaEventRecord(fork_[2], s));
+    PARODE_CUDA(cudaStreamWaitEvent(side_, fork_[2], 0));
+    const bool more_levels = levels_ > shape_.R;
+    if (more_levels) {
+        launch_blocked_tables(shape_, dPow_, shape_.R, levels_, nullptr, nullptr, p_, side_);
+        ++launches;
+    }
+    PARODE_CUDA(cudaEventRecord(fork_[3], side_));
+    PARODE_CUDA(cudaStreamWaitEvent(s, fork_[1], 0));
+    mark("inputs+tables", s);
+
+    LeafArgs a;
+    a.solver = solver_;
+    a.n = sys_.n;
+    a.m = mu_;
+    a.p = p_;
+    a.zeroB = sys_.zeroB;
+    a.zeroC = sys_.zeroC;
+    a.zeroD = sys_.zeroD;
+    a.nScan = nScan_;
+    a.ntiles = ntiles_;
+    a.ybase = solver_ == kRK4 ? 0 : 3;
+    a.P = dPow_;
+    a.Bbar = dBbar_;
+    a.C = dC_;
+    a.D = dD_;
+    a.U = dU_;
+    a.gen = gen_ ? 1 : 0;
+    if (gen_) {
+        const double* d = inputs_->sinusoid_device(input_, device_);
+        const long q = (long)input_->m * input_->K;
+        a.sa = d;
+        a.sf = d + q;
+        a.sphi = d + 2 * q;
+        a.K = input_->K;
+    }
+    a.u_base = u_base_;
+    a.u_dt = u_dt_;
+    a.Y = Y;
+    a.G = dG_;
+    a.stage = stage_bytes_ > 0 ? 1 : 0;
+    // one SM stays free for the side stream's power-table kernel
+    launch_blocked_leaf(shape_, a, more_levels ? std::max(1, sms_ - 1) : sms_, s);
+    ++launches;
+    mark("leaf", s);
+    PARODE_CUDA(cudaStreamWaitEvent(s, fork_[3], 0));
+    // exclusive scan of the block aggregates, seeded with the initial state
+    launches += launch_blocked_carry(shape_, dG_, nblocks_, shape_.R, dPow_, dX0_, dWork_, sms_, s);
+    mark("carry", s);
+    // y += C Phi^j X_block
+    launch_blocked_fixup(shape_, Y, a.ybase, nScan_, p_, dCP_, dG_, s);
+    ++launches;
+    if (solver_ == kABM)
+        PARODE_CUDA(cudaMemcpyAsync(Y, dYpre_, sizeof(double) * 3 * p_, cudaMemcpyDeviceToDevice, s));
+    mark("fixup", s);
     launches_ = launches;
     last_y_ = Y;
 }

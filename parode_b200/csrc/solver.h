@@ -6,6 +6,7 @@
 // every per-step stage on the device, no host round trip inside a solve.
 #pragma once
 
+#include "blocked.h"
 #include "host_math.h"
 #include "inputs.h"
 
@@ -55,6 +56,7 @@ public:
 private:
     void alloc(double** p, long n);
     void mark(const char* stage, cudaStream_t s);
+    void execute_blocked(double* Y, cudaStream_t s);
     void fill_inputs(cudaStream_t s);
 
     int device_ = 0;
@@ -75,6 +77,14 @@ private:
     double *dPow_ = nullptr, *dBbar_ = nullptr, *dC_ = nullptr, *dD_ = nullptr, *dX0_ = nullptr;
     double *dU_ = nullptr, *dV_ = nullptr, *dY_ = nullptr, *dYpre_ = nullptr;
     double* last_y_ = nullptr;
+    BlockedShape shape_;
+    long ntiles_ = 0, nblocks_ = 0;
+    bool gen_ = false;
+    int sms_ = 148;
+    double *dG_ = nullptr, *dWork_ = nullptr, *dCP_ = nullptr, *dCext_ = nullptr;
+    size_t stage_bytes_ = 0;
+    cudaStream_t side_ = nullptr;
+    cudaEvent_t fork_[4] = {nullptr, nullptr, nullptr, nullptr};
     bool profiling_ = false;
     std::vector<cudaEvent_t> events_;
     std::vector<std::string> marks_;
