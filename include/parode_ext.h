@@ -77,6 +77,11 @@ long long ParODE_PlanNumOutputs(const ParODE_Plan* plan);
 int ParODE_PlanNumOutputChannels(const ParODE_Plan* plan);
 /* Device kernel launches one PlanExecute enqueues (for launch accounting). */
 int ParODE_PlanLaunchCount(const ParODE_Plan* plan);
+/* Precision form the plan actually runs (PARODE_PRECISION_*): the mixed form
+ * falls back to FP64 for shapes its tensor-core leaf does not cover. */
+int ParODE_PlanPrecision(const ParODE_Plan* plan);
+/* Sweep organisation: 1 level-synchronous, 2 blocked. */
+int ParODE_PlanPath(const ParODE_Plan* plan);
 void ParODE_PlanDestroy(ParODE_Plan* plan);
 /* Stage timing: when enabled, PlanExecute records CUDA events between its
  * stages on the execution stream.  PlanStageTimes synchronises on the last

@@ -92,6 +92,8 @@ def _load():
     L.ParODE_PlanNumOutputChannels.argtypes = [C.c_void_p]
     L.ParODE_PlanLaunchCount.argtypes = [C.c_void_p]
     L.ParODE_PlanDestroy.argtypes = [C.c_void_p]
+    L.ParODE_PlanPrecision.argtypes = [C.c_void_p]
+    L.ParODE_PlanPath.argtypes = [C.c_void_p]
     L.ParODE_PlanSetProfiling.argtypes = [C.c_void_p, C.c_int, ip]
     L.ParODE_PlanStageTimes.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_int, C.c_char_p, C.c_int, ip]
     L.ParODE_PlanStageTimes.restype = C.c_int
@@ -280,6 +282,15 @@ class Plan:
         _check(e, "ParODE_PlanStageTimes")
         labels = names.value.decode().split("\n")
         return [(labels[i], float(ms[i])) for i in range(min(n, 64))]
+
+    @property
+    def precision(self) -> int:
+        """Precision form actually used (FP64 or MIXED)."""
+        return int(lib.ParODE_PlanPrecision(self._h))
+
+    @property
+    def path(self) -> int:
+        return int(lib.ParODE_PlanPath(self._h))
 
     @property
     def launch_count(self) -> int:

@@ -482,6 +482,10 @@ int ParODE_PlanNumOutputChannels(const ParODE_Plan* plan) { return plan && plan-
 
 int ParODE_PlanLaunchCount(const ParODE_Plan* plan) { return plan && plan->plan ? plan->plan->launch_count() : 0; }
 
+int ParODE_PlanPrecision(const ParODE_Plan* plan) { return plan && plan->plan ? plan->plan->precision_used() : -1; }
+
+int ParODE_PlanPath(const ParODE_Plan* plan) { return plan && plan->plan ? plan->plan->path() : -1; }
+
 void ParODE_PlanDestroy(ParODE_Plan* plan) { delete plan; }
 
 void ParODE_PlanSetProfiling(ParODE_Plan* plan, int enable, int nErr[])

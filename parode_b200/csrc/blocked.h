@@ -49,7 +49,13 @@ struct LeafArgs {
     double u_base = 0, u_dt = 0;   // sample time base + dt * j
     double* Y = nullptr;           // outputs (rows ybase .. ybase + nScan)
     double* G = nullptr;           // block aggregates (ntiles*S/B x NP)
+    int* status = nullptr;         // set non-zero by a device wait that gave up
 };
+
+// Mixed-precision (3xTF32 tcgen05) leaf: shared-memory bytes, or 0 when the
+// shape is not supported (NP < 16 or too large).
+size_t blocked_leaf_tc_bytes(const BlockedShape& sh, int n, int m, int p, int solver);
+void launch_blocked_leaf_tc(const BlockedShape& sh, const LeafArgs& a, int grid, cudaStream_t s);
 
 // Shared-memory bytes of the leaf with Bbar, C and D staged, or 0 when they
 // do not fit next to the tile.

@@ -60,6 +60,39 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
         // FP64 sin evaluations would compete with the scan for issue slots)
         gen_ = false;
         stage_bytes_ = blocked_leaf_stage_bytes(shape_, sys.n, mu_, p_, solver);
+        // the mixed form runs the leaf on the tensor cores (3xTF32) when the
+        // shape allows it, with the longest tile that fits its shared-memory
+        // layout; otherwise the solve stays in FP64
+        if (opt.precision == kMixed) {
+            // largest (levels per block, tile) that fits: the tensor-core
+            // operands need bucket starts on 8-row boundaries (S >= 4B) and
+            // M = 128 slices (S >= 128)
+            BlockedShape tc = shape_;
+            bool fits = false;
+            for (int R = shape_.R; R >= 2 && !fits; --R) {
+                tc = shape_;
+                tc.R = R;
+                tc.B = 1 << R;
+                tc.items_smem = (size_t)R * tc.NP * tc.NP * sizeof(double) + (size_t)tc.S_items * tc.NP * sizeof(double);
+                for (int S = shape_.S; S >= std::max(128, 4 * tc.B) && !fits; S >>= 1) {
+                    tc.S = S;
+                    fits = blocked_leaf_tc_bytes(tc, sys.n, mu_, p_, solver) > 0;
+                }
+            }
+            if (fits) {
+                shape_ = tc;
+                precision_used_ = kMixed;
+                ntiles_ = (nScan_ + shape_.S - 1) / shape_.S;
+                nblocks_ = ntiles_ * (shape_.S / shape_.B);
+                long c2 = nblocks_;
+                int lev2 = shape_.R;
+                while (c2 > shape_.S_items) {
+                    c2 = (c2 + shape_.B - 1) / shape_.B;
+                    lev2 += shape_.R;
+                }
+                levels_ = std::max(lev2 + ilog2(next_pow2(c2)), shape_.R);
+            }
+        }
     }
     PARODE_CUDA(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_));
 
@@ -87,6 +120,12 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
     alloc(&dC_, std::max<long>(1, (long)p_ * n));
     alloc(&dD_, std::max<long>(1, (long)p_ * std::max(sys.m, 1)));
     alloc(&dX0_, Np_);
+    {
+        double* st = nullptr;
+        alloc(&st, 1);
+        dStatus_ = reinterpret_cast<int*>(st);
+        PARODE_CUDA(cudaMemsetAsync(dStatus_, 0, sizeof(int), stream_));
+    }
     if (path_ == kPathLevel) {
         alloc(&dV_, Tp_ * (long)Np_);
     } else {
@@ -388,8 +427,11 @@ void Plan::execute_blocked(double* Y, cudaStream_t s)
     a.Y = Y;
     a.G = dG_;
     a.stage = stage_bytes_ > 0 ? 1 : 0;
+    a.status = dStatus_;
     // one SM stays free for the side stream's power-table kernel
-    launch_blocked_leaf(shape_, a, more_levels ? std::max(1, sms_ - 1) : sms_, s);
+    const int grid = more_levels ? std::max(1, sms_ - 1) : sms_;
+    if (precision_used_ == kMixed) launch_blocked_leaf_tc(shape_, a, grid, s);
+    else launch_blocked_leaf(shape_, a, grid, s);
     ++launches;
     mark("leaf", s);
     PARODE_CUDA(cudaStreamWaitEvent(s, fork_[3], 0));
@@ -410,6 +452,9 @@ void Plan::get_output(double* t, double* y)
 {
     PARODE_CUDA(cudaSetDevice(device_));
     PARODE_CUDA(cudaDeviceSynchronize());
+    int status = 0;
+    PARODE_CUDA(cudaMemcpy(&status, dStatus_, sizeof(int), cudaMemcpyDeviceToHost));
+    if (status != 0) throw Error(kDeviceError, "a device-side wait gave up (tensor-core completion not observed)");
     if (y) PARODE_CUDA(cudaMemcpy(y, last_y_ ? last_y_ : dY_, sizeof(double) * nOut_ * p_, cudaMemcpyDeviceToHost));
     if (t) time_vector(solver_, t0_, tEnd_, h_, t);
 }

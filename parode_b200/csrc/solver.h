@@ -47,6 +47,7 @@ public:
     cudaStream_t stream() const { return stream_; }
     const double* device_output() const { return dY_; }
     int path() const { return path_; }
+    int precision_used() const { return precision_used_; }
 
     // Optional stage timing with CUDA events on the execution stream.
     void set_profiling(bool on);
@@ -83,6 +84,8 @@ private:
     int sms_ = 148;
     double *dG_ = nullptr, *dWork_ = nullptr, *dCP_ = nullptr, *dCext_ = nullptr;
     size_t stage_bytes_ = 0;
+    int precision_used_ = 0;
+    int* dStatus_ = nullptr;
     cudaStream_t side_ = nullptr;
     cudaEvent_t fork_[4] = {nullptr, nullptr, nullptr, nullptr};
     bool profiling_ = false;
