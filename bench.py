@@ -3,13 +3,14 @@
 Workload (one step = one full solve): RK4, n=64 states, m=8 inputs, p=8
 outputs, h=1e-4, T=2^20 steps, seeded synthetic system and sum-of-sinusoids
 input (parode_b200/workloads.py: cfg2).  Metric: state*steps/s = n*T per solve
-/ solve time.
+/ solve time, for the mixed-precision form (3xTF32 tensor-core leaf, FP64
+carry), with the plain FP64 form timed beside it.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--precision mixed|fp64]
   python bench.py --impl reference ...   # the reference's CPU path, timed on host cores
 
 Under torchrun every rank solves its own replica of the workload on its GPU
-(the path has no cross-system exchange: replicas only); rank 0 prints one
+(the solve has no cross-system exchange: replicas only); rank 0 prints one
 JSON line.
 """
 from __future__ import annotations
@@ -28,20 +29,22 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "state*steps/s (RK4 n=64 T=2^20 solve, rel err <= 1e-6 vs FP64 oracle)"
+METRIC = "state*steps/s (RK4 n=64 T=2^20 solve, mixed 3xTF32 form, rel err <= 1e-6 vs FP64)"
 UNIT = "state*steps/s"
+WORKLOAD = "cfg2: RK4 n=64 m=8 p=8 h=1e-4 T=2^20, seeded system + sum-of-sinusoids input"
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="auto", choices=["auto", "mixed", "fp64"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--T", type=int, default=1 << 20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the FP64 comparison run")
     return ap.parse_args()
 
 
@@ -55,32 +58,44 @@ def dist_env():
 # under oracle/ and run on the host cores.
 # ---------------------------------------------------------------------------
 
+def reference_sample(T_sample):
+    from oracle import oracle
+    from parode_b200 import workloads as wl
+
+    case = wl.cfg2(T=T_sample)
+    sysd = oracle.System(case.A, case.B, case.C, case.D, case.x0)
+    inp = oracle.Input.sinusoid(case.u.a, case.u.f, case.u.phi)
+
+    def run():
+        oracle.stepper(sysd, inp, 0, 0.0, case.h, T_sample, use_float=True)
+
+    return case, run
+
+
 def run_reference(args):
     rank, _, world = dist_env()
     if rank != 0:
         return
-    from oracle import oracle
-    from parode_b200 import workloads as wl
-
-    T_sample = 1 << 16
-    case = wl.cfg2(T=T_sample)
-    sysd = oracle.System(case.A, case.B, case.C, case.D, case.x0)
-    inp = oracle.Input.sinusoid(case.u.a, case.u.f, case.u.phi)
+    # a bounded sample per step (about 30 s of CPU work for the whole run at ~1.3e5 steps/s)
+    k = int(np.floor(np.log2(4.0e6 / max(1, args.steps + args.warmup))))
+    T_sample = 1 << min(16, max(12, k))
+    case, run = reference_sample(T_sample)
     times = []
     for it in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        oracle.stepper(sysd, inp, 0, 0.0, case.h, T_sample, use_float=True)
+        run()
         dt = time.perf_counter() - t0
         if it >= args.warmup:
             times.append(dt)
     per = statistics.mean(times)
     value = case.n * T_sample / per
-    sample = f"cfg2 system, first {T_sample} of 2^20 steps per step; sequential FP32 RK4 loop (1 system => 1 thread)"
+    sample = (f"cfg2 system (RK4 n=64 m=8 p=8), first {T_sample} of 2^20 steps per step; the reference's sequential "
+              f"FP32 RK4 test loop restated in C (one system is one sequential chain: 1 thread)")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": per * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "RK4 n=64 m=8 p=8 h=1e-4 T=2^20 (sampled)", "sample_steps": T_sample},
+        "config": {"workload": WORKLOAD, "sampled_steps_per_step": T_sample},
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -93,7 +108,7 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks / throttle reasons sampled while the GPU is busy."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -102,20 +117,18 @@ class ClockSampler:
     def __init__(self, gpu: int):
         self.gpu = gpu
         self.proc = None
-        self.path = None
-
-    def __enter__(self):
         fd, self.path = tempfile.mkstemp(prefix="clocks", suffix=".csv")
         os.close(fd)
+
+    def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
-        return self
 
-    def __exit__(self, *exc):
+    def stop(self):
         if self.proc:
             self.proc.terminate()
             try:
@@ -128,11 +141,9 @@ class ClockSampler:
         try:
             with open(self.path) as fh:
                 for ln in fh:
-                    parts = [p.strip() for p in ln.split(",")]
+                    parts = [q.strip() for q in ln.split(",")]
                     if len(parts) >= 9:
                         rows.append(parts)
-        except Exception:
-            pass
         finally:
             try:
                 os.unlink(self.path)
@@ -140,8 +151,15 @@ class ClockSampler:
                 pass
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [v for v in (num(r[1]) for r in rows) if v is not None]
+        smax = [v for v in (num(r[2]) for r in rows) if v is not None]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
@@ -156,11 +174,12 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
 
 
-def fp64_peak_tflops(torch, dev):
-    """FP64 tensor throughput measured here with a cuBLAS DGEMM (torch.matmul)."""
-    N = 4096
-    a = torch.randn(N, N, dtype=torch.float64, device=dev)
-    b = torch.randn(N, N, dtype=torch.float64, device=dev)
+def gemm_peak_tflops(torch, dev, dtype, tf32=False):
+    """Dense GEMM throughput measured here with cuBLAS (torch.matmul)."""
+    N = 8192 if dtype != torch.float64 else 4096
+    torch.backends.cuda.matmul.allow_tf32 = tf32
+    a = torch.randn(N, N, dtype=dtype, device=dev)
+    b = torch.randn(N, N, dtype=dtype, device=dev)
     for _ in range(2):
         torch.matmul(a, b)
     torch.cuda.synchronize()
@@ -173,7 +192,17 @@ def fp64_peak_tflops(torch, dev):
         e.synchronize()
         best = min(best, s.elapsed_time(e) / 1e3)
     del a, b
+    torch.backends.cuda.matmul.allow_tf32 = False
     return 2.0 * N ** 3 / best / 1e12
+
+
+def leaf_flops(case, T, B):
+    """Algorithmic FLOPs of the leaf kernel for one solve: forcing, the in-block
+    up/down vector sweeps (2 (B-1)/B matvecs of Ns^2 per step) and outputs."""
+    n, m, p, Ns = case.n, case.m, case.p, case.scan_dim
+    W = 3 if case.solver == 0 else 5
+    per_step = 2 * n * W * m + 4.0 * Ns * Ns * (B - 1) / B + 2 * p * (n + m)
+    return per_step * T
 
 
 def run_ours(args):
@@ -192,73 +221,80 @@ def run_ours(args):
     from parode_b200 import workloads as wl
 
     pb.init([local_rank])
-    precision = {"auto": pb.FP64, "mixed": pb.MIXED, "fp64": pb.FP64}[args.precision]
     case = wl.cfg2(T=args.T)
     u = pb.register_sinusoid(case.u.a, case.u.f, case.u.phi)
-    plan = pb.Plan(case.A, case.B, case.C, case.D, case.x0, u, case.t0, case.t_end, case.h, solver=case.solver,
-                   precision=precision)
-    T, p, n = plan.num_outputs, plan.channels, case.n
     stream = torch.cuda.Stream(device=dev)
-    y_dev = torch.empty((T, p), dtype=torch.float64, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+    clk = ClockSampler(local_rank)
 
-    def one(prof=False):
-        plan.execute(y_dev.data_ptr(), stream.cuda_stream)
-
-    with torch.cuda.stream(stream):
-        for _ in range(args.warmup):
-            one()
-            flush.zero_()
-    torch.cuda.synchronize()
-
-    # stage split of one solve (CUDA events inside the library, same stream)
-    plan.set_profiling(True)
-    with torch.cuda.stream(stream):
-        one()
-    stages = plan.stage_times()
-    plan.set_profiling(False)
-    torch.cuda.synchronize()
-
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    step_ms = []
-    with ClockSampler(local_rank) as clk:
+    def time_plan(precision, sample_clocks):
+        plan = pb.Plan(case.A, case.B, case.C, case.D, case.x0, u, case.t0, case.t_end, case.h,
+                       solver=case.solver, precision=precision)
+        y = torch.empty((plan.num_outputs, plan.channels), dtype=torch.float64, device=dev)
+        run = lambda: plan.execute(y.data_ptr(), stream.cuda_stream)
+        if sample_clocks:
+            clk.start()  # sampled through the warm-up and the timed region, both under load
+        with torch.cuda.stream(stream):
+            t_end = time.perf_counter() + 0.5  # at least 0.5 s of warm-up under load
+            it = 0
+            while it < args.warmup or time.perf_counter() < t_end:
+                run()
+                flush.zero_()
+                it += 1
+                if it % 8 == 0:
+                    stream.synchronize()
+        torch.cuda.synchronize()
+        plan.set_profiling(True)
+        with torch.cuda.stream(stream):
+            run()
+        stages = dict(plan.stage_times())
+        plan.set_profiling(False)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        pairs = []
         with torch.cuda.stream(stream):
             for _ in range(args.steps):
                 s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 s.record(stream)
-                one()
+                run()
                 e.record(stream)
                 flush.zero_()  # L2 flush between timed solves, outside the events
-                step_ms.append((s, e))
+                pairs.append((s, e))
         torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
-    ms = [s.elapsed_time(e) for s, e in step_ms]
-    total_ms = float(sum(ms))
-    clocks = clk.summary()
+        if sample_clocks:
+            clk.stop()
+        if world > 1:
+            torch.distributed.barrier()
+        total = torch.tensor([sum(s.elapsed_time(e) for s, e in pairs)], dtype=torch.float64, device=dev)
+        if world > 1:
+            torch.distributed.all_reduce(total, op=torch.distributed.ReduceOp.MAX)
+        per = sorted(s.elapsed_time(e) for s, e in pairs)
+        info = {"ms_per_step": float(total.item()) / args.steps, "stages_ms": stages, "launches": plan.launch_count,
+                "solve_ms": {"p50": float(np.percentile(per, 50)), "p99": float(np.percentile(per, 99))},
+                "precision_used": plan.precision, "path": plan.path}
+        y_host = y.cpu().numpy()
+        plan.close()
+        return info, y_host
 
-    # parity of the timed configuration against the last result
-    _, y_host = None, y_dev.cpu().numpy()
-
-    total = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(total, op=torch.distributed.ReduceOp.MAX)
-    total_ms = float(total.item())
-    value = world * n * case.T * args.steps / (total_ms / 1e3)
+    precision = pb.MIXED if args.precision == "mixed" else pb.FP64
+    main, y_main = time_plan(precision, True)
+    plain, y_plain = (None, None)
+    if not args.no_plain and precision != pb.FP64:
+        plain, y_plain = time_plan(pb.FP64, False)
+    value = world * case.n * case.T / (main["ms_per_step"] / 1e3)
 
     # e2e: the C-ABI call with host buffers (plan set-up, H2D, solve, D2H of y)
     e2e = None
     if not args.no_e2e:
-        A, B, Cm, D, x0 = case.A, case.B, case.C, case.D, case.x0
         e2e_ms = []
         for it in range(1 + max(1, min(args.steps, 3))):
             torch.cuda.synchronize()
             s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             s.record()
-            _, y_e2e = pb.simulate(A, B, Cm, D, x0, u, case.t0, case.t_end, case.h, solver=case.solver,
-                                   precision=precision)
+            pb.simulate(case.A, case.B, case.C, case.D, case.x0, u, case.t0, case.t_end, case.h, solver=case.solver,
+                        precision=precision)
             e.record()
             e.synchronize()
             if it > 0:
@@ -266,59 +302,69 @@ def run_ours(args):
         e2e_t = torch.tensor([statistics.mean(e2e_ms)], dtype=torch.float64, device=dev)
         if world > 1:
             torch.distributed.all_reduce(e2e_t, op=torch.distributed.ReduceOp.MAX)
-        h2d = 8 * (A.size + B.size + Cm.size + D.size + x0.size + 3 * case.u.a.size)
-        d2h = 8 * T * p
-        e2e = {"value": world * n * case.T / (float(e2e_t.item()) / 1e3), "unit": UNIT,
-               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "ms_per_step": float(e2e_t.item())}
+        h2d = 8 * (case.A.size + case.B.size + case.C.size + case.D.size + case.x0.size + 3 * case.u.a.size)
+        d2h = 8 * case.T * case.p
+        e2e = {"value": world * case.n * case.T / (float(e2e_t.item()) / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "ms_per_step": float(e2e_t.item()),
+               "call": "ParODE_SimulateODE_d (host arrays in, host y out)"}
 
-    line = None
     if rank == 0:
         peaks, peaks_kind = measured_peaks()
-        fp64_tf = fp64_peak_tflops(torch, dev)
-        st = dict(stages)
-        sweep_ms = st.get("sweeps", total_ms / args.steps)
-        Ns = case.scan_dim
-        flops_sweep = 4.0 * Ns * Ns * case.T  # up + down vector sweeps (algorithmic)
-        achieved = flops_sweep / (sweep_ms / 1e3) / 1e12
-        roofline = {"bound": "tensor", "kernel": "affine-level sweeps (DMMA FP64)", "achieved": achieved,
-                    "peak": fp64_tf, "unit": "TFLOP/s", "frac": achieved / fp64_tf,
-                    "peak_source": "FP64 DGEMM measured in this run (torch.matmul float64 4096^3)",
-                    "traffic": None, "stages_ms": st}
+        used_mixed = main["precision_used"] == pb.MIXED
+        B = 16  # blocks of the leaf for n = 64 (R = 4)
+        leaf_ms = main["stages_ms"].get("leaf")
+        if used_mixed:
+            tf32 = gemm_peak_tflops(torch, dev, torch.float32, tf32=True)
+            peak = tf32 / 3.0
+            peak_src = (f"dense TF32 GEMM measured in this run ({tf32:.0f} TFLOP/s, cuBLAS via torch.matmul) / 3: "
+                        f"3xTF32 spends three tensor products per algorithmic product")
+        else:
+            peak = gemm_peak_tflops(torch, dev, torch.float64)
+            peak_src = "dense FP64 GEMM measured in this run (cuBLAS DGEMM via torch.matmul)"
+        achieved = leaf_flops(case, case.T, B) / (leaf_ms / 1e3) / 1e12 if leaf_ms else None
+        roofline = {"bound": "tensor", "kernel": "k_leaf_tc (3xTF32 tcgen05)" if used_mixed else "k_leaf (DMMA FP64)",
+                    "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                    "frac": (achieved / peak) if achieved else None, "peak_source": peak_src,
+                    "traffic": None, "stages_ms": main["stages_ms"],
+                    "whole_solve_tflops": (4.0 * case.scan_dim ** 2 + 6 * case.n * case.m +
+                                           2 * case.p * (case.n + case.m)) * case.T / (main["ms_per_step"] / 1e3) / 1e12}
+        rel_vs_fp64 = None
+        if y_plain is not None:
+            from oracle import oracle
+            rel_vs_fp64 = oracle.rel_err(y_main, y_plain)
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            from oracle import oracle
-
             T_cpu = 1 << 20
-            c2 = wl.cfg2(T=T_cpu)
-            sysd = oracle.System(c2.A, c2.B, c2.C, c2.D, c2.x0)
-            inp = oracle.Input.sinusoid(c2.u.a, c2.u.f, c2.u.phi)
+            c2, run = reference_sample(T_cpu)
             t0 = time.perf_counter()
-            oracle.stepper(sysd, inp, 0, 0.0, c2.h, T_cpu, use_float=True)
+            run()
             dt = time.perf_counter() - t0
             cpu = {"value": c2.n * T_cpu / dt, "unit": UNIT, "cores": 1, "kind": "port",
-                   "sample": f"reference CPU path (sequential FP32 RK4 loop of the reference tests) on cfg2, "
-                             f"{T_cpu} steps, {dt:.1f} s"}
+                   "sample": f"the reference's CPU path (its tests' sequential FP32 RK4 loop, restated in C) on the "
+                             f"full cfg2 horizon, {T_cpu} steps in {dt:.1f} s on 1 host core"}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if precision == pb.FP64 else "tf32x3+f64",
-            "data": "synthetic",
-            "config": {"workload": "cfg2: RK4 n=64 m=8 p=8 h=1e-4 T=2^20, seeded system + sinusoid input",
-                       "precision": "fp64" if precision == pb.FP64 else "mixed", "path": plan_path_name(pb),
-                       "l2": "256 MB flush between timed solves", "parallelism": f"replicas x{world}"},
-            "gpu_launches": plan.launch_count * args.steps,
-            "clocks": clocks, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "warmup": args.warmup, "ms_per_step": main["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "tf32x3+f64" if used_mixed else "f64", "data": "synthetic (seeded system and input)",
+            "config": {"workload": WORKLOAD,
+                       "precision": "mixed" if used_mixed else "fp64",
+                       "path": {1: "level-synchronous", 2: "blocked"}.get(main["path"], "?"),
+                       "l2": "256 MB flush between timed solves (outside the events)",
+                       "parallelism": f"replicas x{world}"},
+            "gpu_launches": main["launches"] * args.steps, "solve_ms": main["solve_ms"],
+            "clocks": clk.summary(), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "plain_fp64": None if plain is None else {
+                "value": world * case.n * case.T / (plain["ms_per_step"] / 1e3), "ms_per_step": plain["ms_per_step"],
+                "stages_ms": plain["stages_ms"]},
+            "mixed_over_plain": None if plain is None else plain["ms_per_step"] / main["ms_per_step"],
+            "rel_err_mixed_vs_fp64": rel_vs_fp64,
             "peaks": {k: peaks.get(k) for k in ("hbm_gbs", "bf16_tflops", "bf16_tflops_sustained")},
             "peaks_source": peaks_kind,
         }
         print(json.dumps(line), flush=True)
-    plan.close()
     if world > 1:
         torch.distributed.destroy_process_group()
-
-
-def plan_path_name(pb):
-    return {0: "auto", 1: "level-synchronous", 2: "blocked"}.get(pb.get_option(pb.OPT_PATH), "?")
 
 
 def main():

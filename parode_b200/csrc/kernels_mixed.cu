@@ -26,6 +26,11 @@
 
 #include <algorithm>
 
+// Phase hook for timing harnesses; compiled out in the library.
+#ifndef PARODE_TRACE
+#define PARODE_TRACE() ((void)0)
+#endif
+
 namespace parode {
 
 namespace {
@@ -158,6 +163,7 @@ __device__ void tc_level(unsigned char* sm, const TcLayout& L, uint64_t* bar, ui
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (tid == 0) {
         fence_after_sync();
+        PARODE_TRACE();
         const uint32_t base = smem_u32(sm);
         const uint32_t ph = base + L.ph + (uint32_t)l * 2 * NP * NP * 4;
         for (int z = 0; z < slices; ++z) {
@@ -166,9 +172,11 @@ __device__ void tc_level(unsigned char* sm, const TcLayout& L, uint64_t* bar, ui
                  ph + NP * NP * 4, 128, SBO, 256, NP / 8, make_idesc(128, NP), true);
         }
         mma_commit(bar);
+        PARODE_TRACE();
     }
     __syncwarp();
     round_wait(bar, phase, status);
+    PARODE_TRACE();
     const int sub = warp & 3, half = warp >> 2;
     if (half < H) {
         for (int z = 0; z < slices; ++z) {
@@ -195,6 +203,7 @@ __device__ void tc_level(unsigned char* sm, const TcLayout& L, uint64_t* bar, ui
         }
     }
     round_end();
+    PARODE_TRACE();
 }
 
 // Down-sweep bookkeeping of level l: V[left(g)] <-> V[right(g)] for g < c.
@@ -203,8 +212,11 @@ __device__ void tc_swap(unsigned char* sm, const TcLayout& L, int R, int S, int 
 {
     const int c = S >> (l + 1);
     const int rs = S - (S >> l);
+    // consecutive threads take consecutive vectors (rows) of the same 16-byte
+    // chunk: a row's chunks are 128 bytes apart in the K-major layout, so
+    // walking a row with neighbouring threads would hit one bank group
     for (int e = threadIdx.x; e < c * (NP / 4); e += kTcThreads) {
-        const int g = e / (NP / 4), k = 4 * (e - g * (NP / 4));
+        const int k = 4 * (e / c), g = e - (k >> 2) * c;
         const int rl = rs + g, rr = row_of(((g + 1) << (l + 1)) - 1, R, S);
 #pragma unroll
         for (int part = 0; part < 2; ++part) {
@@ -217,6 +229,7 @@ __device__ void tc_swap(unsigned char* sm, const TcLayout& L, int R, int S, int 
         }
     }
     round_end();
+    PARODE_TRACE();
 }
 
 template <int NP>
@@ -280,6 +293,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_leaf_tc(LeafArgs a, int R, in
     uint32_t phase = 0;
 
     for (long tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+        PARODE_TRACE();
         const long j0 = tile * S;
         // 1. input samples (hi/lo, 16-byte rows): RK4 arrays of even / odd
         //    half-step samples, ABM one array of whole-step samples
@@ -294,6 +308,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_leaf_tc(LeafArgs a, int R, in
             *sptr(sm, L, arr, 1, r, i) = lo;
         }
         round_end();
+        PARODE_TRACE();
         // 2. forcing on the tensor cores: Gamma (S x NP) = sum_w U_w B_w^T
         {
             const int slices = (S + 127) >> 7;
@@ -312,9 +327,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_leaf_tc(LeafArgs a, int R, in
                     }
                 }
                 mma_commit(bar);
+                PARODE_TRACE();
             }
             __syncwarp();
             round_wait(bar, phase, a.status);
+            PARODE_TRACE();
             const int sub = warp & 3, half = warp >> 2;
             if (half < H) {
                 for (int z = 0; z < slices; ++z) {
@@ -339,6 +356,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_leaf_tc(LeafArgs a, int R, in
                 }
             }
             round_end();
+            PARODE_TRACE();
         }
         // 3. up-sweep on the tensor cores
         for (int l = 0; l < R; ++l) tc_level<NP>(sm, L, bar, tbase, R, S, l, phase, a.status);
@@ -354,6 +372,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_leaf_tc(LeafArgs a, int R, in
                 *lp = 0.f;
             }
             round_end();
+            PARODE_TRACE();
         }
         // 5. down-sweep from the zero roots
         for (int l = R - 1; l >= 0; --l) {
