@@ -90,6 +90,21 @@ void ParODE_PlanDestroy(ParODE_Plan* plan);
 void ParODE_PlanSetProfiling(ParODE_Plan* plan, int enable, int nErr[]);
 int ParODE_PlanStageTimes(ParODE_Plan* plan, float* ms, int cap, char* names, int names_cap, int nErr[]);
 
+/* Affine scan on device data with no allocation (no counterpart in the
+ * reference).  With all pointers in device memory of the current device:
+ *   dX[k] = x_k for k < count, x_0 = dX0, x_{k+1} = Phi x_k + dGamma[k],
+ * Phi ns x ns, dGamma count x ns, dX count x ns, all row-major FP64;
+ * dGamma or dX0 may be NULL (zero).  ns in [1, 64].  Enqueued on `stream`
+ * (NULL: the legacy default stream); returns after enqueueing.
+ * It allocates nothing: its scratch is a static 16 MiB device array, looked
+ * up on the first call on each device (make that call before any stream
+ * capture).  A call needs levels*NP^2 + NP + count*NP*(1 + ~1/(B-1))
+ * doubles of it (NP = power of two >= max(8, ns)): count <= ~29,000 at
+ * ns = 64, ~230,000 at ns = 8; larger calls fail with -4 (NotEnoughResources).
+ * The scratch is shared: calls that overlap on the GPU race on it. */
+void ParODE_AffineScanDevice(const double* dPhi, const double* dGamma, const double* dX0, int ns,
+                             long long count, double* dX, void* stream, int nErr[]);
+
 #ifdef __cplusplus
 }
 #endif
