@@ -32,6 +32,10 @@ sys.path.insert(0, ROOT)
 METRIC = "state*steps/s (RK4 n=64 T=2^20 solve, mixed 3xTF32 form, rel err <= 1e-6 vs FP64)"
 UNIT = "state*steps/s"
 WORKLOAD = "cfg2: RK4 n=64 m=8 p=8 h=1e-4 T=2^20, seeded system + sum-of-sinusoids input"
+# DRAM bytes (read + write) of one leaf launch on this workload, from the ncu
+# captures summarised in profiles/k_leaf_tc_cfg2_rk4_n64.md (mixed) and
+# profiles/k_leaf_fp64_cfg2_rk4_n64.md (FP64); keyed by (T, mixed).
+LEAF_TRAFFIC = {(1 << 20, True): 199.13e6, (1 << 20, False): 202.22e6}
 
 
 def parse():
@@ -45,6 +49,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the FP64 comparison run")
+    ap.add_argument("--min-warmup-s", type=float, default=0.5, help="least warm-up time under load (clock sampling)")
     return ap.parse_args()
 
 
@@ -235,7 +240,7 @@ def run_ours(args):
         if sample_clocks:
             clk.start()  # sampled through the warm-up and the timed region, both under load
         with torch.cuda.stream(stream):
-            t_end = time.perf_counter() + 0.5  # at least 0.5 s of warm-up under load
+            t_end = time.perf_counter() + args.min_warmup_s  # warm-up under load, sampled by the clock monitor
             it = 0
             while it < args.warmup or time.perf_counter() < t_end:
                 run()
@@ -325,7 +330,7 @@ def run_ours(args):
         roofline = {"bound": "tensor", "kernel": "k_leaf_tc (3xTF32 tcgen05)" if used_mixed else "k_leaf (DMMA FP64)",
                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                     "frac": (achieved / peak) if achieved else None, "peak_source": peak_src,
-                    "traffic": None, "stages_ms": main["stages_ms"],
+                    "traffic": LEAF_TRAFFIC.get((case.T, used_mixed)), "stages_ms": main["stages_ms"],
                     "whole_solve_tflops": (4.0 * case.scan_dim ** 2 + 6 * case.n * case.m +
                                            2 * case.p * (case.n + case.m)) * case.T / (main["ms_per_step"] / 1e3) / 1e12}
         rel_vs_fp64 = None
