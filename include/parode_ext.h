@@ -90,6 +90,43 @@ void ParODE_PlanDestroy(ParODE_Plan* plan);
 void ParODE_PlanSetProfiling(ParODE_Plan* plan, int enable, int nErr[]);
 int ParODE_PlanStageTimes(ParODE_Plan* plan, float* ms, int cap, char* names, int names_cap, int nErr[]);
 
+/* ---- batches: many independent systems solved together -----------------
+ * One call set-up for nSystems systems (per-system arrays of the
+ * SimulateODE_d arguments; B, C, D may be NULL arrays when every system has
+ * that matrix absent).  Device-resident afterwards: BatchExecute enqueues all
+ * solves on `stream` with a fixed, small number of launches (scan dimension
+ * <= 64: batched blocked path per padded dimension; larger: one grouped
+ * contraction launch per Blelloch level).  The reference has no batch entry
+ * point: it solves one system per SimulateODE call (Sources/ParODE.cpp:281-337). */
+typedef struct ParODE_Batch ParODE_Batch;
+ParODE_Batch* ParODE_BatchCreate(int nSystems, const double* const A[], const double* const B[],
+                                 const double* const C[], const double* const D[], const int nInputs[],
+                                 const int nStates[], const int nOutputs[], const int ZeroB[], const int ZeroC[],
+                                 const int ZeroD[], const int uIndex[], const double tStart[], const double tEnd[],
+                                 const double tStep[], const double* const x0[], const int solver[], int precision,
+                                 int nErr[]);
+void ParODE_BatchExecute(ParODE_Batch* batch, void* stream, int nErr[]);
+long long ParODE_BatchNumOutputs(const ParODE_Batch* batch, int i);
+int ParODE_BatchNumOutputChannels(const ParODE_Batch* batch, int i);
+/* Device pointer to system i's outputs (NumOutputs x channels doubles). */
+const double* ParODE_BatchDeviceOutput(const ParODE_Batch* batch, int i);
+/* Synchronises and copies system i's time vector and outputs (either may be NULL). */
+void ParODE_BatchGetOutput(ParODE_Batch* batch, int i, double* tVect, double* yVect, int nErr[]);
+int ParODE_BatchLaunchCount(const ParODE_Batch* batch);
+int ParODE_BatchPath(const ParODE_Batch* batch, int i);
+int ParODE_BatchPrecision(const ParODE_Batch* batch, int i);
+/* Sum over systems of states x outputs: the state*steps of one execute. */
+double ParODE_BatchStateSteps(const ParODE_Batch* batch);
+void ParODE_BatchDestroy(ParODE_Batch* batch);
+/* Create + execute + copy out + destroy; tVect[i] / yVect[i] are host arrays
+ * sized for system i (NumOutputs), nSteps[i] receives its output count. */
+void ParODE_SimulateODEBatch(int nSystems, const double* const A[], const double* const B[], const double* const C[],
+                             const double* const D[], const int nInputs[], const int nStates[], const int nOutputs[],
+                             const int ZeroB[], const int ZeroC[], const int ZeroD[], const int uIndex[],
+                             const double tStart[], const double tEnd[], const double tStep[],
+                             const double* const x0[], const int solver[], int precision, double* const tVect[],
+                             double* const yVect[], long long nSteps[], int nErr[]);
+
 /* Affine scan on device data with no allocation (no counterpart in the
  * reference).  With all pointers in device memory of the current device:
  *   dX[k] = x_k for k < count, x_0 = dX0, x_{k+1} = Phi x_k + dGamma[k],

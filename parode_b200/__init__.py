@@ -97,6 +97,23 @@ def _load():
     L.ParODE_PlanSetProfiling.argtypes = [C.c_void_p, C.c_int, ip]
     L.ParODE_PlanStageTimes.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_int, C.c_char_p, C.c_int, ip]
     L.ParODE_PlanStageTimes.restype = C.c_int
+    pp = C.POINTER(C.c_void_p)
+    L.ParODE_BatchCreate.argtypes = [C.c_int, pp, pp, pp, pp, ip, ip, ip, ip, ip, ip, ip, dp, dp, dp, pp, ip,
+                                     C.c_int, ip]
+    L.ParODE_BatchCreate.restype = C.c_void_p
+    L.ParODE_BatchExecute.argtypes = [C.c_void_p, C.c_void_p, ip]
+    L.ParODE_BatchNumOutputs.argtypes = [C.c_void_p, C.c_int]
+    L.ParODE_BatchNumOutputs.restype = C.c_longlong
+    L.ParODE_BatchNumOutputChannels.argtypes = [C.c_void_p, C.c_int]
+    L.ParODE_BatchDeviceOutput.argtypes = [C.c_void_p, C.c_int]
+    L.ParODE_BatchDeviceOutput.restype = C.c_void_p
+    L.ParODE_BatchGetOutput.argtypes = [C.c_void_p, C.c_int, dp, dp, ip]
+    L.ParODE_BatchLaunchCount.argtypes = [C.c_void_p]
+    L.ParODE_BatchPath.argtypes = [C.c_void_p, C.c_int]
+    L.ParODE_BatchPrecision.argtypes = [C.c_void_p, C.c_int]
+    L.ParODE_BatchStateSteps.argtypes = [C.c_void_p]
+    L.ParODE_BatchStateSteps.restype = C.c_double
+    L.ParODE_BatchDestroy.argtypes = [C.c_void_p]
     return L
 
 
@@ -299,6 +316,84 @@ class Plan:
     def close(self) -> None:
         if getattr(self, "_h", None):
             lib.ParODE_PlanDestroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many independent solves set up once and run together (ParODE_Batch*).
+
+    systems: a sequence of dicts with keys A, B, C, D (None = absent), x0,
+    u (input index), t0, t_end, h, solver."""
+
+    def __init__(self, systems, precision: int = FP64):
+        N = len(systems)
+        keep = []
+        arrs = {k: (C.c_void_p * N)() for k in ("A", "B", "C", "D", "x0")}
+        ints = {k: (C.c_int * N)() for k in ("m", "n", "p", "zB", "zC", "zD", "u", "solver")}
+        dbl = {k: (C.c_double * N)() for k in ("t0", "t1", "h")}
+        for i, s in enumerate(systems):
+            A, B, Cm, D, x0, n, m, p = _sys_arrays(s["A"], s.get("B"), s.get("C"), s.get("D"), s["x0"])
+            for k, v in (("A", A), ("B", B), ("C", Cm), ("D", D), ("x0", x0)):
+                if v is not None:
+                    keep.append(v)
+                    arrs[k][i] = v.ctypes.data
+            ints["m"][i], ints["n"][i], ints["p"][i] = m, n, p
+            ints["zB"][i], ints["zC"][i], ints["zD"][i] = int(B is None), int(Cm is None), int(D is None)
+            ints["u"][i] = int(s.get("u", 0))
+            ints["solver"][i] = int(s.get("solver", RK4))
+            dbl["t0"][i], dbl["t1"][i], dbl["h"][i] = s["t0"], s["t_end"], s["h"]
+        e = C.c_int(0)
+        ip = lambda a: C.cast(a, C.POINTER(C.c_int))
+        dpp = lambda a: C.cast(a, C.POINTER(C.c_double))
+        vp = lambda a: C.cast(a, C.POINTER(C.c_void_p))
+        self._h = lib.ParODE_BatchCreate(N, vp(arrs["A"]), vp(arrs["B"]), vp(arrs["C"]), vp(arrs["D"]),
+                                         ip(ints["m"]), ip(ints["n"]), ip(ints["p"]), ip(ints["zB"]), ip(ints["zC"]),
+                                         ip(ints["zD"]), ip(ints["u"]), dpp(dbl["t0"]), dpp(dbl["t1"]), dpp(dbl["h"]),
+                                         vp(arrs["x0"]), ip(ints["solver"]), precision, C.byref(e))
+        _check(e, "ParODE_BatchCreate")
+        self.size = N
+        self.num_outputs = [int(lib.ParODE_BatchNumOutputs(self._h, i)) for i in range(N)]
+        self.channels = [int(lib.ParODE_BatchNumOutputChannels(self._h, i)) for i in range(N)]
+
+    def execute(self, stream: int = 0) -> None:
+        e = C.c_int(0)
+        lib.ParODE_BatchExecute(self._h, C.c_void_p(stream or None), C.byref(e))
+        _check(e, "ParODE_BatchExecute")
+
+    def output(self, i: int):
+        t = np.zeros(self.num_outputs[i])
+        y = np.zeros((self.num_outputs[i], self.channels[i]))
+        e = C.c_int(0)
+        lib.ParODE_BatchGetOutput(self._h, i, _dp(t), _dp(y), C.byref(e))
+        _check(e, "ParODE_BatchGetOutput")
+        return t, y
+
+    def device_output(self, i: int) -> int:
+        return int(lib.ParODE_BatchDeviceOutput(self._h, i) or 0)
+
+    def path(self, i: int) -> int:
+        return int(lib.ParODE_BatchPath(self._h, i))
+
+    def precision(self, i: int) -> int:
+        return int(lib.ParODE_BatchPrecision(self._h, i))
+
+    @property
+    def launch_count(self) -> int:
+        return int(lib.ParODE_BatchLaunchCount(self._h))
+
+    @property
+    def state_steps(self) -> float:
+        return float(lib.ParODE_BatchStateSteps(self._h))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib.ParODE_BatchDestroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -10,6 +10,7 @@
 #include "host_math.h"
 #include "inputs.h"
 #include "solver.h"
+#include "batch.h"
 
 #include "FTypeDef.h"
 #include "ParODECInterface.h"
@@ -514,6 +515,135 @@ int ParODE_PlanStageTimes(ParODE_Plan* plan, float* ms, int cap, char* names, in
     });
     if (nErr) nErr[0] = rc;
     return count;
+}
+
+// ---- batches ---------------------------------------------------------------
+
+struct ParODE_Batch {
+    std::unique_ptr<BatchPlan> batch;
+};
+
+ParODE_Batch* ParODE_BatchCreate(int nSystems, const double* const A[], const double* const B[],
+                                 const double* const C[], const double* const D[], const int nInputs[],
+                                 const int nStates[], const int nOutputs[], const int ZeroB[], const int ZeroC[],
+                                 const int ZeroD[], const int uIndex[], const double tStart[], const double tEnd[],
+                                 const double tStep[], const double* const x0[], const int solver[], int precision,
+                                 int nErr[])
+{
+    Library& L = lib();
+    std::lock_guard<std::recursive_mutex> g(L.mu);
+    ParODE_Batch* out = nullptr;
+    int rc = guarded([&] {
+        int dev = current_device_locked(L);
+        if (precision != PARODE_PRECISION_FP64 && precision != PARODE_PRECISION_MIXED)
+            throw Error(kInvalidArgument, "unknown precision");
+        if (nSystems <= 0 || !A || !x0 || !nInputs || !nStates || !nOutputs || !ZeroB || !ZeroC || !ZeroD ||
+            !uIndex || !tStart || !tEnd || !tStep || !solver)
+            throw Error(kInvalidArgument, "batch arrays missing");
+        std::vector<BatchSpec> specs((size_t)nSystems);
+        for (int i = 0; i < nSystems; ++i) {
+            specs[i].sys = make_system<double>(A[i], B ? B[i] : nullptr, C ? C[i] : nullptr, D ? D[i] : nullptr,
+                                               nInputs[i], nStates[i], nOutputs[i], ZeroB[i], ZeroC[i], ZeroD[i],
+                                               x0[i]);
+            specs[i].uIndex = uIndex[i];
+            specs[i].solver = solver[i];
+            specs[i].t0 = tStart[i];
+            specs[i].tEnd = tEnd[i];
+            specs[i].h = tStep[i];
+        }
+        PlanOptions opt;
+        opt.precision = precision;
+        opt.path = L.path;
+        opt.input_double = true;
+        auto h = std::make_unique<ParODE_Batch>();
+        h->batch = std::make_unique<BatchPlan>(dev, std::move(specs), &L.inputs, opt);
+        out = h.release();
+    });
+    if (nErr) nErr[0] = rc;
+    return out;
+}
+
+void ParODE_BatchExecute(ParODE_Batch* batch, void* stream, int nErr[])
+{
+    int rc = guarded([&] {
+        if (!batch || !batch->batch) throw Error(kInvalidArgument, "null batch");
+        batch->batch->execute((cudaStream_t)stream);
+    });
+    if (nErr) nErr[0] = rc;
+}
+
+long long ParODE_BatchNumOutputs(const ParODE_Batch* batch, int i)
+{
+    if (!batch || !batch->batch || i < 0 || i >= batch->batch->size()) return -1;
+    return batch->batch->num_outputs(i);
+}
+
+int ParODE_BatchNumOutputChannels(const ParODE_Batch* batch, int i)
+{
+    if (!batch || !batch->batch || i < 0 || i >= batch->batch->size()) return -1;
+    return batch->batch->channels(i);
+}
+
+const double* ParODE_BatchDeviceOutput(const ParODE_Batch* batch, int i)
+{
+    if (!batch || !batch->batch || i < 0 || i >= batch->batch->size()) return nullptr;
+    return batch->batch->device_output(i);
+}
+
+void ParODE_BatchGetOutput(ParODE_Batch* batch, int i, double* tVect, double* yVect, int nErr[])
+{
+    int rc = guarded([&] {
+        if (!batch || !batch->batch) throw Error(kInvalidArgument, "null batch");
+        batch->batch->get_output(i, tVect, yVect);
+    });
+    if (nErr) nErr[0] = rc;
+}
+
+int ParODE_BatchLaunchCount(const ParODE_Batch* batch)
+{
+    return (batch && batch->batch) ? batch->batch->launch_count() : 0;
+}
+
+int ParODE_BatchPath(const ParODE_Batch* batch, int i)
+{
+    if (!batch || !batch->batch || i < 0 || i >= batch->batch->size()) return -1;
+    return batch->batch->path(i);
+}
+
+int ParODE_BatchPrecision(const ParODE_Batch* batch, int i)
+{
+    if (!batch || !batch->batch || i < 0 || i >= batch->batch->size()) return -1;
+    return batch->batch->precision_used(i);
+}
+
+double ParODE_BatchStateSteps(const ParODE_Batch* batch)
+{
+    return (batch && batch->batch) ? batch->batch->state_steps() : 0.0;
+}
+
+void ParODE_BatchDestroy(ParODE_Batch* batch) { delete batch; }
+
+void ParODE_SimulateODEBatch(int nSystems, const double* const A[], const double* const B[], const double* const C[],
+                             const double* const D[], const int nInputs[], const int nStates[], const int nOutputs[],
+                             const int ZeroB[], const int ZeroC[], const int ZeroD[], const int uIndex[],
+                             const double tStart[], const double tEnd[], const double tStep[],
+                             const double* const x0[], const int solver[], int precision, double* const tVect[],
+                             double* const yVect[], long long nSteps[], int nErr[])
+{
+    Library& L = lib();
+    std::lock_guard<std::recursive_mutex> g(L.mu);
+    int err = 0;
+    ParODE_Batch* b = ParODE_BatchCreate(nSystems, A, B, C, D, nInputs, nStates, nOutputs, ZeroB, ZeroC, ZeroD,
+                                         uIndex, tStart, tEnd, tStep, x0, solver, precision, &err);
+    if (err == 0) {
+        ParODE_BatchExecute(b, nullptr, &err);
+        for (int i = 0; err == 0 && i < nSystems; ++i) {
+            ParODE_BatchGetOutput(b, i, tVect ? tVect[i] : nullptr, yVect ? yVect[i] : nullptr, &err);
+            if (nSteps) nSteps[i] = ParODE_BatchNumOutputs(b, i);
+        }
+    }
+    ParODE_BatchDestroy(b);
+    if (nErr) nErr[0] = err;
 }
 
 }  // extern "C"

@@ -1,0 +1,731 @@
+// batch.cpp -- BatchPlan: set-up on the host (FP64 discretisation, one arena,
+// one staged copy), execution as a fixed sequence of batched launches.
+#include "batch.h"
+
+#include "common.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <thread>
+
+namespace parode {
+
+namespace {
+
+constexpr size_t kAlign = 256;
+constexpr size_t kSmemOptIn = 232448 - 1024;
+
+size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
+
+// Byte layout of the arena, built before allocation.
+struct Layout {
+    size_t bytes = 0;
+    size_t take(size_t n)
+    {
+        size_t off = bytes;
+        bytes = align_up(bytes + std::max<size_t>(n, 1));
+        return off;
+    }
+};
+
+// Host staging of the constant part of the arena (copied once).
+struct Stage {
+    std::vector<char> buf;
+    size_t put(const void* src, size_t n, Layout& L)
+    {
+        size_t off = L.take(n);
+        if (buf.size() < L.bytes) buf.resize(L.bytes, 0);
+        if (n && src) std::memcpy(buf.data() + off, src, n);
+        return off;
+    }
+};
+
+double sinusoid_host(const InputEntry* e, int i, double t)
+{
+    const double two_pi = 6.283185307179586476925286766559;
+    double v = 0.0;
+    for (int k = 0; k < e->K; ++k) {
+        const int q = i * e->K + k;
+        v += e->a[q] * std::sin(two_pi * e->f[q] * t + e->phi[q]);
+    }
+    return v;
+}
+
+template <class F>
+void parallel_for(int n, F&& f)
+{
+    int nt = (int)std::min<unsigned>(std::max(1u, std::thread::hardware_concurrency()), 32u);
+    nt = std::min(nt, std::max(1, n));
+    std::vector<std::thread> th;
+    std::vector<std::exception_ptr> err(nt);
+    for (int t = 0; t < nt; ++t)
+        th.emplace_back([&, t] {
+            try {
+                for (int i = t; i < n; i += nt) f(i);
+            } catch (...) {
+                err[t] = std::current_exception();
+            }
+        });
+    for (auto& x : th) x.join();
+    for (auto& e : err)
+        if (e) std::rethrow_exception(e);
+}
+
+}  // namespace
+
+BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* inputs, const PlanOptions& opt)
+    : device_(device), inputs_(inputs), opt_(opt)
+{
+    if (specs.empty()) throw Error(kInvalidArgument, "empty batch");
+    if (specs.size() > 65535) throw Error(kInvalidArgument, "at most 65535 systems per batch");
+    PARODE_CUDA(cudaSetDevice(device_));
+    PARODE_CUDA(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_));
+    const int N = (int)specs.size();
+    sys_.resize(N);
+
+    // ---- classification and sizes ----------------------------------------
+    for (int i = 0; i < N; ++i) {
+        const BatchSpec& b = specs[i];
+        const SystemDesc& s = b.sys;
+        Sys& q = sys_[i];
+        if (b.solver != kRK4 && b.solver != kABM) throw Error(kInvalidSolverType, "unknown solver type");
+        if (s.n <= 0) throw Error(kInvalidSystem, "the system has no states");
+        if ((long)s.A.size() < (long)s.n * s.n || (long)s.x0.size() < s.n)
+            throw Error(kInvalidSystem, "A or x0 too small");
+        if (!s.zeroB && (s.m <= 0 || (long)s.B.size() < (long)s.n * s.m))
+            throw Error(kInvalidSystem, "B has the wrong size");
+        if (!s.zeroC && (s.p <= 0 || (long)s.C.size() < (long)s.p * s.n))
+            throw Error(kInvalidSystem, "C has the wrong size");
+        if (!s.zeroD && (s.p <= 0 || s.m <= 0 || (long)s.D.size() < (long)s.p * s.m))
+            throw Error(kInvalidSystem, "D has the wrong size");
+        q.solver = b.solver;
+        q.n = s.n;
+        q.m = s.m;
+        q.t0 = b.t0;
+        q.tEnd = b.tEnd;
+        q.h = b.h;
+        q.zeroB = s.zeroB;
+        q.zeroC = s.zeroC;
+        q.zeroD = s.zeroD;
+        q.nOut = parode::num_outputs(b.solver, b.t0, b.tEnd, b.h, &q.nScan);
+        if (q.nOut <= 0 || q.nScan <= 0) throw Error(kInvalidSystem, "empty time horizon");
+        q.p = s.out_size();
+        q.mu = (!s.zeroB || !s.zeroD) ? s.m : 0;
+        if (q.mu > 0) {
+            q.input = inputs ? inputs->get(b.uIndex) : nullptr;
+            if (!q.input) throw Error(kInvalidInput, "uIndex does not name a registered input");
+            if (q.input->kind == InputEntry::kSinusoid && q.input->m < q.mu)
+                throw Error(kInvalidInput, "the sinusoid input has fewer channels than the system's inputs");
+        }
+        q.W = b.solver == kRK4 ? 3 : 5;
+        q.Ns = b.solver == kRK4 ? s.n : 4 * s.n;
+        if (q.solver == kRK4) {
+            q.nU = 2 * q.nScan + 1;
+            q.u_base = b.t0;
+            q.u_dt = 0.5 * b.h;
+        } else {
+            q.nU = q.nScan + 4;
+            q.u_base = (b.t0 + 3.0 * b.h) - 3.0 * b.h;
+            q.u_dt = b.h;
+        }
+        BlockedShape sh;
+        q.blocked = opt.path != kPathLevel && blocked_shape(q.Ns, std::max(q.mu, 1), 0, &sh);
+        if (q.blocked) {
+            q.Np = sh.NP;
+            int bi = -1;
+            for (int k = 0; k < (int)buckets_.size(); ++k)
+                if (buckets_[k].sh.NP == q.Np) bi = k;
+            if (bi < 0) {
+                buckets_.emplace_back();
+                bi = (int)buckets_.size() - 1;
+                buckets_[bi].sh.NP = q.Np;
+            }
+            q.bucket = bi;
+            buckets_[bi].systems.push_back(i);
+            buckets_[bi].ms = std::max(buckets_[bi].ms, q.mu);
+            buckets_[bi].pmax = std::max(buckets_[bi].pmax, q.p);
+        } else {
+            q.Np = (int)round_up(q.Ns, 8);
+            if (q.Np > 1024) throw Error(kInvalidSystem, "scan dimension above 1024 is not supported");
+            q.Tp = next_pow2(q.nScan);
+            q.levels = ilog2(q.Tp);
+            ls_.push_back(i);
+        }
+        q.precision = kFP64;
+    }
+    // bucket shapes: the widest input of the bucket sizes the sample staging
+    for (Bucket& bk : buckets_) {
+        if (!blocked_shape(bk.sh.NP, std::max(bk.ms, 1), 0, &bk.sh))
+            throw Error(kInvalidArgument, "blocked shape for the batch");
+        long stage = 0;
+        for (int i : bk.systems) {
+            const Sys& q = sys_[i];
+            stage = std::max<long>(stage, (long)q.n * q.W * q.m + (long)q.p * q.n + (long)q.p * q.m);
+        }
+        bk.stage = batch_leaf_smem(bk.sh, bk.ms, stage) <= kSmemOptIn;
+        bk.leaf_smem = batch_leaf_smem(bk.sh, bk.ms, bk.stage ? stage : 0);
+        for (int i : bk.systems) {
+            Sys& q = sys_[i];
+            q.ntiles = (q.nScan + bk.sh.S - 1) / bk.sh.S;
+            bk.max_blocks = std::max(bk.max_blocks, q.ntiles * (bk.sh.S / bk.sh.B));
+        }
+    }
+
+    // ---- host FP64 discretisation (threads over systems) --------------------
+    std::vector<std::vector<double>> Phi(N), Bbar(N), X0(N), Ypre(N);
+    parallel_for(N, [&](int i) {
+        const SystemDesc& s = specs[i].sys;
+        Sys& q = sys_[i];
+        const int mB = s.zeroB ? 0 : s.m;
+        std::vector<double> P((size_t)q.Ns * q.Ns);
+        Bbar[i].assign((size_t)q.n * q.W * std::max(mB, 1), 0.0);
+        if (q.solver == kRK4)
+            discretise_rk4(q.n, mB, s.A.data(), mB ? s.B.data() : nullptr, q.h, P.data(), Bbar[i].data());
+        else
+            discretise_abm(q.n, mB, s.A.data(), mB ? s.B.data() : nullptr, q.h, P.data(), Bbar[i].data());
+        Phi[i].assign((size_t)q.Np * q.Np, 0.0);
+        for (int r = 0; r < q.Ns; ++r) std::memcpy(&Phi[i][(size_t)r * q.Np], &P[(size_t)r * q.Ns], sizeof(double) * q.Ns);
+        X0[i].assign((size_t)q.Np, 0.0);
+        if (q.solver == kRK4) {
+            for (int r = 0; r < q.n; ++r) X0[i][r] = s.x0[r];
+        }
+    });
+    // ABM start-up: nine inputs at t0 + j h/2 (sinusoids on the host; user
+    // functions through their compiled kernel)
+    for (int i = 0; i < N; ++i) {
+        Sys& q = sys_[i];
+        if (q.solver != kABM) continue;
+        const SystemDesc& s = specs[i].sys;
+        std::vector<double> U9((size_t)9 * std::max(s.m, 1), 0.0);
+        if (q.mu > 0) {
+            if (q.input->kind == InputEntry::kSinusoid) {
+                for (int j = 0; j < 9; ++j)
+                    for (int c = 0; c < q.mu; ++c) U9[(size_t)j * q.mu + c] = sinusoid_host(q.input, c, q.t0 + j * 0.5 * q.h);
+            } else {
+                double* dU9 = nullptr;
+                PARODE_CUDA(cudaMalloc(&dU9, sizeof(double) * 9 * q.mu));
+                inputs_->fill(q.input, device_, dU9, q.mu, q.t0, 0.5 * q.h, 9, opt_.input_double, nullptr);
+                cudaError_t e = cudaMemcpy(U9.data(), dU9, sizeof(double) * 9 * q.mu, cudaMemcpyDeviceToHost);
+                cudaFree(dU9);
+                PARODE_CUDA(e);
+            }
+        }
+        SystemDesc s0 = s;
+        if (s0.zeroB) s0.m = 0;
+        std::vector<double> Xs((size_t)4 * q.n);
+        abm_startup(s0, U9.data(), q.h, Xs.data());
+        for (int r = 0; r < 4 * q.n; ++r) X0[i][r] = Xs[r];
+        Ypre[i].assign((size_t)3 * q.p, 0.0);
+        for (int k = 0; k < 3; ++k) {
+            const double* x = &Xs[(size_t)k * q.n];
+            const double* u = &U9[(size_t)(2 * k) * std::max(s.m, 1)];
+            for (int o = 0; o < q.p; ++o) {
+                double v = 0.0;
+                if (s.zeroC && s.zeroD) {
+                    v = x[o];
+                } else {
+                    if (!s.zeroC)
+                        for (int c = 0; c < q.n; ++c) v += s.C[(size_t)o * q.n + c] * x[c];
+                    if (!s.zeroD)
+                        for (int c = 0; c < s.m; ++c) v += s.D[(size_t)o * s.m + c] * u[c];
+                }
+                Ypre[i][(size_t)k * q.p + o] = v;
+            }
+        }
+    }
+
+    // ---- arena layout: constants (staged) first, then work buffers ----------
+    Layout L;
+    Stage st;
+    struct Off {
+        size_t phi0, bbar, c, d, cext, x0, sin, ypre;
+        size_t P, U, Y, V, G, CP;
+    };
+    std::vector<Off> off(N);
+    for (int i = 0; i < N; ++i) {
+        const SystemDesc& s = specs[i].sys;
+        Sys& q = sys_[i];
+        Off& o = off[i];
+        o.phi0 = st.put(Phi[i].data(), sizeof(double) * Phi[i].size(), L);
+        o.bbar = st.put(Bbar[i].data(), sizeof(double) * Bbar[i].size(), L);
+        o.c = st.put(s.zeroC ? nullptr : s.C.data(), sizeof(double) * (s.zeroC ? 1 : (size_t)q.p * q.n), L);
+        o.d = st.put(s.zeroD ? nullptr : s.D.data(), sizeof(double) * (s.zeroD ? 1 : (size_t)q.p * s.m), L);
+        o.x0 = st.put(X0[i].data(), sizeof(double) * X0[i].size(), L);
+        if (q.blocked) {
+            std::vector<double> Cext((size_t)q.p * q.Np, 0.0);
+            const int xoff = q.solver == kRK4 ? 0 : 3 * q.n;
+            for (int r = 0; r < q.p; ++r)
+                for (int c = 0; c < q.n; ++c) {
+                    double v = 0.0;
+                    if (!s.zeroC) v = s.C[(size_t)r * q.n + c];
+                    else if (s.zeroD) v = (r == c) ? 1.0 : 0.0;
+                    Cext[(size_t)r * q.Np + xoff + c] = v;
+                }
+            o.cext = st.put(Cext.data(), sizeof(double) * Cext.size(), L);
+        }
+        if (q.mu > 0 && q.input->kind == InputEntry::kSinusoid) {
+            const InputEntry* e = q.input;
+            std::vector<double> prm;
+            prm.insert(prm.end(), e->a.begin(), e->a.end());
+            prm.insert(prm.end(), e->f.begin(), e->f.end());
+            prm.insert(prm.end(), e->phi.begin(), e->phi.end());
+            q.K = e->K;
+            o.sin = st.put(prm.data(), sizeof(double) * prm.size(), L);
+        }
+        if (q.solver == kABM) o.ypre = st.put(Ypre[i].data(), sizeof(double) * Ypre[i].size(), L);
+    }
+    const size_t const_bytes_sys = L.bytes;
+    (void)const_bytes_sys;
+    // work buffers (offsets only; not staged)
+    for (int i = 0; i < N; ++i) {
+        Sys& q = sys_[i];
+        Off& o = off[i];
+        if (q.blocked) {
+            const Bucket& bk = buckets_[q.bucket];
+            o.P = L.take(sizeof(double) * (size_t)(bk.sh.R + 1) * q.Np * q.Np);
+            o.G = L.take(sizeof(double) * (size_t)q.ntiles * (bk.sh.S / bk.sh.B) * q.Np);
+            o.CP = L.take(sizeof(double) * (size_t)bk.sh.B * q.p * q.Np);
+        } else {
+            o.P = L.take(sizeof(double) * (size_t)std::max(q.levels, 1) * q.Np * q.Np);
+            o.V = L.take(sizeof(double) * (size_t)q.Tp * q.Np);
+        }
+        o.U = q.mu > 0 ? L.take(sizeof(double) * (size_t)q.nU * q.mu) : 0;
+        o.Y = L.take(sizeof(double) * (size_t)q.nOut * q.p);
+    }
+    const size_t work_end = L.bytes;
+
+    // job arrays go after the work region, staged; their pointers are
+    // computed from the arena base, so allocate first
+    arena_bytes_ = work_end;  // grows below
+    // pre-compute the job array sizes to reserve space
+    size_t job_bytes = 0;
+    {
+        size_t nb = 0;
+        for (Bucket& bk : buckets_) {
+            long tiles = 0;
+            for (int i : bk.systems) tiles += sys_[i].ntiles;
+            (void)tiles;
+            nb += bk.systems.size();
+        }
+        // upper bounds: LeafArgs + 3 pointer arrays per blocked system, items
+        // (<= tiles), jobs and level args per LS system and level
+        long items_ub = 0;
+        for (Bucket& bk : buckets_)
+            for (int i : bk.systems) items_ub += sys_[i].ntiles;
+        long lev_entries = 0;
+        for (int i : ls_) lev_entries += 3L * std::max(sys_[i].levels, 1);
+        job_bytes = nb * (sizeof(LeafArgs) + 3 * sizeof(double*) + 4 * kAlign) +
+                    (size_t)items_ub * sizeof(BatchItem) + buckets_.size() * 8 * kAlign +
+                    (size_t)N * (sizeof(SampleJob) + sizeof(ForcingJob) + sizeof(OutputJob) + 2 * sizeof(CopyJob)) +
+                    8 * kAlign + (size_t)lev_entries * (sizeof(LevelArgs) + sizeof(long)) +
+                    (size_t)(3 * 64 * 8) * 2 * kAlign;
+    }
+    arena_bytes_ = align_up(work_end + job_bytes);
+    {
+        cudaError_t e = cudaMalloc(&arena_, arena_bytes_);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            arena_ = nullptr;
+            throw Error(kNotEnoughResources, "batch arena allocation failed");
+        }
+    }
+    char* base = static_cast<char*>(arena_);
+    auto dp = [&](size_t o) { return reinterpret_cast<double*>(base + o); };
+    for (int i = 0; i < N; ++i) {
+        Sys& q = sys_[i];
+        const Off& o = off[i];
+        q.P = dp(o.P);
+        q.Bbar = dp(o.bbar);
+        q.C = dp(o.c);
+        q.D = dp(o.d);
+        q.X0 = dp(o.x0);
+        q.Y = dp(o.Y);
+        q.U = q.mu > 0 ? dp(o.U) : nullptr;
+        if (q.blocked) {
+            q.G = dp(o.G);
+            q.CP = dp(o.CP);
+            q.Cext = dp(o.cext);
+        } else {
+            q.V = dp(o.V);
+        }
+        if (q.mu > 0 && q.input->kind == InputEntry::kSinusoid) q.sin = dp(o.sin);
+    }
+
+    // ---- job arrays (staged after the work region) ----------------------------
+    Layout J;
+    J.bytes = work_end;
+    std::vector<char> jstage;
+    auto jput = [&](const void* src, size_t n) {
+        size_t at = J.take(n);
+        if (jstage.size() < J.bytes - work_end) jstage.resize(J.bytes - work_end, 0);
+        std::memcpy(jstage.data() + (at - work_end), src, n);
+        return at;
+    };
+    std::vector<CopyJob> setup_copies;
+    for (Bucket& bk : buckets_) {
+        std::vector<LeafArgs> la;
+        std::vector<double*> cps;
+        std::vector<const double*> cexts, x0s;
+        std::vector<BatchItem> items;
+        long total_tiles = 0;
+        for (int i : bk.systems) total_tiles += sys_[i].ntiles;
+        const long target_items = 4L * sms_;
+        const long chunk = std::max<long>(1, (total_tiles + target_items - 1) / target_items);
+        for (int k = 0; k < (int)bk.systems.size(); ++k) {
+            const Sys& q = sys_[bk.systems[k]];
+            LeafArgs a;
+            a.solver = q.solver;
+            a.n = q.n;
+            a.m = q.mu;
+            a.p = q.p;
+            a.zeroB = q.zeroB;
+            a.zeroC = q.zeroC;
+            a.zeroD = q.zeroD;
+            a.nScan = q.nScan;
+            a.ntiles = q.ntiles;
+            a.ybase = q.solver == kRK4 ? 0 : 3;
+            a.P = q.P;
+            a.Bbar = q.Bbar;
+            a.C = q.C;
+            a.D = q.D;
+            a.U = q.U;
+            a.gen = 0;
+            a.stage = bk.stage ? 1 : 0;
+            a.Y = q.Y;
+            a.G = q.G;
+            la.push_back(a);
+            cps.push_back(q.CP);
+            cexts.push_back(q.Cext);
+            x0s.push_back(q.X0);
+            for (long t = 0; t < q.ntiles; t += chunk) {
+                BatchItem it;
+                it.sys = k;
+                it.t0 = t;
+                it.t1 = std::min(q.ntiles, t + chunk);
+                items.push_back(it);
+            }
+        }
+        std::stable_sort(items.begin(), items.end(),
+                         [](const BatchItem& x, const BatchItem& y) { return (x.t1 - x.t0) > (y.t1 - y.t0); });
+        BatchLaunch& b = bk.launch;
+        b.nsys = (int)la.size();
+        b.nitems = (int)items.size();
+        b.grid = (int)std::min<long>(b.nitems, sms_);
+        b.ms = bk.ms;
+        b.leaf_smem = bk.leaf_smem;
+        b.max_blocks = bk.max_blocks;
+        b.pmax = bk.pmax;
+        b.sys = reinterpret_cast<const LeafArgs*>(base + jput(la.data(), sizeof(LeafArgs) * la.size()));
+        b.items = reinterpret_cast<const BatchItem*>(base + jput(items.data(), sizeof(BatchItem) * items.size()));
+        b.CPs = reinterpret_cast<double* const*>(base + jput(cps.data(), sizeof(double*) * cps.size()));
+        b.Cexts = reinterpret_cast<const double* const*>(base + jput(cexts.data(), sizeof(double*) * cexts.size()));
+        b.X0s = reinterpret_cast<const double* const*>(base + jput(x0s.data(), sizeof(double*) * x0s.size()));
+    }
+    // input samples
+    {
+        std::vector<SampleJob> sj;
+        for (int i = 0; i < N; ++i) {
+            const Sys& q = sys_[i];
+            if (q.mu <= 0) continue;
+            if (q.input->kind != InputEntry::kSinusoid) {
+                user_inputs_.push_back(i);
+                continue;
+            }
+            SampleJob j;
+            j.U = q.U;
+            j.m = q.mu;
+            j.K = q.K;
+            const int mi = q.input->m;
+            j.a = q.sin;
+            j.f = q.sin + (long)mi * q.K;
+            j.phi = q.sin + 2L * mi * q.K;
+            j.base = q.u_base;
+            j.dt = q.u_dt;
+            j.count = q.nU;
+            maxSample_ = std::max(maxSample_, q.nU * q.mu);
+            sj.push_back(j);
+        }
+        nSampleJobs_ = (int)sj.size();
+        if (nSampleJobs_)
+            dSampleJobs_ = reinterpret_cast<SampleJob*>(base + jput(sj.data(), sizeof(SampleJob) * sj.size()));
+    }
+    // level-synchronous systems: forcing, seed, output jobs and the grouped levels
+    if (!ls_.empty()) {
+        std::vector<ForcingJob> fj;
+        std::vector<OutputJob> oj;
+        std::vector<CopyJob> cj;
+        int Lmax = 0;
+        for (int i : ls_) {
+            const Sys& q = sys_[i];
+            ForcingJob f;
+            f.V = q.V;
+            f.Np = q.Np;
+            f.n = q.n;
+            f.m = q.zeroB ? 0 : q.m;
+            f.solver = q.solver;
+            f.Bbar = q.Bbar;
+            f.U = q.U;
+            f.T = q.nScan;
+            f.Tp = q.Tp;
+            fj.push_back(f);
+            maxForcing_ = std::max(maxForcing_, q.Tp * (long)q.Np);
+            OutputJob o;
+            o.Y = q.Y;
+            o.V = q.V;
+            o.Np = q.Np;
+            o.xoff = q.solver == kRK4 ? 0 : 3 * q.n;
+            o.n = q.n;
+            o.m = q.mu;
+            o.p = q.p;
+            o.C = q.C;
+            o.D = q.D;
+            o.zeroC = q.zeroC;
+            o.zeroD = q.zeroD;
+            o.U = q.U;
+            o.ustride = q.solver == kRK4 ? 2 : 1;
+            o.uoff = q.solver == kRK4 ? 0 : 3;
+            o.count = q.nScan;
+            o.ybase = q.solver == kRK4 ? 0 : 3;
+            oj.push_back(o);
+            maxOutput_ = std::max(maxOutput_, q.nScan * (long)q.p);
+            CopyJob c;
+            c.dst = q.V + (q.Tp - 1) * (long)q.Np;
+            c.src = q.X0;
+            c.N = q.Np;
+            cj.push_back(c);
+            maxSeed_ = std::max<long>(maxSeed_, q.Np);
+            Lmax = std::max(Lmax, q.levels);
+        }
+        dForcing_ = reinterpret_cast<ForcingJob*>(base + jput(fj.data(), sizeof(ForcingJob) * fj.size()));
+        dOutput_ = reinterpret_cast<OutputJob*>(base + jput(oj.data(), sizeof(OutputJob) * oj.size()));
+        dSeed_ = reinterpret_cast<CopyJob*>(base + jput(cj.data(), sizeof(CopyJob) * cj.size()));
+        // grouped level launches: for each level, entries grouped by tiling config
+        auto add_level = [&](std::vector<GroupedLaunch>& out, const std::vector<std::pair<int, LevelArgs>>& ents) {
+            // group by (config id, CW)
+            std::vector<std::pair<std::pair<int, int>, std::vector<LevelArgs>>> groups;
+            for (const auto& e : ents) {
+                LevelConfig c = level_config(e.second.Np);
+                std::pair<int, int> key(c.id, c.CW);
+                auto it = std::find_if(groups.begin(), groups.end(), [&](const auto& g) { return g.first == key; });
+                if (it == groups.end()) {
+                    groups.push_back({key, {}});
+                    it = groups.end() - 1;
+                }
+                it->second.push_back(e.second);
+            }
+            for (auto& g : groups) {
+                GroupedLaunch gl;
+                std::vector<long> start;
+                long tiles = 0;
+                size_t smem = 0;
+                for (const LevelArgs& a : g.second) {
+                    LevelConfig c = level_config(a.Np);
+                    gl.cfg = c;
+                    start.push_back(tiles);
+                    tiles += (a.ncols + c.NC - 1) / c.NC;
+                    smem = std::max(smem, c.smem);
+                }
+                gl.nent = (int)g.second.size();
+                gl.tiles = tiles;
+                gl.smem = smem;
+                gl.args = reinterpret_cast<LevelArgs*>(base + jput(g.second.data(), sizeof(LevelArgs) * g.second.size()));
+                gl.start = reinterpret_cast<long*>(base + jput(start.data(), sizeof(long) * start.size()));
+                out.push_back(gl);
+            }
+        };
+        for (int l = 1; l < Lmax; ++l) {
+            std::vector<std::pair<int, LevelArgs>> ents;
+            for (int i : ls_) {
+                const Sys& q = sys_[i];
+                if (l >= q.levels) continue;
+                const long Np = q.Np;
+                LevelArgs a;
+                a.P = q.P + (long)(l - 1) * Np * Np;
+                a.ldp = Np;
+                a.Np = q.Np;
+                a.ncols = Np;
+                a.src = a.P;
+                a.src_gs = 1;
+                a.src_ks = Np;
+                a.dst = q.P + (long)l * Np * Np;
+                a.dst_gs = 1;
+                a.dst_is = Np;
+                ents.push_back({i, a});
+            }
+            add_level(ls_power_, ents);
+        }
+        for (int l = 0; l < Lmax; ++l) {
+            std::vector<std::pair<int, LevelArgs>> ents;
+            for (int i : ls_) {
+                const Sys& q = sys_[i];
+                if (l >= q.levels) continue;
+                const long Np = q.Np, d = 1L << l;
+                LevelArgs a;
+                a.P = q.P + (long)l * Np * Np;
+                a.ldp = Np;
+                a.Np = q.Np;
+                a.ncols = q.Tp / (2 * d);
+                a.src = q.V + (d - 1) * Np;
+                a.src_gs = 2 * d * Np;
+                a.acc = q.V + (2 * d - 1) * Np;
+                a.acc_gs = 2 * d * Np;
+                a.dst = q.V + (2 * d - 1) * Np;
+                a.dst_gs = 2 * d * Np;
+                ents.push_back({i, a});
+            }
+            add_level(ls_up_, ents);
+        }
+        for (int l = Lmax - 1; l >= 0; --l) {
+            std::vector<std::pair<int, LevelArgs>> ents;
+            for (int i : ls_) {
+                const Sys& q = sys_[i];
+                if (l >= q.levels) continue;
+                const long Np = q.Np, d = 1L << l;
+                LevelArgs a;
+                a.P = q.P + (long)l * Np * Np;
+                a.ldp = Np;
+                a.Np = q.Np;
+                a.ncols = q.Tp / (2 * d);
+                a.src = q.V + (2 * d - 1) * Np;
+                a.src_gs = 2 * d * Np;
+                a.acc = q.V + (d - 1) * Np;
+                a.acc_gs = 2 * d * Np;
+                a.dst = q.V + (2 * d - 1) * Np;
+                a.dst_gs = 2 * d * Np;
+                a.cpy = q.V + (d - 1) * Np;
+                a.cpy_gs = 2 * d * Np;
+                ents.push_back({i, a});
+            }
+            add_level(ls_down_, ents);
+        }
+    }
+    // set-up copies: Phi -> P level 0, ABM outputs 0..2 -> Y rows 0..2
+    for (int i = 0; i < N; ++i) {
+        const Sys& q = sys_[i];
+        CopyJob c;
+        c.dst = q.P;
+        c.src = dp(off[i].phi0);
+        c.N = (long)q.Np * q.Np;
+        setup_copies.push_back(c);
+        if (q.solver == kABM) {
+            CopyJob y;
+            y.dst = q.Y;
+            y.src = dp(off[i].ypre);
+            y.N = 3L * q.p;
+            setup_copies.push_back(y);
+        }
+    }
+    long max_copy = 0;
+    for (const CopyJob& c : setup_copies) max_copy = std::max(max_copy, c.N);
+    const CopyJob* dSetup =
+        reinterpret_cast<const CopyJob*>(base + jput(setup_copies.data(), sizeof(CopyJob) * setup_copies.size()));
+    if (J.bytes > arena_bytes_) throw Error(kDeviceError, "batch job arrays overflow the arena reservation");
+
+    // ---- upload and set-up launches ------------------------------------------
+    PARODE_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    PARODE_CUDA(cudaMemcpyAsync(base, st.buf.data(), st.buf.size(), cudaMemcpyHostToDevice, stream_));
+    PARODE_CUDA(cudaMemcpyAsync(base + work_end, jstage.data(), jstage.size(), cudaMemcpyHostToDevice, stream_));
+    for (size_t k = 0; k < setup_copies.size(); k += 65535)
+        launch_copy_batch(dSetup + k, (int)std::min<size_t>(65535, setup_copies.size() - k), max_copy, stream_);
+    const int nforks = (int)buckets_.size() + (ls_.empty() ? 0 : 1);
+    forks_.resize(nforks, nullptr);
+    for (auto& f : forks_) PARODE_CUDA(cudaStreamCreateWithFlags(&f, cudaStreamNonBlocking));
+    events_.resize(nforks + 1, nullptr);
+    for (auto& e : events_) PARODE_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    PARODE_CUDA(cudaStreamSynchronize(stream_));
+}
+
+BatchPlan::~BatchPlan()
+{
+    cudaSetDevice(device_);
+    if (stream_) cudaStreamSynchronize(stream_);
+    for (auto f : forks_)
+        if (f) {
+            cudaStreamSynchronize(f);
+            cudaStreamDestroy(f);
+        }
+    for (auto e : events_)
+        if (e) cudaEventDestroy(e);
+    if (arena_) cudaFree(arena_);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+double BatchPlan::state_steps() const
+{
+    double t = 0;
+    for (const Sys& q : sys_) t += (double)q.n * (double)q.nOut;
+    return t;
+}
+
+void BatchPlan::execute(cudaStream_t s)
+{
+    PARODE_CUDA(cudaSetDevice(device_));
+    if (!s) s = stream_;
+    int launches = 0;
+    // inputs for everything first
+    if (nSampleJobs_ > 0) {
+        for (int k = 0; k < nSampleJobs_; k += 65535) {
+            launch_samples_batch(dSampleJobs_ + k, std::min(65535, nSampleJobs_ - k), maxSample_, s);
+            ++launches;
+        }
+    }
+    for (int i : user_inputs_) {
+        const Sys& q = sys_[i];
+        inputs_->fill(q.input, device_, q.U, q.mu, q.u_base, q.u_dt, q.nU, opt_.input_double, s);
+        ++launches;
+    }
+    // fork: one stream per blocked bucket and one for the level-synchronous set
+    PARODE_CUDA(cudaEventRecord(events_[0], s));
+    int f = 0;
+    for (Bucket& bk : buckets_) {
+        cudaStream_t fs = forks_[f++];
+        PARODE_CUDA(cudaStreamWaitEvent(fs, events_[0], 0));
+        for (int stage = 0; stage < 4; ++stage) {
+            launch_batch_stage(stage, bk.sh, bk.launch, fs);
+            ++launches;
+        }
+    }
+    if (!ls_.empty()) {
+        cudaStream_t fs = forks_[f++];
+        PARODE_CUDA(cudaStreamWaitEvent(fs, events_[0], 0));
+        const int nls = (int)ls_.size();
+        launch_forcing_batch(dForcing_, nls, maxForcing_, fs);
+        ++launches;
+        for (const GroupedLaunch& g : ls_power_) {
+            launch_affine_level_grouped(g.cfg, g.args, g.start, g.nent, g.tiles, g.smem, fs);
+            ++launches;
+        }
+        for (const GroupedLaunch& g : ls_up_) {
+            launch_affine_level_grouped(g.cfg, g.args, g.start, g.nent, g.tiles, g.smem, fs);
+            ++launches;
+        }
+        launch_copy_batch(dSeed_, nls, maxSeed_, fs);
+        ++launches;
+        for (const GroupedLaunch& g : ls_down_) {
+            launch_affine_level_grouped(g.cfg, g.args, g.start, g.nent, g.tiles, g.smem, fs);
+            ++launches;
+        }
+        launch_output_batch(dOutput_, nls, maxOutput_, fs);
+        ++launches;
+    }
+    // join
+    for (int k = 0; k < f; ++k) {
+        PARODE_CUDA(cudaEventRecord(events_[k + 1], forks_[k]));
+        PARODE_CUDA(cudaStreamWaitEvent(s, events_[k + 1], 0));
+    }
+    launches_ = launches;
+}
+
+void BatchPlan::get_output(int i, double* t, double* y)
+{
+    if (i < 0 || i >= size()) throw Error(kInvalidArgument, "system index out of range");
+    const Sys& q = sys_[i];
+    PARODE_CUDA(cudaSetDevice(device_));
+    PARODE_CUDA(cudaStreamSynchronize(stream_));
+    PARODE_CUDA(cudaDeviceSynchronize());
+    if (y) PARODE_CUDA(cudaMemcpy(y, q.Y, sizeof(double) * (size_t)q.nOut * q.p, cudaMemcpyDeviceToHost));
+    if (t) time_vector(q.solver, q.t0, q.tEnd, q.h, t);
+}
+
+}  // namespace parode

@@ -1,0 +1,119 @@
+// batch.h -- many independent LTI solves in one set of launches.
+//
+// The reference solves one system per SimulateODE call, creating its solver
+// and buffers each time (Sources/ParODE.cpp:281-337).  A batch keeps every
+// system's matrices, power tables, scan buffers and outputs resident in one
+// device arena and runs all systems together:
+//  - scan dimension <= 64: the blocked path per padded dimension NP, batched
+//    (one tables launch, one persistent leaf launch over work items of all
+//    systems, one chain launch, one fix-up launch per NP);
+//  - larger scan dimensions: the level-synchronous path with one grouped
+//    contraction launch per level and tiling configuration over all systems.
+// Inputs: sum-of-sinusoid inputs are sampled by one batched launch; user
+// (NVRTC) inputs by one launch per system.
+#pragma once
+
+#include "blocked.h"
+#include "host_math.h"
+#include "inputs.h"
+#include "kernels.h"
+#include "solver.h"
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <vector>
+
+namespace parode {
+
+struct BatchSpec {
+    SystemDesc sys;
+    int uIndex = 0;
+    int solver = 0;
+    double t0 = 0, tEnd = 0, h = 0;
+};
+
+class BatchPlan {
+public:
+    BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* inputs, const PlanOptions& opt);
+    ~BatchPlan();
+    BatchPlan(const BatchPlan&) = delete;
+    BatchPlan& operator=(const BatchPlan&) = delete;
+
+    // Enqueue all solves on `s` (nullptr: the batch's stream).
+    void execute(cudaStream_t s);
+    int size() const { return (int)sys_.size(); }
+    long num_outputs(int i) const { return sys_[i].nOut; }
+    int channels(int i) const { return sys_[i].p; }
+    // Synchronises and copies system i's time vector and outputs to the host.
+    void get_output(int i, double* t, double* y);
+    const double* device_output(int i) const { return sys_[i].Y; }
+    int launch_count() const { return launches_; }
+    int precision_used(int i) const { return sys_[i].precision; }
+    int path(int i) const { return sys_[i].blocked ? kPathBlocked : kPathLevel; }
+    // Sum over systems of n * outputs (state*steps of one execute).
+    double state_steps() const;
+    size_t device_bytes() const { return arena_bytes_; }
+    cudaStream_t stream() const { return stream_; }
+
+private:
+    struct Sys {
+        int solver = 0, n = 0, m = 0, mu = 0, p = 0, Ns = 0, Np = 0, W = 3;
+        long nOut = 0, nScan = 0, nU = 0, Tp = 1;
+        int levels = 0;
+        bool blocked = false;
+        int bucket = -1;          // blocked: index into buckets_
+        int precision = 0;
+        InputEntry* input = nullptr;
+        double u_base = 0, u_dt = 0;
+        double t0 = 0, tEnd = 0, h = 0;
+        // device pointers inside the arena
+        double *P = nullptr, *Bbar = nullptr, *C = nullptr, *D = nullptr, *X0 = nullptr, *U = nullptr;
+        double *Y = nullptr, *V = nullptr, *G = nullptr, *CP = nullptr, *Cext = nullptr, *sin = nullptr;
+        int K = 0;
+        bool zeroB = true, zeroC = true, zeroD = true;
+        long ntiles = 0;
+    };
+    struct Bucket {
+        BlockedShape sh;
+        std::vector<int> systems;
+        int ms = 0, pmax = 1;
+        long max_blocks = 0;
+        bool stage = false;
+        size_t leaf_smem = 0;
+        BatchLaunch launch;  // device arrays filled at set-up
+    };
+    struct GroupedLaunch {
+        LevelConfig cfg;
+        LevelArgs* args = nullptr;  // device
+        long* start = nullptr;      // device
+        int nent = 0;
+        long tiles = 0;
+        size_t smem = 0;
+    };
+
+    int device_ = 0;
+    int sms_ = 148;
+    cudaStream_t stream_ = nullptr;
+    std::vector<cudaStream_t> forks_;
+    std::vector<cudaEvent_t> events_;
+    InputRegistry* inputs_ = nullptr;
+    PlanOptions opt_;
+    std::vector<Sys> sys_;
+    std::vector<Bucket> buckets_;
+    std::vector<int> ls_;  // level-synchronous systems
+    std::vector<GroupedLaunch> ls_power_, ls_up_, ls_down_;
+    SampleJob* dSampleJobs_ = nullptr;
+    int nSampleJobs_ = 0;
+    long maxSample_ = 0;
+    std::vector<int> user_inputs_;  // systems sampled by their own launch
+    ForcingJob* dForcing_ = nullptr;
+    OutputJob* dOutput_ = nullptr;
+    CopyJob* dSeed_ = nullptr;
+    long maxForcing_ = 0, maxOutput_ = 0, maxSeed_ = 0;
+    void* arena_ = nullptr;
+    size_t arena_bytes_ = 0;
+    int launches_ = 0;
+};
+
+}  // namespace parode

@@ -80,4 +80,40 @@ void launch_blocked_fixup(const BlockedShape& sh, double* Y, long ybase, long nS
 void launch_blocked_tables(const BlockedShape& sh, double* P, int l0, int l1, double* CP, const double* Cext, int p,
                            cudaStream_t s);
 
+// ---------------------------------------------------------------------------
+// Batched form: many independent systems of one padded dimension NP.  Each
+// system is described by a LeafArgs (P holds power-table levels 0..R, G its
+// block aggregates, which the chain stage turns into block carries).  Stages,
+// in order: 0 tables (one CTA per system: P levels 1..R and CP), 1 leaf
+// (work items = tile ranges, largest first, dealt round-robin to the CTAs),
+// 2 chain (one CTA per system: X_{b+1} = P_R X_b + G_b in FP64, sequential
+// over the system's blocks), 3 fix-up (y += C Phi^j X_b).
+// ---------------------------------------------------------------------------
+
+struct BatchItem {
+    int sys = 0;
+    int pad = 0;
+    long t0 = 0, t1 = 0;  // tiles [t0, t1) of system `sys`
+};
+
+struct BatchLaunch {
+    const LeafArgs* sys = nullptr;     // device, nsys entries
+    int nsys = 0;
+    const BatchItem* items = nullptr;  // device, nitems entries
+    int nitems = 0;
+    int grid = 0;                      // leaf CTAs
+    int ms = 0;                        // largest m (sample staging width)
+    size_t leaf_smem = 0;
+    double* const* CPs = nullptr;      // device array of per-system CP tables (B x p x NP)
+    const double* const* Cexts = nullptr;
+    const double* const* X0s = nullptr;
+    long max_blocks = 0;               // largest block count of a system
+    int pmax = 1;
+};
+
+// Leaf shared memory for a batch: sample staging for the widest input and
+// `stage_doubles` of staged Bbar | C | D (0 when not staged).
+size_t batch_leaf_smem(const BlockedShape& sh, int ms, long stage_doubles);
+void launch_batch_stage(int what, const BlockedShape& sh, const BatchLaunch& b, cudaStream_t s);
+
 }  // namespace parode

@@ -46,4 +46,59 @@ void launch_copy(double* dst, const double* src, long N, cudaStream_t s);
 // Kernel launches made by the last call of each launcher (for accounting).
 int launches_per_level();
 
+// ---------------------------------------------------------------------------
+// Batched forms (many systems per launch).  Every batched kernel takes a
+// device array of jobs; blockIdx.y selects the job.
+// ---------------------------------------------------------------------------
+
+// Tiling of the level contraction for a contraction length Np: entries of one
+// grouped launch must share the config id (and CW).
+struct LevelConfig {
+    int id = 0;     // template configuration
+    int CW = 1;     // column warps
+    int NC = 0;     // columns per CTA
+    size_t smem = 0;
+};
+LevelConfig level_config(int Np);
+
+// One level over nent systems: dStart (device, nent entries) holds each
+// entry's first CTA; `tiles` CTAs in total; smem = max over entries.
+void launch_affine_level_grouped(const LevelConfig& c, const LevelArgs* dArgs, const long* dStart, int nent,
+                                 long tiles, size_t smem, cudaStream_t s);
+
+struct SampleJob {
+    double* U = nullptr;
+    int m = 0, K = 0;
+    const double *a = nullptr, *f = nullptr, *phi = nullptr;
+    double base = 0, dt = 0;
+    long count = 0;
+};
+struct ForcingJob {
+    double* V = nullptr;
+    int Np = 0, n = 0, m = 0, solver = 0;
+    const double* Bbar = nullptr;
+    const double* U = nullptr;
+    long T = 0, Tp = 0;
+};
+struct OutputJob {
+    double* Y = nullptr;
+    const double* V = nullptr;
+    int Np = 0, xoff = 0, n = 0, m = 0, p = 0;
+    const double *C = nullptr, *D = nullptr;
+    int zeroC = 1, zeroD = 1;
+    const double* U = nullptr;
+    int ustride = 1, uoff = 0;
+    long count = 0, ybase = 0;
+};
+struct CopyJob {
+    double* dst = nullptr;
+    const double* src = nullptr;
+    long N = 0;
+};
+// max_elems: the largest element count of a job (sizes the x dimension).
+void launch_samples_batch(const SampleJob* dJobs, int njobs, long max_elems, cudaStream_t s);
+void launch_forcing_batch(const ForcingJob* dJobs, int njobs, long max_elems, cudaStream_t s);
+void launch_output_batch(const OutputJob* dJobs, int njobs, long max_elems, cudaStream_t s);
+void launch_copy_batch(const CopyJob* dJobs, int njobs, long max_elems, cudaStream_t s);
+
 }  // namespace parode

@@ -166,13 +166,86 @@ __device__ void level_swap(double* sV, int c, int d)
 // leaf kernel
 // ---------------------------------------------------------------------------
 
+// Shared-memory regions of the leaf: R power-table levels, the tile's vectors,
+// its input samples (su_doubles) and, when a.stage is set, Bbar | C | D.
+template <int NP>
+struct LeafSmem {
+    double* sP;
+    double* sV;
+    double* sU;
+    const double* pB;
+    const double* pC;
+    const double* pD;
+};
+
+// Per-system set-up of the leaf: power-table levels (and Bbar / C / D when
+// staged) into shared memory.  Ends with the staged data visible to the CTA
+// only after the caller's next __syncthreads (every tile starts with one).
+template <int NP>
+__device__ LeafSmem<NP> leaf_setup(const LeafArgs& a, double* sm, int R, int S, long su_doubles)
+{
+    LeafSmem<NP> L;
+    L.sP = sm;
+    L.sV = L.sP + (long)R * NP * NP;
+    L.sU = L.sV + (long)S * NP;
+    const int m = a.m, n = a.n, p = a.p;
+    const int Wm = (a.solver == 0 ? 3 : 5) * m;
+    for (int l = 0; l < R; ++l) load_matrix<NP>(L.sP + (long)l * NP * NP, a.P + (long)l * NP * NP);
+    L.pB = a.Bbar;
+    L.pC = a.C;
+    L.pD = a.D;
+    if (a.stage) {
+        double* sM = L.sU + su_doubles;
+        // Bbar is n x W m only when B is present (it is never read otherwise)
+        const long nb = a.zeroB ? 0 : (long)n * Wm, nc = (long)p * n, nd = (long)p * m;
+        for (long e = threadIdx.x; e < nb; e += kThreads) sM[e] = a.Bbar[e];
+        for (long e = threadIdx.x; e < nc; e += kThreads) sM[nb + e] = a.zeroC ? 0.0 : a.C[e];
+        for (long e = threadIdx.x; e < nd; e += kThreads) sM[nb + nc + e] = a.zeroD ? 0.0 : a.D[e];
+        L.pB = sM;
+        L.pC = sM + nb;
+        L.pD = sM + nb + nc;
+    }
+    return L;
+}
+
+template <int NP>
+__device__ void leaf_tile(const LeafArgs& a, const LeafSmem<NP>& L, long tile, int R, int S);
+
 template <int NP>
 __global__ void __launch_bounds__(kThreads, 1) k_leaf(LeafArgs a, int R, int S)
 {
     extern __shared__ double sm[];
-    double* sP = sm;
-    double* sV = sP + (long)R * NP * NP;
-    double* sU = sV + (long)S * NP;
+    const long su = (long)(a.solver == 0 ? 2 * S + 1 : S + 4) * (a.m > 0 ? a.m : 1);
+    const LeafSmem<NP> L = leaf_setup<NP>(a, sm, R, S, su);
+    for (long tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) leaf_tile<NP>(a, L, tile, R, S);
+}
+
+// Batched leaf: work items (system, tile range), dealt round-robin to the
+// CTAs in the order given (largest first).
+template <int NP>
+__global__ void __launch_bounds__(kThreads, 1) k_leaf_batch(const LeafArgs* __restrict__ sys,
+                                                            const BatchItem* __restrict__ items, int nitems, int R,
+                                                            int S, int ms)
+{
+    extern __shared__ double sm[];
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const BatchItem w = items[it];
+        const LeafArgs a = sys[w.sys];
+        __syncthreads();  // the previous item's tiles are done with shared memory
+        const LeafSmem<NP> L = leaf_setup<NP>(a, sm, R, S, (long)(2 * S + 1) * (ms > 0 ? ms : 1));
+        for (long tile = w.t0; tile < w.t1; ++tile) leaf_tile<NP>(a, L, tile, R, S);
+    }
+}
+
+template <int NP>
+__device__ void leaf_tile(const LeafArgs& a, const LeafSmem<NP>& L, long tile, int R, int S)
+{
+    double* sV = L.sV;
+    double* sU = L.sU;
+    const double* sP = L.sP;
+    const double* pB = L.pB;
+    const double* pC = L.pC;
+    const double* pD = L.pD;
     const int B = 1 << R;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int gq = lane >> 2, tq = lane & 3;
@@ -184,24 +257,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_leaf(LeafArgs a, int R, int S)
     const int nsamp = rk4 ? 2 * S + 1 : S + 4;
     const int coff = rk4 ? 0 : 3 * n;  // forcing rows / output state block
     const long nU = rk4 ? 2 * a.nScan + 1 : a.nScan + 4;
-
-    for (int l = 0; l < R; ++l) load_matrix<NP>(sP + (long)l * NP * NP, a.P + (long)l * NP * NP);
-    // Bbar, C and D stay on chip for the whole kernel when they fit
-    const double* pB = a.Bbar;
-    const double* pC = a.C;
-    const double* pD = a.D;
-    if (a.stage) {
-        double* sM = sU + (long)nsamp * (m > 0 ? m : 1);
-        const long nb = (long)n * Wm, nc = (long)p * n, nd = (long)p * m;
-        for (long e = tid; e < nb; e += kThreads) sM[e] = a.Bbar[e];
-        for (long e = tid; e < nc; e += kThreads) sM[nb + e] = a.zeroC ? 0.0 : a.C[e];
-        for (long e = tid; e < nd; e += kThreads) sM[nb + nc + e] = a.zeroD ? 0.0 : a.D[e];
-        pB = sM;
-        pC = sM + nb;
-        pD = sM + nb + nc;
-    }
-
-    for (long tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+    {
         const long j0 = tile * S;
         const long js0 = rk4 ? 2 * j0 : j0;
         // 1. input samples of the tile (u-kernel of the reference)
@@ -447,10 +503,31 @@ __global__ void __launch_bounds__(kThreads, 1) k_items_top(double* items, long c
 // y[(ybase + j) p + o] += CP[j mod B][o] . X[j div B] as a DMMA GEMM with
 // M = B p (rows (jj, o), contiguous in y per block), K = NP, N = blocks.
 template <int NP>
+__device__ void fixup_body(double* Y, long ybase, long nScan, int p, const double* CP, const double* X, int B,
+                           long cta, long ncta, double* sm);
+
+template <int NP>
 __global__ void __launch_bounds__(kThreads) k_fixup(double* Y, long ybase, long nScan, int p, const double* CP,
                                                     const double* X, int B)
 {
     extern __shared__ double sm[];
+    fixup_body<NP>(Y, ybase, nScan, p, CP, X, B, blockIdx.x, gridDim.x, sm);
+}
+
+// Batched fix-up: blockIdx.y selects the system, blockIdx.x strides its blocks.
+template <int NP>
+__global__ void __launch_bounds__(kThreads) k_fixup_batch(const LeafArgs* __restrict__ sys, const double* const* CPs,
+                                                          int B)
+{
+    extern __shared__ double sm[];
+    const LeafArgs& a = sys[blockIdx.y];
+    fixup_body<NP>(a.Y, a.ybase, a.nScan, a.p, CPs[blockIdx.y], a.G, B, blockIdx.x, gridDim.x, sm);
+}
+
+template <int NP>
+__device__ void fixup_body(double* Y, long ybase, long nScan, int p, const double* CP, const double* X, int B,
+                           long cta, long ncta, double* sm)
+{
     const int M = B * p;
     const int Mp = (M + 7) & ~7;
     const int rfs = Mp >> 3;
@@ -471,7 +548,7 @@ __global__ void __launch_bounds__(kThreads) k_fixup(double* Y, long ybase, long 
         __syncthreads();
     // a warp owns 8 blocks (one fragment column): their carries are loaded
     // once per CP chunk as B fragments and reused for every fragment row
-    for (long cb = (long)blockIdx.x * 8 + warp; cb < cfs; cb += (long)gridDim.x * 8) {
+    for (long cb = cta * 8 + warp; cb < cfs; cb += ncta * 8) {
         const long bb = cb * 8 + gq;
         double bv[NP / 4];
 #pragma unroll
@@ -506,10 +583,69 @@ __global__ void __launch_bounds__(kThreads) k_fixup(double* Y, long ybase, long 
 
 // Power table continuation and the output table CP (one CTA).
 template <int NP>
+__device__ void tables_body(double* P, int l0, int l1, double* CP, const double* Cext, int p, int R, double* sm);
+
+template <int NP>
 __global__ void __launch_bounds__(kThreads, 1) k_tables(double* P, int l0, int l1, double* CP, const double* Cext,
                                                         int p, int R)
 {
     extern __shared__ double sm[];
+    tables_body<NP>(P, l0, l1, CP, Cext, p, R, sm);
+}
+
+// Batched tables: one CTA per system (P levels 1..l1-1, CP for B = 2^R).
+template <int NP>
+__global__ void __launch_bounds__(kThreads, 1) k_tables_batch(const LeafArgs* __restrict__ sys, double* const* CPs,
+                                                              const double* const* Cexts, int l1, int R)
+{
+    extern __shared__ double sm[];
+    const LeafArgs& a = sys[blockIdx.x];
+    tables_body<NP>(const_cast<double*>(a.P), 1, l1, CPs[blockIdx.x], Cexts[blockIdx.x], a.p, R, sm);
+}
+
+// Sequential carry over the blocks of one system per CTA (FP64):
+//   X_0 = x0, X_{b+1} = P_R X_b + G_b, and G_b <- X_b (the block's carry).
+// Row i of the product is owned by thread i (NP <= 64 threads active).
+template <int NP>
+__global__ void __launch_bounds__(kThreads, 1) k_chain_batch(const LeafArgs* __restrict__ sys,
+                                                             const double* const* X0s, int R, int bpt)
+{
+    __shared__ double sA[NP * (NP + 1)];
+    __shared__ double sX[2][NP];
+    const LeafArgs& a = sys[blockIdx.x];
+    const double* PR = a.P + (long)R * NP * NP;
+    for (int e = threadIdx.x; e < NP * NP; e += kThreads) sA[(e / NP) * (NP + 1) + e % NP] = PR[e];
+    if (threadIdx.x < NP) sX[0][threadIdx.x] = X0s[blockIdx.x][threadIdx.x];
+    __syncthreads();
+    const long nb = a.ntiles * bpt;
+    const int i = threadIdx.x;
+    int cur = 0;
+    double g = (i < NP && nb > 0) ? a.G[i] : 0.0;
+    for (long b = 0; b < nb; ++b) {
+        double gn = (i < NP && b + 1 < nb) ? a.G[(b + 1) * NP + i] : 0.0;  // prefetch the next aggregate
+        if (i < NP) {
+            const double* row = sA + i * (NP + 1);
+            const double* x = sX[cur];
+            double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+#pragma unroll
+            for (int k = 0; k < NP; k += 4) {
+                s0 = fma(row[k], x[k], s0);
+                s1 = fma(row[k + 1], x[k + 1], s1);
+                s2 = fma(row[k + 2], x[k + 2], s2);
+                s3 = fma(row[k + 3], x[k + 3], s3);
+            }
+            a.G[b * NP + i] = x[i];
+            sX[cur ^ 1][i] = ((s0 + s1) + (s2 + s3)) + g;
+        }
+        g = gn;
+        cur ^= 1;
+        __syncthreads();
+    }
+}
+
+template <int NP>
+__device__ void tables_body(double* P, int l0, int l1, double* CP, const double* Cext, int p, int R, double* sm)
+{
     double* sA = sm;             // current P_l (swizzled)
     double* sN = sm + NP * NP;   // next
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -750,6 +886,61 @@ void launch_blocked_tables(const BlockedShape& sh, double* P, int l0, int l1, do
     case 32: tables_t<32>(sh, P, l0, l1, CP, Cext, p, s); break;
     case 64: tables_t<64>(sh, P, l0, l1, CP, Cext, p, s); break;
     default: throw Error(kInvalidArgument, "blocked path: unsupported NP");
+    }
+}
+
+// ---------------------------------------------------------------------------
+// batched launchers
+// ---------------------------------------------------------------------------
+
+size_t batch_leaf_smem(const BlockedShape& sh, int ms, long stage_doubles)
+{
+    size_t base = (size_t)sh.R * sh.NP * sh.NP * sizeof(double) + (size_t)sh.S * sh.NP * sizeof(double) +
+                  (size_t)(2 * sh.S + 1) * std::max(ms, 1) * sizeof(double);
+    return base + (size_t)stage_doubles * sizeof(double);
+}
+
+template <int NP>
+static void batch_t(int what, const BlockedShape& sh, const BatchLaunch& b, cudaStream_t s)
+{
+    switch (what) {
+    case 0: {
+        size_t smem = 2 * (size_t)NP * NP * sizeof(double);
+        set_smem(k_tables_batch<NP>, smem);
+        k_tables_batch<NP><<<b.nsys, kThreads, smem, s>>>(b.sys, b.CPs, b.Cexts, sh.R + 1, sh.R);
+        break;
+    }
+    case 1: {
+        set_smem(k_leaf_batch<NP>, b.leaf_smem);
+        k_leaf_batch<NP><<<b.grid, kThreads, b.leaf_smem, s>>>(b.sys, b.items, b.nitems, sh.R, sh.S, b.ms);
+        break;
+    }
+    case 2:
+        k_chain_batch<NP><<<b.nsys, kThreads, 0, s>>>(b.sys, b.X0s, sh.R, sh.S / sh.B);
+        break;
+    case 3: {
+        const int Mp = (sh.B * b.pmax + 7) & ~7;
+        size_t smem = (size_t)std::min(Mp, fixup_chunk_rows<NP>()) * NP * sizeof(double);
+        set_smem(k_fixup_batch<NP>, smem);
+        long cfs = (b.max_blocks + 7) / 8;
+        unsigned gx = (unsigned)std::max<long>(1, std::min<long>((cfs + 7) / 8, 16));
+        dim3 grid(gx, (unsigned)b.nsys);
+        k_fixup_batch<NP><<<grid, kThreads, smem, s>>>(b.sys, b.CPs, sh.B);
+        break;
+    }
+    }
+    PARODE_CUDA(cudaGetLastError());
+}
+
+void launch_batch_stage(int what, const BlockedShape& sh, const BatchLaunch& b, cudaStream_t s)
+{
+    if (b.nsys <= 0) return;
+    switch (sh.NP) {
+    case 8: batch_t<8>(what, sh, b, s); break;
+    case 16: batch_t<16>(what, sh, b, s); break;
+    case 32: batch_t<32>(what, sh, b, s); break;
+    case 64: batch_t<64>(what, sh, b, s); break;
+    default: throw Error(kInvalidArgument, "batched blocked path: unsupported NP");
     }
 }
 

@@ -20,19 +20,54 @@ namespace {
 
 constexpr int kThreads = 256;
 
+// K-slice of the staged operands for a contraction length Np.
+__host__ __device__ inline int level_ks(int Np)
+{
+    int ks = 8192 / Np;
+    ks = ks < 4 ? 4 : (ks > 32 ? 32 : ks);
+    return ks & ~3;
+}
+
 // One CTA owns NC = 8*FC*CW columns and all Np rows of the result; each warp
 // owns an FR x FC block of 8x8 fragments.  P and the source columns are
 // staged through shared memory in K slices of KS (row pitch KS+4 doubles,
 // which spreads the 8 fragment rows over distinct bank groups).
 template <int FR, int FC>
+__device__ void affine_level_body(const LevelArgs& a, long tile, int CW, int KS, double* smem);
+
+template <int FR, int FC>
 __global__ void __launch_bounds__(kThreads) k_affine_level(LevelArgs a, int CW, int KS)
 {
     extern __shared__ double smem[];
+    affine_level_body<FR, FC>(a, blockIdx.x, CW, KS, smem);
+}
+
+// Grouped form: entry e owns tiles [start[e], start[e+1]) of the grid; each
+// CTA finds its entry by binary search.  KS follows each entry's Np.
+template <int FR, int FC>
+__global__ void __launch_bounds__(kThreads) k_affine_level_grouped(const LevelArgs* __restrict__ args,
+                                                                   const long* __restrict__ start, int nent, int CW)
+{
+    extern __shared__ double smem[];
+    const long t = blockIdx.x;
+    int lo = 0, hi = nent - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (start[mid] <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    const LevelArgs a = args[lo];
+    affine_level_body<FR, FC>(a, t - start[lo], CW, level_ks(a.Np), smem);
+}
+
+template <int FR, int FC>
+__device__ void affine_level_body(const LevelArgs& a, long tile, int CW, int KS, double* smem)
+{
     const int ldk = KS + 4;
     double* sP = smem;
     const int NC = 8 * FC * CW;
     double* sV = smem + (long)a.Np * ldk;
-    const long g0 = (long)blockIdx.x * NC;
+    const long g0 = tile * NC;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wr = warp / CW, wc = warp % CW;
     const int gq = lane >> 2, tq = lane & 3;
@@ -163,13 +198,83 @@ __global__ void k_copy(double* dst, const double* src, long N)
     if (e < N) dst[e] = src[e];
 }
 
+// Batched element kernels: blockIdx.y selects the job, the x dimension
+// strides over its elements; each element is computed as by the single-system
+// kernels above.
+__global__ void k_samples_batch(const SampleJob* __restrict__ jobs)
+{
+    const SampleJob J = jobs[blockIdx.y];
+    const long total = J.count * J.m;
+    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+        const long j = e / J.m;
+        const int i = (int)(e - j * J.m);
+        J.U[e] = sinusoid_value(J.a, J.f, J.phi, J.K, i, sample_time(J.base, J.dt, j));
+    }
+}
+
+__global__ void k_forcing_batch(const ForcingJob* __restrict__ jobs)
+{
+    const ForcingJob J = jobs[blockIdx.y];
+    const long total = J.Tp * (long)J.Np;
+    const int n = J.n, m = J.m;
+    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+        const long k = e / J.Np;
+        const int i = (int)(e - k * J.Np);
+        double v = 0.0;
+        if (k < J.T && m > 0) {
+            if (J.solver == 0) {
+                if (i < n) {
+                    const double* b = J.Bbar + (long)i * 3 * m;
+                    const double* u = J.U + 2 * k * m;
+                    for (int q = 0; q < 3 * m; ++q) v = fma(b[q], u[q], v);
+                }
+            } else if (i >= 3 * n && i < 4 * n) {
+                const double* b = J.Bbar + (long)(i - 3 * n) * 5 * m;
+                const double* u = J.U + k * m;
+                for (int q = 0; q < 5 * m; ++q) v = fma(b[q], u[q], v);
+            }
+        }
+        J.V[e] = v;
+    }
+}
+
+__global__ void k_output_batch(const OutputJob* __restrict__ jobs)
+{
+    const OutputJob J = jobs[blockIdx.y];
+    const int p = J.p, n = J.n, m = J.m;
+    const long total = J.count * (long)p;
+    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+        const long k = e / p;
+        const int o = (int)(e - k * p);
+        const double* x = J.V + k * J.Np + J.xoff;
+        double v = 0.0;
+        if (J.zeroC && J.zeroD) {
+            v = x[o];
+        } else {
+            if (!J.zeroC)
+                for (int c = 0; c < n; ++c) v = fma(J.C[(long)o * n + c], x[c], v);
+            if (!J.zeroD && m > 0) {
+                const double* u = J.U + (k * J.ustride + J.uoff) * m;
+                for (int c = 0; c < m; ++c) v = fma(J.D[(long)o * m + c], u[c], v);
+            }
+        }
+        J.Y[(J.ybase + k) * p + o] = v;
+    }
+}
+
+__global__ void k_copy_batch(const CopyJob* __restrict__ jobs)
+{
+    const CopyJob J = jobs[blockIdx.y];
+    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < J.N; e += (long)gridDim.x * blockDim.x)
+        J.dst[e] = J.src[e];
+}
+
 inline unsigned blocks_for(long n, int t) { return (unsigned)((n + t - 1) / t); }
 
 template <int FR, int FC>
 void launch_level_t(const LevelArgs& a, int CW, cudaStream_t s)
 {
-    int KS = (int)std::min<long>(32, std::max<long>(4, 8192 / a.Np));
-    KS &= ~3;
+    const int KS = level_ks(a.Np);
     const int NC = 8 * FC * CW;
     size_t smem = (size_t)(a.Np + NC) * (KS + 4) * sizeof(double);
     static bool attr_set = false;
@@ -242,5 +347,95 @@ void launch_copy(double* dst, const double* src, long N, cudaStream_t s)
 }
 
 int launches_per_level() { return 1; }
+
+// ---------------------------------------------------------------------------
+// grouped / batched launchers
+// ---------------------------------------------------------------------------
+
+LevelConfig level_config(int Np)
+{
+    LevelConfig c;
+    const int rf = Np / 8;
+    if (rf <= 8) {
+        int RW = 1;
+        while (RW < rf) RW <<= 1;
+        c.id = 0;
+        c.CW = 8 / RW;
+    } else if (rf <= 16) {
+        c.id = 1;
+    } else if (rf <= 32) {
+        c.id = 2;
+    } else if (rf <= 64) {
+        c.id = 3;
+    } else {
+        c.id = 4;
+    }
+    static const int fc[5] = {4, 4, 4, 2, 1};
+    c.NC = 8 * fc[c.id] * c.CW;
+    c.smem = (size_t)(Np + c.NC) * (level_ks(Np) + 4) * sizeof(double);
+    return c;
+}
+
+namespace {
+template <int FR, int FC>
+void grouped_t(const LevelConfig& c, const LevelArgs* args, const long* start, int nent, long tiles, size_t smem,
+               cudaStream_t s)
+{
+    static bool attr_set = false;
+    if (!attr_set) {
+        PARODE_CUDA(cudaFuncSetAttribute(k_affine_level_grouped<FR, FC>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        attr_set = true;
+    }
+    k_affine_level_grouped<FR, FC><<<(unsigned)tiles, kThreads, smem, s>>>(args, start, nent, c.CW);
+    PARODE_CUDA(cudaGetLastError());
+}
+}  // namespace
+
+void launch_affine_level_grouped(const LevelConfig& c, const LevelArgs* dArgs, const long* dStart, int nent,
+                                 long tiles, size_t smem, cudaStream_t s)
+{
+    if (nent <= 0 || tiles <= 0) return;
+    if (smem > 200 * 1024) throw Error(kInvalidArgument, "grouped level: shared memory above 200 KB");
+    switch (c.id) {
+    case 0: grouped_t<1, 4>(c, dArgs, dStart, nent, tiles, smem, s); break;
+    case 1: grouped_t<2, 4>(c, dArgs, dStart, nent, tiles, smem, s); break;
+    case 2: grouped_t<4, 4>(c, dArgs, dStart, nent, tiles, smem, s); break;
+    case 3: grouped_t<8, 2>(c, dArgs, dStart, nent, tiles, smem, s); break;
+    default: grouped_t<16, 1>(c, dArgs, dStart, nent, tiles, smem, s); break;
+    }
+}
+
+void launch_samples_batch(const SampleJob* dJobs, int njobs, long max_elems, cudaStream_t s)
+{
+    if (njobs <= 0 || max_elems <= 0) return;
+    dim3 grid((unsigned)std::min<long>(blocks_for(max_elems, 256), 64), (unsigned)njobs);
+    k_samples_batch<<<grid, 256, 0, s>>>(dJobs);
+    PARODE_CUDA(cudaGetLastError());
+}
+
+void launch_forcing_batch(const ForcingJob* dJobs, int njobs, long max_elems, cudaStream_t s)
+{
+    if (njobs <= 0 || max_elems <= 0) return;
+    dim3 grid((unsigned)std::min<long>(blocks_for(max_elems, 256), 64), (unsigned)njobs);
+    k_forcing_batch<<<grid, 256, 0, s>>>(dJobs);
+    PARODE_CUDA(cudaGetLastError());
+}
+
+void launch_output_batch(const OutputJob* dJobs, int njobs, long max_elems, cudaStream_t s)
+{
+    if (njobs <= 0 || max_elems <= 0) return;
+    dim3 grid((unsigned)std::min<long>(blocks_for(max_elems, 256), 64), (unsigned)njobs);
+    k_output_batch<<<grid, 256, 0, s>>>(dJobs);
+    PARODE_CUDA(cudaGetLastError());
+}
+
+void launch_copy_batch(const CopyJob* dJobs, int njobs, long max_elems, cudaStream_t s)
+{
+    if (njobs <= 0 || max_elems <= 0) return;
+    dim3 grid((unsigned)std::min<long>(blocks_for(max_elems, 256), 16), (unsigned)njobs);
+    k_copy_batch<<<grid, 256, 0, s>>>(dJobs);
+    PARODE_CUDA(cudaGetLastError());
+}
 
 }  // namespace parode

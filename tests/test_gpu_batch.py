@@ -1,0 +1,121 @@
+"""GPU parity of the batched form (ParODE_Batch*) against the CPU FP64 oracle.
+
+Every system of a batch must match its own sequential FP64 recurrence (O1)
+to the plain-scan gate, 1e-12 per-channel relative error, whatever the mix of
+scan dimensions (blocked buckets NP = 8..64 and level-synchronous systems),
+integrators, horizons and absent matrices in the batch.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle
+from parode_b200 import workloads as wl
+
+pytestmark = pytest.mark.gpu
+
+TOL_FP64 = 1e-12
+
+
+def _oracle_y(case, B=True, Cm=True, D=True):
+    sysd = oracle.System(case.A, case.B if B else None, case.C if Cm else None, case.D if D else None, case.x0)
+    inp = oracle.Input.sinusoid(case.u.a, case.u.f, case.u.phi)
+    return oracle.simulate_affine(sysd, inp, case.solver, case.t0, case.t_end, case.h)
+
+
+def _spec(pb, case, B=True, Cm=True, D=True):
+    u = pb.register_sinusoid(case.u.a, case.u.f, case.u.phi)
+    return {"A": case.A, "B": case.B if B else None, "C": case.C if Cm else None, "D": case.D if D else None,
+            "x0": case.x0, "u": u, "t0": case.t0, "t_end": case.t_end, "h": case.h, "solver": case.solver}
+
+
+MIX = [  # (solver, n, m, p, T, B, C, D)
+    (0, 3, 1, 2, 700, True, True, True),      # NP 8
+    (0, 13, 2, 2, 2500, True, True, True),    # NP 16
+    (0, 40, 4, 5, 3000, True, True, True),    # NP 64
+    (1, 2, 1, 1, 900, True, True, True),      # ABM, N_s 8
+    (1, 10, 2, 3, 1500, True, True, True),    # ABM, N_s 40
+    (1, 20, 3, 2, 1200, True, True, True),    # ABM, N_s 80: level-synchronous
+    (0, 70, 5, 4, 1000, True, True, True),    # RK4 n 70: level-synchronous
+    (0, 6, 2, 2, 333, False, True, True),     # no B
+    (0, 9, 2, 2, 444, True, False, False),    # y = x
+    (1, 5, 2, 2, 555, True, False, True),     # ABM, no C
+    (0, 1, 1, 1, 1, True, True, True),        # one step
+    (1, 1, 1, 1, 4, True, True, True),        # ABM, one scan step
+    (0, 33, 3, 3, 4097, True, True, True),    # NP 64, ragged tiles
+    (1, 30, 2, 2, 2049, True, True, False),   # ABM N_s 120, level-synchronous
+]
+
+
+def _mix_cases():
+    out = []
+    for k, (solver, n, m, p, T, B, Cm, D) in enumerate(MIX):
+        case = wl.small(7000 + 13 * k, solver, n, m, p, T, h=1e-3)
+        out.append((case, B, Cm, D))
+    return out
+
+
+def test_batch_mixed_sizes_match_oracle(pb):
+    pb.set_option(pb.OPT_PATH, 0)
+    cases = _mix_cases()
+    batch = pb.Batch([_spec(pb, c, B, Cm, D) for c, B, Cm, D in cases], precision=pb.FP64)
+    batch.execute()
+    for i, (c, B, Cm, D) in enumerate(cases):
+        _, y = batch.output(i)
+        ref = _oracle_y(c, B, Cm, D)
+        assert y.shape == ref.shape, (i, y.shape, ref.shape)
+        err = oracle.rel_err(y, ref)
+        assert err <= TOL_FP64, (i, MIX[i], err)
+    # paths: scan dimension <= 64 blocked, larger level-synchronous
+    paths = [batch.path(i) for i in range(len(cases))]
+    for i, (c, *_rest) in enumerate(cases):
+        assert paths[i] == (2 if c.scan_dim <= 64 else 1), (i, paths[i])
+    batch.close()
+
+
+def test_batch_repeat_and_launch_count(pb):
+    pb.set_option(pb.OPT_PATH, 0)
+    cases = _mix_cases()
+    batch = pb.Batch([_spec(pb, c, B, Cm, D) for c, B, Cm, D in cases], precision=pb.FP64)
+    batch.execute()
+    first = [batch.output(i)[1].copy() for i in range(len(cases))]
+    batch.execute()
+    for i in range(len(cases)):
+        assert np.array_equal(first[i], batch.output(i)[1])
+    # a fixed number of launches, independent of the number of systems
+    assert batch.launch_count < 120, batch.launch_count
+    batch.close()
+
+
+def test_batch_equals_single_solves(pb):
+    pb.set_option(pb.OPT_PATH, 0)
+    cases = _mix_cases()[:6]
+    batch = pb.Batch([_spec(pb, c) for c, *_ in cases], precision=pb.FP64)
+    batch.execute()
+    for i, (c, *_r) in enumerate(cases):
+        u = pb.register_sinusoid(c.u.a, c.u.f, c.u.phi)
+        _, ys = pb.simulate(c.A, c.B, c.C, c.D, c.x0, u, c.t0, c.t_end, c.h, solver=c.solver)
+        _, yb = batch.output(i)
+        assert oracle.rel_err(yb, ys) <= TOL_FP64
+    batch.close()
+
+
+def test_batch_cfg4_subset(pb):
+    """The first 48 systems of the 4096-system batched workload, FP64."""
+    pb.set_option(pb.OPT_PATH, 0)
+    cases = wl.cfg4()[:48]
+    batch = pb.Batch([_spec(pb, c) for c in cases], precision=pb.FP64)
+    batch.execute()
+    worst = 0.0
+    for i, c in enumerate(cases):
+        _, y = batch.output(i)
+        worst = max(worst, oracle.rel_err(y, _oracle_y(c)))
+    assert worst <= TOL_FP64, worst
+    batch.close()
+
+
+def test_batch_rejects_bad_system(pb):
+    c = wl.small(1, 0, 4, 1, 1, 10)
+    bad = _spec(pb, c)
+    bad["solver"] = 7
+    with pytest.raises(pb.ParODEError):
+        pb.Batch([_spec(pb, c), bad])
