@@ -52,6 +52,16 @@ double sinusoid_host(const InputEntry* e, int i, double t)
     return v;
 }
 
+// Columns of a level that can reach an output.  Column g combines the
+// segments [g 2d, g 2d + d) and [g 2d + d, g 2d + 2d) of the time axis; when
+// g 2d >= nScan both segments are padding: the column holds zeros in the
+// up-sweep and writes only padding positions in the down-sweep, so it is
+// skipped.
+long sweep_columns(long nScan, long Tp, long d)
+{
+    return std::min(Tp / (2 * d), (nScan + 2 * d - 1) / (2 * d));
+}
+
 template <class F>
 void parallel_for(int n, F&& f)
 {
@@ -314,7 +324,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         for (Bucket& bk : buckets_)
             for (int i : bk.systems) items_ub += sys_[i].ntiles;
         long lev_entries = 0;
-        for (int i : ls_) lev_entries += 3L * std::max(sys_[i].levels, 1);
+        for (int i : ls_) lev_entries += 4L * std::max(sys_[i].levels, 1);
         job_bytes = nb * (sizeof(LeafArgs) + 3 * sizeof(double*) + 4 * kAlign) +
                     (size_t)items_ub * sizeof(BatchItem) + buckets_.size() * 8 * kAlign +
                     (size_t)N * (sizeof(SampleJob) + sizeof(ForcingJob) + sizeof(OutputJob) + 2 * sizeof(CopyJob)) +
@@ -502,35 +512,48 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         dSeed_ = reinterpret_cast<CopyJob*>(base + jput(cj.data(), sizeof(CopyJob) * cj.size()));
         // grouped level launches: for each level, entries grouped by tiling config
         auto add_level = [&](std::vector<GroupedLaunch>& out, const std::vector<std::pair<int, LevelArgs>>& ents) {
-            // group by (config id, CW)
-            std::vector<std::pair<std::pair<int, int>, std::vector<LevelArgs>>> groups;
+            // group by (config id, CW); entries keep the original form for the
+            // swap of a tiled down-sweep and the stored form for the contraction
+            struct Group {
+                std::pair<int, int> key;
+                LevelConfig cfg;
+                std::vector<LevelArgs> stored, swaps;
+            };
+            std::vector<Group> groups;
             for (const auto& e : ents) {
-                LevelConfig c = level_config(e.second.Np);
+                if (e.second.ncols <= 0) continue;
+                LevelConfig c = level_config(e.second);
                 std::pair<int, int> key(c.id, c.CW);
-                auto it = std::find_if(groups.begin(), groups.end(), [&](const auto& g) { return g.first == key; });
+                auto it = std::find_if(groups.begin(), groups.end(), [&](const Group& g) { return g.key == key; });
                 if (it == groups.end()) {
-                    groups.push_back({key, {}});
+                    groups.push_back(Group{key, c, {}, {}});
                     it = groups.end() - 1;
                 }
-                it->second.push_back(e.second);
+                it->stored.push_back(level_grouped_args(e.second));
+                if (c.id >= 5 && e.second.cpy) it->swaps.push_back(e.second);
             }
             for (auto& g : groups) {
                 GroupedLaunch gl;
+                gl.cfg = g.cfg;
                 std::vector<long> start;
                 long tiles = 0;
                 size_t smem = 0;
-                for (const LevelArgs& a : g.second) {
-                    LevelConfig c = level_config(a.Np);
-                    gl.cfg = c;
+                for (const LevelArgs& a : g.stored) {
+                    LevelConfig c = level_config(a);
                     start.push_back(tiles);
-                    tiles += (a.ncols + c.NC - 1) / c.NC;
+                    tiles += level_tiles(c, a);
                     smem = std::max(smem, c.smem);
                 }
-                gl.nent = (int)g.second.size();
+                gl.nent = (int)g.stored.size();
                 gl.tiles = tiles;
                 gl.smem = smem;
-                gl.args = reinterpret_cast<LevelArgs*>(base + jput(g.second.data(), sizeof(LevelArgs) * g.second.size()));
+                gl.args = reinterpret_cast<LevelArgs*>(base + jput(g.stored.data(), sizeof(LevelArgs) * g.stored.size()));
                 gl.start = reinterpret_cast<long*>(base + jput(start.data(), sizeof(long) * start.size()));
+                if (!g.swaps.empty()) {
+                    for (const LevelArgs& a : g.swaps) gl.swap_elems = std::max(gl.swap_elems, a.ncols * (long)a.Np);
+                    gl.nswap = (int)g.swaps.size();
+                    gl.swaps = reinterpret_cast<LevelArgs*>(base + jput(g.swaps.data(), sizeof(LevelArgs) * g.swaps.size()));
+                }
                 out.push_back(gl);
             }
         };
@@ -565,7 +588,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
                 a.P = q.P + (long)l * Np * Np;
                 a.ldp = Np;
                 a.Np = q.Np;
-                a.ncols = q.Tp / (2 * d);
+                a.ncols = sweep_columns(q.nScan, q.Tp, d);
                 a.src = q.V + (d - 1) * Np;
                 a.src_gs = 2 * d * Np;
                 a.acc = q.V + (2 * d - 1) * Np;
@@ -586,7 +609,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
                 a.P = q.P + (long)l * Np * Np;
                 a.ldp = Np;
                 a.Np = q.Np;
-                a.ncols = q.Tp / (2 * d);
+                a.ncols = sweep_columns(q.nScan, q.Tp, d);
                 a.src = q.V + (2 * d - 1) * Np;
                 a.src_gs = 2 * d * Np;
                 a.acc = q.V + (d - 1) * Np;
@@ -703,6 +726,10 @@ void BatchPlan::execute(cudaStream_t s)
         launch_copy_batch(dSeed_, nls, maxSeed_, fs);
         ++launches;
         for (const GroupedLaunch& g : ls_down_) {
+            if (g.nswap > 0) {
+                launch_swap_grouped(g.swaps, g.nswap, g.swap_elems, fs);
+                ++launches;
+            }
             launch_affine_level_grouped(g.cfg, g.args, g.start, g.nent, g.tiles, g.smem, fs);
             ++launches;
         }

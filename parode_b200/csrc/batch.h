@@ -90,6 +90,9 @@ private:
         int nent = 0;
         long tiles = 0;
         size_t smem = 0;
+        LevelArgs* swaps = nullptr;  // device: down-sweep entries of the tiled form, swapped first
+        int nswap = 0;
+        long swap_elems = 0;
     };
 
     int device_ = 0;

@@ -51,20 +51,29 @@ int launches_per_level();
 // device array of jobs; blockIdx.y selects the job.
 // ---------------------------------------------------------------------------
 
-// Tiling of the level contraction for a contraction length Np: entries of one
-// grouped launch must share the config id (and CW).
+// Tiling of the level contraction: entries of one grouped launch must share
+// the config id (and CW).  Ids 0..4: one CTA owns all Np rows of NC columns
+// (Np <= 64 here); ids 5/6: 64 x 64 tiles with cp.async staging (Np > 64;
+// 5: K-contiguous source columns, 6: N-contiguous, the power table).
 struct LevelConfig {
     int id = 0;     // template configuration
     int CW = 1;     // column warps
     int NC = 0;     // columns per CTA
     size_t smem = 0;
 };
-LevelConfig level_config(int Np);
+// `a` as for launch_affine_level (the down-sweep with cpy set).
+LevelConfig level_config(const LevelArgs& a);
+// The arguments a grouped launch stores for `a` (tiled: the swapped form of
+// the down-sweep, whose swap launch_swap_grouped performs beforehand).
+LevelArgs level_grouped_args(const LevelArgs& a);
+long level_tiles(const LevelConfig& c, const LevelArgs& stored);
 
 // One level over nent systems: dStart (device, nent entries) holds each
 // entry's first CTA; `tiles` CTAs in total; smem = max over entries.
 void launch_affine_level_grouped(const LevelConfig& c, const LevelArgs* dArgs, const long* dStart, int nent,
                                  long tiles, size_t smem, cudaStream_t s);
+// cpy(g, i) <-> dst(g, i) for every entry (original down-sweep arguments).
+void launch_swap_grouped(const LevelArgs* dArgs, int nent, long max_elems, cudaStream_t s);
 
 struct SampleJob {
     double* U = nullptr;

@@ -129,6 +129,188 @@ __device__ void affine_level_body(const LevelArgs& a, long tile, int CW, int KS,
     }
 }
 
+// ---------------------------------------------------------------------------
+// Tiled level contraction for contraction lengths above 64: CTA tile of
+// 64 rows x 64 columns, K slices of 32 staged by cp.async in a 3-stage ring,
+// 8 warps of 32 x 16 (eight independent m8n8k4 DMMA accumulators each).
+// The result must not alias the source (the down-sweep swaps first).
+// kTileKC: the source columns are K-contiguous (src_ks == 1, the sweeps);
+// otherwise N-contiguous (src_gs == 1, the power-table squaring).
+// ---------------------------------------------------------------------------
+
+constexpr int kTM = 64, kTN = 64, kTK = 32, kTStages = 3;
+constexpr int kLdA = kTK + 4;   // A tile [64 rows][36]: rows g and g+4 of a fragment in distinct bank halves
+constexpr int kLdBk = kTK + 4;  // B tile, K-contiguous: [64 cols][36]
+constexpr int kLdBn = kTN + 4;  // B tile, N-contiguous: [32 k][68]
+constexpr int kStageA = kTM * kLdA;
+constexpr int kStageB = (kTN * kLdBk > kTK * kLdBn) ? kTN * kLdBk : kTK * kLdBn;
+constexpr size_t kTiledSmem = (size_t)kTStages * (kStageA + kStageB) * sizeof(double);
+
+__device__ __forceinline__ void cp_async16(double* dst, const double* src, bool valid)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+    const int bytes = valid ? 16 : 0;  // 0: the 16 bytes are zero-filled and src is not read
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+template <bool kKC>
+__device__ void tiled_load(const LevelArgs& a, int m0, long n0, int k0, double* sA, double* sB)
+{
+    const int tid = threadIdx.x;
+    // A: 64 rows x 32 doubles = 1024 chunks of 16 bytes
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int c = tid + q * 256;
+        const int r = c >> 4, kc = (c & 15) * 2;
+        const bool ok = (m0 + r < a.Np) && (k0 + kc < a.Np);
+        const double* src = ok ? a.P + (long)(m0 + r) * a.ldp + k0 + kc : a.P;
+        cp_async16(sA + r * kLdA + kc, src, ok);
+    }
+    if (kKC) {
+        // B: 64 columns x 32 doubles of K, each column contiguous in K
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int c = tid + q * 256;
+            const int col = c >> 4, kc = (c & 15) * 2;
+            const long g = n0 + col;
+            const bool ok = (g < a.ncols) && (k0 + kc < a.Np);
+            const double* src = ok ? a.src + g * a.src_gs + k0 + kc : a.src;
+            cp_async16(sB + col * kLdBk + kc, src, ok);
+        }
+    } else {
+        // B: 32 rows of K x 64 columns, each row contiguous in N
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int c = tid + q * 256;
+            const int kr = c >> 5, nc = (c & 31) * 2;
+            const long g = n0 + nc;
+            const bool ok = (g < a.ncols) && (k0 + kr < a.Np);
+            const double* src = ok ? a.src + (long)(k0 + kr) * a.src_ks + g : a.src;
+            cp_async16(sB + kr * kLdBn + nc, src, ok);
+        }
+    }
+}
+
+template <bool kKC>
+__device__ void tiled_level_body(const LevelArgs& a, long tile, double* smem)
+{
+    const int mt = (a.Np + kTM - 1) / kTM;
+    const int m0 = (int)(tile % mt) * kTM;
+    const long n0 = (tile / mt) * kTN;
+    double* sA = smem;
+    double* sB = smem + kTStages * kStageA;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int wm = warp & 1, wn = warp >> 1;
+    const int gq = lane >> 2, tq = lane & 3;
+    const int nk = (a.Np + kTK - 1) / kTK;
+
+    double acc[4][2][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+#pragma unroll
+    for (int s = 0; s < kTStages - 1; ++s) {
+        if (s < nk) tiled_load<kKC>(a, m0, n0, s * kTK, sA + s * kStageA, sB + s * kStageB);
+        cp_async_commit();
+    }
+    for (int kt = 0; kt < nk; ++kt) {
+        cp_async_wait<kTStages - 2>();
+        __syncthreads();
+        {
+            const int nx = kt + kTStages - 1;
+            const int st = nx % kTStages;
+            if (nx < nk) tiled_load<kKC>(a, m0, n0, nx * kTK, sA + st * kStageA, sB + st * kStageB);
+            cp_async_commit();
+        }
+        const double* A = sA + (kt % kTStages) * kStageA;
+        const double* B = sB + (kt % kTStages) * kStageB;
+#pragma unroll
+        for (int kk = 0; kk < kTK; kk += 4) {
+            double af[4], bf[2];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) af[i] = A[(wm * 32 + i * 8 + gq) * kLdA + kk + tq];
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const int col = wn * 16 + j * 8 + gq;
+                bf[j] = kKC ? B[col * kLdBk + kk + tq] : B[(kk + tq) * kLdBn + col];
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) dmma_m8n8k4(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+        }
+    }
+    cp_async_wait<0>();
+
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const long r = m0 + wm * 32 + i * 8 + gq;
+        if (r >= a.Np) continue;
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const long g = n0 + wn * 16 + j * 8 + 2 * tq + e;
+                if (g >= a.ncols) continue;
+                double v = acc[i][j][e];
+                if (a.acc) v += a.acc[g * a.acc_gs + r * a.acc_is];
+                a.dst[g * a.dst_gs + r * a.dst_is] = v;
+            }
+    }
+}
+
+template <bool kKC>
+__global__ void __launch_bounds__(kThreads, 2) k_level_tiled(LevelArgs a)
+{
+    extern __shared__ double smem[];
+    tiled_level_body<kKC>(a, blockIdx.x, smem);
+}
+
+template <bool kKC>
+__global__ void __launch_bounds__(kThreads, 2) k_level_tiled_grouped(const LevelArgs* __restrict__ args,
+                                                                     const long* __restrict__ start, int nent)
+{
+    extern __shared__ double smem[];
+    const long t = blockIdx.x;
+    int lo = 0, hi = nent - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (start[mid] <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    const LevelArgs a = args[lo];
+    tiled_level_body<kKC>(a, t - start[lo], smem);
+}
+
+// Down-sweep bookkeeping before a tiled level: cpy(g, i) <-> dst(g, i).
+__device__ void swap_body(const LevelArgs& a)
+{
+    const long total = a.ncols * (long)a.Np;
+    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+        const long g = e / a.Np;
+        const long i = e - g * a.Np;
+        double* x = a.cpy + g * a.cpy_gs + i * a.cpy_is;
+        double* y = a.dst + g * a.dst_gs + i * a.dst_is;
+        const double t = *x;
+        *x = *y;
+        *y = t;
+    }
+}
+
+__global__ void k_swap(LevelArgs a) { swap_body(a); }
+
+// Grouped form: blockIdx.y selects the entry.
+__global__ void k_swap_grouped(const LevelArgs* __restrict__ args)
+{
+    const LevelArgs a = args[blockIdx.y];
+    swap_body(a);
+}
+
 __global__ void k_sinusoid_samples(double* U, int m, int K, const double* a, const double* f, const double* phi,
                                    double base, double dt, long count)
 {
@@ -271,6 +453,26 @@ __global__ void k_copy_batch(const CopyJob* __restrict__ jobs)
 
 inline unsigned blocks_for(long n, int t) { return (unsigned)((n + t - 1) / t); }
 
+// Arguments of the tiled contraction for a level: the down-sweep (cpy set)
+// becomes, after the swap, right = P left + right.
+LevelArgs tiled_args(const LevelArgs& a)
+{
+    LevelArgs b = a;
+    if (a.cpy) {
+        b.src = a.cpy;
+        b.src_gs = a.cpy_gs;
+        b.src_ks = a.cpy_is;
+        b.acc = a.dst;
+        b.acc_gs = a.dst_gs;
+        b.acc_is = a.dst_is;
+        b.cpy = nullptr;
+    }
+    if (b.src_ks != 1 && b.src_gs != 1) throw Error(kInvalidArgument, "tiled level: source neither K- nor N-contiguous");
+    return b;
+}
+
+long tiled_tiles(const LevelArgs& b) { return (long)((b.Np + kTM - 1) / kTM) * ((b.ncols + kTN - 1) / kTN); }
+
 template <int FR, int FC>
 void launch_level_t(const LevelArgs& a, int CW, cudaStream_t s)
 {
@@ -295,6 +497,28 @@ void launch_affine_level(const LevelArgs& a, cudaStream_t s)
     if (a.ncols <= 0) return;
     if (a.Np <= 0 || (a.Np & 7) != 0 || a.Np > 1024)
         throw Error(kInvalidArgument, "scan dimension must be a positive multiple of 8 up to 1024");
+    if (a.Np > 64) {
+        // tiled contraction; the down-sweep first swaps (left, right), then
+        // right = P left + right (the tile's result must not alias its source)
+        LevelArgs b = tiled_args(a);
+        if (a.cpy) {
+            k_swap<<<(unsigned)std::min<long>(blocks_for(a.ncols * (long)a.Np, 256), 4096), 256, 0, s>>>(a);
+            PARODE_CUDA(cudaGetLastError());
+        }
+        static bool attr_set = false;
+        if (!attr_set) {
+            PARODE_CUDA(cudaFuncSetAttribute(k_level_tiled<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)kTiledSmem));
+            PARODE_CUDA(cudaFuncSetAttribute(k_level_tiled<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)kTiledSmem));
+            attr_set = true;
+        }
+        const long tiles = tiled_tiles(b);
+        if (b.src_ks == 1) k_level_tiled<true><<<(unsigned)tiles, kThreads, kTiledSmem, s>>>(b);
+        else k_level_tiled<false><<<(unsigned)tiles, kThreads, kTiledSmem, s>>>(b);
+        PARODE_CUDA(cudaGetLastError());
+        return;
+    }
     const int rf = a.Np / 8;
     if (rf <= 8) {
         int RW = 1;
@@ -352,9 +576,17 @@ int launches_per_level() { return 1; }
 // grouped / batched launchers
 // ---------------------------------------------------------------------------
 
-LevelConfig level_config(int Np)
+LevelConfig level_config(const LevelArgs& a)
 {
     LevelConfig c;
+    const int Np = a.Np;
+    if (Np > 64) {
+        const LevelArgs b = tiled_args(a);
+        c.id = b.src_ks == 1 ? 5 : 6;
+        c.NC = kTN;
+        c.smem = kTiledSmem;
+        return c;
+    }
     const int rf = Np / 8;
     if (rf <= 8) {
         int RW = 1;
@@ -396,6 +628,20 @@ void launch_affine_level_grouped(const LevelConfig& c, const LevelArgs* dArgs, c
                                  long tiles, size_t smem, cudaStream_t s)
 {
     if (nent <= 0 || tiles <= 0) return;
+    if (c.id >= 5) {
+        static bool attr_set = false;
+        if (!attr_set) {
+            PARODE_CUDA(cudaFuncSetAttribute(k_level_tiled_grouped<true>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTiledSmem));
+            PARODE_CUDA(cudaFuncSetAttribute(k_level_tiled_grouped<false>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTiledSmem));
+            attr_set = true;
+        }
+        if (c.id == 5) k_level_tiled_grouped<true><<<(unsigned)tiles, kThreads, kTiledSmem, s>>>(dArgs, dStart, nent);
+        else k_level_tiled_grouped<false><<<(unsigned)tiles, kThreads, kTiledSmem, s>>>(dArgs, dStart, nent);
+        PARODE_CUDA(cudaGetLastError());
+        return;
+    }
     if (smem > 200 * 1024) throw Error(kInvalidArgument, "grouped level: shared memory above 200 KB");
     switch (c.id) {
     case 0: grouped_t<1, 4>(c, dArgs, dStart, nent, tiles, smem, s); break;
@@ -404,6 +650,22 @@ void launch_affine_level_grouped(const LevelConfig& c, const LevelArgs* dArgs, c
     case 3: grouped_t<8, 2>(c, dArgs, dStart, nent, tiles, smem, s); break;
     default: grouped_t<16, 1>(c, dArgs, dStart, nent, tiles, smem, s); break;
     }
+}
+
+LevelArgs level_grouped_args(const LevelArgs& a) { return a.Np > 64 ? tiled_args(a) : a; }
+
+long level_tiles(const LevelConfig& c, const LevelArgs& stored)
+{
+    if (c.id >= 5) return tiled_tiles(stored);
+    return (stored.ncols + c.NC - 1) / c.NC;
+}
+
+void launch_swap_grouped(const LevelArgs* dArgs, int nent, long max_elems, cudaStream_t s)
+{
+    if (nent <= 0 || max_elems <= 0) return;
+    dim3 grid((unsigned)std::min<long>(blocks_for(max_elems, 256), 64), (unsigned)nent);
+    k_swap_grouped<<<grid, 256, 0, s>>>(dArgs);
+    PARODE_CUDA(cudaGetLastError());
 }
 
 void launch_samples_batch(const SampleJob* dJobs, int njobs, long max_elems, cudaStream_t s)
