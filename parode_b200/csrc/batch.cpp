@@ -52,16 +52,6 @@ double sinusoid_host(const InputEntry* e, int i, double t)
     return v;
 }
 
-// Columns of a level that can reach an output.  Column g combines the
-// segments [g 2d, g 2d + d) and [g 2d + d, g 2d + 2d) of the time axis; when
-// g 2d >= nScan both segments are padding: the column holds zeros in the
-// up-sweep and writes only padding positions in the down-sweep, so it is
-// skipped.
-long sweep_columns(long nScan, long Tp, long d)
-{
-    return std::min(Tp / (2 * d), (nScan + 2 * d - 1) / (2 * d));
-}
-
 template <class F>
 void parallel_for(int n, F&& f)
 {
@@ -250,6 +240,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
     Stage st;
     struct Off {
         size_t phi0, bbar, c, d, cext, x0, sin, ypre;
+        size_t bbarT, cT, dT;  // level-synchronous systems: transposed copies (coalesced per-row kernels)
         size_t P, U, Y, V, G, CP;
     };
     std::vector<Off> off(N);
@@ -284,6 +275,22 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             o.sin = st.put(prm.data(), sizeof(double) * prm.size(), L);
         }
         if (q.solver == kABM) o.ypre = st.put(Ypre[i].data(), sizeof(double) * Ypre[i].size(), L);
+        if (!q.blocked) {
+            const int Wm = q.W * (s.zeroB ? 0 : s.m);
+            std::vector<double> bt((size_t)std::max(Wm, 1) * q.n, 0.0);
+            for (int r = 0; r < q.n; ++r)
+                for (int c = 0; c < Wm; ++c) bt[(size_t)c * q.n + r] = Bbar[i][(size_t)r * Wm + c];
+            o.bbarT = st.put(bt.data(), sizeof(double) * bt.size(), L);
+            std::vector<double> ct((size_t)q.n * q.p, 0.0), dt((size_t)std::max(s.m, 1) * q.p, 0.0);
+            if (!s.zeroC)
+                for (int r = 0; r < q.p; ++r)
+                    for (int c = 0; c < q.n; ++c) ct[(size_t)c * q.p + r] = s.C[(size_t)r * q.n + c];
+            if (!s.zeroD)
+                for (int r = 0; r < q.p; ++r)
+                    for (int c = 0; c < s.m; ++c) dt[(size_t)c * q.p + r] = s.D[(size_t)r * s.m + c];
+            o.cT = st.put(ct.data(), sizeof(double) * ct.size(), L);
+            o.dT = st.put(dt.data(), sizeof(double) * dt.size(), L);
+        }
     }
     const size_t const_bytes_sys = L.bytes;
     (void)const_bytes_sys;
@@ -298,7 +305,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             o.CP = L.take(sizeof(double) * (size_t)bk.sh.B * q.p * q.Np);
         } else {
             o.P = L.take(sizeof(double) * (size_t)std::max(q.levels, 1) * q.Np * q.Np);
-            o.V = L.take(sizeof(double) * (size_t)q.Tp * q.Np);
+            o.V = L.take(sizeof(double) * (size_t)(q.Tp + 1) * q.Np);  // slot -1 holds the initial state
         }
         o.U = q.mu > 0 ? L.take(sizeof(double) * (size_t)q.nU * q.mu) : 0;
         o.Y = L.take(sizeof(double) * (size_t)q.nOut * q.p);
@@ -469,12 +476,12 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         for (int i : ls_) {
             const Sys& q = sys_[i];
             ForcingJob f;
-            f.V = q.V;
+            f.V = q.V + q.Np;
             f.Np = q.Np;
             f.n = q.n;
             f.m = q.zeroB ? 0 : q.m;
             f.solver = q.solver;
-            f.Bbar = q.Bbar;
+            f.BbarT = dp(off[i].bbarT);
             f.U = q.U;
             f.T = q.nScan;
             f.Tp = q.Tp;
@@ -488,8 +495,8 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             o.n = q.n;
             o.m = q.mu;
             o.p = q.p;
-            o.C = q.C;
-            o.D = q.D;
+            o.CT = dp(off[i].cT);
+            o.DT = dp(off[i].dT);
             o.zeroC = q.zeroC;
             o.zeroD = q.zeroD;
             o.U = q.U;
@@ -500,7 +507,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             oj.push_back(o);
             maxOutput_ = std::max(maxOutput_, q.nScan * (long)q.p);
             CopyJob c;
-            c.dst = q.V + (q.Tp - 1) * (long)q.Np;
+            c.dst = q.V;
             c.src = q.X0;
             c.N = q.Np;
             cj.push_back(c);
@@ -589,11 +596,11 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
                 a.ldp = Np;
                 a.Np = q.Np;
                 a.ncols = sweep_columns(q.nScan, q.Tp, d);
-                a.src = q.V + (d - 1) * Np;
+                a.src = q.V + d * Np;
                 a.src_gs = 2 * d * Np;
-                a.acc = q.V + (2 * d - 1) * Np;
+                a.acc = q.V + 2 * d * Np;
                 a.acc_gs = 2 * d * Np;
-                a.dst = q.V + (2 * d - 1) * Np;
+                a.dst = q.V + 2 * d * Np;
                 a.dst_gs = 2 * d * Np;
                 ents.push_back({i, a});
             }
@@ -610,14 +617,14 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
                 a.ldp = Np;
                 a.Np = q.Np;
                 a.ncols = sweep_columns(q.nScan, q.Tp, d);
-                a.src = q.V + (2 * d - 1) * Np;
+                // in place: node prefix in slot g 2d - 1, right half's prefix
+                // replaces the left half's aggregate in slot g 2d + d - 1
+                a.src = q.V;
                 a.src_gs = 2 * d * Np;
-                a.acc = q.V + (d - 1) * Np;
+                a.acc = q.V + d * Np;
                 a.acc_gs = 2 * d * Np;
-                a.dst = q.V + (2 * d - 1) * Np;
+                a.dst = q.V + d * Np;
                 a.dst_gs = 2 * d * Np;
-                a.cpy = q.V + (d - 1) * Np;
-                a.cpy_gs = 2 * d * Np;
                 ents.push_back({i, a});
             }
             add_level(ls_down_, ents);

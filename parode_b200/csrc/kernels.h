@@ -26,6 +26,16 @@ struct LevelArgs {
 // One Blelloch level over all columns (up-sweep, down-sweep or P*P).
 void launch_affine_level(const LevelArgs& a, cudaStream_t s);
 
+// Columns of a level that can reach an output.  Column g combines the
+// segments [g 2d, g 2d + d) and [g 2d + d, g 2d + 2d) of the time axis; when
+// g 2d >= nScan both segments are padding: the column holds zeros in the
+// up-sweep and writes only padding slots in the down-sweep, so it is skipped.
+inline long sweep_columns(long nScan, long Tp, long d)
+{
+    const long all = Tp / (2 * d), used = (nScan + 2 * d - 1) / (2 * d);
+    return used < all ? used : all;
+}
+
 // U[j*m + i] = sum_k a sin(2 pi f t_j + phi), t_j = base + dt*j, j < count.
 void launch_sinusoid_samples(double* U, int m, int K, const double* a, const double* f, const double* phi,
                              double base, double dt, long count, cudaStream_t s);
@@ -85,7 +95,7 @@ struct SampleJob {
 struct ForcingJob {
     double* V = nullptr;
     int Np = 0, n = 0, m = 0, solver = 0;
-    const double* Bbar = nullptr;
+    const double* BbarT = nullptr;  // Bbar transposed: W m rows of n
     const double* U = nullptr;
     long T = 0, Tp = 0;
 };
@@ -93,7 +103,7 @@ struct OutputJob {
     double* Y = nullptr;
     const double* V = nullptr;
     int Np = 0, xoff = 0, n = 0, m = 0, p = 0;
-    const double *C = nullptr, *D = nullptr;
+    const double *CT = nullptr, *DT = nullptr;  // C and D transposed: n (m) rows of p
     int zeroC = 1, zeroD = 1;
     const double* U = nullptr;
     int ustride = 1, uoff = 0;

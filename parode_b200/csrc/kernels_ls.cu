@@ -394,53 +394,54 @@ __global__ void k_samples_batch(const SampleJob* __restrict__ jobs)
     }
 }
 
+// Rows (steps) are dealt to the CTAs of the job; a row's components to the
+// threads (no per-element division).  Forcing rows: RK4 0..n-1, ABM 3n..4n-1.
 __global__ void k_forcing_batch(const ForcingJob* __restrict__ jobs)
 {
-    const ForcingJob J = jobs[blockIdx.y];
-    const long total = J.Tp * (long)J.Np;
-    const int n = J.n, m = J.m;
-    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
-        const long k = e / J.Np;
-        const int i = (int)(e - k * J.Np);
-        double v = 0.0;
-        if (k < J.T && m > 0) {
-            if (J.solver == 0) {
-                if (i < n) {
-                    const double* b = J.Bbar + (long)i * 3 * m;
-                    const double* u = J.U + 2 * k * m;
-                    for (int q = 0; q < 3 * m; ++q) v = fma(b[q], u[q], v);
-                }
-            } else if (i >= 3 * n && i < 4 * n) {
-                const double* b = J.Bbar + (long)(i - 3 * n) * 5 * m;
-                const double* u = J.U + k * m;
-                for (int q = 0; q < 5 * m; ++q) v = fma(b[q], u[q], v);
+    const ForcingJob& J = jobs[blockIdx.y];
+    const int n = J.n, m = J.m, Np = J.Np;
+    const bool rk4 = J.solver == 0;
+    const int lo = rk4 ? 0 : 3 * n, W = rk4 ? 3 : 5;
+    const long ustep = rk4 ? 2L * m : (long)m;
+    for (long k = blockIdx.x; k < J.Tp; k += gridDim.x) {
+        double* row = J.V + k * Np;
+        const double* u = J.U + k * ustep;
+        for (int i = threadIdx.x; i < Np; i += blockDim.x) {
+            double v = 0.0;
+            if (k < J.T && m > 0 && i >= lo && i < lo + n) {
+                const double* b = J.BbarT + (i - lo);  // consecutive threads, consecutive addresses
+                for (int q = 0; q < W * m; ++q) v = fma(b[(long)q * n], u[q], v);
             }
+            row[i] = v;
         }
-        J.V[e] = v;
     }
 }
 
+// Output rows: a CTA covers blockDim/p rows at a time, thread (r, o) one output.
 __global__ void k_output_batch(const OutputJob* __restrict__ jobs)
 {
-    const OutputJob J = jobs[blockIdx.y];
+    const OutputJob& J = jobs[blockIdx.y];
     const int p = J.p, n = J.n, m = J.m;
-    const long total = J.count * (long)p;
-    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
-        const long k = e / p;
-        const int o = (int)(e - k * p);
+    const int rows = p <= (int)blockDim.x ? (int)blockDim.x / p : 1;
+    const int r = p <= (int)blockDim.x ? (int)threadIdx.x / p : 0;
+    if (r >= rows) return;
+    const int o0 = p <= (int)blockDim.x ? (int)threadIdx.x - r * p : (int)threadIdx.x;
+    const int ostep = p <= (int)blockDim.x ? p : (int)blockDim.x;
+    for (long k = (long)blockIdx.x * rows + r; k < J.count; k += (long)gridDim.x * rows) {
         const double* x = J.V + k * J.Np + J.xoff;
-        double v = 0.0;
-        if (J.zeroC && J.zeroD) {
-            v = x[o];
-        } else {
-            if (!J.zeroC)
-                for (int c = 0; c < n; ++c) v = fma(J.C[(long)o * n + c], x[c], v);
-            if (!J.zeroD && m > 0) {
-                const double* u = J.U + (k * J.ustride + J.uoff) * m;
-                for (int c = 0; c < m; ++c) v = fma(J.D[(long)o * m + c], u[c], v);
+        const double* u = (!J.zeroD && m > 0) ? J.U + (k * J.ustride + J.uoff) * m : nullptr;
+        for (int o = o0; o < p; o += ostep) {
+            double v = 0.0;
+            if (J.zeroC && J.zeroD) {
+                v = x[o];
+            } else {
+                if (!J.zeroC)
+                    for (int c = 0; c < n; ++c) v = fma(J.CT[(long)c * p + o], x[c], v);
+                if (u)
+                    for (int c = 0; c < m; ++c) v = fma(J.DT[(long)c * p + o], u[c], v);
             }
+            J.Y[(J.ybase + k) * p + o] = v;
         }
-        J.Y[(J.ybase + k) * p + o] = v;
     }
 }
 
@@ -679,15 +680,16 @@ void launch_samples_batch(const SampleJob* dJobs, int njobs, long max_elems, cud
 void launch_forcing_batch(const ForcingJob* dJobs, int njobs, long max_elems, cudaStream_t s)
 {
     if (njobs <= 0 || max_elems <= 0) return;
-    dim3 grid((unsigned)std::min<long>(blocks_for(max_elems, 256), 64), (unsigned)njobs);
-    k_forcing_batch<<<grid, 256, 0, s>>>(dJobs);
+    // max_elems: the largest Tp x Np; a CTA of 128 threads walks rows
+    dim3 grid((unsigned)std::min<long>(blocks_for(max_elems, 1024), 256), (unsigned)njobs);
+    k_forcing_batch<<<grid, 128, 0, s>>>(dJobs);
     PARODE_CUDA(cudaGetLastError());
 }
 
 void launch_output_batch(const OutputJob* dJobs, int njobs, long max_elems, cudaStream_t s)
 {
     if (njobs <= 0 || max_elems <= 0) return;
-    dim3 grid((unsigned)std::min<long>(blocks_for(max_elems, 256), 64), (unsigned)njobs);
+    dim3 grid((unsigned)std::min<long>(blocks_for(max_elems, 2048), 128), (unsigned)njobs);
     k_output_batch<<<grid, 256, 0, s>>>(dJobs);
     PARODE_CUDA(cudaGetLastError());
 }

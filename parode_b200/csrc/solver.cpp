@@ -127,7 +127,7 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
         PARODE_CUDA(cudaMemsetAsync(dStatus_, 0, sizeof(int), stream_));
     }
     if (path_ == kPathLevel) {
-        alloc(&dV_, Tp_ * (long)Np_);
+        alloc(&dV_, (Tp_ + 1) * (long)Np_);  // a leading slot holds the initial state
     } else {
         alloc(&dG_, nblocks_ * (long)Np_);
         alloc(&dWork_, blocked_items_scratch(shape_, nblocks_) * (long)Np_);
@@ -289,7 +289,9 @@ void Plan::execute(double* y, cudaStream_t s)
     fill_inputs(s);
     launches += mu_ > 0 ? 1 : 0;
     mark("inputs", s);
-    launch_forcing(dV_, Np_, n, sys_.zeroB ? 0 : sys_.m, solver_, dBbar_, dU_, nScan_, Tp_, s);
+    // V slots: dV_ = slot -1 (the initial state), V1 = slots 0 .. Tp-1
+    double* V1 = dV_ + Np;
+    launch_forcing(V1, Np_, n, sys_.zeroB ? 0 : sys_.m, solver_, dBbar_, dU_, nScan_, Tp_, s);
     ++launches;
     mark("forcing", s);
 
@@ -318,44 +320,47 @@ void Plan::execute(double* y, cudaStream_t s)
         a.P = dPow_ + (long)l * Np * Np;
         a.ldp = Np;
         a.Np = Np_;
-        a.ncols = Tp_ / (2 * d);
-        a.src = dV_ + (d - 1) * Np;
+        a.ncols = sweep_columns(nScan_, Tp_, d);
+        a.src = V1 + (d - 1) * Np;
         a.src_gs = 2 * d * Np;
-        a.acc = dV_ + (2 * d - 1) * Np;
+        a.acc = V1 + (2 * d - 1) * Np;
         a.acc_gs = 2 * d * Np;
-        a.dst = dV_ + (2 * d - 1) * Np;
+        a.dst = V1 + (2 * d - 1) * Np;
         a.dst_gs = 2 * d * Np;
         launch_affine_level(a, s);
         ++launches;
     }
-    // exclusive scan seeded with the initial state at the root (the
-    // reference's carry (I, x0), Sources/GPUFixedStepIterative.cpp:191-198,327-330)
-    launch_copy(dV_ + (Tp_ - 1) * Np, dX0_, Np, s);
+    // the scan is seeded with the initial state (the reference's carry
+    // (I, x0), Sources/GPUFixedStepIterative.cpp:191-198,327-330), held in slot -1
+    launch_copy(dV_, dX0_, Np, s);
     ++launches;
-    // down-sweep: v[k] <- P_l v[k] + v[k-d], v[k-d] <- v[k]
-    // (reference Kernels/MVVKernelScanDownsweep.cl:25-48 and RootCopyKernelScanDownsweep.cl:11-19)
+    // down-sweep, in place: the node over [g 2d, g 2d + 2d) has its prefix
+    // (the state at its start) in slot g 2d - 1 and its left half's aggregate in
+    // slot g 2d + d - 1; the right half's prefix P_l prefix + aggregate replaces
+    // the aggregate, the left half keeps the node's slot.  This is the
+    // reference's down-sweep (Kernels/MVVKernelScanDownsweep.cl:25-48 with
+    // RootCopyKernelScanDownsweep.cl:11-19) without its copy: the state x_k
+    // ends in slot k - 1, x_0 in slot -1.
     for (int l = levels_ - 1; l >= 0; --l) {
         long d = 1L << l;
         LevelArgs a;
         a.P = dPow_ + (long)l * Np * Np;
         a.ldp = Np;
         a.Np = Np_;
-        a.ncols = Tp_ / (2 * d);
-        a.src = dV_ + (2 * d - 1) * Np;
+        a.ncols = sweep_columns(nScan_, Tp_, d);
+        a.src = dV_;
         a.src_gs = 2 * d * Np;
-        a.acc = dV_ + (d - 1) * Np;
+        a.acc = V1 + (d - 1) * Np;
         a.acc_gs = 2 * d * Np;
-        a.dst = dV_ + (2 * d - 1) * Np;
+        a.dst = V1 + (d - 1) * Np;
         a.dst_gs = 2 * d * Np;
-        a.cpy = dV_ + (d - 1) * Np;
-        a.cpy_gs = 2 * d * Np;
         launch_affine_level(a, s);
         ++launches;
     }
     mark("sweeps", s);
     // outputs (reference Kernels/SystemOutput.cl with strides (1,0)/(2,0) for
     // RK4 and (4,3)/(1,3) for ABM, Sources/RungeKutta4thOrder.cpp:209,
-    // Sources/AdamsMoulton.cpp:398)
+    // Sources/AdamsMoulton.cpp:398); x_k is read from slot k - 1
     if (solver_ == kRK4) {
         launch_output(Y, dV_, Np_, 0, n, mu_, p_, dC_, dD_, sys_.zeroC, sys_.zeroD, dU_, 2, 0, nScan_, 0, s);
     } else {
