@@ -15,6 +15,7 @@ namespace {
 
 constexpr size_t kAlign = 256;
 constexpr size_t kSmemOptIn = 232448 - 1024;
+constexpr int kTcConfig = 100;  // grouped launch of the tensor-core (3xTF32) level contraction
 
 size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
 
@@ -152,7 +153,9 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             q.levels = ilog2(q.Tp);
             ls_.push_back(i);
         }
-        q.precision = kFP64;
+        // mixed form: level-synchronous systems run their lower levels on the
+        // tensor cores; the blocked buckets stay FP64 here
+        q.precision = (opt.precision == kMixed && !q.blocked) ? kMixed : kFP64;
     }
     // bucket shapes: the widest input of the bucket sizes the sample staging
     for (Bucket& bk : buckets_) {
@@ -518,7 +521,8 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         dOutput_ = reinterpret_cast<OutputJob*>(base + jput(oj.data(), sizeof(OutputJob) * oj.size()));
         dSeed_ = reinterpret_cast<CopyJob*>(base + jput(cj.data(), sizeof(CopyJob) * cj.size()));
         // grouped level launches: for each level, entries grouped by tiling config
-        auto add_level = [&](std::vector<GroupedLaunch>& out, const std::vector<std::pair<int, LevelArgs>>& ents) {
+        auto add_level = [&](std::vector<GroupedLaunch>& out, const std::vector<std::pair<int, LevelArgs>>& ents,
+                             int l) {
             // group by (config id, CW); entries keep the original form for the
             // swap of a tiled down-sweep and the stored form for the contraction
             struct Group {
@@ -527,8 +531,22 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
                 std::vector<LevelArgs> stored, swaps;
             };
             std::vector<Group> groups;
+            // mixed form: levels below the top four of a system run on the
+            // tensor cores (3xTF32); the top four, where high powers of Phi
+            // amplify rounding, stay FP64
+            std::vector<LevelArgs> tc;
             for (const auto& e : ents) {
                 if (e.second.ncols <= 0) continue;
+                const Sys& q = sys_[e.first];
+                if (l >= 0 && q.precision == kMixed && l < q.levels - 4 && level_tc_supported(e.second)) {
+                    // exact part of P_l = Phi^(2^l): I for RK4; for ABM the
+                    // companion shift S^(2^l) (block b reads block min(b + 2^l, 3))
+                    LevelArgs t = e.second;
+                    t.rn = q.solver == kRK4 ? 0 : q.n;
+                    t.rsh = std::min(1 << std::min(l, 2), 3);
+                    tc.push_back(t);
+                    continue;
+                }
                 LevelConfig c = level_config(e.second);
                 std::pair<int, int> key(c.id, c.CW);
                 auto it = std::find_if(groups.begin(), groups.end(), [&](const Group& g) { return g.key == key; });
@@ -563,6 +581,21 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
                 }
                 out.push_back(gl);
             }
+            if (!tc.empty()) {
+                GroupedLaunch gl;
+                gl.cfg.id = kTcConfig;
+                std::vector<long> start;
+                long tiles = 0;
+                for (const LevelArgs& a : tc) {
+                    start.push_back(tiles);
+                    tiles += level_tc_tiles(a);
+                }
+                gl.nent = (int)tc.size();
+                gl.tiles = tiles;
+                gl.args = reinterpret_cast<LevelArgs*>(base + jput(tc.data(), sizeof(LevelArgs) * tc.size()));
+                gl.start = reinterpret_cast<long*>(base + jput(start.data(), sizeof(long) * start.size()));
+                out.push_back(gl);
+            }
         };
         for (int l = 1; l < Lmax; ++l) {
             std::vector<std::pair<int, LevelArgs>> ents;
@@ -583,7 +616,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
                 a.dst_is = Np;
                 ents.push_back({i, a});
             }
-            add_level(ls_power_, ents);
+            add_level(ls_power_, ents, -1);  // the power table stays FP64
         }
         for (int l = 0; l < Lmax; ++l) {
             std::vector<std::pair<int, LevelArgs>> ents;
@@ -604,7 +637,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
                 a.dst_gs = 2 * d * Np;
                 ents.push_back({i, a});
             }
-            add_level(ls_up_, ents);
+            add_level(ls_up_, ents, l);
         }
         for (int l = Lmax - 1; l >= 0; --l) {
             std::vector<std::pair<int, LevelArgs>> ents;
@@ -627,7 +660,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
                 a.dst_gs = 2 * d * Np;
                 ents.push_back({i, a});
             }
-            add_level(ls_down_, ents);
+            add_level(ls_down_, ents, l);
         }
     }
     // set-up copies: Phi -> P level 0, ABM outputs 0..2 -> Y rows 0..2
@@ -645,6 +678,10 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             y.N = 3L * q.p;
             setup_copies.push_back(y);
         }
+    }
+    {
+        const int zero[4] = {0, 0, 0, 0};
+        dStatus_ = reinterpret_cast<int*>(base + jput(zero, sizeof(zero)));
     }
     long max_copy = 0;
     for (const CopyJob& c : setup_copies) max_copy = std::max(max_copy, c.N);
@@ -723,11 +760,11 @@ void BatchPlan::execute(cudaStream_t s)
         launch_forcing_batch(dForcing_, nls, maxForcing_, fs);
         ++launches;
         for (const GroupedLaunch& g : ls_power_) {
-            launch_affine_level_grouped(g.cfg, g.args, g.start, g.nent, g.tiles, g.smem, fs);
+            launch_grouped(g, fs);
             ++launches;
         }
         for (const GroupedLaunch& g : ls_up_) {
-            launch_affine_level_grouped(g.cfg, g.args, g.start, g.nent, g.tiles, g.smem, fs);
+            launch_grouped(g, fs);
             ++launches;
         }
         launch_copy_batch(dSeed_, nls, maxSeed_, fs);
@@ -737,7 +774,7 @@ void BatchPlan::execute(cudaStream_t s)
                 launch_swap_grouped(g.swaps, g.nswap, g.swap_elems, fs);
                 ++launches;
             }
-            launch_affine_level_grouped(g.cfg, g.args, g.start, g.nent, g.tiles, g.smem, fs);
+            launch_grouped(g, fs);
             ++launches;
         }
         launch_output_batch(dOutput_, nls, maxOutput_, fs);
@@ -751,6 +788,12 @@ void BatchPlan::execute(cudaStream_t s)
     launches_ = launches;
 }
 
+void BatchPlan::launch_grouped(const GroupedLaunch& g, cudaStream_t s)
+{
+    if (g.cfg.id == kTcConfig) launch_level_tc(g.args, g.start, g.nent, g.tiles, sms_, dStatus_, s);
+    else launch_affine_level_grouped(g.cfg, g.args, g.start, g.nent, g.tiles, g.smem, s);
+}
+
 void BatchPlan::get_output(int i, double* t, double* y)
 {
     if (i < 0 || i >= size()) throw Error(kInvalidArgument, "system index out of range");
@@ -758,6 +801,9 @@ void BatchPlan::get_output(int i, double* t, double* y)
     PARODE_CUDA(cudaSetDevice(device_));
     PARODE_CUDA(cudaStreamSynchronize(stream_));
     PARODE_CUDA(cudaDeviceSynchronize());
+    int st = 0;
+    PARODE_CUDA(cudaMemcpy(&st, dStatus_, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st != 0) throw Error(kDeviceError, "a tensor-core wait gave up (the result is incomplete)");
     if (y) PARODE_CUDA(cudaMemcpy(y, q.Y, sizeof(double) * (size_t)q.nOut * q.p, cudaMemcpyDeviceToHost));
     if (t) time_vector(q.solver, q.t0, q.tEnd, q.h, t);
 }

@@ -95,8 +95,11 @@ private:
         long swap_elems = 0;
     };
 
+    void launch_grouped(const GroupedLaunch& g, cudaStream_t s);
+
     int device_ = 0;
     int sms_ = 148;
+    int* dStatus_ = nullptr;  // set by a device wait that gave up
     cudaStream_t stream_ = nullptr;
     std::vector<cudaStream_t> forks_;
     std::vector<cudaEvent_t> events_;

@@ -21,6 +21,11 @@ struct LevelArgs {
     long dst_gs = 0, dst_is = 1;
     double* cpy = nullptr;  // down-sweep: cpy(g,i) <- old src(g,i)
     long cpy_gs = 0, cpy_is = 1;
+    // Mixed form only: an exact 0/1 part R of P with one 1 per row, taken out
+    // of the tensor-core product and added back in FP64 (P v = R v + (P - R) v).
+    // rn < 0: none; rn == 0: R = I; rn > 0: ABM companion blocks of rn rows,
+    // row block b reads block min(b + rsh, 3).
+    int rn = -1, rsh = 0;
 };
 
 // One Blelloch level over all columns (up-sweep, down-sweep or P*P).
@@ -84,6 +89,15 @@ void launch_affine_level_grouped(const LevelConfig& c, const LevelArgs* dArgs, c
                                  long tiles, size_t smem, cudaStream_t s);
 // cpy(g, i) <-> dst(g, i) for every entry (original down-sweep arguments).
 void launch_swap_grouped(const LevelArgs* dArgs, int nent, long max_elems, cudaStream_t s);
+
+// Mixed-precision level contraction (3xTF32 tcgen05, FP64 in and out) for
+// scan dimensions 72..1024 with K-contiguous sources and no in-place copy.
+// Grouped like launch_affine_level_grouped: dStart[e] = first tile of entry e,
+// level_tc_tiles(a) tiles per entry.  A device wait that gives up sets *status.
+bool level_tc_supported(const LevelArgs& a);
+long level_tc_tiles(const LevelArgs& a);
+void launch_level_tc(const LevelArgs* dArgs, const long* dStart, int nent, long tiles, int sms, int* status,
+                     cudaStream_t s);
 
 struct SampleJob {
     double* U = nullptr;

@@ -113,6 +113,27 @@ def test_batch_cfg4_subset(pb):
     batch.close()
 
 
+TOL_MIXED = 1e-6
+
+MIXED_LS = [  # level-synchronous systems (scan dimension > 64): tensor-core levels below the top four
+    (0, 72, 6, 4, 5000), (0, 96, 8, 8, 20000), (1, 20, 3, 3, 3000), (1, 33, 4, 4, 9000), (1, 96, 12, 12, 4000),
+    (0, 130, 8, 6, 1500), (1, 64, 8, 8, 2500),
+]
+
+
+def test_batch_mixed_level_synchronous(pb):
+    pb.set_option(pb.OPT_PATH, 0)
+    cases = [wl.small(9100 + 7 * k, s, n, m, p, T, h=1e-3) for k, (s, n, m, p, T) in enumerate(MIXED_LS)]
+    batch = pb.Batch([_spec(pb, c) for c in cases], precision=pb.MIXED)
+    batch.execute()
+    for i, c in enumerate(cases):
+        assert batch.path(i) == 1 and batch.precision(i) == pb.MIXED, i
+        _, y = batch.output(i)
+        err = oracle.rel_err(y, _oracle_y(c))
+        assert err <= TOL_MIXED, (i, MIXED_LS[i], err)
+    batch.close()
+
+
 def test_batch_rejects_bad_system(pb):
     c = wl.small(1, 0, 4, 1, 1, 10)
     bad = _spec(pb, c)
