@@ -190,6 +190,17 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         Phi[i].assign((size_t)q.Np * q.Np, 0.0);
         for (int r = 0; r < q.Ns; ++r) std::memcpy(&Phi[i][(size_t)r * q.Np], &P[(size_t)r * q.Ns], sizeof(double) * q.Ns);
         X0[i].assign((size_t)q.Np, 0.0);
+        // distance of Phi from its exact 0/1 part (I for RK4; for ABM the
+        // companion shift: block row b < 3 reads block b + 1, the last row
+        // block reads itself)
+        double dmax = 0.0;
+        for (int r = 0; r < q.Ns; ++r) {
+            const int rc = q.solver == kRK4 ? r : (std::min(r / q.n + 1, 3) * q.n + r % q.n);
+            double sum = 0.0;
+            for (int c = 0; c < q.Ns; ++c) sum += std::fabs(P[(size_t)r * q.Ns + c] - (c == rc ? 1.0 : 0.0));
+            dmax = std::max(dmax, sum);
+        }
+        q.delta = dmax;
         if (q.solver == kRK4) {
             for (int r = 0; r < q.n; ++r) X0[i][r] = s.x0[r];
         }
@@ -244,7 +255,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
     struct Off {
         size_t phi0, bbar, c, d, cext, x0, sin, ypre;
         size_t bbarT, cT, dT;  // level-synchronous systems: transposed copies (coalesced per-row kernels)
-        size_t P, U, Y, V, G, CP;
+        size_t P, U, Y, V, G, CP, Ps;
     };
     std::vector<Off> off(N);
     for (int i = 0; i < N; ++i) {
@@ -309,6 +320,15 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         } else {
             o.P = L.take(sizeof(double) * (size_t)std::max(q.levels, 1) * q.Np * q.Np);
             o.V = L.take(sizeof(double) * (size_t)(q.Tp + 1) * q.Np);  // slot -1 holds the initial state
+            // mixed: tensor cores for the levels below the top four whose
+            // P_l - R_l stays small (|P_l - R_l| <~ 2^l |Phi - R|: at most 1/4);
+            // the rest, and the power table, stay FP64
+            if (q.precision == kMixed) {
+                int lv = 0;
+                while (lv < q.levels - 4 && std::ldexp(q.delta, lv) <= 0.25) ++lv;
+                q.tc_levels = lv;
+            }
+            o.Ps = q.tc_levels > 0 ? L.take(level_split_bytes(q.Np) * (size_t)q.tc_levels) : 0;
         }
         o.U = q.mu > 0 ? L.take(sizeof(double) * (size_t)q.nU * q.mu) : 0;
         o.Y = L.take(sizeof(double) * (size_t)q.nOut * q.p);
@@ -338,8 +358,9 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         job_bytes = nb * (sizeof(LeafArgs) + 3 * sizeof(double*) + 4 * kAlign) +
                     (size_t)items_ub * sizeof(BatchItem) + buckets_.size() * 8 * kAlign +
                     (size_t)N * (sizeof(SampleJob) + sizeof(ForcingJob) + sizeof(OutputJob) + 2 * sizeof(CopyJob)) +
-                    8 * kAlign + (size_t)lev_entries * (sizeof(LevelArgs) + sizeof(long)) +
-                    (size_t)(3 * 64 * 8) * 2 * kAlign;
+                    8 * kAlign + (size_t)lev_entries * (2 * sizeof(LevelArgs) + sizeof(long)) +
+                    (size_t)(3 * 64 * 8) * 2 * kAlign + (size_t)2 * 64 * (2 * sms_ + 1) * sizeof(long) +
+                    ((size_t)1 << 20);
     }
     arena_bytes_ = align_up(work_end + job_bytes);
     {
@@ -368,6 +389,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             q.Cext = dp(o.cext);
         } else {
             q.V = dp(o.V);
+            if (q.tc_levels > 0) q.Ps = reinterpret_cast<float*>(base + o.Ps);
         }
         if (q.mu > 0 && q.input->kind == InputEntry::kSinusoid) q.sin = dp(o.sin);
     }
@@ -538,12 +560,13 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             for (const auto& e : ents) {
                 if (e.second.ncols <= 0) continue;
                 const Sys& q = sys_[e.first];
-                if (l >= 0 && q.precision == kMixed && l < q.levels - 4 && level_tc_supported(e.second)) {
+                if (l >= 0 && l < q.tc_levels && level_tc_supported(e.second)) {
                     // exact part of P_l = Phi^(2^l): I for RK4; for ABM the
                     // companion shift S^(2^l) (block b reads block min(b + 2^l, 3))
                     LevelArgs t = e.second;
                     t.rn = q.solver == kRK4 ? 0 : q.n;
                     t.rsh = std::min(1 << std::min(l, 2), 3);
+                    t.Ps = q.Ps + (size_t)l * (level_split_bytes(q.Np) / sizeof(float));
                     tc.push_back(t);
                     continue;
                 }
@@ -594,6 +617,10 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
                 gl.tiles = tiles;
                 gl.args = reinterpret_cast<LevelArgs*>(base + jput(tc.data(), sizeof(LevelArgs) * tc.size()));
                 gl.start = reinterpret_cast<long*>(base + jput(start.data(), sizeof(long) * start.size()));
+                // two persistent CTAs per SM, tile ranges balanced by work
+                gl.ctas = (int)std::min<long>(2L * sms_, tiles);
+                std::vector<long> r = level_tc_ranges(tc, gl.ctas);
+                gl.cta = reinterpret_cast<long*>(base + jput(r.data(), sizeof(long) * r.size()));
                 out.push_back(gl);
             }
         };
@@ -662,6 +689,27 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             }
             add_level(ls_down_, ents, l);
         }
+    }
+    // mixed: P_l - R_l of every tensor-core level, split once per execute
+    // after the power table
+    {
+        std::vector<LevelArgs> sp;
+        for (int i : ls_) {
+            const Sys& q = sys_[i];
+            for (int l = 0; l < q.tc_levels; ++l) {
+                LevelArgs a;
+                a.P = q.P + (long)l * q.Np * q.Np;
+                a.ldp = q.Np;
+                a.Np = q.Np;
+                a.rn = q.solver == kRK4 ? 0 : q.n;
+                a.rsh = std::min(1 << std::min(l, 2), 3);
+                a.Ps = q.Ps + (size_t)l * (level_split_bytes(q.Np) / sizeof(float));
+                sp.push_back(a);
+                maxSplitNp_ = std::max(maxSplitNp_, q.Np);
+            }
+        }
+        nSplit_ = (int)sp.size();
+        if (nSplit_ > 0) dSplit_ = reinterpret_cast<LevelArgs*>(base + jput(sp.data(), sizeof(LevelArgs) * sp.size()));
     }
     // set-up copies: Phi -> P level 0, ABM outputs 0..2 -> Y rows 0..2
     for (int i = 0; i < N; ++i) {
@@ -763,6 +811,10 @@ void BatchPlan::execute(cudaStream_t s)
             launch_grouped(g, fs);
             ++launches;
         }
+        for (int k = 0; k < nSplit_; k += 65535) {
+            launch_level_split(dSplit_ + k, std::min(65535, nSplit_ - k), maxSplitNp_, fs);
+            ++launches;
+        }
         for (const GroupedLaunch& g : ls_up_) {
             launch_grouped(g, fs);
             ++launches;
@@ -790,7 +842,7 @@ void BatchPlan::execute(cudaStream_t s)
 
 void BatchPlan::launch_grouped(const GroupedLaunch& g, cudaStream_t s)
 {
-    if (g.cfg.id == kTcConfig) launch_level_tc(g.args, g.start, g.nent, g.tiles, sms_, dStatus_, s);
+    if (g.cfg.id == kTcConfig) launch_level_tc(g.args, g.start, g.nent, g.cta, g.ctas, dStatus_, s);
     else launch_affine_level_grouped(g.cfg, g.args, g.start, g.nent, g.tiles, g.smem, s);
 }
 

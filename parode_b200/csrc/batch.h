@@ -63,6 +63,9 @@ private:
         int levels = 0;
         bool blocked = false;
         int bucket = -1;          // blocked: index into buckets_
+        double delta = 0;         // |Phi - R|_inf, R the exact 0/1 part (I or the ABM shift)
+        int tc_levels = 0;        // mixed: lowest levels run on the tensor cores
+        float* Ps = nullptr;      // mixed: pre-split P_l - R_l per tensor-core level
         int precision = 0;
         InputEntry* input = nullptr;
         double u_base = 0, u_dt = 0;
@@ -93,6 +96,8 @@ private:
         LevelArgs* swaps = nullptr;  // device: down-sweep entries of the tiled form, swapped first
         int nswap = 0;
         long swap_elems = 0;
+        long* cta = nullptr;         // tensor-core launch: per-CTA tile ranges (ctas + 1)
+        int ctas = 0;
     };
 
     void launch_grouped(const GroupedLaunch& g, cudaStream_t s);
@@ -116,6 +121,8 @@ private:
     ForcingJob* dForcing_ = nullptr;
     OutputJob* dOutput_ = nullptr;
     CopyJob* dSeed_ = nullptr;
+    LevelArgs* dSplit_ = nullptr;  // mixed: P_l - R_l splits (one per system and tensor-core level)
+    int nSplit_ = 0, maxSplitNp_ = 0;
     long maxForcing_ = 0, maxOutput_ = 0, maxSeed_ = 0;
     void* arena_ = nullptr;
     size_t arena_bytes_ = 0;

@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 
+#include <vector>
+
 namespace parode {
 
 // Column addressing of the batched affine-level contraction:
@@ -26,6 +28,8 @@ struct LevelArgs {
     // rn < 0: none; rn == 0: R = I; rn > 0: ABM companion blocks of rn rows,
     // row block b reads block min(b + rsh, 3).
     int rn = -1, rsh = 0;
+    // Mixed form only: P - R pre-split into TF32 hi/lo tiles (level_split_bytes).
+    const float* Ps = nullptr;
 };
 
 // One Blelloch level over all columns (up-sweep, down-sweep or P*P).
@@ -96,8 +100,14 @@ void launch_swap_grouped(const LevelArgs* dArgs, int nent, long max_elems, cudaS
 // level_tc_tiles(a) tiles per entry.  A device wait that gives up sets *status.
 bool level_tc_supported(const LevelArgs& a);
 long level_tc_tiles(const LevelArgs& a);
-void launch_level_tc(const LevelArgs* dArgs, const long* dStart, int nent, long tiles, int sms, int* status,
+// dCta: ctas + 1 tile boundaries (level_tc_ranges), one persistent CTA each.
+void launch_level_tc(const LevelArgs* dArgs, const long* dStart, int nent, const long* dCta, int ctas, int* status,
                      cudaStream_t s);
+std::vector<long> level_tc_ranges(const std::vector<LevelArgs>& ents, int ctas);
+// Bytes of the pre-split P - R of one level (tiles of 128 rows x 16 K, hi then lo).
+size_t level_split_bytes(int Np);
+// Pre-split P - R for every entry (a.P, a.rn, a.rsh -> a.Ps); blockIdx.y = entry.
+void launch_level_split(const LevelArgs* dArgs, int nent, int max_np, cudaStream_t s);
 
 struct SampleJob {
     double* U = nullptr;

@@ -6,12 +6,22 @@
 // Kernels/MVVKernelScanUpsweep.cl:25-48, MVVKernelScanDownsweep.cl:25-48, as
 // one contraction per level).  P rows sit on the MMA's M (128 per tile), the
 // level's vectors on N (64 per tile), K runs over the scan dimension in
-// slices of 32.  Operands stay FP64 in HBM; each slice is converted on the
-// way into shared memory into TF32 hi/lo pairs (x = hi + lo) in the K-major
-// no-swizzle canonical layout, and the tensor core forms hi*hi + hi*lo + lo*hi
-// in FP32.  The FP32 partial sum of every K slice is drained from TMEM into
-// FP64 registers (two TMEM accumulators in turn, so the next slice's MMAs run
-// while the previous one drains): FP32 rounding is confined to 32-term sums.
+// slices of 16.
+//
+// Exact part: P = R + E with R an exact 0/1 matrix, one 1 per row (I for RK4,
+// the companion shift S^(2^l) for ABM).  Only E goes through the tensor
+// cores; R v is added in FP64 in the epilogue.  For the lower levels E is
+// small (P_l = Phi^(2^l) is within about 2^l h |A| of R_l), so the TF32
+// representation error and the FP32 accumulation in TMEM are relative to
+// |E v|, far below |v|.
+//
+// Data path: E is split once per level (k_split) into TF32 hi/lo tiles laid
+// out exactly as the MMA reads them (K-major, no swizzle), so a slice of A is
+// a 16 KB block that cp.async copies straight into shared memory; the
+// level's vectors (B) are loaded as FP64 into registers two slices ahead and
+// split into hi/lo on the way to shared memory.  A 3-stage operand ring lets
+// one thread issue hi*hi + hi*lo + lo*hi for slice s while the CTA fills
+// slice s+1; completion of each slice's MMAs frees its stage (mbarrier).
 #include "common.h"
 #include "kernels.h"
 #include "tc05.cuh"
@@ -25,19 +35,21 @@ namespace {
 using namespace tc05;
 
 constexpr int kThreads = 256;
-constexpr int kBM = 128, kBN = 64, kBK = 32;
-constexpr uint32_t kAHalf = kBM * kBK * 4;  // bytes of A hi (or lo) per stage
-constexpr uint32_t kBHalf = kBN * kBK * 4;
-constexpr uint32_t kStage = 2 * kAHalf + 2 * kBHalf;
-constexpr uint32_t kSmem = 2 * kStage + 64;  // two stages + mbarrier + TMEM slot
-constexpr uint32_t kTmemCols = 2 * kBN;      // two accumulators of 64 FP32 columns
+constexpr int kBM = 128, kBN = 64, kBK = 16;
+constexpr int kStages = 3;
+constexpr uint32_t kAHalf = kBM * kBK * 4;  // A hi (or lo) per slice: 8 KB
+constexpr uint32_t kBHalf = kBN * kBK * 4;  // B hi (or lo): 4 KB
+constexpr uint32_t kABlock = 2 * kAHalf;    // one pre-split A block (hi | lo)
+constexpr uint32_t kStage = kABlock + 2 * kBHalf;
+constexpr uint32_t kOffBar = kStages * kStage;
+constexpr uint32_t kSmem = kOffBar + 64;    // + mbarriers + TMEM slot
+constexpr uint32_t kTmemCols = kBN;
 constexpr long long kWaitLimit = 1LL << 31;
 
-// K-major canonical offset inside a tile with kBK tf32 per row.
-__device__ __forceinline__ uint32_t koff(int r, int k) { return kmajor_off(r, k, kBK); }
+__host__ __device__ constexpr uint32_t koff(int r, int k) { return kmajor_off(r, k, kBK); }
 
 // Column of the 1 in row i of the exact part R (-1: no R).
-__device__ __forceinline__ int r_col(const LevelArgs& a, int i)
+__host__ __device__ inline int r_col(const LevelArgs& a, int i)
 {
     if (a.rn < 0) return -1;
     if (a.rn == 0) return i;
@@ -46,82 +58,90 @@ __device__ __forceinline__ int r_col(const LevelArgs& a, int i)
     return bt * a.rn + (i - b * a.rn);
 }
 
-// Slice s of the tile into shared-memory stage `st` (hi/lo TF32 pairs).
-__device__ __forceinline__ void load_slice(const LevelArgs& a, int m0, long n0, int k0, unsigned char* st)
+// ---------------------------------------------------------------------------
+// E = P - R split into TF32 hi/lo blocks: block (mt, s) = rows [128 mt, +128),
+// K [16 s, +16), hi then lo, each in the canonical K-major layout.
+// ---------------------------------------------------------------------------
+__global__ void k_split(const LevelArgs* __restrict__ args)
 {
-    const int tid = threadIdx.x;
-    // A: 128 rows x 32 K; thread -> (row tid/2, 16 consecutive K)
-    {
-        const int r = tid >> 1, kb = (tid & 1) * 16;
-        const int i = m0 + r;
-        double v[16];
-        if (i < a.Np && k0 + kb < a.Np) {
-            const double2* p = reinterpret_cast<const double2*>(a.P + (long)i * a.ldp + k0 + kb);
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                const double2 t = (k0 + kb + 2 * q < a.Np) ? p[q] : make_double2(0.0, 0.0);
-                v[2 * q] = t.x;
-                v[2 * q + 1] = t.y;
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < 16; ++q) v[q] = 0.0;
+    const LevelArgs& a = args[blockIdx.y];
+    const int Np = a.Np;
+    const int mt = (Np + kBM - 1) / kBM, nk = (Np + kBK - 1) / kBK;
+    const long total = (long)mt * kBM * nk * kBK;  // padded elements
+    unsigned char* out = reinterpret_cast<unsigned char*>(const_cast<float*>(a.Ps));
+    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+        // e walks (row, k) of the padded matrix row-major
+        const long kp = (long)nk * kBK;
+        const int i = (int)(e / kp), k = (int)(e - (long)i * kp);
+        double v = 0.0;
+        if (i < Np && k < Np) {
+            v = a.P[(long)i * a.ldp + k];
+            if (k == r_col(a, i)) v -= 1.0;
         }
-        // P - R: the tensor cores only see the small remainder
-        const int rc = i < a.Np ? r_col(a, i) - (k0 + kb) : -1;
-#pragma unroll
-        for (int q = 0; q < 16; ++q)
-            if (q == rc) v[q] -= 1.0;
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            float4 h, l;
-            split_tf32((float)v[4 * c + 0], h.x, l.x);
-            split_tf32((float)v[4 * c + 1], h.y, l.y);
-            split_tf32((float)v[4 * c + 2], h.z, l.z);
-            split_tf32((float)v[4 * c + 3], h.w, l.w);
-            // the FP32 rounding of x is itself split off: x - (float)x is
-            // below 2^-24 |x| and is dropped, as in every 3xTF32 scheme
-            *reinterpret_cast<float4*>(st + koff(r, kb + 4 * c)) = h;
-            *reinterpret_cast<float4*>(st + kAHalf + koff(r, kb + 4 * c)) = l;
-        }
-    }
-    // B: 64 vectors x 32 K; thread -> (vector tid/4, 8 consecutive K)
-    {
-        const int c = tid >> 2, kb = (tid & 3) * 8;
-        const long g = n0 + c;
-        double v[8];
-        if (g < a.ncols && k0 + kb < a.Np) {
-            const double2* p = reinterpret_cast<const double2*>(a.src + g * a.src_gs + k0 + kb);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const double2 t = (k0 + kb + 2 * q < a.Np) ? p[q] : make_double2(0.0, 0.0);
-                v[2 * q] = t.x;
-                v[2 * q + 1] = t.y;
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < 8; ++q) v[q] = 0.0;
-        }
-        unsigned char* b = st + 2 * kAHalf;
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            float4 h, l;
-            split_tf32((float)v[4 * q + 0], h.x, l.x);
-            split_tf32((float)v[4 * q + 1], h.y, l.y);
-            split_tf32((float)v[4 * q + 2], h.z, l.z);
-            split_tf32((float)v[4 * q + 3], h.w, l.w);
-            *reinterpret_cast<float4*>(b + koff(c, kb + 4 * q)) = h;
-            *reinterpret_cast<float4*>(b + kBHalf + koff(c, kb + 4 * q)) = l;
-        }
+        float hi, lo;
+        split_tf32((float)v, hi, lo);
+        const int mi = i / kBM, s = k / kBK;
+        unsigned char* blk = out + ((size_t)mi * nk + s) * kABlock;
+        *reinterpret_cast<float*>(blk + koff(i - mi * kBM, k - s * kBK)) = hi;
+        *reinterpret_cast<float*>(blk + kAHalf + koff(i - mi * kBM, k - s * kBK)) = lo;
     }
 }
 
-// Thread 0: the 3xTF32 MMAs of one staged slice into TMEM column base `d`.
-__device__ __forceinline__ void issue_slice(uint32_t d, uint32_t st)
+__device__ __forceinline__ void cp16(void* dst, const void* src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// A block of slice s (16 KB, pre-split) into stage memory `st`.
+__device__ __forceinline__ void fetch_a(const LevelArgs& a, int mi, int nk, int s, unsigned char* st)
+{
+    const unsigned char* src = reinterpret_cast<const unsigned char*>(a.Ps) + ((size_t)mi * nk + s) * kABlock;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int c = threadIdx.x + q * kThreads;  // 1024 chunks of 16 bytes
+        cp16(st + c * 16, src + c * 16);
+    }
+}
+
+// B values of slice s for this thread: vector tid/4, K [16 s + 4 (tid&3), +4).
+__device__ __forceinline__ void load_b(const LevelArgs& a, long n0, int s, double (&b)[4])
+{
+    const int v = threadIdx.x >> 2, kb = s * kBK + (threadIdx.x & 3) * 4;
+    const long g = n0 + v;
+    if (g < a.ncols && kb < a.Np) {
+        const double2* p = reinterpret_cast<const double2*>(a.src + g * a.src_gs + kb);
+        const double2 t0 = p[0], t1 = p[1];
+        b[0] = t0.x;
+        b[1] = t0.y;
+        b[2] = t1.x;
+        b[3] = t1.y;
+    } else {
+        b[0] = b[1] = b[2] = b[3] = 0.0;
+    }
+}
+
+__device__ __forceinline__ void store_b(const double (&b)[4], unsigned char* st)
+{
+    const int v = threadIdx.x >> 2, kb = (threadIdx.x & 3) * 4;
+    float4 h, l;
+    split_tf32((float)b[0], h.x, l.x);
+    split_tf32((float)b[1], h.y, l.y);
+    split_tf32((float)b[2], h.z, l.z);
+    split_tf32((float)b[3], h.w, l.w);
+    unsigned char* bb = st + kABlock;
+    *reinterpret_cast<float4*>(bb + koff(v, kb)) = h;
+    *reinterpret_cast<float4*>(bb + kBHalf + koff(v, kb)) = l;
+}
+
+// Thread 0: the 3xTF32 MMAs of one staged slice.
+__device__ __forceinline__ void issue_slice(uint32_t d, uint32_t st, bool first)
 {
     constexpr uint32_t SBO = kBK * 32;  // 8-row groups
     const uint64_t ah = make_desc(st, 128, SBO), al = make_desc(st + kAHalf, 128, SBO);
-    const uint64_t bh = make_desc(st + 2 * kAHalf, 128, SBO), bl = make_desc(st + 2 * kAHalf + kBHalf, 128, SBO);
+    const uint64_t bh = make_desc(st + kABlock, 128, SBO), bl = make_desc(st + kABlock + kBHalf, 128, SBO);
     const uint64_t A[3] = {ah, ah, al};
     const uint64_t B[3] = {bh, bl, bh};
     constexpr uint32_t idesc = make_idesc(kBM, kBN);
@@ -129,89 +149,96 @@ __device__ __forceinline__ void issue_slice(uint32_t d, uint32_t st)
     for (int q = 0; q < 3; ++q)
 #pragma unroll
         for (int s = 0; s < kBK / 8; ++s)
-            mma_tf32(d, A[q] + (uint64_t)(s * 16), B[q] + (uint64_t)(s * 16), idesc, (q == 0 && s == 0) ? 0u : 1u);
+            mma_tf32(d, A[q] + (uint64_t)(s * 16), B[q] + (uint64_t)(s * 16), idesc,
+                     (first && q == 0 && s == 0) ? 0u : 1u);
 }
 
-// Drain TMEM accumulator `d` (this warp's 32 lanes, 32 columns) into FP64.
-__device__ __forceinline__ void drain(uint32_t taddr, double (&acc)[32])
+struct Ring {
+    uint32_t phase[kStages];
+};
+
+__device__ __forceinline__ void ring_wait(uint64_t* bar, Ring& r, int st, int* status)
 {
-    uint32_t r[32];
-    tmem_ld32(taddr, r);
-    tmem_wait_ld();
-#pragma unroll
-    for (int j = 0; j < 32; ++j) acc[j] += (double)__uint_as_float(r[j]);
+    if (!mbar_wait(&bar[st], r.phase[st], kWaitLimit) && (threadIdx.x & 31) == 0) atomicExch(status, 1);
+    r.phase[st] ^= 1u;
 }
 
-__device__ void tc_tile(const LevelArgs& a, long tile, unsigned char* sm, uint64_t* bar, uint32_t tbase,
-                        uint32_t& phase, int* status)
+__device__ void tc_tile(const LevelArgs& a, long tile, unsigned char* sm, uint64_t* bar, uint32_t tbase, Ring& ring,
+                        int* status)
 {
     const int mt = (a.Np + kBM - 1) / kBM;
-    const int m0 = (int)(tile % mt) * kBM;
+    const int mi = (int)(tile % mt);
+    const int m0 = mi * kBM;
     const long n0 = (tile / mt) * kBN;
     const int nk = (a.Np + kBK - 1) / kBK;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int quarter = warp & 3, half = warp >> 2;
-    const uint32_t lane_addr = (uint32_t)(32 * quarter) << 16;
     const uint32_t base = smem_u32(sm);
-    double acc[32];
-#pragma unroll
-    for (int j = 0; j < 32; ++j) acc[j] = 0.0;
 
-    load_slice(a, m0, n0, 0, sm);
-    fence_async_smem();
-    fence_before_sync();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        fence_after_sync();
-        issue_slice(tbase, base);
-        mma_commit(bar);
-    }
+    // slice s uses stage s % 3; its MMAs commit to bar[s % 3]
+    double b0[4], b1[4];
+    load_b(a, n0, 0, b0);
+    if (nk > 1) load_b(a, n0, 1, b1);
+    fetch_a(a, mi, nk, 0, sm);
+    cp_commit();
     for (int s = 0; s < nk; ++s) {
-        if (s + 1 < nk) load_slice(a, m0, n0, (s + 1) * kBK, sm + ((s + 1) & 1) * kStage);
-        // MMAs of slice s done: its stage may be refilled, its accumulator read
-        if (!mbar_wait(bar, phase, kWaitLimit) && lane == 0) atomicExch(status, 1);
-        phase ^= 1u;
+        const int st = s % kStages, nx = (s + 1) % kStages;
+        // stage nx was last read by MMA(s - 2)
+        if (s >= 2) ring_wait(bar, ring, nx, status);
+        if (s + 1 < nk) fetch_a(a, mi, nk, s + 1, sm + nx * kStage);
+        cp_commit();
+        store_b(b0, sm + st * kStage);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) b0[q] = b1[q];
+        if (s + 2 < nk) load_b(a, n0, s + 2, b1);
+        cp_wait1();  // A of slice s has landed (this thread's chunks)
         fence_async_smem();
         fence_before_sync();
         __syncthreads();
-        if (threadIdx.x == 0 && s + 1 < nk) {
+        if (threadIdx.x == 0) {
             fence_after_sync();
-            issue_slice(tbase + (uint32_t)(((s + 1) & 1) * kBN), base + ((s + 1) & 1) * kStage);
-            mma_commit(bar);
+            issue_slice(tbase, base + st * kStage, s == 0);
+            mma_commit(&bar[st]);
         }
-        fence_after_sync();
-        drain(tbase + lane_addr + (uint32_t)((s & 1) * kBN + half * 32), acc);
     }
-    // results: row i of P, vectors g = n0 + 32 half + j
+    cp_wait0();
+    // consume the completions not yet waited for: MMA(nk-2) (if any) and MMA(nk-1)
+    for (int s = std::max(0, nk - 2); s < nk; ++s) ring_wait(bar, ring, s % kStages, status);
+    fence_after_sync();
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int quarter = warp & 3, half = warp >> 2;
+    uint32_t r[32];
+    tmem_ld32(tbase + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(half * 32), r);
+    tmem_wait_ld();
     const long i = m0 + 32 * quarter + lane;
     if (i < a.Np) {
         const int rc = r_col(a, (int)i);
-#pragma unroll
+#pragma unroll 8
         for (int j = 0; j < 32; ++j) {
             const long g = n0 + 32 * half + j;
             if (g < a.ncols) {
-                double v = acc[j];
+                double v = (double)__uint_as_float(r[j]);
                 if (rc >= 0) v += a.src[g * a.src_gs + rc];  // R v, exact
                 if (a.acc) v += a.acc[g * a.acc_gs + i * a.acc_is];
                 a.dst[g * a.dst_gs + i * a.dst_is] = v;
             }
         }
     }
-    // every thread's TMEM reads are complete before the next tile's MMAs
+    // TMEM reads complete before the next tile's first MMA overwrites it
     fence_before_sync();
     __syncthreads();
 }
 
-// Persistent grouped kernel: CTAs walk the tiles of all entries.
-__global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __restrict__ args,
-                                                          const long* __restrict__ start, int nent, long tiles,
-                                                          int* status)
+// Persistent grouped kernel: CTA c walks tiles [cta[c], cta[c+1]) in order
+// (ranges balanced on the host); entries are found by a forward scan.
+__global__ void __launch_bounds__(kThreads, 2) k_level_tc(const LevelArgs* __restrict__ args,
+                                                          const long* __restrict__ start, int nent,
+                                                          const long* __restrict__ cta, int* status)
 {
     extern __shared__ __align__(1024) unsigned char sm[];
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + 2 * kStage);
-    uint32_t* slot = reinterpret_cast<uint32_t*>(sm + 2 * kStage + 16);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kOffBar);
+    uint32_t* slot = reinterpret_cast<uint32_t*>(sm + kOffBar + 32);
     if (threadIdx.x == 0) {
-        mbar_init(bar, 1);
+        for (int q = 0; q < kStages; ++q) mbar_init(&bar[q], 1);
         mbar_fence_init();
     }
     if ((threadIdx.x >> 5) == 0) tmem_alloc(slot, kTmemCols);
@@ -219,16 +246,27 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
     __syncthreads();
     fence_after_sync();
     const uint32_t tbase = *slot;
-    uint32_t phase = 0;
-    for (long t = blockIdx.x; t < tiles; t += gridDim.x) {
-        int lo = 0, hi = nent - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (start[mid] <= t) lo = mid;
+    Ring ring;
+    for (int q = 0; q < kStages; ++q) ring.phase[q] = 0;
+    const long t0 = cta[blockIdx.x], t1 = cta[blockIdx.x + 1];
+    int e = 0;
+    {
+        int hi = nent - 1;
+        while (e < hi) {
+            const int mid = (e + hi + 1) >> 1;
+            if (start[mid] <= t0) e = mid;
             else hi = mid - 1;
         }
-        const LevelArgs a = args[lo];
-        tc_tile(a, t - start[lo], sm, bar, tbase, phase, status);
+    }
+    LevelArgs a = args[e];
+    long next = e + 1 < nent ? start[e + 1] : t1;
+    for (long t = t0; t < t1; ++t) {
+        while (t >= next) {
+            ++e;
+            a = args[e];
+            next = e + 1 < nent ? start[e + 1] : t1;
+        }
+        tc_tile(a, t - start[e], sm, bar, tbase, ring, status);
     }
     fence_after_sync();
     if ((threadIdx.x >> 5) == 0) tmem_dealloc(tbase, kTmemCols);
@@ -241,26 +279,62 @@ long level_tc_tiles(const LevelArgs& a)
     return (long)((a.Np + kBM - 1) / kBM) * ((a.ncols + kBN - 1) / kBN);
 }
 
+size_t level_split_bytes(int Np)
+{
+    return (size_t)((Np + kBM - 1) / kBM) * ((Np + kBK - 1) / kBK) * kABlock;
+}
+
 bool level_tc_supported(const LevelArgs& a)
 {
     // K-contiguous FP64 sources with 16-byte aligned rows, no in-place copy
     return a.cpy == nullptr && a.src_ks == 1 && (a.src_gs % 2) == 0 && (a.ldp % 2) == 0 && (a.Np % 8) == 0 &&
-           a.Np > 64 && a.Np <= 1024 && (reinterpret_cast<uintptr_t>(a.src) & 15) == 0 &&
-           (reinterpret_cast<uintptr_t>(a.P) & 15) == 0;
+           a.Np > 64 && a.Np <= 1024 && (reinterpret_cast<uintptr_t>(a.src) & 15) == 0;
 }
 
-void launch_level_tc(const LevelArgs* dArgs, const long* dStart, int nent, long tiles, int sms, int* status,
+void launch_level_split(const LevelArgs* dArgs, int nent, int max_np, cudaStream_t s)
+{
+    if (nent <= 0) return;
+    const long elems = (long)level_split_bytes(max_np) / 8;
+    dim3 grid((unsigned)std::max<long>(1, std::min<long>((elems + 255) / 256, 512)), (unsigned)nent);
+    k_split<<<grid, 256, 0, s>>>(dArgs);
+    PARODE_CUDA(cudaGetLastError());
+}
+
+void launch_level_tc(const LevelArgs* dArgs, const long* dStart, int nent, const long* dCta, int ctas, int* status,
                      cudaStream_t s)
 {
-    if (nent <= 0 || tiles <= 0) return;
+    if (nent <= 0 || ctas <= 0) return;
     static bool attr_set = false;
     if (!attr_set) {
         PARODE_CUDA(cudaFuncSetAttribute(k_level_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));
         attr_set = true;
     }
-    const unsigned grid = (unsigned)std::min<long>(tiles, sms);
-    k_level_tc<<<grid, kThreads, kSmem, s>>>(dArgs, dStart, nent, tiles, status);
+    k_level_tc<<<(unsigned)ctas, kThreads, kSmem, s>>>(dArgs, dStart, nent, dCta, status);
     PARODE_CUDA(cudaGetLastError());
+}
+
+// Host: tile ranges of `ctas` CTAs with about equal work (a tile costs its
+// K slices plus a fixed overhead).
+std::vector<long> level_tc_ranges(const std::vector<LevelArgs>& ents, int ctas)
+{
+    std::vector<double> cost;
+    double total = 0;
+    for (const LevelArgs& a : ents) {
+        const long n = level_tc_tiles(a);
+        const double c = (a.Np + kBK - 1) / kBK + 4.0;
+        for (long t = 0; t < n; ++t) cost.push_back(c);
+        total += c * n;
+    }
+    std::vector<long> r(ctas + 1, (long)cost.size());
+    r[0] = 0;
+    double acc = 0;
+    int k = 1;
+    for (long t = 0; t < (long)cost.size() && k < ctas; ++t) {
+        acc += cost[t];
+        while (k < ctas && acc >= total * k / ctas) r[k++] = t + 1;
+    }
+    for (; k < ctas; ++k) r[k] = (long)cost.size();
+    return r;
 }
 
 }  // namespace parode
