@@ -358,7 +358,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         job_bytes = nb * (sizeof(LeafArgs) + 3 * sizeof(double*) + 4 * kAlign) +
                     (size_t)items_ub * sizeof(BatchItem) + buckets_.size() * 8 * kAlign +
                     (size_t)N * (sizeof(SampleJob) + sizeof(ForcingJob) + sizeof(OutputJob) + 2 * sizeof(CopyJob)) +
-                    8 * kAlign + (size_t)lev_entries * (2 * sizeof(LevelArgs) + sizeof(long)) +
+                    8 * kAlign + (size_t)lev_entries * (2 * sizeof(LevelArgs) + sizeof(long) + 128) +
                     (size_t)(3 * 64 * 8) * 2 * kAlign + (size_t)2 * 64 * (2 * sms_ + 1) * sizeof(long) +
                     ((size_t)1 << 20);
     }
@@ -605,6 +605,11 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
                 out.push_back(gl);
             }
             if (!tc.empty()) {
+                // TMA tensor maps of the entries' source columns (128 bytes each)
+                std::vector<unsigned char> maps(tc.size() * 128);
+                for (size_t k = 0; k < tc.size(); ++k) level_encode_src_map(tc[k], &maps[k * 128]);
+                const size_t moff = jput(maps.data(), maps.size());
+                for (size_t k = 0; k < tc.size(); ++k) tc[k].src_map = base + moff + k * 128;
                 GroupedLaunch gl;
                 gl.cfg.id = kTcConfig;
                 std::vector<long> start;
@@ -617,8 +622,8 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
                 gl.tiles = tiles;
                 gl.args = reinterpret_cast<LevelArgs*>(base + jput(tc.data(), sizeof(LevelArgs) * tc.size()));
                 gl.start = reinterpret_cast<long*>(base + jput(start.data(), sizeof(long) * start.size()));
-                // two persistent CTAs per SM, tile ranges balanced by work
-                gl.ctas = (int)std::min<long>(2L * sms_, tiles);
+                // one persistent CTA per SM, tile ranges balanced by work
+                gl.ctas = (int)std::min<long>(sms_, tiles);
                 std::vector<long> r = level_tc_ranges(tc, gl.ctas);
                 gl.cta = reinterpret_cast<long*>(base + jput(r.data(), sizeof(long) * r.size()));
                 out.push_back(gl);

@@ -30,6 +30,9 @@ struct LevelArgs {
     int rn = -1, rsh = 0;
     // Mixed form only: P - R pre-split into TF32 hi/lo tiles (level_split_bytes).
     const float* Ps = nullptr;
+    // Mixed form only: device address of a 128-byte TMA tensor map over the
+    // source columns (level_encode_src_map).
+    const void* src_map = nullptr;
 };
 
 // One Blelloch level over all columns (up-sweep, down-sweep or P*P).
@@ -104,6 +107,10 @@ long level_tc_tiles(const LevelArgs& a);
 void launch_level_tc(const LevelArgs* dArgs, const long* dStart, int nent, const long* dCta, int ctas, int* status,
                      cudaStream_t s);
 std::vector<long> level_tc_ranges(const std::vector<LevelArgs>& ents, int ctas);
+// Encodes into out[0..127] (host) the TMA tensor map of a's source columns:
+// FP64, inner dimension Np (K), outer dimension ncols at stride src_gs, box
+// 16 x 64, zero fill outside.  Throws on failure.
+void level_encode_src_map(const LevelArgs& a, void* out);
 // Bytes of the pre-split P - R of one level (tiles of 128 rows x 16 K, hi then lo).
 size_t level_split_bytes(int Np);
 // Pre-split P - R for every entry (a.P, a.rn, a.rsh -> a.Ps); blockIdx.y = entry.

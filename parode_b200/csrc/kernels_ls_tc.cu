@@ -15,16 +15,26 @@
 // representation error and the FP32 accumulation in TMEM are relative to
 // |E v|, far below |v|.
 //
-// Data path: E is split once per level (k_split) into TF32 hi/lo tiles laid
-// out exactly as the MMA reads them (K-major, no swizzle), so a slice of A is
-// a 16 KB block that cp.async copies straight into shared memory; the
-// level's vectors (B) are loaded as FP64 into registers two slices ahead and
-// split into hi/lo on the way to shared memory.  A 3-stage operand ring lets
-// one thread issue hi*hi + hi*lo + lo*hi for slice s while the CTA fills
-// slice s+1; completion of each slice's MMAs frees its stage (mbarrier).
+// E is split once per level (k_split) into TF32 hi/lo blocks laid out as the
+// MMA reads them (K-major, no swizzle).  The contraction kernel is
+// warp-specialised around a ring of shared-memory stages:
+//   warp 0      producer: per slice one bulk copy (TMA engine) of the 16 KB A
+//               block and one 128-byte bulk copy per vector of B (FP64),
+//               completing on the stage's `full` mbarrier;
+//   warps 2-3   converters: B FP64 -> TF32 hi/lo in the canonical layout,
+//               then arrive on `conv`;
+//   warp 1      one thread issues hi*hi + hi*lo + lo*hi into one of two TMEM
+//               accumulators and commits to `empty` (stage free) and, after a
+//               tile's last slice, to `acc_full`;
+//   warps 4-7   epilogue: TMEM -> FP64, + R v + acc, store; arrive `acc_empty`.
+// Every wait is bounded; a wait that gives up sets the status word and an
+// abort flag that makes every role leave its loop.
 #include "common.h"
 #include "kernels.h"
 #include "tc05.cuh"
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 
@@ -36,17 +46,36 @@ using namespace tc05;
 
 constexpr int kThreads = 256;
 constexpr int kBM = 128, kBN = 64, kBK = 16;
-constexpr int kStages = 3;
-constexpr uint32_t kAHalf = kBM * kBK * 4;  // A hi (or lo) per slice: 8 KB
-constexpr uint32_t kBHalf = kBN * kBK * 4;  // B hi (or lo): 4 KB
-constexpr uint32_t kABlock = 2 * kAHalf;    // one pre-split A block (hi | lo)
-constexpr uint32_t kStage = kABlock + 2 * kBHalf;
-constexpr uint32_t kOffBar = kStages * kStage;
-constexpr uint32_t kSmem = kOffBar + 64;    // + mbarriers + TMEM slot
-constexpr uint32_t kTmemCols = kBN;
+constexpr int kS = 5;                        // ring stages
+constexpr uint32_t kAHalf = kBM * kBK * 4;   // A hi (or lo) per slice: 8 KB
+constexpr uint32_t kBHalf = kBN * kBK * 4;   // B hi (or lo): 4 KB
+constexpr uint32_t kABlock = 2 * kAHalf;     // pre-split A block (hi | lo)
+constexpr uint32_t kBRaw = kBN * kBK * 8;    // B FP64, vector v at v * 128 bytes
+constexpr uint32_t kOffRaw = kABlock;
+constexpr uint32_t kOffConvB = kABlock + kBRaw;
+constexpr uint32_t kStage = kABlock + kBRaw + 2 * kBHalf;  // 32 KB
+constexpr uint32_t kOffBars = kS * kStage;
+// barriers: full[kS], conv[kS], empty[kS], acc_full[2], acc_empty[2]
+constexpr uint32_t kNumBars = 3 * kS + 4;
+constexpr uint32_t kOffSlot = kOffBars + 8 * kNumBars;
+constexpr uint32_t kSmem = kOffSlot + 16;
+constexpr uint32_t kTmemCols = 2 * kBN;
 constexpr long long kWaitLimit = 1LL << 31;
 
+// Phase-trace hook (no-op unless a timing harness defines it).
+#ifndef PARODE_TC_TRACE
+#define PARODE_TC_TRACE_INIT() ((void)0)
+#define PARODE_TC_TRACE(ev) ((void)0)
+#endif
+
 __host__ __device__ constexpr uint32_t koff(int r, int k) { return kmajor_off(r, k, kBK); }
+
+// K elements of slice s (16, or 8 for the last slice when Np = 8 mod 16).
+__device__ __forceinline__ int slice_len(int Np, int s)
+{
+    const int rest = Np - s * kBK;
+    return rest < kBK ? rest : kBK;
+}
 
 // Column of the 1 in row i of the exact part R (-1: no R).
 __host__ __device__ inline int r_col(const LevelArgs& a, int i)
@@ -70,7 +99,6 @@ __global__ void k_split(const LevelArgs* __restrict__ args)
     const long total = (long)mt * kBM * nk * kBK;  // padded elements
     unsigned char* out = reinterpret_cast<unsigned char*>(const_cast<float*>(a.Ps));
     for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
-        // e walks (row, k) of the padded matrix row-major
         const long kp = (long)nk * kBK;
         const int i = (int)(e / kp), k = (int)(e - (long)i * kp);
         double v = 0.0;
@@ -87,189 +115,335 @@ __global__ void k_split(const LevelArgs* __restrict__ args)
     }
 }
 
-__device__ __forceinline__ void cp16(void* dst, const void* src)
-{
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+// ---- mbarrier / bulk-copy helpers --------------------------------------------
 
-// A block of slice s (16 KB, pre-split) into stage memory `st`.
-__device__ __forceinline__ void fetch_a(const LevelArgs& a, int mi, int nk, int s, unsigned char* st)
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
 {
-    const unsigned char* src = reinterpret_cast<const unsigned char*>(a.Ps) + ((size_t)mi * nk + s) * kABlock;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int c = threadIdx.x + q * kThreads;  // 1024 chunks of 16 bytes
-        cp16(st + c * 16, src + c * 16);
-    }
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-// B values of slice s for this thread: vector tid/4, K [16 s + 4 (tid&3), +4).
-__device__ __forceinline__ void load_b(const LevelArgs& a, long n0, int s, double (&b)[4])
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t* bar, uint32_t bytes)
 {
-    const int v = threadIdx.x >> 2, kb = s * kBK + (threadIdx.x & 3) * 4;
-    const long g = n0 + v;
-    if (g < a.ncols && kb < a.Np) {
-        const double2* p = reinterpret_cast<const double2*>(a.src + g * a.src_gs + kb);
-        const double2 t0 = p[0], t1 = p[1];
-        b[0] = t0.x;
-        b[1] = t0.y;
-        b[2] = t1.x;
-        b[3] = t1.y;
-    } else {
-        b[0] = b[1] = b[2] = b[3] = 0.0;
-    }
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
 }
 
-__device__ __forceinline__ void store_b(const double (&b)[4], unsigned char* st)
+// Bulk copy (TMA engine, no tensor map) of `bytes` (multiple of 16, both
+// addresses 16-byte aligned) into this CTA's shared memory.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
 {
-    const int v = threadIdx.x >> 2, kb = (threadIdx.x & 3) * 4;
-    float4 h, l;
-    split_tf32((float)b[0], h.x, l.x);
-    split_tf32((float)b[1], h.y, l.y);
-    split_tf32((float)b[2], h.z, l.z);
-    split_tf32((float)b[3], h.w, l.w);
-    unsigned char* bb = st + kABlock;
-    *reinterpret_cast<float4*>(bb + koff(v, kb)) = h;
-    *reinterpret_cast<float4*>(bb + kBHalf + koff(v, kb)) = l;
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
 }
 
-// Thread 0: the 3xTF32 MMAs of one staged slice.
-__device__ __forceinline__ void issue_slice(uint32_t d, uint32_t st, bool first)
+// 2D tensor load (TMA, this GPU's memory, no multicast) of the box at
+// coordinates (x, y) of the tensor map at device address `map`.
+__device__ __forceinline__ void tma_load_2d(void* dst, const void* map, int x, int y, uint64_t* bar)
 {
-    constexpr uint32_t SBO = kBK * 32;  // 8-row groups
-    const uint64_t ah = make_desc(st, 128, SBO), al = make_desc(st + kAHalf, 128, SBO);
-    const uint64_t bh = make_desc(st + kABlock, 128, SBO), bl = make_desc(st + kABlock + kBHalf, 128, SBO);
-    const uint64_t A[3] = {ah, ah, al};
-    const uint64_t B[3] = {bh, bl, bh};
-    constexpr uint32_t idesc = make_idesc(kBM, kBN);
-#pragma unroll
-    for (int q = 0; q < 3; ++q)
-#pragma unroll
-        for (int s = 0; s < kBK / 8; ++s)
-            mma_tf32(d, A[q] + (uint64_t)(s * 16), B[q] + (uint64_t)(s * 16), idesc,
-                     (first && q == 0 && s == 0) ? 0u : 1u);
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];" ::"r"(smem_u32(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
 }
 
-struct Ring {
-    uint32_t phase[kStages];
-};
-
-__device__ __forceinline__ void ring_wait(uint64_t* bar, Ring& r, int st, int* status)
+// Bounded wait shared by all roles: on time-out, record it and raise abort.
+__device__ __forceinline__ bool role_wait(uint64_t* bar, uint32_t parity, volatile int* abort, int* status)
 {
-    if (!mbar_wait(&bar[st], r.phase[st], kWaitLimit) && (threadIdx.x & 31) == 0) atomicExch(status, 1);
-    r.phase[st] ^= 1u;
+    if (*abort) return false;
+    if (mbar_wait(bar, parity, kWaitLimit)) return true;
+    *abort = 1;
+    atomicExch(status, 1);
+    return false;
 }
 
-__device__ void tc_tile(const LevelArgs& a, long tile, unsigned char* sm, uint64_t* bar, uint32_t tbase, Ring& ring,
-                        int* status)
-{
-    const int mt = (a.Np + kBM - 1) / kBM;
-    const int mi = (int)(tile % mt);
-    const int m0 = mi * kBM;
-    const long n0 = (tile / mt) * kBN;
-    const int nk = (a.Np + kBK - 1) / kBK;
-    const uint32_t base = smem_u32(sm);
-
-    // slice s uses stage s % 3; its MMAs commit to bar[s % 3]
-    double b0[4], b1[4];
-    load_b(a, n0, 0, b0);
-    if (nk > 1) load_b(a, n0, 1, b1);
-    fetch_a(a, mi, nk, 0, sm);
-    cp_commit();
-    for (int s = 0; s < nk; ++s) {
-        const int st = s % kStages, nx = (s + 1) % kStages;
-        // stage nx was last read by MMA(s - 2)
-        if (s >= 2) ring_wait(bar, ring, nx, status);
-        if (s + 1 < nk) fetch_a(a, mi, nk, s + 1, sm + nx * kStage);
-        cp_commit();
-        store_b(b0, sm + st * kStage);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) b0[q] = b1[q];
-        if (s + 2 < nk) load_b(a, n0, s + 2, b1);
-        cp_wait1();  // A of slice s has landed (this thread's chunks)
-        fence_async_smem();
-        fence_before_sync();
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            fence_after_sync();
-            issue_slice(tbase, base + st * kStage, s == 0);
-            mma_commit(&bar[st]);
-        }
-    }
-    cp_wait0();
-    // consume the completions not yet waited for: MMA(nk-2) (if any) and MMA(nk-1)
-    for (int s = std::max(0, nk - 2); s < nk; ++s) ring_wait(bar, ring, s % kStages, status);
-    fence_after_sync();
-
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int quarter = warp & 3, half = warp >> 2;
-    uint32_t r[32];
-    tmem_ld32(tbase + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(half * 32), r);
-    tmem_wait_ld();
-    const long i = m0 + 32 * quarter + lane;
-    if (i < a.Np) {
-        const int rc = r_col(a, (int)i);
-#pragma unroll 8
-        for (int j = 0; j < 32; ++j) {
-            const long g = n0 + 32 * half + j;
-            if (g < a.ncols) {
-                double v = (double)__uint_as_float(r[j]);
-                if (rc >= 0) v += a.src[g * a.src_gs + rc];  // R v, exact
-                if (a.acc) v += a.acc[g * a.acc_gs + i * a.acc_is];
-                a.dst[g * a.dst_gs + i * a.dst_is] = v;
-            }
-        }
-    }
-    // TMEM reads complete before the next tile's first MMA overwrites it
-    fence_before_sync();
-    __syncthreads();
-}
-
-// Persistent grouped kernel: CTA c walks tiles [cta[c], cta[c+1]) in order
-// (ranges balanced on the host); entries are found by a forward scan.
-__global__ void __launch_bounds__(kThreads, 2) k_level_tc(const LevelArgs* __restrict__ args,
-                                                          const long* __restrict__ start, int nent,
-                                                          const long* __restrict__ cta, int* status)
-{
-    extern __shared__ __align__(1024) unsigned char sm[];
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kOffBar);
-    uint32_t* slot = reinterpret_cast<uint32_t*>(sm + kOffBar + 32);
-    if (threadIdx.x == 0) {
-        for (int q = 0; q < kStages; ++q) mbar_init(&bar[q], 1);
-        mbar_fence_init();
-    }
-    if ((threadIdx.x >> 5) == 0) tmem_alloc(slot, kTmemCols);
-    fence_before_sync();
-    __syncthreads();
-    fence_after_sync();
-    const uint32_t tbase = *slot;
-    Ring ring;
-    for (int q = 0; q < kStages; ++q) ring.phase[q] = 0;
-    const long t0 = cta[blockIdx.x], t1 = cta[blockIdx.x + 1];
-    int e = 0;
+// Tile sequence of one CTA: entries found by a forward scan.
+struct Cursor {
+    const LevelArgs* args;
+    const long* start;
+    int nent;
+    int e;
+    long next;
+    LevelArgs a;
+    __device__ void init(const LevelArgs* ar, const long* st, int n, long t0, long t1)
     {
+        args = ar;
+        start = st;
+        nent = n;
+        e = 0;
         int hi = nent - 1;
         while (e < hi) {
             const int mid = (e + hi + 1) >> 1;
             if (start[mid] <= t0) e = mid;
             else hi = mid - 1;
         }
+        a = args[e];
+        next = e + 1 < nent ? start[e + 1] : t1;
+        end = t1;
     }
-    LevelArgs a = args[e];
-    long next = e + 1 < nent ? start[e + 1] : t1;
-    for (long t = t0; t < t1; ++t) {
-        while (t >= next) {
+    long end;
+    // entry of tile t (t non-decreasing); returns the tile index inside it
+    __device__ long seek(long t)
+    {
+        while (t >= next && e + 1 < nent) {
             ++e;
             a = args[e];
-            next = e + 1 < nent ? start[e + 1] : t1;
+            next = e + 1 < nent ? start[e + 1] : end;
         }
-        tc_tile(a, t - start[e], sm, bar, tbase, ring, status);
+        return t - start[e];
+    }
+};
+
+__device__ __forceinline__ void tile_coords(const LevelArgs& a, long lt, int& mi, int& m0, long& n0, int& nk)
+{
+    const int mt = (a.Np + kBM - 1) / kBM;
+    mi = (int)(lt % mt);
+    m0 = mi * kBM;
+    n0 = (lt / mt) * kBN;
+    nk = (a.Np + kBK - 1) / kBK;
+}
+
+// Persistent grouped kernel: CTA c walks tiles [cta[c], cta[c+1]) in order.
+__global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __restrict__ args,
+                                                          const long* __restrict__ start, int nent,
+                                                          const long* __restrict__ cta, int* status)
+{
+    extern __shared__ __align__(1024) unsigned char sm[];
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sm + kOffBars);
+    uint64_t* full = bars;
+    uint64_t* conv = bars + kS;
+    uint64_t* empty = bars + 2 * kS;
+    uint64_t* acc_full = bars + 3 * kS;
+    uint64_t* acc_empty = bars + 3 * kS + 2;
+    uint32_t* slot = reinterpret_cast<uint32_t*>(sm + kOffSlot);
+    volatile int* abort = reinterpret_cast<volatile int*>(sm + kOffSlot + 8);
+    PARODE_TC_TRACE_INIT();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < kS; ++q) {
+            mbar_init(&full[q], 1);  // the producer's expect-tx arrive; the copies complete the bytes
+            mbar_init(&conv[q], 2);
+            mbar_init(&empty[q], 1);
+        }
+        for (int q = 0; q < 2; ++q) {
+            mbar_init(&acc_full[q], 1);
+            mbar_init(&acc_empty[q], 4);
+        }
+        *abort = 0;
+        mbar_fence_init();
+    }
+    if (warp == 0) tmem_alloc(slot, kTmemCols);
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    const uint32_t tbase = *slot;
+    const long t0 = cta[blockIdx.x], t1 = cta[blockIdx.x + 1];
+
+    if (warp == 0) {
+        // ---------------- producer ----------------
+        Cursor c;
+        c.init(args, start, nent, t0, t1);
+        long j = 0;  // slice counter
+        for (long t = t0; t < t1 && !*abort; ++t) {
+            const long lt = c.seek(t);
+            const LevelArgs& a = c.a;
+            int mi, m0, nk;
+            long n0;
+            tile_coords(a, lt, mi, m0, n0, nk);
+            const int nv = (int)std::min<long>(kBN, a.ncols - n0);
+            // the epilogue's acc rows of this tile into L2 ahead of time
+            if (a.acc) {
+                const int rows = a.Np - m0 < kBM ? a.Np - m0 : kBM;
+                const int lines = (rows * 8 + 127) / 128;
+                for (int q = lane; q < nv * lines; q += 32) {
+                    const int v = q / lines, ln = q - v * lines;
+                    const double* p = a.acc + (n0 + v) * a.acc_gs + (long)m0 * a.acc_is + ln * 16;
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+                }
+            }
+            for (int s = 0; s < nk && !*abort; ++s, ++j) {
+                const int st = (int)(j % kS);
+                const long use = j / kS;
+                if (use >= 1 && !role_wait(&empty[st], (uint32_t)((use - 1) & 1), abort, status)) break;
+                const int kl = slice_len(a.Np, s);  // 16 or 8 doubles
+                unsigned char* stg = sm + st * kStage;
+                // A: one 16 KB bulk copy; B: one 2D tensor load of 64 vectors x
+                // 16 K (FP64; x = 16 s, a multiple of 16 bytes; the tails beyond
+                // Np or ncols are zero-filled by the TMA engine)
+                if (lane == 0) {
+                    mbar_arrive_tx(&full[st], kABlock + kBRaw);
+                    bulk_g2s(stg, reinterpret_cast<const unsigned char*>(a.Ps) + ((size_t)mi * nk + s) * kABlock,
+                             kABlock, &full[st]);
+                    tma_load_2d(stg + kOffRaw, a.src_map, s * kBK, (int)n0, &full[st]);
+                }
+                __syncwarp();
+                PARODE_TC_TRACE(0);
+            }
+        }
+    } else if (warp == 1) {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0) {
+            Cursor c;
+            c.init(args, start, nent, t0, t1);
+            long j = 0, u = 0;  // slice and tile counters
+            constexpr uint32_t SBO = kBK * 32;
+            constexpr uint32_t idesc = make_idesc(kBM, kBN);
+            for (long t = t0; t < t1 && !*abort; ++t, ++u) {
+                const long lt = c.seek(t);
+                int mi, m0, nk;
+                long n0;
+                tile_coords(c.a, lt, mi, m0, n0, nk);
+                const int ab = (int)(u & 1);
+                const long ause = u >> 1;
+                if (ause >= 1 && !role_wait(&acc_empty[ab], (uint32_t)((ause - 1) & 1), abort, status)) break;
+                fence_after_sync();
+                const uint32_t d = tbase + (uint32_t)(ab * kBN);
+                bool ok = true;
+                for (int s = 0; s < nk; ++s, ++j) {
+                    const int st = (int)(j % kS);
+                    // A landed (bulk copy) and B converted
+                    if (!role_wait(&full[st], (uint32_t)((j / kS) & 1), abort, status) ||
+                        !role_wait(&conv[st], (uint32_t)((j / kS) & 1), abort, status)) {
+                        ok = false;
+                        break;
+                    }
+                    fence_after_sync();
+                    const uint32_t stg = smem_u32(sm + st * kStage);
+                    const uint64_t ah = make_desc(stg, 128, SBO), al = make_desc(stg + kAHalf, 128, SBO);
+                    const uint64_t bh = make_desc(stg + kOffConvB, 128, SBO);
+                    const uint64_t bl = make_desc(stg + kOffConvB + kBHalf, 128, SBO);
+                    const uint64_t A[3] = {ah, ah, al};
+                    const uint64_t B[3] = {bh, bl, bh};
+#pragma unroll
+                    for (int q = 0; q < 3; ++q)
+#pragma unroll
+                        for (int k = 0; k < kBK / 8; ++k)
+                            mma_tf32(d, A[q] + (uint64_t)(k * 16), B[q] + (uint64_t)(k * 16), idesc,
+                                     (s == 0 && q == 0 && k == 0) ? 0u : 1u);
+                    mma_commit(&empty[st]);
+                    PARODE_TC_TRACE(1);
+                }
+                if (!ok) break;
+                mma_commit(&acc_full[ab]);
+            }
+        }
+        __syncwarp();
+    } else if (warp == 2 || warp == 3) {
+        // ---------------- converters (64 threads) ----------------
+        const int ct = threadIdx.x - 64;
+        Cursor c;
+        c.init(args, start, nent, t0, t1);
+        long j = 0;
+        for (long t = t0; t < t1 && !*abort; ++t) {
+            const long lt = c.seek(t);
+            const LevelArgs& a = c.a;
+            int mi, m0, nk;
+            long n0;
+            tile_coords(a, lt, mi, m0, n0, nk);
+            bool ok = true;
+            for (int s = 0; s < nk; ++s, ++j) {
+                const int st = (int)(j % kS);
+                if (!role_wait(&full[st], (uint32_t)((j / kS) & 1), abort, status)) {
+                    ok = false;
+                    break;
+                }
+                unsigned char* stg = sm + st * kStage;
+                const double* raw = reinterpret_cast<const double*>(stg + kOffRaw);
+                const int kl = slice_len(a.Np, s);
+                // 64 vectors x 4 chunks of 4 K; item w -> vector w/4, chunk w%4, so a
+                // warp reads 1 KB and writes 512 B contiguous (no bank conflicts)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int w = ct + 64 * q;
+                    const int v = w >> 2, kc = (w & 3) * 4;
+                    const bool ok = n0 + v < a.ncols && kc < kl;
+                    const double2* p = reinterpret_cast<const double2*>(raw + v * kBK + kc);
+                    const double2 x0 = ok ? p[0] : make_double2(0.0, 0.0);
+                    const double2 x1 = ok ? p[1] : make_double2(0.0, 0.0);
+                    float4 h, l;
+                    split_tf32((float)x0.x, h.x, l.x);
+                    split_tf32((float)x0.y, h.y, l.y);
+                    split_tf32((float)x1.x, h.z, l.z);
+                    split_tf32((float)x1.y, h.w, l.w);
+                    *reinterpret_cast<float4*>(stg + kOffConvB + koff(v, kc)) = h;
+                    *reinterpret_cast<float4*>(stg + kOffConvB + kBHalf + koff(v, kc)) = l;
+                }
+                fence_async_smem();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&conv[st]);
+                PARODE_TC_TRACE(2);
+            }
+            if (!ok) break;
+        }
+    } else {
+        // ---------------- epilogue (warps 4-7: TMEM lane quarters 0-3) ----------------
+        const int quarter = warp & 3;
+        Cursor c;
+        c.init(args, start, nent, t0, t1);
+        long u = 0;
+        for (long t = t0; t < t1 && !*abort; ++t, ++u) {
+            const long lt = c.seek(t);
+            const LevelArgs& a = c.a;
+            int mi, m0, nk;
+            long n0;
+            tile_coords(a, lt, mi, m0, n0, nk);
+            const int ab = (int)(u & 1);
+            if (!role_wait(&acc_full[ab], (uint32_t)((u >> 1) & 1), abort, status)) break;
+            PARODE_TC_TRACE(3);
+            fence_after_sync();
+            const long i = m0 + 32 * quarter + lane;
+            const int rc = i < a.Np ? r_col(a, (int)i) : -1;
+            // loop-invariant fields in registers
+            const double* srow = a.src + (rc >= 0 ? rc : 0);
+            const long sgs = a.src_gs;
+            const double* arow = a.acc ? a.acc + i * a.acc_is : nullptr;
+            const long ags = a.acc_gs;
+            double* drow = a.dst + i * a.dst_is;
+            const long dgs = a.dst_gs;
+            const int nvt = (int)std::min<long>(kBN, a.ncols - n0);
+            const bool live = i < a.Np;
+#pragma unroll 1
+            for (int h = 0; h < 2; ++h) {
+                uint32_t r[32];
+                tmem_ld32(tbase + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(ab * kBN + h * 32), r);
+                tmem_wait_ld();
+                if (live) {
+                    // 16 columns at a time: all loads in flight before the sums
+#pragma unroll 1
+                    for (int c0 = 0; c0 < 32; c0 += 16) {
+                        double xa[16], xs[16];
+                        const int jb = 32 * h + c0;
+#pragma unroll
+                        for (int jj = 0; jj < 16; ++jj) {
+                            const bool ok = jb + jj < nvt;
+                            const long g = n0 + jb + jj;
+                            xs[jj] = (ok && rc >= 0) ? srow[g * sgs] : 0.0;  // R v, exact
+                            xa[jj] = (ok && arow) ? arow[g * ags] : 0.0;
+                        }
+#pragma unroll
+                        for (int jj = 0; jj < 16; ++jj)
+                            if (jb + jj < nvt)
+                                drow[(n0 + jb + jj) * dgs] = ((double)__uint_as_float(r[c0 + jj]) + xs[jj]) + xa[jj];
+                    }
+                }
+            }
+            fence_before_sync();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acc_empty[ab]);
+            PARODE_TC_TRACE(4);
+        }
+    }
+
+    // all roles done (or aborted); bulk copies of an aborted producer are
+    // drained by waiting on their stages (bounded) before the CTA exits
+    __syncthreads();
+    if (*abort && threadIdx.x == 0) {
+        for (int q = 0; q < kS; ++q) mbar_wait(&full[q], 0, 1 << 20);
     }
     fence_after_sync();
-    if ((threadIdx.x >> 5) == 0) tmem_dealloc(tbase, kTmemCols);
+    if (warp == 0) tmem_dealloc(tbase, kTmemCols);
 }
 
 }  // namespace
@@ -313,6 +487,29 @@ void launch_level_tc(const LevelArgs* dArgs, const long* dStart, int nent, const
     PARODE_CUDA(cudaGetLastError());
 }
 
+void level_encode_src_map(const LevelArgs& a, void* out)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        PARODE_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        if (!fn || q != cudaDriverEntryPointSuccess) throw Error(kDeviceError, "cuTensorMapEncodeTiled unavailable");
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    if ((reinterpret_cast<uintptr_t>(a.src) & 15) || ((a.src_gs * 8) & 15))
+        throw Error(kInvalidArgument, "source map: 16-byte alignment");
+    CUtensorMap* m = static_cast<CUtensorMap*>(out);
+    const cuuint64_t dims[2] = {(cuuint64_t)a.Np, (cuuint64_t)a.ncols};
+    const cuuint64_t strides[1] = {(cuuint64_t)a.src_gs * 8};
+    const cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)kBN};
+    const cuuint32_t estr[2] = {1, 1};
+    CUresult r = encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(a.src), dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw Error(kDeviceError, "cuTensorMapEncodeTiled failed");
+}
+
 // Host: tile ranges of `ctas` CTAs with about equal work (a tile costs its
 // K slices plus a fixed overhead).
 std::vector<long> level_tc_ranges(const std::vector<LevelArgs>& ents, int ctas)
@@ -321,7 +518,7 @@ std::vector<long> level_tc_ranges(const std::vector<LevelArgs>& ents, int ctas)
     double total = 0;
     for (const LevelArgs& a : ents) {
         const long n = level_tc_tiles(a);
-        const double c = (a.Np + kBK - 1) / kBK + 4.0;
+        const double c = (a.Np + kBK - 1) / kBK + 2.0;
         for (long t = 0; t < n; ++t) cost.push_back(c);
         total += c * n;
     }
