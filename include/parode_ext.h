@@ -127,6 +127,31 @@ void ParODE_SimulateODEBatch(int nSystems, const double* const A[], const double
                              const double* const x0[], const int solver[], int precision, double* const tVect[],
                              double* const yVect[], long long nSteps[], int nErr[]);
 
+/* ---- serving loop: asynchronous solves with continuous batching ---------
+ * A scheduler thread admits submitted solves against an HBM budget (bytes;
+ * <= 0: 150e9), batches whatever is pending (at most maxBatch systems per
+ * batch, maxInflight batches on the device at once) as soon as memory and a
+ * slot free up, runs each batch on its own stream so batches overlap, and
+ * copies results to host memory.  No counterpart in the reference.
+ * ServerSubmit returns a request id (> 0) or a negative error code; a request
+ * larger than the whole budget fails with -4.  ServerPoll returns 1 when the
+ * request is finished (its output count and channels filled in).
+ * ServerResult copies tVect / yVect (NumOutputs x channels) and the latency
+ * (submission to completion, ms) and releases the request.
+ * ServerStats fills stats[12]: submitted, completed, failed, p50 ms, p99 ms,
+ * mean ms, max ms, state*steps completed, span s (first submission to last
+ * completion), peak in-flight bytes, batches, 0. */
+typedef struct ParODE_Server ParODE_Server;
+ParODE_Server* ParODE_ServerCreate(int precision, double hbmBudgetBytes, int maxBatch, int maxInflight, int nErr[]);
+long long ParODE_ServerSubmit(ParODE_Server* srv, const double* A, const double* B, const double* C, const double* D,
+                              int nInputs, int nStates, int nOutputs, int ZeroB, int ZeroC, int ZeroD, int uIndex,
+                              double tStart, double tEnd, double tStep, const double* x0, int solver, int nErr[]);
+int ParODE_ServerPoll(ParODE_Server* srv, long long id, long long nSteps[], int nChannels[], int nErr[]);
+void ParODE_ServerResult(ParODE_Server* srv, long long id, double* tVect, double* yVect, double latencyMs[],
+                         int nErr[]);
+void ParODE_ServerStats(ParODE_Server* srv, double stats[], int nErr[]);
+void ParODE_ServerDestroy(ParODE_Server* srv);
+
 /* Affine scan on device data with no allocation (no counterpart in the
  * reference).  With all pointers in device memory of the current device:
  *   dX[k] = x_k for k < count, x_0 = dX0, x_{k+1} = Phi x_k + dGamma[k],

@@ -114,6 +114,16 @@ def _load():
     L.ParODE_BatchStateSteps.argtypes = [C.c_void_p]
     L.ParODE_BatchStateSteps.restype = C.c_double
     L.ParODE_BatchDestroy.argtypes = [C.c_void_p]
+    L.ParODE_ServerCreate.argtypes = [C.c_int, C.c_double, C.c_int, C.c_int, ip]
+    L.ParODE_ServerCreate.restype = C.c_void_p
+    L.ParODE_ServerSubmit.argtypes = [C.c_void_p, dp, dp, dp, dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                      C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, dp, C.c_int, ip]
+    L.ParODE_ServerSubmit.restype = C.c_longlong
+    L.ParODE_ServerPoll.argtypes = [C.c_void_p, C.c_longlong, C.POINTER(C.c_longlong), ip, ip]
+    L.ParODE_ServerPoll.restype = C.c_int
+    L.ParODE_ServerResult.argtypes = [C.c_void_p, C.c_longlong, dp, dp, dp, ip]
+    L.ParODE_ServerStats.argtypes = [C.c_void_p, dp, ip]
+    L.ParODE_ServerDestroy.argtypes = [C.c_void_p]
     return L
 
 
@@ -394,6 +404,81 @@ class Batch:
     def close(self) -> None:
         if getattr(self, "_h", None):
             lib.ParODE_BatchDestroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Asynchronous solves with continuous batching (ParODE_Server*).
+
+    submit() queues a solve and returns its id; poll(id) tells whether it is
+    finished; result(id) returns (t, y, latency_ms) and releases it."""
+
+    STAT_KEYS = ("submitted", "completed", "failed", "p50_ms", "p99_ms", "mean_ms", "max_ms", "state_steps",
+                 "span_s", "peak_bytes", "batches")
+
+    def __init__(self, precision: int = FP64, hbm_budget_bytes: float = 150e9, max_batch: int = 256,
+                 max_inflight: int = 8):
+        e = C.c_int(0)
+        self._h = lib.ParODE_ServerCreate(precision, float(hbm_budget_bytes), max_batch, max_inflight, C.byref(e))
+        _check(e, "ParODE_ServerCreate")
+        self._shape = {}
+
+    def submit(self, A, B, Cm, D, x0, u_index: int, t0: float, t_end: float, h: float, solver: int = RK4) -> int:
+        A, B, Cm, D, x0, n, m, p = _sys_arrays(A, B, Cm, D, x0)
+        e = C.c_int(0)
+        rid = lib.ParODE_ServerSubmit(self._h, _dp(A), _dp(B), _dp(Cm), _dp(D), m, n, p, int(B is None),
+                                      int(Cm is None), int(D is None), u_index, t0, t_end, h, _dp(x0), solver,
+                                      C.byref(e))
+        _check(e, "ParODE_ServerSubmit")
+        return int(rid)
+
+    def poll(self, rid: int) -> bool:
+        n = C.c_longlong(0)
+        c = C.c_int(0)
+        e = C.c_int(0)
+        done = lib.ParODE_ServerPoll(self._h, rid, C.byref(n), C.byref(c), C.byref(e))
+        _check(e, "ParODE_ServerPoll")
+        if done:
+            self._shape[rid] = (int(n.value), int(c.value))
+        return bool(done)
+
+    def result(self, rid: int):
+        if rid not in self._shape and not self.poll(rid):
+            raise ParODEError(-9, "ParODE_ServerResult: request not finished")
+        T, p = self._shape.pop(rid)
+        t = np.zeros(T)
+        y = np.zeros((T, p))
+        lat = C.c_double(0)
+        e = C.c_int(0)
+        lib.ParODE_ServerResult(self._h, rid, _dp(t), _dp(y), C.byref(lat), C.byref(e))
+        _check(e, "ParODE_ServerResult")
+        return t, y, float(lat.value)
+
+    def wait(self, rid: int, timeout_s: float = 600.0, interval_s: float = 0.0005):
+        import time as _time
+        t_end = _time.monotonic() + timeout_s
+        while not self.poll(rid):
+            if _time.monotonic() > t_end:
+                raise TimeoutError(f"request {rid} not finished after {timeout_s} s")
+            _time.sleep(interval_s)
+        return self.result(rid)
+
+    def stats(self) -> dict:
+        v = (C.c_double * 12)()
+        e = C.c_int(0)
+        lib.ParODE_ServerStats(self._h, v, C.byref(e))
+        _check(e, "ParODE_ServerStats")
+        return {k: float(v[i]) for i, k in enumerate(self.STAT_KEYS)}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib.ParODE_ServerDestroy(self._h)
             self._h = None
 
     def __del__(self):

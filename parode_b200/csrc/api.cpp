@@ -11,6 +11,7 @@
 #include "inputs.h"
 #include "solver.h"
 #include "batch.h"
+#include "server.h"
 
 #include "FTypeDef.h"
 #include "ParODECInterface.h"
@@ -622,6 +623,97 @@ double ParODE_BatchStateSteps(const ParODE_Batch* batch)
 }
 
 void ParODE_BatchDestroy(ParODE_Batch* batch) { delete batch; }
+
+// ---- serving loop -------------------------------------------------------------
+
+struct ParODE_Server {
+    std::unique_ptr<Server> server;
+};
+
+ParODE_Server* ParODE_ServerCreate(int precision, double hbmBudgetBytes, int maxBatch, int maxInflight, int nErr[])
+{
+    Library& L = lib();
+    std::lock_guard<std::recursive_mutex> g(L.mu);
+    ParODE_Server* out = nullptr;
+    int rc = guarded([&] {
+        int dev = current_device_locked(L);
+        if (precision != PARODE_PRECISION_FP64 && precision != PARODE_PRECISION_MIXED)
+            throw Error(kInvalidArgument, "unknown precision");
+        ServerOptions o;
+        o.precision = precision;
+        if (hbmBudgetBytes > 0) o.hbm_budget = hbmBudgetBytes;
+        if (maxBatch > 0) o.max_batch = maxBatch;
+        if (maxInflight > 0) o.max_inflight = maxInflight;
+        auto h = std::make_unique<ParODE_Server>();
+        h->server = std::make_unique<Server>(dev, &L.inputs, &L.mu, o);
+        out = h.release();
+    });
+    if (nErr) nErr[0] = rc;
+    return out;
+}
+
+long long ParODE_ServerSubmit(ParODE_Server* srv, const double* A, const double* B, const double* C, const double* D,
+                              int nInputs, int nStates, int nOutputs, int ZeroB, int ZeroC, int ZeroD, int uIndex,
+                              double tStart, double tEnd, double tStep, const double* x0, int solver, int nErr[])
+{
+    long long id = 0;
+    int rc = guarded([&] {
+        if (!srv || !srv->server) throw Error(kInvalidArgument, "null server");
+        BatchSpec s;
+        s.sys = make_system<double>(A, B, C, D, nInputs, nStates, nOutputs, ZeroB, ZeroC, ZeroD, x0);
+        if (solver != kRK4 && solver != kABM) throw Error(kInvalidSolverType, "unknown solver type");
+        s.uIndex = uIndex;
+        s.solver = solver;
+        s.t0 = tStart;
+        s.tEnd = tEnd;
+        s.h = tStep;
+        id = srv->server->submit(std::move(s));
+    });
+    if (nErr) nErr[0] = rc;
+    return rc == kOK ? id : rc;
+}
+
+int ParODE_ServerPoll(ParODE_Server* srv, long long id, long long nSteps[], int nChannels[], int nErr[])
+{
+    int done = 0;
+    int rc = guarded([&] {
+        if (!srv || !srv->server) throw Error(kInvalidArgument, "null server");
+        int err = 0;
+        long long n = 0;
+        int c = 0;
+        done = srv->server->poll(id, &n, &c, &err);
+        if (nSteps) nSteps[0] = n;
+        if (nChannels) nChannels[0] = c;
+        if (done && err) throw Error(err, "the request failed");
+    });
+    if (nErr) nErr[0] = rc;
+    return done;
+}
+
+void ParODE_ServerResult(ParODE_Server* srv, long long id, double* tVect, double* yVect, double latencyMs[],
+                         int nErr[])
+{
+    int rc = guarded([&] {
+        if (!srv || !srv->server) throw Error(kInvalidArgument, "null server");
+        srv->server->result(id, tVect, yVect, latencyMs);
+    });
+    if (nErr) nErr[0] = rc;
+}
+
+void ParODE_ServerStats(ParODE_Server* srv, double stats[], int nErr[])
+{
+    int rc = guarded([&] {
+        if (!srv || !srv->server) throw Error(kInvalidArgument, "null server");
+        if (!stats) return;
+        ServerStats s = srv->server->stats();
+        const double v[12] = {(double)s.submitted, (double)s.completed, (double)s.failed, s.p50_ms, s.p99_ms,
+                              s.mean_ms, s.max_ms, s.state_steps, s.span_s, s.peak_bytes, (double)s.batches, 0.0};
+        for (int k = 0; k < 12; ++k) stats[k] = v[k];
+    });
+    if (nErr) nErr[0] = rc;
+}
+
+void ParODE_ServerDestroy(ParODE_Server* srv) { delete srv; }
 
 void ParODE_SimulateODEBatch(int nSystems, const double* const A[], const double* const B[], const double* const C[],
                              const double* const D[], const int nInputs[], const int nStates[], const int nOutputs[],

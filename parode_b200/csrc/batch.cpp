@@ -364,7 +364,10 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
     }
     arena_bytes_ = align_up(work_end + job_bytes);
     {
-        cudaError_t e = cudaMalloc(&arena_, arena_bytes_);
+        // stream-ordered: creating or destroying a batch does not synchronise
+        // the device, so batches can come and go while others run
+        PARODE_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+        cudaError_t e = cudaMallocAsync(&arena_, arena_bytes_, stream_);
         if (e != cudaSuccess) {
             cudaGetLastError();
             arena_ = nullptr;
@@ -743,7 +746,6 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
     if (J.bytes > arena_bytes_) throw Error(kDeviceError, "batch job arrays overflow the arena reservation");
 
     // ---- upload and set-up launches ------------------------------------------
-    PARODE_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     PARODE_CUDA(cudaMemcpyAsync(base, st.buf.data(), st.buf.size(), cudaMemcpyHostToDevice, stream_));
     PARODE_CUDA(cudaMemcpyAsync(base + work_end, jstage.data(), jstage.size(), cudaMemcpyHostToDevice, stream_));
     for (size_t k = 0; k < setup_copies.size(); k += 65535)
@@ -767,7 +769,7 @@ BatchPlan::~BatchPlan()
         }
     for (auto e : events_)
         if (e) cudaEventDestroy(e);
-    if (arena_) cudaFree(arena_);
+    if (arena_) cudaFreeAsync(arena_, stream_ ? stream_ : cudaStreamPerThread);
     if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -782,6 +784,7 @@ void BatchPlan::execute(cudaStream_t s)
 {
     PARODE_CUDA(cudaSetDevice(device_));
     if (!s) s = stream_;
+    last_stream_ = s;
     int launches = 0;
     // inputs for everything first
     if (nSampleJobs_ > 0) {
@@ -856,12 +859,16 @@ void BatchPlan::get_output(int i, double* t, double* y)
     if (i < 0 || i >= size()) throw Error(kInvalidArgument, "system index out of range");
     const Sys& q = sys_[i];
     PARODE_CUDA(cudaSetDevice(device_));
+    // the last execute's stream (joined from the batch's fork streams) and
+    // the batch stream; no device-wide synchronisation, other batches run on
+    PARODE_CUDA(cudaStreamSynchronize(last_stream_ ? last_stream_ : stream_));
     PARODE_CUDA(cudaStreamSynchronize(stream_));
-    PARODE_CUDA(cudaDeviceSynchronize());
     int st = 0;
-    PARODE_CUDA(cudaMemcpy(&st, dStatus_, sizeof(int), cudaMemcpyDeviceToHost));
+    PARODE_CUDA(cudaMemcpyAsync(&st, dStatus_, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+    if (y)
+        PARODE_CUDA(cudaMemcpyAsync(y, q.Y, sizeof(double) * (size_t)q.nOut * q.p, cudaMemcpyDeviceToHost, stream_));
+    PARODE_CUDA(cudaStreamSynchronize(stream_));
     if (st != 0) throw Error(kDeviceError, "a tensor-core wait gave up (the result is incomplete)");
-    if (y) PARODE_CUDA(cudaMemcpy(y, q.Y, sizeof(double) * (size_t)q.nOut * q.p, cudaMemcpyDeviceToHost));
     if (t) time_vector(q.solver, q.t0, q.tEnd, q.h, t);
 }
 

@@ -105,6 +105,7 @@ private:
     int device_ = 0;
     int sms_ = 148;
     int* dStatus_ = nullptr;  // set by a device wait that gave up
+    cudaStream_t last_stream_ = nullptr;
     cudaStream_t stream_ = nullptr;
     std::vector<cudaStream_t> forks_;
     std::vector<cudaEvent_t> events_;

@@ -1,0 +1,268 @@
+// server.cpp -- continuous-batching request loop (see server.h).
+#include "server.h"
+
+#include "blocked.h"
+#include "common.h"
+#include "kernels.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+
+namespace parode {
+
+namespace {
+
+double now_s()
+{
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+double percentile(std::vector<double> v, double q)
+{
+    if (v.empty()) return 0.0;
+    std::sort(v.begin(), v.end());
+    const double pos = q * (double)(v.size() - 1);
+    const size_t i = (size_t)pos;
+    const double f = pos - (double)i;
+    return i + 1 < v.size() ? v[i] * (1 - f) + v[i + 1] * f : v[i];
+}
+
+}  // namespace
+
+size_t estimate_request_bytes(const BatchSpec& b, int precision)
+{
+    const SystemDesc& s = b.sys;
+    long nScan = 0;
+    const long nOut = num_outputs(b.solver, b.t0, b.tEnd, b.h, &nScan);
+    if (nOut <= 0 || nScan <= 0 || s.n <= 0) return 0;
+    const int Ns = b.solver == kRK4 ? s.n : 4 * s.n;
+    const int p = s.out_size();
+    const int mu = (!s.zeroB || !s.zeroD) ? s.m : 0;
+    const int W = b.solver == kRK4 ? 3 : 5;
+    const long nU = b.solver == kRK4 ? 2 * nScan + 1 : nScan + 4;
+    double bytes = 8.0 * ((double)nU * mu + (double)nOut * p);              // inputs, outputs
+    bytes += 8.0 * ((double)s.n * W * std::max(mu, 1) + 2.0 * p * (s.n + s.m) + 4.0 * Ns);  // constants
+    BlockedShape sh;
+    if (blocked_shape(Ns, std::max(mu, 1), 0, &sh)) {
+        const double NP = sh.NP;
+        bytes += 8.0 * NP * NP * (sh.R + 2);                                  // power table + Phi
+        bytes += 8.0 * ((double)(nScan + sh.S) / sh.B + 1) * NP;              // block aggregates
+        bytes += 8.0 * sh.B * p * NP + 8.0 * p * NP;                          // output tables
+    } else {
+        const double Np = (double)round_up(Ns, 8);
+        const long Tp = next_pow2(nScan);
+        const int levels = std::max(ilog2(Tp), 1);
+        bytes += 8.0 * (double)(Tp + 1) * Np;                                 // scan vectors
+        bytes += 8.0 * Np * Np * (levels + 1);                                // power table + Phi
+        if (precision == kMixed) bytes += (double)level_split_bytes((int)Np) * levels;
+        bytes += 8.0 * (double)levels * 1024;                                 // launch descriptors
+    }
+    return (size_t)(bytes * 1.05) + (1u << 20);
+}
+
+Server::Server(int device, InputRegistry* inputs, std::recursive_mutex* inputs_mu, const ServerOptions& opt)
+    : device_(device), inputs_(inputs), inputs_mu_(inputs_mu), opt_(opt)
+{
+    if (opt_.max_batch < 1 || opt_.max_inflight < 1 || !(opt_.hbm_budget > 0))
+        throw Error(kInvalidArgument, "server options");
+    thread_ = std::thread([this] { loop(); });
+}
+
+Server::~Server()
+{
+    {
+        std::lock_guard<std::mutex> g(mu_);
+        stop_ = true;
+        // requests not yet admitted are dropped
+        for (auto& r : pending_) {
+            r->done = true;
+            r->err = kInvalidArgument;
+        }
+        pending_.clear();
+    }
+    cv_.notify_all();
+    if (thread_.joinable()) thread_.join();
+}
+
+long long Server::submit(BatchSpec spec)
+{
+    auto r = std::make_shared<Request>();
+    r->bytes = estimate_request_bytes(spec, opt_.precision);
+    if (r->bytes == 0) throw Error(kInvalidSystem, "empty time horizon or no states");
+    if ((double)r->bytes > opt_.hbm_budget) throw Error(kNotEnoughResources, "request larger than the HBM budget");
+    long nScan = 0;
+    r->n_out = num_outputs(spec.solver, spec.t0, spec.tEnd, spec.h, &nScan);
+    r->channels = spec.sys.out_size();
+    r->state_steps = (double)spec.sys.n * (double)r->n_out;
+    r->spec = std::move(spec);
+    r->t_submit = now_s();
+    {
+        std::lock_guard<std::mutex> g(mu_);
+        if (stop_) throw Error(kInvalidArgument, "server stopped");
+        r->id = next_id_++;
+        all_[r->id] = r;
+        pending_.push_back(r);
+        ++st_.submitted;
+        if (t_first_ < 0) t_first_ = r->t_submit;
+    }
+    cv_.notify_all();
+    return r->id;
+}
+
+int Server::poll(long long id, long long* n_out, int* channels, int* err)
+{
+    std::lock_guard<std::mutex> g(mu_);
+    auto it = all_.find(id);
+    if (it == all_.end()) throw Error(kInvalidArgument, "unknown request id");
+    const Request& r = *it->second;
+    if (n_out) *n_out = r.n_out;
+    if (channels) *channels = r.channels;
+    if (err) *err = r.err;
+    return r.done ? 1 : 0;
+}
+
+void Server::result(long long id, double* t, double* y, double* latency_ms)
+{
+    std::shared_ptr<Request> r;
+    {
+        std::lock_guard<std::mutex> g(mu_);
+        auto it = all_.find(id);
+        if (it == all_.end()) throw Error(kInvalidArgument, "unknown request id");
+        r = it->second;
+        if (!r->done) throw Error(kInvalidArgument, "request not finished");
+        all_.erase(it);
+    }
+    if (r->err != 0) throw Error(r->err, "the request failed");
+    if (y) std::copy(r->y.begin(), r->y.end(), y);
+    if (t) time_vector(r->spec.solver, r->spec.t0, r->spec.tEnd, r->spec.h, t);
+    if (latency_ms) *latency_ms = (r->t_done - r->t_submit) * 1e3;
+}
+
+ServerStats Server::stats()
+{
+    std::lock_guard<std::mutex> g(mu_);
+    ServerStats s = st_;
+    s.p50_ms = percentile(latencies_, 0.50);
+    s.p99_ms = percentile(latencies_, 0.99);
+    s.max_ms = latencies_.empty() ? 0.0 : *std::max_element(latencies_.begin(), latencies_.end());
+    double sum = 0;
+    for (double v : latencies_) sum += v;
+    s.mean_ms = latencies_.empty() ? 0.0 : sum / (double)latencies_.size();
+    s.span_s = t_first_ >= 0 ? t_last_ - t_first_ : 0.0;
+    return s;
+}
+
+// Scheduler thread: retire, admit, wait for news.
+void Server::loop()
+{
+    cudaSetDevice(device_);
+    std::unique_lock<std::mutex> lk(mu_);
+    for (;;) {
+        for (size_t k = 0; k < inflight_.size();) {
+            if (cudaEventQuery(inflight_[k].done) == cudaErrorNotReady) {
+                ++k;
+                continue;
+            }
+            Inflight f = std::move(inflight_[k]);
+            inflight_.erase(inflight_.begin() + (long)k);
+            lk.unlock();
+            retire(f);
+            lk.lock();
+            inflight_bytes_ -= f.bytes;
+            for (auto& r : f.reqs) {
+                r->done = true;
+                if (r->err == 0) {
+                    latencies_.push_back((r->t_done - r->t_submit) * 1e3);
+                    ++st_.completed;
+                    st_.state_steps += r->state_steps;
+                } else {
+                    ++st_.failed;
+                }
+                t_last_ = std::max(t_last_, r->t_done);
+            }
+        }
+        if (stop_ && pending_.empty() && inflight_.empty()) break;
+        admit_locked(lk);
+        cv_.wait_for(lk, std::chrono::microseconds(inflight_.empty() ? 2000 : 50));
+    }
+}
+
+// Forms batches from the pending requests while the budget and the in-flight
+// limit allow (first come, first served; a request that does not fit waits).
+void Server::admit_locked(std::unique_lock<std::mutex>& lk)
+{
+    while (!pending_.empty() && (int)inflight_.size() < opt_.max_inflight) {
+        std::vector<std::shared_ptr<Request>> take;
+        size_t bytes = 0;
+        while (!pending_.empty() && (int)take.size() < opt_.max_batch) {
+            const auto& r = pending_.front();
+            if ((double)(inflight_bytes_ + bytes + r->bytes) > opt_.hbm_budget) break;
+            bytes += r->bytes;
+            take.push_back(r);
+            pending_.pop_front();
+        }
+        if (take.empty()) break;  // waits for memory to free up
+        inflight_bytes_ += bytes;
+        st_.peak_bytes = std::max(st_.peak_bytes, (double)inflight_bytes_);
+        ++st_.batches;
+        lk.unlock();
+        Inflight f;
+        f.reqs = take;
+        f.bytes = bytes;
+        try {
+            std::vector<BatchSpec> specs;
+            specs.reserve(take.size());
+            for (auto& r : take) specs.push_back(r->spec);
+            PlanOptions po;
+            po.precision = opt_.precision;
+            po.input_double = true;
+            {
+                std::lock_guard<std::recursive_mutex> g(*inputs_mu_);  // the input registry is shared
+                f.plan = std::make_unique<BatchPlan>(device_, std::move(specs), inputs_, po);
+            }
+            f.plan->execute(nullptr);
+            PARODE_CUDA(cudaEventCreateWithFlags(&f.done, cudaEventDisableTiming));
+            PARODE_CUDA(cudaEventRecord(f.done, f.plan->stream()));
+        } catch (const Error& e) {
+            for (auto& r : take) r->err = e.code;
+            f.plan.reset();
+        } catch (...) {
+            for (auto& r : take) r->err = kDeviceError;
+            f.plan.reset();
+        }
+        lk.lock();
+        if (!f.plan) {
+            // failed set-up: finish the requests right away
+            inflight_bytes_ -= f.bytes;
+            const double t = now_s();
+            for (auto& r : f.reqs) {
+                r->done = true;
+                r->t_done = t;
+                ++st_.failed;
+            }
+            continue;
+        }
+        inflight_.push_back(std::move(f));
+    }
+}
+
+// Copies every request's outputs to host memory and frees the batch.
+void Server::retire(Inflight& f)
+{
+    for (size_t i = 0; i < f.reqs.size(); ++i) {
+        auto& r = f.reqs[i];
+        try {
+            r->y.resize((size_t)f.plan->num_outputs((int)i) * f.plan->channels((int)i));
+            f.plan->get_output((int)i, nullptr, r->y.data());
+        } catch (const Error& e) {
+            r->err = e.code;
+        }
+        r->t_done = now_s();
+    }
+    if (f.done) cudaEventDestroy(f.done);
+    f.plan.reset();
+}
+
+}  // namespace parode

@@ -159,6 +159,28 @@ def cfg4(count: int = 4096, seed: int = 1238) -> List[Case]:
     return cases
 
 
+def cfg5(count: int, rate: float, seed: int = 1239, n_range=(8, 256), T_range=(1e3, 1e6)):
+    """Serving workload: `count` requests with Poisson arrivals at `rate` per
+    second; n and T log-uniform in the given ranges, RK4 / ABM 50/50,
+    m = p = max(1, n/8), A = -(1+U(0,1)) I + 0.5 G/sqrt(n), h = 1e-3.
+    Returns [(arrival_s, Case)]."""
+    rng = Rng(seed)
+    out = []
+    t = 0.0
+    for i in range(count):
+        t += -math.log(max(1e-300, 1.0 - float(rng.uniform(1)[0]))) / rate
+        n = int(round(math.exp(math.log(n_range[0]) + (math.log(n_range[1]) - math.log(n_range[0])) *
+                               float(rng.uniform(1)[0]))))
+        T = int(round(math.exp(math.log(T_range[0]) + (math.log(T_range[1]) - math.log(T_range[0])) *
+                               float(rng.uniform(1)[0]))))
+        T = max(T, 5)
+        m = p = max(1, n // 8)
+        solver = 0 if float(rng.uniform(1)[0]) < 0.5 else 1
+        diag = -(1.0 + float(rng.uniform(1)[0]))
+        out.append((t, lti(rng, f"cfg5[{i}]", solver, n, m, p, diag, 0.5, 1e-3, T)))
+    return out
+
+
 def small(seed: int, solver: int, n: int, m: int, p: int, T: int, h: float = 1e-2, diag: float = -1.0,
           scale: float = 0.5) -> Case:
     """A small random stable case for parity sweeps."""
