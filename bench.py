@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--min-warmup-s", type=float, default=0.5, help="least warm-up time under load (clock sampling)")
+    ap.add_argument("--no-extra", action="store_true", help="skip the batched (4096 systems) and serving runs")
+    ap.add_argument("--serve-requests", type=int, default=64)
     return ap.parse_args()
 
 
@@ -210,6 +212,112 @@ def leaf_flops(case, T, B):
     return per_step * T
 
 
+def _spec(pb, c):
+    u = pb.register_sinusoid(c.u.a, c.u.f, c.u.phi)
+    return {"A": c.A, "B": c.B, "C": c.C, "D": c.D, "x0": c.x0, "u": u, "t0": c.t0, "t_end": c.t_end, "h": c.h,
+            "solver": c.solver}
+
+
+def _cheap_sample(cases, k):
+    """k systems the oracle checks quickly: the cheapest half from the scan
+    dimensions <= 64 (blocked path) and half from the larger ones (level-
+    synchronous path, where the mixed form runs its tensor-core levels)."""
+    cost = lambda i: cases[i].scan_dim ** 2 * cases[i].T
+    small = sorted((i for i in range(len(cases)) if cases[i].scan_dim <= 64), key=cost)
+    large = sorted((i for i in range(len(cases)) if cases[i].scan_dim > 64), key=cost)
+    return small[: k // 2] + large[: k - k // 2]
+
+
+def measure_batched(pb, wl, torch, dev, reps=3):
+    """The batched form: 4096 independent systems (cfg4) in one batch, FP64 and mixed."""
+    from oracle import oracle
+
+    cases = wl.cfg4()
+    specs = [_spec(pb, c) for c in cases]
+    check = _cheap_sample(cases, 8)
+    out = {"workload": "cfg4: 4096 systems, n log-uniform [4,96], T log-uniform [2^10,2^16], RK4/ABM 50/50",
+           "state_steps": None}
+    stream = torch.cuda.Stream(device=dev)
+    for name, prec in (("fp64", pb.FP64), ("mixed", pb.MIXED)):
+        t0 = time.perf_counter()
+        b = pb.Batch(specs, precision=prec)
+        setup_s = time.perf_counter() - t0
+        b.execute(stream.cuda_stream)
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            b.execute(stream.cuda_stream)
+            e.record(stream)
+            e.synchronize()
+            ts.append(s.elapsed_time(e))
+        ms = statistics.median(ts)
+        worst = 0.0
+        for i in check:
+            c = cases[i]
+            _, y = b.output(i)
+            ref = oracle.simulate_affine(oracle.System(c.A, c.B, c.C, c.D, c.x0),
+                                         oracle.Input.sinusoid(c.u.a, c.u.f, c.u.phi), c.solver, c.t0, c.t_end, c.h)
+            worst = max(worst, oracle.rel_err(y, ref))
+        out["state_steps"] = b.state_steps
+        out[name] = {"ms": ms, "value": b.state_steps / (ms / 1e3), "unit": UNIT, "launches": b.launch_count,
+                     "setup_s": setup_s, "rel_err_sampled": worst, "sampled_systems": len(check)}
+        b.close()
+    out["mixed_over_fp64"] = out["fp64"]["ms"] / out["mixed"]["ms"]
+    return out
+
+
+def measure_serving(pb, wl, torch, count=64, rates=(500.0, 2000.0, 8000.0)):
+    """The serving loop on cfg5-shaped requests (Poisson arrivals), mixed form,
+    beside one offline batch of the same requests."""
+    out = {"workload": f"cfg5: {count} requests per rate, n log-uniform [8,256], T log-uniform [1e3,1e6], "
+                       f"RK4/ABM 50/50, Poisson arrivals", "budget_bytes": 150e9, "precision": "mixed",
+           "rates": {}}
+    reqs_all = {}
+    for rate in rates:
+        reqs = wl.cfg5(count, rate)
+        reqs_all[rate] = reqs
+        server = pb.Server(precision=pb.MIXED, hbm_budget_bytes=150e9, max_batch=16, max_inflight=8)
+        specs = [(arr, c, _spec(pb, c)) for arr, c in reqs]
+        ids = []
+        t0 = time.monotonic()
+        for arr, c, s in specs:
+            d = t0 + arr - time.monotonic()
+            if d > 0:
+                time.sleep(d)
+            ids.append(server.submit(s["A"], s["B"], s["C"], s["D"], s["x0"], s["u"], s["t0"], s["t_end"], s["h"],
+                                     solver=s["solver"]))
+        for rid in ids:
+            server.wait(rid, timeout_s=600)
+        st = server.stats()
+        server.close()
+        out["rates"][str(int(rate))] = {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
+                                        "value": st["state_steps"] / st["span_s"] if st["span_s"] else None,
+                                        "unit": UNIT, "batches": int(st["batches"]),
+                                        "peak_gb": st["peak_bytes"] / 1e9, "span_s": st["span_s"]}
+    # offline: all requests of the middle rate in one batch (set-up excluded and included)
+    reqs = reqs_all[rates[len(rates) // 2]]
+    t0 = time.perf_counter()
+    b = pb.Batch([_spec(pb, c) for _, c in reqs], precision=pb.MIXED)
+    setup = time.perf_counter() - t0
+    stream = torch.cuda.Stream()
+    b.execute(stream.cuda_stream)
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record(stream)
+    b.execute(stream.cuda_stream)
+    e.record(stream)
+    e.synchronize()
+    ms = s.elapsed_time(e)
+    out["offline"] = {"value": b.state_steps / (ms / 1e3), "value_with_setup": b.state_steps / (ms / 1e3 + setup),
+                      "unit": UNIT, "ms": ms, "setup_s": setup}
+    b.close()
+    mid = out["rates"][str(int(rates[len(rates) // 2]))]
+    out["serving_over_offline"] = (mid["value"] / out["offline"]["value"]) if mid["value"] else None
+    return out
+
+
 def run_ours(args):
     import torch
 
@@ -313,6 +421,11 @@ def run_ours(args):
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "ms_per_step": float(e2e_t.item()),
                "call": "ParODE_SimulateODE_d (host arrays in, host y out)"}
 
+    batched = serving = None
+    if world == 1 and not args.no_extra:
+        batched = measure_batched(pb, wl, torch, dev)
+        serving = measure_serving(pb, wl, torch, count=args.serve_requests)
+
     if rank == 0:
         peaks, peaks_kind = measured_peaks()
         used_mixed = main["precision_used"] == pb.MIXED
@@ -366,6 +479,8 @@ def run_ours(args):
             "rel_err_mixed_vs_fp64": rel_vs_fp64,
             "peaks": {k: peaks.get(k) for k in ("hbm_gbs", "bf16_tflops", "bf16_tflops_sustained")},
             "peaks_source": peaks_kind,
+            "batched": batched,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -67,6 +67,15 @@ Server::Server(int device, InputRegistry* inputs, std::recursive_mutex* inputs_m
 {
     if (opt_.max_batch < 1 || opt_.max_inflight < 1 || !(opt_.hbm_budget > 0))
         throw Error(kInvalidArgument, "server options");
+    // batches allocate from the device's stream-ordered pool; keep freed
+    // memory in the pool (up to the budget) so that later batches reuse it
+    // instead of mapping fresh memory on the request path
+    {
+        cudaMemPool_t pool = nullptr;
+        PARODE_CUDA(cudaDeviceGetDefaultMemPool(&pool, device_));
+        uint64_t keep = (uint64_t)opt_.hbm_budget;
+        PARODE_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    }
     thread_ = std::thread([this] { loop(); });
 }
 
