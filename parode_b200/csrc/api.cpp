@@ -667,6 +667,14 @@ long long ParODE_ServerSubmit(ParODE_Server* srv, const double* A, const double*
         s.t0 = tStart;
         s.tEnd = tEnd;
         s.h = tStep;
+        if (!s.sys.zeroB || !s.sys.zeroD) {
+            // resolve the input now, under the library lock: the server's
+            // set-up threads then never touch the shared registry
+            Library& L = lib();
+            std::lock_guard<std::recursive_mutex> g(L.mu);
+            s.input = L.inputs.get(uIndex);
+            if (!s.input) throw Error(kInvalidInput, "uIndex does not name a registered input");
+        }
         id = srv->server->submit(std::move(s));
     });
     if (nErr) nErr[0] = rc;

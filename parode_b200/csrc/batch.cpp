@@ -114,7 +114,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         q.p = s.out_size();
         q.mu = (!s.zeroB || !s.zeroD) ? s.m : 0;
         if (q.mu > 0) {
-            q.input = inputs ? inputs->get(b.uIndex) : nullptr;
+            q.input = b.input ? b.input : (inputs ? inputs->get(b.uIndex) : nullptr);
             if (!q.input) throw Error(kInvalidInput, "uIndex does not name a registered input");
             if (q.input->kind == InputEntry::kSinusoid && q.input->m < q.mu)
                 throw Error(kInvalidInput, "the sinusoid input has fewer channels than the system's inputs");

@@ -31,6 +31,9 @@ struct BatchSpec {
     int uIndex = 0;
     int solver = 0;
     double t0 = 0, tEnd = 0, h = 0;
+    // the registered input, resolved by the caller under the library lock
+    // (nullptr: looked up from uIndex during set-up)
+    InputEntry* input = nullptr;
 };
 
 class BatchPlan {

@@ -480,12 +480,8 @@ void launch_level_t(const LevelArgs& a, int CW, cudaStream_t s)
     const int KS = level_ks(a.Np);
     const int NC = 8 * FC * CW;
     size_t smem = (size_t)(a.Np + NC) * (KS + 4) * sizeof(double);
-    static bool attr_set = false;
-    if (!attr_set) {
-        PARODE_CUDA(cudaFuncSetAttribute(k_affine_level<FR, FC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         200 * 1024));
-        attr_set = true;
-    }
+    // set on every launch: per device, and safe with several host threads
+    PARODE_CUDA(cudaFuncSetAttribute(k_affine_level<FR, FC>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     unsigned grid = blocks_for(a.ncols, NC);
     k_affine_level<FR, FC><<<grid, kThreads, smem, s>>>(a, CW, KS);
     PARODE_CUDA(cudaGetLastError());
@@ -506,14 +502,10 @@ void launch_affine_level(const LevelArgs& a, cudaStream_t s)
             k_swap<<<(unsigned)std::min<long>(blocks_for(a.ncols * (long)a.Np, 256), 4096), 256, 0, s>>>(a);
             PARODE_CUDA(cudaGetLastError());
         }
-        static bool attr_set = false;
-        if (!attr_set) {
-            PARODE_CUDA(cudaFuncSetAttribute(k_level_tiled<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)kTiledSmem));
-            PARODE_CUDA(cudaFuncSetAttribute(k_level_tiled<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)kTiledSmem));
-            attr_set = true;
-        }
+        PARODE_CUDA(cudaFuncSetAttribute(k_level_tiled<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kTiledSmem));
+        PARODE_CUDA(cudaFuncSetAttribute(k_level_tiled<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kTiledSmem));
         const long tiles = tiled_tiles(b);
         if (b.src_ks == 1) k_level_tiled<true><<<(unsigned)tiles, kThreads, kTiledSmem, s>>>(b);
         else k_level_tiled<false><<<(unsigned)tiles, kThreads, kTiledSmem, s>>>(b);
@@ -614,12 +606,8 @@ template <int FR, int FC>
 void grouped_t(const LevelConfig& c, const LevelArgs* args, const long* start, int nent, long tiles, size_t smem,
                cudaStream_t s)
 {
-    static bool attr_set = false;
-    if (!attr_set) {
-        PARODE_CUDA(cudaFuncSetAttribute(k_affine_level_grouped<FR, FC>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        attr_set = true;
-    }
+    PARODE_CUDA(cudaFuncSetAttribute(k_affine_level_grouped<FR, FC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     200 * 1024));
     k_affine_level_grouped<FR, FC><<<(unsigned)tiles, kThreads, smem, s>>>(args, start, nent, c.CW);
     PARODE_CUDA(cudaGetLastError());
 }
@@ -630,14 +618,10 @@ void launch_affine_level_grouped(const LevelConfig& c, const LevelArgs* dArgs, c
 {
     if (nent <= 0 || tiles <= 0) return;
     if (c.id >= 5) {
-        static bool attr_set = false;
-        if (!attr_set) {
-            PARODE_CUDA(cudaFuncSetAttribute(k_level_tiled_grouped<true>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTiledSmem));
-            PARODE_CUDA(cudaFuncSetAttribute(k_level_tiled_grouped<false>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTiledSmem));
-            attr_set = true;
-        }
+        PARODE_CUDA(cudaFuncSetAttribute(k_level_tiled_grouped<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kTiledSmem));
+        PARODE_CUDA(cudaFuncSetAttribute(k_level_tiled_grouped<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kTiledSmem));
         if (c.id == 5) k_level_tiled_grouped<true><<<(unsigned)tiles, kThreads, kTiledSmem, s>>>(dArgs, dStart, nent);
         else k_level_tiled_grouped<false><<<(unsigned)tiles, kThreads, kTiledSmem, s>>>(dArgs, dStart, nent);
         PARODE_CUDA(cudaGetLastError());

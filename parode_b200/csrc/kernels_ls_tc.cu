@@ -478,25 +478,24 @@ void launch_level_tc(const LevelArgs* dArgs, const long* dStart, int nent, const
                      cudaStream_t s)
 {
     if (nent <= 0 || ctas <= 0) return;
-    static bool attr_set = false;
-    if (!attr_set) {
-        PARODE_CUDA(cudaFuncSetAttribute(k_level_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));
-        attr_set = true;
-    }
+    // set on every launch: per device, and safe with several host threads
+    PARODE_CUDA(cudaFuncSetAttribute(k_level_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));
     k_level_tc<<<(unsigned)ctas, kThreads, kSmem, s>>>(dArgs, dStart, nent, dCta, status);
     PARODE_CUDA(cudaGetLastError());
 }
 
 void level_encode_src_map(const LevelArgs& a, void* out)
 {
-    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-    if (!encode) {
+    // resolved once (thread-safe static initialisation)
+    static const PFN_cuTensorMapEncodeTiled_v12000 encode = [] {
         void* fn = nullptr;
         cudaDriverEntryPointQueryResult q;
-        PARODE_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
-        if (!fn || q != cudaDriverEntryPointSuccess) throw Error(kDeviceError, "cuTensorMapEncodeTiled unavailable");
-        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
-    }
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            fn = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }();
+    if (!encode) throw Error(kDeviceError, "cuTensorMapEncodeTiled unavailable");
     if ((reinterpret_cast<uintptr_t>(a.src) & 15) || ((a.src_gs * 8) & 15))
         throw Error(kInvalidArgument, "source map: 16-byte alignment");
     CUtensorMap* m = static_cast<CUtensorMap*>(out);

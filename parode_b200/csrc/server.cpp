@@ -76,6 +76,7 @@ Server::Server(int device, InputRegistry* inputs, std::recursive_mutex* inputs_m
         uint64_t keep = (uint64_t)opt_.hbm_budget;
         PARODE_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
     }
+    for (int k = 0; k < std::max(1, opt_.setup_threads); ++k) workers_.emplace_back([this] { worker(); });
     thread_ = std::thread([this] { loop(); });
 }
 
@@ -92,7 +93,14 @@ Server::~Server()
         pending_.clear();
     }
     cv_.notify_all();
-    if (thread_.joinable()) thread_.join();
+    if (thread_.joinable()) thread_.join();  // returns once every admitted batch is retired
+    {
+        std::lock_guard<std::mutex> g(mu_);
+        workers_stop_ = true;
+    }
+    jobs_cv_.notify_all();
+    for (auto& w : workers_)
+        if (w.joinable()) w.join();
 }
 
 long long Server::submit(BatchSpec spec)
@@ -192,42 +200,70 @@ void Server::loop()
                 t_last_ = std::max(t_last_, r->t_done);
             }
         }
-        if (stop_ && pending_.empty() && inflight_.empty()) break;
-        admit_locked(lk);
-        cv_.wait_for(lk, std::chrono::microseconds(inflight_.empty() ? 2000 : 50));
+        if (stop_ && pending_.empty() && jobs_.empty() && setting_up_ == 0 && inflight_.empty()) break;
+        admit_locked();
+        cv_.wait_for(lk, std::chrono::microseconds(inflight_.empty() && setting_up_ == 0 ? 2000 : 50));
     }
 }
 
 // Forms batches from the pending requests while the budget and the in-flight
-// limit allow (first come, first served; a request that does not fit waits).
-void Server::admit_locked(std::unique_lock<std::mutex>& lk)
+// limit allow (first come, first served; a request that does not fit waits)
+// and hands them to the set-up workers.
+void Server::admit_locked()
 {
-    while (!pending_.empty() && (int)inflight_.size() < opt_.max_inflight) {
-        std::vector<std::shared_ptr<Request>> take;
-        size_t bytes = 0;
-        while (!pending_.empty() && (int)take.size() < opt_.max_batch) {
+    while (!pending_.empty() && (int)inflight_.size() + setting_up_ < opt_.max_inflight) {
+        Job j;
+        while (!pending_.empty() && (int)j.reqs.size() < opt_.max_batch) {
             const auto& r = pending_.front();
-            if ((double)(inflight_bytes_ + bytes + r->bytes) > opt_.hbm_budget) break;
-            bytes += r->bytes;
-            take.push_back(r);
+            if ((double)(inflight_bytes_ + j.bytes + r->bytes) > opt_.hbm_budget) break;
+            j.bytes += r->bytes;
+            j.reqs.push_back(r);
             pending_.pop_front();
         }
-        if (take.empty()) break;  // waits for memory to free up
-        inflight_bytes_ += bytes;
+        if (j.reqs.empty()) break;  // waits for memory to free up
+        inflight_bytes_ += j.bytes;
         st_.peak_bytes = std::max(st_.peak_bytes, (double)inflight_bytes_);
         ++st_.batches;
+        ++setting_up_;
+        jobs_.push_back(std::move(j));
+        jobs_cv_.notify_one();
+    }
+}
+
+// Set-up worker: builds an admitted batch (host discretisation, arena,
+// staged copy) and enqueues its solve on its own stream, concurrently with
+// the other workers and with batches already on the device.
+void Server::worker()
+{
+    cudaSetDevice(device_);
+    std::unique_lock<std::mutex> lk(mu_);
+    for (;;) {
+        jobs_cv_.wait(lk, [&] { return workers_stop_ || !jobs_.empty(); });
+        if (jobs_.empty()) {
+            if (workers_stop_) break;
+            continue;
+        }
+        Job j = std::move(jobs_.front());
+        jobs_.pop_front();
         lk.unlock();
         Inflight f;
-        f.reqs = take;
-        f.bytes = bytes;
+        f.reqs = j.reqs;
+        f.bytes = j.bytes;
         try {
             std::vector<BatchSpec> specs;
-            specs.reserve(take.size());
-            for (auto& r : take) specs.push_back(r->spec);
+            specs.reserve(j.reqs.size());
+            bool resolved = true;
+            for (auto& r : j.reqs) {
+                specs.push_back(r->spec);
+                const SystemDesc& s = r->spec.sys;
+                if ((!s.zeroB || !s.zeroD) && !r->spec.input) resolved = false;
+            }
             PlanOptions po;
             po.precision = opt_.precision;
             po.input_double = true;
-            {
+            if (resolved) {
+                f.plan = std::make_unique<BatchPlan>(device_, std::move(specs), inputs_, po);
+            } else {
                 std::lock_guard<std::recursive_mutex> g(*inputs_mu_);  // the input registry is shared
                 f.plan = std::make_unique<BatchPlan>(device_, std::move(specs), inputs_, po);
             }
@@ -235,13 +271,14 @@ void Server::admit_locked(std::unique_lock<std::mutex>& lk)
             PARODE_CUDA(cudaEventCreateWithFlags(&f.done, cudaEventDisableTiming));
             PARODE_CUDA(cudaEventRecord(f.done, f.plan->stream()));
         } catch (const Error& e) {
-            for (auto& r : take) r->err = e.code;
+            for (auto& r : j.reqs) r->err = e.code;
             f.plan.reset();
         } catch (...) {
-            for (auto& r : take) r->err = kDeviceError;
+            for (auto& r : j.reqs) r->err = kDeviceError;
             f.plan.reset();
         }
         lk.lock();
+        --setting_up_;
         if (!f.plan) {
             // failed set-up: finish the requests right away
             inflight_bytes_ -= f.bytes;
@@ -251,9 +288,10 @@ void Server::admit_locked(std::unique_lock<std::mutex>& lk)
                 r->t_done = t;
                 ++st_.failed;
             }
-            continue;
+        } else {
+            inflight_.push_back(std::move(f));
         }
-        inflight_.push_back(std::move(f));
+        cv_.notify_all();
     }
 }
 

@@ -31,7 +31,8 @@ struct ServerOptions {
     int precision = 0;
     double hbm_budget = 150e9;  // bytes of device memory for in-flight batches
     int max_batch = 256;        // systems per batch
-    int max_inflight = 8;       // batches on the device at once
+    int max_inflight = 8;       // batches on the device (or being set up) at once
+    int setup_threads = 4;      // host threads building batches concurrently
 };
 
 struct ServerStats {
@@ -84,8 +85,14 @@ private:
         size_t bytes = 0;
     };
 
+    struct Job {
+        std::vector<std::shared_ptr<Request>> reqs;
+        size_t bytes = 0;
+    };
+
     void loop();
-    void admit_locked(std::unique_lock<std::mutex>& lk);
+    void worker();
+    void admit_locked();
     void retire(Inflight& f);
 
     int device_;
@@ -103,6 +110,11 @@ private:
     std::vector<double> latencies_;
     ServerStats st_;
     double t_first_ = -1, t_last_ = 0;
+    std::deque<Job> jobs_;      // admitted batches waiting for a set-up worker
+    int setting_up_ = 0;        // batches admitted and not yet on the device
+    bool workers_stop_ = false;
+    std::condition_variable jobs_cv_;
+    std::vector<std::thread> workers_;
     std::thread thread_;
 };
 
