@@ -268,6 +268,38 @@ def measure_batched(pb, wl, torch, dev, reps=3):
     return out
 
 
+def measure_cfg3(pb, wl, torch, reps=3):
+    """ABM4, n=128 (scan dimension 512), m=p=16, h=5e-4, T=2^18: the level-
+    synchronous path, FP64 and mixed (one-system batch), rel err mixed vs FP64."""
+    from oracle import oracle
+
+    c = wl.cfg3()
+    out = {"workload": "cfg3: ABM4 n=128 (N_s=512) m=p=16 h=5e-4 T=2^18"}
+    stream = torch.cuda.Stream()
+    ys = {}
+    for name, prec in (("fp64", pb.FP64), ("mixed", pb.MIXED)):
+        b = pb.Batch([_spec(pb, c)], precision=prec)
+        b.execute(stream.cuda_stream)
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            b.execute(stream.cuda_stream)
+            e.record(stream)
+            e.synchronize()
+            ts.append(s.elapsed_time(e))
+        ms = statistics.median(ts)
+        ys[name] = b.output(0)[1]
+        flops = 4.0 * c.scan_dim ** 2 * c.T
+        out[name] = {"ms": ms, "value": b.state_steps / (ms / 1e3), "unit": UNIT,
+                     "sweep_tflops": flops / (ms / 1e3) / 1e12, "launches": b.launch_count}
+        b.close()
+    out["mixed_over_fp64"] = out["fp64"]["ms"] / out["mixed"]["ms"]
+    out["rel_err_mixed_vs_fp64"] = oracle.rel_err(ys["mixed"], ys["fp64"])
+    return out
+
+
 def measure_serving(pb, wl, torch, count=64, rates=(500.0, 2000.0, 8000.0)):
     """The serving loop on cfg5-shaped requests (Poisson arrivals), mixed form,
     beside one offline batch of the same requests."""
@@ -421,9 +453,10 @@ def run_ours(args):
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "ms_per_step": float(e2e_t.item()),
                "call": "ParODE_SimulateODE_d (host arrays in, host y out)"}
 
-    batched = serving = None
+    batched = serving = cfg3 = None
     if world == 1 and not args.no_extra:
         batched = measure_batched(pb, wl, torch, dev)
+        cfg3 = measure_cfg3(pb, wl, torch)
         serving = measure_serving(pb, wl, torch, count=args.serve_requests)
 
     if rank == 0:
@@ -481,6 +514,7 @@ def run_ours(args):
             "peaks_source": peaks_kind,
             "batched": batched,
             "serving": serving,
+            "abm_n128": cfg3,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
