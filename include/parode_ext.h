@@ -27,7 +27,9 @@ extern "C" {
 
 /* Options (ParODE_SetOption / ParODE_GetOption). */
 #define PARODE_OPT_PRECISION    1  /* PARODE_PRECISION_* used by SimulateODE (default FP64) */
-#define PARODE_OPT_PATH         2  /* 0 auto, 1 level-synchronous sweeps, 2 blocked fused sweeps */
+#define PARODE_OPT_PATH         2  /* 0 auto, 1 level-synchronous sweeps, 2 blocked (leaf chosen by cost),
+                                      3 blocked with the block-response GEMM leaf (FP64, inputs present),
+                                      4 blocked with the in-block sweep leaf */
 #define PARODE_OPT_LOG          3  /* non-zero: one line per solve on stderr */
 
 void ParODE_SetOption(int option, long long value, int nErr[]);

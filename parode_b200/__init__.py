@@ -37,6 +37,8 @@ OPT_LOG = 3
 PATH_AUTO = 0
 PATH_LEVEL = 1
 PATH_BLOCKED = 2
+PATH_BLOCKED_RESPONSE = 3
+PATH_BLOCKED_SWEEP = 4
 
 ERRORS = {
     0: "OK", -1: "NoGPU", -2: "NotInitialized", -3: "CouldNotCreateGPUKernels", -4: "NotEnoughResources",

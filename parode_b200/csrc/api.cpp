@@ -362,7 +362,7 @@ void ParODE_SetOption(int option, long long value, int nErr[])
         else L.precision = (int)value;
         break;
     case PARODE_OPT_PATH:
-        if (value < 0 || value > 2) rc = kInvalidArgument;
+        if (value < 0 || value > 4) rc = kInvalidArgument;
         else L.path = (int)value;
         break;
     case PARODE_OPT_LOG: L.log = (int)value; break;

@@ -33,10 +33,39 @@ struct LevelArgs {
     // Mixed form only: device address of a 128-byte TMA tensor map over the
     // source columns (level_encode_src_map).
     const void* src_map = nullptr;
+    // General shapes (tiled kernel only): rows of P (0: Np) and contraction
+    // length (0: Np); dst_limit >= 0 drops every result whose linear offset
+    // g*dst_gs + i*dst_is is at or beyond it (a ragged last column).
+    int M = 0, K = 0;
+    long dst_limit = -1;
 };
+
+__host__ __device__ inline int level_rows(const LevelArgs& a) { return a.M > 0 ? a.M : a.Np; }
+__host__ __device__ inline int level_k(const LevelArgs& a) { return a.K > 0 ? a.K : a.Np; }
 
 // One Blelloch level over all columns (up-sweep, down-sweep or P*P).
 void launch_affine_level(const LevelArgs& a, cudaStream_t s);
+
+// dst(g, i) = sum_k P[i][k] src(g, k) (+ acc) for a general rows x K matrix P
+// (a.M, a.K; K even) with the tiled FP64 DMMA kernel.
+void launch_gemm_tiled(const LevelArgs& a, cudaStream_t s);
+
+// Block response matrix of one system (kernels_br.cu): W (B p + NP rows, Kpad
+// columns, row-major) maps a block's input-sample window to its zero-seeded
+// local outputs (rows j p + o) and aggregate (rows B p + r).
+struct ResponseArgs {
+    int solver = 0, n = 0, m = 0, p = 0, NP = 0, B = 0;
+    int zeroB = 1, zeroD = 1;
+    const double* Phi = nullptr;   // NP x NP
+    const double* Bbar = nullptr;  // n x W m
+    const double* Cext = nullptr;  // p x NP (output rows of the scan state)
+    const double* D = nullptr;     // p x m
+    double* Wm = nullptr;
+    int K = 0, Kpad = 0;           // window columns, padded to even
+};
+// Window length (columns of W) for B steps: RK4 (2B + 1) m, ABM (B + 4) m.
+int response_window(int solver, int B, int m);
+void launch_block_response(const ResponseArgs* dArgs, int nsys, int max_np, int max_p, int max_kpad, cudaStream_t s);
 
 // Columns of a level that can reach an output.  Column g combines the
 // segments [g 2d, g 2d + d) and [g 2d + d, g 2d + 2d) of the time axis; when

@@ -160,12 +160,13 @@ template <bool kKC>
 __device__ void tiled_load(const LevelArgs& a, int m0, long n0, int k0, double* sA, double* sB)
 {
     const int tid = threadIdx.x;
+    const int rows = level_rows(a), K = level_k(a);  // K even: a 2-double chunk is wholly in or out
     // A: 64 rows x 32 doubles = 1024 chunks of 16 bytes
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const int c = tid + q * 256;
         const int r = c >> 4, kc = (c & 15) * 2;
-        const bool ok = (m0 + r < a.Np) && (k0 + kc < a.Np);
+        const bool ok = (m0 + r < rows) && (k0 + kc < K);
         const double* src = ok ? a.P + (long)(m0 + r) * a.ldp + k0 + kc : a.P;
         cp_async16(sA + r * kLdA + kc, src, ok);
     }
@@ -176,7 +177,7 @@ __device__ void tiled_load(const LevelArgs& a, int m0, long n0, int k0, double* 
             const int c = tid + q * 256;
             const int col = c >> 4, kc = (c & 15) * 2;
             const long g = n0 + col;
-            const bool ok = (g < a.ncols) && (k0 + kc < a.Np);
+            const bool ok = (g < a.ncols) && (k0 + kc < K);
             const double* src = ok ? a.src + g * a.src_gs + k0 + kc : a.src;
             cp_async16(sB + col * kLdBk + kc, src, ok);
         }
@@ -187,7 +188,7 @@ __device__ void tiled_load(const LevelArgs& a, int m0, long n0, int k0, double* 
             const int c = tid + q * 256;
             const int kr = c >> 5, nc = (c & 31) * 2;
             const long g = n0 + nc;
-            const bool ok = (g < a.ncols) && (k0 + kr < a.Np);
+            const bool ok = (g < a.ncols) && (k0 + kr < K);
             const double* src = ok ? a.src + (long)(k0 + kr) * a.src_ks + g : a.src;
             cp_async16(sB + kr * kLdBn + nc, src, ok);
         }
@@ -197,7 +198,8 @@ __device__ void tiled_load(const LevelArgs& a, int m0, long n0, int k0, double* 
 template <bool kKC>
 __device__ void tiled_level_body(const LevelArgs& a, long tile, double* smem)
 {
-    const int mt = (a.Np + kTM - 1) / kTM;
+    const int rows = level_rows(a);
+    const int mt = (rows + kTM - 1) / kTM;
     const int m0 = (int)(tile % mt) * kTM;
     const long n0 = (tile / mt) * kTN;
     double* sA = smem;
@@ -205,7 +207,7 @@ __device__ void tiled_level_body(const LevelArgs& a, long tile, double* smem)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int wm = warp & 1, wn = warp >> 1;
     const int gq = lane >> 2, tq = lane & 3;
-    const int nk = (a.Np + kTK - 1) / kTK;
+    const int nk = (level_k(a) + kTK - 1) / kTK;
 
     double acc[4][2][2];
 #pragma unroll
@@ -250,16 +252,18 @@ __device__ void tiled_level_body(const LevelArgs& a, long tile, double* smem)
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         const long r = m0 + wm * 32 + i * 8 + gq;
-        if (r >= a.Np) continue;
+        if (r >= rows) continue;
 #pragma unroll
         for (int j = 0; j < 2; ++j)
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
                 const long g = n0 + wn * 16 + j * 8 + 2 * tq + e;
                 if (g >= a.ncols) continue;
+                const long o = g * a.dst_gs + r * a.dst_is;
+                if (a.dst_limit >= 0 && o >= a.dst_limit) continue;
                 double v = acc[i][j][e];
                 if (a.acc) v += a.acc[g * a.acc_gs + r * a.acc_is];
-                a.dst[g * a.dst_gs + r * a.dst_is] = v;
+                a.dst[o] = v;
             }
     }
 }
@@ -472,7 +476,10 @@ LevelArgs tiled_args(const LevelArgs& a)
     return b;
 }
 
-long tiled_tiles(const LevelArgs& b) { return (long)((b.Np + kTM - 1) / kTM) * ((b.ncols + kTN - 1) / kTN); }
+long tiled_tiles(const LevelArgs& b)
+{
+    return (long)((level_rows(b) + kTM - 1) / kTM) * ((b.ncols + kTN - 1) / kTN);
+}
 
 template <int FR, int FC>
 void launch_level_t(const LevelArgs& a, int CW, cudaStream_t s)
@@ -573,7 +580,7 @@ LevelConfig level_config(const LevelArgs& a)
 {
     LevelConfig c;
     const int Np = a.Np;
-    if (Np > 64) {
+    if (Np > 64 || a.M > 0 || a.K > 0) {
         const LevelArgs b = tiled_args(a);
         c.id = b.src_ks == 1 ? 5 : 6;
         c.NC = kTN;
@@ -637,7 +644,23 @@ void launch_affine_level_grouped(const LevelConfig& c, const LevelArgs* dArgs, c
     }
 }
 
-LevelArgs level_grouped_args(const LevelArgs& a) { return a.Np > 64 ? tiled_args(a) : a; }
+LevelArgs level_grouped_args(const LevelArgs& a) { return (a.Np > 64 || a.M > 0 || a.K > 0) ? tiled_args(a) : a; }
+
+void launch_gemm_tiled(const LevelArgs& a, cudaStream_t s)
+{
+    if (a.ncols <= 0) return;
+    if (level_k(a) <= 0 || (level_k(a) & 1) || level_rows(a) <= 0 || (a.src_ks != 1 && a.src_gs != 1) ||
+        (a.ldp & 1) || a.cpy)
+        throw Error(kInvalidArgument, "tiled GEMM: even K, even ldp, K- or N-contiguous source, no copy");
+    PARODE_CUDA(cudaFuncSetAttribute(k_level_tiled<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)kTiledSmem));
+    PARODE_CUDA(cudaFuncSetAttribute(k_level_tiled<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)kTiledSmem));
+    const long tiles = tiled_tiles(a);
+    if (a.src_ks == 1) k_level_tiled<true><<<(unsigned)tiles, kThreads, kTiledSmem, s>>>(a);
+    else k_level_tiled<false><<<(unsigned)tiles, kThreads, kTiledSmem, s>>>(a);
+    PARODE_CUDA(cudaGetLastError());
+}
 
 long level_tiles(const LevelConfig& c, const LevelArgs& stored)
 {

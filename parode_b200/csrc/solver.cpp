@@ -40,7 +40,7 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
     path_ = kPathLevel;
     {
         const bool can_block = blocked_shape(Ns_, mu_, solver, &shape_);
-        if (opt.path == kPathBlocked && !can_block)
+        if (opt.path >= kPathBlocked && !can_block)
             throw Error(kInvalidArgument, "the blocked path supports scan dimensions up to 64");
         if (opt.path != kPathLevel && can_block) path_ = kPathBlocked;
     }
@@ -93,6 +93,29 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
                 levels_ = std::max(lev2 + ilog2(next_pow2(c2)), shape_.R);
             }
         }
+        // FP64: the leaf as one GEMM with the block response matrix (see
+        // kernels_br.cu) when that costs fewer flops than the in-block sweeps:
+        // about 2 (B p + NP) K / B per step against 4 NP^2
+        if (precision_used_ != kMixed && mu_ > 0 && opt.path != kPathBlockedSweep) {
+            const int K = response_window(solver, shape_.B, mu_);
+            const double resp = 2.0 * ((double)shape_.B * p_ + Np_) * K / shape_.B;
+            const double sweeps = 4.0 * Np_ * Np_;
+            if (opt.path == kPathBlockedResponse || resp < 0.5 * sweeps) {
+                br_ = true;
+                brK_ = K;
+                brKpad_ = (K + 1) & ~1;
+                nblocks_ = (nScan_ + shape_.B - 1) / shape_.B;
+                long c3 = nblocks_;
+                int lev3 = shape_.R;
+                while (c3 > shape_.S_items) {
+                    c3 = (c3 + shape_.B - 1) / shape_.B;
+                    lev3 += shape_.R;
+                }
+                levels_ = std::max(lev3 + ilog2(next_pow2(c3)), shape_.R);
+            }
+        }
+        if (opt.path == kPathBlockedResponse && !br_)
+            throw Error(kInvalidArgument, "the response leaf needs inputs and the FP64 form");
     }
     PARODE_CUDA(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_));
 
@@ -159,7 +182,13 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
         u_base_ = (t0 + 3.0 * h) - 3.0 * h;
         u_dt_ = h;
     }
-    if (mu_ > 0 && !gen_) alloc(&dU_, nU_ * (long)mu_);
+    if (mu_ > 0 && !gen_) {
+        // the response leaf reads whole windows: the last block's window runs
+        // past the samples into a zero padding
+        const long pad = br_ ? (2L * shape_.B + 8) * mu_ + 2 : 0;
+        alloc(&dU_, nU_ * (long)mu_ + pad);
+        if (pad) PARODE_CUDA(cudaMemsetAsync(dU_, 0, sizeof(double) * (size_t)(nU_ * mu_ + pad), stream_));
+    }
     PARODE_CUDA(cudaMemcpyAsync(dPow_, PhiP.data(), sizeof(double) * PhiP.size(), cudaMemcpyHostToDevice, stream_));
     PARODE_CUDA(cudaMemcpyAsync(dBbar_, Bbar.data(), sizeof(double) * Bbar.size(), cudaMemcpyHostToDevice, stream_));
     if (!sys.zeroC)
@@ -211,6 +240,30 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
                                     stream_));
     }
     PARODE_CUDA(cudaMemcpyAsync(dX0_, X0.data(), sizeof(double) * Np_, cudaMemcpyHostToDevice, stream_));
+    if (br_) {
+        // block response matrix from Phi (power-table level 0), Bbar, Cext, D
+        alloc(&dW_, (long)(shape_.B * p_ + Np_) * brKpad_);
+        ResponseArgs ra;
+        ra.solver = solver;
+        ra.n = n;
+        ra.m = mu_;
+        ra.p = p_;
+        ra.NP = Np_;
+        ra.B = shape_.B;
+        ra.zeroB = sys.zeroB;
+        ra.zeroD = sys.zeroD;
+        ra.Phi = dPow_;
+        ra.Bbar = dBbar_;
+        ra.Cext = dCext_;
+        ra.D = dD_;
+        ra.Wm = dW_;
+        ra.K = brK_;
+        ra.Kpad = brKpad_;
+        double* dra = nullptr;
+        alloc(&dra, (long)((sizeof(ResponseArgs) + 7) / 8));
+        PARODE_CUDA(cudaMemcpyAsync(dra, &ra, sizeof(ra), cudaMemcpyHostToDevice, stream_));
+        launch_block_response(reinterpret_cast<const ResponseArgs*>(dra), 1, Np_, p_, brKpad_, stream_);
+    }
     PARODE_CUDA(cudaStreamSynchronize(stream_));
 }
 
@@ -435,9 +488,37 @@ void Plan::execute_blocked(double* Y, cudaStream_t s)
     a.status = dStatus_;
     // one SM stays free for the side stream's power-table kernel
     const int grid = more_levels ? std::max(1, sms_ - 1) : sms_;
-    if (precision_used_ == kMixed) launch_blocked_leaf_tc(shape_, a, grid, s);
-    else launch_blocked_leaf(shape_, a, grid, s);
-    ++launches;
+    if (br_) {
+        // leaf = W x [sample windows of all blocks]: outputs straight into y
+        // (rows (j, o) of block b are contiguous there), aggregates into G
+        LevelArgs g;
+        g.P = dW_;
+        g.ldp = brKpad_;
+        g.Np = Np_;
+        g.M = shape_.B * p_;
+        g.K = brKpad_;
+        g.ncols = nblocks_;
+        g.src = dU_;
+        g.src_gs = (solver_ == kRK4 ? 2L : 1L) * shape_.B * mu_;
+        g.src_ks = 1;
+        g.dst = Y + a.ybase * p_;
+        g.dst_gs = (long)shape_.B * p_;
+        g.dst_is = 1;
+        g.dst_limit = nScan_ * p_;
+        launch_gemm_tiled(g, s);
+        LevelArgs h = g;
+        h.P = dW_ + (long)shape_.B * p_ * brKpad_;
+        h.M = Np_;
+        h.dst = dG_;
+        h.dst_gs = Np_;
+        h.dst_limit = -1;
+        launch_gemm_tiled(h, s);
+        launches += 2;
+    } else {
+        if (precision_used_ == kMixed) launch_blocked_leaf_tc(shape_, a, grid, s);
+        else launch_blocked_leaf(shape_, a, grid, s);
+        ++launches;
+    }
     mark("leaf", s);
     PARODE_CUDA(cudaStreamWaitEvent(s, fork_[3], 0));
     // exclusive scan of the block aggregates, seeded with the initial state

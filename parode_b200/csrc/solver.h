@@ -18,7 +18,9 @@
 
 namespace parode {
 
-enum Path : int { kPathAuto = 0, kPathLevel = 1, kPathBlocked = 2 };
+// kPathBlocked chooses the leaf by cost; kPathBlockedResponse / kPathBlockedSweep
+// force the block-response GEMM leaf / the in-block sweep leaf.
+enum Path : int { kPathAuto = 0, kPathLevel = 1, kPathBlocked = 2, kPathBlockedResponse = 3, kPathBlockedSweep = 4 };
 
 struct PlanOptions {
     int precision = 0;  // Precision
@@ -85,6 +87,9 @@ private:
     double *dG_ = nullptr, *dWork_ = nullptr, *dCP_ = nullptr, *dCext_ = nullptr;
     size_t stage_bytes_ = 0;
     int precision_used_ = 0;
+    bool br_ = false;           // leaf = block response GEMM (kernels_br.cu)
+    int brK_ = 0, brKpad_ = 0;  // window columns (padded to even)
+    double* dW_ = nullptr;      // response matrix, (B p + NP) x brKpad_
     int* dStatus_ = nullptr;
     cudaStream_t side_ = nullptr;
     cudaEvent_t fork_[4] = {nullptr, nullptr, nullptr, nullptr};

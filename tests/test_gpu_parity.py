@@ -38,11 +38,13 @@ def _gpu_y(pb, case, path, precision=0, Cm="C", D="D", B="B"):
     return y
 
 
-PATHS = [1, 2]  # level-synchronous, blocked (scan dimension <= 64)
+# level-synchronous; blocked (scan dimension <= 64) with the leaf chosen by
+# cost, with the block-response GEMM leaf, with the in-block sweep leaf
+PATHS = [1, 2, 3, 4]
 
 
 def _skip_unsupported(path, case):
-    if path == 2 and case.scan_dim > 64:
+    if path >= 2 and case.scan_dim > 64:
         pytest.skip("blocked path covers scan dimensions up to 64")
 
 
@@ -67,7 +69,9 @@ def test_fp64_parity_sizes(pb, path, solver, n, m, p, T):
 def test_fp64_absent_matrices(pb, path, solver):
     case = wl.small(77 + solver, solver, 6, 2, 3, 200, h=0.02)
     _skip_unsupported(path, case)
-    for Cm, D, B in [("C", None, "B"), (None, "D", "B"), (None, None, "B"), ("C", "D", None)]:
+    for Cm, D, B in [("C", None, "B"), (None, "D", "B"), (None, None, "B"), ("C", "D", None), (None, None, None)]:
+        if path == 3 and B is None and D is None:
+            continue  # the response leaf maps input samples: nothing to map without inputs
         y = _gpu_y(pb, case, path, Cm=Cm, D=D, B=B)
         yo = _oracle_y(case, Cm=Cm, D=D, B=B)
         assert y.shape == yo.shape
