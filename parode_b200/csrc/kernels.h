@@ -38,6 +38,11 @@ struct LevelArgs {
     // g*dst_gs + i*dst_is is at or beyond it (a ragged last column).
     int M = 0, K = 0;
     long dst_limit = -1;
+    // Two-part source (tiled kernel, K-contiguous only): contraction indices
+    // k >= K1 (K1 > 0, even) read src2(g, k - K1) = src2[g*src2_gs + k - K1].
+    int K1 = 0;
+    const double* src2 = nullptr;
+    long src2_gs = 0;
 };
 
 __host__ __device__ inline int level_rows(const LevelArgs& a) { return a.M > 0 ? a.M : a.Np; }
@@ -60,8 +65,9 @@ struct ResponseArgs {
     const double* Bbar = nullptr;  // n x W m
     const double* Cext = nullptr;  // p x NP (output rows of the scan state)
     const double* D = nullptr;     // p x m
-    double* Wm = nullptr;
+    double* Wm = nullptr;          // row stride Kpad + NPstate
     int K = 0, Kpad = 0;           // window columns, padded to even
+    int NPstate = 0;               // NP: also the initial-state columns (z_0 = I on them), or 0
 };
 // Window length (columns of W) for B steps: RK4 (2B + 1) m, ABM (B + 4) m.
 int response_window(int solver, int B, int m);

@@ -9,12 +9,16 @@
 // so they are one matrix W per system,
 //   rows [0, B p)        -> y_j[o] (row j p + o),
 //   rows [B p, B p + NP) -> z_B,
-//   columns              -> the block's sample window, sample s input i at s m + i
+//   columns [0, Kpad)    -> the block's sample window, sample s input i at s m + i
 //                           (RK4: samples 2bB .. 2bB + 2B, ABM: bB .. bB + B + 3),
+//   columns [Kpad, Kpad + NPstate) -> the block's initial state (its carry X_b),
 // and the leaf becomes W times the windows of all blocks: one GEMM.  The
-// composition across blocks (carry hierarchy, fix-up) is unchanged, so the
-// result is the blocked Blelloch scan's.  W is built once per plan in FP64
-// by running the block recurrence on the window basis.
+// aggregates (state-free part of rows [B p, B p + NP)) go to the carry
+// hierarchy first; the outputs are then W's output rows times [window; X_b],
+// which folds the fix-up C Phi^j X_b into the same GEMM.  The composition
+// across blocks is unchanged, so the result is the blocked Blelloch scan's.
+// W is built once per plan in FP64 by running the block recurrence on the
+// basis of the window and state columns.
 #include "common.h"
 #include "kernels.h"
 
@@ -35,7 +39,8 @@ __global__ void __launch_bounds__(kThreads) k_block_response(const ResponseArgs*
     const ResponseArgs a = args[blockIdx.y];
     const int NP = a.NP, B = a.B, p = a.p, m = a.m, n = a.n;
     const int c0 = blockIdx.x * kCols;
-    if (c0 >= a.Kpad) return;
+    const int ld = a.Kpad + a.NPstate;  // window columns, then the block's initial-state columns
+    if (c0 >= ld) return;
     const bool rk4 = a.solver == 0;
     const int W = rk4 ? 3 : 5;
     const int coff = rk4 ? 0 : 3 * n;  // forcing rows / output state block
@@ -45,20 +50,24 @@ __global__ void __launch_bounds__(kThreads) k_block_response(const ResponseArgs*
     double* sC = zn + (long)NP * kCols;           // p x NP
     for (int e = threadIdx.x; e < NP * NP; e += kThreads) sPhi[e] = a.Phi[e];
     for (int e = threadIdx.x; e < p * NP; e += kThreads) sC[e] = a.Cext[e];
-    for (int e = threadIdx.x; e < NP * kCols; e += kThreads) z[e] = 0.0;
+    // z_0: zero on the window columns, the identity on the state columns
+    for (int e = threadIdx.x; e < NP * kCols; e += kThreads) {
+        const int r = e / kCols, col = c0 + (e - r * kCols);
+        z[e] = (col >= a.Kpad && col - a.Kpad == r) ? 1.0 : 0.0;
+    }
     __syncthreads();
     for (int j = 0; j < B; ++j) {
         // outputs of step j: Cext z_j + D u_j (u_j: sample 2j for RK4, j + 3 for ABM)
         const int su = rk4 ? 2 * j : j + 3;
         for (int e = threadIdx.x; e < p * kCols; e += kThreads) {
             const int o = e / kCols, c = e - o * kCols, col = c0 + c;
-            if (col >= a.Kpad) continue;
+            if (col >= ld) continue;
             double v = 0.0;
-            if (col < a.K) {
+            if (col < a.K || col >= a.Kpad) {
                 for (int r = 0; r < NP; ++r) v = fma(sC[o * NP + r], z[r * kCols + c], v);
-                if (!a.zeroD && m > 0 && col / m == su) v += a.D[(long)o * m + col % m];
+                if (col < a.K && !a.zeroD && m > 0 && col / m == su) v += a.D[(long)o * m + col % m];
             }
-            a.Wm[(long)(j * p + o) * a.Kpad + col] = v;
+            a.Wm[(long)(j * p + o) * ld + col] = v;
         }
         // z_{j+1} = Phi z_j + S_j, S_j = the forcing of step j on the window
         for (int e = threadIdx.x; e < NP * kCols; e += kThreads) {
@@ -81,7 +90,7 @@ __global__ void __launch_bounds__(kThreads) k_block_response(const ResponseArgs*
     // aggregate rows: z_B
     for (int e = threadIdx.x; e < NP * kCols; e += kThreads) {
         const int r = e / kCols, c = e - r * kCols, col = c0 + c;
-        if (col < a.Kpad) a.Wm[(long)(B * p + r) * a.Kpad + col] = col < a.K ? z[e] : 0.0;
+        if (col < ld) a.Wm[(long)(B * p + r) * ld + col] = (col < a.K || col >= a.Kpad) ? z[e] : 0.0;
     }
 }
 
@@ -98,7 +107,7 @@ void launch_block_response(const ResponseArgs* dArgs, int nsys, int max_np, int 
     const size_t smem = ((size_t)max_np * max_np + 2 * (size_t)max_np * kCols + (size_t)max_p * max_np) * sizeof(double);
     if (smem > 220 * 1024) throw Error(kInvalidArgument, "block response: shared memory");
     PARODE_CUDA(cudaFuncSetAttribute(k_block_response, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 grid((unsigned)((max_kpad + kCols - 1) / kCols), (unsigned)nsys);
+    dim3 grid((unsigned)((max_kpad + max_np + kCols - 1) / kCols), (unsigned)nsys);
     k_block_response<<<grid, kThreads, smem, s>>>(dArgs);
     PARODE_CUDA(cudaGetLastError());
 }

@@ -177,8 +177,11 @@ __device__ void tiled_load(const LevelArgs& a, int m0, long n0, int k0, double* 
             const int c = tid + q * 256;
             const int col = c >> 4, kc = (c & 15) * 2;
             const long g = n0 + col;
-            const bool ok = (g < a.ncols) && (k0 + kc < K);
-            const double* src = ok ? a.src + g * a.src_gs + k0 + kc : a.src;
+            const int k = k0 + kc;
+            const bool ok = (g < a.ncols) && (k < K);
+            const double* src = !ok ? a.src
+                                    : (a.K1 > 0 && k >= a.K1) ? a.src2 + g * a.src2_gs + (k - a.K1)
+                                                              : a.src + g * a.src_gs + k;
             cp_async16(sB + col * kLdBk + kc, src, ok);
         }
     } else {
@@ -652,6 +655,9 @@ void launch_gemm_tiled(const LevelArgs& a, cudaStream_t s)
     if (level_k(a) <= 0 || (level_k(a) & 1) || level_rows(a) <= 0 || (a.src_ks != 1 && a.src_gs != 1) ||
         (a.ldp & 1) || a.cpy)
         throw Error(kInvalidArgument, "tiled GEMM: even K, even ldp, K- or N-contiguous source, no copy");
+    if (a.K1 > 0 && ((a.K1 & 1) || a.K1 >= level_k(a) || a.src_ks != 1 || !a.src2 || (a.src2_gs & 1) ||
+                     (a.src_gs & 1)))
+        throw Error(kInvalidArgument, "tiled GEMM: two-part source needs even K1 < K, K-contiguous, even strides");
     PARODE_CUDA(cudaFuncSetAttribute(k_level_tiled<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)kTiledSmem));
     PARODE_CUDA(cudaFuncSetAttribute(k_level_tiled<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,

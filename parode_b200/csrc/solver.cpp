@@ -242,7 +242,7 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
     PARODE_CUDA(cudaMemcpyAsync(dX0_, X0.data(), sizeof(double) * Np_, cudaMemcpyHostToDevice, stream_));
     if (br_) {
         // block response matrix from Phi (power-table level 0), Bbar, Cext, D
-        alloc(&dW_, (long)(shape_.B * p_ + Np_) * brKpad_);
+        alloc(&dW_, (long)(shape_.B * p_ + Np_) * (brKpad_ + Np_));
         ResponseArgs ra;
         ra.solver = solver;
         ra.n = n;
@@ -259,6 +259,7 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
         ra.Wm = dW_;
         ra.K = brK_;
         ra.Kpad = brKpad_;
+        ra.NPstate = Np_;
         double* dra = nullptr;
         alloc(&dra, (long)((sizeof(ResponseArgs) + 7) / 8));
         PARODE_CUDA(cudaMemcpyAsync(dra, &ra, sizeof(ra), cudaMemcpyHostToDevice, stream_));
@@ -426,8 +427,71 @@ void Plan::execute(double* y, cudaStream_t s)
     last_y_ = Y;
 }
 
+void Plan::execute_response(double* Y, cudaStream_t s)
+{
+    // leaf = W x [sample window; initial state] per block (kernels_br.cu):
+    // aggregates first (the state columns are not used), then the carry, then
+    // the outputs with the carried block states, written straight into y
+    // (rows (j, o) of block b are contiguous there).  The power table
+    // P_1..P_levels (one CTA) runs on the side stream beside the sampling and
+    // the aggregate GEMM.
+    int launches = 0;
+    marks_.clear();
+    mark("start", s);
+    PARODE_CUDA(cudaEventRecord(fork_[0], s));
+    PARODE_CUDA(cudaStreamWaitEvent(side_, fork_[0], 0));
+    launch_blocked_tables(shape_, dPow_, 1, levels_, nullptr, nullptr, p_, side_);
+    ++launches;
+    PARODE_CUDA(cudaEventRecord(fork_[3], side_));
+    fill_inputs(s);
+    ++launches;
+    mark("inputs", s);
+    const int ybase = solver_ == kRK4 ? 0 : 3;
+    const long ld = brKpad_ + Np_;
+    LevelArgs g;
+    g.P = dW_ + (long)shape_.B * p_ * ld;
+    g.ldp = ld;
+    g.Np = Np_;
+    g.M = Np_;
+    g.K = brKpad_;
+    g.ncols = nblocks_;
+    g.src = dU_;
+    g.src_gs = (solver_ == kRK4 ? 2L : 1L) * shape_.B * mu_;
+    g.src_ks = 1;
+    g.dst = dG_;
+    g.dst_gs = Np_;
+    g.dst_is = 1;
+    launch_gemm_tiled(g, s);
+    ++launches;
+    mark("aggregates", s);
+    PARODE_CUDA(cudaStreamWaitEvent(s, fork_[3], 0));
+    launches += launch_blocked_carry(shape_, dG_, nblocks_, shape_.R, dPow_, dX0_, dWork_, sms_, s);
+    mark("carry", s);
+    LevelArgs h = g;
+    h.P = dW_;
+    h.M = shape_.B * p_;
+    h.K = (int)ld;
+    h.K1 = brKpad_;
+    h.src2 = dG_;
+    h.src2_gs = Np_;
+    h.dst = Y + ybase * p_;
+    h.dst_gs = (long)shape_.B * p_;
+    h.dst_limit = nScan_ * p_;
+    launch_gemm_tiled(h, s);
+    ++launches;
+    if (solver_ == kABM)
+        PARODE_CUDA(cudaMemcpyAsync(Y, dYpre_, sizeof(double) * 3 * p_, cudaMemcpyDeviceToDevice, s));
+    mark("outputs", s);
+    launches_ = launches;
+    last_y_ = Y;
+}
+
 void Plan::execute_blocked(double* Y, cudaStream_t s)
 {
+    if (br_) {
+        execute_response(Y, s);
+        return;
+    }
     int launches = 0;
     marks_.clear();
     mark("start", s);
@@ -488,37 +552,9 @@ void Plan::execute_blocked(double* Y, cudaStream_t s)
     a.status = dStatus_;
     // one SM stays free for the side stream's power-table kernel
     const int grid = more_levels ? std::max(1, sms_ - 1) : sms_;
-    if (br_) {
-        // leaf = W x [sample windows of all blocks]: outputs straight into y
-        // (rows (j, o) of block b are contiguous there), aggregates into G
-        LevelArgs g;
-        g.P = dW_;
-        g.ldp = brKpad_;
-        g.Np = Np_;
-        g.M = shape_.B * p_;
-        g.K = brKpad_;
-        g.ncols = nblocks_;
-        g.src = dU_;
-        g.src_gs = (solver_ == kRK4 ? 2L : 1L) * shape_.B * mu_;
-        g.src_ks = 1;
-        g.dst = Y + a.ybase * p_;
-        g.dst_gs = (long)shape_.B * p_;
-        g.dst_is = 1;
-        g.dst_limit = nScan_ * p_;
-        launch_gemm_tiled(g, s);
-        LevelArgs h = g;
-        h.P = dW_ + (long)shape_.B * p_ * brKpad_;
-        h.M = Np_;
-        h.dst = dG_;
-        h.dst_gs = Np_;
-        h.dst_limit = -1;
-        launch_gemm_tiled(h, s);
-        launches += 2;
-    } else {
-        if (precision_used_ == kMixed) launch_blocked_leaf_tc(shape_, a, grid, s);
-        else launch_blocked_leaf(shape_, a, grid, s);
-        ++launches;
-    }
+    if (precision_used_ == kMixed) launch_blocked_leaf_tc(shape_, a, grid, s);
+    else launch_blocked_leaf(shape_, a, grid, s);
+    ++launches;
     mark("leaf", s);
     PARODE_CUDA(cudaStreamWaitEvent(s, fork_[3], 0));
     // exclusive scan of the block aggregates, seeded with the initial state

@@ -60,6 +60,7 @@ private:
     void alloc(double** p, long n);
     void mark(const char* stage, cudaStream_t s);
     void execute_blocked(double* Y, cudaStream_t s);
+    void execute_response(double* Y, cudaStream_t s);
     void fill_inputs(cudaStream_t s);
 
     int device_ = 0;
