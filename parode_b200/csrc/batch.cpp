@@ -131,8 +131,33 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             q.u_dt = b.h;
         }
         BlockedShape sh;
-        q.blocked = opt.path != kPathLevel && blocked_shape(q.Ns, std::max(q.mu, 1), 0, &sh);
-        if (q.blocked) {
+        const bool can_block = blocked_shape(q.Ns, std::max(q.mu, 1), 0, &sh);
+        // block-response leaf for systems with inputs when it costs less than
+        // the level-synchronous sweeps (4 Np^2 per step) or, for scan
+        // dimensions <= 64, half the in-block sweeps
+        if (q.mu > 0 && opt.path != kPathLevel && opt.path != kPathBlockedSweep) {
+            const int np = (int)round_up(q.Ns, 8);
+            double cost = 0.0;
+            const int R = response_log2_block(q.solver, np, q.mu, q.p, q.nScan, &cost);
+            const double sweeps = 4.0 * np * np;
+            if (opt.path == kPathBlockedResponse || cost < (can_block ? 0.5 : 1.0) * sweeps) {
+                if (np > 1024) throw Error(kInvalidSystem, "scan dimension above 1024 is not supported");
+                q.resp = true;
+                q.Np = np;
+                q.lev0 = R;
+                q.Bk = 1 << R;
+                q.Kw = response_window(q.solver, q.Bk, q.mu);
+                q.Kpad = (q.Kw + 1) & ~1;
+                q.nblocks = (q.nScan + q.Bk - 1) / q.Bk;
+                q.Tp = next_pow2(q.nblocks);
+                q.levels = ilog2(q.Tp);
+                q.pow_levels = q.levels > 0 ? R + q.levels : 1;
+                rs_.push_back(i);
+            }
+        }
+        q.blocked = !q.resp && opt.path != kPathLevel && can_block;
+        if (q.resp) {
+        } else if (q.blocked) {
             q.Np = sh.NP;
             int bi = -1;
             for (int k = 0; k < (int)buckets_.size(); ++k)
@@ -151,10 +176,12 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             if (q.Np > 1024) throw Error(kInvalidSystem, "scan dimension above 1024 is not supported");
             q.Tp = next_pow2(q.nScan);
             q.levels = ilog2(q.Tp);
+            q.pow_levels = q.levels;
             ls_.push_back(i);
         }
-        // mixed form: level-synchronous systems run their lower levels on the
-        // tensor cores; the blocked buckets stay FP64 here
+        // mixed form: level-synchronous scans (over steps or over response
+        // blocks) run their lower levels on the tensor cores; the blocked
+        // buckets stay FP64 here
         q.precision = (opt.precision == kMixed && !q.blocked) ? kMixed : kFP64;
     }
     // bucket shapes: the widest input of the bucket sizes the sample staging
@@ -255,7 +282,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
     struct Off {
         size_t phi0, bbar, c, d, cext, x0, sin, ypre;
         size_t bbarT, cT, dT;  // level-synchronous systems: transposed copies (coalesced per-row kernels)
-        size_t P, U, Y, V, G, CP, Ps;
+        size_t P, U, Y, V, G, CP, Ps, W;
     };
     std::vector<Off> off(N);
     for (int i = 0; i < N; ++i) {
@@ -267,7 +294,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         o.c = st.put(s.zeroC ? nullptr : s.C.data(), sizeof(double) * (s.zeroC ? 1 : (size_t)q.p * q.n), L);
         o.d = st.put(s.zeroD ? nullptr : s.D.data(), sizeof(double) * (s.zeroD ? 1 : (size_t)q.p * s.m), L);
         o.x0 = st.put(X0[i].data(), sizeof(double) * X0[i].size(), L);
-        if (q.blocked) {
+        if (q.blocked || q.resp) {
             std::vector<double> Cext((size_t)q.p * q.Np, 0.0);
             const int xoff = q.solver == kRK4 ? 0 : 3 * q.n;
             for (int r = 0; r < q.p; ++r)
@@ -289,7 +316,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             o.sin = st.put(prm.data(), sizeof(double) * prm.size(), L);
         }
         if (q.solver == kABM) o.ypre = st.put(Ypre[i].data(), sizeof(double) * Ypre[i].size(), L);
-        if (!q.blocked) {
+        if (!q.blocked && !q.resp) {
             const int Wm = q.W * (s.zeroB ? 0 : s.m);
             std::vector<double> bt((size_t)std::max(Wm, 1) * q.n, 0.0);
             for (int r = 0; r < q.n; ++r)
@@ -306,8 +333,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             o.dT = st.put(dt.data(), sizeof(double) * dt.size(), L);
         }
     }
-    const size_t const_bytes_sys = L.bytes;
-    (void)const_bytes_sys;
+    const size_t const_end = L.bytes;
     // work buffers (offsets only; not staged)
     for (int i = 0; i < N; ++i) {
         Sys& q = sys_[i];
@@ -318,19 +344,23 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             o.G = L.take(sizeof(double) * (size_t)q.ntiles * (bk.sh.S / bk.sh.B) * q.Np);
             o.CP = L.take(sizeof(double) * (size_t)bk.sh.B * q.p * q.Np);
         } else {
-            o.P = L.take(sizeof(double) * (size_t)std::max(q.levels, 1) * q.Np * q.Np);
+            o.P = L.take(sizeof(double) * (size_t)std::max(q.pow_levels, 1) * q.Np * q.Np);
             o.V = L.take(sizeof(double) * (size_t)(q.Tp + 1) * q.Np);  // slot -1 holds the initial state
-            // mixed: tensor cores for the levels below the top four whose
-            // P_l - R_l stays small (|P_l - R_l| <~ 2^l |Phi - R|: at most 1/4);
+            // mixed: tensor cores for the scan levels below the top four whose
+            // P - R stays small (|P_l - R_l| <~ 2^l |Phi - R|: at most 1/4);
             // the rest, and the power table, stay FP64
             if (q.precision == kMixed) {
                 int lv = 0;
-                while (lv < q.levels - 4 && std::ldexp(q.delta, lv) <= 0.25) ++lv;
+                while (lv < q.levels - 4 && std::ldexp(q.delta, q.lev0 + lv) <= 0.25) ++lv;
                 q.tc_levels = lv;
             }
             o.Ps = q.tc_levels > 0 ? L.take(level_split_bytes(q.Np) * (size_t)q.tc_levels) : 0;
+            if (q.resp) o.W = L.take(sizeof(double) * ((size_t)q.Bk * q.p + q.Np) * ((size_t)q.Kpad + q.Np));
         }
-        o.U = q.mu > 0 ? L.take(sizeof(double) * (size_t)q.nU * q.mu) : 0;
+        // the response GEMMs read whole sample windows: the last block's
+        // window runs past the samples into a zero padding
+        const size_t upad = q.resp ? (size_t)(2 * q.Bk + 8) * q.mu + 2 : 0;
+        o.U = q.mu > 0 ? L.take(sizeof(double) * ((size_t)q.nU * q.mu + upad)) : 0;
         o.Y = L.take(sizeof(double) * (size_t)q.nOut * q.p);
     }
     const size_t work_end = L.bytes;
@@ -355,6 +385,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             for (int i : bk.systems) items_ub += sys_[i].ntiles;
         long lev_entries = 0;
         for (int i : ls_) lev_entries += 4L * std::max(sys_[i].levels, 1);
+        for (int i : rs_) lev_entries += 4L * std::max(sys_[i].pow_levels, 1) + 8;
         job_bytes = nb * (sizeof(LeafArgs) + 3 * sizeof(double*) + 4 * kAlign) +
                     (size_t)items_ub * sizeof(BatchItem) + buckets_.size() * 8 * kAlign +
                     (size_t)N * (sizeof(SampleJob) + sizeof(ForcingJob) + sizeof(OutputJob) + 2 * sizeof(CopyJob)) +
@@ -393,6 +424,10 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         } else {
             q.V = dp(o.V);
             if (q.tc_levels > 0) q.Ps = reinterpret_cast<float*>(base + o.Ps);
+            if (q.resp) {
+                q.Cext = dp(o.cext);
+                q.Wm = dp(o.W);
+            }
         }
         if (q.mu > 0 && q.input->kind == InputEntry::kSinusoid) q.sin = dp(o.sin);
     }
@@ -495,12 +530,26 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         if (nSampleJobs_)
             dSampleJobs_ = reinterpret_cast<SampleJob*>(base + jput(sj.data(), sizeof(SampleJob) * sj.size()));
     }
-    // level-synchronous systems: forcing, seed, output jobs and the grouped levels
-    if (!ls_.empty()) {
+    // level-synchronous systems: forcing, seed, output jobs and the grouped
+    // levels; response systems: their GEMMs, seed and block-scan levels
+    std::vector<int> lv = ls_;
+    lv.insert(lv.end(), rs_.begin(), rs_.end());
+    if (!lv.empty()) {
         std::vector<ForcingJob> fj;
         std::vector<OutputJob> oj;
         std::vector<CopyJob> cj;
-        int Lmax = 0;
+        int Lmax = 0, Pmax = 0;
+        for (int i : rs_) {
+            const Sys& q = sys_[i];
+            CopyJob c;
+            c.dst = q.V;
+            c.src = q.X0;
+            c.N = q.Np;
+            cj.push_back(c);
+            maxSeed_ = std::max<long>(maxSeed_, q.Np);
+            Lmax = std::max(Lmax, q.levels);
+            Pmax = std::max(Pmax, q.pow_levels);
+        }
         for (int i : ls_) {
             const Sys& q = sys_[i];
             ForcingJob f;
@@ -541,10 +590,14 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             cj.push_back(c);
             maxSeed_ = std::max<long>(maxSeed_, q.Np);
             Lmax = std::max(Lmax, q.levels);
+            Pmax = std::max(Pmax, q.pow_levels);
         }
-        dForcing_ = reinterpret_cast<ForcingJob*>(base + jput(fj.data(), sizeof(ForcingJob) * fj.size()));
-        dOutput_ = reinterpret_cast<OutputJob*>(base + jput(oj.data(), sizeof(OutputJob) * oj.size()));
+        if (!fj.empty()) {
+            dForcing_ = reinterpret_cast<ForcingJob*>(base + jput(fj.data(), sizeof(ForcingJob) * fj.size()));
+            dOutput_ = reinterpret_cast<OutputJob*>(base + jput(oj.data(), sizeof(OutputJob) * oj.size()));
+        }
         dSeed_ = reinterpret_cast<CopyJob*>(base + jput(cj.data(), sizeof(CopyJob) * cj.size()));
+        nSeed_ = (int)cj.size();
         // grouped level launches: for each level, entries grouped by tiling config
         auto add_level = [&](std::vector<GroupedLaunch>& out, const std::vector<std::pair<int, LevelArgs>>& ents,
                              int l) {
@@ -564,11 +617,13 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
                 if (e.second.ncols <= 0) continue;
                 const Sys& q = sys_[e.first];
                 if (l >= 0 && l < q.tc_levels && level_tc_supported(e.second)) {
-                    // exact part of P_l = Phi^(2^l): I for RK4; for ABM the
-                    // companion shift S^(2^l) (block b reads block min(b + 2^l, 3))
+                    // exact part of P = Phi^(2^k), k = lev0 + l: I for RK4; for
+                    // ABM the companion shift S^(2^k) (block b reads block
+                    // min(b + 2^k, 3))
+                    const int k = q.lev0 + l;
                     LevelArgs t = e.second;
                     t.rn = q.solver == kRK4 ? 0 : q.n;
-                    t.rsh = std::min(1 << std::min(l, 2), 3);
+                    t.rsh = std::min(1 << std::min(k, 2), 3);
                     t.Ps = q.Ps + (size_t)l * (level_split_bytes(q.Np) / sizeof(float));
                     tc.push_back(t);
                     continue;
@@ -632,11 +687,11 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
                 out.push_back(gl);
             }
         };
-        for (int l = 1; l < Lmax; ++l) {
+        for (int l = 1; l < Pmax; ++l) {
             std::vector<std::pair<int, LevelArgs>> ents;
-            for (int i : ls_) {
+            for (int i : lv) {
                 const Sys& q = sys_[i];
-                if (l >= q.levels) continue;
+                if (l >= q.pow_levels) continue;
                 const long Np = q.Np;
                 LevelArgs a;
                 a.P = q.P + (long)(l - 1) * Np * Np;
@@ -655,15 +710,16 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         }
         for (int l = 0; l < Lmax; ++l) {
             std::vector<std::pair<int, LevelArgs>> ents;
-            for (int i : ls_) {
+            for (int i : lv) {
                 const Sys& q = sys_[i];
                 if (l >= q.levels) continue;
                 const long Np = q.Np, d = 1L << l;
+                const long items = q.resp ? q.nblocks : q.nScan;
                 LevelArgs a;
-                a.P = q.P + (long)l * Np * Np;
+                a.P = q.P + (long)(q.lev0 + l) * Np * Np;
                 a.ldp = Np;
                 a.Np = q.Np;
-                a.ncols = sweep_columns(q.nScan, q.Tp, d);
+                a.ncols = sweep_columns(items, q.Tp, d);
                 a.src = q.V + d * Np;
                 a.src_gs = 2 * d * Np;
                 a.acc = q.V + 2 * d * Np;
@@ -676,15 +732,16 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         }
         for (int l = Lmax - 1; l >= 0; --l) {
             std::vector<std::pair<int, LevelArgs>> ents;
-            for (int i : ls_) {
+            for (int i : lv) {
                 const Sys& q = sys_[i];
                 if (l >= q.levels) continue;
                 const long Np = q.Np, d = 1L << l;
+                const long items = q.resp ? q.nblocks : q.nScan;
                 LevelArgs a;
-                a.P = q.P + (long)l * Np * Np;
+                a.P = q.P + (long)(q.lev0 + l) * Np * Np;
                 a.ldp = Np;
                 a.Np = q.Np;
-                a.ncols = sweep_columns(q.nScan, q.Tp, d);
+                a.ncols = sweep_columns(items, q.Tp, d);
                 // in place: node prefix in slot g 2d - 1, right half's prefix
                 // replaces the left half's aggregate in slot g 2d + d - 1
                 a.src = q.V;
@@ -697,20 +754,63 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             }
             add_level(ls_down_, ents, l);
         }
+        // response GEMMs (FP64 tiled DMMA): the block aggregates into scan
+        // slots 0 .. Tp - 1 (zeros past the last block), then the outputs from
+        // [sample window; X_b], X_b = the scanned state in slot b - 1
+        std::vector<std::pair<int, LevelArgs>> agg, out;
+        for (int i : rs_) {
+            const Sys& q = sys_[i];
+            const long ld = q.Kpad + q.Np;
+            LevelArgs a;
+            a.P = q.Wm + (long)q.Bk * q.p * ld;
+            a.ldp = ld;
+            a.Np = q.Np;
+            a.M = q.Np;
+            a.K = q.Kpad;
+            a.ncols = q.Tp;
+            a.src_cols = q.nblocks;
+            a.src = q.U;
+            a.src_gs = (q.solver == kRK4 ? 2L : 1L) * q.Bk * q.mu;
+            a.src_ks = 1;
+            a.dst = q.V + q.Np;
+            a.dst_gs = q.Np;
+            a.dst_is = 1;
+            agg.push_back({i, a});
+            LevelArgs b = a;
+            b.P = q.Wm;
+            b.M = q.Bk * q.p;
+            b.K = (int)ld;
+            b.K1 = q.Kpad;
+            b.src2 = q.V;
+            b.src2_gs = q.Np;
+            b.ncols = q.nblocks;
+            b.src_cols = 0;
+            b.dst = q.Y + (q.solver == kRK4 ? 0L : 3L * q.p);
+            b.dst_gs = (long)q.Bk * q.p;
+            b.dst_limit = q.nScan * (long)q.p;
+            out.push_back({i, b});
+            if ((a.K & 1) || (b.K & 1) || (ld & 1) || (a.src_gs & 1))
+                throw Error(kInvalidArgument, "response GEMM shapes must be even");
+        }
+        if (!agg.empty()) {
+            add_level(rs_agg_, agg, -1);
+            add_level(rs_out_, out, -1);
+        }
     }
     // mixed: P_l - R_l of every tensor-core level, split once per execute
     // after the power table
     {
         std::vector<LevelArgs> sp;
-        for (int i : ls_) {
+        for (int i : lv) {
             const Sys& q = sys_[i];
             for (int l = 0; l < q.tc_levels; ++l) {
+                const int k = q.lev0 + l;
                 LevelArgs a;
-                a.P = q.P + (long)l * q.Np * q.Np;
+                a.P = q.P + (long)k * q.Np * q.Np;
                 a.ldp = q.Np;
                 a.Np = q.Np;
                 a.rn = q.solver == kRK4 ? 0 : q.n;
-                a.rsh = std::min(1 << std::min(l, 2), 3);
+                a.rsh = std::min(1 << std::min(k, 2), 3);
                 a.Ps = q.Ps + (size_t)l * (level_split_bytes(q.Np) / sizeof(float));
                 sp.push_back(a);
                 maxSplitNp_ = std::max(maxSplitNp_, q.Np);
@@ -746,16 +846,87 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
     if (J.bytes > arena_bytes_) throw Error(kDeviceError, "batch job arrays overflow the arena reservation");
 
     // ---- upload and set-up launches ------------------------------------------
+    // work buffers start zeroed (the response windows' sample padding relies on it)
+    if (!rs_.empty()) PARODE_CUDA(cudaMemsetAsync(base + const_end, 0, work_end - const_end, stream_));
     PARODE_CUDA(cudaMemcpyAsync(base, st.buf.data(), st.buf.size(), cudaMemcpyHostToDevice, stream_));
     PARODE_CUDA(cudaMemcpyAsync(base + work_end, jstage.data(), jstage.size(), cudaMemcpyHostToDevice, stream_));
     for (size_t k = 0; k < setup_copies.size(); k += 65535)
         launch_copy_batch(dSetup + k, (int)std::min<size_t>(65535, setup_copies.size() - k), max_copy, stream_);
-    const int nforks = (int)buckets_.size() + (ls_.empty() ? 0 : 1);
+    build_responses();
+    const int nforks = (int)buckets_.size() + (lv.empty() ? 0 : 1);
     forks_.resize(nforks, nullptr);
     for (auto& f : forks_) PARODE_CUDA(cudaStreamCreateWithFlags(&f, cudaStreamNonBlocking));
     events_.resize(nforks + 1, nullptr);
     for (auto& e : events_) PARODE_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     PARODE_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void BatchPlan::build_responses()
+{
+    // W of every response system from Phi (power-table level 0), Bbar, Cext
+    // and D, in groups whose table workspace stays under 1 GiB
+    const size_t cap = (size_t)1 << 30;
+    size_t k = 0;
+    while (k < rs_.size()) {
+        std::vector<ResponseArgs> ra;
+        size_t ws = 0;
+        int maxB = 0;
+        for (; k < rs_.size(); ++k) {
+            const Sys& q = sys_[rs_[k]];
+            const size_t need = sizeof(double) * (size_t)q.Bk * q.Np * ((size_t)q.p + q.n);
+            if (!ra.empty() && ws + need > cap) break;
+            ResponseArgs a;
+            a.solver = q.solver;
+            a.n = q.n;
+            a.m = q.mu;
+            a.p = q.p;
+            a.NP = q.Np;
+            a.B = q.Bk;
+            a.zeroB = q.zeroB;
+            a.zeroD = q.zeroD;
+            a.Phi = q.P;
+            a.Bbar = q.Bbar;
+            a.Cext = q.Cext;
+            a.D = q.D;
+            a.Wm = q.Wm;
+            a.K = q.Kw;
+            a.Kpad = q.Kpad;
+            a.NPstate = q.Np;
+            a.CPt = reinterpret_cast<double*>(ws);  // offsets for now
+            ra.push_back(a);
+            ws += need;
+            maxB = std::max(maxB, q.Bk);
+        }
+        const int nent = (int)ra.size();
+        std::vector<long> ts(nent), fs(nent);
+        long tctas = 0, fctas = 0;
+        for (int e = 0; e < nent; ++e) {
+            ts[e] = tctas;
+            fs[e] = fctas;
+            tctas += response_tables_ctas(ra[e]);
+            fctas += response_fill_ctas(ra[e]);
+        }
+        const size_t meta = align_up(sizeof(ResponseArgs) * nent) + 2 * align_up(sizeof(long) * nent);
+        char* buf = nullptr;
+        PARODE_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&buf), ws + meta, stream_));
+        for (ResponseArgs& a : ra) {
+            const size_t off = reinterpret_cast<size_t>(a.CPt);
+            a.CPt = reinterpret_cast<double*>(buf + off);
+            a.Qt = a.CPt + (size_t)a.B * a.p * a.NP;
+        }
+        char* mb = buf + ws;
+        ResponseArgs* dArgs = reinterpret_cast<ResponseArgs*>(mb);
+        long* dTs = reinterpret_cast<long*>(mb + align_up(sizeof(ResponseArgs) * nent));
+        long* dFs = reinterpret_cast<long*>(mb + align_up(sizeof(ResponseArgs) * nent) + align_up(sizeof(long) * nent));
+        PARODE_CUDA(cudaMemcpyAsync(dArgs, ra.data(), sizeof(ResponseArgs) * nent, cudaMemcpyHostToDevice, stream_));
+        PARODE_CUDA(cudaMemcpyAsync(dTs, ts.data(), sizeof(long) * nent, cudaMemcpyHostToDevice, stream_));
+        PARODE_CUDA(cudaMemcpyAsync(dFs, fs.data(), sizeof(long) * nent, cudaMemcpyHostToDevice, stream_));
+        for (int j = 0; j < maxB; ++j) launch_response_tables(dArgs, dTs, nent, tctas, j, stream_);
+        launch_response_fill(dArgs, dFs, nent, fctas, stream_);
+        PARODE_CUDA(cudaFreeAsync(buf, stream_));
+        // the host arrays above are read by the copies before they return
+        PARODE_CUDA(cudaStreamSynchronize(stream_));
+    }
 }
 
 BatchPlan::~BatchPlan()
@@ -809,12 +980,18 @@ void BatchPlan::execute(cudaStream_t s)
             ++launches;
         }
     }
-    if (!ls_.empty()) {
+    if (!ls_.empty() || !rs_.empty()) {
         cudaStream_t fs = forks_[f++];
         PARODE_CUDA(cudaStreamWaitEvent(fs, events_[0], 0));
         const int nls = (int)ls_.size();
-        launch_forcing_batch(dForcing_, nls, maxForcing_, fs);
-        ++launches;
+        if (nls > 0) {
+            launch_forcing_batch(dForcing_, nls, maxForcing_, fs);
+            ++launches;
+        }
+        for (const GroupedLaunch& g : rs_agg_) {
+            launch_grouped(g, fs);
+            ++launches;
+        }
         for (const GroupedLaunch& g : ls_power_) {
             launch_grouped(g, fs);
             ++launches;
@@ -827,7 +1004,7 @@ void BatchPlan::execute(cudaStream_t s)
             launch_grouped(g, fs);
             ++launches;
         }
-        launch_copy_batch(dSeed_, nls, maxSeed_, fs);
+        launch_copy_batch(dSeed_, nSeed_, maxSeed_, fs);
         ++launches;
         for (const GroupedLaunch& g : ls_down_) {
             if (g.nswap > 0) {
@@ -837,8 +1014,14 @@ void BatchPlan::execute(cudaStream_t s)
             launch_grouped(g, fs);
             ++launches;
         }
-        launch_output_batch(dOutput_, nls, maxOutput_, fs);
-        ++launches;
+        if (nls > 0) {
+            launch_output_batch(dOutput_, nls, maxOutput_, fs);
+            ++launches;
+        }
+        for (const GroupedLaunch& g : rs_out_) {
+            launch_grouped(g, fs);
+            ++launches;
+        }
     }
     // join
     for (int k = 0; k < f; ++k) {

@@ -8,7 +8,11 @@
 //    (one tables launch, one persistent leaf launch over work items of all
 //    systems, one chain launch, one fix-up launch per NP);
 //  - larger scan dimensions: the level-synchronous path with one grouped
-//    contraction launch per level and tiling configuration over all systems.
+//    contraction launch per level and tiling configuration over all systems;
+//  - systems with inputs where it costs less: the block-response leaf (one
+//    GEMM of W x [sample windows] per system for the block aggregates, the
+//    level-synchronous scan over the blocks, one GEMM for the outputs), the
+//    GEMMs of all such systems grouped into one launch each.
 // Inputs: sum-of-sinusoid inputs are sampled by one batched launch; user
 // (NVRTC) inputs by one launch per system.
 #pragma once
@@ -53,7 +57,10 @@ public:
     const double* device_output(int i) const { return sys_[i].Y; }
     int launch_count() const { return launches_; }
     int precision_used(int i) const { return sys_[i].precision; }
-    int path(int i) const { return sys_[i].blocked ? kPathBlocked : kPathLevel; }
+    int path(int i) const
+    {
+        return sys_[i].resp ? kPathBlockedResponse : sys_[i].blocked ? kPathBlocked : kPathLevel;
+    }
     // Sum over systems of n * outputs (state*steps of one execute).
     double state_steps() const;
     size_t device_bytes() const { return arena_bytes_; }
@@ -63,8 +70,14 @@ private:
     struct Sys {
         int solver = 0, n = 0, m = 0, mu = 0, p = 0, Ns = 0, Np = 0, W = 3;
         long nOut = 0, nScan = 0, nU = 0, Tp = 1;
-        int levels = 0;
+        int levels = 0;           // levels of the level-synchronous scan (over steps, or over blocks)
+        int lev0 = 0;             // power-table level of scan level 0 (log2 of the block length)
+        int pow_levels = 0;       // power-table levels P_0 .. P_{pow_levels - 1}
         bool blocked = false;
+        bool resp = false;        // block-response leaf
+        int Bk = 0, Kw = 0, Kpad = 0;  // response: block length, window columns (padded to even)
+        long nblocks = 0;
+        double* Wm = nullptr;     // response matrix: Bk p + Np rows of Kpad + Np
         int bucket = -1;          // blocked: index into buckets_
         double delta = 0;         // |Phi - R|_inf, R the exact 0/1 part (I or the ABM shift)
         int tc_levels = 0;        // mixed: lowest levels run on the tensor cores
@@ -104,6 +117,7 @@ private:
     };
 
     void launch_grouped(const GroupedLaunch& g, cudaStream_t s);
+    void build_responses();
 
     int device_ = 0;
     int sms_ = 148;
@@ -117,7 +131,9 @@ private:
     std::vector<Sys> sys_;
     std::vector<Bucket> buckets_;
     std::vector<int> ls_;  // level-synchronous systems
+    std::vector<int> rs_;  // block-response systems (their block scan joins the level launches)
     std::vector<GroupedLaunch> ls_power_, ls_up_, ls_down_;
+    std::vector<GroupedLaunch> rs_agg_, rs_out_;  // response GEMMs: block aggregates, outputs
     SampleJob* dSampleJobs_ = nullptr;
     int nSampleJobs_ = 0;
     long maxSample_ = 0;
@@ -125,6 +141,7 @@ private:
     ForcingJob* dForcing_ = nullptr;
     OutputJob* dOutput_ = nullptr;
     CopyJob* dSeed_ = nullptr;
+    int nSeed_ = 0;
     LevelArgs* dSplit_ = nullptr;  // mixed: P_l - R_l splits (one per system and tensor-core level)
     int nSplit_ = 0, maxSplitNp_ = 0;
     long maxForcing_ = 0, maxOutput_ = 0, maxSeed_ = 0;

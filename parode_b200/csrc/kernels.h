@@ -43,6 +43,9 @@ struct LevelArgs {
     int K1 = 0;
     const double* src2 = nullptr;
     long src2_gs = 0;
+    // Tiled kernel: columns g >= src_cols (> 0) read a zero source, so their
+    // results are acc or 0 (a zero padding written by the same launch).
+    long src_cols = 0;
 };
 
 __host__ __device__ inline int level_rows(const LevelArgs& a) { return a.M > 0 ? a.M : a.Np; }
@@ -68,10 +71,27 @@ struct ResponseArgs {
     double* Wm = nullptr;          // row stride Kpad + NPstate
     int K = 0, Kpad = 0;           // window columns, padded to even
     int NPstate = 0;               // NP: also the initial-state columns (z_0 = I on them), or 0
+    // launch_response_tables / launch_response_fill only: workspace of
+    // B p NP (CP_j = Cext Phi^j) and B NP n (Q_k = Phi^k restricted to the
+    // n forcing columns) doubles
+    double* CPt = nullptr;
+    double* Qt = nullptr;
 };
 // Window length (columns of W) for B steps: RK4 (2B + 1) m, ABM (B + 4) m.
 int response_window(int solver, int B, int m);
 void launch_block_response(const ResponseArgs* dArgs, int nsys, int max_np, int max_p, int max_kpad, cudaStream_t s);
+// The same W for any NP, over many systems.  dStart[e] is entry e's first CTA
+// (response_tables_ctas / response_fill_ctas CTAs each, `ctas` in total).
+// Tables: call with j = 0 .. maxB - 1 in order (step j from step j - 1);
+// then one fill.
+long response_tables_ctas(const ResponseArgs& a);
+long response_fill_ctas(const ResponseArgs& a);
+void launch_response_tables(const ResponseArgs* dArgs, const long* dStart, int nent, long ctas, int j,
+                            cudaStream_t s);
+void launch_response_fill(const ResponseArgs* dArgs, const long* dStart, int nent, long ctas, cudaStream_t s);
+// Block length 2^R of the response leaf for one system, and its cost in
+// flops per step (the two GEMMs and a level-synchronous carry over blocks).
+int response_log2_block(int solver, int NP, int m, int p, long nScan, double* flops_per_step);
 
 // Columns of a level that can reach an output.  Column g combines the
 // segments [g 2d, g 2d + d) and [g 2d + d, g 2d + 2d) of the time axis; when

@@ -94,11 +94,185 @@ __global__ void __launch_bounds__(kThreads) k_block_response(const ResponseArgs*
     }
 }
 
+// ---------------------------------------------------------------------------
+// W for any NP, many systems per launch.  By linearity
+//   y_j   = sum_{i<j} Cext Phi^(j-1-i) S_i (+ D u_j),   z_B = sum_{i<B} Phi^(B-1-i) S_i,
+// where S_i (the forcing of step i) is non-zero only on the n forcing rows
+// coff .. coff + n and reads samples i..i+4 (ABM) or 2i..2i+2 (RK4) through
+// the slots of Bbar.  So W needs only CP_k = Cext Phi^k (p x NP) and
+// Q_k = Phi^k restricted to the forcing columns (NP x n), k < B: B
+// row-times-matrix steps instead of B full NP x NP products.
+// ---------------------------------------------------------------------------
+
+constexpr int kPerThread = 4;
+constexpr int kPerCta = kThreads * kPerThread;
+
+__device__ __forceinline__ int find_entry(const long* __restrict__ start, int nent, long t)
+{
+    int lo = 0, hi = nent - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (start[mid] <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Step j of the tables: CP_j = CP_{j-1} Phi and Q_j = Phi Q_{j-1}
+// (j = 0: CP_0 = Cext, Q_0 = the identity's forcing columns).
+__global__ void __launch_bounds__(kThreads) k_response_tables(const ResponseArgs* __restrict__ args,
+                                                               const long* __restrict__ start, int nent, int j)
+{
+    const int e = find_entry(start, nent, blockIdx.x);
+    const ResponseArgs& a = args[e];
+    if (j >= a.B) return;
+    const int NP = a.NP, p = a.p, n = a.n;
+    const int coff = a.solver == 0 ? 0 : 3 * n;
+    const long ncp = (long)p * NP, total = ncp + (long)NP * n;
+    const double* __restrict__ Phi = a.Phi;
+    const double* __restrict__ cp_prev = a.CPt + (long)(j - 1) * ncp;
+    const double* __restrict__ q_prev = a.Qt + (long)(j - 1) * NP * n;
+    double* cp = a.CPt + (long)j * ncp;
+    double* q = a.Qt + (long)j * NP * n;
+    const long base = (blockIdx.x - start[e]) * (long)kPerCta + threadIdx.x;
+    for (int t = 0; t < kPerThread; ++t) {
+        const long idx = base + (long)t * kThreads;
+        if (idx >= total) break;
+        if (idx < ncp) {
+            const int o = (int)(idx / NP), c = (int)(idx - (long)o * NP);
+            double v;
+            if (j == 0) {
+                v = a.Cext[idx];
+            } else {
+                v = 0.0;
+                for (int r = 0; r < NP; ++r) v = fma(cp_prev[(long)o * NP + r], Phi[(long)r * NP + c], v);
+            }
+            cp[idx] = v;
+        } else {
+            const long u = idx - ncp;
+            const int r = (int)(u / n), c = (int)(u - (long)r * n);
+            double v;
+            if (j == 0) {
+                v = (r == coff + c) ? 1.0 : 0.0;
+            } else {
+                v = 0.0;
+                for (int s = 0; s < NP; ++s) v = fma(Phi[(long)r * NP + s], q_prev[(long)s * n + c], v);
+            }
+            q[u] = v;
+        }
+    }
+}
+
+// Every element of W from the tables.
+__global__ void __launch_bounds__(kThreads) k_response_fill(const ResponseArgs* __restrict__ args,
+                                                             const long* __restrict__ start, int nent)
+{
+    const int e = find_entry(start, nent, blockIdx.x);
+    const ResponseArgs& a = args[e];
+    const int NP = a.NP, p = a.p, n = a.n, m = a.m, B = a.B;
+    const bool rk4 = a.solver == 0;
+    const int W = rk4 ? 3 : 5;
+    const int coff = rk4 ? 0 : 3 * n;
+    const long ld = a.Kpad + a.NPstate;
+    const long total = ((long)B * p + NP) * ld;
+    const long ncp = (long)p * NP;
+    const long base = (blockIdx.x - start[e]) * (long)kPerCta + threadIdx.x;
+    for (int t = 0; t < kPerThread; ++t) {
+        const long idx = base + (long)t * kThreads;
+        if (idx >= total) break;
+        const long row = idx / ld;
+        const int col = (int)(idx - row * ld);
+        double v = 0.0;
+        if (col < a.K) {
+            const int s = col / m, c = col - s * m;
+            // steps i whose forcing reads sample s (slot w = s - 2i or s - i)
+            const int ilo = rk4 ? (s - 1) / 2 : s - 4;  // (s - 2 + 1) / 2 rounds up for s >= 1
+            const int ihi = rk4 ? s / 2 : s;
+            if (row < (long)B * p) {
+                const int j = (int)(row / p), o = (int)(row - (long)j * p);
+                if (!a.zeroB)
+                    for (int i = max(ilo, 0); i <= min(ihi, j - 1); ++i) {
+                        const int w = rk4 ? s - 2 * i : s - i;
+                        const double* cpr = a.CPt + (long)(j - 1 - i) * ncp + (long)o * NP + coff;
+                        const double* bb = a.Bbar + (long)w * m + c;
+                        for (int r = 0; r < n; ++r) v = fma(cpr[r], bb[(long)r * W * m], v);
+                    }
+                if (!a.zeroD && s == (rk4 ? 2 * j : j + 3)) v += a.D[(long)o * m + c];
+            } else {
+                const int r = (int)(row - (long)B * p);
+                if (!a.zeroB)
+                    for (int i = max(ilo, 0); i <= min(ihi, B - 1); ++i) {
+                        const int w = rk4 ? s - 2 * i : s - i;
+                        const double* qr = a.Qt + (long)(B - 1 - i) * NP * n + (long)r * n;
+                        const double* bb = a.Bbar + (long)w * m + c;
+                        for (int k = 0; k < n; ++k) v = fma(qr[k], bb[(long)k * W * m], v);
+                    }
+            }
+        } else if (col >= a.Kpad && row < (long)B * p) {
+            // initial-state columns of the output rows: Cext Phi^j
+            const int j = (int)(row / p), o = (int)(row - (long)j * p);
+            v = a.CPt[(long)j * ncp + (long)o * NP + (col - a.Kpad)];
+        }
+        a.Wm[idx] = v;
+    }
+}
+
 }  // namespace
 
 int response_window(int solver, int B, int m)
 {
     return (solver == 0 ? 2 * B + 1 : B + 4) * m;
+}
+
+long response_tables_ctas(const ResponseArgs& a)
+{
+    const long total = (long)a.p * a.NP + (long)a.NP * a.n;
+    return (total + kPerCta - 1) / kPerCta;
+}
+
+long response_fill_ctas(const ResponseArgs& a)
+{
+    const long total = ((long)a.B * a.p + a.NP) * (a.Kpad + a.NPstate);
+    return (total + kPerCta - 1) / kPerCta;
+}
+
+void launch_response_tables(const ResponseArgs* dArgs, const long* dStart, int nent, long ctas, int j, cudaStream_t s)
+{
+    if (nent <= 0 || ctas <= 0) return;
+    if (ctas > 0x7fffffffL) throw Error(kInvalidArgument, "response tables: grid too large");
+    k_response_tables<<<(unsigned)ctas, kThreads, 0, s>>>(dArgs, dStart, nent, j);
+    PARODE_CUDA(cudaGetLastError());
+}
+
+void launch_response_fill(const ResponseArgs* dArgs, const long* dStart, int nent, long ctas, cudaStream_t s)
+{
+    if (nent <= 0 || ctas <= 0) return;
+    if (ctas > 0x7fffffffL) throw Error(kInvalidArgument, "response fill: grid too large");
+    k_response_fill<<<(unsigned)ctas, kThreads, 0, s>>>(dArgs, dStart, nent);
+    PARODE_CUDA(cudaGetLastError());
+}
+
+int response_log2_block(int solver, int NP, int m, int p, long nScan, double* flops_per_step)
+{
+    // per block: aggregates 2 NP Kpad, outputs 2 B p (Kpad + NP), and about
+    // 6 NP^2 for the level-synchronous carry (up- and down-sweep, 4 NP^2,
+    // at a lower efficiency than the GEMMs)
+    int best = 2;
+    double best_cost = -1.0;
+    for (int R = 2; R <= 7; ++R) {
+        const long B = 1L << R;
+        if (R > 2 && B / 2 >= nScan) break;
+        const long K = response_window(solver, (int)B, m), Kp = (K + 1) & ~1L;
+        const double wbytes = 8.0 * ((double)B * p + NP) * ((double)Kp + NP);
+        if (R > 2 && wbytes > 256e6) break;
+        const double cost = (2.0 * NP * Kp + 2.0 * B * p * (double)(Kp + NP) + 6.0 * NP * NP) / B;
+        if (best_cost < 0 || cost < best_cost) {
+            best_cost = cost;
+            best = R;
+        }
+    }
+    if (flops_per_step) *flops_per_step = best_cost;
+    return best;
 }
 
 void launch_block_response(const ResponseArgs* dArgs, int nsys, int max_np, int max_p, int max_kpad, cudaStream_t s)

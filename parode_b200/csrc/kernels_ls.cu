@@ -161,6 +161,7 @@ __device__ void tiled_load(const LevelArgs& a, int m0, long n0, int k0, double* 
 {
     const int tid = threadIdx.x;
     const int rows = level_rows(a), K = level_k(a);  // K even: a 2-double chunk is wholly in or out
+    const long scols = a.src_cols > 0 ? a.src_cols : a.ncols;
     // A: 64 rows x 32 doubles = 1024 chunks of 16 bytes
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
@@ -178,7 +179,7 @@ __device__ void tiled_load(const LevelArgs& a, int m0, long n0, int k0, double* 
             const int col = c >> 4, kc = (c & 15) * 2;
             const long g = n0 + col;
             const int k = k0 + kc;
-            const bool ok = (g < a.ncols) && (k < K);
+            const bool ok = (g < scols) && (k < K);
             const double* src = !ok ? a.src
                                     : (a.K1 > 0 && k >= a.K1) ? a.src2 + g * a.src2_gs + (k - a.K1)
                                                               : a.src + g * a.src_gs + k;
@@ -191,7 +192,7 @@ __device__ void tiled_load(const LevelArgs& a, int m0, long n0, int k0, double* 
             const int c = tid + q * 256;
             const int kr = c >> 5, nc = (c & 31) * 2;
             const long g = n0 + nc;
-            const bool ok = (g < a.ncols) && (k0 + kr < K);
+            const bool ok = (g < scols) && (k0 + kr < K);
             const double* src = ok ? a.src + (long)(k0 + kr) * a.src_ks + g : a.src;
             cp_async16(sB + kr * kLdBn + nc, src, ok);
         }
@@ -210,7 +211,9 @@ __device__ void tiled_level_body(const LevelArgs& a, long tile, double* smem)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int wm = warp & 1, wn = warp >> 1;
     const int gq = lane >> 2, tq = lane & 3;
-    const int nk = (level_k(a) + kTK - 1) / kTK;
+    // a tile wholly beyond the source columns only writes acc (or zeros)
+    const long scols = a.src_cols > 0 ? a.src_cols : a.ncols;
+    const int nk = n0 >= scols ? 0 : (level_k(a) + kTK - 1) / kTK;
 
     double acc[4][2][2];
 #pragma unroll

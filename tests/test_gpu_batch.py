@@ -54,8 +54,9 @@ def _mix_cases():
     return out
 
 
-def test_batch_mixed_sizes_match_oracle(pb):
-    pb.set_option(pb.OPT_PATH, 0)
+@pytest.mark.parametrize("path", [0, 1, 3])
+def test_batch_mixed_sizes_match_oracle(pb, path):
+    pb.set_option(pb.OPT_PATH, path)
     cases = _mix_cases()
     batch = pb.Batch([_spec(pb, c, B, Cm, D) for c, B, Cm, D in cases], precision=pb.FP64)
     batch.execute()
@@ -65,10 +66,16 @@ def test_batch_mixed_sizes_match_oracle(pb):
         assert y.shape == ref.shape, (i, y.shape, ref.shape)
         err = oracle.rel_err(y, ref)
         assert err <= TOL_FP64, (i, MIX[i], err)
-    # paths: scan dimension <= 64 blocked, larger level-synchronous
+    # paths: 1 level-synchronous (forced), 3 block response (forced: every
+    # system here has inputs); automatic: scan dimension <= 64 blocked or
+    # block response, larger level-synchronous or block response
     paths = [batch.path(i) for i in range(len(cases))]
     for i, (c, *_rest) in enumerate(cases):
-        assert paths[i] == (2 if c.scan_dim <= 64 else 1), (i, paths[i])
+        if path in (1, 3):
+            assert paths[i] == path, (i, paths[i])
+        else:
+            assert paths[i] in ((2, 3) if c.scan_dim <= 64 else (1, 3)), (i, paths[i])
+    pb.set_option(pb.OPT_PATH, 0)
     batch.close()
 
 
@@ -121,16 +128,46 @@ MIXED_LS = [  # level-synchronous systems (scan dimension > 64): tensor-core lev
 ]
 
 
-def test_batch_mixed_level_synchronous(pb):
-    pb.set_option(pb.OPT_PATH, 0)
+@pytest.mark.parametrize("path", [1, 3])
+def test_batch_mixed_level_synchronous(pb, path):
+    """Mixed form: the level-synchronous scan over steps (path 1) or over the
+    blocks of the response leaf (path 3), lower levels on the tensor cores."""
+    pb.set_option(pb.OPT_PATH, path)
     cases = [wl.small(9100 + 7 * k, s, n, m, p, T, h=1e-3) for k, (s, n, m, p, T) in enumerate(MIXED_LS)]
     batch = pb.Batch([_spec(pb, c) for c in cases], precision=pb.MIXED)
     batch.execute()
+    pb.set_option(pb.OPT_PATH, 0)
     for i, c in enumerate(cases):
-        assert batch.path(i) == 1 and batch.precision(i) == pb.MIXED, i
+        assert batch.path(i) == path and batch.precision(i) == pb.MIXED, i
         _, y = batch.output(i)
         err = oracle.rel_err(y, _oracle_y(c))
         assert err <= TOL_MIXED, (i, MIXED_LS[i], err)
+    batch.close()
+
+
+RESPONSE = [  # (solver, n, m, p, T, B, C, D): block-response systems, FP64
+    (1, 128, 16, 16, 3000, True, True, True),   # ABM N_s 512 (the n=128 workload's shape)
+    (0, 200, 12, 9, 2100, True, True, True),    # RK4 N_s 200
+    (1, 24, 3, 5, 777, False, True, True),      # no B: D only
+    (0, 17, 1, 1, 65, True, False, False),      # y = x, T below two blocks
+    (1, 7, 2, 3, 4, True, True, True),          # ABM, one scan step
+    (0, 64, 8, 8, 5000, True, True, True),      # the n=64 RK4 workload's shape
+]
+
+
+def test_batch_response_leaf_matches_oracle(pb):
+    pb.set_option(pb.OPT_PATH, 3)
+    cases = [(wl.small(9300 + 11 * k, s, n, m, p, T, h=1e-3), B, Cm, D)
+             for k, (s, n, m, p, T, B, Cm, D) in enumerate(RESPONSE)]
+    batch = pb.Batch([_spec(pb, c, B, Cm, D) for c, B, Cm, D in cases], precision=pb.FP64)
+    batch.execute()
+    batch.execute()  # repeat: the block scan's padding is rewritten every execute
+    pb.set_option(pb.OPT_PATH, 0)
+    for i, (c, B, Cm, D) in enumerate(cases):
+        assert batch.path(i) == 3, i
+        _, y = batch.output(i)
+        err = oracle.rel_err(y, _oracle_y(c, B, Cm, D))
+        assert err <= TOL_FP64, (i, RESPONSE[i], err)
     batch.close()
 
 
