@@ -556,6 +556,7 @@ ParODE_Batch* ParODE_BatchCreate(int nSystems, const double* const A[], const do
         opt.precision = precision;
         opt.path = L.path;
         opt.input_double = true;
+        opt.log = L.log != 0;
         auto h = std::make_unique<ParODE_Batch>();
         h->batch = std::make_unique<BatchPlan>(dev, std::move(specs), &L.inputs, opt);
         out = h.release();

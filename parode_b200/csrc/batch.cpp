@@ -5,7 +5,9 @@
 #include "common.h"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <thread>
 
@@ -84,6 +86,18 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
     PARODE_CUDA(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_));
     const int N = (int)specs.size();
     sys_.resize(N);
+    // set-up phase times (PARODE_OPT_LOG)
+    auto clock0 = std::chrono::steady_clock::now();
+    std::string phases;
+    auto phase = [&](const char* name, bool device) {
+        if (!opt.log) return;
+        if (device && stream_) PARODE_CUDA(cudaStreamSynchronize(stream_));
+        const auto now = std::chrono::steady_clock::now();
+        char b[64];
+        std::snprintf(b, sizeof b, " %s %.1f ms", name, std::chrono::duration<double, std::milli>(now - clock0).count());
+        phases += b;
+        clock0 = now;
+    };
 
     // ---- classification and sizes ----------------------------------------
     for (int i = 0; i < N; ++i) {
@@ -202,6 +216,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         }
     }
 
+    phase("classify", false);
     // ---- host FP64 discretisation (threads over systems) --------------------
     std::vector<std::vector<double>> Phi(N), Bbar(N), X0(N), Ypre(N);
     parallel_for(N, [&](int i) {
@@ -232,6 +247,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             for (int r = 0; r < q.n; ++r) X0[i][r] = s.x0[r];
         }
     });
+    phase("discretise", false);
     // ABM start-up: nine inputs at t0 + j h/2 (sinusoids on the host; user
     // functions through their compiled kernel)
     for (int i = 0; i < N; ++i) {
@@ -276,6 +292,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         }
     }
 
+    phase("abm-start-up", false);
     // ---- arena layout: constants (staged) first, then work buffers ----------
     Layout L;
     Stage st;
@@ -432,6 +449,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         if (q.mu > 0 && q.input->kind == InputEntry::kSinusoid) q.sin = dp(o.sin);
     }
 
+    phase("layout+arena", true);
     // ---- job arrays (staged after the work region) ----------------------------
     Layout J;
     J.bytes = work_end;
@@ -845,6 +863,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         reinterpret_cast<const CopyJob*>(base + jput(setup_copies.data(), sizeof(CopyJob) * setup_copies.size()));
     if (J.bytes > arena_bytes_) throw Error(kDeviceError, "batch job arrays overflow the arena reservation");
 
+    phase("jobs", false);
     // ---- upload and set-up launches ------------------------------------------
     // work buffers start zeroed (the response windows' sample padding relies on it)
     if (!rs_.empty()) PARODE_CUDA(cudaMemsetAsync(base + const_end, 0, work_end - const_end, stream_));
@@ -852,13 +871,26 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
     PARODE_CUDA(cudaMemcpyAsync(base + work_end, jstage.data(), jstage.size(), cudaMemcpyHostToDevice, stream_));
     for (size_t k = 0; k < setup_copies.size(); k += 65535)
         launch_copy_batch(dSetup + k, (int)std::min<size_t>(65535, setup_copies.size() - k), max_copy, stream_);
+    phase("upload", true);
     build_responses();
+    phase("responses", true);
+    // the power table P_l = Phi^(2^l) and, in the mixed form, the splits of
+    // its tensor-core levels depend on Phi alone: formed here with Phi, once
+    // per batch, like the rest of the discretisation
+    for (const Bucket& bk : buckets_) launch_batch_stage(0, bk.sh, bk.launch, stream_);
+    for (const GroupedLaunch& g : ls_power_) launch_grouped(g, stream_);
+    for (int k = 0; k < nSplit_; k += 65535)
+        launch_level_split(dSplit_ + k, std::min(65535, nSplit_ - k), maxSplitNp_, stream_);
     const int nforks = (int)buckets_.size() + (lv.empty() ? 0 : 1);
     forks_.resize(nforks, nullptr);
     for (auto& f : forks_) PARODE_CUDA(cudaStreamCreateWithFlags(&f, cudaStreamNonBlocking));
     events_.resize(nforks + 1, nullptr);
     for (auto& e : events_) PARODE_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     PARODE_CUDA(cudaStreamSynchronize(stream_));
+    phase("tables", true);
+    if (opt.log)
+        std::fprintf(stderr, "ParODE batch set-up (%d systems, %zu response, %zu level, %zu buckets, %.2f GB):%s\n", N,
+                     rs_.size(), ls_.size(), buckets_.size(), arena_bytes_ / 1e9, phases.c_str());
 }
 
 void BatchPlan::build_responses()
@@ -975,7 +1007,7 @@ void BatchPlan::execute(cudaStream_t s)
     for (Bucket& bk : buckets_) {
         cudaStream_t fs = forks_[f++];
         PARODE_CUDA(cudaStreamWaitEvent(fs, events_[0], 0));
-        for (int stage = 0; stage < 4; ++stage) {
+        for (int stage = 1; stage < 4; ++stage) {
             launch_batch_stage(stage, bk.sh, bk.launch, fs);
             ++launches;
         }
@@ -990,14 +1022,6 @@ void BatchPlan::execute(cudaStream_t s)
         }
         for (const GroupedLaunch& g : rs_agg_) {
             launch_grouped(g, fs);
-            ++launches;
-        }
-        for (const GroupedLaunch& g : ls_power_) {
-            launch_grouped(g, fs);
-            ++launches;
-        }
-        for (int k = 0; k < nSplit_; k += 65535) {
-            launch_level_split(dSplit_ + k, std::min(65535, nSplit_ - k), maxSplitNp_, fs);
             ++launches;
         }
         for (const GroupedLaunch& g : ls_up_) {

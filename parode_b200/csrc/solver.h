@@ -26,6 +26,7 @@ struct PlanOptions {
     int precision = 0;  // Precision
     int path = kPathAuto;
     bool input_double = true;  // fType of a user input function: double (true) or float
+    bool log = false;          // set-up phase times on stderr
 };
 
 class Plan {
