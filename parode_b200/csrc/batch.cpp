@@ -152,9 +152,14 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         if (q.mu > 0 && opt.path != kPathLevel && opt.path != kPathBlockedSweep) {
             const int np = (int)round_up(q.Ns, 8);
             double cost = 0.0;
-            const int R = response_log2_block(q.solver, np, q.mu, q.p, q.nScan, &cost);
+            // mixed: the window and aggregate products run on the tensor cores
+            const double wweight = opt.precision == kMixed ? 0.25 : 1.0;
+            const int R = response_log2_block(q.solver, np, q.mu, q.p, q.nScan, wweight, &cost);
             const double sweeps = 4.0 * np * np;
-            if (opt.path == kPathBlockedResponse || cost < (can_block ? 0.5 : 1.0) * sweeps) {
+            // a blocked bucket chains its tiles one after another: long
+            // horizons go to the response leaf's level-synchronous block scan
+            const bool long_chain = can_block && q.nScan >= (1L << 15);
+            if (opt.path == kPathBlockedResponse || long_chain || cost < (can_block ? 0.5 : 1.0) * sweeps) {
                 if (np > 1024) throw Error(kInvalidSystem, "scan dimension above 1024 is not supported");
                 q.resp = true;
                 q.Np = np;
@@ -165,7 +170,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
                 q.nblocks = (q.nScan + q.Bk - 1) / q.Bk;
                 q.Tp = next_pow2(q.nblocks);
                 q.levels = ilog2(q.Tp);
-                q.pow_levels = q.levels > 0 ? R + q.levels : 1;
+                q.pow_levels = R + q.levels;  // P_0 .. P_{R-1} also double W's tables
                 rs_.push_back(i);
             }
         }
@@ -299,7 +304,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
     struct Off {
         size_t phi0, bbar, c, d, cext, x0, sin, ypre;
         size_t bbarT, cT, dT;  // level-synchronous systems: transposed copies (coalesced per-row kernels)
-        size_t P, U, Y, V, G, CP, Ps, W;
+        size_t P, U, Y, V, G, CP, Ps, W, Psa, Psw;
     };
     std::vector<Off> off(N);
     for (int i = 0; i < N; ++i) {
@@ -373,6 +378,11 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             }
             o.Ps = q.tc_levels > 0 ? L.take(level_split_bytes(q.Np) * (size_t)q.tc_levels) : 0;
             if (q.resp) o.W = L.take(sizeof(double) * ((size_t)q.Bk * q.p + q.Np) * ((size_t)q.Kpad + q.Np));
+            if (q.resp && q.precision == kMixed) {
+                q.resp_tc = true;
+                o.Psa = L.take(gemm_split_bytes(q.Np, q.Kw));
+                o.Psw = L.take(gemm_split_bytes(q.Bk * q.p, q.Kw));
+            }
         }
         // the response GEMMs read whole sample windows: the last block's
         // window runs past the samples into a zero padding
@@ -444,6 +454,10 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             if (q.resp) {
                 q.Cext = dp(o.cext);
                 q.Wm = dp(o.W);
+            }
+            if (q.resp_tc) {
+                q.Psa = reinterpret_cast<float*>(base + o.Psa);
+                q.Psw = reinterpret_cast<float*>(base + o.Psw);
             }
         }
         if (q.mu > 0 && q.input->kind == InputEntry::kSinusoid) q.sin = dp(o.sin);
@@ -617,6 +631,31 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         dSeed_ = reinterpret_cast<CopyJob*>(base + jput(cj.data(), sizeof(CopyJob) * cj.size()));
         nSeed_ = (int)cj.size();
         // grouped level launches: for each level, entries grouped by tiling config
+        // one persistent tensor-core launch over the entries' tiles
+        auto make_tc = [&](std::vector<LevelArgs>& tc) {
+            // TMA tensor maps of the entries' source columns (128 bytes each)
+            std::vector<unsigned char> maps(tc.size() * 128);
+            for (size_t k = 0; k < tc.size(); ++k) level_encode_src_map(tc[k], &maps[k * 128]);
+            const size_t moff = jput(maps.data(), maps.size());
+            for (size_t k = 0; k < tc.size(); ++k) tc[k].src_map = base + moff + k * 128;
+            GroupedLaunch gl;
+            gl.cfg.id = kTcConfig;
+            std::vector<long> start;
+            long tiles = 0;
+            for (const LevelArgs& a : tc) {
+                start.push_back(tiles);
+                tiles += level_tc_tiles(a);
+            }
+            gl.nent = (int)tc.size();
+            gl.tiles = tiles;
+            gl.args = reinterpret_cast<LevelArgs*>(base + jput(tc.data(), sizeof(LevelArgs) * tc.size()));
+            gl.start = reinterpret_cast<long*>(base + jput(start.data(), sizeof(long) * start.size()));
+            // one persistent CTA per SM, tile ranges balanced by work
+            gl.ctas = (int)std::min<long>(sms_, tiles);
+            std::vector<long> r = level_tc_ranges(tc, gl.ctas);
+            gl.cta = reinterpret_cast<long*>(base + jput(r.data(), sizeof(long) * r.size()));
+            return gl;
+        };
         auto add_level = [&](std::vector<GroupedLaunch>& out, const std::vector<std::pair<int, LevelArgs>>& ents,
                              int l) {
             // group by (config id, CW); entries keep the original form for the
@@ -680,30 +719,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
                 }
                 out.push_back(gl);
             }
-            if (!tc.empty()) {
-                // TMA tensor maps of the entries' source columns (128 bytes each)
-                std::vector<unsigned char> maps(tc.size() * 128);
-                for (size_t k = 0; k < tc.size(); ++k) level_encode_src_map(tc[k], &maps[k * 128]);
-                const size_t moff = jput(maps.data(), maps.size());
-                for (size_t k = 0; k < tc.size(); ++k) tc[k].src_map = base + moff + k * 128;
-                GroupedLaunch gl;
-                gl.cfg.id = kTcConfig;
-                std::vector<long> start;
-                long tiles = 0;
-                for (const LevelArgs& a : tc) {
-                    start.push_back(tiles);
-                    tiles += level_tc_tiles(a);
-                }
-                gl.nent = (int)tc.size();
-                gl.tiles = tiles;
-                gl.args = reinterpret_cast<LevelArgs*>(base + jput(tc.data(), sizeof(LevelArgs) * tc.size()));
-                gl.start = reinterpret_cast<long*>(base + jput(start.data(), sizeof(long) * start.size()));
-                // one persistent CTA per SM, tile ranges balanced by work
-                gl.ctas = (int)std::min<long>(sms_, tiles);
-                std::vector<long> r = level_tc_ranges(tc, gl.ctas);
-                gl.cta = reinterpret_cast<long*>(base + jput(r.data(), sizeof(long) * r.size()));
-                out.push_back(gl);
-            }
+            if (!tc.empty()) out.push_back(make_tc(tc));
         };
         for (int l = 1; l < Pmax; ++l) {
             std::vector<std::pair<int, LevelArgs>> ents;
@@ -775,10 +791,65 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         // response GEMMs (FP64 tiled DMMA): the block aggregates into scan
         // slots 0 .. Tp - 1 (zeros past the last block), then the outputs from
         // [sample window; X_b], X_b = the scanned state in slot b - 1
-        std::vector<std::pair<int, LevelArgs>> agg, out;
+        std::vector<std::pair<int, LevelArgs>> agg, out, state;
+        std::vector<LevelArgs> tcg;
+        std::vector<CopyJob> zero;
         for (int i : rs_) {
             const Sys& q = sys_[i];
             const long ld = q.Kpad + q.Np;
+            if (q.resp_tc) {
+                // mixed: the aggregates and the window part of the outputs on
+                // the tensor cores (3xTF32, W pre-split at set-up); the
+                // initial-state part C Phi^j X_b of the outputs stays FP64
+                LevelArgs a;
+                a.P = q.Wm + (long)q.Bk * q.p * ld;
+                a.ldp = ld;
+                a.Np = q.Np;
+                a.M = q.Np;
+                a.K = q.Kw;
+                a.ncols = q.nblocks;
+                a.src = q.U;
+                a.src_gs = (q.solver == kRK4 ? 2L : 1L) * q.Bk * q.mu;
+                a.src_ks = 1;
+                a.dst = q.V + q.Np;
+                a.dst_gs = q.Np;
+                a.Ps = q.Psa;
+                LevelArgs w = a;
+                w.P = q.Wm;
+                w.M = q.Bk * q.p;
+                w.dst = q.Y + (q.solver == kRK4 ? 0L : 3L * q.p);
+                w.dst_gs = (long)q.Bk * q.p;
+                w.dst_limit = q.nScan * (long)q.p;
+                w.Ps = q.Psw;
+                if (!level_tc_supported(a) || !level_tc_supported(w))
+                    throw Error(kInvalidArgument, "response GEMM not supported by the tensor-core kernel");
+                tcg.push_back(a);
+                tcg.push_back(w);
+                LevelArgs x;
+                x.P = q.Wm + q.Kpad;
+                x.ldp = ld;
+                x.Np = q.Np;
+                x.M = q.Bk * q.p;
+                x.K = q.Np;
+                x.ncols = q.nblocks;
+                x.src = q.V;
+                x.src_gs = q.Np;
+                x.src_ks = 1;
+                x.acc = w.dst;
+                x.acc_gs = w.dst_gs;
+                x.dst = w.dst;
+                x.dst_gs = w.dst_gs;
+                x.dst_limit = w.dst_limit;
+                state.push_back({i, x});
+                if (q.Tp > q.nblocks) {
+                    CopyJob z;
+                    z.dst = q.V + (1 + q.nblocks) * (long)q.Np;
+                    z.N = (q.Tp - q.nblocks) * (long)q.Np;
+                    zero.push_back(z);
+                    maxZero_ = std::max(maxZero_, z.N);
+                }
+                continue;
+            }
             LevelArgs a;
             a.P = q.Wm + (long)q.Bk * q.p * ld;
             a.ldp = ld;
@@ -814,6 +885,12 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             add_level(rs_agg_, agg, -1);
             add_level(rs_out_, out, -1);
         }
+        if (!tcg.empty()) {
+            rs_tc_.push_back(make_tc(tcg));
+            add_level(rs_state_, state, -1);
+        }
+        nZero_ = (int)zero.size();
+        if (nZero_ > 0) dZero_ = reinterpret_cast<CopyJob*>(base + jput(zero.data(), sizeof(CopyJob) * zero.size()));
     }
     // mixed: P_l - R_l of every tensor-core level, split once per execute
     // after the power table
@@ -831,8 +908,27 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
                 a.rsh = std::min(1 << std::min(k, 2), 3);
                 a.Ps = q.Ps + (size_t)l * (level_split_bytes(q.Np) / sizeof(float));
                 sp.push_back(a);
-                maxSplitNp_ = std::max(maxSplitNp_, q.Np);
+                maxSplitElems_ = std::max<long>(maxSplitElems_, (long)level_split_bytes(q.Np) / 8);
             }
+        }
+        for (int i : rs_) {
+            const Sys& q = sys_[i];
+            if (!q.resp_tc) continue;
+            const long ld = q.Kpad + q.Np;
+            LevelArgs a;
+            a.P = q.Wm + (long)q.Bk * q.p * ld;
+            a.ldp = ld;
+            a.Np = q.Np;
+            a.M = q.Np;
+            a.K = q.Kw;
+            a.Ps = q.Psa;
+            sp.push_back(a);
+            maxSplitElems_ = std::max<long>(maxSplitElems_, (long)gemm_split_bytes(a.M, a.K) / 8);
+            a.P = q.Wm;
+            a.M = q.Bk * q.p;
+            a.Ps = q.Psw;
+            sp.push_back(a);
+            maxSplitElems_ = std::max<long>(maxSplitElems_, (long)gemm_split_bytes(a.M, a.K) / 8);
         }
         nSplit_ = (int)sp.size();
         if (nSplit_ > 0) dSplit_ = reinterpret_cast<LevelArgs*>(base + jput(sp.data(), sizeof(LevelArgs) * sp.size()));
@@ -872,22 +968,23 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
     for (size_t k = 0; k < setup_copies.size(); k += 65535)
         launch_copy_batch(dSetup + k, (int)std::min<size_t>(65535, setup_copies.size() - k), max_copy, stream_);
     phase("upload", true);
-    build_responses();
-    phase("responses", true);
-    // the power table P_l = Phi^(2^l) and, in the mixed form, the splits of
-    // its tensor-core levels depend on Phi alone: formed here with Phi, once
-    // per batch, like the rest of the discretisation
+    // the power table P_l = Phi^(2^l), the response matrices and, in the
+    // mixed form, the splits of the tensor-core operands depend on Phi alone:
+    // formed here with Phi, once per batch, like the rest of the discretisation
     for (const Bucket& bk : buckets_) launch_batch_stage(0, bk.sh, bk.launch, stream_);
     for (const GroupedLaunch& g : ls_power_) launch_grouped(g, stream_);
+    phase("power-tables", true);
+    build_responses();
+    phase("responses", true);
     for (int k = 0; k < nSplit_; k += 65535)
-        launch_level_split(dSplit_ + k, std::min(65535, nSplit_ - k), maxSplitNp_, stream_);
+        launch_level_split(dSplit_ + k, std::min(65535, nSplit_ - k), maxSplitElems_, stream_);
     const int nforks = (int)buckets_.size() + (lv.empty() ? 0 : 1);
     forks_.resize(nforks, nullptr);
     for (auto& f : forks_) PARODE_CUDA(cudaStreamCreateWithFlags(&f, cudaStreamNonBlocking));
     events_.resize(nforks + 1, nullptr);
     for (auto& e : events_) PARODE_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     PARODE_CUDA(cudaStreamSynchronize(stream_));
-    phase("tables", true);
+    phase("splits", true);
     if (opt.log)
         std::fprintf(stderr, "ParODE batch set-up (%d systems, %zu response, %zu level, %zu buckets, %.2f GB):%s\n", N,
                      rs_.size(), ls_.size(), buckets_.size(), arena_bytes_ / 1e9, phases.c_str());
@@ -895,14 +992,15 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
 
 void BatchPlan::build_responses()
 {
-    // W of every response system from Phi (power-table level 0), Bbar, Cext
-    // and D, in groups whose table workspace stays under 1 GiB
+    // W of every response system from Phi, its power table, Bbar, Cext and
+    // D, in groups whose table workspace stays under 1 GiB
     const size_t cap = (size_t)1 << 30;
     size_t k = 0;
     while (k < rs_.size()) {
         std::vector<ResponseArgs> ra;
+        std::vector<const double*> pow;
         size_t ws = 0;
-        int maxB = 0;
+        int maxR = 0;
         for (; k < rs_.size(); ++k) {
             const Sys& q = sys_[rs_[k]];
             const size_t need = sizeof(double) * (size_t)q.Bk * q.Np * ((size_t)q.p + q.n);
@@ -924,39 +1022,82 @@ void BatchPlan::build_responses()
             a.K = q.Kw;
             a.Kpad = q.Kpad;
             a.NPstate = q.Np;
-            a.CPt = reinterpret_cast<double*>(ws);  // offsets for now
+            a.CPt = reinterpret_cast<double*>(ws);  // offsets until the workspace exists
             ra.push_back(a);
+            pow.push_back(q.P);
             ws += need;
-            maxB = std::max(maxB, q.Bk);
+            maxR = std::max(maxR, q.lev0);
         }
         const int nent = (int)ra.size();
-        std::vector<long> ts(nent), fs(nent);
-        long tctas = 0, fctas = 0;
-        for (int e = 0; e < nent; ++e) {
-            ts[e] = tctas;
-            fs[e] = fctas;
-            tctas += response_tables_ctas(ra[e]);
-            fctas += response_fill_ctas(ra[e]);
-        }
-        const size_t meta = align_up(sizeof(ResponseArgs) * nent) + 2 * align_up(sizeof(long) * nent);
         char* buf = nullptr;
+        // meta: the entries, their CTA starts, and per doubling step the GEMM
+        // arguments and tile starts
+        const size_t meta = align_up(sizeof(ResponseArgs) * nent) + 2 * align_up(sizeof(long) * nent) +
+                            (size_t)maxR * (align_up(2 * sizeof(LevelArgs) * nent) + align_up(2 * sizeof(long) * nent));
         PARODE_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&buf), ws + meta, stream_));
         for (ResponseArgs& a : ra) {
             const size_t off = reinterpret_cast<size_t>(a.CPt);
             a.CPt = reinterpret_cast<double*>(buf + off);
             a.Qt = a.CPt + (size_t)a.B * a.p * a.NP;
         }
-        char* mb = buf + ws;
-        ResponseArgs* dArgs = reinterpret_cast<ResponseArgs*>(mb);
-        long* dTs = reinterpret_cast<long*>(mb + align_up(sizeof(ResponseArgs) * nent));
-        long* dFs = reinterpret_cast<long*>(mb + align_up(sizeof(ResponseArgs) * nent) + align_up(sizeof(long) * nent));
-        PARODE_CUDA(cudaMemcpyAsync(dArgs, ra.data(), sizeof(ResponseArgs) * nent, cudaMemcpyHostToDevice, stream_));
-        PARODE_CUDA(cudaMemcpyAsync(dTs, ts.data(), sizeof(long) * nent, cudaMemcpyHostToDevice, stream_));
-        PARODE_CUDA(cudaMemcpyAsync(dFs, fs.data(), sizeof(long) * nent, cudaMemcpyHostToDevice, stream_));
-        for (int j = 0; j < maxB; ++j) launch_response_tables(dArgs, dTs, nent, tctas, j, stream_);
+        std::vector<long> is(nent), fs(nent);
+        long ictas = 0, fctas = 0;
+        for (int e = 0; e < nent; ++e) {
+            is[e] = ictas;
+            fs[e] = fctas;
+            ictas += response_init_ctas(ra[e]);
+            fctas += response_fill_ctas(ra[e]);
+        }
+        // host image of the meta region
+        std::vector<char> img(meta, 0);
+        size_t at = 0;
+        auto put = [&](const void* src, size_t n) {
+            const size_t o = at;
+            std::memcpy(img.data() + o, src, n);
+            at = align_up(at + std::max<size_t>(n, 1));
+            return buf + ws + o;
+        };
+        const ResponseArgs* dArgs = reinterpret_cast<const ResponseArgs*>(put(ra.data(), sizeof(ResponseArgs) * nent));
+        const long* dIs = reinterpret_cast<const long*>(put(is.data(), sizeof(long) * nent));
+        const long* dFs = reinterpret_cast<const long*>(put(fs.data(), sizeof(long) * nent));
+        struct Step {
+            LevelConfig cfg;
+            const LevelArgs* args;
+            const long* start;
+            int nent;
+            long tiles;
+        };
+        std::vector<Step> steps;
+        for (int l = 0; l < maxR; ++l) {
+            std::vector<LevelArgs> ents;
+            for (int e = 0; e < nent; ++e) {
+                LevelArgs two[2];
+                const int c = response_doubling_args(ra[e], pow[e], l, two);
+                for (int q = 0; q < c; ++q) ents.push_back(level_grouped_args(two[q]));
+            }
+            if (ents.empty()) continue;
+            Step st;
+            st.cfg = level_config(ents[0]);
+            std::vector<long> start;
+            long tiles = 0;
+            for (const LevelArgs& a : ents) {
+                if (level_config(a).id != st.cfg.id) throw Error(kDeviceError, "response tables: mixed tilings");
+                start.push_back(tiles);
+                tiles += level_tiles(st.cfg, a);
+            }
+            st.nent = (int)ents.size();
+            st.tiles = tiles;
+            st.args = reinterpret_cast<const LevelArgs*>(put(ents.data(), sizeof(LevelArgs) * ents.size()));
+            st.start = reinterpret_cast<const long*>(put(start.data(), sizeof(long) * start.size()));
+            steps.push_back(st);
+        }
+        PARODE_CUDA(cudaMemcpyAsync(buf + ws, img.data(), meta, cudaMemcpyHostToDevice, stream_));
+        launch_response_init(dArgs, dIs, nent, ictas, stream_);
+        for (const Step& st : steps)
+            launch_affine_level_grouped(st.cfg, st.args, st.start, st.nent, st.tiles, st.cfg.smem, stream_);
         launch_response_fill(dArgs, dFs, nent, fctas, stream_);
         PARODE_CUDA(cudaFreeAsync(buf, stream_));
-        // the host arrays above are read by the copies before they return
+        // the host image above is read by the copy before it is released
         PARODE_CUDA(cudaStreamSynchronize(stream_));
     }
 }
@@ -1024,6 +1165,16 @@ void BatchPlan::execute(cudaStream_t s)
             launch_grouped(g, fs);
             ++launches;
         }
+        for (const GroupedLaunch& g : rs_tc_) {
+            launch_grouped(g, fs);
+            ++launches;
+        }
+        if (nZero_ > 0) {
+            for (int k = 0; k < nZero_; k += 65535) {
+                launch_copy_batch(dZero_ + k, std::min(65535, nZero_ - k), maxZero_, fs);
+                ++launches;
+            }
+        }
         for (const GroupedLaunch& g : ls_up_) {
             launch_grouped(g, fs);
             ++launches;
@@ -1043,6 +1194,10 @@ void BatchPlan::execute(cudaStream_t s)
             ++launches;
         }
         for (const GroupedLaunch& g : rs_out_) {
+            launch_grouped(g, fs);
+            ++launches;
+        }
+        for (const GroupedLaunch& g : rs_state_) {
             launch_grouped(g, fs);
             ++launches;
         }

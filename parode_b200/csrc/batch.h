@@ -78,6 +78,9 @@ private:
         int Bk = 0, Kw = 0, Kpad = 0;  // response: block length, window columns (padded to even)
         long nblocks = 0;
         double* Wm = nullptr;     // response matrix: Bk p + Np rows of Kpad + Np
+        bool resp_tc = false;     // mixed: response GEMMs on the tensor cores
+        float* Psa = nullptr;     // W's aggregate rows, TF32-split
+        float* Psw = nullptr;     // W's output rows (window columns), TF32-split
         int bucket = -1;          // blocked: index into buckets_
         double delta = 0;         // |Phi - R|_inf, R the exact 0/1 part (I or the ABM shift)
         int tc_levels = 0;        // mixed: lowest levels run on the tensor cores
@@ -134,6 +137,10 @@ private:
     std::vector<int> rs_;  // block-response systems (their block scan joins the level launches)
     std::vector<GroupedLaunch> ls_power_, ls_up_, ls_down_;
     std::vector<GroupedLaunch> rs_agg_, rs_out_;  // response GEMMs: block aggregates, outputs
+    std::vector<GroupedLaunch> rs_tc_, rs_state_;  // mixed: tensor-core aggregates + windows; FP64 state part
+    CopyJob* dZero_ = nullptr;                     // mixed: the block scans' padding slots
+    int nZero_ = 0;
+    long maxZero_ = 0;
     SampleJob* dSampleJobs_ = nullptr;
     int nSampleJobs_ = 0;
     long maxSample_ = 0;
@@ -143,7 +150,8 @@ private:
     CopyJob* dSeed_ = nullptr;
     int nSeed_ = 0;
     LevelArgs* dSplit_ = nullptr;  // mixed: P_l - R_l splits (one per system and tensor-core level)
-    int nSplit_ = 0, maxSplitNp_ = 0;
+    int nSplit_ = 0;
+    long maxSplitElems_ = 0;
     long maxForcing_ = 0, maxOutput_ = 0, maxSeed_ = 0;
     void* arena_ = nullptr;
     size_t arena_bytes_ = 0;

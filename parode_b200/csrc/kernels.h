@@ -71,9 +71,10 @@ struct ResponseArgs {
     double* Wm = nullptr;          // row stride Kpad + NPstate
     int K = 0, Kpad = 0;           // window columns, padded to even
     int NPstate = 0;               // NP: also the initial-state columns (z_0 = I on them), or 0
-    // launch_response_tables / launch_response_fill only: workspace of
-    // B p NP (CP_j = Cext Phi^j) and B NP n (Q_k = Phi^k restricted to the
-    // n forcing columns) doubles
+    // launch_response_init / response_doubling_args / launch_response_fill
+    // only: workspace of B p NP doubles (CP_j = Cext Phi^j, block j at j p NP)
+    // and NP x B n doubles (Q_k = Phi^k restricted to the n forcing columns,
+    // row-major with pitch B n, Q_k at columns k n .. k n + n)
     double* CPt = nullptr;
     double* Qt = nullptr;
 };
@@ -81,17 +82,21 @@ struct ResponseArgs {
 int response_window(int solver, int B, int m);
 void launch_block_response(const ResponseArgs* dArgs, int nsys, int max_np, int max_p, int max_kpad, cudaStream_t s);
 // The same W for any NP, over many systems.  dStart[e] is entry e's first CTA
-// (response_tables_ctas / response_fill_ctas CTAs each, `ctas` in total).
-// Tables: call with j = 0 .. maxB - 1 in order (step j from step j - 1);
-// then one fill.
-long response_tables_ctas(const ResponseArgs& a);
+// (response_init_ctas / response_fill_ctas CTAs each, `ctas` in total).
+// Order: init (CP_0, Q_0); for l = 0 .. log2(B) - 1 the tiled GEMMs of
+// response_doubling_args (P = the power table, P_l at l NP^2), which double
+// the tables from 2^l to 2^(l+1) entries; then one fill.
+long response_init_ctas(const ResponseArgs& a);
 long response_fill_ctas(const ResponseArgs& a);
-void launch_response_tables(const ResponseArgs* dArgs, const long* dStart, int nent, long ctas, int j,
-                            cudaStream_t s);
+void launch_response_init(const ResponseArgs* dArgs, const long* dStart, int nent, long ctas, cudaStream_t s);
+// Fills out[0..1] (N-contiguous tiled GEMMs) and returns their count (0 once 2^l >= B).
+int response_doubling_args(const ResponseArgs& a, const double* P, int l, LevelArgs out[2]);
 void launch_response_fill(const ResponseArgs* dArgs, const long* dStart, int nent, long ctas, cudaStream_t s);
 // Block length 2^R of the response leaf for one system, and its cost in
-// flops per step (the two GEMMs and a level-synchronous carry over blocks).
-int response_log2_block(int solver, int NP, int m, int p, long nScan, double* flops_per_step);
+// FP64-equivalent flops per step (the two GEMMs and a level-synchronous carry
+// over blocks); window_weight scales the window and aggregate products (1 in
+// FP64, the tensor cores' relative cost in the mixed form).
+int response_log2_block(int solver, int NP, int m, int p, long nScan, double window_weight, double* flops_per_step);
 
 // Columns of a level that can reach an output.  Column g combines the
 // segments [g 2d, g 2d + d) and [g 2d + d, g 2d + 2d) of the time axis; when
@@ -153,7 +158,8 @@ void launch_affine_level_grouped(const LevelConfig& c, const LevelArgs* dArgs, c
 void launch_swap_grouped(const LevelArgs* dArgs, int nent, long max_elems, cudaStream_t s);
 
 // Mixed-precision level contraction (3xTF32 tcgen05, FP64 in and out) for
-// scan dimensions 72..1024 with K-contiguous sources and no in-place copy.
+// scan dimensions 72..1024 with K-contiguous sources and no in-place copy,
+// or a general rows x K GEMM (M, K set; one source; dst_limit honoured).
 // Grouped like launch_affine_level_grouped: dStart[e] = first tile of entry e,
 // level_tc_tiles(a) tiles per entry.  A device wait that gives up sets *status.
 bool level_tc_supported(const LevelArgs& a);
@@ -168,8 +174,11 @@ std::vector<long> level_tc_ranges(const std::vector<LevelArgs>& ents, int ctas);
 void level_encode_src_map(const LevelArgs& a, void* out);
 // Bytes of the pre-split P - R of one level (tiles of 128 rows x 16 K, hi then lo).
 size_t level_split_bytes(int Np);
+// The same for a general rows x K matrix (LevelArgs M, K; no exact part: rn = -1).
+size_t gemm_split_bytes(int rows, int K);
 // Pre-split P - R for every entry (a.P, a.rn, a.rsh -> a.Ps); blockIdx.y = entry.
-void launch_level_split(const LevelArgs* dArgs, int nent, int max_np, cudaStream_t s);
+// max_elems: the largest split of an entry, in 8-byte units (sizes the grid).
+void launch_level_split(const LevelArgs* dArgs, int nent, long max_elems, cudaStream_t s);
 
 struct SampleJob {
     double* U = nullptr;
@@ -197,7 +206,7 @@ struct OutputJob {
 };
 struct CopyJob {
     double* dst = nullptr;
-    const double* src = nullptr;
+    const double* src = nullptr;  // nullptr: fill with zeros
     long N = 0;
 };
 // max_elems: the largest element count of a job (sizes the x dimension).

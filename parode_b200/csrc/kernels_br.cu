@@ -100,8 +100,10 @@ __global__ void __launch_bounds__(kThreads) k_block_response(const ResponseArgs*
 // where S_i (the forcing of step i) is non-zero only on the n forcing rows
 // coff .. coff + n and reads samples i..i+4 (ABM) or 2i..2i+2 (RK4) through
 // the slots of Bbar.  So W needs only CP_k = Cext Phi^k (p x NP) and
-// Q_k = Phi^k restricted to the forcing columns (NP x n), k < B: B
-// row-times-matrix steps instead of B full NP x NP products.
+// Q_k = Phi^k restricted to the forcing columns (NP x n), k < B, instead of
+// B full NP x NP products.  Both tables double with the power table
+// P_l = Phi^(2^l): CP_{k + 2^l} = CP_k P_l and Q_{k + 2^l} = P_l Q_k, one
+// GEMM launch per l for all k < 2^l (response_doubling_args).
 // ---------------------------------------------------------------------------
 
 constexpr int kPerThread = 4;
@@ -118,47 +120,25 @@ __device__ __forceinline__ int find_entry(const long* __restrict__ start, int ne
     return lo;
 }
 
-// Step j of the tables: CP_j = CP_{j-1} Phi and Q_j = Phi Q_{j-1}
-// (j = 0: CP_0 = Cext, Q_0 = the identity's forcing columns).
-__global__ void __launch_bounds__(kThreads) k_response_tables(const ResponseArgs* __restrict__ args,
-                                                               const long* __restrict__ start, int nent, int j)
+// CP_0 = Cext and Q_0 = the identity's forcing columns.
+__global__ void __launch_bounds__(kThreads) k_response_init(const ResponseArgs* __restrict__ args,
+                                                             const long* __restrict__ start, int nent)
 {
     const int e = find_entry(start, nent, blockIdx.x);
     const ResponseArgs& a = args[e];
-    if (j >= a.B) return;
     const int NP = a.NP, p = a.p, n = a.n;
     const int coff = a.solver == 0 ? 0 : 3 * n;
-    const long ncp = (long)p * NP, total = ncp + (long)NP * n;
-    const double* __restrict__ Phi = a.Phi;
-    const double* __restrict__ cp_prev = a.CPt + (long)(j - 1) * ncp;
-    const double* __restrict__ q_prev = a.Qt + (long)(j - 1) * NP * n;
-    double* cp = a.CPt + (long)j * ncp;
-    double* q = a.Qt + (long)j * NP * n;
+    const long ncp = (long)p * NP, total = ncp + (long)NP * n, ldq = (long)a.B * n;
     const long base = (blockIdx.x - start[e]) * (long)kPerCta + threadIdx.x;
     for (int t = 0; t < kPerThread; ++t) {
         const long idx = base + (long)t * kThreads;
         if (idx >= total) break;
         if (idx < ncp) {
-            const int o = (int)(idx / NP), c = (int)(idx - (long)o * NP);
-            double v;
-            if (j == 0) {
-                v = a.Cext[idx];
-            } else {
-                v = 0.0;
-                for (int r = 0; r < NP; ++r) v = fma(cp_prev[(long)o * NP + r], Phi[(long)r * NP + c], v);
-            }
-            cp[idx] = v;
+            a.CPt[idx] = a.Cext[idx];
         } else {
             const long u = idx - ncp;
             const int r = (int)(u / n), c = (int)(u - (long)r * n);
-            double v;
-            if (j == 0) {
-                v = (r == coff + c) ? 1.0 : 0.0;
-            } else {
-                v = 0.0;
-                for (int s = 0; s < NP; ++s) v = fma(Phi[(long)r * NP + s], q_prev[(long)s * n + c], v);
-            }
-            q[u] = v;
+            a.Qt[r * ldq + c] = (r == coff + c) ? 1.0 : 0.0;
         }
     }
 }
@@ -203,7 +183,7 @@ __global__ void __launch_bounds__(kThreads) k_response_fill(const ResponseArgs* 
                 if (!a.zeroB)
                     for (int i = max(ilo, 0); i <= min(ihi, B - 1); ++i) {
                         const int w = rk4 ? s - 2 * i : s - i;
-                        const double* qr = a.Qt + (long)(B - 1 - i) * NP * n + (long)r * n;
+                        const double* qr = a.Qt + (long)r * B * n + (long)(B - 1 - i) * n;
                         const double* bb = a.Bbar + (long)w * m + c;
                         for (int k = 0; k < n; ++k) v = fma(qr[k], bb[(long)k * W * m], v);
                     }
@@ -224,7 +204,7 @@ int response_window(int solver, int B, int m)
     return (solver == 0 ? 2 * B + 1 : B + 4) * m;
 }
 
-long response_tables_ctas(const ResponseArgs& a)
+long response_init_ctas(const ResponseArgs& a)
 {
     const long total = (long)a.p * a.NP + (long)a.NP * a.n;
     return (total + kPerCta - 1) / kPerCta;
@@ -236,12 +216,53 @@ long response_fill_ctas(const ResponseArgs& a)
     return (total + kPerCta - 1) / kPerCta;
 }
 
-void launch_response_tables(const ResponseArgs* dArgs, const long* dStart, int nent, long ctas, int j, cudaStream_t s)
+void launch_response_init(const ResponseArgs* dArgs, const long* dStart, int nent, long ctas, cudaStream_t s)
 {
     if (nent <= 0 || ctas <= 0) return;
     if (ctas > 0x7fffffffL) throw Error(kInvalidArgument, "response tables: grid too large");
-    k_response_tables<<<(unsigned)ctas, kThreads, 0, s>>>(dArgs, dStart, nent, j);
+    k_response_init<<<(unsigned)ctas, kThreads, 0, s>>>(dArgs, dStart, nent);
     PARODE_CUDA(cudaGetLastError());
+}
+
+int response_doubling_args(const ResponseArgs& a, const double* P, int l, LevelArgs out[2])
+{
+    const int half = 1 << l;
+    if (half >= a.B) return 0;
+    const long NP = a.NP, ldq = (long)a.B * a.n;
+    const double* Pl = P + (long)l * NP * NP;
+    // Q_{k + 2^l} = P_l Q_k, k < 2^l: the first 2^l n columns of Qt (row pitch
+    // B n) into the next 2^l n; the source is N-contiguous
+    LevelArgs q;
+    q.P = Pl;
+    q.ldp = NP;
+    q.Np = a.NP;
+    q.M = a.NP;
+    q.K = a.NP;
+    q.ncols = (long)half * a.n;
+    q.src = a.Qt;
+    q.src_gs = 1;
+    q.src_ks = ldq;
+    q.dst = a.Qt + (long)half * a.n;
+    q.dst_gs = 1;
+    q.dst_is = ldq;
+    // CP_{k + 2^l} = CP_k P_l, k < 2^l: rows (k, o) of CPt are the MMA's rows,
+    // P_l's columns its columns (result(c, (k, o)) = sum_r CP_k[o][r] P_l[r][c])
+    LevelArgs c;
+    c.P = a.CPt;
+    c.ldp = NP;
+    c.Np = a.NP;
+    c.M = half * a.p;
+    c.K = a.NP;
+    c.ncols = NP;
+    c.src = Pl;
+    c.src_gs = 1;
+    c.src_ks = NP;
+    c.dst = a.CPt + (long)half * a.p * NP;
+    c.dst_gs = 1;
+    c.dst_is = NP;
+    out[0] = q;
+    out[1] = c;
+    return 2;
 }
 
 void launch_response_fill(const ResponseArgs* dArgs, const long* dStart, int nent, long ctas, cudaStream_t s)
@@ -252,11 +273,13 @@ void launch_response_fill(const ResponseArgs* dArgs, const long* dStart, int nen
     PARODE_CUDA(cudaGetLastError());
 }
 
-int response_log2_block(int solver, int NP, int m, int p, long nScan, double* flops_per_step)
+int response_log2_block(int solver, int NP, int m, int p, long nScan, double window_weight, double* flops_per_step)
 {
-    // per block: aggregates 2 NP Kpad, outputs 2 B p (Kpad + NP), and about
-    // 6 NP^2 for the level-synchronous carry (up- and down-sweep, 4 NP^2,
-    // at a lower efficiency than the GEMMs)
+    // per block: aggregates 2 NP Kpad and the outputs' window part 2 B p Kpad
+    // (scaled by window_weight: below 1 when they run on the tensor cores),
+    // the outputs' state part 2 B p NP, and about 6 NP^2 for the
+    // level-synchronous carry (up- and down-sweep, 4 NP^2, at a lower
+    // efficiency than the GEMMs)
     int best = 2;
     double best_cost = -1.0;
     for (int R = 2; R <= 7; ++R) {
@@ -265,7 +288,8 @@ int response_log2_block(int solver, int NP, int m, int p, long nScan, double* fl
         const long K = response_window(solver, (int)B, m), Kp = (K + 1) & ~1L;
         const double wbytes = 8.0 * ((double)B * p + NP) * ((double)Kp + NP);
         if (R > 2 && wbytes > 256e6) break;
-        const double cost = (2.0 * NP * Kp + 2.0 * B * p * (double)(Kp + NP) + 6.0 * NP * NP) / B;
+        const double cost =
+            (window_weight * (2.0 * NP * Kp + 2.0 * B * p * (double)Kp) + 2.0 * B * p * (double)NP + 6.0 * NP * NP) / B;
         if (best_cost < 0 || cost < best_cost) {
             best_cost = cost;
             best = R;

@@ -459,10 +459,19 @@ __global__ void k_copy_batch(const CopyJob* __restrict__ jobs)
 {
     const CopyJob J = jobs[blockIdx.y];
     for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < J.N; e += (long)gridDim.x * blockDim.x)
-        J.dst[e] = J.src[e];
+        J.dst[e] = J.src ? J.src[e] : 0.0;
 }
 
 inline unsigned blocks_for(long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// x extent of a batched launch (y = jobs): `cap` CTAs per job, raised so
+// that the whole grid has about 2048 CTAs when the jobs are few, and never
+// more than the largest job needs.
+inline unsigned batch_grid_x(long max_elems, int per_cta, int cap, int njobs)
+{
+    const long want = std::max<long>(cap, (2048 + njobs - 1) / njobs);
+    return (unsigned)std::max<long>(1, std::min<long>(blocks_for(max_elems, per_cta), want));
+}
 
 // Arguments of the tiled contraction for a level: the down-sweep (cpy set)
 // becomes, after the swap, right = P left + right.
@@ -688,7 +697,7 @@ void launch_swap_grouped(const LevelArgs* dArgs, int nent, long max_elems, cudaS
 void launch_samples_batch(const SampleJob* dJobs, int njobs, long max_elems, cudaStream_t s)
 {
     if (njobs <= 0 || max_elems <= 0) return;
-    dim3 grid((unsigned)std::min<long>(blocks_for(max_elems, 256), 64), (unsigned)njobs);
+    dim3 grid(batch_grid_x(max_elems, 256, 64, njobs), (unsigned)njobs);
     k_samples_batch<<<grid, 256, 0, s>>>(dJobs);
     PARODE_CUDA(cudaGetLastError());
 }
@@ -697,7 +706,7 @@ void launch_forcing_batch(const ForcingJob* dJobs, int njobs, long max_elems, cu
 {
     if (njobs <= 0 || max_elems <= 0) return;
     // max_elems: the largest Tp x Np; a CTA of 128 threads walks rows
-    dim3 grid((unsigned)std::min<long>(blocks_for(max_elems, 1024), 256), (unsigned)njobs);
+    dim3 grid(batch_grid_x(max_elems, 1024, 256, njobs), (unsigned)njobs);
     k_forcing_batch<<<grid, 128, 0, s>>>(dJobs);
     PARODE_CUDA(cudaGetLastError());
 }
@@ -705,7 +714,7 @@ void launch_forcing_batch(const ForcingJob* dJobs, int njobs, long max_elems, cu
 void launch_output_batch(const OutputJob* dJobs, int njobs, long max_elems, cudaStream_t s)
 {
     if (njobs <= 0 || max_elems <= 0) return;
-    dim3 grid((unsigned)std::min<long>(blocks_for(max_elems, 2048), 128), (unsigned)njobs);
+    dim3 grid(batch_grid_x(max_elems, 2048, 128, njobs), (unsigned)njobs);
     k_output_batch<<<grid, 256, 0, s>>>(dJobs);
     PARODE_CUDA(cudaGetLastError());
 }
@@ -713,7 +722,7 @@ void launch_output_batch(const OutputJob* dJobs, int njobs, long max_elems, cuda
 void launch_copy_batch(const CopyJob* dJobs, int njobs, long max_elems, cudaStream_t s)
 {
     if (njobs <= 0 || max_elems <= 0) return;
-    dim3 grid((unsigned)std::min<long>(blocks_for(max_elems, 256), 16), (unsigned)njobs);
+    dim3 grid(batch_grid_x(max_elems, 256, 16, njobs), (unsigned)njobs);
     k_copy_batch<<<grid, 256, 0, s>>>(dJobs);
     PARODE_CUDA(cudaGetLastError());
 }

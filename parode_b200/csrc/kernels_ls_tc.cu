@@ -24,9 +24,14 @@
 //   warps 2-3   converters: B FP64 -> TF32 hi/lo in the canonical layout,
 //               then arrive on `conv`;
 //   warp 1      one thread issues hi*hi + hi*lo + lo*hi into one of two TMEM
-//               accumulators and commits to `empty` (stage free) and, after a
-//               tile's last slice, to `acc_full`;
-//   warps 4-7   epilogue: TMEM -> FP64, + R v + acc, store; arrive `acc_empty`.
+//               accumulators and commits to `empty` (stage free) and, after
+//               every kDrain slices (a drain unit), to `acc_full`;
+//   warps 4-7   epilogue: per drain unit TMEM (FP32) -> FP64 running sums in
+//               registers, arrive `acc_empty`; after a tile's last unit
+//               + R v + acc, store.
+// The drains keep each FP32 accumulation chain to kDrain slices (6 kDrain
+// MMAs): the tensor cores' FP32 accumulation error grows with the chain,
+// the FP64 sums across units do not.
 // Every wait is bounded; a wait that gives up sets the status word and an
 // abort flag that makes every role leave its loop.
 #include "common.h"
@@ -60,6 +65,7 @@ constexpr uint32_t kNumBars = 3 * kS + 4;
 constexpr uint32_t kOffSlot = kOffBars + 8 * kNumBars;
 constexpr uint32_t kSmem = kOffSlot + 16;
 constexpr uint32_t kTmemCols = 2 * kBN;
+constexpr int kDrain = 2;  // K slices per FP32 accumulation chain
 constexpr long long kWaitLimit = 1LL << 31;
 
 // Phase-trace hook (no-op unless a timing harness defines it).
@@ -70,10 +76,10 @@ constexpr long long kWaitLimit = 1LL << 31;
 
 __host__ __device__ constexpr uint32_t koff(int r, int k) { return kmajor_off(r, k, kBK); }
 
-// K elements of slice s (16, or 8 for the last slice when Np = 8 mod 16).
-__device__ __forceinline__ int slice_len(int Np, int s)
+// K elements of slice s (16, or fewer in the last slice).
+__device__ __forceinline__ int slice_len(int K, int s)
 {
-    const int rest = Np - s * kBK;
+    const int rest = K - s * kBK;
     return rest < kBK ? rest : kBK;
 }
 
@@ -89,20 +95,21 @@ __host__ __device__ inline int r_col(const LevelArgs& a, int i)
 
 // ---------------------------------------------------------------------------
 // E = P - R split into TF32 hi/lo blocks: block (mt, s) = rows [128 mt, +128),
-// K [16 s, +16), hi then lo, each in the canonical K-major layout.
+// K [16 s, +16), hi then lo, each in the canonical K-major layout.  P is
+// rows x K (level_rows, level_k), zero-padded to whole blocks.
 // ---------------------------------------------------------------------------
 __global__ void k_split(const LevelArgs* __restrict__ args)
 {
     const LevelArgs& a = args[blockIdx.y];
-    const int Np = a.Np;
-    const int mt = (Np + kBM - 1) / kBM, nk = (Np + kBK - 1) / kBK;
+    const int rows = level_rows(a), K = level_k(a);
+    const int mt = (rows + kBM - 1) / kBM, nk = (K + kBK - 1) / kBK;
     const long total = (long)mt * kBM * nk * kBK;  // padded elements
     unsigned char* out = reinterpret_cast<unsigned char*>(const_cast<float*>(a.Ps));
     for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
         const long kp = (long)nk * kBK;
         const int i = (int)(e / kp), k = (int)(e - (long)i * kp);
         double v = 0.0;
-        if (i < Np && k < Np) {
+        if (i < rows && k < K) {
             v = a.P[(long)i * a.ldp + k];
             if (k == r_col(a, i)) v -= 1.0;
         }
@@ -198,11 +205,11 @@ struct Cursor {
 
 __device__ __forceinline__ void tile_coords(const LevelArgs& a, long lt, int& mi, int& m0, long& n0, int& nk)
 {
-    const int mt = (a.Np + kBM - 1) / kBM;
+    const int mt = (level_rows(a) + kBM - 1) / kBM;
     mi = (int)(lt % mt);
     m0 = mi * kBM;
     n0 = (lt / mt) * kBN;
-    nk = (a.Np + kBK - 1) / kBK;
+    nk = (level_k(a) + kBK - 1) / kBK;
 }
 
 // Persistent grouped kernel: CTA c walks tiles [cta[c], cta[c+1]) in order.
@@ -255,7 +262,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
             const int nv = (int)std::min<long>(kBN, a.ncols - n0);
             // the epilogue's acc rows of this tile into L2 ahead of time
             if (a.acc) {
-                const int rows = a.Np - m0 < kBM ? a.Np - m0 : kBM;
+                const int rows = level_rows(a) - m0 < kBM ? level_rows(a) - m0 : kBM;
                 const int lines = (rows * 8 + 127) / 128;
                 for (int q = lane; q < nv * lines; q += 32) {
                     const int v = q / lines, ln = q - v * lines;
@@ -267,11 +274,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
                 const int st = (int)(j % kS);
                 const long use = j / kS;
                 if (use >= 1 && !role_wait(&empty[st], (uint32_t)((use - 1) & 1), abort, status)) break;
-                const int kl = slice_len(a.Np, s);  // 16 or 8 doubles
                 unsigned char* stg = sm + st * kStage;
                 // A: one 16 KB bulk copy; B: one 2D tensor load of 64 vectors x
                 // 16 K (FP64; x = 16 s, a multiple of 16 bytes; the tails beyond
-                // Np or ncols are zero-filled by the TMA engine)
+                // K or ncols are zero-filled by the TMA engine)
                 if (lane == 0) {
                     mbar_arrive_tx(&full[st], kABlock + kBRaw);
                     bulk_g2s(stg, reinterpret_cast<const unsigned char*>(a.Ps) + ((size_t)mi * nk + s) * kABlock,
@@ -287,21 +293,29 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
         if (lane == 0) {
             Cursor c;
             c.init(args, start, nent, t0, t1);
-            long j = 0, u = 0;  // slice and tile counters
+            long j = 0, u = 0;  // slice and drain-unit counters
             constexpr uint32_t SBO = kBK * 32;
             constexpr uint32_t idesc = make_idesc(kBM, kBN);
-            for (long t = t0; t < t1 && !*abort; ++t, ++u) {
+            bool ok = true;
+            for (long t = t0; t < t1 && ok && !*abort; ++t) {
                 const long lt = c.seek(t);
                 int mi, m0, nk;
                 long n0;
                 tile_coords(c.a, lt, mi, m0, n0, nk);
-                const int ab = (int)(u & 1);
-                const long ause = u >> 1;
-                if (ause >= 1 && !role_wait(&acc_empty[ab], (uint32_t)((ause - 1) & 1), abort, status)) break;
-                fence_after_sync();
-                const uint32_t d = tbase + (uint32_t)(ab * kBN);
-                bool ok = true;
+                int ab = 0;
+                uint32_t d = 0;
                 for (int s = 0; s < nk; ++s, ++j) {
+                    if (s % kDrain == 0) {
+                        // a new drain unit: wait until the epilogue has read this accumulator
+                        ab = (int)(u & 1);
+                        const long ause = u >> 1;
+                        if (ause >= 1 && !role_wait(&acc_empty[ab], (uint32_t)((ause - 1) & 1), abort, status)) {
+                            ok = false;
+                            break;
+                        }
+                        fence_after_sync();
+                        d = tbase + (uint32_t)(ab * kBN);
+                    }
                     const int st = (int)(j % kS);
                     // A landed (bulk copy) and B converted
                     if (!role_wait(&full[st], (uint32_t)((j / kS) & 1), abort, status) ||
@@ -321,12 +335,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
 #pragma unroll
                         for (int k = 0; k < kBK / 8; ++k)
                             mma_tf32(d, A[q] + (uint64_t)(k * 16), B[q] + (uint64_t)(k * 16), idesc,
-                                     (s == 0 && q == 0 && k == 0) ? 0u : 1u);
+                                     (s % kDrain == 0 && q == 0 && k == 0) ? 0u : 1u);
                     mma_commit(&empty[st]);
                     PARODE_TC_TRACE(1);
+                    if (s % kDrain == kDrain - 1 || s == nk - 1) {
+                        mma_commit(&acc_full[ab]);
+                        ++u;
+                    }
                 }
-                if (!ok) break;
-                mma_commit(&acc_full[ab]);
             }
         }
         __syncwarp();
@@ -351,7 +367,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
                 }
                 unsigned char* stg = sm + st * kStage;
                 const double* raw = reinterpret_cast<const double*>(stg + kOffRaw);
-                const int kl = slice_len(a.Np, s);
+                const int kl = slice_len(level_k(a), s);
                 // 64 vectors x 4 chunks of 4 K; item w -> vector w/4, chunk w%4, so a
                 // warp reads 1 KB and writes 512 B contiguous (no bank conflicts)
 #pragma unroll
@@ -382,19 +398,43 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
         const int quarter = warp & 3;
         Cursor c;
         c.init(args, start, nent, t0, t1);
-        long u = 0;
-        for (long t = t0; t < t1 && !*abort; ++t, ++u) {
+        long u = 0;  // drain units
+        bool ok = true;
+        for (long t = t0; t < t1 && ok && !*abort; ++t) {
             const long lt = c.seek(t);
             const LevelArgs& a = c.a;
             int mi, m0, nk;
             long n0;
             tile_coords(a, lt, mi, m0, n0, nk);
-            const int ab = (int)(u & 1);
-            if (!role_wait(&acc_full[ab], (uint32_t)((u >> 1) & 1), abort, status)) break;
-            PARODE_TC_TRACE(3);
-            fence_after_sync();
+            // FP64 sums of this thread's row over the tile's drain units
+            double sum[kBN];
+#pragma unroll
+            for (int q = 0; q < kBN; ++q) sum[q] = 0.0;
+            const int units = (nk + kDrain - 1) / kDrain;
+            for (int v = 0; v < units; ++v, ++u) {
+                const int ab = (int)(u & 1);
+                if (!role_wait(&acc_full[ab], (uint32_t)((u >> 1) & 1), abort, status)) {
+                    ok = false;
+                    break;
+                }
+                PARODE_TC_TRACE(3);
+                fence_after_sync();
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    uint32_t r[32];
+                    tmem_ld32(tbase + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(ab * kBN + h * 32), r);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int q = 0; q < 32; ++q) sum[32 * h + q] += (double)__uint_as_float(r[q]);
+                }
+                fence_before_sync();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&acc_empty[ab]);
+            }
+            if (!ok) break;
             const long i = m0 + 32 * quarter + lane;
-            const int rc = i < a.Np ? r_col(a, (int)i) : -1;
+            const int rows = level_rows(a);
+            const int rc = i < rows ? r_col(a, (int)i) : -1;
             // loop-invariant fields in registers
             const double* srow = a.src + (rc >= 0 ? rc : 0);
             const long sgs = a.src_gs;
@@ -402,36 +442,31 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
             const long ags = a.acc_gs;
             double* drow = a.dst + i * a.dst_is;
             const long dgs = a.dst_gs;
-            const int nvt = (int)std::min<long>(kBN, a.ncols - n0);
-            const bool live = i < a.Np;
-#pragma unroll 1
-            for (int h = 0; h < 2; ++h) {
-                uint32_t r[32];
-                tmem_ld32(tbase + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(ab * kBN + h * 32), r);
-                tmem_wait_ld();
-                if (live) {
-                    // 16 columns at a time: all loads in flight before the sums
-#pragma unroll 1
-                    for (int c0 = 0; c0 < 32; c0 += 16) {
-                        double xa[16], xs[16];
-                        const int jb = 32 * h + c0;
+            int nvt = (int)std::min<long>(kBN, a.ncols - n0);
+            if (a.dst_limit >= 0 && i < rows) {
+                // columns whose result offset g dgs + i dst_is reaches the limit are dropped
+                const long lim = a.dst_limit - i * a.dst_is;
+                const long gmax = lim <= 0 ? n0 : (lim + dgs - 1) / dgs;  // first dropped column
+                nvt = (int)std::max<long>(0, std::min<long>(nvt, gmax - n0));
+            }
+            const bool live = i < rows;
+            if (live) {
+                // 16 columns at a time: all loads in flight before the sums
 #pragma unroll
-                        for (int jj = 0; jj < 16; ++jj) {
-                            const bool ok = jb + jj < nvt;
-                            const long g = n0 + jb + jj;
-                            xs[jj] = (ok && rc >= 0) ? srow[g * sgs] : 0.0;  // R v, exact
-                            xa[jj] = (ok && arow) ? arow[g * ags] : 0.0;
-                        }
+                for (int c0 = 0; c0 < kBN; c0 += 16) {
+                    double xa[16], xs[16];
 #pragma unroll
-                        for (int jj = 0; jj < 16; ++jj)
-                            if (jb + jj < nvt)
-                                drow[(n0 + jb + jj) * dgs] = ((double)__uint_as_float(r[c0 + jj]) + xs[jj]) + xa[jj];
+                    for (int jj = 0; jj < 16; ++jj) {
+                        const bool in = c0 + jj < nvt;
+                        const long g = n0 + c0 + jj;
+                        xs[jj] = (in && rc >= 0) ? srow[g * sgs] : 0.0;  // R v, exact
+                        xa[jj] = (in && arow) ? arow[g * ags] : 0.0;
                     }
+#pragma unroll
+                    for (int jj = 0; jj < 16; ++jj)
+                        if (c0 + jj < nvt) drow[(n0 + c0 + jj) * dgs] = (sum[c0 + jj] + xs[jj]) + xa[jj];
                 }
             }
-            fence_before_sync();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&acc_empty[ab]);
             PARODE_TC_TRACE(4);
         }
     }
@@ -450,25 +485,30 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
 
 long level_tc_tiles(const LevelArgs& a)
 {
-    return (long)((a.Np + kBM - 1) / kBM) * ((a.ncols + kBN - 1) / kBN);
+    return (long)((level_rows(a) + kBM - 1) / kBM) * ((a.ncols + kBN - 1) / kBN);
 }
 
-size_t level_split_bytes(int Np)
+size_t gemm_split_bytes(int rows, int K)
 {
-    return (size_t)((Np + kBM - 1) / kBM) * ((Np + kBK - 1) / kBK) * kABlock;
+    return (size_t)((rows + kBM - 1) / kBM) * ((K + kBK - 1) / kBK) * kABlock;
 }
+
+size_t level_split_bytes(int Np) { return gemm_split_bytes(Np, Np); }
 
 bool level_tc_supported(const LevelArgs& a)
 {
-    // K-contiguous FP64 sources with 16-byte aligned rows, no in-place copy
-    return a.cpy == nullptr && a.src_ks == 1 && (a.src_gs % 2) == 0 && (a.ldp % 2) == 0 && (a.Np % 8) == 0 &&
-           a.Np > 64 && a.Np <= 1024 && (reinterpret_cast<uintptr_t>(a.src) & 15) == 0;
+    // K-contiguous FP64 sources with 16-byte aligned rows, no in-place copy,
+    // one source; square levels of scan dimension 72..1024, or general shapes
+    const bool general = a.M > 0 || a.K > 0;
+    return a.cpy == nullptr && a.K1 == 0 && a.src_ks == 1 && (a.src_gs % 2) == 0 && (a.ldp % 2) == 0 &&
+           (reinterpret_cast<uintptr_t>(a.src) & 15) == 0 &&
+           (general ? (level_rows(a) > 0 && level_k(a) > 0) : ((a.Np % 8) == 0 && a.Np > 64 && a.Np <= 1024));
 }
 
-void launch_level_split(const LevelArgs* dArgs, int nent, int max_np, cudaStream_t s)
+void launch_level_split(const LevelArgs* dArgs, int nent, long max_elems, cudaStream_t s)
 {
     if (nent <= 0) return;
-    const long elems = (long)level_split_bytes(max_np) / 8;
+    const long elems = max_elems;
     dim3 grid((unsigned)std::max<long>(1, std::min<long>((elems + 255) / 256, 512)), (unsigned)nent);
     k_split<<<grid, 256, 0, s>>>(dArgs);
     PARODE_CUDA(cudaGetLastError());
@@ -499,7 +539,7 @@ void level_encode_src_map(const LevelArgs& a, void* out)
     if ((reinterpret_cast<uintptr_t>(a.src) & 15) || ((a.src_gs * 8) & 15))
         throw Error(kInvalidArgument, "source map: 16-byte alignment");
     CUtensorMap* m = static_cast<CUtensorMap*>(out);
-    const cuuint64_t dims[2] = {(cuuint64_t)a.Np, (cuuint64_t)a.ncols};
+    const cuuint64_t dims[2] = {(cuuint64_t)level_k(a), (cuuint64_t)a.ncols};
     const cuuint64_t strides[1] = {(cuuint64_t)a.src_gs * 8};
     const cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)kBN};
     const cuuint32_t estr[2] = {1, 1};
@@ -517,7 +557,7 @@ std::vector<long> level_tc_ranges(const std::vector<LevelArgs>& ents, int ctas)
     double total = 0;
     for (const LevelArgs& a : ents) {
         const long n = level_tc_tiles(a);
-        const double c = (a.Np + kBK - 1) / kBK + 2.0;
+        const double c = (level_k(a) + kBK - 1) / kBK + 2.0;
         for (long t = 0; t < n; ++t) cost.push_back(c);
         total += c * n;
     }

@@ -60,10 +60,35 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
         // FP64 sin evaluations would compete with the scan for issue slots)
         gen_ = false;
         stage_bytes_ = blocked_leaf_stage_bytes(shape_, sys.n, mu_, p_, solver);
-        // the mixed form runs the leaf on the tensor cores (3xTF32) when the
-        // shape allows it, with the longest tile that fits its shared-memory
-        // layout; otherwise the solve stays in FP64
-        if (opt.precision == kMixed) {
+        // the leaf as GEMMs with the block response matrix (kernels_br.cu)
+        // when that costs fewer flops than the in-block sweeps: about
+        // 2 (B p + NP) K / B per step against 4 NP^2.  The mixed form runs the
+        // aggregate and output-window products on the tensor cores (3xTF32)
+        // and keeps the initial-state part of the outputs in FP64.
+        if (mu_ > 0 && opt.path != kPathBlockedSweep) {
+            const int K = response_window(solver, shape_.B, mu_);
+            const double resp = 2.0 * ((double)shape_.B * p_ + Np_) * K / shape_.B;
+            const double sweeps = 4.0 * Np_ * Np_;
+            if (opt.path == kPathBlockedResponse || resp < 0.5 * sweeps) {
+                br_ = true;
+                br_tc_ = opt.precision == kMixed;
+                if (br_tc_) precision_used_ = kMixed;
+                brK_ = K;
+                brKpad_ = (K + 1) & ~1;
+                nblocks_ = (nScan_ + shape_.B - 1) / shape_.B;
+                long c3 = nblocks_;
+                int lev3 = shape_.R;
+                while (c3 > shape_.S_items) {
+                    c3 = (c3 + shape_.B - 1) / shape_.B;
+                    lev3 += shape_.R;
+                }
+                levels_ = std::max(lev3 + ilog2(next_pow2(c3)), shape_.R);
+            }
+        }
+        // otherwise the mixed form runs the in-block sweeps on the tensor
+        // cores (3xTF32) when the shape allows it, with the longest tile that
+        // fits its shared-memory layout; otherwise the solve stays in FP64
+        if (opt.precision == kMixed && !br_) {
             // largest (levels per block, tile) that fits: the tensor-core
             // operands need bucket starts on 8-row boundaries (S >= 4B) and
             // M = 128 slices (S >= 128)
@@ -93,29 +118,8 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
                 levels_ = std::max(lev2 + ilog2(next_pow2(c2)), shape_.R);
             }
         }
-        // FP64: the leaf as one GEMM with the block response matrix (see
-        // kernels_br.cu) when that costs fewer flops than the in-block sweeps:
-        // about 2 (B p + NP) K / B per step against 4 NP^2
-        if (precision_used_ != kMixed && mu_ > 0 && opt.path != kPathBlockedSweep) {
-            const int K = response_window(solver, shape_.B, mu_);
-            const double resp = 2.0 * ((double)shape_.B * p_ + Np_) * K / shape_.B;
-            const double sweeps = 4.0 * Np_ * Np_;
-            if (opt.path == kPathBlockedResponse || resp < 0.5 * sweeps) {
-                br_ = true;
-                brK_ = K;
-                brKpad_ = (K + 1) & ~1;
-                nblocks_ = (nScan_ + shape_.B - 1) / shape_.B;
-                long c3 = nblocks_;
-                int lev3 = shape_.R;
-                while (c3 > shape_.S_items) {
-                    c3 = (c3 + shape_.B - 1) / shape_.B;
-                    lev3 += shape_.R;
-                }
-                levels_ = std::max(lev3 + ilog2(next_pow2(c3)), shape_.R);
-            }
-        }
         if (opt.path == kPathBlockedResponse && !br_)
-            throw Error(kInvalidArgument, "the response leaf needs inputs and the FP64 form");
+            throw Error(kInvalidArgument, "the response leaf needs inputs");
     }
     PARODE_CUDA(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_));
 
@@ -264,6 +268,62 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
         alloc(&dra, (long)((sizeof(ResponseArgs) + 7) / 8));
         PARODE_CUDA(cudaMemcpyAsync(dra, &ra, sizeof(ra), cudaMemcpyHostToDevice, stream_));
         launch_block_response(reinterpret_cast<const ResponseArgs*>(dra), 1, Np_, p_, brKpad_, stream_);
+        if (br_tc_) {
+            // the two tensor-core GEMMs over the sample windows: aggregates
+            // into G, output windows into the plan's y buffer (the FP64 state
+            // part then adds into the caller's y); W pre-split into TF32 hi/lo
+            const long ld = brKpad_ + Np_;
+            LevelArgs e[2];
+            LevelArgs& a = e[0];
+            a.P = dW_ + (long)shape_.B * p_ * ld;
+            a.ldp = ld;
+            a.Np = Np_;
+            a.M = Np_;
+            a.K = brK_;
+            a.ncols = nblocks_;
+            a.src = dU_;
+            a.src_gs = (solver == kRK4 ? 2L : 1L) * shape_.B * mu_;
+            a.src_ks = 1;
+            a.dst = dG_;
+            a.dst_gs = Np_;
+            LevelArgs& w = e[1];
+            w = a;
+            w.P = dW_;
+            w.M = shape_.B * p_;
+            w.dst = dY_ + (solver == kRK4 ? 0L : 3L * p_);
+            w.dst_gs = (long)shape_.B * p_;
+            w.dst_limit = nScan_ * (long)p_;
+            if (!level_tc_supported(a) || !level_tc_supported(w))
+                throw Error(kDeviceError, "response GEMMs not supported by the tensor-core kernel");
+            const size_t sa = gemm_split_bytes(a.M, a.K), sw = gemm_split_bytes(w.M, w.K);
+            double* ps = nullptr;
+            alloc(&ps, (long)((sa + sw) / 8));
+            a.Ps = reinterpret_cast<const float*>(ps);
+            w.Ps = reinterpret_cast<const float*>(reinterpret_cast<char*>(ps) + sa);
+            double* map = nullptr;
+            alloc(&map, 16);  // one 128-byte tensor map, shared: same source, K and columns
+            unsigned char host_map[128];
+            level_encode_src_map(a, host_map);
+            PARODE_CUDA(cudaMemcpyAsync(map, host_map, 128, cudaMemcpyHostToDevice, stream_));
+            a.src_map = map;
+            w.src_map = map;
+            const long start[2] = {0, level_tc_tiles(a)};
+            const long tiles = start[1] + level_tc_tiles(w);
+            tcCtas_ = (int)std::min<long>(sms_, tiles);
+            const std::vector<long> ranges = level_tc_ranges({a, w}, tcCtas_);
+            double* d = nullptr;
+            alloc(&d, (long)((2 * sizeof(LevelArgs) + 7) / 8));
+            dTc_ = reinterpret_cast<LevelArgs*>(d);
+            alloc(&d, 2);
+            dTcStart_ = reinterpret_cast<long*>(d);
+            alloc(&d, (long)ranges.size());
+            dTcCta_ = reinterpret_cast<long*>(d);
+            PARODE_CUDA(cudaMemcpyAsync(dTc_, e, sizeof(e), cudaMemcpyHostToDevice, stream_));
+            PARODE_CUDA(cudaMemcpyAsync(dTcStart_, start, sizeof(start), cudaMemcpyHostToDevice, stream_));
+            PARODE_CUDA(cudaMemcpyAsync(dTcCta_, ranges.data(), sizeof(long) * ranges.size(), cudaMemcpyHostToDevice,
+                                        stream_));
+            launch_level_split(dTc_, 2, (long)std::max(sa, sw) / 8, stream_);
+        }
     }
     PARODE_CUDA(cudaStreamSynchronize(stream_));
 }
@@ -448,6 +508,39 @@ void Plan::execute_response(double* Y, cudaStream_t s)
     mark("inputs", s);
     const int ybase = solver_ == kRK4 ? 0 : 3;
     const long ld = brKpad_ + Np_;
+    if (br_tc_) {
+        // mixed: aggregates and output windows (tensor cores) -> carry ->
+        // y = windows + C Phi^j X_b (FP64)
+        launch_level_tc(dTc_, dTcStart_, 2, dTcCta_, tcCtas_, dStatus_, s);
+        ++launches;
+        mark("aggregates+windows", s);
+        PARODE_CUDA(cudaStreamWaitEvent(s, fork_[3], 0));
+        launches += launch_blocked_carry(shape_, dG_, nblocks_, shape_.R, dPow_, dX0_, dWork_, sms_, s);
+        mark("carry", s);
+        LevelArgs x;
+        x.P = dW_ + brKpad_;
+        x.ldp = ld;
+        x.Np = Np_;
+        x.M = shape_.B * p_;
+        x.K = Np_;
+        x.ncols = nblocks_;
+        x.src = dG_;
+        x.src_gs = Np_;
+        x.src_ks = 1;
+        x.acc = dY_ + ybase * p_;
+        x.acc_gs = (long)shape_.B * p_;
+        x.dst = Y + ybase * p_;
+        x.dst_gs = (long)shape_.B * p_;
+        x.dst_limit = nScan_ * p_;
+        launch_gemm_tiled(x, s);
+        ++launches;
+        if (solver_ == kABM)
+            PARODE_CUDA(cudaMemcpyAsync(Y, dYpre_, sizeof(double) * 3 * p_, cudaMemcpyDeviceToDevice, s));
+        mark("outputs", s);
+        launches_ = launches;
+        last_y_ = Y;
+        return;
+    }
     LevelArgs g;
     g.P = dW_ + (long)shape_.B * p_ * ld;
     g.ldp = ld;

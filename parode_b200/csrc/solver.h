@@ -9,6 +9,7 @@
 #include "blocked.h"
 #include "host_math.h"
 #include "inputs.h"
+#include "kernels.h"
 
 #include <cuda_runtime.h>
 
@@ -91,7 +92,14 @@ private:
     int precision_used_ = 0;
     bool br_ = false;           // leaf = block response GEMM (kernels_br.cu)
     int brK_ = 0, brKpad_ = 0;  // window columns (padded to even)
-    double* dW_ = nullptr;      // response matrix, (B p + NP) x brKpad_
+    double* dW_ = nullptr;      // response matrix, (B p + NP) x (brKpad_ + NP)
+    // mixed form of the response leaf: aggregates and output windows on the
+    // tensor cores (one grouped launch of two GEMMs), state part in FP64
+    bool br_tc_ = false;
+    LevelArgs* dTc_ = nullptr;  // device: the two GEMMs
+    long* dTcStart_ = nullptr;  // device: their first tiles
+    long* dTcCta_ = nullptr;    // device: tile ranges of the persistent CTAs
+    int tcCtas_ = 0;
     int* dStatus_ = nullptr;
     cudaStream_t side_ = nullptr;
     cudaEvent_t fork_[4] = {nullptr, nullptr, nullptr, nullptr};

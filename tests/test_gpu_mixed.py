@@ -1,5 +1,7 @@
-"""GPU parity of the mixed-precision form (3xTF32 tcgen05 leaf, FP64 power
-table / carry / fix-up) against the CPU FP64 oracle.
+"""GPU parity of the mixed-precision form against the CPU FP64 oracle: the
+3xTF32 tcgen05 leaf (in-block sweeps, path 4) or the block-response GEMMs on
+tcgen05 (aggregates and output windows, path 3), with the power table, the
+carry and the initial-state part of the outputs in FP64.
 
 Tolerance: per-channel relative error <= 1e-6 (max_k |y - y_oracle| /
 max_k |y_oracle|), the bound the mixed form is specified to meet at T = 2^20.
@@ -15,8 +17,8 @@ pytestmark = pytest.mark.gpu
 TOL_MIXED = 1e-6
 
 
-def _run(pb, case, precision):
-    pb.set_option(pb.OPT_PATH, 0)
+def _run(pb, case, precision, path=0):
+    pb.set_option(pb.OPT_PATH, path)
     u = pb.register_sinusoid(case.u.a, case.u.f, case.u.phi)
     plan = pb.Plan(case.A, case.B, case.C, case.D, case.x0, u, case.t0, case.t_end, case.h, solver=case.solver,
                    precision=precision)
@@ -24,6 +26,7 @@ def _run(pb, case, precision):
     _, y = plan.output()
     used = plan.precision
     plan.close()
+    pb.set_option(pb.OPT_PATH, 0)
     return y, used
 
 
@@ -36,18 +39,20 @@ def _oracle(case):
 @pytest.mark.parametrize("solver,n,m,p,T", [(0, 16, 2, 2, 5000), (0, 24, 3, 4, 3000), (0, 32, 4, 4, 20000),
                                             (0, 48, 6, 6, 7777), (0, 64, 8, 8, 4096), (1, 4, 1, 1, 3000),
                                             (1, 8, 2, 2, 5000), (1, 16, 2, 2, 10000)])
-def test_mixed_parity(pb, solver, n, m, p, T):
+@pytest.mark.parametrize("path", [0, 3, 4])
+def test_mixed_parity(pb, solver, n, m, p, T, path):
     case = wl.small(500 + n + 3 * T + solver, solver, n, m, p, T, h=1e-3)
-    y, used = _run(pb, case, pb.MIXED)
-    assert used == pb.MIXED, "the tensor-core leaf should cover scan dimensions 16..64"
+    y, used = _run(pb, case, pb.MIXED, path)
+    assert used == pb.MIXED, "the tensor-core leaves should cover scan dimensions 16..64"
     err = oracle.rel_err(y, _oracle(case))
     assert err <= TOL_MIXED, err
 
 
-def test_mixed_cfg2_full_size(pb):
+@pytest.mark.parametrize("path", [0, 4])
+def test_mixed_cfg2_full_size(pb, path):
     """The benchmark workload (RK4 n=64, T=2^20) in the mixed form."""
     case = wl.cfg2()
-    y, used = _run(pb, case, pb.MIXED)
+    y, used = _run(pb, case, pb.MIXED, path)
     assert used == pb.MIXED
     err = oracle.rel_err(y, _oracle(case))
     assert err <= TOL_MIXED, err
