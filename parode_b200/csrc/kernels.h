@@ -98,6 +98,17 @@ void launch_response_fill(const ResponseArgs* dArgs, const long* dStart, int nen
 // FP64, the tensor cores' relative cost in the mixed form).
 int response_log2_block(int solver, int NP, int m, int p, long nScan, double window_weight, double* flops_per_step);
 
+// Exclusive scan of block aggregates for NP <= 64 (a multiple of 8),
+// kernels_carry.cu: items[b] <- X_b with X_0 = X0, X_{b+1} = Q X_b + items[b],
+// Q = P_{l0} (P: power table, level l at l NP^2).  Chunks of 16 per level;
+// level h uses P_{l0 + 4h}, so the table must reach level
+// l0 + 4 chunk_carry_levels(count).  work: chunk_carry_scratch(count) NP
+// doubles.  Returns the launches made.
+int chunk_carry_levels(long count);
+long chunk_carry_scratch(long count);
+int launch_chunk_carry(int NP, double* items, long count, const double* P, int l0, const double* X0, double* work,
+                       cudaStream_t s);
+
 // Columns of a level that can reach an output.  Column g combines the
 // segments [g 2d, g 2d + d) and [g 2d + d, g 2d + 2d) of the time axis; when
 // g 2d >= nScan both segments are padding: the column holds zeros in the

@@ -1,0 +1,290 @@
+// kernels_carry.cu -- exclusive scan of block aggregates for scan dimensions <= 64.
+//
+// The blocked and block-response leaves leave one aggregate G_b per block of
+// B steps; the state entering block b is the exclusive scan
+//   X_0 = x0,  X_{b+1} = Q X_b + G_b,  Q = Phi^B,
+// which is the reference's Blelloch composition (Kernels/MVVKernelScanUpsweep.cl,
+// MVVKernelScanDownsweep.cl) applied to the blocks.  Here it runs as a chunked
+// scan: chunks of F = 16 items, each chunk's aggregate by 16 sequential steps
+// (up), the chunk aggregates scanned one level higher with Q^16, and each
+// chunk's items rewritten by 16 sequential steps from its carried-in state
+// (down).  A CTA owns 8 chunks as the 8 columns of an NP x 8 tile: every step
+// is one NP x NP x 8 product on the FP64 tensor cores (DMMA m8n8k4) with Q's
+// fragments held in registers, so the sequential depth is 16 steps per level
+// while the chunks spread over all SMs (narrow tiles keep the few-chunk upper
+// levels short: a step's time is set by one SM's FP64 rate).  The flops equal
+// the Blelloch up- plus down-sweep's (2 NP^2 per item each way).
+#include "common.h"
+#include "device_common.cuh"
+#include "kernels.h"
+
+namespace parode {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kCols = 8;        // chunks per CTA (the tile's columns)
+constexpr int kNT = kCols / 8;  // n-tiles of the tile
+constexpr int kChunk = 16;      // items per chunk: Q^16 = 4 power-table levels up
+constexpr int kLd = kCols + 4;  // shared-memory row pitch (doubles): conflict-free B fragments
+
+// Warp roles: m-tile mt (8 rows of Q) and n-tiles nt0 .. nt0 + nts - 1 (8
+// chunk columns each) of the NP x kCols tile.
+template <int NP>
+struct Roles {
+    int g, t, mt, nt0, nts;
+    bool active;
+    __device__ Roles()
+    {
+        constexpr int MT = NP / 8, NT = kCols / 8, WPM = 8 / MT;
+        constexpr int NTS = NT / WPM > 0 ? NT / WPM : 1;
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        g = lane >> 2;
+        t = lane & 3;
+        mt = warp % MT;
+        nts = NTS;
+        nt0 = (warp / MT) * NTS;
+        active = nt0 < NT;
+    }
+};
+
+template <int NP>
+__device__ __forceinline__ void load_q(const double* __restrict__ Q, const Roles<NP>& r, double (&qa)[NP / 4])
+{
+#pragma unroll
+    for (int kk = 0; kk < NP / 4; ++kk) qa[kk] = Q[(r.mt * 8 + r.g) * NP + 4 * kk + r.t];
+}
+
+// G of step j for this lane's D-fragment positions: item (c0 + col) F + j, row.
+template <int NP>
+__device__ __forceinline__ void load_g(const double* __restrict__ items, long count, long c0, int F, int j,
+                                       const Roles<NP>& r, double (&v)[kNT][2])
+{
+    const int row = r.mt * 8 + r.g;
+#pragma unroll
+    for (int u = 0; u < kNT; ++u)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const long item = (c0 + (r.nt0 + u) * 8 + 2 * r.t + e) * F + j;
+            v[u][e] = (u < r.nts && item < count) ? items[item * NP + row] : 0.0;
+        }
+}
+
+// acc += Q X on the tile (X in shared memory, row pitch kLd).  The K
+// products go to kSplit independent partial sums, so the dependent MMA chain
+// (the step's latency) is NP / 4 / kSplit long.
+template <int NP>
+__device__ __forceinline__ void step_mma(const double* X, const double (&qa)[NP / 4], double (&acc)[kNT][2],
+                                         const Roles<NP>& r)
+{
+    constexpr int kSplit = NP / 4 < 4 ? NP / 4 : 4;
+    double part[kSplit][kNT][2];
+#pragma unroll
+    for (int q = 0; q < kSplit; ++q)
+#pragma unroll
+        for (int u = 0; u < kNT; ++u) part[q][u][0] = part[q][u][1] = 0.0;
+#pragma unroll
+    for (int kk = 0; kk < NP / 4; ++kk) {
+        const double* xr = X + (4 * kk + r.t) * kLd + r.g;
+#pragma unroll
+        for (int u = 0; u < kNT; ++u)
+            if (u < r.nts) dmma_m8n8k4(part[kk % kSplit][u][0], part[kk % kSplit][u][1], qa[kk], xr[(r.nt0 + u) * 8]);
+    }
+#pragma unroll
+    for (int u = 0; u < kNT; ++u)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            double v = acc[u][e];
+#pragma unroll
+            for (int q = 0; q < kSplit; ++q) v += part[q][u][e];
+            acc[u][e] = v;
+        }
+}
+
+// This lane's D-fragment positions of the states into item slot j.
+template <int NP>
+__device__ __forceinline__ void store_g(double* __restrict__ items, long count, long c0, int F, int j,
+                                        const Roles<NP>& r, const double (&v)[kNT][2])
+{
+    const int row = r.mt * 8 + r.g;
+#pragma unroll
+    for (int u = 0; u < kNT; ++u)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const long item = (c0 + (r.nt0 + u) * 8 + 2 * r.t + e) * F + j;
+            if (u < r.nts && item < count) items[item * NP + row] = v[u][e];
+        }
+}
+
+template <int NP>
+__device__ __forceinline__ void store_tile(double* X, const double (&acc)[kNT][2], const Roles<NP>& r)
+{
+    const int row = r.mt * 8 + r.g;
+#pragma unroll
+    for (int u = 0; u < kNT; ++u)
+        if (u < r.nts) {
+            X[row * kLd + (r.nt0 + u) * 8 + 2 * r.t] = acc[u][0];
+            X[row * kLd + (r.nt0 + u) * 8 + 2 * r.t + 1] = acc[u][1];
+        }
+}
+
+// Chunk aggregates: next[c] = sum_{j<16} Q^(15-j) items[16 c + j] (items past
+// count are zero; the last chunk's aggregate is never read by the scan).
+template <int NP>
+__global__ void __launch_bounds__(kThreads) k_chunk_up(const double* __restrict__ items, long count,
+                                                        const double* __restrict__ Q, double* __restrict__ next)
+{
+    __shared__ double Xs[2][NP * kLd];
+    const Roles<NP> r;
+    const long c0 = (long)blockIdx.x * kCols;
+    const long nchunks = (count + kChunk - 1) / kChunk;
+    double qa[NP / 4];
+    load_q<NP>(Q, r, qa);
+    for (int e = threadIdx.x; e < NP * kLd; e += kThreads) Xs[0][e] = 0.0;
+    double pre[kNT][2];
+    if (r.active) load_g<NP>(items, count, c0, kChunk, 0, r, pre);
+    __syncthreads();
+    int cur = 0;
+    for (int j = 0; j < kChunk; ++j) {
+        if (r.active) {
+            double acc[kNT][2];
+#pragma unroll
+            for (int u = 0; u < kNT; ++u) acc[u][0] = pre[u][0], acc[u][1] = pre[u][1];
+            if (j + 1 < kChunk) load_g<NP>(items, count, c0, kChunk, j + 1, r, pre);
+            step_mma<NP>(Xs[cur], qa, acc, r);
+            store_tile<NP>(Xs[cur ^ 1], acc, r);
+        }
+        __syncthreads();
+        cur ^= 1;
+    }
+    for (int e = threadIdx.x; e < NP * kCols; e += kThreads) {
+        const int col = e / NP, row = e - col * NP;
+        if (c0 + col < nchunks) next[(c0 + col) * NP + row] = Xs[cur][row * kLd + col];
+    }
+}
+
+// Chunk rewrite: from the chunk's carried-in state x = carries[c], items
+// [F c, F c + F) become the states entering them (x, then Q x + item, ...).
+// Each lane reads item j + 1 (its D-fragment positions) before it writes the
+// state into the same positions, so slots need no barrier.
+template <int NP>
+__global__ void __launch_bounds__(kThreads) k_chunk_down(double* __restrict__ items, long count,
+                                                          const double* __restrict__ Q,
+                                                          const double* __restrict__ carries, int F)
+{
+    __shared__ double Xs[2][NP * kLd];
+    const Roles<NP> r;
+    const long c0 = (long)blockIdx.x * kCols;
+    const long nchunks = (count + F - 1) / F;
+    double qa[NP / 4];
+    load_q<NP>(Q, r, qa);
+    for (int e = threadIdx.x; e < NP * kLd; e += kThreads) {
+        const int row = e / kLd, col = e - row * kLd;
+        Xs[0][e] = (col < kCols && c0 + col < nchunks) ? carries[(c0 + col) * NP + row] : 0.0;
+    }
+    double pre[kNT][2];
+    if (r.active) load_g<NP>(items, count, c0, F, 0, r, pre);
+    __syncthreads();
+    if (r.active) {
+        // slot 0 <- the carried-in state (item 0 is already in pre)
+        double x0[kNT][2];
+        const int row = r.mt * 8 + r.g;
+#pragma unroll
+        for (int u = 0; u < kNT; ++u)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) x0[u][e] = Xs[0][row * kLd + (r.nt0 + u) * 8 + 2 * r.t + e];
+        store_g<NP>(items, count, c0, F, 0, r, x0);
+    }
+    int cur = 0;
+    for (int j = 0; j + 1 < F; ++j) {
+        if (r.active) {
+            double acc[kNT][2];
+#pragma unroll
+            for (int u = 0; u < kNT; ++u) acc[u][0] = pre[u][0], acc[u][1] = pre[u][1];
+            load_g<NP>(items, count, c0, F, j + 1, r, pre);
+            step_mma<NP>(Xs[cur], qa, acc, r);
+            store_tile<NP>(Xs[cur ^ 1], acc, r);
+            store_g<NP>(items, count, c0, F, j + 1, r, acc);
+        }
+        __syncthreads();
+        cur ^= 1;
+    }
+}
+
+template <int NP>
+int chunk_carry_t(double* items, long count, const double* P, int l0, const double* X0, double* work, cudaStream_t s)
+{
+    const long mat = (long)NP * NP;
+    double* arr[16];
+    long cnt[16];
+    int h = 0;
+    arr[0] = items;
+    cnt[0] = count;
+    double* w = work;
+    int launches = 0;
+    while (cnt[h] > kChunk) {
+        if (h + 1 >= 16) throw Error(kInvalidArgument, "chunk carry: too many levels");
+        const long nc = (cnt[h] + kChunk - 1) / kChunk;
+        const unsigned grid = (unsigned)((nc + kCols - 1) / kCols);
+        k_chunk_up<NP><<<grid, kThreads, 0, s>>>(arr[h], cnt[h], P + (long)(l0 + 4 * h) * mat, w);
+        PARODE_CUDA(cudaGetLastError());
+        ++launches;
+        arr[h + 1] = w;
+        cnt[h + 1] = nc;
+        w += nc * NP;
+        ++h;
+    }
+    // top: one chunk of the remaining items, entered with the initial state
+    k_chunk_down<NP><<<1, kThreads, 0, s>>>(arr[h], cnt[h], P + (long)(l0 + 4 * h) * mat, X0, (int)cnt[h]);
+    PARODE_CUDA(cudaGetLastError());
+    ++launches;
+    for (int k = h - 1; k >= 0; --k) {
+        const long nc = (cnt[k] + kChunk - 1) / kChunk;
+        const unsigned grid = (unsigned)((nc + kCols - 1) / kCols);
+        k_chunk_down<NP><<<grid, kThreads, 0, s>>>(arr[k], cnt[k], P + (long)(l0 + 4 * k) * mat, arr[k + 1], kChunk);
+        PARODE_CUDA(cudaGetLastError());
+        ++launches;
+    }
+    return launches;
+}
+
+}  // namespace
+
+int chunk_carry_levels(long count)
+{
+    int h = 0;
+    while (count > kChunk) {
+        count = (count + kChunk - 1) / kChunk;
+        ++h;
+    }
+    return h;
+}
+
+long chunk_carry_scratch(long count)
+{
+    long total = 0;
+    while (count > kChunk) {
+        count = (count + kChunk - 1) / kChunk;
+        total += count;
+    }
+    return total;
+}
+
+int launch_chunk_carry(int NP, double* items, long count, const double* P, int l0, const double* X0, double* work,
+                       cudaStream_t s)
+{
+    if (count <= 0) return 0;
+    switch (NP) {
+    case 8: return chunk_carry_t<8>(items, count, P, l0, X0, work, s);
+    case 16: return chunk_carry_t<16>(items, count, P, l0, X0, work, s);
+    case 24: return chunk_carry_t<24>(items, count, P, l0, X0, work, s);
+    case 32: return chunk_carry_t<32>(items, count, P, l0, X0, work, s);
+    case 40: return chunk_carry_t<40>(items, count, P, l0, X0, work, s);
+    case 48: return chunk_carry_t<48>(items, count, P, l0, X0, work, s);
+    case 56: return chunk_carry_t<56>(items, count, P, l0, X0, work, s);
+    case 64: return chunk_carry_t<64>(items, count, P, l0, X0, work, s);
+    default: throw Error(kInvalidArgument, "chunk carry: NP must be a multiple of 8 up to 64");
+    }
+}
+
+}  // namespace parode

@@ -76,13 +76,8 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
                 brK_ = K;
                 brKpad_ = (K + 1) & ~1;
                 nblocks_ = (nScan_ + shape_.B - 1) / shape_.B;
-                long c3 = nblocks_;
-                int lev3 = shape_.R;
-                while (c3 > shape_.S_items) {
-                    c3 = (c3 + shape_.B - 1) / shape_.B;
-                    lev3 += shape_.R;
-                }
-                levels_ = std::max(lev3 + ilog2(next_pow2(c3)), shape_.R);
+                // the chunked carry over blocks reads P_R .. P_{R + 4 h}
+                levels_ = shape_.R + 4 * chunk_carry_levels(nblocks_) + 1;
             }
         }
         // otherwise the mixed form runs the in-block sweeps on the tensor
@@ -157,7 +152,7 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
         alloc(&dV_, (Tp_ + 1) * (long)Np_);  // a leading slot holds the initial state
     } else {
         alloc(&dG_, nblocks_ * (long)Np_);
-        alloc(&dWork_, blocked_items_scratch(shape_, nblocks_) * (long)Np_);
+        alloc(&dWork_, std::max(blocked_items_scratch(shape_, nblocks_), chunk_carry_scratch(nblocks_) + 1) * (long)Np_);
         alloc(&dCP_, (long)shape_.B * p_ * Np_);
         alloc(&dCext_, (long)p_ * Np_);
         // output rows of the scan state: C at the state block (the last n of
@@ -515,7 +510,7 @@ void Plan::execute_response(double* Y, cudaStream_t s)
         ++launches;
         mark("aggregates+windows", s);
         PARODE_CUDA(cudaStreamWaitEvent(s, fork_[3], 0));
-        launches += launch_blocked_carry(shape_, dG_, nblocks_, shape_.R, dPow_, dX0_, dWork_, sms_, s);
+        launches += launch_chunk_carry(Np_, dG_, nblocks_, dPow_, shape_.R, dX0_, dWork_, s);
         mark("carry", s);
         LevelArgs x;
         x.P = dW_ + brKpad_;
@@ -558,7 +553,7 @@ void Plan::execute_response(double* Y, cudaStream_t s)
     ++launches;
     mark("aggregates", s);
     PARODE_CUDA(cudaStreamWaitEvent(s, fork_[3], 0));
-    launches += launch_blocked_carry(shape_, dG_, nblocks_, shape_.R, dPow_, dX0_, dWork_, sms_, s);
+    launches += launch_chunk_carry(Np_, dG_, nblocks_, dPow_, shape_.R, dX0_, dWork_, s);
     mark("carry", s);
     LevelArgs h = g;
     h.P = dW_;
