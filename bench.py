@@ -35,7 +35,9 @@ WORKLOAD = "cfg2: RK4 n=64 m=8 p=8 h=1e-4 T=2^20, seeded system + sum-of-sinusoi
 # DRAM bytes (read + write) of one leaf launch on this workload, from the ncu
 # captures summarised in profiles/k_leaf_tc_cfg2_rk4_n64.md (mixed) and
 # profiles/k_leaf_fp64_cfg2_rk4_n64.md (FP64); keyed by (T, mixed).
-LEAF_TRAFFIC = {(1 << 20, True): 199.13e6, (1 << 20, False): 202.22e6}
+# DRAM bytes (read + write) of one launch of the dominant kernel at T = 2^20
+# (key: (T, mixed)), from the ncu captures summarised under profiles/.
+DOMINANT_TRAFFIC = {(1 << 20, False): 168.18e6 + 45.27e6, (1 << 20, True): 134.96e6 + 70.68e6}
 
 
 def parse():
@@ -203,13 +205,20 @@ def gemm_peak_tflops(torch, dev, dtype, tf32=False):
     return 2.0 * N ** 3 / best / 1e12
 
 
-def leaf_flops(case, T, B):
-    """Algorithmic FLOPs of the leaf kernel for one solve: forcing, the in-block
-    up/down vector sweeps (2 (B-1)/B matvecs of Ns^2 per step) and outputs."""
-    n, m, p, Ns = case.n, case.m, case.p, case.scan_dim
-    W = 3 if case.solver == 0 else 5
-    per_step = 2 * n * W * m + 4.0 * Ns * Ns * (B - 1) / B + 2 * p * (n + m)
-    return per_step * T
+def response_flops(case, shape, mixed):
+    """Algorithmic FLOPs of one solve on the block-response path, per launch
+    kind.  shape = (B, K, NP, blocks) from the plan.  The aggregate GEMM
+    costs 2 NP K per block; the output GEMM 2 B p (K + NP) per block (window
+    part 2 B p K, initial-state part 2 B p NP); the carry over blocks 4 NP^2
+    per block (up- and down-sweep).  The dominant launch is the output GEMM
+    in FP64 and, in the mixed form, the tensor-core launch that computes the
+    aggregates and the output windows together."""
+    B, K, NP, blocks = shape
+    p = case.p
+    agg, win, state, carry = 2.0 * NP * K * blocks, 2.0 * B * p * K * blocks, 2.0 * B * p * NP * blocks, \
+        4.0 * NP * NP * blocks
+    dominant = (agg + win) if mixed else (win + state)
+    return {"dominant": dominant, "solve": agg + win + state + carry}
 
 
 def _spec(pb, c):
@@ -418,7 +427,7 @@ def run_ours(args):
         per = sorted(s.elapsed_time(e) for s, e in pairs)
         info = {"ms_per_step": float(total.item()) / args.steps, "stages_ms": stages, "launches": plan.launch_count,
                 "solve_ms": {"p50": float(np.percentile(per, 50)), "p99": float(np.percentile(per, 99))},
-                "precision_used": plan.precision, "path": plan.path}
+                "precision_used": plan.precision, "path": plan.path, "response_shape": plan.response_shape}
         y_host = y.cpu().numpy()
         plan.close()
         return info, y_host
@@ -462,8 +471,9 @@ def run_ours(args):
     if rank == 0:
         peaks, peaks_kind = measured_peaks()
         used_mixed = main["precision_used"] == pb.MIXED
-        B = 16  # blocks of the leaf for n = 64 (R = 4)
-        leaf_ms = main["stages_ms"].get("leaf")
+        fl = response_flops(case, main["response_shape"], used_mixed) if main["path"] == 3 else None
+        stage = "aggregates+windows" if used_mixed else "outputs"
+        dom_ms = main["stages_ms"].get(stage)
         if used_mixed:
             tf32 = gemm_peak_tflops(torch, dev, torch.float32, tf32=True)
             peak = tf32 / 3.0
@@ -472,13 +482,17 @@ def run_ours(args):
         else:
             peak = gemm_peak_tflops(torch, dev, torch.float64)
             peak_src = "dense FP64 GEMM measured in this run (cuBLAS DGEMM via torch.matmul)"
-        achieved = leaf_flops(case, case.T, B) / (leaf_ms / 1e3) / 1e12 if leaf_ms else None
-        roofline = {"bound": "tensor", "kernel": "k_leaf_tc (3xTF32 tcgen05)" if used_mixed else "k_leaf (DMMA FP64)",
-                    "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+        achieved = fl["dominant"] / (dom_ms / 1e3) / 1e12 if (fl and dom_ms) else None
+        roofline = {"bound": "tensor",
+                    "kernel": ("k_level_tc: 3xTF32 tcgen05 GEMM of the block aggregates and output windows"
+                               if used_mixed else "k_level_tiled: FP64 DMMA output GEMM y = W [window; X_b]"),
+                    "stage": stage, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                     "frac": (achieved / peak) if achieved else None, "peak_source": peak_src,
-                    "traffic": LEAF_TRAFFIC.get((case.T, used_mixed)), "stages_ms": main["stages_ms"],
-                    "whole_solve_tflops": (4.0 * case.scan_dim ** 2 + 6 * case.n * case.m +
-                                           2 * case.p * (case.n + case.m)) * case.T / (main["ms_per_step"] / 1e3) / 1e12}
+                    "algorithmic_flops_per_launch": fl["dominant"] if fl else None,
+                    "traffic": DOMINANT_TRAFFIC.get((case.T, used_mixed)),
+                    "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch (profiles/)",
+                    "stages_ms": main["stages_ms"],
+                    "whole_solve_tflops": fl["solve"] / (main["ms_per_step"] / 1e3) / 1e12 if fl else None}
         rel_vs_fp64 = None
         if y_plain is not None:
             from oracle import oracle
@@ -500,14 +514,18 @@ def run_ours(args):
             "dtype": "tf32x3+f64" if used_mixed else "f64", "data": "synthetic (seeded system and input)",
             "config": {"workload": WORKLOAD,
                        "precision": "mixed" if used_mixed else "fp64",
-                       "path": {1: "level-synchronous", 2: "blocked"}.get(main["path"], "?"),
+                       "path": {1: "level-synchronous", 2: "blocked, in-block sweeps",
+                                3: "blocked, block-response GEMMs"}.get(main["path"], "?"),
                        "l2": "256 MB flush between timed solves (outside the events)",
                        "parallelism": f"replicas x{world}"},
             "gpu_launches": main["launches"] * args.steps, "solve_ms": main["solve_ms"],
             "clocks": clk.summary(), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "plain_fp64": None if plain is None else {
                 "value": world * case.n * case.T / (plain["ms_per_step"] / 1e3), "ms_per_step": plain["ms_per_step"],
-                "stages_ms": plain["stages_ms"]},
+                "stages_ms": plain["stages_ms"],
+                "output_gemm_tflops": (response_flops(case, plain["response_shape"], False)["dominant"] /
+                                       (plain["stages_ms"]["outputs"] / 1e3) / 1e12)
+                if plain["path"] == 3 and plain["stages_ms"].get("outputs") else None},
             "mixed_over_plain": None if plain is None else plain["ms_per_step"] / main["ms_per_step"],
             "rel_err_mixed_vs_fp64": rel_vs_fp64,
             "peaks": {k: peaks.get(k) for k in ("hbm_gbs", "bf16_tflops", "bf16_tflops_sustained")},

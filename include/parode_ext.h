@@ -82,8 +82,12 @@ int ParODE_PlanLaunchCount(const ParODE_Plan* plan);
 /* Precision form the plan actually runs (PARODE_PRECISION_*): the mixed form
  * falls back to FP64 for shapes its tensor-core leaf does not cover. */
 int ParODE_PlanPrecision(const ParODE_Plan* plan);
-/* Sweep organisation: 1 level-synchronous, 2 blocked. */
+/* Sweep organisation: 1 level-synchronous, 2 blocked with the in-block sweep
+ * leaf, 3 blocked with the block-response GEMM leaf. */
 int ParODE_PlanPath(const ParODE_Plan* plan);
+/* Response leaf geometry (path 3; zeros otherwise): info[0] block length B,
+ * info[1] window columns K, info[2] padded scan dimension NP, info[3] blocks. */
+void ParODE_PlanResponseShape(const ParODE_Plan* plan, long long info[4]);
 void ParODE_PlanDestroy(ParODE_Plan* plan);
 /* Stage timing: when enabled, PlanExecute records CUDA events between its
  * stages on the execution stream.  PlanStageTimes synchronises on the last

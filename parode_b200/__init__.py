@@ -96,6 +96,8 @@ def _load():
     L.ParODE_PlanDestroy.argtypes = [C.c_void_p]
     L.ParODE_PlanPrecision.argtypes = [C.c_void_p]
     L.ParODE_PlanPath.argtypes = [C.c_void_p]
+    L.ParODE_PlanResponseShape.argtypes = [C.c_void_p, C.POINTER(C.c_longlong)]
+    L.ParODE_PlanResponseShape.restype = None
     L.ParODE_PlanSetProfiling.argtypes = [C.c_void_p, C.c_int, ip]
     L.ParODE_PlanStageTimes.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_int, C.c_char_p, C.c_int, ip]
     L.ParODE_PlanStageTimes.restype = C.c_int
@@ -320,6 +322,13 @@ class Plan:
     @property
     def path(self) -> int:
         return int(lib.ParODE_PlanPath(self._h))
+
+    @property
+    def response_shape(self):
+        """(B, K, NP, blocks) of the block-response leaf, zeros on other paths."""
+        info = (C.c_longlong * 4)()
+        lib.ParODE_PlanResponseShape(self._h, info)
+        return tuple(int(v) for v in info)
 
     @property
     def launch_count(self) -> int:

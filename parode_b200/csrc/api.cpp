@@ -488,6 +488,18 @@ int ParODE_PlanPrecision(const ParODE_Plan* plan) { return plan && plan->plan ? 
 
 int ParODE_PlanPath(const ParODE_Plan* plan) { return plan && plan->plan ? plan->plan->path() : -1; }
 
+void ParODE_PlanResponseShape(const ParODE_Plan* plan, long long info[4])
+{
+    if (!info) return;
+    info[0] = info[1] = info[2] = info[3] = 0;
+    if (!plan || !plan->plan || plan->plan->path() != kPathBlockedResponse) return;
+    const Plan& p = *plan->plan;
+    info[0] = p.response_block();
+    info[1] = p.response_window_columns();
+    info[2] = p.padded_dim();
+    info[3] = (p.scan_steps() + info[0] - 1) / info[0];
+}
+
 void ParODE_PlanDestroy(ParODE_Plan* plan) { delete plan; }
 
 void ParODE_PlanSetProfiling(ParODE_Plan* plan, int enable, int nErr[])

@@ -45,12 +45,18 @@ public:
     void get_output(double* t, double* y);
 
     long num_outputs() const { return nOut_; }
+    long scan_steps() const { return nScan_; }
+    int padded_dim() const { return Np_; }
     int channels() const { return p_; }
     int launch_count() const { return launches_; }
     int device() const { return device_; }
     cudaStream_t stream() const { return stream_; }
     const double* device_output() const { return dY_; }
-    int path() const { return path_; }
+    // kPathLevel, kPathBlocked (in-block sweep leaf) or kPathBlockedResponse
+    int path() const { return br_ ? (int)kPathBlockedResponse : path_; }
+    // Response leaf: block length, window columns (0 when not that path)
+    int response_block() const { return br_ ? shape_.B : 0; }
+    int response_window_columns() const { return br_ ? brK_ : 0; }
     int precision_used() const { return precision_used_; }
 
     // Optional stage timing with CUDA events on the execution stream.
