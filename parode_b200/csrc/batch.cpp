@@ -555,7 +555,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             j.base = q.u_base;
             j.dt = q.u_dt;
             j.count = q.nU;
-            maxSample_ = std::max(maxSample_, q.nU * q.mu);
+            maxSample_ = std::max(maxSample_, (q.nU + 31) / 32 * q.mu);  // threads: runs of 32 samples x channels
             sj.push_back(j);
         }
         nSampleJobs_ = (int)sj.size();

@@ -220,7 +220,8 @@ struct CopyJob {
     const double* src = nullptr;  // nullptr: fill with zeros
     long N = 0;
 };
-// max_elems: the largest element count of a job (sizes the x dimension).
+// max_elems: the largest element count of a job (sizes the x dimension); for
+// the samples, runs of 32 samples x channels (one thread each).
 void launch_samples_batch(const SampleJob* dJobs, int njobs, long max_elems, cudaStream_t s);
 void launch_forcing_batch(const ForcingJob* dJobs, int njobs, long max_elems, cudaStream_t s);
 void launch_output_batch(const OutputJob* dJobs, int njobs, long max_elems, cudaStream_t s);

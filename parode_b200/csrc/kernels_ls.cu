@@ -321,15 +321,17 @@ __global__ void k_swap_grouped(const LevelArgs* __restrict__ args)
     swap_body(a);
 }
 
+// One thread per (run of kSampleRun samples, channel); channels fastest.
 __global__ void k_sinusoid_samples(double* U, int m, int K, const double* a, const double* f, const double* phi,
                                    double base, double dt, long count)
 {
-    long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    long total = count * m;
-    if (e >= total) return;
-    long j = e / m;
-    int i = (int)(e - j * m);
-    U[e] = sinusoid_value(a, f, phi, K, i, sample_time(base, dt, j));
+    const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long runs = (count + kSampleRun - 1) / kSampleRun;
+    if (e >= runs * m) return;
+    const long r = e / m;
+    const int i = (int)(e - r * m);
+    const long j0 = r * kSampleRun;
+    sinusoid_run<kSampleRun>(a, f, phi, K, i, base, dt, j0, count, U + j0 * m + i, m);
 }
 
 // V[k][i] = Gamma_k[i]; RK4: Gamma_k = Bbar [u_2k; u_2k+1; u_2k+2] in rows
@@ -396,11 +398,13 @@ __global__ void k_copy(double* dst, const double* src, long N)
 __global__ void k_samples_batch(const SampleJob* __restrict__ jobs)
 {
     const SampleJob J = jobs[blockIdx.y];
-    const long total = J.count * J.m;
+    const long runs = (J.count + kSampleRun - 1) / kSampleRun;
+    const long total = runs * J.m;
     for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
-        const long j = e / J.m;
-        const int i = (int)(e - j * J.m);
-        J.U[e] = sinusoid_value(J.a, J.f, J.phi, J.K, i, sample_time(J.base, J.dt, j));
+        const long r = e / J.m;
+        const int i = (int)(e - r * J.m);
+        const long j0 = r * kSampleRun;
+        sinusoid_run<kSampleRun>(J.a, J.f, J.phi, J.K, i, J.base, J.dt, j0, J.count, J.U + j0 * J.m + i, J.m);
     }
 }
 
@@ -553,8 +557,8 @@ void launch_affine_level(const LevelArgs& a, cudaStream_t s)
 void launch_sinusoid_samples(double* U, int m, int K, const double* a, const double* f, const double* phi,
                              double base, double dt, long count, cudaStream_t s)
 {
-    long total = count * m;
-    if (total <= 0) return;
+    if (count <= 0 || m <= 0) return;
+    const long total = (count + kSampleRun - 1) / kSampleRun * m;
     k_sinusoid_samples<<<blocks_for(total, 256), 256, 0, s>>>(U, m, K, a, f, phi, base, dt, count);
     PARODE_CUDA(cudaGetLastError());
 }
