@@ -229,15 +229,22 @@ def _sys_arrays(A, B, Cm, D, x0):
 
 
 def simulate(A, B, Cm, D, x0, u_index: int, t0: float, t_end: float, h: float, solver: int = RK4,
-             precision: int = FP64):
-    """ParODE_SimulateODE_d: returns (t, y) with y of shape (T, outputs)."""
+             precision: int = FP64, t_out=None, y_out=None):
+    """ParODE_SimulateODE_d: returns (t, y) with y of shape (T, outputs).
+
+    t_out / y_out: optional caller-owned float64 arrays of T and (T, outputs)
+    elements (C-contiguous; pinned host memory makes the copy-out fastest),
+    filled in place and returned instead of new arrays."""
     A, B, Cm, D, x0, n, m, p = _sys_arrays(A, B, Cm, D, x0)
     T = num_outputs(solver, t0, t_end, h)
     if T <= 0:
         raise ParODEError(-6, "simulate")
     q = n if (Cm is None and D is None) else p
-    t = np.zeros(T)
-    y = np.zeros((T, q))
+    t = np.zeros(T) if t_out is None else t_out
+    y = np.zeros((T, q)) if y_out is None else y_out
+    for arr, size in ((t, T), (y, T * q)):
+        if arr.dtype != np.float64 or not arr.flags.c_contiguous or arr.size < size:
+            raise ValueError("simulate: output arrays must be C-contiguous float64 of the output size")
     ns = C.c_longlong(0)
     e = C.c_int(0)
     lib.ParODE_SimulateODE_d(_dp(A), _dp(B), _dp(Cm), _dp(D), m, n, p, int(B is None), int(Cm is None),

@@ -19,19 +19,23 @@
 // MMA reads them (K-major, no swizzle).  The contraction kernel is
 // warp-specialised around a ring of shared-memory stages:
 //   warp 0      producer: per slice one bulk copy (TMA engine) of the 16 KB A
-//               block and one 128-byte bulk copy per vector of B (FP64),
+//               block and one 2D tensor load of B (64 vectors x 16 K, FP64),
 //               completing on the stage's `full` mbarrier;
 //   warps 2-3   converters: B FP64 -> TF32 hi/lo in the canonical layout,
 //               then arrive on `conv`;
-//   warp 1      one thread issues hi*hi + hi*lo + lo*hi into one of two TMEM
-//               accumulators and commits to `empty` (stage free) and, after
-//               every kDrain slices (a drain unit), to `acc_full`;
+//   warp 1      one thread issues hi*hi into one of kAcc TMEM accumulators
+//               and hi*lo + lo*hi into the tile's correction accumulator,
+//               commits to `empty` (stage free) and, after every kDrain
+//               slices (a drain unit), to `acc_full`;
 //   warps 4-7   epilogue: per drain unit TMEM (FP32) -> FP64 running sums in
-//               registers, arrive `acc_empty`; after a tile's last unit
-//               + R v + acc, store.
-// The drains keep each FP32 accumulation chain to kDrain slices (6 kDrain
-// MMAs): the tensor cores' FP32 accumulation error grows with the chain,
-// the FP64 sums across units do not.
+//               registers, arrive `acc_empty`; after a tile's last unit the
+//               corrections too (arrive `corr_empty`), + R v + acc, store.
+// The drains keep each FP32 accumulation chain of hi*hi to kDrain slices
+// (2 kDrain MMAs), and the two corrections accumulate apart, over the whole
+// tile, in a second accumulator read once per tile (they are about 2^-11 of
+// hi*hi, so their FP32 roundings are that much smaller): the tensor cores'
+// FP32 accumulation error grows with the chain, the FP64 sums across units
+// do not.
 // Every wait is bounded; a wait that gives up sets the status word and an
 // abort flag that makes every role leave its loop.
 #include "common.h"
@@ -60,12 +64,14 @@ constexpr uint32_t kOffRaw = kABlock;
 constexpr uint32_t kOffConvB = kABlock + kBRaw;
 constexpr uint32_t kStage = kABlock + kBRaw + 2 * kBHalf;  // 32 KB
 constexpr uint32_t kOffBars = kS * kStage;
-// barriers: full[kS], conv[kS], empty[kS], acc_full[2], acc_empty[2]
-constexpr uint32_t kNumBars = 3 * kS + 4;
+// TMEM: kAcc hi*hi drain buffers of kBN columns, then 2 per-tile correction buffers
+constexpr int kAcc = 4;
+// barriers: full[kS], conv[kS], empty[kS], acc_full[kAcc], acc_empty[kAcc], corr_empty[2]
+constexpr uint32_t kNumBars = 3 * kS + 2 * kAcc + 2;
 constexpr uint32_t kOffSlot = kOffBars + 8 * kNumBars;
 constexpr uint32_t kSmem = kOffSlot + 16;
-constexpr uint32_t kTmemCols = 2 * kBN;
-constexpr int kDrain = 2;  // K slices per FP32 accumulation chain
+constexpr uint32_t kTmemCols = 512;  // hi*hi: kAcc drain buffers; corrections: 2 tile buffers (384 used)
+constexpr int kDrain = 8;  // K slices per FP32 accumulation chain
 constexpr long long kWaitLimit = 1LL << 31;
 
 // Phase-trace hook (no-op unless a timing harness defines it).
@@ -223,7 +229,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
     uint64_t* conv = bars + kS;
     uint64_t* empty = bars + 2 * kS;
     uint64_t* acc_full = bars + 3 * kS;
-    uint64_t* acc_empty = bars + 3 * kS + 2;
+    uint64_t* acc_empty = bars + 3 * kS + kAcc;
+    uint64_t* corr_empty = bars + 3 * kS + 2 * kAcc;
     uint32_t* slot = reinterpret_cast<uint32_t*>(sm + kOffSlot);
     volatile int* abort = reinterpret_cast<volatile int*>(sm + kOffSlot + 8);
     PARODE_TC_TRACE_INIT();
@@ -234,10 +241,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
             mbar_init(&conv[q], 2);
             mbar_init(&empty[q], 1);
         }
-        for (int q = 0; q < 2; ++q) {
+        for (int q = 0; q < kAcc; ++q) {
             mbar_init(&acc_full[q], 1);
             mbar_init(&acc_empty[q], 4);
         }
+        for (int q = 0; q < 2; ++q) mbar_init(&corr_empty[q], 4);
         *abort = 0;
         mbar_fence_init();
     }
@@ -293,22 +301,29 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
         if (lane == 0) {
             Cursor c;
             c.init(args, start, nent, t0, t1);
-            long j = 0, u = 0;  // slice and drain-unit counters
+            long j = 0, u = 0, tt = 0;  // slice, drain-unit and tile counters
             constexpr uint32_t SBO = kBK * 32;
             constexpr uint32_t idesc = make_idesc(kBM, kBN);
             bool ok = true;
-            for (long t = t0; t < t1 && ok && !*abort; ++t) {
+            for (long t = t0; t < t1 && ok && !*abort; ++t, ++tt) {
                 const long lt = c.seek(t);
                 int mi, m0, nk;
                 long n0;
                 tile_coords(c.a, lt, mi, m0, n0, nk);
                 int ab = 0;
                 uint32_t d = 0;
+                // the corrections accumulate over the whole tile, in the
+                // tile-parity buffer, once the epilogue has read it two tiles ago
+                const uint32_t dc = tbase + (uint32_t)(kAcc * kBN + (tt & 1) * kBN);
+                if (tt >= 2 && !role_wait(&corr_empty[tt & 1], (uint32_t)(((tt >> 1) - 1) & 1), abort, status)) {
+                    ok = false;
+                    break;
+                }
                 for (int s = 0; s < nk; ++s, ++j) {
                     if (s % kDrain == 0) {
                         // a new drain unit: wait until the epilogue has read this accumulator
-                        ab = (int)(u & 1);
-                        const long ause = u >> 1;
+                        ab = (int)(u % kAcc);
+                        const long ause = u / kAcc;
                         if (ause >= 1 && !role_wait(&acc_empty[ab], (uint32_t)((ause - 1) & 1), abort, status)) {
                             ok = false;
                             break;
@@ -330,12 +345,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
                     const uint64_t bl = make_desc(stg + kOffConvB + kBHalf, 128, SBO);
                     const uint64_t A[3] = {ah, ah, al};
                     const uint64_t B[3] = {bh, bl, bh};
+                    // hi*hi into the drain unit's accumulator (K/8 FP32
+                    // roundings per unit in the large sum), the two
+                    // corrections (about 2^-11 smaller) into the tile's
+                    // correction accumulator, read once at the tile's end
 #pragma unroll
                     for (int q = 0; q < 3; ++q)
 #pragma unroll
                         for (int k = 0; k < kBK / 8; ++k)
-                            mma_tf32(d, A[q] + (uint64_t)(k * 16), B[q] + (uint64_t)(k * 16), idesc,
-                                     (s % kDrain == 0 && q == 0 && k == 0) ? 0u : 1u);
+                            mma_tf32(q == 0 ? d : dc, A[q] + (uint64_t)(k * 16), B[q] + (uint64_t)(k * 16), idesc,
+                                     ((q == 0 && s % kDrain == 0) || (q == 1 && s == 0)) && k == 0 ? 0u : 1u);
                     mma_commit(&empty[st]);
                     PARODE_TC_TRACE(1);
                     if (s % kDrain == kDrain - 1 || s == nk - 1) {
@@ -368,12 +387,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
                 unsigned char* stg = sm + st * kStage;
                 const double* raw = reinterpret_cast<const double*>(stg + kOffRaw);
                 const int kl = slice_len(level_k(a), s);
-                // 64 vectors x 4 chunks of 4 K; item w -> vector w/4, chunk w%4, so a
-                // warp reads 1 KB and writes 512 B contiguous (no bank conflicts)
+                // 64 vectors x kBK/4 chunks of 4 K; item w -> vector w / (kBK/4),
+                // chunk w % (kBK/4): a warp reads whole vectors and writes
+                // contiguous core-matrix rows
+                constexpr int kChunks = kBK / 4;
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
+                for (int q = 0; q < kChunks; ++q) {
                     const int w = ct + 64 * q;
-                    const int v = w >> 2, kc = (w & 3) * 4;
+                    const int v = w / kChunks, kc = (w % kChunks) * 4;
                     const bool ok = n0 + v < a.ncols && kc < kl;
                     const double2* p = reinterpret_cast<const double2*>(raw + v * kBK + kc);
                     const double2 x0 = ok ? p[0] : make_double2(0.0, 0.0);
@@ -398,9 +419,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
         const int quarter = warp & 3;
         Cursor c;
         c.init(args, start, nent, t0, t1);
-        long u = 0;  // drain units
+        long u = 0, tt = 0;  // drain units, tiles
         bool ok = true;
-        for (long t = t0; t < t1 && ok && !*abort; ++t) {
+        for (long t = t0; t < t1 && ok && !*abort; ++t, ++tt) {
             const long lt = c.seek(t);
             const LevelArgs& a = c.a;
             int mi, m0, nk;
@@ -412,24 +433,34 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
             for (int q = 0; q < kBN; ++q) sum[q] = 0.0;
             const int units = (nk + kDrain - 1) / kDrain;
             for (int v = 0; v < units; ++v, ++u) {
-                const int ab = (int)(u & 1);
-                if (!role_wait(&acc_full[ab], (uint32_t)((u >> 1) & 1), abort, status)) {
+                const int ab = (int)(u % kAcc);
+                if (!role_wait(&acc_full[ab], (uint32_t)((u / kAcc) & 1), abort, status)) {
                     ok = false;
                     break;
                 }
                 PARODE_TC_TRACE(3);
                 fence_after_sync();
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
+                // hi*hi of this unit; at the tile's last unit also the corrections
+                // (read before the arrive below, so a later arrive implies them)
+                const int halves = v == units - 1 ? 4 : 2;
+                for (int h = 0; h < halves; ++h) {
+                    const uint32_t col = h < 2 ? (uint32_t)(ab * kBN + h * 32)
+                                               : (uint32_t)(kAcc * kBN + (tt & 1) * kBN + (h - 2) * 32);
                     uint32_t r[32];
-                    tmem_ld32(tbase + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(ab * kBN + h * 32), r);
+                    tmem_ld32(tbase + ((uint32_t)(32 * quarter) << 16) + col, r);
                     tmem_wait_ld();
 #pragma unroll
-                    for (int q = 0; q < 32; ++q) sum[32 * h + q] += (double)__uint_as_float(r[q]);
+                    for (int q = 0; q < 32; ++q) {
+                        if (h & 1) sum[32 + q] += (double)__uint_as_float(r[q]);
+                        else sum[q] += (double)__uint_as_float(r[q]);
+                    }
                 }
                 fence_before_sync();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&acc_empty[ab]);
+                if (lane == 0) {
+                    mbar_arrive(&acc_empty[ab]);
+                    if (v == units - 1) mbar_arrive(&corr_empty[tt & 1]);
+                }
             }
             if (!ok) break;
             const long i = m0 + 32 * quarter + lane;

@@ -122,6 +122,7 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
     PARODE_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     PARODE_CUDA(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
     for (auto& e : fork_) PARODE_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    PARODE_CUDA(cudaEventCreateWithFlags(&done_, cudaEventDisableTiming));
 
     // ---- host FP64 discretisation --------------------------------------
     const int n = sys.n, mB = sys.zeroB ? 0 : sys.m;
@@ -321,30 +322,62 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
         }
     }
     PARODE_CUDA(cudaStreamSynchronize(stream_));
+    // keep a plan's worth of freed memory in the pool, so that the next plan
+    // of this size (the next SimulateODE call) maps nothing new
+    {
+        cudaMemPool_t pool = nullptr;
+        PARODE_CUDA(cudaDeviceGetDefaultMemPool(&pool, device_));
+        uint64_t keep = 0;
+        PARODE_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+        if (keep < (uint64_t)bytes_) {
+            keep = (uint64_t)bytes_;
+            PARODE_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+        }
+    }
 }
 
 Plan::~Plan()
 {
     cudaSetDevice(device_);
+    // the buffers return to the device's stream-ordered pool once the last
+    // execute (on whatever stream) and the plan's own work are done
+    if (stream_ && done_) cudaStreamWaitEvent(stream_, done_, 0);
+    if (stream_ && side_) {
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess) {
+            cudaEventRecord(e, side_);
+            cudaStreamWaitEvent(stream_, e, 0);
+            cudaEventDestroy(e);
+        }
+    }
+    for (double* p : bufs_) {
+        if (stream_) cudaFreeAsync(p, stream_);
+        else cudaFree(p);
+    }
     if (stream_) cudaStreamSynchronize(stream_);
-    for (cudaEvent_t e : events_) cudaEventDestroy(e);
     if (side_) cudaStreamSynchronize(side_);
+    for (cudaEvent_t e : events_) cudaEventDestroy(e);
     for (cudaEvent_t e : fork_)
         if (e) cudaEventDestroy(e);
+    if (done_) cudaEventDestroy(done_);
     if (side_) cudaStreamDestroy(side_);
-    for (double* p : bufs_) cudaFree(p);
     if (stream_) cudaStreamDestroy(stream_);
 }
 
 void Plan::alloc(double** p, long n)
 {
+    // stream-ordered: plans that come and go (every SimulateODE call makes
+    // one) reuse the pool's memory instead of mapping and unmapping it
     *p = nullptr;
-    cudaError_t e = cudaMalloc((void**)p, sizeof(double) * (size_t)std::max<long>(n, 1));
+    const size_t bytes = sizeof(double) * (size_t)std::max<long>(n, 1);
+    cudaError_t e = cudaMallocAsync((void**)p, bytes, stream_);
     if (e != cudaSuccess) {
         cudaGetLastError();
+        *p = nullptr;
         throw Error(kNotEnoughResources, "device allocation failed");
     }
     bufs_.push_back(*p);
+    bytes_ += bytes;
 }
 
 void Plan::set_profiling(bool on) { profiling_ = on; }
@@ -384,6 +417,12 @@ void Plan::execute(double* y, cudaStream_t s)
 {
     PARODE_CUDA(cudaSetDevice(device_));
     if (!s) s = stream_;
+    execute_body(y, s);
+    PARODE_CUDA(cudaEventRecord(done_, s));
+}
+
+void Plan::execute_body(double* y, cudaStream_t s)
+{
     if (path_ == kPathBlocked) {
         execute_blocked(y ? y : dY_, s);
         return;
@@ -661,12 +700,19 @@ void Plan::execute_blocked(double* Y, cudaStream_t s)
 void Plan::get_output(double* t, double* y)
 {
     PARODE_CUDA(cudaSetDevice(device_));
-    PARODE_CUDA(cudaDeviceSynchronize());
+    // the copy of y queues behind the last execute (whatever its stream); the
+    // host computes the time vector meanwhile (into pinned memory the copy
+    // runs asynchronously; into pageable memory cudaMemcpyAsync returns when
+    // it is done)
+    PARODE_CUDA(cudaStreamWaitEvent(stream_, done_, 0));
+    if (y)
+        PARODE_CUDA(cudaMemcpyAsync(y, last_y_ ? last_y_ : dY_, sizeof(double) * nOut_ * p_, cudaMemcpyDeviceToHost,
+                                    stream_));
+    if (t) time_vector(solver_, t0_, tEnd_, h_, t);
+    PARODE_CUDA(cudaStreamSynchronize(stream_));
     int status = 0;
     PARODE_CUDA(cudaMemcpy(&status, dStatus_, sizeof(int), cudaMemcpyDeviceToHost));
     if (status != 0) throw Error(kDeviceError, "a device-side wait gave up (tensor-core completion not observed)");
-    if (y) PARODE_CUDA(cudaMemcpy(y, last_y_ ? last_y_ : dY_, sizeof(double) * nOut_ * p_, cudaMemcpyDeviceToHost));
-    if (t) time_vector(solver_, t0_, tEnd_, h_, t);
 }
 
 }  // namespace parode

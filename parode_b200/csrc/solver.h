@@ -67,6 +67,7 @@ public:
 private:
     void alloc(double** p, long n);
     void mark(const char* stage, cudaStream_t s);
+    void execute_body(double* y, cudaStream_t s);
     void execute_blocked(double* Y, cudaStream_t s);
     void execute_response(double* Y, cudaStream_t s);
     void fill_inputs(cudaStream_t s);
@@ -109,6 +110,8 @@ private:
     int* dStatus_ = nullptr;
     cudaStream_t side_ = nullptr;
     cudaEvent_t fork_[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t done_ = nullptr;  // recorded after each execute on its stream
+    size_t bytes_ = 0;            // device bytes the plan holds
     bool profiling_ = false;
     std::vector<cudaEvent_t> events_;
     std::vector<std::string> marks_;
