@@ -492,12 +492,8 @@ void ParODE_PlanResponseShape(const ParODE_Plan* plan, long long info[4])
 {
     if (!info) return;
     info[0] = info[1] = info[2] = info[3] = 0;
-    if (!plan || !plan->plan || plan->plan->path() != kPathBlockedResponse) return;
-    const Plan& p = *plan->plan;
-    info[0] = p.response_block();
-    info[1] = p.response_window_columns();
-    info[2] = p.padded_dim();
-    info[3] = (p.scan_steps() + info[0] - 1) / info[0];
+    if (!plan || !plan->plan) return;
+    plan->plan->response_shape(info);
 }
 
 void ParODE_PlanDestroy(ParODE_Plan* plan) { delete plan; }

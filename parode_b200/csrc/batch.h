@@ -61,6 +61,16 @@ public:
     {
         return sys_[i].resp ? kPathBlockedResponse : sys_[i].blocked ? kPathBlocked : kPathLevel;
     }
+    // Response leaf geometry of system i: block length, window columns,
+    // padded scan dimension, blocks (zeros on other paths).
+    void response_shape(int i, long long info[4]) const
+    {
+        const Sys& q = sys_[i];
+        info[0] = q.resp ? q.Bk : 0;
+        info[1] = q.resp ? q.Kw : 0;
+        info[2] = q.resp ? q.Np : 0;
+        info[3] = q.resp ? q.nblocks : 0;
+    }
     // Sum over systems of n * outputs (state*steps of one execute).
     double state_steps() const;
     size_t device_bytes() const { return arena_bytes_; }

@@ -1,6 +1,7 @@
 // solver.cpp -- plan set-up and execution (see solver.h).
 #include "solver.h"
 
+#include "batch.h"
 #include "common.h"
 #include "kernels.h"
 
@@ -35,6 +36,28 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
     Ns_ = solver == kRK4 ? sys.n : 4 * sys.n;
     Np_ = (int)round_up(Ns_, 8);
     if (Np_ > 1024) throw Error(kInvalidSystem, "scan dimension above 1024 is not supported");
+    if (Ns_ > 64 && opt.path != kPathBlocked && opt.path != kPathBlockedSweep) {
+        // scan dimensions above 64: the batch engine's one-system form (the
+        // response leaf or the level-synchronous scan, tensor-core levels in
+        // the mixed form)
+        PARODE_CUDA(cudaSetDevice(device_));
+        PARODE_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+        PARODE_CUDA(cudaEventCreateWithFlags(&done_, cudaEventDisableTiming));
+        BatchSpec b;
+        b.sys = sys;
+        b.uIndex = uIndex;
+        b.solver = solver;
+        b.t0 = t0;
+        b.tEnd = tEnd;
+        b.h = h;
+        b.input = input_;
+        std::vector<BatchSpec> specs;
+        specs.push_back(std::move(b));
+        batch_ = std::make_unique<BatchPlan>(device, std::move(specs), inputs, opt);
+        precision_used_ = batch_->precision_used(0);
+        path_ = batch_->path(0);
+        return;
+    }
     Tp_ = next_pow2(nScan_);
     levels_ = ilog2(Tp_);
     path_ = kPathLevel;
@@ -339,6 +362,14 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
 Plan::~Plan()
 {
     cudaSetDevice(device_);
+    if (batch_) {
+        // the batch's work joins into the caller's stream or this plan's
+        if (stream_) {
+            if (done_) cudaStreamWaitEvent(stream_, done_, 0);
+            cudaStreamSynchronize(stream_);
+        }
+        batch_.reset();
+    }
     // the buffers return to the device's stream-ordered pool once the last
     // execute (on whatever stream) and the plan's own work are done
     if (stream_ && done_) cudaStreamWaitEvent(stream_, done_, 0);
@@ -421,8 +452,33 @@ void Plan::execute(double* y, cudaStream_t s)
     PARODE_CUDA(cudaEventRecord(done_, s));
 }
 
+const double* Plan::device_output() const { return batch_ ? batch_->device_output(0) : dY_; }
+
+void Plan::response_shape(long long info[4]) const
+{
+    info[0] = info[1] = info[2] = info[3] = 0;
+    if (batch_) {
+        batch_->response_shape(0, info);
+        return;
+    }
+    if (!br_) return;
+    info[0] = shape_.B;
+    info[1] = brK_;
+    info[2] = Np_;
+    info[3] = (nScan_ + shape_.B - 1) / shape_.B;
+}
+
 void Plan::execute_body(double* y, cudaStream_t s)
 {
+    if (batch_) {
+        batch_->execute(s);
+        if (y)
+            PARODE_CUDA(cudaMemcpyAsync(y, batch_->device_output(0), sizeof(double) * (size_t)nOut_ * p_,
+                                        cudaMemcpyDeviceToDevice, s));
+        launches_ = batch_->launch_count() + (y ? 1 : 0);
+        last_y_ = y;
+        return;
+    }
     if (path_ == kPathBlocked) {
         execute_blocked(y ? y : dY_, s);
         return;
@@ -700,6 +756,12 @@ void Plan::execute_blocked(double* Y, cudaStream_t s)
 void Plan::get_output(double* t, double* y)
 {
     PARODE_CUDA(cudaSetDevice(device_));
+    if (batch_) {
+        PARODE_CUDA(cudaStreamWaitEvent(stream_, done_, 0));
+        PARODE_CUDA(cudaStreamSynchronize(stream_));
+        batch_->get_output(0, t, y);
+        return;
+    }
     // the copy of y queues behind the last execute (whatever its stream); the
     // host computes the time vector meanwhile (into pinned memory the copy
     // runs asynchronously; into pageable memory cudaMemcpyAsync returns when

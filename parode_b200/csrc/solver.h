@@ -13,11 +13,14 @@
 
 #include <cuda_runtime.h>
 
+#include <memory>
 #include <string>
 #include <utility>
 #include <vector>
 
 namespace parode {
+
+class BatchPlan;
 
 // kPathBlocked chooses the leaf by cost; kPathBlockedResponse / kPathBlockedSweep
 // force the block-response GEMM leaf / the in-block sweep leaf.
@@ -47,16 +50,20 @@ public:
     long num_outputs() const { return nOut_; }
     long scan_steps() const { return nScan_; }
     int padded_dim() const { return Np_; }
+    // Scan dimensions above 64 run as a one-system BatchPlan (batch.h): the
+    // response leaf with a level-synchronous scan over blocks, or the
+    // level-synchronous scan over steps, with the batch's tensor-core levels.
+    bool delegated() const { return (bool)batch_; }
     int channels() const { return p_; }
     int launch_count() const { return launches_; }
     int device() const { return device_; }
     cudaStream_t stream() const { return stream_; }
-    const double* device_output() const { return dY_; }
+    const double* device_output() const;
     // kPathLevel, kPathBlocked (in-block sweep leaf) or kPathBlockedResponse
     int path() const { return br_ ? (int)kPathBlockedResponse : path_; }
-    // Response leaf: block length, window columns (0 when not that path)
-    int response_block() const { return br_ ? shape_.B : 0; }
-    int response_window_columns() const { return br_ ? brK_ : 0; }
+    // Response leaf: block length, window columns, padded scan dimension,
+    // blocks (zeros when not that path)
+    void response_shape(long long info[4]) const;
     int precision_used() const { return precision_used_; }
 
     // Optional stage timing with CUDA events on the execution stream.
@@ -112,6 +119,7 @@ private:
     cudaEvent_t fork_[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t done_ = nullptr;  // recorded after each execute on its stream
     size_t bytes_ = 0;            // device bytes the plan holds
+    std::unique_ptr<BatchPlan> batch_;
     bool profiling_ = false;
     std::vector<cudaEvent_t> events_;
     std::vector<std::string> marks_;

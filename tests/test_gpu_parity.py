@@ -110,6 +110,31 @@ def test_plan_reuse_and_launch_count(pb):
     plan.close()
 
 
+@pytest.mark.parametrize("solver,n,m,p,T", [(1, 40, 4, 3, 2500), (0, 100, 6, 5, 3000)])
+def test_large_scan_plan_runs_as_one_system_batch(pb, solver, n, m, p, T):
+    """Scan dimensions above 64: the plan runs the batch engine's one-system
+    form (response leaf, scan over blocks); repeated executes, a caller
+    device buffer on a caller stream, and the host copy all agree."""
+    import torch
+
+    pb.set_option(pb.OPT_PATH, 0)
+    case = wl.small(7100 + n, solver, n, m, p, T, h=1e-3)
+    u = pb.register_sinusoid(case.u.a, case.u.f, case.u.phi)
+    plan = pb.Plan(case.A, case.B, case.C, case.D, case.x0, u, case.t0, case.t_end, case.h, solver=solver)
+    assert plan.path == 3 and plan.response_shape[0] > 0, (plan.path, plan.response_shape)
+    plan.execute()
+    _, y1 = plan.output()
+    ydev = torch.zeros((plan.num_outputs, plan.channels), dtype=torch.float64, device="cuda")
+    stream = torch.cuda.Stream()
+    plan.execute(ydev.data_ptr(), stream.cuda_stream)
+    stream.synchronize()
+    _, y2 = plan.output()
+    assert np.array_equal(y1, y2)
+    assert np.array_equal(ydev.cpu().numpy(), y1)
+    assert oracle.rel_err(y1, _oracle_y(case)) <= TOL_FP64
+    plan.close()
+
+
 def _fx_input(kind):
     if kind == "sin_cos":
         return lambda t, i: math.sin(t) if i == 0 else (math.cos(t) if i == 1 else 0.0)
