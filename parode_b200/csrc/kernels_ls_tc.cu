@@ -286,10 +286,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
                 // A: one 16 KB bulk copy; B: one 2D tensor load of 64 vectors x
                 // 16 K (FP64; x = 16 s, a multiple of 16 bytes; the tails beyond
                 // K or ncols are zero-filled by the TMA engine)
+                // Only the M-tile's valid rows of A travel (8-row core-matrix
+                // groups, hi and lo): the MMA's other rows read whatever the
+                // stage held, and their results are never stored.
                 if (lane == 0) {
-                    mbar_arrive_tx(&full[st], kABlock + kBRaw);
-                    bulk_g2s(stg, reinterpret_cast<const unsigned char*>(a.Ps) + ((size_t)mi * nk + s) * kABlock,
-                             kABlock, &full[st]);
+                    const int rowsv = level_rows(a) - m0 < kBM ? level_rows(a) - m0 : kBM;
+                    const uint32_t abytes = (uint32_t)((rowsv + 7) / 8) * (uint32_t)(kBK * 32);
+                    const unsigned char* ab = reinterpret_cast<const unsigned char*>(a.Ps) + ((size_t)mi * nk + s) * kABlock;
+                    mbar_arrive_tx(&full[st], 2 * abytes + kBRaw);
+                    bulk_g2s(stg, ab, abytes, &full[st]);
+                    bulk_g2s(stg + kAHalf, ab + kAHalf, abytes, &full[st]);
                     tma_load_2d(stg + kOffRaw, a.src_map, s * kBK, (int)n0, &full[st]);
                 }
                 __syncwarp();
