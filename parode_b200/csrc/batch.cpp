@@ -1003,8 +1003,6 @@ void BatchPlan::build_responses()
         int maxR = 0;
         for (; k < rs_.size(); ++k) {
             const Sys& q = sys_[rs_[k]];
-            const size_t need = sizeof(double) * (size_t)q.Bk * q.Np * ((size_t)q.p + q.n);
-            if (!ra.empty() && ws + need > cap) break;
             ResponseArgs a;
             a.solver = q.solver;
             a.n = q.n;
@@ -1022,6 +1020,8 @@ void BatchPlan::build_responses()
             a.K = q.Kw;
             a.Kpad = q.Kpad;
             a.NPstate = q.Np;
+            const size_t need = sizeof(double) * response_workspace_doubles(a);
+            if (!ra.empty() && ws + need > cap) break;
             a.CPt = reinterpret_cast<double*>(ws);  // offsets until the workspace exists
             ra.push_back(a);
             pow.push_back(q.P);
@@ -1030,15 +1030,14 @@ void BatchPlan::build_responses()
         }
         const int nent = (int)ra.size();
         char* buf = nullptr;
-        // meta: the entries, their CTA starts, and per doubling step the GEMM
-        // arguments and tile starts
+        // meta: the entries, their CTA starts, and per doubling step (and the
+        // product step) the GEMM arguments and tile starts
         const size_t meta = align_up(sizeof(ResponseArgs) * nent) + 2 * align_up(sizeof(long) * nent) +
-                            (size_t)maxR * (align_up(2 * sizeof(LevelArgs) * nent) + align_up(2 * sizeof(long) * nent));
+                            (size_t)(maxR + 1) * (align_up(2 * sizeof(LevelArgs) * nent) + align_up(2 * sizeof(long) * nent));
         PARODE_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&buf), ws + meta, stream_));
         for (ResponseArgs& a : ra) {
             const size_t off = reinterpret_cast<size_t>(a.CPt);
-            a.CPt = reinterpret_cast<double*>(buf + off);
-            a.Qt = a.CPt + (size_t)a.B * a.p * a.NP;
+            response_workspace_carve(a, reinterpret_cast<double*>(buf + off));
         }
         std::vector<long> is(nent), fs(nent);
         long ictas = 0, fctas = 0;
@@ -1068,11 +1067,14 @@ void BatchPlan::build_responses()
             long tiles;
         };
         std::vector<Step> steps;
-        for (int l = 0; l < maxR; ++l) {
+        for (int l = 0; l <= maxR; ++l) {
+            // l < maxR: doubling step l; l == maxR: the products with Bbar
             std::vector<LevelArgs> ents;
             for (int e = 0; e < nent; ++e) {
                 LevelArgs two[2];
-                const int c = response_doubling_args(ra[e], pow[e], l, two);
+                int c = 2;
+                if (l < maxR) c = response_doubling_args(ra[e], pow[e], l, two);
+                else response_product_args(ra[e], two);
                 for (int q = 0; q < c; ++q) ents.push_back(level_grouped_args(two[q]));
             }
             if (ents.empty()) continue;

@@ -71,26 +71,38 @@ struct ResponseArgs {
     double* Wm = nullptr;          // row stride Kpad + NPstate
     int K = 0, Kpad = 0;           // window columns, padded to even
     int NPstate = 0;               // NP: also the initial-state columns (z_0 = I on them), or 0
-    // launch_response_init / response_doubling_args / launch_response_fill
-    // only: workspace of B p NP doubles (CP_j = Cext Phi^j, block j at j p NP)
-    // and NP x B n doubles (Q_k = Phi^k restricted to the n forcing columns,
-    // row-major with pitch B n, Q_k at columns k n .. k n + n)
+    // launch_response_init / response_doubling_args / response_product_args /
+    // launch_response_fill only, carved from one workspace of
+    // response_workspace_doubles by response_workspace_carve:
+    // CPt: B p x NP (CP_j = Cext Phi^j, block j at j p NP);
+    // Qt: NP x B n2 (Q_k = Phi^k restricted to the n forcing columns, row-major
+    //     with pitch B n2, Q_k at columns k n2, n2 = n rounded up to even);
+    // BbarE: NP x WM2 (Bbar in the forcing rows, WM2 = W m rounded up to even);
+    // MT: B p x WM2 (CP_L Bbar per slot), NT: NP B x WM2 (Q_L Bbar per slot).
     double* CPt = nullptr;
     double* Qt = nullptr;
+    double* BbarE = nullptr;
+    double* MT = nullptr;
+    double* NT = nullptr;
 };
 // Window length (columns of W) for B steps: RK4 (2B + 1) m, ABM (B + 4) m.
 int response_window(int solver, int B, int m);
 void launch_block_response(const ResponseArgs* dArgs, int nsys, int max_np, int max_p, int max_kpad, cudaStream_t s);
 // The same W for any NP, over many systems.  dStart[e] is entry e's first CTA
 // (response_init_ctas / response_fill_ctas CTAs each, `ctas` in total).
-// Order: init (CP_0, Q_0); for l = 0 .. log2(B) - 1 the tiled GEMMs of
+// Order: init (CP_0, Q_0, BbarE); for l = 0 .. log2(B) - 1 the tiled GEMMs of
 // response_doubling_args (P = the power table, P_l at l NP^2), which double
-// the tables from 2^l to 2^(l+1) entries; then one fill.
+// the tables from 2^l to 2^(l+1) entries; the two GEMMs of
+// response_product_args; then one fill.
 long response_init_ctas(const ResponseArgs& a);
 long response_fill_ctas(const ResponseArgs& a);
 void launch_response_init(const ResponseArgs* dArgs, const long* dStart, int nent, long ctas, cudaStream_t s);
 // Fills out[0..1] (N-contiguous tiled GEMMs) and returns their count (0 once 2^l >= B).
 int response_doubling_args(const ResponseArgs& a, const double* P, int l, LevelArgs out[2]);
+// The two GEMMs that fold the slots of Bbar into the tables (MT and NT), after the doubling.
+void response_product_args(const ResponseArgs& a, LevelArgs out[2]);
+size_t response_workspace_doubles(const ResponseArgs& a);
+void response_workspace_carve(ResponseArgs& a, double* ws);
 void launch_response_fill(const ResponseArgs* dArgs, const long* dStart, int nent, long ctas, cudaStream_t s);
 // Block length 2^R of the response leaf for one system, and its cost in
 // FP64-equivalent flops per step (the two GEMMs and a level-synchronous carry

@@ -103,8 +103,14 @@ __global__ void __launch_bounds__(kThreads) k_block_response(const ResponseArgs*
 // Q_k = Phi^k restricted to the forcing columns (NP x n), k < B, instead of
 // B full NP x NP products.  Both tables double with the power table
 // P_l = Phi^(2^l): CP_{k + 2^l} = CP_k P_l and Q_{k + 2^l} = P_l Q_k, one
-// GEMM launch per l for all k < 2^l (response_doubling_args).
+// GEMM launch per l for all k < 2^l (response_doubling_args).  Then two
+// GEMMs fold in the slots of Bbar (response_product_args):
+//   MT[(L, o)][(w, c)] = (CP_L Bbar_w)[o][c],   NT[(r, L)][(w, c)] = (Q_L Bbar_w)[r][c],
+// so every element of W is a sum of at most 5 table entries.
 // ---------------------------------------------------------------------------
+
+__host__ __device__ inline int resp_n2(const ResponseArgs& a) { return (a.n + 1) & ~1; }
+__host__ __device__ inline int resp_wm2(const ResponseArgs& a) { return ((a.solver == 0 ? 3 : 5) * a.m + 1) & ~1; }
 
 constexpr int kPerThread = 4;
 constexpr int kPerCta = kThreads * kPerThread;
@@ -120,39 +126,46 @@ __device__ __forceinline__ int find_entry(const long* __restrict__ start, int ne
     return lo;
 }
 
-// CP_0 = Cext and Q_0 = the identity's forcing columns.
+// CP_0 = Cext, Q_0 = the identity's forcing columns (n2 = n rounded up to
+// even columns, the last one zero when n is odd), and BbarE = Bbar in the
+// forcing rows of an NP x WM2 zero matrix (WM2 = W m rounded up to even).
 __global__ void __launch_bounds__(kThreads) k_response_init(const ResponseArgs* __restrict__ args,
                                                              const long* __restrict__ start, int nent)
 {
     const int e = find_entry(start, nent, blockIdx.x);
     const ResponseArgs& a = args[e];
-    const int NP = a.NP, p = a.p, n = a.n;
+    const int NP = a.NP, p = a.p, n = a.n, n2 = resp_n2(a), wm2 = resp_wm2(a);
+    const int Wm = (a.solver == 0 ? 3 : 5) * a.m;
     const int coff = a.solver == 0 ? 0 : 3 * n;
-    const long ncp = (long)p * NP, total = ncp + (long)NP * n, ldq = (long)a.B * n;
+    const long ncp = (long)p * NP, nq = (long)NP * n2, ldq = (long)a.B * n2;
+    const long total = ncp + nq + (long)NP * wm2;
     const long base = (blockIdx.x - start[e]) * (long)kPerCta + threadIdx.x;
     for (int t = 0; t < kPerThread; ++t) {
         const long idx = base + (long)t * kThreads;
         if (idx >= total) break;
         if (idx < ncp) {
             a.CPt[idx] = a.Cext[idx];
-        } else {
+        } else if (idx < ncp + nq) {
             const long u = idx - ncp;
-            const int r = (int)(u / n), c = (int)(u - (long)r * n);
-            a.Qt[r * ldq + c] = (r == coff + c) ? 1.0 : 0.0;
+            const int r = (int)(u / n2), c = (int)(u - (long)r * n2);
+            a.Qt[r * ldq + c] = (c < n && r == coff + c) ? 1.0 : 0.0;
+        } else {
+            const long u = idx - ncp - nq;
+            const int r = (int)(u / wm2), c = (int)(u - (long)r * wm2);
+            a.BbarE[u] = (!a.zeroB && r >= coff && r < coff + n && c < Wm) ? a.Bbar[(long)(r - coff) * Wm + c] : 0.0;
         }
     }
 }
 
-// Every element of W from the tables.
+// Every element of W from the tables: sums over the steps i whose forcing
+// reads the element's sample (slot w = s - 2i for RK4, s - i for ABM).
 __global__ void __launch_bounds__(kThreads) k_response_fill(const ResponseArgs* __restrict__ args,
                                                              const long* __restrict__ start, int nent)
 {
     const int e = find_entry(start, nent, blockIdx.x);
     const ResponseArgs& a = args[e];
-    const int NP = a.NP, p = a.p, n = a.n, m = a.m, B = a.B;
+    const int NP = a.NP, p = a.p, m = a.m, B = a.B, wm2 = resp_wm2(a);
     const bool rk4 = a.solver == 0;
-    const int W = rk4 ? 3 : 5;
-    const int coff = rk4 ? 0 : 3 * n;
     const long ld = a.Kpad + a.NPstate;
     const long total = ((long)B * p + NP) * ld;
     const long ncp = (long)p * NP;
@@ -165,28 +178,21 @@ __global__ void __launch_bounds__(kThreads) k_response_fill(const ResponseArgs* 
         double v = 0.0;
         if (col < a.K) {
             const int s = col / m, c = col - s * m;
-            // steps i whose forcing reads sample s (slot w = s - 2i or s - i)
             const int ilo = rk4 ? (s - 1) / 2 : s - 4;  // (s - 2 + 1) / 2 rounds up for s >= 1
             const int ihi = rk4 ? s / 2 : s;
             if (row < (long)B * p) {
                 const int j = (int)(row / p), o = (int)(row - (long)j * p);
-                if (!a.zeroB)
-                    for (int i = max(ilo, 0); i <= min(ihi, j - 1); ++i) {
-                        const int w = rk4 ? s - 2 * i : s - i;
-                        const double* cpr = a.CPt + (long)(j - 1 - i) * ncp + (long)o * NP + coff;
-                        const double* bb = a.Bbar + (long)w * m + c;
-                        for (int r = 0; r < n; ++r) v = fma(cpr[r], bb[(long)r * W * m], v);
-                    }
+                for (int i = max(ilo, 0); i <= min(ihi, j - 1); ++i) {
+                    const int w = rk4 ? s - 2 * i : s - i;
+                    v += a.MT[((long)(j - 1 - i) * p + o) * wm2 + w * m + c];
+                }
                 if (!a.zeroD && s == (rk4 ? 2 * j : j + 3)) v += a.D[(long)o * m + c];
             } else {
-                const int r = (int)(row - (long)B * p);
-                if (!a.zeroB)
-                    for (int i = max(ilo, 0); i <= min(ihi, B - 1); ++i) {
-                        const int w = rk4 ? s - 2 * i : s - i;
-                        const double* qr = a.Qt + (long)r * B * n + (long)(B - 1 - i) * n;
-                        const double* bb = a.Bbar + (long)w * m + c;
-                        for (int k = 0; k < n; ++k) v = fma(qr[k], bb[(long)k * W * m], v);
-                    }
+                const long r = row - (long)B * p;
+                for (int i = max(ilo, 0); i <= min(ihi, B - 1); ++i) {
+                    const int w = rk4 ? s - 2 * i : s - i;
+                    v += a.NT[(r * B + (B - 1 - i)) * wm2 + w * m + c];
+                }
             }
         } else if (col >= a.Kpad && row < (long)B * p) {
             // initial-state columns of the output rows: Cext Phi^j
@@ -206,8 +212,60 @@ int response_window(int solver, int B, int m)
 
 long response_init_ctas(const ResponseArgs& a)
 {
-    const long total = (long)a.p * a.NP + (long)a.NP * a.n;
+    const long total = (long)a.p * a.NP + (long)a.NP * resp_n2(a) + (long)a.NP * resp_wm2(a);
     return (total + kPerCta - 1) / kPerCta;
+}
+
+size_t response_workspace_doubles(const ResponseArgs& a)
+{
+    const size_t B = a.B, NP = a.NP, n2 = resp_n2(a), wm2 = resp_wm2(a);
+    // CPt, Qt, BbarE, MT, NT
+    return B * a.p * NP + NP * B * n2 + NP * wm2 + B * a.p * wm2 + NP * B * wm2;
+}
+
+void response_workspace_carve(ResponseArgs& a, double* ws)
+{
+    const size_t B = a.B, NP = a.NP, n2 = resp_n2(a), wm2 = resp_wm2(a);
+    a.CPt = ws;
+    a.Qt = a.CPt + B * a.p * NP;
+    a.BbarE = a.Qt + NP * B * n2;
+    a.MT = a.BbarE + NP * wm2;
+    a.NT = a.MT + B * a.p * wm2;
+}
+
+void response_product_args(const ResponseArgs& a, LevelArgs out[2])
+{
+    const int wm2 = resp_wm2(a), n2 = resp_n2(a), coff = a.solver == 0 ? 0 : 3 * a.n;
+    // MT = CPt (B p x NP) x BbarE (NP x WM2), the source N-contiguous
+    LevelArgs mt;
+    mt.P = a.CPt;
+    mt.ldp = a.NP;
+    mt.Np = a.NP;
+    mt.M = a.B * a.p;
+    mt.K = a.NP;
+    mt.ncols = wm2;
+    mt.src = a.BbarE;
+    mt.src_gs = 1;
+    mt.src_ks = wm2;
+    mt.dst = a.MT;
+    mt.dst_gs = 1;
+    mt.dst_is = wm2;
+    // NT = Qt as NP B rows (r, L) of n2 (row pitch n2) x the forcing rows of BbarE
+    LevelArgs nt;
+    nt.P = a.Qt;
+    nt.ldp = n2;
+    nt.Np = a.NP;
+    nt.M = a.NP * a.B;
+    nt.K = n2;
+    nt.ncols = wm2;
+    nt.src = a.BbarE + (long)coff * wm2;
+    nt.src_gs = 1;
+    nt.src_ks = wm2;
+    nt.dst = a.NT;
+    nt.dst_gs = 1;
+    nt.dst_is = wm2;
+    out[0] = mt;
+    out[1] = nt;
 }
 
 long response_fill_ctas(const ResponseArgs& a)
@@ -228,21 +286,21 @@ int response_doubling_args(const ResponseArgs& a, const double* P, int l, LevelA
 {
     const int half = 1 << l;
     if (half >= a.B) return 0;
-    const long NP = a.NP, ldq = (long)a.B * a.n;
+    const long NP = a.NP, n2 = resp_n2(a), ldq = (long)a.B * n2;
     const double* Pl = P + (long)l * NP * NP;
-    // Q_{k + 2^l} = P_l Q_k, k < 2^l: the first 2^l n columns of Qt (row pitch
-    // B n) into the next 2^l n; the source is N-contiguous
+    // Q_{k + 2^l} = P_l Q_k, k < 2^l: the first 2^l n2 columns of Qt (row pitch
+    // B n2) into the next 2^l n2; the source is N-contiguous
     LevelArgs q;
     q.P = Pl;
     q.ldp = NP;
     q.Np = a.NP;
     q.M = a.NP;
     q.K = a.NP;
-    q.ncols = (long)half * a.n;
+    q.ncols = (long)half * n2;
     q.src = a.Qt;
     q.src_gs = 1;
     q.src_ks = ldq;
-    q.dst = a.Qt + (long)half * a.n;
+    q.dst = a.Qt + (long)half * n2;
     q.dst_gs = 1;
     q.dst_is = ldq;
     // CP_{k + 2^l} = CP_k P_l, k < 2^l: rows (k, o) of CPt are the MMA's rows,

@@ -75,6 +75,23 @@ Server::Server(int device, InputRegistry* inputs, std::recursive_mutex* inputs_m
         PARODE_CUDA(cudaDeviceGetDefaultMemPool(&pool, device_));
         uint64_t keep = (uint64_t)opt_.hbm_budget;
         PARODE_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+        // map part of the budget now (the pool keeps it once freed), so the
+        // first batches do not pay for growing the pool on the request path
+        size_t free_b = 0, total_b = 0;
+        PARODE_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        const size_t warm = std::min<size_t>({(size_t)opt_.hbm_budget, free_b / 2, opt_.prewarm_bytes});
+        if (warm > 0) {
+            cudaStream_t st = nullptr;
+            PARODE_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+            void* p = nullptr;
+            if (cudaMallocAsync(&p, warm, st) == cudaSuccess) {
+                cudaFreeAsync(p, st);
+            } else {
+                cudaGetLastError();  // a smaller pool just grows later
+            }
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+        }
     }
     for (int k = 0; k < std::max(1, opt_.setup_threads); ++k) workers_.emplace_back([this] { worker(); });
     thread_ = std::thread([this] { loop(); });
@@ -261,6 +278,7 @@ void Server::worker()
             PlanOptions po;
             po.precision = opt_.precision;
             po.input_double = true;
+            po.log = opt_.log;
             if (resolved) {
                 f.plan = std::make_unique<BatchPlan>(device_, std::move(specs), inputs_, po);
             } else {

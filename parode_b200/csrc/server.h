@@ -33,6 +33,10 @@ struct ServerOptions {
     int max_batch = 256;        // systems per batch
     int max_inflight = 8;       // batches on the device (or being set up) at once
     int setup_threads = 4;      // host threads building batches concurrently
+    bool log = false;           // each batch's set-up phase times on stderr
+    // device memory mapped into the stream-ordered pool at creation (at most
+    // the budget and half the free memory)
+    size_t prewarm_bytes = (size_t)32 << 30;
 };
 
 struct ServerStats {
