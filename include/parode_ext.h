@@ -138,12 +138,18 @@ void ParODE_SimulateODEBatch(int nSystems, const double* const A[], const double
  * <= 0: 150e9), batches whatever is pending (at most maxBatch systems per
  * batch, maxInflight batches on the device at once) as soon as memory and a
  * slot free up, runs each batch on its own stream so batches overlap, and
- * copies results to host memory.  No counterpart in the reference.
+ * keeps each finished request's outputs in device memory (counted against
+ * the budget) until it is collected.  ServerCreate maps part of the budget
+ * (up to 32 GiB, at most half the free memory) into the device's
+ * stream-ordered pool up front.  No counterpart in the reference.
  * ServerSubmit returns a request id (> 0) or a negative error code; a request
  * larger than the whole budget fails with -4.  ServerPoll returns 1 when the
- * request is finished (its output count and channels filled in).
- * ServerResult copies tVect / yVect (NumOutputs x channels) and the latency
- * (submission to completion, ms) and releases the request.
+ * request is finished (its outputs ready in device memory; output count and
+ * channels filled in).  ServerResult copies tVect / yVect (NumOutputs x
+ * channels; pinned host memory makes the copy fastest) and the latency
+ * (submission to completion, ms), and releases the request and its device
+ * memory.  Results that are never collected hold their share of the budget
+ * until ServerDestroy.
  * ServerStats fills stats[12]: submitted, completed, failed, p50 ms, p99 ms,
  * mean ms, max ms, state*steps completed, span s (first submission to last
  * completion), peak in-flight bytes, batches, 0. */

@@ -94,6 +94,8 @@ Server::Server(int device, InputRegistry* inputs, std::recursive_mutex* inputs_m
         }
     }
     for (int k = 0; k < std::max(1, opt_.setup_threads); ++k) workers_.emplace_back([this] { worker(); });
+    PARODE_CUDA(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
+    for (int k = 0; k < 2; ++k) retirers_.emplace_back([this] { retirer(); });
     thread_ = std::thread([this] { loop(); });
 }
 
@@ -116,8 +118,19 @@ Server::~Server()
         workers_stop_ = true;
     }
     jobs_cv_.notify_all();
+    retire_cv_.notify_all();
     for (auto& w : workers_)
         if (w.joinable()) w.join();
+    for (auto& w : retirers_)
+        if (w.joinable()) w.join();
+    // results nobody collected
+    cudaSetDevice(device_);
+    for (auto& kv : all_)
+        if (kv.second->dy) cudaFreeAsync(kv.second->dy, copy_stream_);
+    if (copy_stream_) {
+        cudaStreamSynchronize(copy_stream_);
+        cudaStreamDestroy(copy_stream_);
+    }
 }
 
 long long Server::submit(BatchSpec spec)
@@ -169,7 +182,19 @@ void Server::result(long long id, double* t, double* y, double* latency_ms)
         all_.erase(it);
     }
     if (r->err != 0) throw Error(r->err, "the request failed");
-    if (y) std::copy(r->y.begin(), r->y.end(), y);
+    if (r->dy) {
+        // the outputs wait on the device until collected: one copy into the
+        // caller's buffer (pinned memory makes it fastest), then the device
+        // memory returns to the pool and to the budget
+        PARODE_CUDA(cudaSetDevice(device_));
+        if (y) PARODE_CUDA(cudaMemcpyAsync(y, r->dy, sizeof(double) * r->ny, cudaMemcpyDeviceToHost, copy_stream_));
+        PARODE_CUDA(cudaFreeAsync(r->dy, copy_stream_));
+        r->dy = nullptr;
+        PARODE_CUDA(cudaStreamSynchronize(copy_stream_));
+        std::lock_guard<std::mutex> g(mu_);
+        held_bytes_ -= sizeof(double) * r->ny;
+        cv_.notify_all();
+    }
     if (t) time_vector(r->spec.solver, r->spec.t0, r->spec.tEnd, r->spec.h, t);
     if (latency_ms) *latency_ms = (r->t_done - r->t_submit) * 1e3;
 }
@@ -199,25 +224,14 @@ void Server::loop()
                 ++k;
                 continue;
             }
-            Inflight f = std::move(inflight_[k]);
+            // to a copy-out thread; its memory stays counted until it is retired
+            retire_q_.push_back(std::move(inflight_[k]));
             inflight_.erase(inflight_.begin() + (long)k);
-            lk.unlock();
-            retire(f);
-            lk.lock();
-            inflight_bytes_ -= f.bytes;
-            for (auto& r : f.reqs) {
-                r->done = true;
-                if (r->err == 0) {
-                    latencies_.push_back((r->t_done - r->t_submit) * 1e3);
-                    ++st_.completed;
-                    st_.state_steps += r->state_steps;
-                } else {
-                    ++st_.failed;
-                }
-                t_last_ = std::max(t_last_, r->t_done);
-            }
+            retire_cv_.notify_one();
         }
-        if (stop_ && pending_.empty() && jobs_.empty() && setting_up_ == 0 && inflight_.empty()) break;
+        if (stop_ && pending_.empty() && jobs_.empty() && setting_up_ == 0 && inflight_.empty() &&
+            retire_q_.empty() && retiring_ == 0)
+            break;
         admit_locked();
         cv_.wait_for(lk, std::chrono::microseconds(inflight_.empty() && setting_up_ == 0 ? 2000 : 50));
     }
@@ -232,14 +246,14 @@ void Server::admit_locked()
         Job j;
         while (!pending_.empty() && (int)j.reqs.size() < opt_.max_batch) {
             const auto& r = pending_.front();
-            if ((double)(inflight_bytes_ + j.bytes + r->bytes) > opt_.hbm_budget) break;
+            if ((double)(inflight_bytes_ + held_bytes_ + j.bytes + r->bytes) > opt_.hbm_budget) break;
             j.bytes += r->bytes;
             j.reqs.push_back(r);
             pending_.pop_front();
         }
         if (j.reqs.empty()) break;  // waits for memory to free up
         inflight_bytes_ += j.bytes;
-        st_.peak_bytes = std::max(st_.peak_bytes, (double)inflight_bytes_);
+        st_.peak_bytes = std::max(st_.peak_bytes, (double)(inflight_bytes_ + held_bytes_));
         ++st_.batches;
         ++setting_up_;
         jobs_.push_back(std::move(j));
@@ -313,18 +327,88 @@ void Server::worker()
     }
 }
 
-// Copies every request's outputs to host memory and frees the batch.
-void Server::retire(Inflight& f)
+// Copy-out thread: retires finished batches (several copies in flight at
+// once, none on the scheduler thread).
+void Server::retirer()
 {
+    cudaSetDevice(device_);
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) st = nullptr;
+    std::unique_lock<std::mutex> lk(mu_);
+    for (;;) {
+        retire_cv_.wait(lk, [this] { return !retire_q_.empty() || (workers_stop_ && retire_q_.empty()); });
+        if (retire_q_.empty()) {
+            if (workers_stop_) {
+                lk.unlock();
+                if (st) cudaStreamDestroy(st);
+                return;
+            }
+            continue;
+        }
+        Inflight f = std::move(retire_q_.front());
+        retire_q_.pop_front();
+        ++retiring_;
+        lk.unlock();
+        retire(f, st);
+        lk.lock();
+        --retiring_;
+        inflight_bytes_ -= f.bytes;
+        for (auto& r : f.reqs)
+            if (r->dy) held_bytes_ += sizeof(double) * r->ny;
+        for (auto& r : f.reqs) {
+            r->done = true;
+            if (r->err == 0) {
+                latencies_.push_back((r->t_done - r->t_submit) * 1e3);
+                ++st_.completed;
+                st_.state_steps += r->state_steps;
+            } else {
+                ++st_.failed;
+            }
+            t_last_ = std::max(t_last_, r->t_done);
+        }
+        cv_.notify_all();
+    }
+}
+
+// Moves every request's outputs into a device buffer of its own (from the
+// stream-ordered pool; device to device), checks the batch's device status,
+// and frees the batch's arena.
+void Server::retire(Inflight& f, cudaStream_t st)
+{
+    int err = 0;
+    try {
+        f.plan->get_output(0, nullptr, nullptr);  // synchronises; throws if a device wait gave up
+    } catch (const Error& e) {
+        err = e.code;
+    }
     for (size_t i = 0; i < f.reqs.size(); ++i) {
         auto& r = f.reqs[i];
-        try {
-            r->y.resize((size_t)f.plan->num_outputs((int)i) * f.plan->channels((int)i));
-            f.plan->get_output((int)i, nullptr, r->y.data());
-        } catch (const Error& e) {
-            r->err = e.code;
+        r->err = err;
+        if (err == 0) {
+            r->ny = (size_t)f.plan->num_outputs((int)i) * f.plan->channels((int)i);
+            if (cudaMallocAsync(reinterpret_cast<void**>(&r->dy), sizeof(double) * std::max<size_t>(r->ny, 1), st) !=
+                cudaSuccess) {
+                cudaGetLastError();
+                r->dy = nullptr;
+                r->err = kNotEnoughResources;
+            } else if (cudaMemcpyAsync(r->dy, f.plan->device_output((int)i), sizeof(double) * r->ny,
+                                       cudaMemcpyDeviceToDevice, st) != cudaSuccess) {
+                cudaGetLastError();
+                r->err = kDeviceError;
+            }
         }
-        r->t_done = now_s();
+    }
+    if (cudaStreamSynchronize(st) != cudaSuccess) {
+        cudaGetLastError();
+        for (auto& r : f.reqs) r->err = kDeviceError;
+    }
+    const double t = now_s();
+    for (auto& r : f.reqs) {
+        r->t_done = t;
+        if (r->err != 0 && r->dy) {
+            cudaFreeAsync(r->dy, st);
+            r->dy = nullptr;
+        }
     }
     if (f.done) cudaEventDestroy(f.done);
     f.plan.reset();

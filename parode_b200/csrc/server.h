@@ -79,7 +79,8 @@ private:
         int err = 0;
         long n_out = 0;
         int channels = 0;
-        std::vector<double> y;
+        double* dy = nullptr;  // n_out x channels on the device until collected
+        size_t ny = 0;
         double state_steps = 0;
     };
     struct Inflight {
@@ -96,8 +97,9 @@ private:
 
     void loop();
     void worker();
+    void retirer();
     void admit_locked();
-    void retire(Inflight& f);
+    void retire(Inflight& f, cudaStream_t st);
 
     int device_;
     InputRegistry* inputs_;
@@ -109,6 +111,8 @@ private:
     std::unordered_map<long long, std::shared_ptr<Request>> all_;
     std::vector<Inflight> inflight_;
     size_t inflight_bytes_ = 0;
+    size_t held_bytes_ = 0;  // finished results not yet collected (device memory)
+    cudaStream_t copy_stream_ = nullptr;  // result(): device -> caller copies
     long long next_id_ = 1;
     bool stop_ = false;
     std::vector<double> latencies_;
@@ -119,6 +123,11 @@ private:
     bool workers_stop_ = false;
     std::condition_variable jobs_cv_;
     std::vector<std::thread> workers_;
+    // finished batches wait here for a copy-out thread, off the scheduler
+    std::deque<Inflight> retire_q_;
+    int retiring_ = 0;
+    std::condition_variable retire_cv_;
+    std::vector<std::thread> retirers_;
     std::thread thread_;
 };
 
