@@ -53,7 +53,7 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--min-warmup-s", type=float, default=0.5, help="least warm-up time under load (clock sampling)")
     ap.add_argument("--no-extra", action="store_true", help="skip the batched (4096 systems) and serving runs")
-    ap.add_argument("--serve-requests", type=int, default=64)
+    ap.add_argument("--serve-requests", type=int, default=256)
     return ap.parse_args()
 
 

@@ -31,6 +31,10 @@ extern "C" {
                                       3 blocked with the block-response GEMM leaf (FP64, inputs present),
                                       4 blocked with the in-block sweep leaf */
 #define PARODE_OPT_LOG          3  /* non-zero: one line per solve on stderr */
+#define PARODE_OPT_EXECUTIONS   4  /* >= 1 (default 1): solves a plan or batch made by ParODE_PlanCreate /
+                                      ParODE_BatchCreate is expected to run; the block-response leaf picks
+                                      its block size against the FP64 build of its tables spread over that
+                                      many solves (SimulateODE and the server always use 1) */
 
 void ParODE_SetOption(int option, long long value, int nErr[]);
 long long ParODE_GetOption(int option, int nErr[]);

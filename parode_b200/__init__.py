@@ -33,6 +33,7 @@ MIXED = 1
 OPT_PRECISION = 1
 OPT_PATH = 2
 OPT_LOG = 3
+OPT_EXECUTIONS = 4
 
 PATH_AUTO = 0
 PATH_LEVEL = 1

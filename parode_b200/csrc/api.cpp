@@ -40,6 +40,7 @@ struct Library {
     int precision = kFP64;
     int path = kPathAuto;
     int log = 0;
+    long long executions = 1;  // PARODE_OPT_EXECUTIONS: plans and batches
     cudaEvent_t t_start = nullptr, t_stop = nullptr;
     bool timer_running = false;
 
@@ -366,6 +367,10 @@ void ParODE_SetOption(int option, long long value, int nErr[])
         else L.path = (int)value;
         break;
     case PARODE_OPT_LOG: L.log = (int)value; break;
+    case PARODE_OPT_EXECUTIONS:
+        if (value < 1) rc = kInvalidArgument;
+        else L.executions = value;
+        break;
     default: rc = kInvalidArgument;
     }
     if (nErr) nErr[0] = rc;
@@ -380,6 +385,7 @@ long long ParODE_GetOption(int option, int nErr[])
     case PARODE_OPT_PRECISION: return L.precision;
     case PARODE_OPT_PATH: return L.path;
     case PARODE_OPT_LOG: return L.log;
+    case PARODE_OPT_EXECUTIONS: return L.executions;
     default:
         if (nErr) nErr[0] = kInvalidArgument;
         return -1;
@@ -452,6 +458,7 @@ ParODE_Plan* ParODE_PlanCreate(const double* A, const double* B, const double* C
         opt.precision = precision;
         opt.path = L.path;
         opt.input_double = true;
+        opt.executions = (double)L.executions;
         auto h = std::make_unique<ParODE_Plan>();
         h->plan = std::make_unique<Plan>(dev, s, &L.inputs, uIndex, solver, tStart, tEnd, tStep, opt);
         out = h.release();
@@ -565,6 +572,7 @@ ParODE_Batch* ParODE_BatchCreate(int nSystems, const double* const A[], const do
         opt.path = L.path;
         opt.input_double = true;
         opt.log = L.log != 0;
+        opt.executions = (double)L.executions;
         auto h = std::make_unique<ParODE_Batch>();
         h->batch = std::make_unique<BatchPlan>(dev, std::move(specs), &L.inputs, opt);
         out = h.release();

@@ -154,7 +154,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             double cost = 0.0;
             // mixed: the window and aggregate products run on the tensor cores
             const double wweight = opt.precision == kMixed ? 0.25 : 1.0;
-            const int R = response_log2_block(q.solver, np, q.mu, q.p, q.nScan, wweight, &cost);
+            const int R = response_log2_block(q.solver, np, q.n, q.mu, q.p, q.nScan, wweight, opt.executions, &cost);
             const double sweeps = 4.0 * np * np;
             // a blocked bucket chains its tiles one after another: long
             // horizons go to the response leaf's level-synchronous block scan
@@ -356,8 +356,10 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         }
     }
     const size_t const_end = L.bytes;
-    // work buffers (offsets only; not staged)
+    // work buffers (offsets only; not staged); per-kind totals for the log
+    size_t kind_bytes[5] = {0, 0, 0, 0, 0};  // power tables + scan vectors, W, W split, samples, outputs
     for (int i = 0; i < N; ++i) {
+        const size_t at0 = L.bytes;
         Sys& q = sys_[i];
         Off& o = off[i];
         if (q.blocked) {
@@ -377,18 +379,28 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
                 q.tc_levels = lv;
             }
             o.Ps = q.tc_levels > 0 ? L.take(level_split_bytes(q.Np) * (size_t)q.tc_levels) : 0;
+            const size_t at1 = L.bytes;
             if (q.resp) o.W = L.take(sizeof(double) * ((size_t)q.Bk * q.p + q.Np) * ((size_t)q.Kpad + q.Np));
+            const size_t at2 = L.bytes;
             if (q.resp && q.precision == kMixed) {
                 q.resp_tc = true;
                 o.Psa = L.take(gemm_split_bytes(q.Np, q.Kw));
                 o.Psw = L.take(gemm_split_bytes(q.Bk * q.p, q.Kw));
             }
+            kind_bytes[1] += at2 - at1;
+            kind_bytes[2] += L.bytes - at2;
+            kind_bytes[0] -= L.bytes - at1;
         }
         // the response GEMMs read whole sample windows: the last block's
         // window runs past the samples into a zero padding
         const size_t upad = q.resp ? (size_t)(2 * q.Bk + 8) * q.mu + 2 : 0;
+        const size_t at3 = L.bytes;
         o.U = q.mu > 0 ? L.take(sizeof(double) * ((size_t)q.nU * q.mu + upad)) : 0;
+        const size_t at4 = L.bytes;
         o.Y = L.take(sizeof(double) * (size_t)q.nOut * q.p);
+        kind_bytes[0] += at3 - at0;
+        kind_bytes[3] += at4 - at3;
+        kind_bytes[4] += L.bytes - at4;
     }
     const size_t work_end = L.bytes;
 
@@ -421,6 +433,17 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
                     ((size_t)1 << 20);
     }
     arena_bytes_ = align_up(work_end + job_bytes);
+    // keep the arena and the response tables' workspace (at most 1 GiB per
+    // group) in the pool once freed: the workspace groups then reuse one
+    // mapping, and the next batch of this size maps nothing new
+    {
+        cudaMemPool_t pool = nullptr;
+        PARODE_CUDA(cudaDeviceGetDefaultMemPool(&pool, device_));
+        uint64_t keep = 0;
+        PARODE_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+        uint64_t want = (uint64_t)arena_bytes_ + (rs_.empty() ? 0 : ((uint64_t)5 << 29));
+        if (keep < want) PARODE_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &want));
+    }
     {
         // stream-ordered: creating or destroying a batch does not synchronise
         // the device, so batches can come and go while others run
@@ -555,7 +578,8 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             j.base = q.u_base;
             j.dt = q.u_dt;
             j.count = q.nU;
-            maxSample_ = std::max(maxSample_, (q.nU + 31) / 32 * q.mu);  // threads: runs of 32 samples x channels
+            maxSample_ = std::max(maxSample_, (q.nU + kSampleRun - 1) / kSampleRun * q.mu);  // threads: runs x channels
+            maxTerms_ = std::max(maxTerms_, q.K);
             sj.push_back(j);
         }
         nSampleJobs_ = (int)sj.size();
@@ -983,11 +1007,19 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
     for (auto& f : forks_) PARODE_CUDA(cudaStreamCreateWithFlags(&f, cudaStreamNonBlocking));
     events_.resize(nforks + 1, nullptr);
     for (auto& e : events_) PARODE_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    PARODE_CUDA(cudaStreamSynchronize(stream_));
+    // no wait for the device here: executes are ordered after the set-up by
+    // ready_, and the host images stay alive with the plan
+    PARODE_CUDA(cudaEventCreateWithFlags(&ready_, cudaEventDisableTiming));
+    PARODE_CUDA(cudaEventRecord(ready_, stream_));
+    host_keep_.push_back(std::move(st.buf));
+    host_keep_.push_back(std::move(jstage));
     phase("splits", true);
     if (opt.log)
-        std::fprintf(stderr, "ParODE batch set-up (%d systems, %zu response, %zu level, %zu buckets, %.2f GB):%s\n", N,
-                     rs_.size(), ls_.size(), buckets_.size(), arena_bytes_ / 1e9, phases.c_str());
+        std::fprintf(stderr,
+                     "ParODE batch set-up (%d systems, %zu response, %zu level, %zu buckets, %.2f GB: tables+scan %.2f, "
+                     "W %.2f, W split %.2f, samples %.2f, outputs %.2f):%s\n",
+                     N, rs_.size(), ls_.size(), buckets_.size(), arena_bytes_ / 1e9, kind_bytes[0] / 1e9,
+                     kind_bytes[1] / 1e9, kind_bytes[2] / 1e9, kind_bytes[3] / 1e9, kind_bytes[4] / 1e9, phases.c_str());
 }
 
 void BatchPlan::build_responses()
@@ -1099,8 +1131,7 @@ void BatchPlan::build_responses()
             launch_affine_level_grouped(st.cfg, st.args, st.start, st.nent, st.tiles, st.cfg.smem, stream_);
         launch_response_fill(dArgs, dFs, nent, fctas, stream_);
         PARODE_CUDA(cudaFreeAsync(buf, stream_));
-        // the host image above is read by the copy before it is released
-        PARODE_CUDA(cudaStreamSynchronize(stream_));
+        host_keep_.push_back(std::move(img));  // the copy may read it until it runs
     }
 }
 
@@ -1115,6 +1146,7 @@ BatchPlan::~BatchPlan()
         }
     for (auto e : events_)
         if (e) cudaEventDestroy(e);
+    if (ready_) cudaEventDestroy(ready_);
     if (arena_) cudaFreeAsync(arena_, stream_ ? stream_ : cudaStreamPerThread);
     if (stream_) cudaStreamDestroy(stream_);
 }
@@ -1130,12 +1162,13 @@ void BatchPlan::execute(cudaStream_t s)
 {
     PARODE_CUDA(cudaSetDevice(device_));
     if (!s) s = stream_;
+    if (s != stream_) PARODE_CUDA(cudaStreamWaitEvent(s, ready_, 0));
     last_stream_ = s;
     int launches = 0;
     // inputs for everything first
     if (nSampleJobs_ > 0) {
         for (int k = 0; k < nSampleJobs_; k += 65535) {
-            launch_samples_batch(dSampleJobs_ + k, std::min(65535, nSampleJobs_ - k), maxSample_, s);
+            launch_samples_batch(dSampleJobs_ + k, std::min(65535, nSampleJobs_ - k), maxSample_, maxTerms_, s);
             ++launches;
         }
     }

@@ -139,6 +139,11 @@ private:
     cudaStream_t stream_ = nullptr;
     std::vector<cudaStream_t> forks_;
     std::vector<cudaEvent_t> events_;
+    // set-up finished on stream_ (an execute on another stream waits for it)
+    cudaEvent_t ready_ = nullptr;
+    // host images of the set-up copies, kept until the plan is destroyed so
+    // that the constructor returns without waiting for the device
+    std::vector<std::vector<char>> host_keep_;
     InputRegistry* inputs_ = nullptr;
     PlanOptions opt_;
     std::vector<Sys> sys_;
@@ -154,6 +159,7 @@ private:
     SampleJob* dSampleJobs_ = nullptr;
     int nSampleJobs_ = 0;
     long maxSample_ = 0;
+    int maxTerms_ = 1;  // the largest sinusoid term count of the sample jobs
     std::vector<int> user_inputs_;  // systems sampled by their own launch
     ForcingJob* dForcing_ = nullptr;
     OutputJob* dOutput_ = nullptr;

@@ -49,64 +49,76 @@ __device__ __forceinline__ double sample_time(double base, double dt, long j)
 // neglected e^2 / 2 is below 1e-20; a residue above 1e-8 takes sincos of the
 // argument instead).  Both differences are exact for
 // arguments of one sign within a factor 2.  The rotations add a few units in
-// the last place per step: about 1e-14 of the amplitude after 32 steps.  The
-// terms advance side by side (independent chains) and are summed in
-// sinusoid_value's order; inputs with more than 4 terms per channel take
-// sinusoid_value per sample.
-template <int L>
-__device__ __forceinline__ void sinusoid_run(const double* a, const double* f, const double* phi, int K, int i,
-                                             double base, double dt, long j0, long count, double* out, long stride)
+// the last place per step: about 2e-14 of the amplitude after 64 steps.  The
+// terms (a compile-time count, so that each has its own registers) advance
+// side by side as independent chains and are summed in sinusoid_value's
+// order; inputs with more than 4 terms per channel take sinusoid_value per
+// sample.
+template <int L, int KT>
+__device__ __forceinline__ void sinusoid_run_terms(const double* a, const double* f, const double* phi, int i,
+                                                   double base, double dt, long j0, int n, double* out, long stride)
 {
-    const long rest = count - j0;
-    const int n = rest < L ? (int)rest : L;
-    if (K > 4) {
-        for (int j = 0; j < n; ++j)
-            out[(long)j * stride] = sinusoid_value(a, f, phi, K, i, sample_time(base, dt, j0 + j));
-        return;
-    }
     const double two_pi = 6.283185307179586476925286766559;
-    double w[4], ph[4], amp[4], prev[4], s[4], c[4], dl[4], sdl[4], cdl[4];
+    double w[KT], ph[KT], amp[KT], prev[KT], s[KT], c[KT], dl[KT], sdl[KT], cdl[KT];
     double v = 0.0;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        if (q < K) {
-            w[q] = __dmul_rn(two_pi, f[i * K + q]);
-            ph[q] = phi[i * K + q];
-            amp[q] = a[i * K + q];
-            prev[q] = __dadd_rn(__dmul_rn(w[q], sample_time(base, dt, j0)), ph[q]);
-            sincos(prev[q], &s[q], &c[q]);
-            dl[q] = __dmul_rn(w[q], dt);
-            sincos(dl[q], &sdl[q], &cdl[q]);
-            v = __dadd_rn(v, __dmul_rn(amp[q], s[q]));
-        }
+    for (int q = 0; q < KT; ++q) {
+        w[q] = __dmul_rn(two_pi, f[i * KT + q]);
+        ph[q] = phi[i * KT + q];
+        amp[q] = a[i * KT + q];
+        prev[q] = __dadd_rn(__dmul_rn(w[q], sample_time(base, dt, j0)), ph[q]);
+        sincos(prev[q], &s[q], &c[q]);
+        dl[q] = __dmul_rn(w[q], dt);
+        sincos(dl[q], &sdl[q], &cdl[q]);
+        v = __dadd_rn(v, __dmul_rn(amp[q], s[q]));
     }
     if (n > 0) out[0] = v;
     for (int j = 1; j < n; ++j) {
         const double t = sample_time(base, dt, j0 + j);
         v = 0.0;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            if (q < K) {
-                const double arg = __dadd_rn(__dmul_rn(w[q], t), ph[q]);
-                const double e = (arg - prev[q]) - dl[q];
-                prev[q] = arg;
-                if (fabs(e) <= 1e-8) {
-                    const double sd = fma(e, cdl[q], sdl[q]);
-                    const double cd = fma(-e, sdl[q], cdl[q]);
-                    const double sn = fma(s[q], cd, c[q] * sd);
-                    c[q] = fma(c[q], cd, -(s[q] * sd));
-                    s[q] = sn;
-                } else {
-                    sincos(arg, &s[q], &c[q]);  // arguments too large for the first-order step
-                }
-                v = __dadd_rn(v, __dmul_rn(amp[q], s[q]));
+        for (int q = 0; q < KT; ++q) {
+            const double arg = __dadd_rn(__dmul_rn(w[q], t), ph[q]);
+            const double e = (arg - prev[q]) - dl[q];
+            prev[q] = arg;
+            if (fabs(e) <= 1e-8) {
+                const double sd = fma(e, cdl[q], sdl[q]);
+                const double cd = fma(-e, sdl[q], cdl[q]);
+                const double sn = fma(s[q], cd, c[q] * sd);
+                c[q] = fma(c[q], cd, -(s[q] * sd));
+                s[q] = sn;
+            } else {
+                sincos(arg, &s[q], &c[q]);  // arguments too large for the first-order step
             }
+            v = __dadd_rn(v, __dmul_rn(amp[q], s[q]));
         }
         out[(long)j * stride] = v;
     }
 }
 
-// Samples per thread of the sampling kernels (sinusoid_run's L).
-constexpr int kSampleRun = 32;
+// KMAX (1..4): the largest term count given its own chains; a kernel's
+// registers follow the largest variant it contains.
+template <int L, int KMAX>
+__device__ __forceinline__ void sinusoid_run(const double* a, const double* f, const double* phi, int K, int i,
+                                             double base, double dt, long j0, long count, double* out, long stride)
+{
+    const long rest = count - j0;
+    const int n = rest < L ? (int)rest : L;
+    if (K == 1) {
+        sinusoid_run_terms<L, 1>(a, f, phi, i, base, dt, j0, n, out, stride);
+    } else if (KMAX >= 2 && K == 2) {
+        sinusoid_run_terms<L, (KMAX >= 2 ? 2 : 1)>(a, f, phi, i, base, dt, j0, n, out, stride);
+    } else if (KMAX >= 3 && K == 3) {
+        sinusoid_run_terms<L, (KMAX >= 3 ? 3 : 1)>(a, f, phi, i, base, dt, j0, n, out, stride);
+    } else if (KMAX >= 4 && K == 4) {
+        sinusoid_run_terms<L, (KMAX >= 4 ? 4 : 1)>(a, f, phi, i, base, dt, j0, n, out, stride);
+    } else {
+        for (int j = 0; j < n; ++j)
+            out[(long)j * stride] = sinusoid_value(a, f, phi, K, i, sample_time(base, dt, j0 + j));
+    }
+}
+
+// The sampling kernels' KMAX for inputs of up to max_terms terms per channel.
+inline int sample_kmax(int max_terms) { return max_terms < 1 ? 1 : (max_terms > 4 ? 4 : max_terms); }
 
 }  // namespace parode

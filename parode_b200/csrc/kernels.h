@@ -7,6 +7,10 @@
 
 namespace parode {
 
+// Samples per thread of the input-sampling kernels: one thread advances one
+// channel over a run of this many consecutive samples.
+constexpr int kSampleRun = 64;
+
 // Column addressing of the batched affine-level contraction:
 //   result(g, i) = sum_k P[i][k] * src(g, k) (+ acc(g, i))
 // src(g,k) = src[g*src_gs + k*src_ks], acc/dst/cpy likewise with (g, i).
@@ -108,7 +112,8 @@ void launch_response_fill(const ResponseArgs* dArgs, const long* dStart, int nen
 // FP64-equivalent flops per step (the two GEMMs and a level-synchronous carry
 // over blocks); window_weight scales the window and aggregate products (1 in
 // FP64, the tensor cores' relative cost in the mixed form).
-int response_log2_block(int solver, int NP, int m, int p, long nScan, double window_weight, double* flops_per_step);
+int response_log2_block(int solver, int NP, int n, int m, int p, long nScan, double window_weight, double executions,
+                        double* flops_per_step);
 
 // Exclusive scan of block aggregates for NP <= 64 (a multiple of 8),
 // kernels_carry.cu: items[b] <- X_b with X_0 = X0, X_{b+1} = Q X_b + items[b],
@@ -234,7 +239,8 @@ struct CopyJob {
 };
 // max_elems: the largest element count of a job (sizes the x dimension); for
 // the samples, runs of 32 samples x channels (one thread each).
-void launch_samples_batch(const SampleJob* dJobs, int njobs, long max_elems, cudaStream_t s);
+// max_terms: the largest term count of the jobs' inputs
+void launch_samples_batch(const SampleJob* dJobs, int njobs, long max_elems, int max_terms, cudaStream_t s);
 void launch_forcing_batch(const ForcingJob* dJobs, int njobs, long max_elems, cudaStream_t s);
 void launch_output_batch(const OutputJob* dJobs, int njobs, long max_elems, cudaStream_t s);
 void launch_copy_batch(const CopyJob* dJobs, int njobs, long max_elems, cudaStream_t s);

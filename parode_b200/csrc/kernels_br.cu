@@ -331,13 +331,21 @@ void launch_response_fill(const ResponseArgs* dArgs, const long* dStart, int nen
     PARODE_CUDA(cudaGetLastError());
 }
 
-int response_log2_block(int solver, int NP, int m, int p, long nScan, double window_weight, double* flops_per_step)
+int response_log2_block(int solver, int NP, int n, int m, int p, long nScan, double window_weight, double executions,
+                        double* flops_per_step)
 {
     // per block: aggregates 2 NP Kpad and the outputs' window part 2 B p Kpad
     // (scaled by window_weight: below 1 when they run on the tensor cores),
     // the outputs' state part 2 B p NP, and about 6 NP^2 for the
     // level-synchronous carry (up- and down-sweep, 4 NP^2, at a lower
-    // efficiency than the GEMMs)
+    // efficiency than the GEMMs).  Per step on top: the FP64 build of W's
+    // tables (C P^k and P^k restricted to the input columns for k < B, by
+    // doubling, then their products with Bbar), spread over the steps of
+    // `executions` solves (0: not counted)
+    const double n2 = (double)(n + (n & 1));
+    const int wm = (solver == 0 ? 3 : 5) * m;
+    const double wm2 = (double)(wm + (wm & 1));
+    const double per_build = executions > 0 ? 1.0 / ((double)nScan * executions) : 0.0;
     int best = 2;
     double best_cost = -1.0;
     for (int R = 2; R <= 7; ++R) {
@@ -346,8 +354,10 @@ int response_log2_block(int solver, int NP, int m, int p, long nScan, double win
         const long K = response_window(solver, (int)B, m), Kp = (K + 1) & ~1L;
         const double wbytes = 8.0 * ((double)B * p + NP) * ((double)Kp + NP);
         if (R > 2 && wbytes > 256e6) break;
+        const double build = 2.0 * B * ((double)NP * NP + wm2 * NP) * (p + n2);
         const double cost =
-            (window_weight * (2.0 * NP * Kp + 2.0 * B * p * (double)Kp) + 2.0 * B * p * (double)NP + 6.0 * NP * NP) / B;
+            (window_weight * (2.0 * NP * Kp + 2.0 * B * p * (double)Kp) + 2.0 * B * p * (double)NP + 6.0 * NP * NP) / B +
+            build * per_build;
         if (best_cost < 0 || cost < best_cost) {
             best_cost = cost;
             best = R;

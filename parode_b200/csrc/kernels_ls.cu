@@ -322,6 +322,7 @@ __global__ void k_swap_grouped(const LevelArgs* __restrict__ args)
 }
 
 // One thread per (run of kSampleRun samples, channel); channels fastest.
+template <int KMAX>
 __global__ void k_sinusoid_samples(double* U, int m, int K, const double* a, const double* f, const double* phi,
                                    double base, double dt, long count)
 {
@@ -331,7 +332,7 @@ __global__ void k_sinusoid_samples(double* U, int m, int K, const double* a, con
     const long r = e / m;
     const int i = (int)(e - r * m);
     const long j0 = r * kSampleRun;
-    sinusoid_run<kSampleRun>(a, f, phi, K, i, base, dt, j0, count, U + j0 * m + i, m);
+    sinusoid_run<kSampleRun, KMAX>(a, f, phi, K, i, base, dt, j0, count, U + j0 * m + i, m);
 }
 
 // V[k][i] = Gamma_k[i]; RK4: Gamma_k = Bbar [u_2k; u_2k+1; u_2k+2] in rows
@@ -395,6 +396,7 @@ __global__ void k_copy(double* dst, const double* src, long N)
 // Batched element kernels: blockIdx.y selects the job, the x dimension
 // strides over its elements; each element is computed as by the single-system
 // kernels above.
+template <int KMAX>
 __global__ void k_samples_batch(const SampleJob* __restrict__ jobs)
 {
     const SampleJob J = jobs[blockIdx.y];
@@ -404,7 +406,8 @@ __global__ void k_samples_batch(const SampleJob* __restrict__ jobs)
         const long r = e / J.m;
         const int i = (int)(e - r * J.m);
         const long j0 = r * kSampleRun;
-        sinusoid_run<kSampleRun>(J.a, J.f, J.phi, J.K, i, J.base, J.dt, j0, J.count, J.U + j0 * J.m + i, J.m);
+        sinusoid_run<kSampleRun, KMAX>(J.a, J.f, J.phi, J.K, i, J.base, J.dt, j0, J.count, J.U + j0 * J.m + i,
+                                       J.m);
     }
 }
 
@@ -559,7 +562,13 @@ void launch_sinusoid_samples(double* U, int m, int K, const double* a, const dou
 {
     if (count <= 0 || m <= 0) return;
     const long total = (count + kSampleRun - 1) / kSampleRun * m;
-    k_sinusoid_samples<<<blocks_for(total, 256), 256, 0, s>>>(U, m, K, a, f, phi, base, dt, count);
+    const unsigned g = (unsigned)blocks_for(total, 256);
+    switch (sample_kmax(K)) {
+    case 1: k_sinusoid_samples<1><<<g, 256, 0, s>>>(U, m, K, a, f, phi, base, dt, count); break;
+    case 2: k_sinusoid_samples<2><<<g, 256, 0, s>>>(U, m, K, a, f, phi, base, dt, count); break;
+    case 3: k_sinusoid_samples<3><<<g, 256, 0, s>>>(U, m, K, a, f, phi, base, dt, count); break;
+    default: k_sinusoid_samples<4><<<g, 256, 0, s>>>(U, m, K, a, f, phi, base, dt, count); break;
+    }
     PARODE_CUDA(cudaGetLastError());
 }
 
@@ -698,11 +707,16 @@ void launch_swap_grouped(const LevelArgs* dArgs, int nent, long max_elems, cudaS
     PARODE_CUDA(cudaGetLastError());
 }
 
-void launch_samples_batch(const SampleJob* dJobs, int njobs, long max_elems, cudaStream_t s)
+void launch_samples_batch(const SampleJob* dJobs, int njobs, long max_elems, int max_terms, cudaStream_t s)
 {
     if (njobs <= 0 || max_elems <= 0) return;
     dim3 grid(batch_grid_x(max_elems, 256, 64, njobs), (unsigned)njobs);
-    k_samples_batch<<<grid, 256, 0, s>>>(dJobs);
+    switch (sample_kmax(max_terms)) {
+    case 1: k_samples_batch<1><<<grid, 256, 0, s>>>(dJobs); break;
+    case 2: k_samples_batch<2><<<grid, 256, 0, s>>>(dJobs); break;
+    case 3: k_samples_batch<3><<<grid, 256, 0, s>>>(dJobs); break;
+    default: k_samples_batch<4><<<grid, 256, 0, s>>>(dJobs); break;
+    }
     PARODE_CUDA(cudaGetLastError());
 }
 

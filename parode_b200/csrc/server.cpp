@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 
 namespace parode {
 
@@ -225,6 +226,7 @@ void Server::loop()
                 continue;
             }
             // to a copy-out thread; its memory stays counted until it is retired
+            inflight_[k].t_seen = now_s();
             retire_q_.push_back(std::move(inflight_[k]));
             inflight_.erase(inflight_.begin() + (long)k);
             retire_cv_.notify_one();
@@ -252,6 +254,7 @@ void Server::admit_locked()
             pending_.pop_front();
         }
         if (j.reqs.empty()) break;  // waits for memory to free up
+        j.t_admit = now_s();
         inflight_bytes_ += j.bytes;
         st_.peak_bytes = std::max(st_.peak_bytes, (double)(inflight_bytes_ + held_bytes_));
         ++st_.batches;
@@ -280,6 +283,7 @@ void Server::worker()
         Inflight f;
         f.reqs = j.reqs;
         f.bytes = j.bytes;
+        f.t_admit = j.t_admit;
         try {
             std::vector<BatchSpec> specs;
             specs.reserve(j.reqs.size());
@@ -302,6 +306,7 @@ void Server::worker()
             f.plan->execute(nullptr);
             PARODE_CUDA(cudaEventCreateWithFlags(&f.done, cudaEventDisableTiming));
             PARODE_CUDA(cudaEventRecord(f.done, f.plan->stream()));
+            f.t_ready = now_s();
         } catch (const Error& e) {
             for (auto& r : j.reqs) r->err = e.code;
             f.plan.reset();
@@ -351,6 +356,13 @@ void Server::retirer()
         lk.unlock();
         retire(f, st);
         lk.lock();
+        if (opt_.log) {
+            const double t = now_s(), z = t_first_;
+            std::fprintf(stderr,
+                         "ParODE server batch (%zu requests): admitted %.1f ms, on the device %.1f ms, seen done %.1f ms, "
+                         "retired %.1f ms (after the first submission)\n",
+                         f.reqs.size(), (f.t_admit - z) * 1e3, (f.t_ready - z) * 1e3, (f.t_seen - z) * 1e3, (t - z) * 1e3);
+        }
         --retiring_;
         inflight_bytes_ -= f.bytes;
         for (auto& r : f.reqs)

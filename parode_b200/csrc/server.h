@@ -88,11 +88,14 @@ private:
         std::vector<std::shared_ptr<Request>> reqs;
         cudaEvent_t done = nullptr;
         size_t bytes = 0;
+        // host times (log): admitted, enqueued on the device, seen finished
+        double t_admit = 0, t_ready = 0, t_seen = 0;
     };
 
     struct Job {
         std::vector<std::shared_ptr<Request>> reqs;
         size_t bytes = 0;
+        double t_admit = 0;
     };
 
     void loop();

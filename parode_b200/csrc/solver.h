@@ -31,6 +31,10 @@ struct PlanOptions {
     int path = kPathAuto;
     bool input_double = true;  // fType of a user input function: double (true) or float
     bool log = false;          // set-up phase times on stderr
+    // solves the plan is expected to run: the response leaf's block size
+    // weighs the FP64 build of its tables against the work of that many
+    // solves (1: one-shot, as SimulateODE and the server)
+    double executions = 1.0;
 };
 
 class Plan {
