@@ -255,6 +255,25 @@ __device__ void tiled_level_body(const LevelArgs& a, long tile, double* smem)
     }
     cp_async_wait<0>();
 
+    // acc may be dst itself (in place): every acc value is loaded before the
+    // first store, so the sixteen loads go out together instead of each
+    // waiting behind the store before it
+    if (a.acc) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const long r = m0 + wm * 32 + i * 8 + gq;
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const long g = n0 + wn * 16 + j * 8 + 2 * tq + e;
+                    const long o = g * a.dst_gs + r * a.dst_is;
+                    // exactly the elements stored below (acc past dst_limit may lie past its buffer)
+                    if (r < rows && g < a.ncols && !(a.dst_limit >= 0 && o >= a.dst_limit))
+                        acc[i][j][e] += a.acc[g * a.acc_gs + r * a.acc_is];
+                }
+        }
+    }
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         const long r = m0 + wm * 32 + i * 8 + gq;
@@ -267,9 +286,7 @@ __device__ void tiled_level_body(const LevelArgs& a, long tile, double* smem)
                 if (g >= a.ncols) continue;
                 const long o = g * a.dst_gs + r * a.dst_is;
                 if (a.dst_limit >= 0 && o >= a.dst_limit) continue;
-                double v = acc[i][j][e];
-                if (a.acc) v += a.acc[g * a.acc_gs + r * a.acc_is];
-                a.dst[o] = v;
+                a.dst[o] = acc[i][j][e];
             }
     }
 }
