@@ -287,6 +287,9 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
         alloc(&dra, (long)((sizeof(ResponseArgs) + 7) / 8));
         PARODE_CUDA(cudaMemcpyAsync(dra, &ra, sizeof(ra), cudaMemcpyHostToDevice, stream_));
         launch_block_response(reinterpret_cast<const ResponseArgs*>(dra), 1, Np_, p_, brKpad_, stream_);
+        // the carry's powers P_1 .. P_levels (Phi^(2^l)) depend on Phi alone:
+        // formed once here, like W
+        launch_blocked_tables(shape_, dPow_, 1, levels_, nullptr, nullptr, p_, stream_);
         if (br_tc_) {
             // the two tensor-core GEMMs over the sample windows: aggregates
             // into G, output windows into the plan's y buffer (the FP64 state
@@ -583,16 +586,10 @@ void Plan::execute_response(double* Y, cudaStream_t s)
     // aggregates first (the state columns are not used), then the carry, then
     // the outputs with the carried block states, written straight into y
     // (rows (j, o) of block b are contiguous there).  The power table
-    // P_1..P_levels (one CTA) runs on the side stream beside the sampling and
-    // the aggregate GEMM.
+    // P_1..P_levels was formed with W when the plan was made.
     int launches = 0;
     marks_.clear();
     mark("start", s);
-    PARODE_CUDA(cudaEventRecord(fork_[0], s));
-    PARODE_CUDA(cudaStreamWaitEvent(side_, fork_[0], 0));
-    launch_blocked_tables(shape_, dPow_, 1, levels_, nullptr, nullptr, p_, side_);
-    ++launches;
-    PARODE_CUDA(cudaEventRecord(fork_[3], side_));
     fill_inputs(s);
     ++launches;
     mark("inputs", s);
@@ -604,7 +601,6 @@ void Plan::execute_response(double* Y, cudaStream_t s)
         launch_level_tc(dTc_, dTcStart_, 2, dTcCta_, tcCtas_, dStatus_, s);
         ++launches;
         mark("aggregates+windows", s);
-        PARODE_CUDA(cudaStreamWaitEvent(s, fork_[3], 0));
         launches += launch_chunk_carry(Np_, dG_, nblocks_, dPow_, shape_.R, dX0_, dWork_, s);
         mark("carry", s);
         LevelArgs x;
@@ -647,7 +643,6 @@ void Plan::execute_response(double* Y, cudaStream_t s)
     launch_gemm_tiled(g, s);
     ++launches;
     mark("aggregates", s);
-    PARODE_CUDA(cudaStreamWaitEvent(s, fork_[3], 0));
     launches += launch_chunk_carry(Np_, dG_, nblocks_, dPow_, shape_.R, dX0_, dWork_, s);
     mark("carry", s);
     LevelArgs h = g;
