@@ -223,28 +223,31 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
 
     phase("classify", false);
     // ---- host FP64 discretisation (threads over systems) --------------------
+    // Phi is kept compact (RK4: n x n; ABM: its last block row, n x 4n, the
+    // rows above being the exact shift) and expanded into the padded power
+    // table's level 0 on the device: an ABM Phi is 16 n^2, its dense part 4 n^2
     std::vector<std::vector<double>> Phi(N), Bbar(N), X0(N), Ypre(N);
     parallel_for(N, [&](int i) {
         const SystemDesc& s = specs[i].sys;
         Sys& q = sys_[i];
         const int mB = s.zeroB ? 0 : s.m;
-        std::vector<double> P((size_t)q.Ns * q.Ns);
         Bbar[i].assign((size_t)q.n * q.W * std::max(mB, 1), 0.0);
+        Phi[i].resize((size_t)q.n * q.Ns);
         if (q.solver == kRK4)
-            discretise_rk4(q.n, mB, s.A.data(), mB ? s.B.data() : nullptr, q.h, P.data(), Bbar[i].data());
+            discretise_rk4(q.n, mB, s.A.data(), mB ? s.B.data() : nullptr, q.h, Phi[i].data(), Bbar[i].data());
         else
-            discretise_abm(q.n, mB, s.A.data(), mB ? s.B.data() : nullptr, q.h, P.data(), Bbar[i].data());
-        Phi[i].assign((size_t)q.Np * q.Np, 0.0);
-        for (int r = 0; r < q.Ns; ++r) std::memcpy(&Phi[i][(size_t)r * q.Np], &P[(size_t)r * q.Ns], sizeof(double) * q.Ns);
+            discretise_abm_last(q.n, mB, s.A.data(), mB ? s.B.data() : nullptr, q.h, Phi[i].data(), Bbar[i].data());
         X0[i].assign((size_t)q.Np, 0.0);
         // distance of Phi from its exact 0/1 part (I for RK4; for ABM the
-        // companion shift: block row b < 3 reads block b + 1, the last row
-        // block reads itself)
+        // companion shift, whose rows above the last block are exact, the
+        // last row block reading itself): the max row sum of |Phi - R| over
+        // the stored rows
+        const int d0 = q.solver == kRK4 ? 0 : 3 * q.n;
         double dmax = 0.0;
-        for (int r = 0; r < q.Ns; ++r) {
-            const int rc = q.solver == kRK4 ? r : (std::min(r / q.n + 1, 3) * q.n + r % q.n);
+        for (int r = 0; r < q.n; ++r) {
+            const int rc = d0 + r;
             double sum = 0.0;
-            for (int c = 0; c < q.Ns; ++c) sum += std::fabs(P[(size_t)r * q.Ns + c] - (c == rc ? 1.0 : 0.0));
+            for (int c = 0; c < q.Ns; ++c) sum += std::fabs(Phi[i][(size_t)r * q.Ns + c] - (c == rc ? 1.0 : 0.0));
             dmax = std::max(dmax, sum);
         }
         q.delta = dmax;
@@ -427,7 +430,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         for (int i : rs_) lev_entries += 4L * std::max(sys_[i].pow_levels, 1) + 8;
         job_bytes = nb * (sizeof(LeafArgs) + 3 * sizeof(double*) + 4 * kAlign) +
                     (size_t)items_ub * sizeof(BatchItem) + buckets_.size() * 8 * kAlign +
-                    (size_t)N * (sizeof(SampleJob) + sizeof(ForcingJob) + sizeof(OutputJob) + 2 * sizeof(CopyJob)) +
+                    (size_t)N * (sizeof(SampleJob) + sizeof(ForcingJob) + sizeof(OutputJob) + 2 * sizeof(CopyJob) + sizeof(PhiJob)) +
                     8 * kAlign + (size_t)lev_entries * (2 * sizeof(LevelArgs) + sizeof(long) + 128) +
                     (size_t)(3 * 64 * 8) * 2 * kAlign + (size_t)2 * 64 * (2 * sms_ + 1) * sizeof(long) +
                     ((size_t)1 << 20);
@@ -957,14 +960,20 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         nSplit_ = (int)sp.size();
         if (nSplit_ > 0) dSplit_ = reinterpret_cast<LevelArgs*>(base + jput(sp.data(), sizeof(LevelArgs) * sp.size()));
     }
-    // set-up copies: Phi -> P level 0, ABM outputs 0..2 -> Y rows 0..2
+    // set-up copies: compact Phi -> P level 0 (padded, the ABM shift rows
+    // written exactly), ABM outputs 0..2 -> Y rows 0..2
+    std::vector<PhiJob> phi_jobs;
+    long max_phi = 0;
     for (int i = 0; i < N; ++i) {
         const Sys& q = sys_[i];
-        CopyJob c;
-        c.dst = q.P;
-        c.src = dp(off[i].phi0);
-        c.N = (long)q.Np * q.Np;
-        setup_copies.push_back(c);
+        PhiJob pj;
+        pj.dst = q.P;
+        pj.src = dp(off[i].phi0);
+        pj.n = q.n;
+        pj.Np = q.Np;
+        pj.solver = q.solver;
+        phi_jobs.push_back(pj);
+        max_phi = std::max(max_phi, (long)q.Np * q.Np);
         if (q.solver == kABM) {
             CopyJob y;
             y.dst = q.Y;
@@ -981,6 +990,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
     for (const CopyJob& c : setup_copies) max_copy = std::max(max_copy, c.N);
     const CopyJob* dSetup =
         reinterpret_cast<const CopyJob*>(base + jput(setup_copies.data(), sizeof(CopyJob) * setup_copies.size()));
+    const PhiJob* dPhi = reinterpret_cast<const PhiJob*>(base + jput(phi_jobs.data(), sizeof(PhiJob) * phi_jobs.size()));
     if (J.bytes > arena_bytes_) throw Error(kDeviceError, "batch job arrays overflow the arena reservation");
 
     phase("jobs", false);
@@ -991,6 +1001,8 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
     PARODE_CUDA(cudaMemcpyAsync(base + work_end, jstage.data(), jstage.size(), cudaMemcpyHostToDevice, stream_));
     for (size_t k = 0; k < setup_copies.size(); k += 65535)
         launch_copy_batch(dSetup + k, (int)std::min<size_t>(65535, setup_copies.size() - k), max_copy, stream_);
+    for (size_t k = 0; k < phi_jobs.size(); k += 65535)
+        launch_phi_batch(dPhi + k, (int)std::min<size_t>(65535, phi_jobs.size() - k), max_phi, stream_);
     phase("upload", true);
     // the power table P_l = Phi^(2^l), the response matrices and, in the
     // mixed form, the splits of the tensor-core operands depend on Phi alone:

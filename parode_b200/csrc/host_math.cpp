@@ -95,14 +95,28 @@ void discretise_rk4(int n, int m, const double* A, const double* B, double h, do
 void discretise_abm(int n, int m, const double* A, const double* B, double h, double* Phi, double* Bbar)
 {
     // Companion map of the linear AB4-predictor / AM4-corrector step
-    // (reference Sources/AdamsMoulton.cpp:253-316).
+    // (reference Sources/AdamsMoulton.cpp:253-316): the shift rows, then the
+    // last block row.
+    const int N = 4 * n;
+    std::memset(Phi, 0, sizeof(double) * (size_t)N * N);
+    for (int r = 0; r < n; ++r) {
+        Phi[(long)r * N + n + r] = 1.0;
+        Phi[(long)(n + r) * N + 2 * n + r] = 1.0;
+        Phi[(long)(2 * n + r) * N + 3 * n + r] = 1.0;
+    }
+    discretise_abm_last(n, m, A, B, h, Phi + (long)3 * n * N, Bbar);
+}
+
+void discretise_abm_last(int n, int m, const double* A, const double* B, double h, double* lastRows, double* Bbar)
+{
+    // coefficients of the AB4 predictor folded into the AM4 corrector
+    // (reference Sources/AdamsMoulton.cpp:253-316)
     const int N = 4 * n;
     std::vector<double> A2((size_t)n * n);
     gemm(n, n, n, A, A, A2.data());
     const double h2 = h * h;
-    std::memset(Phi, 0, sizeof(double) * (size_t)N * N);
     for (int r = 0; r < n; ++r) {
-        double* last = Phi + (long)(3 * n + r) * N;
+        double* last = lastRows + (long)r * N;
         for (int c = 0; c < n; ++c) {
             long q = (long)r * n + c;
             last[c] = (-81.0 * h2 / 576.0) * A2[q];
@@ -110,9 +124,6 @@ void discretise_abm(int n, int m, const double* A, const double* B, double h, do
             last[2 * n + c] = (-5.0 * h / 24.0) * A[q] + (-531.0 * h2 / 576.0) * A2[q];
             last[3 * n + c] = (r == c ? 1.0 : 0.0) + (28.0 * h / 24.0) * A[q] + (495.0 * h2 / 576.0) * A2[q];
         }
-        Phi[(long)r * N + n + r] = 1.0;
-        Phi[(long)(n + r) * N + 2 * n + r] = 1.0;
-        Phi[(long)(2 * n + r) * N + 3 * n + r] = 1.0;
     }
     if (m <= 0) return;
     std::vector<double> AB((size_t)n * m);

@@ -29,6 +29,9 @@ void time_vector(int solver, double t0, double tEnd, double h, double* tv);
 // (W = 3 for RK4, 5 for ABM), both row-major FP64.
 void discretise_rk4(int n, int m, const double* A, const double* B, double h, double* Phi, double* Bbar);
 void discretise_abm(int n, int m, const double* A, const double* B, double h, double* Phi, double* Bbar);
+// The same ABM map with only the last block row of Phi (n x 4n): the block
+// rows above it are the exact shift (block b reads block b + 1).
+void discretise_abm_last(int n, int m, const double* A, const double* B, double h, double* last, double* Bbar);
 
 // ABM start-up: X0 = [x0; x1; x2; x3] from three classical RK4 steps with the
 // nine inputs U[j] = u(t0 + j h/2), j = 0..8 (U is 9 x m, row-major)

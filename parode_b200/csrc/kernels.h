@@ -237,6 +237,15 @@ struct CopyJob {
     const double* src = nullptr;  // nullptr: fill with zeros
     long N = 0;
 };
+// Phi into the power table's level 0 (Np x Np, zero padded) from its compact
+// staged form: RK4 the n x n matrix; ABM the last block row (n x 4n), the
+// block rows above it being the exact shift (block b reads block b + 1).
+struct PhiJob {
+    double* dst = nullptr;
+    const double* src = nullptr;
+    int n = 0, Np = 0, solver = 0;
+};
+void launch_phi_batch(const PhiJob* dJobs, int njobs, long max_elems, cudaStream_t s);
 // max_elems: the largest element count of a job (sizes the x dimension); for
 // the samples, runs of 32 samples x channels (one thread each).
 // max_terms: the largest term count of the jobs' inputs

@@ -486,6 +486,25 @@ __global__ void k_copy_batch(const CopyJob* __restrict__ jobs)
         J.dst[e] = J.src ? J.src[e] : 0.0;
 }
 
+__global__ void k_phi_batch(const PhiJob* __restrict__ jobs)
+{
+    const PhiJob J = jobs[blockIdx.y];
+    const long total = (long)J.Np * J.Np;
+    const int n = J.n;
+    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+        const int r = (int)(e / J.Np), c = (int)(e - (long)r * J.Np);
+        double v = 0.0;
+        if (J.solver == 0) {
+            if (r < n && c < n) v = J.src[(long)r * n + c];
+        } else if (r < 3 * n) {
+            v = (c == r + n) ? 1.0 : 0.0;
+        } else if (r < 4 * n && c < 4 * n) {
+            v = J.src[(long)(r - 3 * n) * (4 * n) + c];
+        }
+        J.dst[e] = v;
+    }
+}
+
 inline unsigned blocks_for(long n, int t) { return (unsigned)((n + t - 1) / t); }
 
 // x extent of a batched launch (y = jobs): `cap` CTAs per job, raised so
@@ -759,6 +778,14 @@ void launch_copy_batch(const CopyJob* dJobs, int njobs, long max_elems, cudaStre
     if (njobs <= 0 || max_elems <= 0) return;
     dim3 grid(batch_grid_x(max_elems, 256, 16, njobs), (unsigned)njobs);
     k_copy_batch<<<grid, 256, 0, s>>>(dJobs);
+    PARODE_CUDA(cudaGetLastError());
+}
+
+void launch_phi_batch(const PhiJob* dJobs, int njobs, long max_elems, cudaStream_t s)
+{
+    if (njobs <= 0 || max_elems <= 0) return;
+    dim3 grid(batch_grid_x(max_elems, 256, 16, njobs), (unsigned)njobs);
+    k_phi_batch<<<grid, 256, 0, s>>>(dJobs);
     PARODE_CUDA(cudaGetLastError());
 }
 
