@@ -319,7 +319,7 @@ def measure_serving(pb, wl, torch, count=64, rates=(500.0, 2000.0, 8000.0)):
     for rate in rates:
         reqs = wl.cfg5(count, rate)
         reqs_all[rate] = reqs
-        server = pb.Server(precision=pb.MIXED, hbm_budget_bytes=150e9, max_batch=16, max_inflight=8)
+        server = pb.Server(precision=pb.MIXED, hbm_budget_bytes=150e9, max_batch=32, max_inflight=8)
         specs = [(arr, c, _spec(pb, c)) for arr, c in reqs]
         ids = []
         t0 = time.monotonic()

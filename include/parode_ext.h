@@ -30,7 +30,9 @@ extern "C" {
 #define PARODE_OPT_PATH         2  /* 0 auto, 1 level-synchronous sweeps, 2 blocked (leaf chosen by cost),
                                       3 blocked with the block-response GEMM leaf (FP64, inputs present),
                                       4 blocked with the in-block sweep leaf */
-#define PARODE_OPT_LOG          3  /* non-zero: one line per solve on stderr */
+#define PARODE_OPT_LOG          3  /* non-zero: one line per solve or batch set-up on stderr; a server logs
+                                      each batch's timeline (1), and its set-up phases too (2, which waits on
+                                      the device between phases) */
 #define PARODE_OPT_EXECUTIONS   4  /* >= 1 (default 1): solves a plan or batch made by ParODE_PlanCreate /
                                       ParODE_BatchCreate is expected to run; the block-response leaf picks
                                       its block size against the FP64 build of its tables spread over that

@@ -661,7 +661,7 @@ ParODE_Server* ParODE_ServerCreate(int precision, double hbmBudgetBytes, int max
         if (hbmBudgetBytes > 0) o.hbm_budget = hbmBudgetBytes;
         if (maxBatch > 0) o.max_batch = maxBatch;
         if (maxInflight > 0) o.max_inflight = maxInflight;
-        o.log = L.log != 0;
+        o.log = L.log;
         auto h = std::make_unique<ParODE_Server>();
         h->server = std::make_unique<Server>(dev, &L.inputs, &L.mu, o);
         out = h.release();

@@ -32,18 +32,6 @@ struct Layout {
     }
 };
 
-// Host staging of the constant part of the arena (copied once).
-struct Stage {
-    std::vector<char> buf;
-    size_t put(const void* src, size_t n, Layout& L)
-    {
-        size_t off = L.take(n);
-        if (buf.size() < L.bytes) buf.resize(L.bytes, 0);
-        if (n && src) std::memcpy(buf.data() + off, src, n);
-        return off;
-    }
-};
-
 double sinusoid_host(const InputEntry* e, int i, double t)
 {
     const double two_pi = 6.283185307179586476925286766559;
@@ -222,22 +210,59 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
     }
 
     phase("classify", false);
-    // ---- host FP64 discretisation (threads over systems) --------------------
-    // Phi is kept compact (RK4: n x n; ABM: its last block row, n x 4n, the
-    // rows above being the exact shift) and expanded into the padded power
-    // table's level 0 on the device: an ABM Phi is 16 n^2, its dense part 4 n^2
-    std::vector<std::vector<double>> Phi(N), Bbar(N), X0(N), Ypre(N);
+    // ---- constant region: layout first, then the host FP64 discretisation
+    // (threads over systems) writes straight into its staged slots.  Phi is
+    // kept compact (RK4: n x n; ABM: its last block row, n x 4n, the rows
+    // above being the exact shift) and expanded into the padded power table's
+    // level 0 on the device: an ABM Phi is 16 n^2, its dense part 4 n^2
+    Layout L;
+    struct Off {
+        size_t phi0, bbar, c, d, cext, x0, sin, ypre;
+        size_t bbarT, cT, dT;  // level-synchronous systems: transposed copies (coalesced per-row kernels)
+        size_t P, U, Y, V, G, CP, Ps, W, Psa, Psw;
+    };
+    std::vector<Off> off(N);
+    for (int i = 0; i < N; ++i) {
+        const SystemDesc& s = specs[i].sys;
+        Sys& q = sys_[i];
+        Off& o = off[i];
+        const int mB = s.zeroB ? 0 : s.m;
+        o.phi0 = L.take(sizeof(double) * (size_t)q.n * q.Ns);
+        o.bbar = L.take(sizeof(double) * (size_t)q.n * q.W * std::max(mB, 1));
+        o.c = L.take(sizeof(double) * (s.zeroC ? 1 : (size_t)q.p * q.n));
+        o.d = L.take(sizeof(double) * (s.zeroD ? 1 : (size_t)q.p * s.m));
+        o.x0 = L.take(sizeof(double) * (size_t)q.Np);
+        o.cext = (q.blocked || q.resp) ? L.take(sizeof(double) * (size_t)q.p * q.Np) : 0;
+        o.sin = 0;
+        if (q.mu > 0 && q.input->kind == InputEntry::kSinusoid) {
+            q.K = q.input->K;
+            o.sin = L.take(sizeof(double) * 3 * q.input->a.size());
+        }
+        o.ypre = q.solver == kABM ? L.take(sizeof(double) * 3 * (size_t)q.p) : 0;
+        o.bbarT = o.cT = o.dT = 0;
+        if (!q.blocked && !q.resp) {
+            o.bbarT = L.take(sizeof(double) * (size_t)std::max(q.W * mB, 1) * q.n);
+            o.cT = L.take(sizeof(double) * (size_t)q.n * q.p);
+            o.dT = L.take(sizeof(double) * (size_t)std::max(s.m, 1) * q.p);
+        }
+    }
+    // uninitialised: every slot is written below (the alignment gaps are
+    // copied but never read)
+    std::unique_ptr<char[]> stage(new char[std::max<size_t>(L.bytes, 1)]);
+    auto slot = [&](size_t o) { return reinterpret_cast<double*>(stage.get() + o); };
     parallel_for(N, [&](int i) {
         const SystemDesc& s = specs[i].sys;
         Sys& q = sys_[i];
+        const Off& o = off[i];
         const int mB = s.zeroB ? 0 : s.m;
-        Bbar[i].assign((size_t)q.n * q.W * std::max(mB, 1), 0.0);
-        Phi[i].resize((size_t)q.n * q.Ns);
+        double* phi = slot(o.phi0);
+        double* bbar = slot(o.bbar);
+        const size_t nb = (size_t)q.n * q.W * std::max(mB, 1);
+        std::fill(bbar, bbar + nb, 0.0);
         if (q.solver == kRK4)
-            discretise_rk4(q.n, mB, s.A.data(), mB ? s.B.data() : nullptr, q.h, Phi[i].data(), Bbar[i].data());
+            discretise_rk4(q.n, mB, s.A.data(), mB ? s.B.data() : nullptr, q.h, phi, bbar);
         else
-            discretise_abm_last(q.n, mB, s.A.data(), mB ? s.B.data() : nullptr, q.h, Phi[i].data(), Bbar[i].data());
-        X0[i].assign((size_t)q.Np, 0.0);
+            discretise_abm_last(q.n, mB, s.A.data(), mB ? s.B.data() : nullptr, q.h, phi, bbar);
         // distance of Phi from its exact 0/1 part (I for RK4; for ABM the
         // companion shift, whose rows above the last block are exact, the
         // last row block reading itself): the max row sum of |Phi - R| over
@@ -247,17 +272,60 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         for (int r = 0; r < q.n; ++r) {
             const int rc = d0 + r;
             double sum = 0.0;
-            for (int c = 0; c < q.Ns; ++c) sum += std::fabs(Phi[i][(size_t)r * q.Ns + c] - (c == rc ? 1.0 : 0.0));
+            for (int c = 0; c < q.Ns; ++c) sum += std::fabs(phi[(size_t)r * q.Ns + c] - (c == rc ? 1.0 : 0.0));
             dmax = std::max(dmax, sum);
         }
         q.delta = dmax;
-        if (q.solver == kRK4) {
-            for (int r = 0; r < q.n; ++r) X0[i][r] = s.x0[r];
+        if (s.zeroC) slot(o.c)[0] = 0.0;
+        else std::memcpy(slot(o.c), s.C.data(), sizeof(double) * (size_t)q.p * q.n);
+        if (s.zeroD) slot(o.d)[0] = 0.0;
+        else std::memcpy(slot(o.d), s.D.data(), sizeof(double) * (size_t)q.p * s.m);
+        double* x0 = slot(o.x0);
+        std::fill(x0, x0 + q.Np, 0.0);
+        if (q.solver == kRK4)
+            for (int r = 0; r < q.n; ++r) x0[r] = s.x0[r];  // ABM: the start-up below
+        if (q.blocked || q.resp) {
+            double* cext = slot(o.cext);
+            std::fill(cext, cext + (size_t)q.p * q.Np, 0.0);
+            const int xoff = q.solver == kRK4 ? 0 : 3 * q.n;
+            for (int r = 0; r < q.p; ++r)
+                for (int c = 0; c < q.n; ++c) {
+                    double v = 0.0;
+                    if (!s.zeroC) v = s.C[(size_t)r * q.n + c];
+                    else if (s.zeroD) v = (r == c) ? 1.0 : 0.0;
+                    cext[(size_t)r * q.Np + xoff + c] = v;
+                }
+        }
+        if (o.sin) {
+            const InputEntry* e = q.input;
+            double* prm = slot(o.sin);
+            const size_t na = e->a.size();
+            std::memcpy(prm, e->a.data(), sizeof(double) * na);
+            std::memcpy(prm + na, e->f.data(), sizeof(double) * na);
+            std::memcpy(prm + 2 * na, e->phi.data(), sizeof(double) * na);
+        }
+        if (!q.blocked && !q.resp) {
+            const int Wm = q.W * mB;
+            double* bt = slot(o.bbarT);
+            std::fill(bt, bt + (size_t)std::max(Wm, 1) * q.n, 0.0);
+            for (int r = 0; r < q.n; ++r)
+                for (int c = 0; c < Wm; ++c) bt[(size_t)c * q.n + r] = bbar[(size_t)r * Wm + c];
+            double* ct = slot(o.cT);
+            double* dt = slot(o.dT);
+            std::fill(ct, ct + (size_t)q.n * q.p, 0.0);
+            std::fill(dt, dt + (size_t)std::max(s.m, 1) * q.p, 0.0);
+            if (!s.zeroC)
+                for (int r = 0; r < q.p; ++r)
+                    for (int c = 0; c < q.n; ++c) ct[(size_t)c * q.p + r] = s.C[(size_t)r * q.n + c];
+            if (!s.zeroD)
+                for (int r = 0; r < q.p; ++r)
+                    for (int c = 0; c < s.m; ++c) dt[(size_t)c * q.p + r] = s.D[(size_t)r * s.m + c];
         }
     });
     phase("discretise", false);
     // ABM start-up: nine inputs at t0 + j h/2 (sinusoids on the host; user
-    // functions through their compiled kernel)
+    // functions through their compiled kernel); the four states into x0, the
+    // outputs 0..2 into their slot
     for (int i = 0; i < N; ++i) {
         Sys& q = sys_[i];
         if (q.solver != kABM) continue;
@@ -278,12 +346,11 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         }
         SystemDesc s0 = s;
         if (s0.zeroB) s0.m = 0;
-        std::vector<double> Xs((size_t)4 * q.n);
-        abm_startup(s0, U9.data(), q.h, Xs.data());
-        for (int r = 0; r < 4 * q.n; ++r) X0[i][r] = Xs[r];
-        Ypre[i].assign((size_t)3 * q.p, 0.0);
+        double* x0 = slot(off[i].x0);
+        abm_startup(s0, U9.data(), q.h, x0);  // the first 4 n of the Np slots
+        double* ypre = slot(off[i].ypre);
         for (int k = 0; k < 3; ++k) {
-            const double* x = &Xs[(size_t)k * q.n];
+            const double* x = x0 + (size_t)k * q.n;
             const double* u = &U9[(size_t)(2 * k) * std::max(s.m, 1)];
             for (int o = 0; o < q.p; ++o) {
                 double v = 0.0;
@@ -295,69 +362,11 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
                     if (!s.zeroD)
                         for (int c = 0; c < s.m; ++c) v += s.D[(size_t)o * s.m + c] * u[c];
                 }
-                Ypre[i][(size_t)k * q.p + o] = v;
+                ypre[(size_t)k * q.p + o] = v;
             }
         }
     }
-
     phase("abm-start-up", false);
-    // ---- arena layout: constants (staged) first, then work buffers ----------
-    Layout L;
-    Stage st;
-    struct Off {
-        size_t phi0, bbar, c, d, cext, x0, sin, ypre;
-        size_t bbarT, cT, dT;  // level-synchronous systems: transposed copies (coalesced per-row kernels)
-        size_t P, U, Y, V, G, CP, Ps, W, Psa, Psw;
-    };
-    std::vector<Off> off(N);
-    for (int i = 0; i < N; ++i) {
-        const SystemDesc& s = specs[i].sys;
-        Sys& q = sys_[i];
-        Off& o = off[i];
-        o.phi0 = st.put(Phi[i].data(), sizeof(double) * Phi[i].size(), L);
-        o.bbar = st.put(Bbar[i].data(), sizeof(double) * Bbar[i].size(), L);
-        o.c = st.put(s.zeroC ? nullptr : s.C.data(), sizeof(double) * (s.zeroC ? 1 : (size_t)q.p * q.n), L);
-        o.d = st.put(s.zeroD ? nullptr : s.D.data(), sizeof(double) * (s.zeroD ? 1 : (size_t)q.p * s.m), L);
-        o.x0 = st.put(X0[i].data(), sizeof(double) * X0[i].size(), L);
-        if (q.blocked || q.resp) {
-            std::vector<double> Cext((size_t)q.p * q.Np, 0.0);
-            const int xoff = q.solver == kRK4 ? 0 : 3 * q.n;
-            for (int r = 0; r < q.p; ++r)
-                for (int c = 0; c < q.n; ++c) {
-                    double v = 0.0;
-                    if (!s.zeroC) v = s.C[(size_t)r * q.n + c];
-                    else if (s.zeroD) v = (r == c) ? 1.0 : 0.0;
-                    Cext[(size_t)r * q.Np + xoff + c] = v;
-                }
-            o.cext = st.put(Cext.data(), sizeof(double) * Cext.size(), L);
-        }
-        if (q.mu > 0 && q.input->kind == InputEntry::kSinusoid) {
-            const InputEntry* e = q.input;
-            std::vector<double> prm;
-            prm.insert(prm.end(), e->a.begin(), e->a.end());
-            prm.insert(prm.end(), e->f.begin(), e->f.end());
-            prm.insert(prm.end(), e->phi.begin(), e->phi.end());
-            q.K = e->K;
-            o.sin = st.put(prm.data(), sizeof(double) * prm.size(), L);
-        }
-        if (q.solver == kABM) o.ypre = st.put(Ypre[i].data(), sizeof(double) * Ypre[i].size(), L);
-        if (!q.blocked && !q.resp) {
-            const int Wm = q.W * (s.zeroB ? 0 : s.m);
-            std::vector<double> bt((size_t)std::max(Wm, 1) * q.n, 0.0);
-            for (int r = 0; r < q.n; ++r)
-                for (int c = 0; c < Wm; ++c) bt[(size_t)c * q.n + r] = Bbar[i][(size_t)r * Wm + c];
-            o.bbarT = st.put(bt.data(), sizeof(double) * bt.size(), L);
-            std::vector<double> ct((size_t)q.n * q.p, 0.0), dt((size_t)std::max(s.m, 1) * q.p, 0.0);
-            if (!s.zeroC)
-                for (int r = 0; r < q.p; ++r)
-                    for (int c = 0; c < q.n; ++c) ct[(size_t)c * q.p + r] = s.C[(size_t)r * q.n + c];
-            if (!s.zeroD)
-                for (int r = 0; r < q.p; ++r)
-                    for (int c = 0; c < s.m; ++c) dt[(size_t)c * q.p + r] = s.D[(size_t)r * s.m + c];
-            o.cT = st.put(ct.data(), sizeof(double) * ct.size(), L);
-            o.dT = st.put(dt.data(), sizeof(double) * dt.size(), L);
-        }
-    }
     const size_t const_end = L.bytes;
     // work buffers (offsets only; not staged); per-kind totals for the log
     size_t kind_bytes[5] = {0, 0, 0, 0, 0};  // power tables + scan vectors, W, W split, samples, outputs
@@ -436,6 +445,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
                     ((size_t)1 << 20);
     }
     arena_bytes_ = align_up(work_end + job_bytes);
+    phase("layout", false);
     // keep the arena and the response tables' workspace (at most 1 GiB per
     // group) in the pool once freed: the workspace groups then reuse one
     // mapping, and the next batch of this size maps nothing new
@@ -489,7 +499,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         if (q.mu > 0 && q.input->kind == InputEntry::kSinusoid) q.sin = dp(o.sin);
     }
 
-    phase("layout+arena", true);
+    phase("arena", true);
     // ---- job arrays (staged after the work region) ----------------------------
     Layout J;
     J.bytes = work_end;
@@ -997,7 +1007,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
     // ---- upload and set-up launches ------------------------------------------
     // work buffers start zeroed (the response windows' sample padding relies on it)
     if (!rs_.empty()) PARODE_CUDA(cudaMemsetAsync(base + const_end, 0, work_end - const_end, stream_));
-    PARODE_CUDA(cudaMemcpyAsync(base, st.buf.data(), st.buf.size(), cudaMemcpyHostToDevice, stream_));
+    PARODE_CUDA(cudaMemcpyAsync(base, stage.get(), const_end, cudaMemcpyHostToDevice, stream_));
     PARODE_CUDA(cudaMemcpyAsync(base + work_end, jstage.data(), jstage.size(), cudaMemcpyHostToDevice, stream_));
     for (size_t k = 0; k < setup_copies.size(); k += 65535)
         launch_copy_batch(dSetup + k, (int)std::min<size_t>(65535, setup_copies.size() - k), max_copy, stream_);
@@ -1023,7 +1033,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
     // ready_, and the host images stay alive with the plan
     PARODE_CUDA(cudaEventCreateWithFlags(&ready_, cudaEventDisableTiming));
     PARODE_CUDA(cudaEventRecord(ready_, stream_));
-    host_keep_.push_back(std::move(st.buf));
+    host_stage_ = std::move(stage);
     host_keep_.push_back(std::move(jstage));
     phase("splits", true);
     if (opt.log)

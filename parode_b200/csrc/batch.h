@@ -144,6 +144,7 @@ private:
     // host images of the set-up copies, kept until the plan is destroyed so
     // that the constructor returns without waiting for the device
     std::vector<std::vector<char>> host_keep_;
+    std::unique_ptr<char[]> host_stage_;  // the staged constant region
     InputRegistry* inputs_ = nullptr;
     PlanOptions opt_;
     std::vector<Sys> sys_;

@@ -284,6 +284,7 @@ void Server::worker()
         f.reqs = j.reqs;
         f.bytes = j.bytes;
         f.t_admit = j.t_admit;
+        f.t_start = now_s();
         try {
             std::vector<BatchSpec> specs;
             specs.reserve(j.reqs.size());
@@ -296,7 +297,7 @@ void Server::worker()
             PlanOptions po;
             po.precision = opt_.precision;
             po.input_double = true;
-            po.log = opt_.log;
+            po.log = opt_.log >= 2;
             if (resolved) {
                 f.plan = std::make_unique<BatchPlan>(device_, std::move(specs), inputs_, po);
             } else {
@@ -359,9 +360,10 @@ void Server::retirer()
         if (opt_.log) {
             const double t = now_s(), z = t_first_;
             std::fprintf(stderr,
-                         "ParODE server batch (%zu requests): admitted %.1f ms, on the device %.1f ms, seen done %.1f ms, "
-                         "retired %.1f ms (after the first submission)\n",
-                         f.reqs.size(), (f.t_admit - z) * 1e3, (f.t_ready - z) * 1e3, (f.t_seen - z) * 1e3, (t - z) * 1e3);
+                         "ParODE server batch (%zu requests): admitted %.1f ms, set-up from %.1f ms, on the device %.1f ms, "
+                         "seen done %.1f ms, retired %.1f ms (after the first submission)\n",
+                         f.reqs.size(), (f.t_admit - z) * 1e3, (f.t_start - z) * 1e3, (f.t_ready - z) * 1e3,
+                         (f.t_seen - z) * 1e3, (t - z) * 1e3);
         }
         --retiring_;
         inflight_bytes_ -= f.bytes;

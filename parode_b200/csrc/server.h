@@ -33,7 +33,7 @@ struct ServerOptions {
     int max_batch = 256;        // systems per batch
     int max_inflight = 8;       // batches on the device (or being set up) at once
     int setup_threads = 4;      // host threads building batches concurrently
-    bool log = false;           // each batch's set-up phase times on stderr
+    int log = 0;                // 1: each batch's timeline on stderr; 2: also its set-up phases (which wait on the device)
     // device memory mapped into the stream-ordered pool at creation (at most
     // the budget and half the free memory)
     size_t prewarm_bytes = (size_t)32 << 30;
@@ -89,7 +89,7 @@ private:
         cudaEvent_t done = nullptr;
         size_t bytes = 0;
         // host times (log): admitted, enqueued on the device, seen finished
-        double t_admit = 0, t_ready = 0, t_seen = 0;
+        double t_admit = 0, t_start = 0, t_ready = 0, t_seen = 0;
     };
 
     struct Job {
