@@ -70,6 +70,19 @@ def test_host_entry_points():
     assert pb.num_outputs(0, 1.0, 0.0, 0.1) == -1
 
 
+
+def test_executions_option_round_trip():
+    import parode_b200 as pb
+
+    assert pb.get_option(pb.OPT_EXECUTIONS) == 1
+    pb.set_option(pb.OPT_EXECUTIONS, 16)
+    assert pb.get_option(pb.OPT_EXECUTIONS) == 16
+    with pytest.raises(pb.ParODEError):
+        pb.set_option(pb.OPT_EXECUTIONS, 0)
+    assert pb.get_option(pb.OPT_EXECUTIONS) == 16
+    pb.set_option(pb.OPT_EXECUTIONS, 1)
+
+
 def test_not_initialised_errors():
     import parode_b200 as pb
 

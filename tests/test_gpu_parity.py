@@ -135,6 +135,35 @@ def test_large_scan_plan_runs_as_one_system_batch(pb, solver, n, m, p, T):
     plan.close()
 
 
+
+@pytest.mark.parametrize("solver,n,m,p,T", [(0, 96, 4, 4, 4000), (1, 40, 3, 3, 3000)])
+def test_executions_option_changes_block_length_not_result(pb, solver, n, m, p, T):
+    """PARODE_OPT_EXECUTIONS: with the table build spread over many solves the
+    block-response leaf takes longer blocks; FP64 and mixed results match the
+    oracle either way."""
+    pb.set_option(pb.OPT_PATH, 0)
+    case = wl.small(7300 + n, solver, n, m, p, T, h=1e-3)
+    u = pb.register_sinusoid(case.u.a, case.u.f, case.u.phi)
+    ref = _oracle_y(case)
+    blocks = {}
+    try:
+        for ex in (1, 1000):
+            pb.set_option(pb.OPT_EXECUTIONS, ex)
+            for prec, tol in ((pb.FP64, TOL_FP64), (pb.MIXED, 1e-6)):
+                plan = pb.Plan(case.A, case.B, case.C, case.D, case.x0, u, case.t0, case.t_end, case.h,
+                               solver=solver, precision=prec)
+                assert plan.path == 3, plan.path
+                blocks[(ex, prec)] = plan.response_shape[0]
+                plan.execute()
+                _, y = plan.output()
+                err = oracle.rel_err(y, ref)
+                assert err <= tol, (ex, prec, err)
+                plan.close()
+    finally:
+        pb.set_option(pb.OPT_EXECUTIONS, 1)
+    assert blocks[(1, pb.FP64)] < blocks[(1000, pb.FP64)], blocks
+
+
 def _fx_input(kind):
     if kind == "sin_cos":
         return lambda t, i: math.sin(t) if i == 0 else (math.cos(t) if i == 1 else 0.0)
