@@ -9,8 +9,10 @@
 //    up (host FP64 discretisation, one stream-ordered arena) and enqueues it on
 //    its own stream, so batches that arrive while others run overlap on the
 //    device,
-//  - retires finished batches (event query), copies each request's outputs to
-//    host memory and releases the batch's device memory.
+//  - hands finished batches (event query) to copy-out threads, which move
+//    each request's outputs device-to-device into a pooled buffer of its own
+//    (counted against the budget until the caller collects it with result())
+//    and release the batch's arena.
 // Latency of a request = completion - submission (host clock).
 #pragma once
 
