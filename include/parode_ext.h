@@ -106,10 +106,13 @@ int ParODE_PlanStageTimes(ParODE_Plan* plan, float* ms, int cap, char* names, in
  * One call set-up for nSystems systems (per-system arrays of the
  * SimulateODE_d arguments; B, C, D may be NULL arrays when every system has
  * that matrix absent).  Device-resident afterwards: BatchExecute enqueues all
- * solves on `stream` with a fixed, small number of launches (scan dimension
- * <= 64: batched blocked path per padded dimension; larger: one grouped
- * contraction launch per Blelloch level).  The reference has no batch entry
- * point: it solves one system per SimulateODE call (Sources/ParODE.cpp:281-337). */
+ * solves on `stream` with a fixed, small number of launches (systems with
+ * inputs: the block-response leaf, one grouped GEMM per stage; scan dimension
+ * <= 64 otherwise: batched blocked path per padded dimension; larger: one
+ * grouped contraction launch per Blelloch level).  BatchCreate returns before
+ * the device has finished the set-up it enqueued; BatchExecute on any stream
+ * is ordered after it.  The reference has no batch entry point: it solves one
+ * system per SimulateODE call (Sources/ParODE.cpp:281-337). */
 typedef struct ParODE_Batch ParODE_Batch;
 ParODE_Batch* ParODE_BatchCreate(int nSystems, const double* const A[], const double* const B[],
                                  const double* const C[], const double* const D[], const int nInputs[],
