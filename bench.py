@@ -32,9 +32,6 @@ sys.path.insert(0, ROOT)
 METRIC = "state*steps/s (RK4 n=64 T=2^20 solve, mixed 3xTF32 form, rel err <= 1e-6 vs FP64)"
 UNIT = "state*steps/s"
 WORKLOAD = "cfg2: RK4 n=64 m=8 p=8 h=1e-4 T=2^20, seeded system + sum-of-sinusoids input"
-# DRAM bytes (read + write) of one leaf launch on this workload, from the ncu
-# captures summarised in profiles/k_leaf_tc_cfg2_rk4_n64.md (mixed) and
-# profiles/k_leaf_fp64_cfg2_rk4_n64.md (FP64); keyed by (T, mixed).
 # DRAM bytes (read + write) of one launch of the dominant kernel at T = 2^20
 # (key: (T, mixed)), from the ncu captures summarised under profiles/.
 DOMINANT_TRAFFIC = {(1 << 20, False): 168.18e6 + 45.27e6, (1 << 20, True): 134.87e6 + 66.91e6}
@@ -43,7 +40,7 @@ DOMINANT_TRAFFIC = {(1 << 20, False): 168.18e6 + 45.27e6, (1 << 20, True): 134.8
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
@@ -54,7 +51,16 @@ def parse():
     ap.add_argument("--min-warmup-s", type=float, default=0.5, help="least warm-up time under load (clock sampling)")
     ap.add_argument("--no-extra", action="store_true", help="skip the batched (4096 systems) and serving runs")
     ap.add_argument("--serve-requests", type=int, default=256)
+    ap.add_argument("--ref-T", type=int, default=1 << 20,
+                    help="reference arm: steps of the cfg2 horizon solved per timed step (default: all 2^20)")
     return ap.parse_args()
+
+
+def bench_config(args, world):
+    """The `config` object of both arms' JSON lines (identical by construction)."""
+    return {"workload": WORKLOAD, "precision": args.precision,
+            "l2": "256 MB flush between timed solves (outside the events)",
+            "parallelism": f"replicas x{world}"}
 
 
 def dist_env():
@@ -85,9 +91,9 @@ def run_reference(args):
     rank, _, world = dist_env()
     if rank != 0:
         return
-    # a bounded sample per step (about 30 s of CPU work for the whole run at ~1.3e5 steps/s)
-    k = int(np.floor(np.log2(4.0e6 / max(1, args.steps + args.warmup))))
-    T_sample = 1 << min(16, max(12, k))
+    # each timed step solves the whole cfg2 horizon (2^20 steps, ~8 s on one
+    # core), so the line's config is the GPU arm's; --ref-T shortens it
+    T_sample = max(1, min(args.ref_T, args.T))
     case, run = reference_sample(T_sample)
     times = []
     for it in range(args.warmup + args.steps):
@@ -98,13 +104,16 @@ def run_reference(args):
             times.append(dt)
     per = statistics.mean(times)
     value = case.n * T_sample / per
-    sample = (f"cfg2 system (RK4 n=64 m=8 p=8), first {T_sample} of 2^20 steps per step; the reference's sequential "
-              f"FP32 RK4 test loop restated in C (one system is one sequential chain: 1 thread)")
+    sample = (f"cfg2 system (RK4 n=64 m=8 p=8), {T_sample} of its {args.T} steps per timed step; the reference's "
+              f"sequential FP32 RK4 test loop restated in C (one system is one sequential chain: 1 thread)")
+    config = bench_config(args, world)
+    if T_sample < args.T:
+        config["sampled_steps_per_step"] = T_sample
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": per * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sampled_steps_per_step": T_sample},
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded system and input)",
+        "config": config,
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -523,12 +532,10 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": main["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": "tf32x3+f64" if used_mixed else "f64", "data": "synthetic (seeded system and input)",
-            "config": {"workload": WORKLOAD,
-                       "precision": "mixed" if used_mixed else "fp64",
-                       "path": {1: "level-synchronous", 2: "blocked, in-block sweeps",
-                                3: "blocked, block-response GEMMs"}.get(main["path"], "?"),
-                       "l2": "256 MB flush between timed solves (outside the events)",
-                       "parallelism": f"replicas x{world}"},
+            "config": bench_config(args, world),
+            "precision_used": "mixed" if used_mixed else "fp64",
+            "path": {1: "level-synchronous", 2: "blocked, in-block sweeps",
+                     3: "blocked, block-response GEMMs"}.get(main["path"], "?"),
             "gpu_launches": main["launches"] * args.steps, "solve_ms": main["solve_ms"],
             "clocks": clk.summary(), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "plain_fp64": None if plain is None else {

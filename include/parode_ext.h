@@ -179,9 +179,15 @@ void ParODE_ServerDestroy(ParODE_Server* srv);
  * Phi ns x ns, dGamma count x ns, dX count x ns, all row-major FP64;
  * dGamma or dX0 may be NULL (zero).  ns in [1, 64].  Enqueued on `stream`
  * (NULL: the legacy default stream); returns after enqueueing.
- * It allocates nothing: its scratch is a static 16 MiB device array, looked
- * up on the first call on each device (make that call before any stream
- * capture).  A call needs levels*NP^2 + NP + count*NP*(1 + ~1/(B-1))
+ * It allocates nothing: its scratch is a static 16 MiB device array.  The
+ * array's address is looked up, and the entry point's kernels loaded, once
+ * per device by InitializeAllGPUs / InitializeSelectedGPUs (or by the first
+ * call on a device when the library was not initialised): with lazy module
+ * loading that is when the array's device memory is mapped, so initialise
+ * (or make a first call) before reserving the device's memory for your own
+ * pool, and before any stream capture.  The address belongs to the device's
+ * primary context (not valid after cudaDeviceReset or under another context).
+ * A call needs levels*NP^2 + NP + count*NP*(1 + ~1/(B-1))
  * doubles of it (NP = power of two >= max(8, ns)): count <= ~29,000 at
  * ns = 64, ~230,000 at ns = 8; larger calls fail with -4 (NotEnoughResources).
  * The scratch is shared: calls that overlap on the GPU race on it. */

@@ -78,6 +78,10 @@ def lib():
                                               C.POINTER(C.c_long)]
         L.po_rel_err.restype = C.c_double
         L.po_rel_err.argtypes = [dp, dp, C.c_long, C.c_int]
+        L.po_simulate_affine_many.restype = C.c_int
+        L.po_simulate_affine_many.argtypes = [C.c_int, C.POINTER(_System), C.POINTER(_Input), C.POINTER(C.c_int),
+                                              dp, dp, dp, C.POINTER(dp)]
+        L.po_threads.restype = C.c_int
         L.po_sinusoid_eval.restype = C.c_double
         L.po_sinusoid_eval.argtypes = [C.c_double, C.c_int, C.c_void_p]
         _lib = L
@@ -189,6 +193,38 @@ def simulate_affine(sys_: System, inp: Input, solver: int, t0: float, t_end: flo
     if rc != 0:
         raise RuntimeError(f"oracle error {rc}")
     return y
+
+
+def simulate_affine_many(jobs):
+    """O1 of many independent systems on all host threads.
+
+    jobs: a sequence of (System, Input, solver, t0, t_end, h) whose inputs are
+    sinusoids (thread-safe).  Returns the list of y arrays, each (T, p)."""
+    count = len(jobs)
+    if count == 0:
+        return []
+    systems = (_System * count)()
+    inputs = (_Input * count)()
+    solvers = (C.c_int * count)()
+    t0s, t1s, hs = (C.c_double * count)(), (C.c_double * count)(), (C.c_double * count)()
+    ys = []
+    yp = (C.POINTER(C.c_double) * count)()
+    for i, (sys_, inp, solver, t0, t_end, h) in enumerate(jobs):
+        if inp._c.fn is not None and inp._c.ctx is None:
+            raise ValueError("simulate_affine_many: Python callables are not thread-safe inputs")
+        nt, _ = num_outputs(solver, t0, t_end, h)
+        if nt <= 0:
+            raise ValueError("empty horizon")
+        y = np.zeros((nt, sys_.out_size), dtype=np.float64)
+        ys.append(y)
+        systems[i] = sys_._c
+        inputs[i] = inp._c
+        solvers[i], t0s[i], t1s[i], hs[i] = solver, t0, t_end, h
+        yp[i] = _dptr(y)
+    rc = lib().po_simulate_affine_many(count, systems, inputs, solvers, t0s, t1s, hs, yp)
+    if rc != 0:
+        raise RuntimeError(f"oracle error {rc}")
+    return ys
 
 
 def stepper(sys_: System, inp: Input, solver: int, t0: float, h: float, T: int, use_float: bool):

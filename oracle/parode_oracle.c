@@ -872,3 +872,41 @@ int po_threads(void)
     return 1;
 #endif
 }
+
+int po_simulate_affine_many(int count, const po_system* s, const po_input* in, const int* solver,
+                            const double* t0, const double* tEnd, const double* h, double* const* y)
+{
+    /* O1 of each system on its own (the systems are independent); the
+     * largest systems first so that the threads finish together. */
+    int worst = 0;
+    long* order = (long*)malloc(sizeof(long) * (size_t)(count > 0 ? count : 1));
+    double* cost = (double*)malloc(sizeof(double) * (size_t)(count > 0 ? count : 1));
+    for (int i = 0; i < count; ++i) {
+        long ns = 0;
+        po_num_outputs(solver[i], t0[i], tEnd[i], h[i], &ns);
+        double N = solver[i] == PO_ABM ? 4.0 * s[i].n : (double)s[i].n;
+        cost[i] = (double)ns * N * (double)s[i].n;
+        order[i] = i;
+    }
+    for (int i = 1; i < count; ++i) {
+        long v = order[i];
+        int j = i - 1;
+        while (j >= 0 && cost[order[j]] < cost[v]) {
+            order[j + 1] = order[j];
+            --j;
+        }
+        order[j + 1] = v;
+    }
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 1) reduction(min : worst)
+#endif
+    for (int q = 0; q < count; ++q) {
+        long i = order[q];
+        long n_out = 0;
+        int rc = po_simulate_affine(&s[i], &in[i], solver[i], t0[i], tEnd[i], h[i], y[i], &n_out);
+        if (rc < worst) worst = rc;
+    }
+    free(order);
+    free(cost);
+    return worst;
+}

@@ -135,6 +135,13 @@ double po_rel_err(const double* y, const double* yref, long T, int p);
 /* Thread-parallel O1 over independent systems (OpenMP when compiled with it). */
 int po_threads(void);
 
+/* O1 (po_simulate_affine) of `count` independent systems, spread over the
+ * OpenMP threads; y[i] receives system i's outputs.  Input functions must be
+ * callable from several threads at once (the built-in sinusoid is).  Returns
+ * 0, or the most negative error code of any system. */
+int po_simulate_affine_many(int count, const po_system* s, const po_input* in, const int* solver,
+                            const double* t0, const double* tEnd, const double* h, double* const* y);
+
 #ifdef __cplusplus
 }
 #endif

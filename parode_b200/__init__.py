@@ -9,9 +9,11 @@ ctypes layer for Python callers, tests and benchmarks:
     u = pb.register_sinusoid(a, f, phi)        # or pb.register_input(src)
     t, y = pb.simulate(A, B, C, D, x0, u, t0, t_end, h, solver=pb.RK4)
 
-Every call goes to the CUDA library.  There is no CPU fallback: importing the
-package fails if libParODEShared.so is missing, and solves report ParODE
-error codes as exceptions.
+Every call goes to the CUDA library.  There is no CPU fallback: the first
+call that needs libParODEShared.so loads it and fails (ImportError) if it is
+missing, and solves report ParODE error codes as exceptions.  Importing the
+package alone maps no library, so `parode_b200.workloads` (the seeded
+generators) serves processes that never touch the GPU.
 """
 from __future__ import annotations
 
@@ -132,7 +134,18 @@ def _load():
     return L
 
 
-lib = _load()
+class _Library:
+    """libParODEShared.so, loaded with its ctypes signatures on first use."""
+
+    _handle = None
+
+    def __getattr__(self, name):
+        if _Library._handle is None:
+            _Library._handle = _load()
+        return getattr(_Library._handle, name)
+
+
+lib = _Library()
 
 
 def _dp(a: Optional[np.ndarray]):

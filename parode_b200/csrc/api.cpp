@@ -11,6 +11,7 @@
 #include "inputs.h"
 #include "solver.h"
 #include "batch.h"
+#include "blocked.h"
 #include "server.h"
 
 #include "FTypeDef.h"
@@ -23,6 +24,8 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
+#include <utility>
 #include <vector>
 
 using namespace parode;
@@ -80,6 +83,13 @@ struct Library {
         for (int d : ids) {
             if (cudaSetDevice(d) != cudaSuccess || cudaFree(nullptr) != cudaSuccess) {
                 cudaGetLastError();
+                return kCouldNotCreateGPUKernels;
+            }
+            // the allocation-free entry point's scratch and kernels are
+            // loaded now, while the device still has memory to map them
+            try {
+                noalloc_setup_device(d);
+            } catch (const Error&) {
                 return kCouldNotCreateGPUKernels;
             }
         }
@@ -162,6 +172,21 @@ int guarded(F&& f)
         return kDeviceError;
     }
 }
+
+// A host thread that is joined on every exit path (including exceptions).
+class HelperThread {
+public:
+    template <class F>
+    void run(F&& f) { t_ = std::thread(std::forward<F>(f)); }
+    void join()
+    {
+        if (t_.joinable()) t_.join();
+    }
+    ~HelperThread() { join(); }
+
+private:
+    std::thread t_;
+};
 
 }  // namespace
 
@@ -277,11 +302,16 @@ void SimulateODE(fType A[], fType B[], fType C[], fType D[], int* nInputs, int* 
         opt.path = L.path;
         opt.input_double = false;  // UFunc(fType t, ...) with fType = float, as the reference ABI
         Plan plan(dev, s, &L.inputs, *uIndex, *solver, *tStart, *tEnd, *tStep, opt);
-        plan.execute(nullptr, nullptr);
         long T = plan.num_outputs();
         int p = plan.channels();
         std::vector<double> t((size_t)T), y((size_t)T * p);
-        plan.get_output(t.data(), y.data());
+        HelperThread tv;
+        const int sv = *solver;
+        const double t0 = *tStart, t1 = *tEnd, h = *tStep;
+        if (tVect) tv.run([&t, sv, t0, t1, h] { time_vector(sv, t0, t1, h, t.data()); });
+        plan.execute(nullptr, nullptr);
+        plan.get_output(nullptr, y.data());
+        tv.join();
         if (tVect)
             for (long k = 0; k < T; ++k) tVect[k] = (fType)t[(size_t)k];
         if (xVect)
@@ -430,8 +460,13 @@ void ParODE_SimulateODE_d(const double* A, const double* B, const double* C, con
         opt.path = L.path;
         opt.input_double = true;
         Plan plan(dev, s, &L.inputs, uIndex, solver, tStart, tEnd, tStep, opt);
+        // the host time vector is built on a helper thread while the plan
+        // is set up, solved and its outputs copied
+        HelperThread tv;
+        if (tVect) tv.run([=] { time_vector(solver, tStart, tEnd, tStep, tVect); });
         plan.execute(nullptr, nullptr);
-        plan.get_output(tVect, yVect);
+        plan.get_output(nullptr, yVect);
+        tv.join();
         if (nSteps) nSteps[0] = plan.num_outputs();
     });
     if (nErr) nErr[0] = rc;

@@ -77,6 +77,16 @@ void launch_blocked_fixup(const BlockedShape& sh, double* Y, long ybase, long nS
 // P_l = P_{l-1}^2 for l in [l0, l1) (single CTA, NP <= 64), then, when CP is
 // not null, CP[i] = Cext Phi^i for i < B (Cext: p x NP, the output rows of the
 // scan state) by doubling with the table: CP[i + 2^k] = CP[i] P_k.
+// Loads the carry kernels (items up / top / down, power tables) on the
+// current device.  With lazy module loading a kernel's module is otherwise
+// loaded, and its device memory mapped, at its first launch.
+void preload_blocked_carry_kernels();
+
+// Set-up of the allocation-free affine scan (noalloc.cu) on device `dev`:
+// resolves its static scratch and loads its kernels, so that no later call
+// maps device memory.
+void noalloc_setup_device(int dev);
+
 void launch_blocked_tables(const BlockedShape& sh, double* P, int l0, int l1, double* CP, const double* Cext, int p,
                            cudaStream_t s);
 

@@ -1,6 +1,7 @@
 // host_math.cpp -- host FP64 set-up of a solve (see host_math.h).
 #include "host_math.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -46,6 +47,51 @@ long num_outputs(int solver, double t0, double tEnd, double h, long* n_scan)
     return solver == 1 ? ns + 3 : ns;
 }
 
+namespace {
+
+// One link of the reference's time accumulation: the float time plus the
+// double step, rounded back to float (Sources/GPUFixedStepIterative.cpp:141-146).
+inline double time_link(double prev, double h) { return (double)(float)(prev + h); }
+
+}  // namespace
+
+void time_chain(double* tv, long count, double h)
+{
+    // The chain tv[i+1] = time_link(tv[i]) is one dependent float round trip
+    // per element (~5 ms for 2^20).  Within a binade of the float values it
+    // advances by a constant increment, so it is filled by speculation and
+    // checked link by link: from a checked element, the arithmetic progression
+    // with the next increment is written for a block, every link of the block
+    // is checked independently (no dependency between the checks), and the
+    // first failing link, if any, is recomputed and the speculation restarts
+    // after it.  Every element is therefore exactly the chain's.  A failure
+    // near the start of a block (an increment that alternates, as at exact
+    // rounding ties) switches to plain chaining for a stretch.
+    constexpr long kBlock = 2048, kEarly = 16, kStretch = 256;
+    long s = 0;
+    while (s + 1 < count) {
+        const double v = tv[s];
+        const double d = time_link(v, h) - v;
+        const long e = std::min(count - 1, s + kBlock);
+        for (long j = s + 1; j <= e; ++j) tv[j] = v + (double)(j - s) * d;
+        int ok = 1;
+        for (long j = s; j < e; ++j) ok &= (time_link(tv[j], h) == tv[j + 1]) ? 1 : 0;
+        if (ok) {
+            s = e;
+            continue;
+        }
+        long j = s;
+        while (time_link(tv[j], h) == tv[j + 1]) ++j;
+        tv[j + 1] = time_link(tv[j], h);
+        long next = j + 1;
+        if (j - s < kEarly) {
+            const long stop = std::min(count - 1, next + kStretch);
+            for (; next < stop; ++next) tv[next + 1] = time_link(tv[next], h);
+        }
+        s = next;
+    }
+}
+
 void time_vector(int solver, double t0, double tEnd, double h, double* tv)
 {
     long ns = 0;
@@ -53,13 +99,9 @@ void time_vector(int solver, double t0, double tEnd, double h, double* tv)
     if (nt <= 0) return;
     long pre = nt - ns;
     double ts = (solver == 1) ? t0 + 3.0 * h : t0;
-    float prev = (float)ts;
     for (long i = 0; i < pre; ++i) tv[i] = (double)(float)(ts - (double)(pre - i) * h);
-    tv[pre] = (double)prev;
-    for (long i = 1; i < ns; ++i) {
-        prev = (float)((double)prev + h);
-        tv[pre + i] = (double)prev;
-    }
+    tv[pre] = (double)(float)ts;
+    time_chain(tv + pre, ns, h);
 }
 
 void discretise_rk4(int n, int m, const double* A, const double* B, double h, double* Phi, double* Bbar)

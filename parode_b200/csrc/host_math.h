@@ -21,6 +21,9 @@ struct SystemDesc {
 // number of outputs or -1 for an empty horizon.
 long num_outputs(int solver, double t0, double tEnd, double h, long* n_scan);
 
+// tv[1..count) from tv[0]: tv[i+1] = float(tv[i] + h), the reference's
+// float time accumulation, element for element.
+void time_chain(double* tv, long count, double h);
 // Time vector with the reference's float accumulation
 // (Sources/GPUFixedStepIterative.cpp:141-146); written as double.
 void time_vector(int solver, double t0, double tEnd, double h, double* tv);

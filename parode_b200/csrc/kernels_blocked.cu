@@ -877,6 +877,24 @@ static void tables_t(const BlockedShape& sh, double* P, int l0, int l1, double* 
     PARODE_CUDA(cudaGetLastError());
 }
 
+template <int NP>
+static void preload_carry_t()
+{
+    cudaFuncAttributes a;
+    PARODE_CUDA(cudaFuncGetAttributes(&a, k_items_up<NP>));
+    PARODE_CUDA(cudaFuncGetAttributes(&a, k_items_down<NP>));
+    PARODE_CUDA(cudaFuncGetAttributes(&a, k_items_top<NP>));
+    PARODE_CUDA(cudaFuncGetAttributes(&a, k_tables<NP>));
+}
+
+void preload_blocked_carry_kernels()
+{
+    preload_carry_t<8>();
+    preload_carry_t<16>();
+    preload_carry_t<32>();
+    preload_carry_t<64>();
+}
+
 void launch_blocked_tables(const BlockedShape& sh, double* P, int l0, int l1, double* CP, const double* Cext, int p,
                            cudaStream_t s)
 {

@@ -74,12 +74,6 @@ constexpr uint32_t kTmemCols = 512;  // hi*hi: kAcc drain buffers; corrections: 
 constexpr int kDrain = 8;  // K slices per FP32 accumulation chain
 constexpr long long kWaitLimit = 1LL << 31;
 
-// Phase-trace hook (no-op unless a timing harness defines it).
-#ifndef PARODE_TC_TRACE
-#define PARODE_TC_TRACE_INIT() ((void)0)
-#define PARODE_TC_TRACE(ev) ((void)0)
-#endif
-
 __host__ __device__ constexpr uint32_t koff(int r, int k) { return kmajor_off(r, k, kBK); }
 
 // K elements of slice s (16, or fewer in the last slice).
@@ -218,6 +212,17 @@ __device__ __forceinline__ void tile_coords(const LevelArgs& a, long lt, int& mi
     nk = (level_k(a) + kBK - 1) / kBK;
 }
 
+// K slice read at position s of tile lt: each tile starts its K loop at its
+// own slice (tile index mod the slice count), so that the CTAs, which all
+// read the same P blocks, spread over the blocks at any moment instead of
+// fetching the same bytes from the same L2 slices together.  The order of a
+// tile depends on the tile alone, so results do not depend on which CTA runs it.
+__device__ __forceinline__ int rotated_slice(long lt, int s, int nk)
+{
+    const int r = (int)(lt % nk) + s;
+    return r < nk ? r : r - nk;
+}
+
 // Persistent grouped kernel: CTA c walks tiles [cta[c], cta[c+1]) in order.
 __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __restrict__ args,
                                                           const long* __restrict__ start, int nent,
@@ -233,7 +238,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
     uint64_t* corr_empty = bars + 3 * kS + 2 * kAcc;
     uint32_t* slot = reinterpret_cast<uint32_t*>(sm + kOffSlot);
     volatile int* abort = reinterpret_cast<volatile int*>(sm + kOffSlot + 8);
-    PARODE_TC_TRACE_INIT();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
         for (int q = 0; q < kS; ++q) {
@@ -290,16 +294,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
                 // groups, hi and lo): the MMA's other rows read whatever the
                 // stage held, and their results are never stored.
                 if (lane == 0) {
+                    const int sr = rotated_slice(lt, s, nk);
                     const int rowsv = level_rows(a) - m0 < kBM ? level_rows(a) - m0 : kBM;
                     const uint32_t abytes = (uint32_t)((rowsv + 7) / 8) * (uint32_t)(kBK * 32);
-                    const unsigned char* ab = reinterpret_cast<const unsigned char*>(a.Ps) + ((size_t)mi * nk + s) * kABlock;
+                    const unsigned char* ab = reinterpret_cast<const unsigned char*>(a.Ps) + ((size_t)mi * nk + sr) * kABlock;
                     mbar_arrive_tx(&full[st], 2 * abytes + kBRaw);
                     bulk_g2s(stg, ab, abytes, &full[st]);
                     bulk_g2s(stg + kAHalf, ab + kAHalf, abytes, &full[st]);
-                    tma_load_2d(stg + kOffRaw, a.src_map, s * kBK, (int)n0, &full[st]);
+                    tma_load_2d(stg + kOffRaw, a.src_map, sr * kBK, (int)n0, &full[st]);
                 }
                 __syncwarp();
-                PARODE_TC_TRACE(0);
             }
         }
     } else if (warp == 1) {
@@ -362,7 +366,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
                             mma_tf32(q == 0 ? d : dc, A[q] + (uint64_t)(k * 16), B[q] + (uint64_t)(k * 16), idesc,
                                      ((q == 0 && s % kDrain == 0) || (q == 1 && s == 0)) && k == 0 ? 0u : 1u);
                     mma_commit(&empty[st]);
-                    PARODE_TC_TRACE(1);
                     if (s % kDrain == kDrain - 1 || s == nk - 1) {
                         mma_commit(&acc_full[ab]);
                         ++u;
@@ -392,7 +395,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
                 }
                 unsigned char* stg = sm + st * kStage;
                 const double* raw = reinterpret_cast<const double*>(stg + kOffRaw);
-                const int kl = slice_len(level_k(a), s);
+                const int kl = slice_len(level_k(a), rotated_slice(lt, s, nk));
                 // 64 vectors x kBK/4 chunks of 4 K; item w -> vector w / (kBK/4),
                 // chunk w % (kBK/4): a warp reads whole vectors and writes
                 // contiguous core-matrix rows
@@ -416,7 +419,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
                 fence_async_smem();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&conv[st]);
-                PARODE_TC_TRACE(2);
             }
             if (!ok) break;
         }
@@ -444,7 +446,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
                     ok = false;
                     break;
                 }
-                PARODE_TC_TRACE(3);
                 fence_after_sync();
                 // hi*hi of this unit; at the tile's last unit also the corrections
                 // (read before the arrive below, so a later arrive implies them)
@@ -504,7 +505,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
                         if (c0 + jj < nvt) drow[(n0 + c0 + jj) * dgs] = (sum[c0 + jj] + xs[jj]) + xa[jj];
                 }
             }
-            PARODE_TC_TRACE(4);
         }
     }
 

@@ -26,11 +26,6 @@
 
 #include <algorithm>
 
-// Phase hook for timing harnesses; compiled out in the library.
-#ifndef PARODE_TRACE
-#define PARODE_TRACE() ((void)0)
-#endif
-
 namespace parode {
 
 namespace {
@@ -163,7 +158,6 @@ __device__ void tc_level(unsigned char* sm, const TcLayout& L, uint64_t* bar, ui
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (tid == 0) {
         fence_after_sync();
-        PARODE_TRACE();
         const uint32_t base = smem_u32(sm);
         const uint32_t ph = base + L.ph + (uint32_t)l * 2 * NP * NP * 4;
         for (int z = 0; z < slices; ++z) {
@@ -172,11 +166,9 @@ __device__ void tc_level(unsigned char* sm, const TcLayout& L, uint64_t* bar, ui
                  ph + NP * NP * 4, 128, SBO, 256, NP / 8, make_idesc(128, NP), true);
         }
         mma_commit(bar);
-        PARODE_TRACE();
     }
     __syncwarp();
     round_wait(bar, phase, status);
-    PARODE_TRACE();
     const int sub = warp & 3, half = warp >> 2;
     if (half < H) {
         for (int z = 0; z < slices; ++z) {
@@ -203,7 +195,6 @@ __device__ void tc_level(unsigned char* sm, const TcLayout& L, uint64_t* bar, ui
         }
     }
     round_end();
-    PARODE_TRACE();
 }
 
 // Down-sweep bookkeeping of level l: V[left(g)] <-> V[right(g)] for g < c.
@@ -229,7 +220,6 @@ __device__ void tc_swap(unsigned char* sm, const TcLayout& L, int R, int S, int 
         }
     }
     round_end();
-    PARODE_TRACE();
 }
 
 template <int NP>
@@ -293,7 +283,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_leaf_tc(LeafArgs a, int R, in
     uint32_t phase = 0;
 
     for (long tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
-        PARODE_TRACE();
         const long j0 = tile * S;
         // 1. input samples (hi/lo, 16-byte rows): RK4 arrays of even / odd
         //    half-step samples, ABM one array of whole-step samples
@@ -308,7 +297,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_leaf_tc(LeafArgs a, int R, in
             *sptr(sm, L, arr, 1, r, i) = lo;
         }
         round_end();
-        PARODE_TRACE();
         // 2. forcing on the tensor cores: Gamma (S x NP) = sum_w U_w B_w^T
         {
             const int slices = (S + 127) >> 7;
@@ -327,11 +315,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_leaf_tc(LeafArgs a, int R, in
                     }
                 }
                 mma_commit(bar);
-                PARODE_TRACE();
             }
             __syncwarp();
             round_wait(bar, phase, a.status);
-            PARODE_TRACE();
             const int sub = warp & 3, half = warp >> 2;
             if (half < H) {
                 for (int z = 0; z < slices; ++z) {
@@ -356,7 +342,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_leaf_tc(LeafArgs a, int R, in
                 }
             }
             round_end();
-            PARODE_TRACE();
         }
         // 3. up-sweep on the tensor cores
         for (int l = 0; l < R; ++l) tc_level<NP>(sm, L, bar, tbase, R, S, l, phase, a.status);
@@ -372,7 +357,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_leaf_tc(LeafArgs a, int R, in
                 *lp = 0.f;
             }
             round_end();
-            PARODE_TRACE();
         }
         // 5. down-sweep from the zero roots
         for (int l = R - 1; l >= 0; --l) {

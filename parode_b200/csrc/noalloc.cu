@@ -11,10 +11,18 @@
 //    cudaMalloc / cudaFree would synchronise the device and stall them,
 //  - a fixed-memory, fixed-latency loop that must not hit the allocator.
 //
-// Set-up: the first call on each device (with that device current) looks up
-// the scratch array's device address with cudaGetSymbolAddress and caches it;
-// later calls reuse the cached pointer.  Make the first call on a device
-// before any stream capture is started on it.
+// Set-up, once per device with that device current: look up the scratch
+// array's device address with cudaGetSymbolAddress, check the return code and
+// cache the pointer; and load every kernel the entry point launches.  With
+// the CUDA runtime's lazy module loading (the default since CUDA 12.2) that
+// set-up is what loads the array's module and maps its device memory, and a
+// kernel's module is otherwise loaded at its first launch.  InitializeAllGPUs
+// and InitializeSelectedGPUs run the set-up for every device they select; a
+// caller that skips them gets it on its first call on a device.  Either must
+// come before the caller reserves the device's memory for itself, and before
+// any stream capture is started on the device.  The cached pointer belongs to
+// the device's primary context: after cudaDeviceReset, or under another
+// context made current by the caller, the address is stale.
 //
 // The scratch is shared by all calls on a device: calls whose work overlaps
 // on the GPU (two streams, or two host threads with no ordering between them)
@@ -86,6 +94,27 @@ unsigned grid_for(long work, int sms)
     return (unsigned)std::max<long>(1, std::min<long>((work + kPadThreads - 1) / kPadThreads, 8L * sms));
 }
 
+// Per-device set-up (see the file comment); idempotent.  Caller holds g_mu.
+void setup_device_locked(int dev)
+{
+    if (g_scratch_ptr[dev] != nullptr) return;
+    void* p = nullptr;
+    cudaError_t rc = cudaGetSymbolAddress(&p, g_scan_scratch);
+    if (rc != cudaSuccess || p == nullptr) {
+        cudaGetLastError();
+        throw Error(kDeviceError, std::string("cudaGetSymbolAddress(scan scratch): ") + cudaGetErrorString(rc));
+    }
+    cudaFuncAttributes fa;
+    PARODE_CUDA(cudaFuncGetAttributes(&fa, k_pad_rows));
+    PARODE_CUDA(cudaFuncGetAttributes(&fa, k_pad_matrix));
+    PARODE_CUDA(cudaFuncGetAttributes(&fa, k_unpad_rows));
+    preload_blocked_carry_kernels();
+    int n = 0;
+    PARODE_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+    g_sms[dev] = n;
+    g_scratch_ptr[dev] = static_cast<double*>(p);
+}
+
 // Scratch pointer and SM count of the current device (set-up on first use).
 double* scratch_for_current_device(int* sms)
 {
@@ -93,16 +122,7 @@ double* scratch_for_current_device(int* sms)
     PARODE_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) throw Error(kInvalidDeviceId, "device id out of range");
     std::lock_guard<std::mutex> g(g_mu);
-    if (g_scratch_ptr[dev] == nullptr) {
-        void* p = nullptr;
-        cudaError_t rc = cudaGetSymbolAddress(&p, g_scan_scratch);
-        if (rc != cudaSuccess || p == nullptr)
-            throw Error(kDeviceError, std::string("cudaGetSymbolAddress(scan scratch): ") + cudaGetErrorString(rc));
-        int n = 0;
-        PARODE_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
-        g_sms[dev] = n;
-        g_scratch_ptr[dev] = static_cast<double*>(p);
-    }
+    setup_device_locked(dev);
     *sms = g_sms[dev];
     return g_scratch_ptr[dev];
 }
@@ -157,6 +177,23 @@ void affine_scan_device(const double* dPhi, const double* dGamma, const double* 
 }
 
 }  // namespace
+
+void noalloc_setup_device(int dev)
+{
+    if (dev < 0 || dev >= kMaxDevices) throw Error(kInvalidDeviceId, "device id out of range");
+    int prev = -1;
+    PARODE_CUDA(cudaGetDevice(&prev));
+    PARODE_CUDA(cudaSetDevice(dev));
+    try {
+        std::lock_guard<std::mutex> g(g_mu);
+        setup_device_locked(dev);
+    } catch (...) {
+        cudaSetDevice(prev);
+        throw;
+    }
+    PARODE_CUDA(cudaSetDevice(prev));
+}
+
 }  // namespace parode
 
 extern "C" void ParODE_AffineScanDevice(const double* dPhi, const double* dGamma, const double* dX0, int ns,

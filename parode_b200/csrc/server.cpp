@@ -285,6 +285,7 @@ void Server::worker()
         f.bytes = j.bytes;
         f.t_admit = j.t_admit;
         f.t_start = now_s();
+        int setup_err = 0;
         try {
             std::vector<BatchSpec> specs;
             specs.reserve(j.reqs.size());
@@ -309,19 +310,21 @@ void Server::worker()
             PARODE_CUDA(cudaEventRecord(f.done, f.plan->stream()));
             f.t_ready = now_s();
         } catch (const Error& e) {
-            for (auto& r : j.reqs) r->err = e.code;
+            setup_err = e.code;
             f.plan.reset();
         } catch (...) {
-            for (auto& r : j.reqs) r->err = kDeviceError;
+            setup_err = kDeviceError;
             f.plan.reset();
         }
         lk.lock();
         --setting_up_;
         if (!f.plan) {
-            // failed set-up: finish the requests right away
+            // failed set-up: finish the requests right away (the error is
+            // published under the lock, as poll() reads it)
             inflight_bytes_ -= f.bytes;
             const double t = now_s();
             for (auto& r : f.reqs) {
+                r->err = setup_err != 0 ? setup_err : kDeviceError;
                 r->done = true;
                 r->t_done = t;
                 ++st_.failed;
@@ -355,8 +358,17 @@ void Server::retirer()
         retire_q_.pop_front();
         ++retiring_;
         lk.unlock();
-        retire(f, st);
+        std::vector<Outcome> out;
+        retire(f, st, out);
         lk.lock();
+        // publish under the lock: poll() and result() read these fields
+        for (size_t i = 0; i < f.reqs.size(); ++i) {
+            auto& r = f.reqs[i];
+            r->err = out[i].err;
+            r->dy = out[i].dy;
+            r->ny = out[i].ny;
+            r->t_done = out[i].t_done;
+        }
         if (opt_.log) {
             const double t = now_s(), z = t_first_;
             std::fprintf(stderr,
@@ -387,7 +399,7 @@ void Server::retirer()
 // Moves every request's outputs into a device buffer of its own (from the
 // stream-ordered pool; device to device), checks the batch's device status,
 // and frees the batch's arena.
-void Server::retire(Inflight& f, cudaStream_t st)
+void Server::retire(Inflight& f, cudaStream_t st, std::vector<Outcome>& out)
 {
     int err = 0;
     try {
@@ -395,33 +407,34 @@ void Server::retire(Inflight& f, cudaStream_t st)
     } catch (const Error& e) {
         err = e.code;
     }
+    out.assign(f.reqs.size(), Outcome());
     for (size_t i = 0; i < f.reqs.size(); ++i) {
-        auto& r = f.reqs[i];
-        r->err = err;
+        Outcome& o = out[i];
+        o.err = err;
         if (err == 0) {
-            r->ny = (size_t)f.plan->num_outputs((int)i) * f.plan->channels((int)i);
-            if (cudaMallocAsync(reinterpret_cast<void**>(&r->dy), sizeof(double) * std::max<size_t>(r->ny, 1), st) !=
+            o.ny = (size_t)f.plan->num_outputs((int)i) * f.plan->channels((int)i);
+            if (cudaMallocAsync(reinterpret_cast<void**>(&o.dy), sizeof(double) * std::max<size_t>(o.ny, 1), st) !=
                 cudaSuccess) {
                 cudaGetLastError();
-                r->dy = nullptr;
-                r->err = kNotEnoughResources;
-            } else if (cudaMemcpyAsync(r->dy, f.plan->device_output((int)i), sizeof(double) * r->ny,
+                o.dy = nullptr;
+                o.err = kNotEnoughResources;
+            } else if (cudaMemcpyAsync(o.dy, f.plan->device_output((int)i), sizeof(double) * o.ny,
                                        cudaMemcpyDeviceToDevice, st) != cudaSuccess) {
                 cudaGetLastError();
-                r->err = kDeviceError;
+                o.err = kDeviceError;
             }
         }
     }
     if (cudaStreamSynchronize(st) != cudaSuccess) {
         cudaGetLastError();
-        for (auto& r : f.reqs) r->err = kDeviceError;
+        for (auto& o : out) o.err = kDeviceError;
     }
     const double t = now_s();
-    for (auto& r : f.reqs) {
-        r->t_done = t;
-        if (r->err != 0 && r->dy) {
-            cudaFreeAsync(r->dy, st);
-            r->dy = nullptr;
+    for (auto& o : out) {
+        o.t_done = t;
+        if (o.err != 0 && o.dy) {
+            cudaFreeAsync(o.dy, st);
+            o.dy = nullptr;
         }
     }
     if (f.done) cudaEventDestroy(f.done);

@@ -104,7 +104,14 @@ private:
     void worker();
     void retirer();
     void admit_locked();
-    void retire(Inflight& f, cudaStream_t st);
+    // What retire() found for one request; published under mu_ by retirer().
+    struct Outcome {
+        int err = 0;
+        double* dy = nullptr;
+        size_t ny = 0;
+        double t_done = 0;
+    };
+    void retire(Inflight& f, cudaStream_t st, std::vector<Outcome>& out);
 
     int device_;
     InputRegistry* inputs_;

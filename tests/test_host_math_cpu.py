@@ -101,3 +101,80 @@ def test_abm_compact_rows_equal_the_full_map(maps):
     N = 4 * n
     assert np.array_equal(res["L"].reshape(n, N), res["PA"].reshape(N, N)[3 * n:])
     assert np.array_equal(res["BL"], res["BA"])
+
+
+TIME_DRIVER = r"""
+#include "host_math.h"
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <random>
+#include <vector>
+using namespace parode;
+// the reference's accumulation, one dependent step at a time
+// (Sources/GPUFixedStepIterative.cpp:141-146)
+static void plain(int solver, double t0, double tEnd, double h, double* tv)
+{
+    long ns = 0;
+    long nt = num_outputs(solver, t0, tEnd, h, &ns);
+    if (nt <= 0) return;
+    long pre = nt - ns;
+    double ts = solver == 1 ? t0 + 3.0 * h : t0;
+    for (long i = 0; i < pre; ++i) tv[i] = (double)(float)(ts - (double)(pre - i) * h);
+    float prev = (float)ts;
+    tv[pre] = prev;
+    for (long i = 1; i < ns; ++i) {
+        prev = (float)((double)prev + h);
+        tv[pre + i] = prev;
+    }
+}
+int main()
+{
+    std::mt19937_64 rng(7);
+    std::uniform_real_distribution<double> U(-1.0, 1.0);
+    std::vector<double> a, b;
+    int cases = 0, bad = 0;
+    const double hs[] = {1e-4, 1e-3, 0.1, 0.5, 1.0 / 3.0, 5e-4, 1e-5, 0.25, 0.7, 1e-7, 0.0625};
+    const double t0s[] = {0.0, 1.0, -1.0, -3.7, 100.0, 1e-3, -0.05, 12345.678, -100.0, 2.5, -0.5};
+    auto run = [&](int solver, double t0, double h, long T) {
+        const double t1 = t0 + (double)(T - 1) * h;
+        long nt = num_outputs(solver, t0, t1, h, nullptr);
+        if (nt <= 0) return;
+        a.assign(nt, 0.0);
+        b.assign(nt, 1.0);
+        plain(solver, t0, t1, h, a.data());
+        time_vector(solver, t0, t1, h, b.data());
+        ++cases;
+        if (std::memcmp(a.data(), b.data(), sizeof(double) * nt) != 0) {
+            ++bad;
+            std::printf("mismatch solver=%d t0=%.17g h=%.17g T=%ld\n", solver, t0, h, T);
+        }
+    };
+    for (double h : hs)
+        for (double t0 : t0s)
+            for (int solver = 0; solver < 2; ++solver) run(solver, t0, h, 300000);
+    for (int r = 0; r < 400; ++r) {
+        const double h = std::pow(10.0, -1.0 - 6.0 * std::fabs(U(rng)));
+        const double t0 = U(rng) * std::pow(10.0, 3.0 * U(rng));
+        run(r & 1, t0, h, 1 + (long)(rng() % 120000));
+    }
+    for (long T = 1; T < 40; ++T) run(0, 0.3, 0.1, T), run(1, -0.3, 0.1, T);
+    std::printf("cases %d bad %d\n", cases, bad);
+    return bad != 0;
+}
+"""
+
+
+def test_time_vector_is_the_reference_accumulation(tmp_path):
+    """The fast time vector equals the reference's float accumulation bit for bit."""
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("g++ not available")
+    drv = tmp_path / "tv.cpp"
+    drv.write_text(TIME_DRIVER)
+    exe = tmp_path / "tv"
+    subprocess.run([gxx, "-O3", "-std=c++17", "-I", CSRC, str(drv), os.path.join(CSRC, "host_math.cpp"), "-o",
+                    str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert out.returncode == 0, out.stdout[-2000:]
+    assert "bad 0" in out.stdout

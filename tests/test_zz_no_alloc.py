@@ -84,6 +84,57 @@ def test_forced_matches_recurrence(pb, n, T):
         assert oracle.rel_err(X, ref) <= TOL
 
 
+def test_no_initial_state_starts_from_zero(pb):
+    """dX0 = NULL: the recurrence starts from x_0 = 0."""
+    torch = pytest.importorskip("torch")
+    n, T = 16, 5000
+    A, _, rng = _system(n, 41)
+    phi, _ = oracle.discretise(oracle.RK4, A, None, 1e-3)
+    gamma = rng.standard_normal((T, n))
+    ref = np.empty((T, n))
+    x = np.zeros(n)
+    for k in range(T):
+        ref[k] = x
+        x = phi @ x + gamma[k]
+    dev = torch.device("cuda", 0)
+    d_phi = torch.from_numpy(phi).to(dev)
+    d_gamma = torch.from_numpy(gamma).to(dev)
+    d_x = torch.full((T, n), float("nan"), dtype=torch.float64, device=dev)
+    err = C.c_int(1)
+    _entry(pb)(d_phi.data_ptr(), d_gamma.data_ptr(), None, n, T, d_x.data_ptr(),
+               torch.cuda.current_stream(dev).cuda_stream, C.byref(err))
+    torch.cuda.synchronize()
+    assert err.value == 0
+    assert oracle.rel_err(d_x.cpu().numpy(), ref) <= TOL
+
+
+def test_calls_map_no_device_memory(pb):
+    """After the first call, further calls leave the device's free memory unchanged."""
+    torch = pytest.importorskip("torch")
+    n, T = 64, 20000
+    A, x0, rng = _system(n, 53)
+    phi, _ = oracle.discretise(oracle.RK4, A, None, 1e-3)
+    gamma = 1e-2 * rng.standard_normal((T, n))
+    dev = torch.device("cuda", 0)
+    d_phi = torch.from_numpy(phi).to(dev)
+    d_gamma = torch.from_numpy(gamma).to(dev)
+    d_x0 = torch.from_numpy(x0).to(dev)
+    d_x = torch.empty((T, n), dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    err = C.c_int(1)
+    f = _entry(pb)
+    f(d_phi.data_ptr(), d_gamma.data_ptr(), d_x0.data_ptr(), n, T, d_x.data_ptr(), stream, C.byref(err))
+    torch.cuda.synchronize()
+    assert err.value == 0
+    free0, _ = torch.cuda.mem_get_info(dev)
+    for _ in range(3):
+        f(d_phi.data_ptr(), d_gamma.data_ptr(), d_x0.data_ptr(), n, T, d_x.data_ptr(), stream, C.byref(err))
+        assert err.value == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(dev)
+    assert free1 == free0
+
+
 def test_rejects_beyond_scratch_and_bad_dimension(pb):
     torch = pytest.importorskip("torch")
     phi = np.eye(64) * 0.5
