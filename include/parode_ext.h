@@ -38,6 +38,21 @@ extern "C" {
                                       its block size against the FP64 build of its tables spread over that
                                       many solves (SimulateODE and the server always use 1) */
 
+/* Test hooks, host side only (nothing faults on the device):
+ *   PARODE_OPT_FAULT_ALLOC   k >= 0: the k-th device allocation of a solve,
+ *                            batch or server from now on (0 = the next) fails
+ *                            as if the device were out of memory; the call
+ *                            reports -4 and later calls allocate normally.
+ *                            -1 (default) disables it.
+ *   PARODE_OPT_FAULT_WITHHOLD non-zero: the mixed-precision response solve's
+ *                            tensor-core kernel withholds one arrive of its
+ *                            first pipeline stage in its first CTA, so that
+ *                            the waits on it give up after their bound (about
+ *                            a second); the solve then reports -10
+ *                            (DeviceError) and the device stays usable. */
+#define PARODE_OPT_FAULT_ALLOC    5
+#define PARODE_OPT_FAULT_WITHHOLD 6
+
 void ParODE_SetOption(int option, long long value, int nErr[]);
 long long ParODE_GetOption(int option, int nErr[]);
 

@@ -602,25 +602,15 @@ static float wg_dot(const float* row, const float* v, int len, int lanes, float*
     return part[0];
 }
 
-int po_simulate_refscan_f32(const po_system* s, const po_input* in, int solver,
-                            double t0, double tEnd, double h, long batch, float* y, long* n_out)
+void po_ref_discretise_f32(const po_system* s, int solver, double h, float* Phi, float* Bb)
 {
-    if (s->n <= 0) return -6;
-    if (solver != PO_RK4 && solver != PO_ABM) return -7;
-    long ns = 0;
-    long nt = po_num_outputs(solver, t0, tEnd, h, &ns);
-    if (nt <= 0) return -6;
-    if (n_out) *n_out = nt;
-    int n = s->n, m = s->zeroB ? 0 : s->m, mu = s->m, p = po_output_size(s);
+    /* float discretisation: uBLAS prod() in float, linear combinations
+     * evaluated in double (double scalars) and stored to float
+     * (Sources/RungeKutta4thOrder.cpp:36-70, Sources/AdamsMoulton.cpp:238-316). */
+    int n = s->n, m = s->zeroB ? 0 : s->m;
     int N = (solver == PO_ABM) ? 4 * n : n;
-    int W = (solver == PO_ABM) ? 5 : 3;
     fcopy fc;
     make_fcopy(s, &fc);
-
-    /* float discretisation: uBLAS prod() in float, linear combinations
-     * evaluated in double (double scalars) and stored to float. */
-    float* Phi = falloc((long)N * N);
-    float* Bb = falloc((long)n * W * (m > 0 ? m : 1));
     {
         long nn = (long)n * n, nm = (long)n * (m > 0 ? m : 1);
         float *A2 = falloc(nn), *A3 = falloc(nn), *A4 = falloc(nn);
@@ -674,6 +664,61 @@ int po_simulate_refscan_f32(const po_system* s, const po_input* in, int solver,
         }
         free(A2); free(A3); free(A4); free(AB); free(A2B); free(A3B);
     }
+    free_fcopy(&fc);
+}
+
+void po_ref_abm_startup_f32(const po_system* s, double h, const float* U9, float* X0, float* ypre)
+{
+    /* x1..x3 by three float RK4 steps with the inputs U9 = u(t0 + j h/2),
+     * j = 0..8 (Sources/AdamsMoulton.cpp:29-104); X0 = [x0; x1; x2; x3];
+     * outputs 0..2 with float accumulation (Sources/GPUFixedStepIterative.cpp:155-171). */
+    int n = s->n, m = s->zeroB ? 0 : s->m, mu = s->m, p = po_output_size(s);
+    fcopy fc;
+    make_fcopy(s, &fc);
+    float *x = falloc(n), *work = falloc(5L * n);
+    for (int r = 0; r < n; ++r) X0[r] = x[r] = (float)s->x0[r];
+    for (int st = 1; st < 4; ++st) {
+        int j = 2 * (st - 1);
+        rk4_step_f(n, m, fc.Af, fc.Bf, s->zeroB, x, U9 + (long)j * mu, U9 + (long)(j + 1) * mu,
+                   U9 + (long)(j + 2) * mu, h, work);
+        for (int r = 0; r < n; ++r) X0[(long)st * n + r] = x[r];
+    }
+    for (int i = 0; i < 3; ++i) {
+        if (s->zeroC && s->zeroD) {
+            for (int r = 0; r < p; ++r) ypre[(long)i * p + r] = X0[(long)i * n + r];
+        } else {
+            for (int r = 0; r < p; ++r) {
+                float v = 0.0f;
+                if (!s->zeroC)
+                    for (int c = 0; c < n; ++c) v += fc.Cf[(long)r * n + c] * X0[(long)i * n + c];
+                if (!s->zeroD)
+                    for (int c = 0; c < mu; ++c) v += fc.Df[(long)r * mu + c] * U9[(long)(2 * i) * mu + c];
+                ypre[(long)i * p + r] = v;
+            }
+        }
+    }
+    free(x); free(work);
+    free_fcopy(&fc);
+}
+
+int po_simulate_refscan_f32(const po_system* s, const po_input* in, int solver,
+                            double t0, double tEnd, double h, long batch, float* y, long* n_out)
+{
+    if (s->n <= 0) return -6;
+    if (solver != PO_RK4 && solver != PO_ABM) return -7;
+    long ns = 0;
+    long nt = po_num_outputs(solver, t0, tEnd, h, &ns);
+    if (nt <= 0) return -6;
+    if (n_out) *n_out = nt;
+    int n = s->n, m = s->zeroB ? 0 : s->m, mu = s->m, p = po_output_size(s);
+    int N = (solver == PO_ABM) ? 4 * n : n;
+    int W = (solver == PO_ABM) ? 5 : 3;
+    fcopy fc;
+    make_fcopy(s, &fc);
+
+    float* Phi = falloc((long)N * N);
+    float* Bb = falloc((long)n * W * (m > 0 ? m : 1));
+    po_ref_discretise_f32(s, solver, h, Phi, Bb);
 
     /* Work-group column widths: next power of two >= 3 m for RK4
      * (Sources/RungeKutta4thOrder.cpp:85), >= 4n for ABM
@@ -694,31 +739,9 @@ int po_simulate_refscan_f32(const po_system* s, const po_input* in, int solver,
         float* U9 = falloc(9L * (mu + 1));
         for (int j = 0; j < 9; ++j)
             for (int i = 0; i < mu; ++i) U9[(long)j * mu + i] = (float)eval_u(in, (double)(tsf + dtf * (float)j), i);
-        float *x = falloc(n), *work = falloc(5L * n);
-        for (int r = 0; r < n; ++r) X0[r] = x[r] = (float)s->x0[r];
-        for (int st = 1; st < 4; ++st) {
-            int j = 2 * (st - 1);
-            rk4_step_f(n, m, fc.Af, fc.Bf, s->zeroB, x, U9 + (long)j * mu, U9 + (long)(j + 1) * mu,
-                       U9 + (long)(j + 2) * mu, h, work);
-            for (int r = 0; r < n; ++r) X0[(long)st * n + r] = x[r];
-        }
+        po_ref_abm_startup_f32(s, h, U9, X0, y);
         pre = 3;
-        for (int i = 0; i < 3; ++i) {
-            /* Sources/GPUFixedStepIterative.cpp:155-171, float accumulation */
-            if (s->zeroC && s->zeroD) {
-                for (int r = 0; r < p; ++r) y[(long)i * p + r] = X0[(long)i * n + r];
-            } else {
-                for (int r = 0; r < p; ++r) {
-                    float v = 0.0f;
-                    if (!s->zeroC)
-                        for (int c = 0; c < n; ++c) v += fc.Cf[(long)r * n + c] * X0[(long)i * n + c];
-                    if (!s->zeroD)
-                        for (int c = 0; c < mu; ++c) v += fc.Df[(long)r * mu + c] * U9[(long)(2 * i) * mu + c];
-                    y[(long)i * p + r] = v;
-                }
-            }
-        }
-        free(U9); free(x); free(work);
+        free(U9);
     }
 
     long NSB = batch > 0 ? batch : next_pow2(ns);

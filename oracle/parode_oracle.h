@@ -132,6 +132,16 @@ int po_simulate_refscan_f32(const po_system* s, const po_input* in, int solver,
  * max_k |y - yref| / max_k |yref|; returns the maximum over channels. */
 double po_rel_err(const double* y, const double* yref, long T, int p);
 
+/* The float host-side set-up of the reference's solvers, shared by O3 and
+ * the harness that runs the reference's own OpenCL kernels (ref_kernels.c):
+ * Phi (N x N) and Bbar (n x W m) as uBLAS forms them in float
+ * (Sources/RungeKutta4thOrder.cpp:36-70, Sources/AdamsMoulton.cpp:238-316),
+ * and the ABM start-up from the nine input samples U9 = u(t0 + j h/2),
+ * j = 0..8 (Sources/AdamsMoulton.cpp:29-116): X0 = [x0; x1; x2; x3] and the
+ * outputs 0..2 (Sources/GPUFixedStepIterative.cpp:155-171). */
+void po_ref_discretise_f32(const po_system* s, int solver, double h, float* Phi, float* Bbar);
+void po_ref_abm_startup_f32(const po_system* s, double h, const float* U9, float* X0, float* ypre);
+
 /* Thread-parallel O1 over independent systems (OpenMP when compiled with it). */
 int po_threads(void);
 

@@ -36,6 +36,8 @@ OPT_PRECISION = 1
 OPT_PATH = 2
 OPT_LOG = 3
 OPT_EXECUTIONS = 4
+OPT_FAULT_ALLOC = 5      # test hook: the k-th device allocation from now fails (-1: off)
+OPT_FAULT_WITHHOLD = 6   # test hook: the mixed response kernel withholds one arrive (bounded waits give up)
 
 PATH_AUTO = 0
 PATH_LEVEL = 1

@@ -18,6 +18,7 @@
 #include "ParODECInterface.h"
 #include "parode_ext.h"
 
+#include <atomic>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -29,6 +30,20 @@
 #include <vector>
 
 using namespace parode;
+
+namespace {
+// PARODE_OPT_FAULT_ALLOC: allocations left before the injected failure (-1: none)
+std::atomic<long long> g_fault_alloc{-1};
+}  // namespace
+
+bool parode::fault_alloc_now()
+{
+    long long v = g_fault_alloc.load();
+    while (v >= 0) {
+        if (g_fault_alloc.compare_exchange_weak(v, v - 1)) return v == 0;
+    }
+    return false;
+}
 
 namespace {
 
@@ -44,6 +59,7 @@ struct Library {
     int path = kPathAuto;
     int log = 0;
     long long executions = 1;  // PARODE_OPT_EXECUTIONS: plans and batches
+    int fault_withhold = 0;    // PARODE_OPT_FAULT_WITHHOLD (test hook)
     cudaEvent_t t_start = nullptr, t_stop = nullptr;
     bool timer_running = false;
 
@@ -401,6 +417,11 @@ void ParODE_SetOption(int option, long long value, int nErr[])
         if (value < 1) rc = kInvalidArgument;
         else L.executions = value;
         break;
+    case PARODE_OPT_FAULT_ALLOC:
+        if (value < -1) rc = kInvalidArgument;
+        else g_fault_alloc.store(value);
+        break;
+    case PARODE_OPT_FAULT_WITHHOLD: L.fault_withhold = value != 0; break;
     default: rc = kInvalidArgument;
     }
     if (nErr) nErr[0] = rc;
@@ -416,6 +437,8 @@ long long ParODE_GetOption(int option, int nErr[])
     case PARODE_OPT_PATH: return L.path;
     case PARODE_OPT_LOG: return L.log;
     case PARODE_OPT_EXECUTIONS: return L.executions;
+    case PARODE_OPT_FAULT_ALLOC: return g_fault_alloc.load();
+    case PARODE_OPT_FAULT_WITHHOLD: return L.fault_withhold;
     default:
         if (nErr) nErr[0] = kInvalidArgument;
         return -1;
@@ -459,6 +482,7 @@ void ParODE_SimulateODE_d(const double* A, const double* B, const double* C, con
         opt.precision = precision;
         opt.path = L.path;
         opt.input_double = true;
+        opt.fault_withhold = L.fault_withhold;
         Plan plan(dev, s, &L.inputs, uIndex, solver, tStart, tEnd, tStep, opt);
         // the host time vector is built on a helper thread while the plan
         // is set up, solved and its outputs copied
@@ -494,6 +518,7 @@ ParODE_Plan* ParODE_PlanCreate(const double* A, const double* B, const double* C
         opt.path = L.path;
         opt.input_double = true;
         opt.executions = (double)L.executions;
+        opt.fault_withhold = L.fault_withhold;
         auto h = std::make_unique<ParODE_Plan>();
         h->plan = std::make_unique<Plan>(dev, s, &L.inputs, uIndex, solver, tStart, tEnd, tStep, opt);
         out = h.release();

@@ -461,6 +461,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         // stream-ordered: creating or destroying a batch does not synchronise
         // the device, so batches can come and go while others run
         PARODE_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+        if (fault_alloc_now()) throw Error(kNotEnoughResources, "batch arena allocation failed (injected)");
         cudaError_t e = cudaMallocAsync(&arena_, arena_bytes_, stream_);
         if (e != cudaSuccess) {
             cudaGetLastError();

@@ -42,6 +42,11 @@ struct Error : std::runtime_error {
         }                                                                                          \
     } while (0)
 
+// Host-side fault injection for tests (PARODE_OPT_FAULT_ALLOC): true when the
+// device allocation being made now is the one set to fail.  Every allocation
+// site of the solve paths asks before allocating.
+bool fault_alloc_now();
+
 enum Solver : int { kRK4 = 0, kABM = 1 };
 enum Precision : int { kFP64 = 0, kMixed = 1 };
 

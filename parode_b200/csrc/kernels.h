@@ -50,6 +50,9 @@ struct LevelArgs {
     // Tiled kernel: columns g >= src_cols (> 0) read a zero source, so their
     // results are acc or 0 (a zero padding written by the same launch).
     long src_cols = 0;
+    // Tensor-core kernel, test hook: non-zero makes CTA 0 withhold the
+    // arrive of its first K slice, so the waits on that stage give up.
+    int fault_withhold = 0;
 };
 
 __host__ __device__ inline int level_rows(const LevelArgs& a) { return a.M > 0 ? a.M : a.Np; }

@@ -293,7 +293,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
                 // Only the M-tile's valid rows of A travel (8-row core-matrix
                 // groups, hi and lo): the MMA's other rows read whatever the
                 // stage held, and their results are never stored.
-                if (lane == 0) {
+                // test hook: CTA 0 issues nothing for its first slice, so that
+                // stage's waits run into their bound (no copy is in flight)
+                const bool withhold = a.fault_withhold && blockIdx.x == 0 && j == 0;
+                if (lane == 0 && !withhold) {
                     const int sr = rotated_slice(lt, s, nk);
                     const int rowsv = level_rows(a) - m0 < kBM ? level_rows(a) - m0 : kBM;
                     const uint32_t abytes = (uint32_t)((rowsv + 7) / 8) * (uint32_t)(kBK * 32);

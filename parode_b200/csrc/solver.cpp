@@ -317,6 +317,7 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
             w.dst_limit = nScan_ * (long)p_;
             if (!level_tc_supported(a) || !level_tc_supported(w))
                 throw Error(kDeviceError, "response GEMMs not supported by the tensor-core kernel");
+            a.fault_withhold = opt.fault_withhold ? 1 : 0;
             const size_t sa = gemm_split_bytes(a.M, a.K), sw = gemm_split_bytes(w.M, w.K);
             double* ps = nullptr;
             alloc(&ps, (long)((sa + sw) / 8));
@@ -404,6 +405,7 @@ void Plan::alloc(double** p, long n)
     // one) reuse the pool's memory instead of mapping and unmapping it
     *p = nullptr;
     const size_t bytes = sizeof(double) * (size_t)std::max<long>(n, 1);
+    if (fault_alloc_now()) throw Error(kNotEnoughResources, "device allocation failed (injected)");
     cudaError_t e = cudaMallocAsync((void**)p, bytes, stream_);
     if (e != cudaSuccess) {
         cudaGetLastError();

@@ -35,6 +35,9 @@ struct PlanOptions {
     // weighs the FP64 build of its tables against the work of that many
     // solves (1: one-shot, as SimulateODE and the server)
     double executions = 1.0;
+    // test hook (PARODE_OPT_FAULT_WITHHOLD): the mixed response kernel's
+    // first CTA withholds one pipeline arrive, so its bounded waits give up
+    bool fault_withhold = false;
 };
 
 class Plan {

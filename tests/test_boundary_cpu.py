@@ -83,6 +83,21 @@ def test_executions_option_round_trip():
     pb.set_option(pb.OPT_EXECUTIONS, 1)
 
 
+def test_fault_injection_options_round_trip():
+    import parode_b200 as pb
+
+    assert pb.get_option(pb.OPT_FAULT_ALLOC) == -1
+    pb.set_option(pb.OPT_FAULT_ALLOC, 3)
+    assert pb.get_option(pb.OPT_FAULT_ALLOC) == 3
+    with pytest.raises(pb.ParODEError):
+        pb.set_option(pb.OPT_FAULT_ALLOC, -2)
+    pb.set_option(pb.OPT_FAULT_ALLOC, -1)
+    assert pb.get_option(pb.OPT_FAULT_WITHHOLD) == 0
+    pb.set_option(pb.OPT_FAULT_WITHHOLD, 1)
+    assert pb.get_option(pb.OPT_FAULT_WITHHOLD) == 1
+    pb.set_option(pb.OPT_FAULT_WITHHOLD, 0)
+
+
 def test_not_initialised_errors():
     import parode_b200 as pb
 
