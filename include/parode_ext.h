@@ -29,7 +29,9 @@ extern "C" {
 #define PARODE_OPT_PRECISION    1  /* PARODE_PRECISION_* used by SimulateODE (default FP64) */
 #define PARODE_OPT_PATH         2  /* 0 auto, 1 level-synchronous sweeps, 2 blocked (leaf chosen by cost),
                                       3 blocked with the block-response GEMM leaf (FP64, inputs present),
-                                      4 blocked with the in-block sweep leaf */
+                                      4 blocked with the in-block sweep leaf, 5 the general scan (the
+                                      reference's pipeline: T copies of Phi composed pair by pair,
+                                      scan dimensions up to 64) */
 #define PARODE_OPT_LOG          3  /* non-zero: one line per solve or batch set-up on stderr; a server logs
                                       each batch's timeline (1), and its set-up phases too (2, which waits on
                                       the device between phases) */
@@ -208,6 +210,23 @@ void ParODE_ServerDestroy(ParODE_Server* srv);
  * The scratch is shared: calls that overlap on the GPU race on it. */
 void ParODE_AffineScanDevice(const double* dPhi, const double* dGamma, const double* dX0, int ns,
                              long long count, double* dX, void* stream, int nErr[]);
+
+/* General affine scan over per-step maps on device data: x_0 = dX0 (NULL:
+ * zero), x_{k+1} = dM[k] x_k + dV[k] (dV NULL: zero), dX[k] = x_k for
+ * k < count; dM count x ns x ns, dV and dX count x ns, row-major FP64, device
+ * memory of the current device; ns in [1, 64].  Every pair of every up-sweep
+ * level is composed, matrices and vectors, as the reference's MM / MVV scan
+ * kernels do (Kernels/MMKernelScanUpsweep.cl:13-56,
+ * Kernels/MVVKernelScanUpsweep.cl:14-50, MVVKernelScanDownsweep.cl:14-50), so
+ * the maps may differ from step to step (a time-varying system).  precision:
+ * PARODE_PRECISION_FP64 (FP64 tensor cores) or PARODE_PRECISION_MIXED (the
+ * matrix products in 3xTF32 on tcgen05 for ns in 17..64, the vectors in FP64).
+ * Enqueued on `stream` (NULL: the legacy default stream); returns once the
+ * scan is done.  Scratch (count rounded up to a power of two, times
+ * ns^2 + ns doubles with ns rounded up to 8, 16, 32 or 64) comes from the
+ * device's stream-ordered pool. */
+void ParODE_AffineScanGeneral(const double* dM, const double* dV, const double* dX0, int ns, long long count,
+                              int precision, double* dX, void* stream, int nErr[]);
 
 #ifdef __cplusplus
 }

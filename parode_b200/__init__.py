@@ -44,6 +44,7 @@ PATH_LEVEL = 1
 PATH_BLOCKED = 2
 PATH_BLOCKED_RESPONSE = 3
 PATH_BLOCKED_SWEEP = 4
+PATH_GENERAL = 5
 
 ERRORS = {
     0: "OK", -1: "NoGPU", -2: "NotInitialized", -3: "CouldNotCreateGPUKernels", -4: "NotEnoughResources",
@@ -133,6 +134,12 @@ def _load():
     L.ParODE_ServerResult.argtypes = [C.c_void_p, C.c_longlong, dp, dp, dp, ip]
     L.ParODE_ServerStats.argtypes = [C.c_void_p, dp, ip]
     L.ParODE_ServerDestroy.argtypes = [C.c_void_p]
+    L.ParODE_AffineScanDevice.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_void_p,
+                                          C.c_void_p, ip]
+    L.ParODE_AffineScanDevice.restype = None
+    L.ParODE_AffineScanGeneral.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_int,
+                                           C.c_void_p, C.c_void_p, ip]
+    L.ParODE_AffineScanGeneral.restype = None
     return L
 
 
@@ -268,6 +275,18 @@ def simulate(A, B, Cm, D, x0, u_index: int, t0: float, t_end: float, h: float, s
                              C.byref(ns), C.byref(e))
     _check(e, "ParODE_SimulateODE_d")
     return t[:ns.value], y[:ns.value]
+
+
+def affine_scan_general(M_ptr: int, V_ptr: int, x0_ptr: int, ns: int, count: int, X_ptr: int,
+                        precision: int = FP64, stream: int = 0) -> None:
+    """ParODE_AffineScanGeneral on device pointers (e.g. torch CUDA tensors'
+    data_ptr()): X[k] = x_k, x_{k+1} = M[k] x_k + V[k], x_0 = x0 (0 pointers:
+    zero), all row-major FP64.  Returns when the scan is done."""
+    e = C.c_int(0)
+    lib.ParODE_AffineScanGeneral(C.c_void_p(M_ptr or None), C.c_void_p(V_ptr or None), C.c_void_p(x0_ptr or None),
+                                 ns, count, precision, C.c_void_p(X_ptr or None), C.c_void_p(stream or None),
+                                 C.byref(e))
+    _check(e, "ParODE_AffineScanGeneral")
 
 
 def simulate_f32(A, B, Cm, D, x0, u_index: int, t0: float, t_end: float, h: float, solver: int = RK4):

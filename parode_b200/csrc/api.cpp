@@ -12,6 +12,7 @@
 #include "solver.h"
 #include "batch.h"
 #include "blocked.h"
+#include "general.h"
 #include "server.h"
 
 #include "FTypeDef.h"
@@ -409,7 +410,7 @@ void ParODE_SetOption(int option, long long value, int nErr[])
         else L.precision = (int)value;
         break;
     case PARODE_OPT_PATH:
-        if (value < 0 || value > 4) rc = kInvalidArgument;
+        if (value < 0 || value > 5) rc = kInvalidArgument;
         else L.path = (int)value;
         break;
     case PARODE_OPT_LOG: L.log = (int)value; break;
@@ -822,6 +823,36 @@ void ParODE_SimulateODEBatch(int nSystems, const double* const A[], const double
     }
     ParODE_BatchDestroy(b);
     if (nErr) nErr[0] = err;
+}
+
+
+void ParODE_AffineScanGeneral(const double* dM, const double* dV, const double* dX0, int ns, long long count,
+                              int precision, double* dX, void* stream, int nErr[])
+{
+    int rc = guarded([&] {
+        if (precision != PARODE_PRECISION_FP64 && precision != PARODE_PRECISION_MIXED)
+            throw Error(kInvalidArgument, "unknown precision");
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        int* status = nullptr;
+        if (fault_alloc_now()) throw Error(kNotEnoughResources, "device allocation failed (injected)");
+        if (cudaMallocAsync(reinterpret_cast<void**>(&status), sizeof(int), s) != cudaSuccess) {
+            cudaGetLastError();
+            throw Error(kNotEnoughResources, "device allocation failed");
+        }
+        int host_status = 0;
+        try {
+            PARODE_CUDA(cudaMemsetAsync(status, 0, sizeof(int), s));
+            general_scan(dM, dV, dX0, ns, (long)count, precision, dX, status, s);
+            PARODE_CUDA(cudaMemcpyAsync(&host_status, status, sizeof(int), cudaMemcpyDeviceToHost, s));
+            PARODE_CUDA(cudaStreamSynchronize(s));
+        } catch (...) {
+            cudaFreeAsync(status, s);
+            throw;
+        }
+        PARODE_CUDA(cudaFreeAsync(status, s));
+        if (host_status != 0) throw Error(kDeviceError, "a device-side wait gave up (tensor-core completion not observed)");
+    });
+    if (nErr) nErr[0] = rc;
 }
 
 }  // extern "C"

@@ -3,6 +3,7 @@
 
 #include "batch.h"
 #include "common.h"
+#include "general.h"
 #include "kernels.h"
 
 #include <algorithm>
@@ -36,6 +37,8 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
     Ns_ = solver == kRK4 ? sys.n : 4 * sys.n;
     Np_ = (int)round_up(Ns_, 8);
     if (Np_ > 1024) throw Error(kInvalidSystem, "scan dimension above 1024 is not supported");
+    if (opt.path == kPathGeneral && Ns_ > 64)
+        throw Error(kInvalidArgument, "the general scan supports scan dimensions up to 64");
     if (Ns_ > 64 && opt.path != kPathBlocked && opt.path != kPathBlockedSweep) {
         // scan dimensions above 64: the batch engine's one-system form (the
         // response leaf or the level-synchronous scan, tensor-core levels in
@@ -61,7 +64,13 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
     Tp_ = next_pow2(nScan_);
     levels_ = ilog2(Tp_);
     path_ = kPathLevel;
-    {
+    if (opt.path == kPathGeneral) {
+        path_ = kPathGeneral;
+        Np_ = general_padded_dim(Ns_);
+        precision_used_ = (opt.precision == kMixed && compose_tc_supported(Np_)) ? kMixed : kFP64;
+        const double bytes = (double)nScan_ * Np_ * Np_ * 8.0 + (double)general_scan_bytes(Np_, nScan_);
+        if (bytes > 24e9) throw Error(kNotEnoughResources, "the general scan holds a copy of Phi per step");
+    } else {
         const bool can_block = blocked_shape(Ns_, mu_, solver, &shape_);
         if (opt.path >= kPathBlocked && !can_block)
             throw Error(kInvalidArgument, "the blocked path supports scan dimensions up to 64");
@@ -172,8 +181,12 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
         dStatus_ = reinterpret_cast<int*>(st);
         PARODE_CUDA(cudaMemsetAsync(dStatus_, 0, sizeof(int), stream_));
     }
-    if (path_ == kPathLevel) {
+    if (path_ == kPathLevel || path_ == kPathGeneral) {
         alloc(&dV_, (Tp_ + 1) * (long)Np_);  // a leading slot holds the initial state
+        if (path_ == kPathGeneral) {
+            alloc(&dMs_, nScan_ * (long)Np_ * Np_);
+            alloc(&dXs_, nScan_ * (long)Np_);
+        }
     } else {
         alloc(&dG_, nblocks_ * (long)Np_);
         alloc(&dWork_, std::max(blocked_items_scratch(shape_, nblocks_), chunk_carry_scratch(nblocks_) + 1) * (long)Np_);
@@ -488,6 +501,10 @@ void Plan::execute_body(double* y, cudaStream_t s)
         execute_blocked(y ? y : dY_, s);
         return;
     }
+    if (path_ == kPathGeneral) {
+        execute_general(y ? y : dY_, s);
+        return;
+    }
     double* Y = y ? y : dY_;
     const long Np = Np_;
     const int n = sys_.n;
@@ -574,6 +591,39 @@ void Plan::execute_body(double* y, cudaStream_t s)
         launch_output(Y, dV_, Np_, 0, n, mu_, p_, dC_, dD_, sys_.zeroC, sys_.zeroD, dU_, 2, 0, nScan_, 0, s);
     } else {
         launch_output(Y, dV_, Np_, 3 * n, n, mu_, p_, dC_, dD_, sys_.zeroC, sys_.zeroD, dU_, 1, 3, nScan_, 3, s);
+        PARODE_CUDA(cudaMemcpyAsync(Y, dYpre_, sizeof(double) * 3 * p_, cudaMemcpyDeviceToDevice, s));
+    }
+    ++launches;
+    mark("output", s);
+    launches_ = launches;
+    last_y_ = Y;
+}
+
+void Plan::execute_general(double* Y, cudaStream_t s)
+{
+    // the reference's pipeline (Sources/RungeKutta4thOrder.cpp:234-288,
+    // Sources/AdamsMoulton.cpp:403-461, Sources/GPUFixedStepIterative.cpp:236-446):
+    // a copy of Phi per step (DistributeA), the forcing vectors, the scan
+    // composing every pair (matrices and vectors), the outputs
+    int launches = 0;
+    marks_.clear();
+    mark("start", s);
+    fill_inputs(s);
+    launches += mu_ > 0 ? 1 : 0;
+    mark("inputs", s);
+    double* V1 = dV_ + Np_;
+    launch_forcing(V1, Np_, sys_.n, sys_.zeroB ? 0 : sys_.m, solver_, dBbar_, dU_, nScan_, Tp_, s);
+    launch_distribute(dMs_, dPow_, Np_, nScan_, sms_, s);
+    launches += 2;
+    mark("maps", s);
+    general_scan(dMs_, V1, dX0_, Np_, nScan_, precision_used_, dXs_, dStatus_, s);
+    launches += 2 * ilog2(Tp_) + 2;
+    mark("scan", s);
+    if (solver_ == kRK4) {
+        launch_output(Y, dXs_, Np_, 0, sys_.n, mu_, p_, dC_, dD_, sys_.zeroC, sys_.zeroD, dU_, 2, 0, nScan_, 0, s);
+    } else {
+        launch_output(Y, dXs_, Np_, 3 * sys_.n, sys_.n, mu_, p_, dC_, dD_, sys_.zeroC, sys_.zeroD, dU_, 1, 3,
+                      nScan_, 3, s);
         PARODE_CUDA(cudaMemcpyAsync(Y, dYpre_, sizeof(double) * 3 * p_, cudaMemcpyDeviceToDevice, s));
     }
     ++launches;

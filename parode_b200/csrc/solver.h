@@ -24,7 +24,16 @@ class BatchPlan;
 
 // kPathBlocked chooses the leaf by cost; kPathBlockedResponse / kPathBlockedSweep
 // force the block-response GEMM leaf / the in-block sweep leaf.
-enum Path : int { kPathAuto = 0, kPathLevel = 1, kPathBlocked = 2, kPathBlockedResponse = 3, kPathBlockedSweep = 4 };
+// kPathGeneral runs the reference's pipeline step for step: T copies of Phi,
+// the forcing vectors, the general scan composing every pair (general.h).
+enum Path : int {
+    kPathAuto = 0,
+    kPathLevel = 1,
+    kPathBlocked = 2,
+    kPathBlockedResponse = 3,
+    kPathBlockedSweep = 4,
+    kPathGeneral = 5
+};
 
 struct PlanOptions {
     int precision = 0;  // Precision
@@ -84,6 +93,7 @@ private:
     void execute_body(double* y, cudaStream_t s);
     void execute_blocked(double* Y, cudaStream_t s);
     void execute_response(double* Y, cudaStream_t s);
+    void execute_general(double* Y, cudaStream_t s);
     void fill_inputs(cudaStream_t s);
 
     int device_ = 0;
@@ -114,6 +124,8 @@ private:
     bool br_ = false;           // leaf = block response GEMM (kernels_br.cu)
     int brK_ = 0, brKpad_ = 0;  // window columns (padded to even)
     double* dW_ = nullptr;      // response matrix, (B p + NP) x (brKpad_ + NP)
+    double* dMs_ = nullptr;     // general path: T copies of Phi (Ns x Ns each)
+    double* dXs_ = nullptr;     // general path: the states x_k (T x Ns)
     // mixed form of the response leaf: aggregates and output windows on the
     // tensor cores (one grouped launch of two GEMMs), state part in FP64
     bool br_tc_ = false;
