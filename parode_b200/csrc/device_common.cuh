@@ -31,6 +31,35 @@ __device__ __forceinline__ double sinusoid_value(const double* a, const double* 
     return v;
 }
 
+// Where a sampler puts sample j of its run: FP64 at out[j * stride], or
+// split into two TF32 planes (hi = TF32(x), lo = TF32(x - hi) with
+// x = float(v), both rounded to nearest) for the tensor-core GEMMs.
+struct SampleOut64 {
+    double* out;
+    long stride;
+    __device__ __forceinline__ void operator()(long j, double v) const { out[j * stride] = v; }
+};
+
+__device__ __forceinline__ float tf32_rna(float x)
+{
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+struct SampleOutSplit {
+    float* hi;
+    float* lo;
+    long stride;
+    __device__ __forceinline__ void operator()(long j, double v) const
+    {
+        const float x = (float)v;
+        const float h = tf32_rna(x);
+        hi[j * stride] = h;
+        lo[j * stride] = tf32_rna(x - h);
+    }
+};
+
 // Sample time t_j = base + dt * j, rounded as the host computes it.
 __device__ __forceinline__ double sample_time(double base, double dt, long j)
 {
@@ -54,9 +83,9 @@ __device__ __forceinline__ double sample_time(double base, double dt, long j)
 // side by side as independent chains and are summed in sinusoid_value's
 // order; inputs with more than 4 terms per channel take sinusoid_value per
 // sample.
-template <int L, int KT>
+template <int L, int KT, class Out>
 __device__ __forceinline__ void sinusoid_run_terms(const double* a, const double* f, const double* phi, int i,
-                                                   double base, double dt, long j0, int n, double* out, long stride)
+                                                   double base, double dt, long j0, int n, const Out& out)
 {
     const double two_pi = 6.283185307179586476925286766559;
     double w[KT], ph[KT], amp[KT], prev[KT], s[KT], c[KT], dl[KT], sdl[KT], cdl[KT];
@@ -72,7 +101,7 @@ __device__ __forceinline__ void sinusoid_run_terms(const double* a, const double
         sincos(dl[q], &sdl[q], &cdl[q]);
         v = __dadd_rn(v, __dmul_rn(amp[q], s[q]));
     }
-    if (n > 0) out[0] = v;
+    if (n > 0) out(0, v);
     for (int j = 1; j < n; ++j) {
         const double t = sample_time(base, dt, j0 + j);
         v = 0.0;
@@ -92,29 +121,28 @@ __device__ __forceinline__ void sinusoid_run_terms(const double* a, const double
             }
             v = __dadd_rn(v, __dmul_rn(amp[q], s[q]));
         }
-        out[(long)j * stride] = v;
+        out(j, v);
     }
 }
 
 // KMAX (1..4): the largest term count given its own chains; a kernel's
 // registers follow the largest variant it contains.
-template <int L, int KMAX>
+template <int L, int KMAX, class Out>
 __device__ __forceinline__ void sinusoid_run(const double* a, const double* f, const double* phi, int K, int i,
-                                             double base, double dt, long j0, long count, double* out, long stride)
+                                             double base, double dt, long j0, long count, const Out& out)
 {
     const long rest = count - j0;
     const int n = rest < L ? (int)rest : L;
     if (K == 1) {
-        sinusoid_run_terms<L, 1>(a, f, phi, i, base, dt, j0, n, out, stride);
+        sinusoid_run_terms<L, 1>(a, f, phi, i, base, dt, j0, n, out);
     } else if (KMAX >= 2 && K == 2) {
-        sinusoid_run_terms<L, (KMAX >= 2 ? 2 : 1)>(a, f, phi, i, base, dt, j0, n, out, stride);
+        sinusoid_run_terms<L, (KMAX >= 2 ? 2 : 1)>(a, f, phi, i, base, dt, j0, n, out);
     } else if (KMAX >= 3 && K == 3) {
-        sinusoid_run_terms<L, (KMAX >= 3 ? 3 : 1)>(a, f, phi, i, base, dt, j0, n, out, stride);
+        sinusoid_run_terms<L, (KMAX >= 3 ? 3 : 1)>(a, f, phi, i, base, dt, j0, n, out);
     } else if (KMAX >= 4 && K == 4) {
-        sinusoid_run_terms<L, (KMAX >= 4 ? 4 : 1)>(a, f, phi, i, base, dt, j0, n, out, stride);
+        sinusoid_run_terms<L, (KMAX >= 4 ? 4 : 1)>(a, f, phi, i, base, dt, j0, n, out);
     } else {
-        for (int j = 0; j < n; ++j)
-            out[(long)j * stride] = sinusoid_value(a, f, phi, K, i, sample_time(base, dt, j0 + j));
+        for (int j = 0; j < n; ++j) out(j, sinusoid_value(a, f, phi, K, i, sample_time(base, dt, j0 + j)));
     }
 }
 

@@ -155,4 +155,20 @@ void InputRegistry::fill(InputEntry* e, int device, double* U, int m, double bas
     PARODE_CUDA(cudaLaunchKernel((const void*)e->kern[v], dim3(grid), dim3(256), args, 0, s));
 }
 
+void InputRegistry::fill_planes(InputEntry* e, int device, float* hi, float* lo, double* scratch, int m, double base,
+                                double dt, long count, bool double_type, cudaStream_t s)
+{
+    if (m <= 0 || count <= 0) return;
+    if (e->kind == InputEntry::kSinusoid) {
+        if (e->m < m) throw Error(kInvalidInput, "sinusoid input has fewer channels than the system");
+        const long q = (long)e->m * e->K;
+        const double* d = sinusoid_device(e, device);
+        launch_sinusoid_planes(hi, lo, m, e->K, d, d + q, d + 2 * q, base, dt, count, s);
+        return;
+    }
+    if (!scratch) throw Error(kInvalidArgument, "a user input function needs FP64 scratch for its samples");
+    fill(e, device, scratch, m, base, dt, count, double_type, s);
+    launch_split_planes(scratch, hi, lo, count * m, s);
+}
+
 }  // namespace parode

@@ -43,6 +43,11 @@ public:
     // `double_type` selects the fType = double variant of a user function.
     void fill(InputEntry* e, int device, double* U, int m, double base, double dt, long count, bool double_type,
               cudaStream_t s);
+    // The same samples as TF32 hi / lo planes (hi[j*m + i], lo[j*m + i]): the
+    // sinusoid input writes them directly; a user function fills `scratch`
+    // (count*m doubles) first.
+    void fill_planes(InputEntry* e, int device, float* hi, float* lo, double* scratch, int m, double base,
+                     double dt, long count, bool double_type, cudaStream_t s);
     // Device copy of a sinusoid input's parameters: a | f | phi, m*K each.
     const double* sinusoid_device(InputEntry* e, int device);
 

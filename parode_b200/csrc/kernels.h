@@ -55,6 +55,30 @@ struct LevelArgs {
     int fault_withhold = 0;
 };
 
+// One GEMM of the mixed block-response leaf (kernels_resp_tc.cu):
+// dst(g, i) = sum_k W[i][k] window_g[k] for rows i < rows of W and windows g,
+// W pre-split (k_split of the LevelArgs with the same rows and K), the
+// windows read from the sample planes through `maps` (two 128-byte TMA maps,
+// resp_encode_plane_maps).  dst_limit >= 0 drops results at or beyond that
+// linear offset (the last block's steps past the horizon).
+struct RespArgs {
+    const float* Ps = nullptr;
+    int rows = 0, K = 0;
+    long ncols = 0;
+    const void* maps = nullptr;
+    double* dst = nullptr;
+    long dst_gs = 0, dst_is = 1, dst_limit = -1;
+    int fault_withhold = 0;  // test hook, as LevelArgs::fault_withhold
+};
+
+long resp_tc_tiles(const RespArgs& a);
+std::vector<long> resp_tc_ranges(const std::vector<RespArgs>& ents, int ctas);
+// Two tensor maps (hi plane, lo plane) of windows: row g starts at sample
+// offset g * block_stride, K samples long; written to out (256 bytes).
+void resp_encode_plane_maps(const float* hi, const float* lo, long ncols, int K, long block_stride, void* out);
+void launch_resp_tc(const RespArgs* dArgs, const long* dStart, int nent, const long* dCta, int ctas, int* status,
+                    cudaStream_t s);
+
 __host__ __device__ inline int level_rows(const LevelArgs& a) { return a.M > 0 ? a.M : a.Np; }
 __host__ __device__ inline int level_k(const LevelArgs& a) { return a.K > 0 ? a.K : a.Np; }
 
@@ -126,6 +150,11 @@ int response_log2_block(int solver, int NP, int n, int m, int p, long nScan, dou
 // doubles.  Returns the launches made.
 int chunk_carry_levels(long count);
 long chunk_carry_scratch(long count);
+// The same carry as one cooperative launch with bounded grid-wide barriers
+// between its levels (bar: two zeroed words of device memory; a barrier wait
+// that gives up writes 2 into *status).
+int launch_chunk_carry_coop(int NP, double* items, long count, const double* P, int l0, const double* X0,
+                            double* work, unsigned* bar, int* status, int sms, cudaStream_t s);
 int launch_chunk_carry(int NP, double* items, long count, const double* P, int l0, const double* X0, double* work,
                        cudaStream_t s);
 
@@ -142,6 +171,13 @@ inline long sweep_columns(long nScan, long Tp, long d)
 // U[j*m + i] = sum_k a sin(2 pi f t_j + phi), t_j = base + dt*j, j < count.
 void launch_sinusoid_samples(double* U, int m, int K, const double* a, const double* f, const double* phi,
                              double base, double dt, long count, cudaStream_t s);
+
+// The same samples written as TF32 hi / lo planes (hi = TF32(x),
+// lo = TF32(x - hi), x = float(u)), the tensor-core GEMMs' operand form.
+void launch_sinusoid_planes(float* hi, float* lo, int m, int K, const double* a, const double* f, const double* phi,
+                            double base, double dt, long count, cudaStream_t s);
+// FP64 samples into those planes (n values).
+void launch_split_planes(const double* U, float* hi, float* lo, long n, cudaStream_t s);
 
 // Scan-vector initialisation with the forcing term Gamma_k (zero padding
 // for k >= T and for the components the solver leaves empty).

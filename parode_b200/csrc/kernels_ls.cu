@@ -349,7 +349,29 @@ __global__ void k_sinusoid_samples(double* U, int m, int K, const double* a, con
     const long r = e / m;
     const int i = (int)(e - r * m);
     const long j0 = r * kSampleRun;
-    sinusoid_run<kSampleRun, KMAX>(a, f, phi, K, i, base, dt, j0, count, U + j0 * m + i, m);
+    sinusoid_run<kSampleRun, KMAX>(a, f, phi, K, i, base, dt, j0, count, SampleOut64{U + j0 * m + i, m});
+}
+
+// The same samples as TF32 hi / lo planes (the tensor-core GEMMs' operands).
+template <int KMAX>
+__global__ void k_sinusoid_planes(float* hi, float* lo, int m, int K, const double* a, const double* f,
+                                  const double* phi, double base, double dt, long count)
+{
+    const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long runs = (count + kSampleRun - 1) / kSampleRun;
+    if (e >= runs * m) return;
+    const long r = e / m;
+    const int i = (int)(e - r * m);
+    const long j0 = r * kSampleRun;
+    sinusoid_run<kSampleRun, KMAX>(a, f, phi, K, i, base, dt, j0, count,
+                                   SampleOutSplit{hi + j0 * m + i, lo + j0 * m + i, m});
+}
+
+// FP64 samples (any input function) into TF32 hi / lo planes.
+__global__ void k_split_planes(const double* __restrict__ U, float* __restrict__ hi, float* __restrict__ lo, long n)
+{
+    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x)
+        SampleOutSplit{hi, lo, 1}(e, U[e]);
 }
 
 // V[k][i] = Gamma_k[i]; RK4: Gamma_k = Bbar [u_2k; u_2k+1; u_2k+2] in rows
@@ -423,8 +445,8 @@ __global__ void k_samples_batch(const SampleJob* __restrict__ jobs)
         const long r = e / J.m;
         const int i = (int)(e - r * J.m);
         const long j0 = r * kSampleRun;
-        sinusoid_run<kSampleRun, KMAX>(J.a, J.f, J.phi, J.K, i, J.base, J.dt, j0, J.count, J.U + j0 * J.m + i,
-                                       J.m);
+        sinusoid_run<kSampleRun, KMAX>(J.a, J.f, J.phi, J.K, i, J.base, J.dt, j0, J.count,
+                                       SampleOut64{J.U + j0 * J.m + i, J.m});
     }
 }
 
@@ -605,6 +627,28 @@ void launch_sinusoid_samples(double* U, int m, int K, const double* a, const dou
     case 3: k_sinusoid_samples<3><<<g, 256, 0, s>>>(U, m, K, a, f, phi, base, dt, count); break;
     default: k_sinusoid_samples<4><<<g, 256, 0, s>>>(U, m, K, a, f, phi, base, dt, count); break;
     }
+    PARODE_CUDA(cudaGetLastError());
+}
+
+void launch_sinusoid_planes(float* hi, float* lo, int m, int K, const double* a, const double* f, const double* phi,
+                            double base, double dt, long count, cudaStream_t s)
+{
+    if (count <= 0 || m <= 0) return;
+    const long total = (count + kSampleRun - 1) / kSampleRun * m;
+    const unsigned g = (unsigned)blocks_for(total, 256);
+    switch (sample_kmax(K)) {
+    case 1: k_sinusoid_planes<1><<<g, 256, 0, s>>>(hi, lo, m, K, a, f, phi, base, dt, count); break;
+    case 2: k_sinusoid_planes<2><<<g, 256, 0, s>>>(hi, lo, m, K, a, f, phi, base, dt, count); break;
+    case 3: k_sinusoid_planes<3><<<g, 256, 0, s>>>(hi, lo, m, K, a, f, phi, base, dt, count); break;
+    default: k_sinusoid_planes<4><<<g, 256, 0, s>>>(hi, lo, m, K, a, f, phi, base, dt, count); break;
+    }
+    PARODE_CUDA(cudaGetLastError());
+}
+
+void launch_split_planes(const double* U, float* hi, float* lo, long n, cudaStream_t s)
+{
+    if (n <= 0) return;
+    k_split_planes<<<(unsigned)std::min<long>((n + 255) / 256, 148L * 16), 256, 0, s>>>(U, hi, lo, n);
     PARODE_CUDA(cudaGetLastError());
 }
 

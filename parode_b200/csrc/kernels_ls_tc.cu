@@ -212,16 +212,6 @@ __device__ __forceinline__ void tile_coords(const LevelArgs& a, long lt, int& mi
     nk = (level_k(a) + kBK - 1) / kBK;
 }
 
-// K slice read at position s of tile lt: each tile starts its K loop at its
-// own slice (tile index mod the slice count), so that the CTAs, which all
-// read the same P blocks, spread over the blocks at any moment instead of
-// fetching the same bytes from the same L2 slices together.  The order of a
-// tile depends on the tile alone, so results do not depend on which CTA runs it.
-__device__ __forceinline__ int rotated_slice(long lt, int s, int nk)
-{
-    const int r = (int)(lt % nk) + s;
-    return r < nk ? r : r - nk;
-}
 
 // Persistent grouped kernel: CTA c walks tiles [cta[c], cta[c+1]) in order.
 __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __restrict__ args,
@@ -297,7 +287,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
                 // stage's waits run into their bound (no copy is in flight)
                 const bool withhold = a.fault_withhold && blockIdx.x == 0 && j == 0;
                 if (lane == 0 && !withhold) {
-                    const int sr = rotated_slice(lt, s, nk);
+                    const int sr = s;
                     const int rowsv = level_rows(a) - m0 < kBM ? level_rows(a) - m0 : kBM;
                     const uint32_t abytes = (uint32_t)((rowsv + 7) / 8) * (uint32_t)(kBK * 32);
                     const unsigned char* ab = reinterpret_cast<const unsigned char*>(a.Ps) + ((size_t)mi * nk + sr) * kABlock;
@@ -398,7 +388,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
                 }
                 unsigned char* stg = sm + st * kStage;
                 const double* raw = reinterpret_cast<const double*>(stg + kOffRaw);
-                const int kl = slice_len(level_k(a), rotated_slice(lt, s, nk));
+                const int kl = slice_len(level_k(a), s);
                 // 64 vectors x kBK/4 chunks of 4 K; item w -> vector w / (kBK/4),
                 // chunk w % (kBK/4): a warp reads whole vectors and writes
                 // contiguous core-matrix rows

@@ -177,9 +177,13 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
     alloc(&dX0_, Np_);
     {
         double* st = nullptr;
-        alloc(&st, 1);
+        alloc(&st, 2);
         dStatus_ = reinterpret_cast<int*>(st);
-        PARODE_CUDA(cudaMemsetAsync(dStatus_, 0, sizeof(int), stream_));
+        dBar_ = reinterpret_cast<unsigned*>(st + 1);
+        PARODE_CUDA(cudaMemsetAsync(st, 0, 2 * sizeof(double), stream_));
+        int coop = 0;
+        PARODE_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device_));
+        coop_ = coop != 0;
     }
     if (path_ == kPathLevel || path_ == kPathGeneral) {
         alloc(&dV_, (Tp_ + 1) * (long)Np_);  // a leading slot holds the initial state
@@ -222,8 +226,24 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
         // the response leaf reads whole windows: the last block's window runs
         // past the samples into a zero padding
         const long pad = br_ ? (2L * shape_.B + 8) * mu_ + 2 : 0;
-        alloc(&dU_, nU_ * (long)mu_ + pad);
-        if (pad) PARODE_CUDA(cudaMemsetAsync(dU_, 0, sizeof(double) * (size_t)(nU_ * mu_ + pad), stream_));
+        // the mixed response GEMMs read the samples as TF32 planes (their TMA
+        // boxes run up to 15 samples past a window); FP64 samples are then
+        // only the scratch a user input function fills before the split
+        const bool planes = br_tc_;
+        if (!planes || input_->kind != InputEntry::kSinusoid) {
+            alloc(&dU_, nU_ * (long)mu_ + pad);
+            if (pad) PARODE_CUDA(cudaMemsetAsync(dU_, 0, sizeof(double) * (size_t)(nU_ * mu_ + pad), stream_));
+        }
+        if (planes) {
+            const long nf = nU_ * (long)mu_ + pad + 16;
+            double* d = nullptr;
+            alloc(&d, (nf + 1) / 2);
+            dUh_ = reinterpret_cast<float*>(d);
+            alloc(&d, (nf + 1) / 2);
+            dUl_ = reinterpret_cast<float*>(d);
+            PARODE_CUDA(cudaMemsetAsync(dUh_, 0, sizeof(float) * (size_t)nf, stream_));
+            PARODE_CUDA(cudaMemsetAsync(dUl_, 0, sizeof(float) * (size_t)nf, stream_));
+        }
     }
     PARODE_CUDA(cudaMemcpyAsync(dPow_, PhiP.data(), sizeof(double) * PhiP.size(), cudaMemcpyHostToDevice, stream_));
     PARODE_CUDA(cudaMemcpyAsync(dBbar_, Bbar.data(), sizeof(double) * Bbar.size(), cudaMemcpyHostToDevice, stream_));
@@ -315,46 +335,53 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
             a.Np = Np_;
             a.M = Np_;
             a.K = brK_;
-            a.ncols = nblocks_;
-            a.src = dU_;
-            a.src_gs = (solver == kRK4 ? 2L : 1L) * shape_.B * mu_;
-            a.src_ks = 1;
-            a.dst = dG_;
-            a.dst_gs = Np_;
             LevelArgs& w = e[1];
             w = a;
             w.P = dW_;
             w.M = shape_.B * p_;
-            w.dst = dY_ + (solver == kRK4 ? 0L : 3L * p_);
-            w.dst_gs = (long)shape_.B * p_;
-            w.dst_limit = nScan_ * (long)p_;
-            if (!level_tc_supported(a) || !level_tc_supported(w))
-                throw Error(kDeviceError, "response GEMMs not supported by the tensor-core kernel");
-            a.fault_withhold = opt.fault_withhold ? 1 : 0;
             const size_t sa = gemm_split_bytes(a.M, a.K), sw = gemm_split_bytes(w.M, w.K);
             double* ps = nullptr;
             alloc(&ps, (long)((sa + sw) / 8));
             a.Ps = reinterpret_cast<const float*>(ps);
             w.Ps = reinterpret_cast<const float*>(reinterpret_cast<char*>(ps) + sa);
-            double* map = nullptr;
-            alloc(&map, 16);  // one 128-byte tensor map, shared: same source, K and columns
-            unsigned char host_map[128];
-            level_encode_src_map(a, host_map);
-            PARODE_CUDA(cudaMemcpyAsync(map, host_map, 128, cudaMemcpyHostToDevice, stream_));
-            a.src_map = map;
-            w.src_map = map;
-            const long start[2] = {0, level_tc_tiles(a)};
-            const long tiles = start[1] + level_tc_tiles(w);
+            // two 128-byte TMA maps (hi and lo planes) over the windows
+            const long stride = (solver == kRK4 ? 2L : 1L) * shape_.B * mu_;
+            double* maps = nullptr;
+            alloc(&maps, 32);
+            unsigned char host_maps[256];
+            resp_encode_plane_maps(dUh_, dUl_, nblocks_, brK_, stride, host_maps);
+            PARODE_CUDA(cudaMemcpyAsync(maps, host_maps, 256, cudaMemcpyHostToDevice, stream_));
+            RespArgs r[2];
+            r[0].Ps = a.Ps;
+            r[0].rows = Np_;
+            r[0].K = brK_;
+            r[0].ncols = nblocks_;
+            r[0].maps = maps;
+            r[0].dst = dG_;
+            r[0].dst_gs = Np_;
+            r[0].fault_withhold = opt.fault_withhold ? 1 : 0;
+            r[1] = r[0];
+            r[1].Ps = w.Ps;
+            r[1].rows = shape_.B * p_;
+            r[1].dst = dY_ + (solver == kRK4 ? 0L : 3L * p_);
+            r[1].dst_gs = (long)shape_.B * p_;
+            r[1].dst_limit = nScan_ * (long)p_;
+            r[1].fault_withhold = 0;
+            const long start[2] = {0, resp_tc_tiles(r[0])};
+            const long tiles = start[1] + resp_tc_tiles(r[1]);
             tcCtas_ = (int)std::min<long>(sms_, tiles);
-            const std::vector<long> ranges = level_tc_ranges({a, w}, tcCtas_);
+            const std::vector<long> ranges = resp_tc_ranges({r[0], r[1]}, tcCtas_);
             double* d = nullptr;
             alloc(&d, (long)((2 * sizeof(LevelArgs) + 7) / 8));
             dTc_ = reinterpret_cast<LevelArgs*>(d);
+            alloc(&d, (long)((2 * sizeof(RespArgs) + 7) / 8));
+            dResp_ = reinterpret_cast<RespArgs*>(d);
             alloc(&d, 2);
             dTcStart_ = reinterpret_cast<long*>(d);
             alloc(&d, (long)ranges.size());
             dTcCta_ = reinterpret_cast<long*>(d);
             PARODE_CUDA(cudaMemcpyAsync(dTc_, e, sizeof(e), cudaMemcpyHostToDevice, stream_));
+            PARODE_CUDA(cudaMemcpyAsync(dResp_, r, sizeof(r), cudaMemcpyHostToDevice, stream_));
             PARODE_CUDA(cudaMemcpyAsync(dTcStart_, start, sizeof(start), cudaMemcpyHostToDevice, stream_));
             PARODE_CUDA(cudaMemcpyAsync(dTcCta_, ranges.data(), sizeof(long) * ranges.size(), cudaMemcpyHostToDevice,
                                         stream_));
@@ -459,7 +486,9 @@ std::vector<std::pair<std::string, float>> Plan::stage_times()
 
 void Plan::fill_inputs(cudaStream_t s)
 {
-    if (mu_ > 0) inputs_->fill(input_, device_, dU_, mu_, u_base_, u_dt_, nU_, opt_.input_double, s);
+    if (mu_ <= 0) return;
+    if (dUh_) inputs_->fill_planes(input_, device_, dUh_, dUl_, dU_, mu_, u_base_, u_dt_, nU_, opt_.input_double, s);
+    else inputs_->fill(input_, device_, dU_, mu_, u_base_, u_dt_, nU_, opt_.input_double, s);
 }
 
 void Plan::execute(double* y, cudaStream_t s)
@@ -632,6 +661,17 @@ void Plan::execute_general(double* Y, cudaStream_t s)
     last_y_ = Y;
 }
 
+int Plan::carry(cudaStream_t s)
+{
+    // the exclusive scan of the block aggregates: one cooperative launch whose
+    // levels are separated by grid barriers (its two barrier words are reset
+    // first), or the chain of per-level launches where cooperative launch is
+    // not available
+    if (!coop_) return launch_chunk_carry(Np_, dG_, nblocks_, dPow_, shape_.R, dX0_, dWork_, s);
+    PARODE_CUDA(cudaMemsetAsync(dBar_, 0, 2 * sizeof(unsigned), s));
+    return launch_chunk_carry_coop(Np_, dG_, nblocks_, dPow_, shape_.R, dX0_, dWork_, dBar_, dStatus_, sms_, s);
+}
+
 void Plan::execute_response(double* Y, cudaStream_t s)
 {
     // leaf = W x [sample window; initial state] per block (kernels_br.cu):
@@ -650,10 +690,10 @@ void Plan::execute_response(double* Y, cudaStream_t s)
     if (br_tc_) {
         // mixed: aggregates and output windows (tensor cores) -> carry ->
         // y = windows + C Phi^j X_b (FP64)
-        launch_level_tc(dTc_, dTcStart_, 2, dTcCta_, tcCtas_, dStatus_, s);
+        launch_resp_tc(dResp_, dTcStart_, 2, dTcCta_, tcCtas_, dStatus_, s);
         ++launches;
         mark("aggregates+windows", s);
-        launches += launch_chunk_carry(Np_, dG_, nblocks_, dPow_, shape_.R, dX0_, dWork_, s);
+        launches += carry(s);
         mark("carry", s);
         LevelArgs x;
         x.P = dW_ + brKpad_;
@@ -695,7 +735,7 @@ void Plan::execute_response(double* Y, cudaStream_t s)
     launch_gemm_tiled(g, s);
     ++launches;
     mark("aggregates", s);
-    launches += launch_chunk_carry(Np_, dG_, nblocks_, dPow_, shape_.R, dX0_, dWork_, s);
+    launches += carry(s);
     mark("carry", s);
     LevelArgs h = g;
     h.P = dW_;

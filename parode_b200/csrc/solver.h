@@ -94,6 +94,7 @@ private:
     void execute_blocked(double* Y, cudaStream_t s);
     void execute_response(double* Y, cudaStream_t s);
     void execute_general(double* Y, cudaStream_t s);
+    int carry(cudaStream_t s);
     void fill_inputs(cudaStream_t s);
 
     int device_ = 0;
@@ -129,11 +130,16 @@ private:
     // mixed form of the response leaf: aggregates and output windows on the
     // tensor cores (one grouped launch of two GEMMs), state part in FP64
     bool br_tc_ = false;
-    LevelArgs* dTc_ = nullptr;  // device: the two GEMMs
+    LevelArgs* dTc_ = nullptr;  // device: the two GEMMs as k_split reads them
+    RespArgs* dResp_ = nullptr; // device: the two GEMMs as the tensor-core kernel reads them
+    float* dUh_ = nullptr;      // input samples as TF32 hi / lo planes
+    float* dUl_ = nullptr;
     long* dTcStart_ = nullptr;  // device: their first tiles
     long* dTcCta_ = nullptr;    // device: tile ranges of the persistent CTAs
     int tcCtas_ = 0;
     int* dStatus_ = nullptr;
+    unsigned* dBar_ = nullptr;  // grid-barrier words of the single-launch carry
+    bool coop_ = false;         // the carry runs as one cooperative launch
     cudaStream_t side_ = nullptr;
     cudaEvent_t fork_[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t done_ = nullptr;  // recorded after each execute on its stream

@@ -197,6 +197,40 @@ def test_reference_fixtures_through_c_abi(pb):
             assert oracle.rel_err(y, yo) < 1e-5, (fx["name"], c["solver"], c["steps"])
 
 
+def test_c_abi_matches_the_reference_kernels(pb):
+    """The drop-in float C ABI (SimulateODE with the case's UFunc through
+    RegisterInput) against the reference's own OpenCL kernels run on a B200
+    (tests/golden/ref_kernel_outputs.json: the reference tests' fixtures, the
+    n=8 benchmark system and its ABM twin, systems with no C and D).  The
+    library computes in FP64, the kernels in FP32: the agreement is the
+    reference's FP32 accuracy."""
+    import base64
+
+    pb.set_option(pb.OPT_PATH, 0)
+    path = os.path.join(os.path.dirname(GOLDEN), "ref_kernel_outputs.json")
+    with open(path) as fh:
+        cases = json.load(fh)["cases"]
+    checked = 0
+    for c in cases:
+        if c["max_batch"]:
+            continue  # the cap on the reference's time batches has no counterpart here
+        # the OpenCL extension pragma is not C++; the function body is
+        src = "\n".join(ln for ln in c["ufunc"].splitlines() if not ln.startswith("#pragma OPENCL"))
+        u = pb.register_input(src)
+        arr = lambda k: None if c[k] is None else np.array(c[k], dtype=np.float64)
+        t, y, err = pb.simulate_f32(arr("A"), arr("B"), arr("C"), arr("D"), arr("x0"), u, c["t0"], c["t_end"], c["h"],
+                                    solver=c["solver"])
+        assert err == 0, c["name"]
+        yk = np.frombuffer(base64.b64decode(c["y_f32"]), dtype=np.float32).reshape(c["T"], c["q"])
+        tk = np.frombuffer(base64.b64decode(c["time_f32"]), dtype=np.float32)
+        assert y.shape == yk.shape, c["name"]
+        assert np.array_equal(t, tk), c["name"]
+        e = oracle.rel_err(y.astype(np.float64), yk.astype(np.float64))
+        assert e <= 5e-5, (c["name"], e)
+        checked += 1
+    assert checked >= 15
+
+
 def test_python_module_reference_script(pb):
     """PythonInterface/TestPythonODESolvers.py of the reference, in Python 3."""
     import ParODE
