@@ -40,11 +40,13 @@ struct SampleOut64 {
     __device__ __forceinline__ void operator()(long j, double v) const { out[j * stride] = v; }
 };
 
+// x rounded to TF32 (10 mantissa bits), to nearest with ties away from zero:
+// half a unit of the kept last bit added to the magnitude, the 13 dropped
+// bits cleared (for finite x the result of cvt.rna.tf32.f32, in two integer
+// operations instead of a conversion).
 __device__ __forceinline__ float tf32_rna(float x)
 {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return __uint_as_float(r);
+    return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
 
 struct SampleOutSplit {

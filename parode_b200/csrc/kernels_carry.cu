@@ -339,9 +339,12 @@ int chunk_carry_coop_t(double* items, long count, const double* P, int l0, const
         w += nc * NP;
         ++L.H;
     }
+    // one CTA per SM: each tile's steps run at its SM's full FP64 tensor
+    // rate, and few CTAs wait at the barriers while an upper level runs
     int per_sm = 0;
     PARODE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_carry_coop<NP>, kThreads, 0));
-    const long grid = std::max<long>(1, std::min<long>(tiles_max, (long)sms * std::max(per_sm, 1)));
+    if (per_sm < 1) throw Error(kDeviceError, "chunk carry: the cooperative kernel does not fit an SM");
+    const long grid = std::max<long>(1, std::min<long>(tiles_max, (long)sms));
     void* args[] = {(void*)&L, (void*)&P, (void*)&X0, (void*)&bar, (void*)&status};
     PARODE_CUDA(cudaLaunchCooperativeKernel((const void*)k_carry_coop<NP>, dim3((unsigned)grid), dim3(kThreads), args,
                                             0, s));

@@ -7,8 +7,10 @@
 // the reference's MM / MVV up-sweep step (Kernels/MMKernelScanUpsweep.cl:24-53,
 // Kernels/MVVKernelScanUpsweep.cl:25-48).  The product is D = A B^T with
 // A = M[k] (rows i, K = l: row-major is K-major) and B[c][l] = M[j][l][c]
-// (M[j] transposed while it is split); both are split into TF32 hi/lo in the
-// MMA's canonical K-major layout (8-row x 16-byte core matrices), and
+// (M[j] transposed while it is split).  Only E = M - I goes through the
+// tensor cores (M[k] M[j] = M[k] + M[j] - I + E[k] E[j], the first three
+// terms in FP64), split into TF32 hi/lo in the MMA's canonical K-major
+// layout (8-row x 16-byte core matrices), and
 // hi*hi goes to one TMEM accumulator, hi*lo + lo*hi to a second, summed in
 // FP64 by the epilogue (the chains are NP/8 and NP/4 MMAs long).  The MMA
 // is M = 128: rows NP..127 of A read whatever follows the A tile in shared
@@ -108,15 +110,19 @@ __global__ void __launch_bounds__(kThreads, 1) k_compose_tc(double* __restrict__
             for (int c = 0; c < NP; ++c) s = fma(Araw[r * NP + c], vj[c], s);
             V[k * NP + r] += s;
         }
-        // split: A rows i, K = l from M[k][i][l]; B rows c, K = l from M[j][l][c]
+        // split of E = M - I (the identity part is exact and stays out of the
+        // tensor cores: M[k] M[j] = M[k] + M[j] - I + E[k] E[j], so the TF32
+        // rounding is relative to E[k] E[j], which is small for maps near the
+        // identity): A rows i, K = l from E[k][i][l]; B rows c, K = l from E[j][l][c]
         for (int e = threadIdx.x; e < NP * NP; e += kThreads) {
             const int r = e / NP, c = e - r * NP;
+            const double id = r == c ? 1.0 : 0.0;
             float hi, lo;
-            split_tf32((float)Araw[e], hi, lo);
+            split_tf32((float)(Araw[e] - id), hi, lo);
             const uint32_t oa = kmajor_off(r, c, NP);
             *reinterpret_cast<float*>(sm + L::offAh + oa) = hi;
             *reinterpret_cast<float*>(sm + L::offAh + L::half + oa) = lo;
-            split_tf32((float)Braw[e], hi, lo);           // Braw[r][c] = M[j][l = r][c]
+            split_tf32((float)(Braw[e] - id), hi, lo);    // Braw[r][c] = M[j][l = r][c]
             const uint32_t ob = kmajor_off(c, r, NP);     // B row c, K index r
             *reinterpret_cast<float*>(sm + L::offBh + ob) = hi;
             *reinterpret_cast<float*>(sm + L::offBh + L::bhalf + ob) = lo;
@@ -160,10 +166,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_compose_tc(double* __restrict__
                 tmem_wait_ld();
                 if (row < NP) {
 #pragma unroll
-                    for (int c = 0; c < 32; ++c)
-                        if (cg * 32 + c < NP)
-                            Araw[row * NP + cg * 32 + c] =
-                                (double)__uint_as_float(hh[c]) + (double)__uint_as_float(cc[c]);
+                    for (int c = 0; c < 32; ++c) {
+                        const int col = cg * 32 + c;
+                        if (col < NP) {
+                            // M[k] + M[j] - I in FP64, plus the tensor-core E[k] E[j]
+                            const double exact = Araw[row * NP + col] + Braw[row * NP + col] - (row == col ? 1.0 : 0.0);
+                            Araw[row * NP + col] = exact + ((double)__uint_as_float(hh[c]) + (double)__uint_as_float(cc[c]));
+                        }
+                    }
                 }
             }
         }
