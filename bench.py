@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--min-warmup-s", type=float, default=0.5, help="least warm-up time under load (clock sampling)")
     ap.add_argument("--no-extra", action="store_true", help="skip the batched (4096 systems) and serving runs")
     ap.add_argument("--serve-requests", type=int, default=256)
+    ap.add_argument("--no-tune", action="store_true", help="time with the untuned block length of the response leaf")
     ap.add_argument("--ref-T", type=int, default=1 << 20,
                     help="reference arm: steps of the cfg2 horizon solved per timed step (default: all 2^20)")
     return ap.parse_args()
@@ -246,7 +247,7 @@ def _cheap_sample(cases, k):
     return small[: k // 2] + large[: k - k // 2]
 
 
-def measure_batched(pb, wl, torch, dev, reps=3):
+def measure_batched(pb, wl, torch, dev, reps=3, tune_classes=0):
     """The batched form: 4096 independent systems (cfg4) in one batch, FP64 and mixed."""
     from oracle import oracle
 
@@ -283,7 +284,88 @@ def measure_batched(pb, wl, torch, dev, reps=3):
                      "setup_s": setup_s, "rel_err_sampled": worst, "sampled_systems": len(check)}
         b.close()
     out["mixed_over_fp64"] = out["fp64"]["ms"] / out["mixed"]["ms"]
+    if tune_classes > 0:
+        # the block length measured for the classes that carry most of the
+        # work (ParODE_TuneResponseBlock), then the mixed batch again
+        tuned = tune_batch_classes(pb, cases, pb.MIXED, tune_classes)
+        b = pb.Batch(specs, precision=pb.MIXED)
+        b.execute(stream.cuda_stream)
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            b.execute(stream.cuda_stream)
+            e.record(stream)
+            e.synchronize()
+            ts.append(s.elapsed_time(e))
+        ms = statistics.median(ts)
+        out["mixed_tuned"] = {"ms": ms, "value": b.state_steps / (ms / 1e3), "unit": UNIT, "launches": b.launch_count,
+                              "classes_tuned": len(tuned), "share_of_work_tuned": sum(w for _, w in tuned),
+                              "gain_over_untuned": out["mixed"]["ms"] / ms}
+        b.close()
+        pb.tune_clear()
     return out
+
+
+def _tune_key(c):
+    pw = lambda v: 1 << max(0, int(v - 1).bit_length())
+    ns = c.scan_dim
+    nscan = c.T if c.solver == 0 else c.T - 3
+    return (c.solver, pw(max(8, ns)), pw(c.m), pw(c.p), max(0, int(nscan - 1).bit_length()))
+
+
+def tune_batch_classes(pb, cases, precision, count):
+    """Tunes the `count` classes of systems with the most state*steps; returns
+    [(class, share of the batch's state*steps)]."""
+    work, rep = {}, {}
+    for c in cases:
+        k = _tune_key(c)
+        work[k] = work.get(k, 0.0) + c.n * c.T
+        if k not in rep or c.n * c.T > rep[k].n * rep[k].T:
+            rep[k] = c
+    total = sum(work.values())
+    top = sorted(work, key=lambda k: -work[k])[:count]
+    for k in top:
+        c = rep[k]
+        pb.tune_response_block(c.solver, c.n, c.m, c.p, c.T, precision)
+    return [(k, work[k] / total) for k in top]
+
+
+def measure_cfg1(pb, wl, torch, reps=200):
+    """The small single solve (cfg1: RK4 n=8 m=2 p=2, T=4096): latency of
+    one execute (CUDA events, inputs resident) and of the whole C-ABI call
+    with host buffers, as p50 / p99 over `reps` solves."""
+    c = wl.cfg1()
+    u = pb.register_sinusoid(c.u.a, c.u.f, c.u.phi)
+    plan = pb.Plan(c.A, c.B, c.C, c.D, c.x0, u, c.t0, c.t_end, c.h, solver=c.solver)
+    stream = torch.cuda.Stream()
+    for _ in range(10):
+        plan.execute(0, stream.cuda_stream)
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        plan.execute(0, stream.cuda_stream)
+        e.record(stream)
+        e.synchronize()
+        ts.append(s.elapsed_time(e))
+    launches = plan.launch_count
+    plan.close()
+    T_out = pb.num_outputs(c.solver, c.t0, c.t_end, c.h)
+    t_host = torch.empty(T_out, dtype=torch.float64, pin_memory=True).numpy()
+    y_host = torch.empty((T_out, c.p), dtype=torch.float64, pin_memory=True).numpy()
+    es = []
+    for it in range(reps // 4 + 5):
+        t0 = time.perf_counter()
+        pb.simulate(c.A, c.B, c.C, c.D, c.x0, u, c.t0, c.t_end, c.h, solver=c.solver, t_out=t_host, y_out=y_host)
+        if it >= 5:
+            es.append((time.perf_counter() - t0) * 1e3)
+    return {"workload": "cfg1: RK4 n=8 m=2 p=2 h=1e-3 T=4096", "precision": "fp64", "launches": launches,
+            "solve_ms": {"p50": float(np.percentile(ts, 50)), "p99": float(np.percentile(ts, 99))},
+            "value": c.n * c.T / (float(np.percentile(ts, 50)) / 1e3), "unit": UNIT,
+            "e2e_ms": {"p50": float(np.percentile(es, 50)), "p99": float(np.percentile(es, 99))}}
 
 
 def measure_cfg3(pb, wl, torch, reps=3):
@@ -445,6 +527,16 @@ def run_ours(args):
         return info, y_host
 
     precision = pb.MIXED if args.precision == "mixed" else pb.FP64
+    # the response leaf's block length measured for this class of systems
+    # (ParODE_TuneResponseBlock); the plans below use it
+    tuner = None
+    if not args.no_tune:
+        tuner = {}
+        for name, prec in (("mixed", pb.MIXED), ("fp64", pb.FP64)):
+            if name == "fp64" and args.no_plain and precision != pb.FP64:
+                continue
+            R, best, untuned = pb.tune_response_block(case.solver, case.n, case.m, case.p, case.T, prec)
+            tuner[name] = {"block": 1 << R, "ms_tuned": best, "ms_untuned": untuned, "gain": untuned / best}
     main, y_main = time_plan(precision, True)
     plain, y_plain = (None, None)
     if not args.no_plain and precision != pb.FP64:
@@ -482,9 +574,41 @@ def run_ours(args):
                "max_ms": max(e2e_ms),
                "call": "ParODE_SimulateODE_d (host arrays in, y out into pinned host memory reused across calls)"}
 
+    # the e2e call's parts, each timed on its own: plan creation (host
+    # discretisation, W and power tables on the device), the solve, the copy
+    # of y into pinned host memory, the host time vector
+    e2e_split = None
+    if not args.no_e2e:
+        T_out = pb.num_outputs(case.solver, case.t0, case.t_end, case.h)
+        t_host = torch.empty(T_out, dtype=torch.float64, pin_memory=True).numpy()
+        y_host = torch.empty((T_out, case.p), dtype=torch.float64, pin_memory=True).numpy()
+        parts = {"plan_ms": [], "solve_ms": [], "copy_ms": []}
+        for it in range(4):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            plan = pb.Plan(case.A, case.B, case.C, case.D, case.x0, u, case.t0, case.t_end, case.h,
+                           solver=case.solver, precision=precision)
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            plan.execute()
+            torch.cuda.synchronize()
+            t2 = time.perf_counter()
+            plan.output(t_out=t_host, y_out=y_host)  # y by DMA while the host builds t
+            t3 = time.perf_counter()
+            plan.close()
+            if it > 0:
+                parts["plan_ms"].append((t1 - t0) * 1e3)
+                parts["solve_ms"].append((t2 - t1) * 1e3)
+                parts["copy_ms"].append((t3 - t2) * 1e3)
+        med = {k: statistics.median(v) for k, v in parts.items()}
+        e2e_split = dict(med, d2h_gbs=8.0 * case.T * case.p / (med["copy_ms"] / 1e3) / 1e9,
+                         note="parts timed separately with host clocks (synchronised); the e2e call overlaps the "
+                              "host time vector with plan creation, the solve and the copy")
+    cfg1 = measure_cfg1(pb, wl, torch) if world == 1 and not args.no_extra else None
+
     batched = serving = cfg3 = None
     if world == 1 and not args.no_extra:
-        batched = measure_batched(pb, wl, torch, dev)
+        batched = measure_batched(pb, wl, torch, dev, tune_classes=0 if args.no_tune else 16)
         cfg3 = measure_cfg3(pb, wl, torch)
         serving = measure_serving(pb, wl, torch, count=args.serve_requests)
 
@@ -548,6 +672,9 @@ def run_ours(args):
             "rel_err_mixed_vs_fp64": rel_vs_fp64,
             "peaks": {k: peaks.get(k) for k in ("hbm_gbs", "bf16_tflops", "bf16_tflops_sustained")},
             "peaks_source": peaks_kind,
+            "tuner": tuner,
+            "e2e_split": e2e_split,
+            "cfg1": cfg1,
             "batched": batched,
             "serving": serving,
             "abm_n128": cfg3,

@@ -228,6 +228,25 @@ void ParODE_AffineScanDevice(const double* dPhi, const double* dGamma, const dou
 void ParODE_AffineScanGeneral(const double* dM, const double* dV, const double* dX0, int ns, long long count,
                               int precision, double* dX, void* stream, int nErr[]);
 
+/* Measured block length of the block-response leaf (no counterpart in the
+ * reference, whose batch sizing is a memory formula,
+ * Sources/RungeKutta4thOrder.cpp:91-144).  TuneResponseBlock times the
+ * candidate block lengths 2^2 .. 2^7 on the current device for a synthetic
+ * stable system of the class (solver, states, inputs, outputs, steps,
+ * precision), five solves each after two warm-ups, and records the fastest;
+ * plans and batches made afterwards for systems of the same class (scan
+ * dimension, input and output counts rounded up to powers of two, steps to
+ * the power of two above) use it.  log2B[0], msBest[0]: the choice and its
+ * median solve time; msModel[0]: the untuned choice's.  Save / Load keep
+ * one GPU's entries in a text file (gpuName NULL: the current device's
+ * name); InitializeAllGPUs / InitializeSelectedGPUs load the file named by
+ * the environment variable PARODE_TUNE_FILE when it is set. */
+void ParODE_TuneResponseBlock(int solver, int nStates, int nInputs, int nOutputs, long long nSteps, int precision,
+                              int log2B[], float msBest[], float msModel[], int nErr[]);
+int ParODE_TuneSave(const char* path, const char* gpuName, int nErr[]);
+int ParODE_TuneLoad(const char* path, const char* gpuName, int nErr[]);
+void ParODE_TuneClear(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -140,6 +140,15 @@ def _load():
     L.ParODE_AffineScanGeneral.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_int,
                                            C.c_void_p, C.c_void_p, ip]
     L.ParODE_AffineScanGeneral.restype = None
+    fp = C.POINTER(C.c_float)
+    L.ParODE_TuneResponseBlock.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_longlong, C.c_int, ip, fp, fp, ip]
+    L.ParODE_TuneResponseBlock.restype = None
+    L.ParODE_TuneSave.argtypes = [C.c_char_p, C.c_char_p, ip]
+    L.ParODE_TuneSave.restype = C.c_int
+    L.ParODE_TuneLoad.argtypes = [C.c_char_p, C.c_char_p, ip]
+    L.ParODE_TuneLoad.restype = C.c_int
+    L.ParODE_TuneClear.argtypes = []
+    L.ParODE_TuneClear.restype = None
     return L
 
 
@@ -289,6 +298,36 @@ def affine_scan_general(M_ptr: int, V_ptr: int, x0_ptr: int, ns: int, count: int
     _check(e, "ParODE_AffineScanGeneral")
 
 
+def tune_response_block(solver: int, n: int, m: int, p: int, T: int, precision: int = FP64):
+    """ParODE_TuneResponseBlock: times the response leaf's block lengths for
+    this class of systems on the current device and records the fastest.
+    Returns (log2 of the block length, its median ms, the untuned choice's ms)."""
+    r = C.c_int(0)
+    best, model = C.c_float(0), C.c_float(0)
+    e = C.c_int(0)
+    lib.ParODE_TuneResponseBlock(solver, n, m, p, T, precision, C.byref(r), C.byref(best), C.byref(model), C.byref(e))
+    _check(e, "ParODE_TuneResponseBlock")
+    return r.value, float(best.value), float(model.value)
+
+
+def tune_save(path: str, gpu: Optional[str] = None) -> int:
+    e = C.c_int(0)
+    n = lib.ParODE_TuneSave(path.encode(), None if gpu is None else gpu.encode(), C.byref(e))
+    _check(e, "ParODE_TuneSave")
+    return int(n)
+
+
+def tune_load(path: str, gpu: Optional[str] = None) -> int:
+    e = C.c_int(0)
+    n = lib.ParODE_TuneLoad(path.encode(), None if gpu is None else gpu.encode(), C.byref(e))
+    _check(e, "ParODE_TuneLoad")
+    return int(n)
+
+
+def tune_clear() -> None:
+    lib.ParODE_TuneClear()
+
+
 def simulate_f32(A, B, Cm, D, x0, u_index: int, t0: float, t_end: float, h: float, solver: int = RK4):
     """The reference C ABI SimulateODE (float arrays).  Returns (t, y, err)."""
     A32 = np.ascontiguousarray(A, dtype=np.float32)
@@ -333,9 +372,11 @@ class Plan:
         lib.ParODE_PlanExecute(self._h, C.c_void_p(y_dev_ptr or None), C.c_void_p(stream or None), C.byref(e))
         _check(e, "ParODE_PlanExecute")
 
-    def output(self):
-        t = np.zeros(self.num_outputs)
-        y = np.zeros((self.num_outputs, self.channels))
+    def output(self, t_out=None, y_out=None):
+        """(t, y) of the last execute; t_out / y_out: optional caller-owned
+        float64 arrays (pinned host memory makes the copy one DMA)."""
+        t = np.zeros(self.num_outputs) if t_out is None else t_out
+        y = np.zeros((self.num_outputs, self.channels)) if y_out is None else y_out
         e = C.c_int(0)
         lib.ParODE_PlanGetOutput(self._h, _dp(t), _dp(y), C.byref(e))
         _check(e, "ParODE_PlanGetOutput")

@@ -13,16 +13,21 @@
 #include "batch.h"
 #include "blocked.h"
 #include "general.h"
+#include "tuner.h"
 #include "server.h"
 
 #include "FTypeDef.h"
 #include "ParODECInterface.h"
 #include "parode_ext.h"
 
+#include <algorithm>
 #include <atomic>
 #include <cstdio>
 #include <cstdlib>
+#include <cmath>
 #include <cstring>
+#include <fstream>
+#include <sstream>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -61,6 +66,7 @@ struct Library {
     int log = 0;
     long long executions = 1;  // PARODE_OPT_EXECUTIONS: plans and batches
     int fault_withhold = 0;    // PARODE_OPT_FAULT_WITHHOLD (test hook)
+    std::vector<int> tune_inputs;  // sinusoid inputs of the tuner's synthetic systems, by input count
     cudaEvent_t t_start = nullptr, t_stop = nullptr;
     bool timer_running = false;
 
@@ -112,6 +118,11 @@ struct Library {
         }
         selected = ids;
         cudaSetDevice(selected[0]);
+        // measured block lengths of an earlier tuning run on this kind of GPU
+        if (const char* tf = std::getenv("PARODE_TUNE_FILE")) {
+            int e = 0;
+            ParODE_TuneLoad(tf, nullptr, &e);
+        }
         if (cudaEventCreate(&t_start) != cudaSuccess || cudaEventCreate(&t_stop) != cudaSuccess) {
             cudaGetLastError();
             return kNotEnoughResources;
@@ -854,5 +865,203 @@ void ParODE_AffineScanGeneral(const double* dM, const double* dV, const double* 
     });
     if (nErr) nErr[0] = rc;
 }
+
+
+// ---------------------------------------------------------------------------
+// measured block length of the response leaf (tuner.h)
+// ---------------------------------------------------------------------------
+
+}  // extern "C"
+
+namespace {
+
+// The GPU's name as the tuning file keys it (spaces replaced).
+std::string gpu_key(const char* given)
+{
+    std::string name;
+    if (given && *given) {
+        name = given;
+    } else {
+        int dev = 0;
+        cudaDeviceProp prop;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
+            cudaGetLastError();
+            throw Error(kNoGPU, "no device to key the tuning table");
+        }
+        name = prop.name;
+    }
+    for (char& c : name)
+        if (c == ' ' || c == '\t') c = '_';
+    return name;
+}
+
+// A stable system of the class with seeded entries: A = -1.5 I + 0.5 G / sqrt(n),
+// B, C, D, x0 of unit scale (a counter-based generator, the same every call).
+SystemDesc tune_system(int n, int m, int p)
+{
+    uint64_t st = 0x9E3779B97F4A7C15ull * (uint64_t)(n * 131 + m * 7 + p);
+    auto unif = [&st]() {
+        st += 0x9E3779B97F4A7C15ull;
+        uint64_t z = st;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+    };
+    auto normal = [&unif]() { return std::sqrt(-2.0 * std::log(1.0 - unif())) * std::cos(6.283185307179586 * unif()); };
+    SystemDesc s;
+    s.n = n;
+    s.m = m;
+    s.p = p;
+    s.A.resize((size_t)n * n);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) s.A[(size_t)i * n + j] = (i == j ? -1.5 : 0.0) + 0.5 * normal() / std::sqrt((double)n);
+    s.B.resize((size_t)n * m);
+    for (double& v : s.B) v = normal();
+    s.C.resize((size_t)p * n);
+    for (double& v : s.C) v = normal();
+    s.D.resize((size_t)p * m);
+    for (double& v : s.D) v = normal();
+    s.x0.resize(n);
+    for (double& v : s.x0) v = normal();
+    return s;
+}
+
+}  // namespace
+
+extern "C" {
+
+void ParODE_TuneResponseBlock(int solver, int nStates, int nInputs, int nOutputs, long long nSteps, int precision,
+                              int log2B[], float msBest[], float msModel[], int nErr[])
+{
+    Library& L = lib();
+    std::lock_guard<std::recursive_mutex> g(L.mu);
+    int rc = guarded([&] {
+        const int dev = current_device_locked(L);
+        if (solver != kRK4 && solver != kABM) throw Error(kInvalidSolverType, "unknown solver");
+        if (nStates < 1 || nInputs < 1 || nOutputs < 1 || nSteps < 2) throw Error(kInvalidSystem, "empty class");
+        if (precision != PARODE_PRECISION_FP64 && precision != PARODE_PRECISION_MIXED)
+            throw Error(kInvalidArgument, "unknown precision");
+        const int Ns = solver == kRK4 ? nStates : 4 * nStates;
+        if (Ns > 1024) throw Error(kInvalidSystem, "scan dimension above 1024 is not supported");
+        SystemDesc s = tune_system(nStates, nInputs, nOutputs);
+        // a three-term sinusoid input per input count, registered once
+        if ((int)L.tune_inputs.size() <= nInputs) L.tune_inputs.resize(nInputs + 1, -1);
+        if (L.tune_inputs[nInputs] < 0) {
+            std::vector<double> a((size_t)nInputs * 3), f(a.size()), ph(a.size());
+            for (size_t q = 0; q < a.size(); ++q) {
+                a[q] = 0.5 + 0.1 * (double)(q % 5);
+                f[q] = 0.3 + 1.7 * (double)(q % 7);
+                ph[q] = 0.4 * (double)q;
+            }
+            L.tune_inputs[nInputs] = L.inputs.add_sinusoid(nInputs, 3, a.data(), f.data(), ph.data());
+        }
+        const int uIndex = L.tune_inputs[nInputs];
+        const double h = 1e-3, tEnd = ((double)nSteps - 0.5) * h;
+        long nScan = 0;
+        num_outputs(solver, 0.0, tEnd, h, &nScan);
+        // the untuned choice: the blocked shape's block for scan dimensions up
+        // to 64 (single solves), else the cost model's
+        const int np = (int)round_up(Ns, 8);
+        int Rdefault = 0;
+        BlockedShape sh;
+        if (Ns <= 64 && blocked_shape(Ns, nInputs, solver, &sh)) {
+            Rdefault = sh.R;
+        } else {
+            double cost = 0.0;
+            Rdefault = response_log2_block(solver, np, nStates, nInputs, nOutputs, nScan,
+                                           precision == PARODE_PRECISION_MIXED ? 0.25 : 1.0, (double)L.executions,
+                                           &cost);
+        }
+        while (Rdefault > 2 && (1L << Rdefault) / 2 >= nScan) --Rdefault;
+        auto time_R = [&](int R) -> float {
+            PlanOptions opt;
+            opt.precision = precision;
+            opt.path = kPathBlockedResponse;
+            opt.input_double = true;
+            opt.force_log2_block = R;
+            Plan plan(dev, s, &L.inputs, uIndex, solver, 0.0, tEnd, h, opt);
+            cudaStream_t st = plan.stream();
+            cudaEvent_t e0 = nullptr, e1 = nullptr;
+            PARODE_CUDA(cudaEventCreate(&e0));
+            PARODE_CUDA(cudaEventCreate(&e1));
+            std::vector<float> ts;
+            try {
+                for (int it = 0; it < 2; ++it) plan.execute(nullptr, st);
+                for (int it = 0; it < 5; ++it) {
+                    PARODE_CUDA(cudaEventRecord(e0, st));
+                    plan.execute(nullptr, st);
+                    PARODE_CUDA(cudaEventRecord(e1, st));
+                    PARODE_CUDA(cudaEventSynchronize(e1));
+                    float ms = 0.f;
+                    PARODE_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                    ts.push_back(ms);
+                }
+                plan.get_output(nullptr, nullptr);  // reports a device wait that gave up
+            } catch (...) {
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                throw;
+            }
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            std::sort(ts.begin(), ts.end());
+            return ts[ts.size() / 2];
+        };
+        int best = -1;
+        float best_ms = 0.f, model_ms = 0.f;
+        for (int R = 2; R <= 7; ++R) {
+            const long B = 1L << R;
+            if (R > 2 && B / 2 >= nScan) break;
+            const long K = response_window(solver, (int)B, nInputs);
+            if (8.0 * ((double)B * nOutputs + np) * ((double)K + np) > 256e6) break;
+            const float ms = time_R(R);
+            if (R == Rdefault) model_ms = ms;
+            if (best < 0 || ms < best_ms) {
+                best = R;
+                best_ms = ms;
+            }
+        }
+        if (best < 0) throw Error(kInvalidSystem, "no block length fits the class");
+        if (model_ms == 0.f) model_ms = time_R(Rdefault);
+        tune_store(tune_class(solver, Ns, nInputs, nOutputs, nScan, precision), best, best_ms);
+        if (log2B) log2B[0] = best;
+        if (msBest) msBest[0] = best_ms;
+        if (msModel) msModel[0] = model_ms;
+    });
+    if (nErr) nErr[0] = rc;
+}
+
+int ParODE_TuneSave(const char* path, const char* gpuName, int nErr[])
+{
+    int n = 0;
+    int rc = guarded([&] {
+        if (!path) throw Error(kInvalidArgument, "no path");
+        const std::string text = tune_dump(gpu_key(gpuName));
+        std::ofstream f(path, std::ios::out | std::ios::trunc);
+        if (!f) throw Error(kInvalidArgument, "cannot write the tuning file");
+        f << text;
+        for (char c : text) n += c == '\n';
+    });
+    if (nErr) nErr[0] = rc;
+    return n;
+}
+
+int ParODE_TuneLoad(const char* path, const char* gpuName, int nErr[])
+{
+    int n = 0;
+    int rc = guarded([&] {
+        if (!path) throw Error(kInvalidArgument, "no path");
+        std::ifstream f(path);
+        if (!f) throw Error(kInvalidArgument, "cannot read the tuning file");
+        std::stringstream ss;
+        ss << f.rdbuf();
+        n = tune_load_text(ss.str(), gpu_key(gpuName));
+    });
+    if (nErr) nErr[0] = rc;
+    return n;
+}
+
+void ParODE_TuneClear() { tune_clear(); }
 
 }  // extern "C"

@@ -1,6 +1,7 @@
 // batch.cpp -- BatchPlan: set-up on the host (FP64 discretisation, one arena,
 // one staged copy), execution as a fixed sequence of batched launches.
 #include "batch.h"
+#include "tuner.h"
 
 #include "common.h"
 
@@ -142,7 +143,15 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             double cost = 0.0;
             // mixed: the window and aggregate products run on the tensor cores
             const double wweight = opt.precision == kMixed ? 0.25 : 1.0;
-            const int R = response_log2_block(q.solver, np, q.n, q.mu, q.p, q.nScan, wweight, opt.executions, &cost);
+            int R = response_log2_block(q.solver, np, q.n, q.mu, q.p, q.nScan, wweight, opt.executions, &cost);
+            // a block length forced by the caller or measured for this class of
+            // systems (tuner.h) replaces the cost model's
+            int Rt = opt.force_log2_block;
+            if (Rt < 2) Rt = tuned_log2_block(tune_class(q.solver, q.Ns, q.mu, q.p, q.nScan, opt.precision));
+            if (Rt >= 2 && Rt <= 7) {
+                while (Rt > 2 && (1L << Rt) / 2 >= q.nScan) --Rt;
+                R = Rt;
+            }
             const double sweeps = 4.0 * np * np;
             // a blocked bucket chains its tiles one after another: long
             // horizons go to the response leaf's level-synchronous block scan

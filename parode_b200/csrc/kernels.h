@@ -71,6 +71,14 @@ struct RespArgs {
     int fault_withhold = 0;  // test hook, as LevelArgs::fault_withhold
 };
 
+// The initial-state part of the block-response outputs (kernels_state.cu):
+// Y[b gs + r] = acc[b gs + r] + sum_k W[r ld + k] X[b NP + k] for r < M,
+// b < nblocks, b gs + r < limit (limit < 0: none).  Returns false when W's
+// M x NP state columns do not fit in shared memory (the caller then uses the
+// tiled GEMM).
+bool launch_state_out(int NP, const double* W, long ld, int M, const double* X, const double* acc, double* Y, long gs,
+                      long nblocks, long limit, int sms, cudaStream_t s);
+
 long resp_tc_tiles(const RespArgs& a);
 std::vector<long> resp_tc_ranges(const std::vector<RespArgs>& ents, int ctas);
 // Two tensor maps (hi plane, lo plane) of windows: row g starts at sample
@@ -150,11 +158,6 @@ int response_log2_block(int solver, int NP, int n, int m, int p, long nScan, dou
 // doubles.  Returns the launches made.
 int chunk_carry_levels(long count);
 long chunk_carry_scratch(long count);
-// The same carry as one cooperative launch with bounded grid-wide barriers
-// between its levels (bar: two zeroed words of device memory; a barrier wait
-// that gives up writes 2 into *status).
-int launch_chunk_carry_coop(int NP, double* items, long count, const double* P, int l0, const double* X0,
-                            double* work, unsigned* bar, int* status, int sms, cudaStream_t s);
 int launch_chunk_carry(int NP, double* items, long count, const double* P, int l0, const double* X0, double* work,
                        cudaStream_t s);
 

@@ -26,9 +26,6 @@ namespace parode {
 namespace {
 
 constexpr int kThreads = 256;
-// rows of the output table C Phi^j staged per pass of the fix-up (64 KB)
-template <int NP>
-__host__ __device__ constexpr int fixup_chunk_rows() { return 8192 / NP; }
 
 __device__ __forceinline__ int fold(int r) { return r ^ (r >> 2) ^ (r >> 4) ^ (r >> 6) ^ (r >> 8) ^ (r >> 10) ^ (r >> 12); }
 
@@ -528,56 +525,48 @@ template <int NP>
 __device__ void fixup_body(double* Y, long ybase, long nScan, int p, const double* CP, const double* X, int B,
                            long cta, long ncta, double* sm)
 {
+    // work items: (8 fragment rows of CP, 8 blocks); one warp per item, so
+    // few long blocks (small systems) spread over rows as many short blocks
+    // spread over columns.  CP (B p x NP) is small and read through L2.
+    (void)sm;
     const int M = B * p;
-    const int Mp = (M + 7) & ~7;
-    const int rfs = Mp >> 3;
-    const int chunk_rf = fixup_chunk_rows<NP>() / 8;  // fragment rows of CP staged at a time
-    double* sCP = sm;                          // chunk x NP, swizzled
+    const int rfs = (M + 7) >> 3;
+    const int rgs = (rfs + 7) >> 3;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int gq = lane >> 2, tq = lane & 3;
     const long nblocks = (nScan + B - 1) / B;
     const long cfs = (nblocks + 7) >> 3;
-    for (int rc0 = 0; rc0 < rfs; rc0 += chunk_rf) {
-        const int rc1 = min(rfs, rc0 + chunk_rf);
-        __syncthreads();
-        for (int e = threadIdx.x; e < (rc1 - rc0) * 8 * NP; e += kThreads) {
-            int r = e / NP, k = e - r * NP;
-            int rg = rc0 * 8 + r;
-            sCP[sidx<NP>(r, k)] = rg < M ? CP[(long)rg * NP + k] : 0.0;
-        }
-        __syncthreads();
-    // a warp owns 8 blocks (one fragment column): their carries are loaded
-    // once per CP chunk as B fragments and reused for every fragment row
-    for (long cb = cta * 8 + warp; cb < cfs; cb += ncta * 8) {
+    const long items = (long)rgs * cfs;
+    for (long it = cta * (kThreads / 32) + warp; it < items; it += ncta * (kThreads / 32)) {
+        const long cb = it % cfs;
+        const int rb0 = (int)(it / cfs) * 8;
         const long bb = cb * 8 + gq;
         double bv[NP / 4];
 #pragma unroll
         for (int k = 0; k < NP; k += 4) bv[k / 4] = bb < nblocks ? X[bb * NP + k + tq] : 0.0;
-        for (int rb0 = rc0; rb0 < rc1; rb0 += 8) {
-            double acc[8][2];
+        double acc[8][2];
 #pragma unroll
-            for (int r = 0; r < 8; ++r) acc[r][0] = acc[r][1] = 0.0;
+        for (int r = 0; r < 8; ++r) acc[r][0] = acc[r][1] = 0.0;
 #pragma unroll
-            for (int k = 0; k < NP; k += 4)
-#pragma unroll
-                for (int r = 0; r < 8; ++r)
-                    if (rb0 + r < rc1)
-                        dmma_m8n8k4(acc[r][0], acc[r][1], sCP[sidx<NP>((rb0 + r - rc0) * 8 + gq, k + tq)],
-                                    bv[k / 4]);
+        for (int k = 0; k < NP; k += 4)
 #pragma unroll
             for (int r = 0; r < 8; ++r) {
                 const int row = (rb0 + r) * 8 + gq;
-                if (rb0 + r >= rc1 || row >= M) continue;
-                const int jj = row / p, o = row - jj * p;
+                const double a = (rb0 + r < rfs && row < M) ? CP[(long)row * NP + k + tq] : 0.0;
+                dmma_m8n8k4(acc[r][0], acc[r][1], a, bv[k / 4]);
+            }
 #pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    const long b = cb * 8 + 2 * tq + e;
-                    const long j = b * B + jj;
-                    if (b < nblocks && j < nScan) Y[(ybase + j) * p + o] += acc[r][e];
-                }
+        for (int r = 0; r < 8; ++r) {
+            const int row = (rb0 + r) * 8 + gq;
+            if (rb0 + r >= rfs || row >= M) continue;
+            const int jj = row / p, o = row - jj * p;
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const long b = cb * 8 + 2 * tq + e;
+                const long j = b * B + jj;
+                if (b < nblocks && j < nScan) Y[(ybase + j) * p + o] += acc[r][e];
             }
         }
-    }
     }
 }
 
@@ -845,13 +834,11 @@ template <int NP>
 static void fixup_t(const BlockedShape& sh, double* Y, long ybase, long nScan, int p, const double* CP,
                     const double* X, cudaStream_t s)
 {
-    const int Mp = (sh.B * p + 7) & ~7;
-    size_t smem = (size_t)std::min(Mp, fixup_chunk_rows<NP>()) * NP * sizeof(double);
-    set_smem(k_fixup<NP>, smem);
-    long nblocks = (nScan + sh.B - 1) / sh.B;
-    long cfs = (nblocks + 7) / 8;
-    unsigned grid = (unsigned)std::max<long>(1, std::min<long>((cfs + 7) / 8, 148L * 4));
-    k_fixup<NP><<<grid, kThreads, smem, s>>>(Y, ybase, nScan, p, CP, X, sh.B);
+    const long rgs = ((sh.B * p + 7) / 8 + 7) / 8;
+    const long nblocks = (nScan + sh.B - 1) / sh.B;
+    const long items = rgs * ((nblocks + 7) / 8);
+    const unsigned grid = (unsigned)std::max<long>(1, std::min<long>((items + 7) / 8, 148L * 8));
+    k_fixup<NP><<<grid, kThreads, 0, s>>>(Y, ybase, nScan, p, CP, X, sh.B);
     PARODE_CUDA(cudaGetLastError());
 }
 
@@ -937,13 +924,11 @@ static void batch_t(int what, const BlockedShape& sh, const BatchLaunch& b, cuda
         k_chain_batch<NP><<<b.nsys, kThreads, 0, s>>>(b.sys, b.X0s, sh.R, sh.S / sh.B);
         break;
     case 3: {
-        const int Mp = (sh.B * b.pmax + 7) & ~7;
-        size_t smem = (size_t)std::min(Mp, fixup_chunk_rows<NP>()) * NP * sizeof(double);
-        set_smem(k_fixup_batch<NP>, smem);
-        long cfs = (b.max_blocks + 7) / 8;
-        unsigned gx = (unsigned)std::max<long>(1, std::min<long>((cfs + 7) / 8, 16));
+        const long rgs = ((sh.B * b.pmax + 7) / 8 + 7) / 8;
+        const long items = rgs * ((b.max_blocks + 7) / 8);
+        const unsigned gx = (unsigned)std::max<long>(1, std::min<long>((items + 7) / 8, 16));
         dim3 grid(gx, (unsigned)b.nsys);
-        k_fixup_batch<NP><<<grid, kThreads, smem, s>>>(b.sys, b.CPs, sh.B);
+        k_fixup_batch<NP><<<grid, kThreads, 0, s>>>(b.sys, b.CPs, sh.B);
         break;
     }
     }

@@ -237,120 +237,6 @@ __global__ void __launch_bounds__(kThreads) k_chunk_down(double* __restrict__ it
 }
 
 // ---------------------------------------------------------------------------
-// The whole carry as one cooperative launch: the levels above run one after
-// the other, separated by grid-wide barriers instead of kernel boundaries
-// (the upper levels have a few CTAs' work each, so the launch gaps were most
-// of their time).  The barrier is a generation counter: each CTA's thread 0
-// makes the CTA's writes visible, arrives on a counter that wraps to zero at
-// the grid size, and the last one to arrive bumps the generation; the others
-// spin on it with a bound (about a second), after which they record status 2,
-// skip the rest of the work and return.  All CTAs are co-resident (the
-// launch is cooperative).
-// ---------------------------------------------------------------------------
-
-struct CarryLevels {
-    int H = 0;   // levels below the top
-    int l0 = 0;  // power-table level of Q = Phi^B
-    long cnt[16] = {};
-    double* arr[16] = {};
-};
-
-constexpr long long kBarrierWait = 1LL << 31;  // SM cycles
-
-__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* status, bool& ok)
-{
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile unsigned* gen = bar + 1;
-        const unsigned g0 = *gen;
-        __threadfence();
-        const unsigned prev = atomicInc(bar, gridDim.x - 1);  // wraps to 0 for the last arrival
-        if (prev == gridDim.x - 1) {
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            const long long t0 = clock64();
-            while (*gen == g0) {
-                if (clock64() - t0 > kBarrierWait) {
-                    atomicExch(status, 2);
-                    ok = false;
-                    break;
-                }
-                __nanosleep(64);
-            }
-        }
-        __threadfence();
-    }
-    __syncthreads();
-    // every thread learns whether its CTA gave up (thread 0 wrote ok)
-    __shared__ int flag;
-    if (threadIdx.x == 0) flag = ok ? 1 : 0;
-    __syncthreads();
-    ok = flag != 0;
-    __syncthreads();
-    return ok;
-}
-
-template <int NP>
-__global__ void __launch_bounds__(kThreads) k_carry_coop(CarryLevels L, const double* __restrict__ P,
-                                                          const double* __restrict__ X0, unsigned* bar, int* status)
-{
-    __shared__ double Xs[2][NP * kLd];
-    const long mat = (long)NP * NP;
-    bool ok = true;
-    for (int h = 0; h < L.H && ok; ++h) {
-        const long nc = (L.cnt[h] + kChunk - 1) / kChunk;
-        const long tiles = (nc + kCols - 1) / kCols;
-        for (long t = blockIdx.x; t < tiles; t += gridDim.x)
-            chunk_up_tile<NP>(L.arr[h], L.cnt[h], P + (long)(L.l0 + 4 * h) * mat, L.arr[h + 1], t, Xs[0], Xs[1]);
-        if (!grid_barrier(bar, status, ok)) return;
-    }
-    if (!ok) return;
-    // top: one chunk of the remaining items, entered with the initial state
-    if (blockIdx.x == 0)
-        chunk_down_tile<NP>(L.arr[L.H], L.cnt[L.H], P + (long)(L.l0 + 4 * L.H) * mat, X0, (int)L.cnt[L.H], 0,
-                            Xs[0], Xs[1]);
-    for (int h = L.H - 1; h >= 0; --h) {
-        if (!grid_barrier(bar, status, ok)) return;
-        const long nc = (L.cnt[h] + kChunk - 1) / kChunk;
-        const long tiles = (nc + kCols - 1) / kCols;
-        for (long t = blockIdx.x; t < tiles; t += gridDim.x)
-            chunk_down_tile<NP>(L.arr[h], L.cnt[h], P + (long)(L.l0 + 4 * h) * mat, L.arr[h + 1], kChunk, t, Xs[0],
-                                Xs[1]);
-    }
-}
-
-template <int NP>
-int chunk_carry_coop_t(double* items, long count, const double* P, int l0, const double* X0, double* work,
-                       unsigned* bar, int* status, int sms, cudaStream_t s)
-{
-    CarryLevels L;
-    L.l0 = l0;
-    L.arr[0] = items;
-    L.cnt[0] = count;
-    double* w = work;
-    long tiles_max = 1;
-    while (L.cnt[L.H] > kChunk) {
-        if (L.H + 1 >= 16) throw Error(kInvalidArgument, "chunk carry: too many levels");
-        const long nc = (L.cnt[L.H] + kChunk - 1) / kChunk;
-        tiles_max = std::max(tiles_max, (nc + kCols - 1) / kCols);
-        L.arr[L.H + 1] = w;
-        L.cnt[L.H + 1] = nc;
-        w += nc * NP;
-        ++L.H;
-    }
-    // one CTA per SM: each tile's steps run at its SM's full FP64 tensor
-    // rate, and few CTAs wait at the barriers while an upper level runs
-    int per_sm = 0;
-    PARODE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_carry_coop<NP>, kThreads, 0));
-    if (per_sm < 1) throw Error(kDeviceError, "chunk carry: the cooperative kernel does not fit an SM");
-    const long grid = std::max<long>(1, std::min<long>(tiles_max, (long)sms));
-    void* args[] = {(void*)&L, (void*)&P, (void*)&X0, (void*)&bar, (void*)&status};
-    PARODE_CUDA(cudaLaunchCooperativeKernel((const void*)k_carry_coop<NP>, dim3((unsigned)grid), dim3(kThreads), args,
-                                            0, s));
-    return 1;
-}
-
 template <int NP>
 int chunk_carry_t(double* items, long count, const double* P, int l0, const double* X0, double* work, cudaStream_t s)
 {
@@ -408,23 +294,6 @@ long chunk_carry_scratch(long count)
         total += count;
     }
     return total;
-}
-
-int launch_chunk_carry_coop(int NP, double* items, long count, const double* P, int l0, const double* X0,
-                            double* work, unsigned* bar, int* status, int sms, cudaStream_t s)
-{
-    if (count <= 0) return 0;
-    switch (NP) {
-    case 8: return chunk_carry_coop_t<8>(items, count, P, l0, X0, work, bar, status, sms, s);
-    case 16: return chunk_carry_coop_t<16>(items, count, P, l0, X0, work, bar, status, sms, s);
-    case 24: return chunk_carry_coop_t<24>(items, count, P, l0, X0, work, bar, status, sms, s);
-    case 32: return chunk_carry_coop_t<32>(items, count, P, l0, X0, work, bar, status, sms, s);
-    case 40: return chunk_carry_coop_t<40>(items, count, P, l0, X0, work, bar, status, sms, s);
-    case 48: return chunk_carry_coop_t<48>(items, count, P, l0, X0, work, bar, status, sms, s);
-    case 56: return chunk_carry_coop_t<56>(items, count, P, l0, X0, work, bar, status, sms, s);
-    case 64: return chunk_carry_coop_t<64>(items, count, P, l0, X0, work, bar, status, sms, s);
-    default: throw Error(kInvalidArgument, "chunk carry: NP must be a multiple of 8 up to 64");
-    }
 }
 
 int launch_chunk_carry(int NP, double* items, long count, const double* P, int l0, const double* X0, double* work,

@@ -5,6 +5,7 @@
 #include "common.h"
 #include "general.h"
 #include "kernels.h"
+#include "tuner.h"
 
 #include <algorithm>
 #include <cstring>
@@ -105,8 +106,18 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
                 br_ = true;
                 br_tc_ = opt.precision == kMixed;
                 if (br_tc_) precision_used_ = kMixed;
-                brK_ = K;
-                brKpad_ = (K + 1) & ~1;
+                // a block length forced by the caller or measured for this
+                // class of systems (tuner.h) replaces the shape's default
+                int Rt = opt.force_log2_block;
+                if (Rt < 2) Rt = tuned_log2_block(tune_class(solver, Ns_, mu_, p_, nScan_, opt.precision));
+                if (Rt >= 2 && Rt <= 7) {
+                    while (Rt > 2 && (1L << Rt) / 2 >= nScan_) --Rt;
+                    shape_.R = Rt;
+                    shape_.B = 1 << Rt;
+                }
+                const int Kb = response_window(solver, shape_.B, mu_);
+                brK_ = Kb;
+                brKpad_ = (Kb + 1) & ~1;
                 nblocks_ = (nScan_ + shape_.B - 1) / shape_.B;
                 // the chunked carry over blocks reads P_R .. P_{R + 4 h}
                 levels_ = shape_.R + 4 * chunk_carry_levels(nblocks_) + 1;
@@ -177,13 +188,9 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
     alloc(&dX0_, Np_);
     {
         double* st = nullptr;
-        alloc(&st, 2);
+        alloc(&st, 1);
         dStatus_ = reinterpret_cast<int*>(st);
-        dBar_ = reinterpret_cast<unsigned*>(st + 1);
-        PARODE_CUDA(cudaMemsetAsync(st, 0, 2 * sizeof(double), stream_));
-        int coop = 0;
-        PARODE_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device_));
-        coop_ = coop != 0;
+        PARODE_CUDA(cudaMemsetAsync(st, 0, sizeof(double), stream_));
     }
     if (path_ == kPathLevel || path_ == kPathGeneral) {
         alloc(&dV_, (Tp_ + 1) * (long)Np_);  // a leading slot holds the initial state
@@ -663,13 +670,8 @@ void Plan::execute_general(double* Y, cudaStream_t s)
 
 int Plan::carry(cudaStream_t s)
 {
-    // the exclusive scan of the block aggregates: one cooperative launch whose
-    // levels are separated by grid barriers (its two barrier words are reset
-    // first), or the chain of per-level launches where cooperative launch is
-    // not available
-    if (!coop_) return launch_chunk_carry(Np_, dG_, nblocks_, dPow_, shape_.R, dX0_, dWork_, s);
-    PARODE_CUDA(cudaMemsetAsync(dBar_, 0, 2 * sizeof(unsigned), s));
-    return launch_chunk_carry_coop(Np_, dG_, nblocks_, dPow_, shape_.R, dX0_, dWork_, dBar_, dStatus_, sms_, s);
+    // the exclusive scan of the block aggregates (kernels_carry.cu)
+    return launch_chunk_carry(Np_, dG_, nblocks_, dPow_, shape_.R, dX0_, dWork_, s);
 }
 
 void Plan::execute_response(double* Y, cudaStream_t s)
@@ -695,22 +697,27 @@ void Plan::execute_response(double* Y, cudaStream_t s)
         mark("aggregates+windows", s);
         launches += carry(s);
         mark("carry", s);
-        LevelArgs x;
-        x.P = dW_ + brKpad_;
-        x.ldp = ld;
-        x.Np = Np_;
-        x.M = shape_.B * p_;
-        x.K = Np_;
-        x.ncols = nblocks_;
-        x.src = dG_;
-        x.src_gs = Np_;
-        x.src_ks = 1;
-        x.acc = dY_ + ybase * p_;
-        x.acc_gs = (long)shape_.B * p_;
-        x.dst = Y + ybase * p_;
-        x.dst_gs = (long)shape_.B * p_;
-        x.dst_limit = nScan_ * p_;
-        launch_gemm_tiled(x, s);
+        // y = windows + (C Phi^j) X_b: W's state columns stay in shared
+        // memory (kernels_state.cu); the general tiled GEMM where they do not fit
+        if (!launch_state_out(Np_, dW_ + brKpad_, ld, shape_.B * p_, dG_, dY_ + ybase * p_, Y + ybase * p_,
+                              (long)shape_.B * p_, nblocks_, nScan_ * p_, sms_, s)) {
+            LevelArgs x;
+            x.P = dW_ + brKpad_;
+            x.ldp = ld;
+            x.Np = Np_;
+            x.M = shape_.B * p_;
+            x.K = Np_;
+            x.ncols = nblocks_;
+            x.src = dG_;
+            x.src_gs = Np_;
+            x.src_ks = 1;
+            x.acc = dY_ + ybase * p_;
+            x.acc_gs = (long)shape_.B * p_;
+            x.dst = Y + ybase * p_;
+            x.dst_gs = (long)shape_.B * p_;
+            x.dst_limit = nScan_ * p_;
+            launch_gemm_tiled(x, s);
+        }
         ++launches;
         if (solver_ == kABM)
             PARODE_CUDA(cudaMemcpyAsync(Y, dYpre_, sizeof(double) * 3 * p_, cudaMemcpyDeviceToDevice, s));

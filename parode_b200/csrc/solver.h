@@ -47,6 +47,9 @@ struct PlanOptions {
     // test hook (PARODE_OPT_FAULT_WITHHOLD): the mixed response kernel's
     // first CTA withholds one pipeline arrive, so its bounded waits give up
     bool fault_withhold = false;
+    // block-response leaf: log2 of the block length (0: the tuned value of
+    // the system's class, else the cost model's / the shape's default)
+    int force_log2_block = 0;
 };
 
 class Plan {
@@ -138,8 +141,6 @@ private:
     long* dTcCta_ = nullptr;    // device: tile ranges of the persistent CTAs
     int tcCtas_ = 0;
     int* dStatus_ = nullptr;
-    unsigned* dBar_ = nullptr;  // grid-barrier words of the single-launch carry
-    bool coop_ = false;         // the carry runs as one cooperative launch
     cudaStream_t side_ = nullptr;
     cudaEvent_t fork_[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t done_ = nullptr;  // recorded after each execute on its stream

@@ -98,6 +98,24 @@ def test_fault_injection_options_round_trip():
     pb.set_option(pb.OPT_FAULT_WITHHOLD, 0)
 
 
+def test_tuning_file_round_trip(tmp_path):
+    """Entries of one GPU survive save and load; other GPUs' lines are skipped."""
+    import parode_b200 as pb
+
+    src = tmp_path / "tune.txt"
+    src.write_text("NVIDIA_B200 0 64 8 8 20 1 5 0.25\nNVIDIA_B200 1 128 2 2 16 0 3 1.5\n"
+                   "Other_GPU 0 64 8 8 20 1 6 0.2\nbad line\n")
+    pb.tune_clear()
+    assert pb.tune_load(str(src), gpu="NVIDIA B200") == 2
+    out = tmp_path / "out.txt"
+    assert pb.tune_save(str(out), gpu="NVIDIA B200") == 2
+    lines = sorted(out.read_text().split("\n"))
+    assert [ln.split()[:8] for ln in lines if ln] == [
+        ["NVIDIA_B200", "0", "64", "8", "8", "20", "1", "5"], ["NVIDIA_B200", "1", "128", "2", "2", "16", "0", "3"]]
+    pb.tune_clear()
+    assert pb.tune_save(str(out), gpu="NVIDIA B200") == 0
+
+
 def test_not_initialised_errors():
     import parode_b200 as pb
 
