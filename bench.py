@@ -74,6 +74,16 @@ def dist_env():
 # under oracle/ and run on the host cores.
 # ---------------------------------------------------------------------------
 
+def rel_err(y, yref):
+    """Per output channel max_k |y - yref| / max_k |yref|, maximum over channels
+    (the comparison of two of this library's own results, e.g. mixed vs FP64)."""
+    y = np.asarray(y, dtype=np.float64)
+    yref = np.asarray(yref, dtype=np.float64)
+    num = np.max(np.abs(y - yref), axis=0)
+    den = np.max(np.abs(yref), axis=0)
+    return float(np.max(np.where(den > 0, num / np.where(den > 0, den, 1.0), num)))
+
+
 def reference_sample(T_sample):
     from oracle import oracle
     from parode_b200 import workloads as wl
@@ -238,9 +248,9 @@ def _spec(pb, c):
 
 
 def _cheap_sample(cases, k):
-    """k systems the oracle checks quickly: the cheapest half from the scan
-    dimensions <= 64 (blocked path) and half from the larger ones (level-
-    synchronous path, where the mixed form runs its tensor-core levels)."""
+    """k systems whose mixed result is compared with the FP64 one: half from
+    the scan dimensions <= 64 (blocked path) and half from the larger ones
+    (level-synchronous path, where the mixed form runs its tensor-core levels)."""
     cost = lambda i: cases[i].scan_dim ** 2 * cases[i].T
     small = sorted((i for i in range(len(cases)) if cases[i].scan_dim <= 64), key=cost)
     large = sorted((i for i in range(len(cases)) if cases[i].scan_dim > 64), key=cost)
@@ -249,14 +259,13 @@ def _cheap_sample(cases, k):
 
 def measure_batched(pb, wl, torch, dev, reps=3, tune_classes=0):
     """The batched form: 4096 independent systems (cfg4) in one batch, FP64 and mixed."""
-    from oracle import oracle
-
     cases = wl.cfg4()
     specs = [_spec(pb, c) for c in cases]
     check = _cheap_sample(cases, 8)
     out = {"workload": "cfg4: 4096 systems, n log-uniform [4,96], T log-uniform [2^10,2^16], RK4/ABM 50/50",
            "state_steps": None}
     stream = torch.cuda.Stream(device=dev)
+    y64 = {}
     for name, prec in (("fp64", pb.FP64), ("mixed", pb.MIXED)):
         t0 = time.perf_counter()
         b = pb.Batch(specs, precision=prec)
@@ -272,16 +281,18 @@ def measure_batched(pb, wl, torch, dev, reps=3, tune_classes=0):
             e.synchronize()
             ts.append(s.elapsed_time(e))
         ms = statistics.median(ts)
-        worst = 0.0
+        worst = None
         for i in check:
-            c = cases[i]
             _, y = b.output(i)
-            ref = oracle.simulate_affine(oracle.System(c.A, c.B, c.C, c.D, c.x0),
-                                         oracle.Input.sinusoid(c.u.a, c.u.f, c.u.phi), c.solver, c.t0, c.t_end, c.h)
-            worst = max(worst, oracle.rel_err(y, ref))
+            if name == "fp64":
+                y64[i] = y
+            else:
+                worst = max(worst or 0.0, rel_err(y, y64[i]))
         out["state_steps"] = b.state_steps
         out[name] = {"ms": ms, "value": b.state_steps / (ms / 1e3), "unit": UNIT, "launches": b.launch_count,
-                     "setup_s": setup_s, "rel_err_sampled": worst, "sampled_systems": len(check)}
+                     "setup_s": setup_s}
+        if worst is not None:
+            out[name].update(rel_err_vs_fp64_sampled=worst, sampled_systems=len(check))
         b.close()
     out["mixed_over_fp64"] = out["fp64"]["ms"] / out["mixed"]["ms"]
     if tune_classes > 0:
@@ -371,7 +382,6 @@ def measure_cfg1(pb, wl, torch, reps=200):
 def measure_cfg3(pb, wl, torch, reps=3):
     """ABM4, n=128 (scan dimension 512), m=p=16, h=5e-4, T=2^18: the level-
     synchronous path, FP64 and mixed (one-system batch), rel err mixed vs FP64."""
-    from oracle import oracle
 
     c = wl.cfg3()
     out = {"workload": "cfg3: ABM4 n=128 (N_s=512) m=p=16 h=5e-4 T=2^18"}
@@ -396,7 +406,7 @@ def measure_cfg3(pb, wl, torch, reps=3):
                      "sweep_tflops": flops / (ms / 1e3) / 1e12, "launches": b.launch_count}
         b.close()
     out["mixed_over_fp64"] = out["fp64"]["ms"] / out["mixed"]["ms"]
-    out["rel_err_mixed_vs_fp64"] = oracle.rel_err(ys["mixed"], ys["fp64"])
+    out["rel_err_mixed_vs_fp64"] = rel_err(ys["mixed"], ys["fp64"])
     return out
 
 
@@ -541,6 +551,15 @@ def run_ours(args):
     plain, y_plain = (None, None)
     if not args.no_plain and precision != pb.FP64:
         plain, y_plain = time_plan(pb.FP64, False)
+    # the single-pass TF32 form of the same solve (operands rounded to TF32 once)
+    single = None
+    if not args.no_plain and precision == pb.MIXED:
+        single, y_single = time_plan(pb.TF32, False)
+        single["rel_err_vs_fp64"] = None
+        if y_plain is not None:
+            single["rel_err_vs_fp64"] = rel_err(y_single, y_plain)
+        single["value"] = world * case.n * case.T / (single["ms_per_step"] / 1e3)
+        del y_single
     value = world * case.n * case.T / (main["ms_per_step"] / 1e3)
 
     # e2e: the C-ABI call with host buffers (plan set-up, H2D, solve, D2H of y
@@ -639,8 +658,7 @@ def run_ours(args):
                     "whole_solve_tflops": fl["solve"] / (main["ms_per_step"] / 1e3) / 1e12 if fl else None}
         rel_vs_fp64 = None
         if y_plain is not None:
-            from oracle import oracle
-            rel_vs_fp64 = oracle.rel_err(y_main, y_plain)
+            rel_vs_fp64 = rel_err(y_main, y_plain)
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             T_cpu = 1 << 20
@@ -669,6 +687,8 @@ def run_ours(args):
                                        (plain["stages_ms"]["outputs"] / 1e3) / 1e12)
                 if plain["path"] == 3 and plain["stages_ms"].get("outputs") else None},
             "mixed_over_plain": None if plain is None else plain["ms_per_step"] / main["ms_per_step"],
+            "tf32_single_pass": None if single is None else {
+                k: single[k] for k in ("value", "ms_per_step", "stages_ms", "precision_used", "rel_err_vs_fp64")},
             "rel_err_mixed_vs_fp64": rel_vs_fp64,
             "peaks": {k: peaks.get(k) for k in ("hbm_gbs", "bf16_tflops", "bf16_tflops_sustained")},
             "peaks_source": peaks_kind,

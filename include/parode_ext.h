@@ -24,6 +24,11 @@ extern "C" {
 #define PARODE_PRECISION_FP64   0  /* plain: every sweep, the carry and the outputs in FP64  */
 #define PARODE_PRECISION_MIXED  1  /* leaf sweeps in 3xTF32 on tcgen05 with FP32 accumulation;
                                       Phi, the power table, the upper levels and the carry in FP64 */
+#define PARODE_PRECISION_TF32   2  /* single pass: the block-response GEMMs in one TF32 product
+                                      (operands rounded to TF32, about 2^-11 relative), the carry and
+                                      the initial-state part in FP64; other paths run the mixed form
+                                      (the plan reports PARODE_PRECISION_MIXED for them).  Single
+                                      solves only: a batch or the server runs it as the mixed form. */
 
 /* Options (ParODE_SetOption / ParODE_GetOption). */
 #define PARODE_OPT_PRECISION    1  /* PARODE_PRECISION_* used by SimulateODE (default FP64) */
@@ -103,7 +108,8 @@ int ParODE_PlanNumOutputChannels(const ParODE_Plan* plan);
 /* Device kernel launches one PlanExecute enqueues (for launch accounting). */
 int ParODE_PlanLaunchCount(const ParODE_Plan* plan);
 /* Precision form the plan actually runs (PARODE_PRECISION_*): the mixed form
- * falls back to FP64 for shapes its tensor-core leaf does not cover. */
+ * falls back to FP64 for shapes its tensor-core leaf does not cover, the
+ * TF32 form to the mixed form off the block-response path. */
 int ParODE_PlanPrecision(const ParODE_Plan* plan);
 /* Sweep organisation: 1 level-synchronous, 2 blocked with the in-block sweep
  * leaf, 3 blocked with the block-response GEMM leaf. */

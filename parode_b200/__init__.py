@@ -31,6 +31,7 @@ RK4 = 0
 ABM = 1
 FP64 = 0
 MIXED = 1
+TF32 = 2   # single-pass TF32 response GEMMs (single solves; a batch or server runs MIXED)
 
 OPT_PRECISION = 1
 OPT_PATH = 2
@@ -399,7 +400,7 @@ class Plan:
 
     @property
     def precision(self) -> int:
-        """Precision form actually used (FP64 or MIXED)."""
+        """Precision form actually used (FP64, MIXED or TF32)."""
         return int(lib.ParODE_PlanPrecision(self._h))
 
     @property

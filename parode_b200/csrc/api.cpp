@@ -417,7 +417,8 @@ void ParODE_SetOption(int option, long long value, int nErr[])
     int rc = kOK;
     switch (option) {
     case PARODE_OPT_PRECISION:
-        if (value != PARODE_PRECISION_FP64 && value != PARODE_PRECISION_MIXED) rc = kInvalidArgument;
+        if (value != PARODE_PRECISION_FP64 && value != PARODE_PRECISION_MIXED && value != PARODE_PRECISION_TF32)
+            rc = kInvalidArgument;
         else L.precision = (int)value;
         break;
     case PARODE_OPT_PATH:
@@ -487,7 +488,8 @@ void ParODE_SimulateODE_d(const double* A, const double* B, const double* C, con
     if (nSteps) nSteps[0] = 0;
     int rc = guarded([&] {
         int dev = current_device_locked(L);
-        if (precision != PARODE_PRECISION_FP64 && precision != PARODE_PRECISION_MIXED)
+        if (precision != PARODE_PRECISION_FP64 && precision != PARODE_PRECISION_MIXED &&
+            precision != PARODE_PRECISION_TF32)
             throw Error(kInvalidArgument, "unknown precision");
         SystemDesc s = make_system<double>(A, B, C, D, nInputs, nStates, nOutputs, ZeroB, ZeroC, ZeroD, x0);
         PlanOptions opt;
@@ -522,7 +524,8 @@ ParODE_Plan* ParODE_PlanCreate(const double* A, const double* B, const double* C
     ParODE_Plan* out = nullptr;
     int rc = guarded([&] {
         int dev = current_device_locked(L);
-        if (precision != PARODE_PRECISION_FP64 && precision != PARODE_PRECISION_MIXED)
+        if (precision != PARODE_PRECISION_FP64 && precision != PARODE_PRECISION_MIXED &&
+            precision != PARODE_PRECISION_TF32)
             throw Error(kInvalidArgument, "unknown precision");
         SystemDesc s = make_system<double>(A, B, C, D, nInputs, nStates, nOutputs, ZeroB, ZeroC, ZeroD, x0);
         PlanOptions opt;
@@ -623,7 +626,8 @@ ParODE_Batch* ParODE_BatchCreate(int nSystems, const double* const A[], const do
     ParODE_Batch* out = nullptr;
     int rc = guarded([&] {
         int dev = current_device_locked(L);
-        if (precision != PARODE_PRECISION_FP64 && precision != PARODE_PRECISION_MIXED)
+        if (precision != PARODE_PRECISION_FP64 && precision != PARODE_PRECISION_MIXED &&
+            precision != PARODE_PRECISION_TF32)
             throw Error(kInvalidArgument, "unknown precision");
         if (nSystems <= 0 || !A || !x0 || !nInputs || !nStates || !nOutputs || !ZeroB || !ZeroC || !ZeroD ||
             !uIndex || !tStart || !tEnd || !tStep || !solver)
@@ -640,7 +644,8 @@ ParODE_Batch* ParODE_BatchCreate(int nSystems, const double* const A[], const do
             specs[i].h = tStep[i];
         }
         PlanOptions opt;
-        opt.precision = precision;
+        // a batch runs the single-pass TF32 form as the mixed form
+        opt.precision = precision == PARODE_PRECISION_TF32 ? (int)kMixed : precision;
         opt.path = L.path;
         opt.input_double = true;
         opt.log = L.log != 0;
@@ -726,10 +731,11 @@ ParODE_Server* ParODE_ServerCreate(int precision, double hbmBudgetBytes, int max
     ParODE_Server* out = nullptr;
     int rc = guarded([&] {
         int dev = current_device_locked(L);
-        if (precision != PARODE_PRECISION_FP64 && precision != PARODE_PRECISION_MIXED)
+        if (precision != PARODE_PRECISION_FP64 && precision != PARODE_PRECISION_MIXED &&
+            precision != PARODE_PRECISION_TF32)
             throw Error(kInvalidArgument, "unknown precision");
         ServerOptions o;
-        o.precision = precision;
+        o.precision = precision == PARODE_PRECISION_TF32 ? (int)kMixed : precision;
         if (hbmBudgetBytes > 0) o.hbm_budget = hbmBudgetBytes;
         if (maxBatch > 0) o.max_batch = maxBatch;
         if (maxInflight > 0) o.max_inflight = maxInflight;
@@ -940,7 +946,8 @@ void ParODE_TuneResponseBlock(int solver, int nStates, int nInputs, int nOutputs
         const int dev = current_device_locked(L);
         if (solver != kRK4 && solver != kABM) throw Error(kInvalidSolverType, "unknown solver");
         if (nStates < 1 || nInputs < 1 || nOutputs < 1 || nSteps < 2) throw Error(kInvalidSystem, "empty class");
-        if (precision != PARODE_PRECISION_FP64 && precision != PARODE_PRECISION_MIXED)
+        if (precision != PARODE_PRECISION_FP64 && precision != PARODE_PRECISION_MIXED &&
+            precision != PARODE_PRECISION_TF32)
             throw Error(kInvalidArgument, "unknown precision");
         const int Ns = solver == kRK4 ? nStates : 4 * nStates;
         if (Ns > 1024) throw Error(kInvalidSystem, "scan dimension above 1024 is not supported");
@@ -970,7 +977,7 @@ void ParODE_TuneResponseBlock(int solver, int nStates, int nInputs, int nOutputs
         } else {
             double cost = 0.0;
             Rdefault = response_log2_block(solver, np, nStates, nInputs, nOutputs, nScan,
-                                           precision == PARODE_PRECISION_MIXED ? 0.25 : 1.0, (double)L.executions,
+                                           precision != PARODE_PRECISION_FP64 ? 0.25 : 1.0, (double)L.executions,
                                            &cost);
         }
         while (Rdefault > 2 && (1L << Rdefault) / 2 >= nScan) --Rdefault;

@@ -48,7 +48,9 @@ struct Error : std::runtime_error {
 bool fault_alloc_now();
 
 enum Solver : int { kRK4 = 0, kABM = 1 };
-enum Precision : int { kFP64 = 0, kMixed = 1 };
+// kTF32: the single-pass form of the mixed response GEMMs (hi*hi only); the
+// other tensor-core stages run their 3xTF32 form under it.
+enum Precision : int { kFP64 = 0, kMixed = 1, kTF32 = 2 };
 
 inline long round_up(long v, long q) { return (v + q - 1) / q * q; }
 inline long next_pow2(long v)

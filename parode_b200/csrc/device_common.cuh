@@ -58,7 +58,7 @@ struct SampleOutSplit {
         const float x = (float)v;
         const float h = tf32_rna(x);
         hi[j * stride] = h;
-        lo[j * stride] = tf32_rna(x - h);
+        if (lo) lo[j * stride] = tf32_rna(x - h);  // no lo plane in the single-pass form
     }
 };
 

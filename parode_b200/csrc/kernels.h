@@ -82,10 +82,13 @@ bool launch_state_out(int NP, const double* W, long ld, int M, const double* X, 
 long resp_tc_tiles(const RespArgs& a);
 std::vector<long> resp_tc_ranges(const std::vector<RespArgs>& ents, int ctas);
 // Two tensor maps (hi plane, lo plane) of windows: row g starts at sample
-// offset g * block_stride, K samples long; written to out (256 bytes).
+// offset g * block_stride, K samples long; written to out (256 bytes; only
+// the first when lo is null).
 void resp_encode_plane_maps(const float* hi, const float* lo, long ncols, int K, long block_stride, void* out);
+// one_pass: hi*hi only (the single-pass TF32 form; the lo planes and W's lo
+// halves are not read).
 void launch_resp_tc(const RespArgs* dArgs, const long* dStart, int nent, const long* dCta, int ctas, int* status,
-                    cudaStream_t s);
+                    bool one_pass, cudaStream_t s);
 
 __host__ __device__ inline int level_rows(const LevelArgs& a) { return a.M > 0 ? a.M : a.Np; }
 __host__ __device__ inline int level_k(const LevelArgs& a) { return a.K > 0 ? a.K : a.Np; }
@@ -179,7 +182,7 @@ void launch_sinusoid_samples(double* U, int m, int K, const double* a, const dou
 // lo = TF32(x - hi), x = float(u)), the tensor-core GEMMs' operand form.
 void launch_sinusoid_planes(float* hi, float* lo, int m, int K, const double* a, const double* f, const double* phi,
                             double base, double dt, long count, cudaStream_t s);
-// FP64 samples into those planes (n values).
+// FP64 samples into those planes (n values).  lo may be null in both (hi only).
 void launch_split_planes(const double* U, float* hi, float* lo, long n, cudaStream_t s);
 
 // Scan-vector initialisation with the forcing term Gamma_k (zero padding

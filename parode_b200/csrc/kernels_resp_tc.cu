@@ -28,6 +28,10 @@
 // a wait that gives up sets the status word and an abort flag that makes
 // every role leave its loop, and the CTA drains its copies (bounded) before
 // it frees its TMEM and exits.
+//
+// The single-pass form (TF32 precision) reads only the hi halves and issues
+// only hi*hi: a third of the tensor work and half of the operand traffic,
+// with the TF32 rounding of both operands (about 2^-11 relative) left in.
 #include "common.h"
 #include "kernels.h"
 #include "tc05.cuh"
@@ -158,6 +162,9 @@ __device__ __forceinline__ void tile_coords(const RespArgs& a, long lt, int& mi,
     nk = (a.K + kBK - 1) / kBK;
 }
 
+// kOne: the single-pass form, hi*hi only (no lo planes are read and no
+// correction buffers used).
+template <bool kOne>
 __global__ void __launch_bounds__(kThreads, 1) k_resp_tc(const RespArgs* __restrict__ args,
                                                          const long* __restrict__ start, int nent,
                                                          const long* __restrict__ cta, int* status)
@@ -217,11 +224,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_resp_tc(const RespArgs* __restr
                     const unsigned char* ab =
                         reinterpret_cast<const unsigned char*>(a.Ps) + ((size_t)mi * nk + sr) * kABlock;
                     const unsigned char* maps = reinterpret_cast<const unsigned char*>(a.maps);
-                    mbar_arrive_tx(&full[st], 2 * abytes + 2 * kBHalf);
+                    mbar_arrive_tx(&full[st], kOne ? abytes + kBHalf : 2 * abytes + 2 * kBHalf);
                     bulk_g2s(stg, ab, abytes, &full[st]);
-                    bulk_g2s(stg + kAHalf, ab + kAHalf, abytes, &full[st]);
                     tma_load_2d(stg + kOffB, maps, sr * kBK, (int)n0, &full[st]);
-                    tma_load_2d(stg + kOffB + kBHalf, maps + 128, sr * kBK, (int)n0, &full[st]);
+                    if (!kOne) {
+                        bulk_g2s(stg + kAHalf, ab + kAHalf, abytes, &full[st]);
+                        tma_load_2d(stg + kOffB + kBHalf, maps + 128, sr * kBK, (int)n0, &full[st]);
+                    }
                 }
                 __syncwarp();
             }
@@ -243,7 +252,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_resp_tc(const RespArgs* __restr
                 int ab = 0;
                 uint32_t d = 0;
                 const uint32_t dc = tbase + (uint32_t)(kAcc * kBN + (tt & 1) * kBN);
-                if (tt >= 2 && !role_wait(&corr_empty[tt & 1], (uint32_t)(((tt >> 1) - 1) & 1), abort, status)) {
+                if (!kOne && tt >= 2 &&
+                    !role_wait(&corr_empty[tt & 1], (uint32_t)(((tt >> 1) - 1) & 1), abort, status)) {
                     ok = false;
                     break;
                 }
@@ -270,7 +280,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_resp_tc(const RespArgs* __restr
                     const uint64_t A[3] = {ah, ah, al};
                     const uint64_t B[3] = {bh, bl, bh};
 #pragma unroll
-                    for (int q = 0; q < 3; ++q)
+                    for (int q = 0; q < (kOne ? 1 : 3); ++q)
 #pragma unroll
                         for (int k = 0; k < kBK / 8; ++k)
                             // A: next 8 K = two 16-byte chunks (256 bytes on); B: 32 bytes on in the swizzled row
@@ -315,7 +325,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_resp_tc(const RespArgs* __restr
                 // 16 columns per load (few registers beside the 64 sums)
                 const uint32_t cu = (uint32_t)(ab * kBN + half * 64);
                 const uint32_t cc = (uint32_t)(kAcc * kBN + (tt & 1) * kBN + half * 64);
-                const int passes = v == units - 1 ? 2 : 1;
+                const int passes = (!kOne && v == units - 1) ? 2 : 1;
                 for (int ps = 0; ps < passes; ++ps) {
                     const uint32_t c0 = ps == 0 ? cu : cc;
 #pragma unroll
@@ -331,7 +341,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_resp_tc(const RespArgs* __restr
                 __syncwarp();
                 if (lane == 0) {
                     mbar_arrive(&acc_empty[ab]);
-                    if (v == units - 1) mbar_arrive(&corr_empty[tt & 1]);
+                    if (!kOne && v == units - 1) mbar_arrive(&corr_empty[tt & 1]);
                 }
             }
             if (!ok) break;
@@ -398,7 +408,7 @@ void resp_encode_plane_maps(const float* hi, const float* lo, long ncols, int K,
     }();
     if (!encode) throw Error(kDeviceError, "cuTensorMapEncodeTiled unavailable");
     const float* planes[2] = {hi, lo};
-    for (int p = 0; p < 2; ++p) {
+    for (int p = 0; p < (lo ? 2 : 1); ++p) {
         if ((reinterpret_cast<uintptr_t>(planes[p]) & 15) || ((block_stride * 4) & 15))
             throw Error(kInvalidArgument, "sample plane map: 16-byte alignment");
         CUtensorMap* m = reinterpret_cast<CUtensorMap*>(static_cast<unsigned char*>(out) + 128 * p);
@@ -416,11 +426,16 @@ void resp_encode_plane_maps(const float* hi, const float* lo, long ncols, int K,
 }
 
 void launch_resp_tc(const RespArgs* dArgs, const long* dStart, int nent, const long* dCta, int ctas, int* status,
-                    cudaStream_t s)
+                    bool one_pass, cudaStream_t s)
 {
     if (nent <= 0 || ctas <= 0) return;
-    PARODE_CUDA(cudaFuncSetAttribute(k_resp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));
-    k_resp_tc<<<(unsigned)ctas, kThreads, kSmem, s>>>(dArgs, dStart, nent, dCta, status);
+    if (one_pass) {
+        PARODE_CUDA(cudaFuncSetAttribute(k_resp_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));
+        k_resp_tc<true><<<(unsigned)ctas, kThreads, kSmem, s>>>(dArgs, dStart, nent, dCta, status);
+    } else {
+        PARODE_CUDA(cudaFuncSetAttribute(k_resp_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));
+        k_resp_tc<false><<<(unsigned)ctas, kThreads, kSmem, s>>>(dArgs, dStart, nent, dCta, status);
+    }
     PARODE_CUDA(cudaGetLastError());
 }
 

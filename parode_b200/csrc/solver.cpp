@@ -57,7 +57,9 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
         b.input = input_;
         std::vector<BatchSpec> specs;
         specs.push_back(std::move(b));
-        batch_ = std::make_unique<BatchPlan>(device, std::move(specs), inputs, opt);
+        PlanOptions bo = opt;
+        if (bo.precision == kTF32) bo.precision = kMixed;  // the batch engine has no single-pass form
+        batch_ = std::make_unique<BatchPlan>(device, std::move(specs), inputs, bo);
         precision_used_ = batch_->precision_used(0);
         path_ = batch_->path(0);
         return;
@@ -68,7 +70,7 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
     if (opt.path == kPathGeneral) {
         path_ = kPathGeneral;
         Np_ = general_padded_dim(Ns_);
-        precision_used_ = (opt.precision == kMixed && compose_tc_supported(Np_)) ? kMixed : kFP64;
+        precision_used_ = (opt.precision != kFP64 && compose_tc_supported(Np_)) ? kMixed : kFP64;
         const double bytes = (double)nScan_ * Np_ * Np_ * 8.0 + (double)general_scan_bytes(Np_, nScan_);
         if (bytes > 24e9) throw Error(kNotEnoughResources, "the general scan holds a copy of Phi per step");
     } else {
@@ -104,8 +106,9 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
             const double sweeps = 4.0 * Np_ * Np_;
             if (opt.path == kPathBlockedResponse || resp < 0.5 * sweeps) {
                 br_ = true;
-                br_tc_ = opt.precision == kMixed;
-                if (br_tc_) precision_used_ = kMixed;
+                br_tc_ = opt.precision != kFP64;
+                one_pass_ = opt.precision == kTF32;
+                if (br_tc_) precision_used_ = one_pass_ ? kTF32 : kMixed;
                 // a block length forced by the caller or measured for this
                 // class of systems (tuner.h) replaces the shape's default
                 int Rt = opt.force_log2_block;
@@ -126,7 +129,7 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
         // otherwise the mixed form runs the in-block sweeps on the tensor
         // cores (3xTF32) when the shape allows it, with the longest tile that
         // fits its shared-memory layout; otherwise the solve stays in FP64
-        if (opt.precision == kMixed && !br_) {
+        if (opt.precision != kFP64 && !br_) {
             // largest (levels per block, tile) that fits: the tensor-core
             // operands need bucket starts on 8-row boundaries (S >= 4B) and
             // M = 128 slices (S >= 128)
@@ -246,10 +249,12 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
             double* d = nullptr;
             alloc(&d, (nf + 1) / 2);
             dUh_ = reinterpret_cast<float*>(d);
-            alloc(&d, (nf + 1) / 2);
-            dUl_ = reinterpret_cast<float*>(d);
             PARODE_CUDA(cudaMemsetAsync(dUh_, 0, sizeof(float) * (size_t)nf, stream_));
-            PARODE_CUDA(cudaMemsetAsync(dUl_, 0, sizeof(float) * (size_t)nf, stream_));
+            if (!one_pass_) {  // the single-pass form reads no lo plane
+                alloc(&d, (nf + 1) / 2);
+                dUl_ = reinterpret_cast<float*>(d);
+                PARODE_CUDA(cudaMemsetAsync(dUl_, 0, sizeof(float) * (size_t)nf, stream_));
+            }
         }
     }
     PARODE_CUDA(cudaMemcpyAsync(dPow_, PhiP.data(), sizeof(double) * PhiP.size(), cudaMemcpyHostToDevice, stream_));
@@ -692,7 +697,7 @@ void Plan::execute_response(double* Y, cudaStream_t s)
     if (br_tc_) {
         // mixed: aggregates and output windows (tensor cores) -> carry ->
         // y = windows + C Phi^j X_b (FP64)
-        launch_resp_tc(dResp_, dTcStart_, 2, dTcCta_, tcCtas_, dStatus_, s);
+        launch_resp_tc(dResp_, dTcStart_, 2, dTcCta_, tcCtas_, dStatus_, one_pass_, s);
         ++launches;
         mark("aggregates+windows", s);
         launches += carry(s);

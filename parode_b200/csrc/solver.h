@@ -141,6 +141,7 @@ private:
     long* dTcCta_ = nullptr;    // device: tile ranges of the persistent CTAs
     int tcCtas_ = 0;
     int* dStatus_ = nullptr;
+    bool one_pass_ = false;  // single-pass TF32 response GEMMs (hi*hi only)
     cudaStream_t side_ = nullptr;
     cudaEvent_t fork_[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t done_ = nullptr;  // recorded after each execute on its stream
