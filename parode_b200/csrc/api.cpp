@@ -919,6 +919,7 @@ SystemDesc tune_system(int n, int m, int p)
     s.n = n;
     s.m = m;
     s.p = p;
+    s.zeroB = s.zeroC = s.zeroD = false;
     s.A.resize((size_t)n * n);
     for (int i = 0; i < n; ++i)
         for (int j = 0; j < n; ++j) s.A[(size_t)i * n + j] = (i == j ? -1.5 : 0.0) + 0.5 * normal() / std::sqrt((double)n);
@@ -1022,7 +1023,15 @@ void ParODE_TuneResponseBlock(int solver, int nStates, int nInputs, int nOutputs
             if (R > 2 && B / 2 >= nScan) break;
             const long K = response_window(solver, (int)B, nInputs);
             if (8.0 * ((double)B * nOutputs + np) * ((double)K + np) > 256e6) break;
-            const float ms = time_R(R);
+            float ms = 0.f;
+            try {
+                ms = time_R(R);
+            } catch (const Error& e) {
+                // a block length the engine cannot build for this class (a
+                // resource limit) is not a candidate; anything else is an error
+                if (e.code != kNotEnoughResources && e.code != kInvalidArgument) throw;
+                continue;
+            }
             if (R == Rdefault) model_ms = ms;
             if (best < 0 || ms < best_ms) {
                 best = R;
