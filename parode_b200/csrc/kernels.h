@@ -158,11 +158,14 @@ int response_log2_block(int solver, int NP, int n, int m, int p, long nScan, dou
 // Q = P_{l0} (P: power table, level l at l NP^2).  Chunks of 16 per level;
 // level h uses P_{l0 + 4h}, so the table must reach level
 // l0 + 4 chunk_carry_levels(count).  work: chunk_carry_scratch(count) NP
-// doubles.  Returns the launches made.
+// doubles.  after_first (optional) is recorded on s once the level-0 up-sweep
+// is issued (at once when there is none): from there on the carry's launches
+// are small, and work beside it can take the other SMs.  Returns the launches
+// made.
 int chunk_carry_levels(long count);
 long chunk_carry_scratch(long count);
 int launch_chunk_carry(int NP, double* items, long count, const double* P, int l0, const double* X0, double* work,
-                       cudaStream_t s);
+                       cudaStream_t s, cudaEvent_t after_first = nullptr);
 
 // Columns of a level that can reach an output.  Column g combines the
 // segments [g 2d, g 2d + d) and [g 2d + d, g 2d + 2d) of the time axis; when

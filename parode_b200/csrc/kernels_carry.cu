@@ -238,7 +238,8 @@ __global__ void __launch_bounds__(kThreads) k_chunk_down(double* __restrict__ it
 
 // ---------------------------------------------------------------------------
 template <int NP>
-int chunk_carry_t(double* items, long count, const double* P, int l0, const double* X0, double* work, cudaStream_t s)
+int chunk_carry_t(double* items, long count, const double* P, int l0, const double* X0, double* work, cudaStream_t s,
+                  cudaEvent_t after_first)
 {
     const long mat = (long)NP * NP;
     double* arr[16];
@@ -254,12 +255,14 @@ int chunk_carry_t(double* items, long count, const double* P, int l0, const doub
         const unsigned grid = (unsigned)((nc + kCols - 1) / kCols);
         k_chunk_up<NP><<<grid, kThreads, 0, s>>>(arr[h], cnt[h], P + (long)(l0 + 4 * h) * mat, w);
         PARODE_CUDA(cudaGetLastError());
+        if (h == 0 && after_first) PARODE_CUDA(cudaEventRecord(after_first, s));
         ++launches;
         arr[h + 1] = w;
         cnt[h + 1] = nc;
         w += nc * NP;
         ++h;
     }
+    if (h == 0 && after_first) PARODE_CUDA(cudaEventRecord(after_first, s));
     // top: one chunk of the remaining items, entered with the initial state
     k_chunk_down<NP><<<1, kThreads, 0, s>>>(arr[h], cnt[h], P + (long)(l0 + 4 * h) * mat, X0, (int)cnt[h]);
     PARODE_CUDA(cudaGetLastError());
@@ -297,18 +300,21 @@ long chunk_carry_scratch(long count)
 }
 
 int launch_chunk_carry(int NP, double* items, long count, const double* P, int l0, const double* X0, double* work,
-                       cudaStream_t s)
+                       cudaStream_t s, cudaEvent_t after_first)
 {
-    if (count <= 0) return 0;
+    if (count <= 0) {
+        if (after_first) PARODE_CUDA(cudaEventRecord(after_first, s));
+        return 0;
+    }
     switch (NP) {
-    case 8: return chunk_carry_t<8>(items, count, P, l0, X0, work, s);
-    case 16: return chunk_carry_t<16>(items, count, P, l0, X0, work, s);
-    case 24: return chunk_carry_t<24>(items, count, P, l0, X0, work, s);
-    case 32: return chunk_carry_t<32>(items, count, P, l0, X0, work, s);
-    case 40: return chunk_carry_t<40>(items, count, P, l0, X0, work, s);
-    case 48: return chunk_carry_t<48>(items, count, P, l0, X0, work, s);
-    case 56: return chunk_carry_t<56>(items, count, P, l0, X0, work, s);
-    case 64: return chunk_carry_t<64>(items, count, P, l0, X0, work, s);
+    case 8: return chunk_carry_t<8>(items, count, P, l0, X0, work, s, after_first);
+    case 16: return chunk_carry_t<16>(items, count, P, l0, X0, work, s, after_first);
+    case 24: return chunk_carry_t<24>(items, count, P, l0, X0, work, s, after_first);
+    case 32: return chunk_carry_t<32>(items, count, P, l0, X0, work, s, after_first);
+    case 40: return chunk_carry_t<40>(items, count, P, l0, X0, work, s, after_first);
+    case 48: return chunk_carry_t<48>(items, count, P, l0, X0, work, s, after_first);
+    case 56: return chunk_carry_t<56>(items, count, P, l0, X0, work, s, after_first);
+    case 64: return chunk_carry_t<64>(items, count, P, l0, X0, work, s, after_first);
     default: throw Error(kInvalidArgument, "chunk carry: NP must be a multiple of 8 up to 64");
     }
 }

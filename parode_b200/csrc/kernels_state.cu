@@ -7,12 +7,13 @@
 // the steps of a block, with the states those steps reach from X[b].
 //
 // FP64 on the DMMA tensor cores.  Ws is small (M x NP) and stays in shared
-// memory for the CTA's whole run; the CTA walks tiles of 8 blocks: their
-// states (8 x NP) into shared memory, each warp the 8-row slices of W it owns
-// times the tile (m8n8k4, K = NP), the 8 x M results staged in shared memory
-// and then added to acc and stored block by block (M consecutive doubles per
-// block).  HBM traffic per block: NP states read, 2 M doubles of y read and
-// written.
+// memory for the CTA's whole run.  Each warp works alone on tiles of 8 blocks:
+// their states as DMMA B fragments in registers (read once from X), then for
+// every 8-row slice of W (m8n8k4, K = NP) the slice's window part is loaded
+// ahead of the product and y written straight to global memory (8 rows of a
+// block are 64 consecutive bytes).  No block-wide barrier after the staging
+// of W, so the warps' loads and products overlap freely.  HBM traffic per
+// block: NP states read, M doubles of the window part read, M of y written.
 #include "common.h"
 #include "device_common.cuh"
 #include "kernels.h"
@@ -34,53 +35,50 @@ constexpr int kpitch()
 
 template <int NP>
 __global__ void __launch_bounds__(kThreads) k_state_out(const double* __restrict__ W, long ld, int M, int Mp,
-                                                        const double* __restrict__ X, const double* __restrict__ acc,
-                                                        double* __restrict__ Y, long gs, long nblocks, long limit)
+                                                        const double* __restrict__ X, const double* acc, double* Y,
+                                                        long gs, long nblocks, long limit)
 {
     extern __shared__ double sm[];
-    double* Ws = sm;                           // Mp x kpitch
-    double* Xs = Ws + (long)Mp * kpitch<NP>();  // 8 x kpitch
-    double* Ys = Xs + 8 * kpitch<NP>();         // 8 x (Mp + 4)
-    const int yp = Mp + 4;
+    double* Ws = sm;  // Mp x kpitch, rows >= M zero
     for (int e = threadIdx.x; e < Mp * NP; e += kThreads) {
         const int r = e / NP, k = e - r * NP;
         Ws[r * kpitch<NP>() + k] = r < M ? W[(long)r * ld + k] : 0.0;
     }
+    __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int g = lane >> 2, t = lane & 3;
     const long tiles = (nblocks + 7) / 8;
-    for (long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    for (long tile = (long)blockIdx.x * kWarps + warp; tile < tiles; tile += (long)gridDim.x * kWarps) {
         const long b0 = tile * 8;
-        for (int e = threadIdx.x; e < 8 * NP; e += kThreads) {
-            const int c = e / NP, k = e - c * NP;
-            Xs[c * kpitch<NP>() + k] = b0 + c < nblocks ? X[(b0 + c) * NP + k] : 0.0;
-        }
-        __syncthreads();
-        for (int mt = warp; mt < Mp / 8; mt += kWarps) {
-            double d0 = 0.0, d1 = 0.0;
+        double bv[NP / 4];
+        {
+            const long bb = b0 + g;
 #pragma unroll
-            for (int kk = 0; kk < NP / 4; ++kk) {
-                const double a = Ws[(mt * 8 + g) * kpitch<NP>() + 4 * kk + t];
-                const double b = Xs[g * kpitch<NP>() + 4 * kk + t];
-                dmma_m8n8k4(d0, d1, a, b);
-            }
-            Ys[(2 * t) * yp + mt * 8 + g] = d0;
-            Ys[(2 * t + 1) * yp + mt * 8 + g] = d1;
+            for (int kk = 0; kk < NP / 4; ++kk) bv[kk] = bb < nblocks ? X[bb * NP + 4 * kk + t] : 0.0;
         }
-        __syncthreads();
-        for (int e = threadIdx.x; e < 8 * M; e += kThreads) {
-            const int c = e / M, r = e - c * M;
-            const long b = b0 + c, off = b * gs + r;
-            if (b < nblocks && (limit < 0 || off < limit)) Y[off] = acc[off] + Ys[c * yp + r];
+        // this lane's two blocks (D fragment columns 2t, 2t + 1)
+        const long c0 = b0 + 2 * t, c1 = c0 + 1;
+#pragma unroll 4
+        for (int mt = 0; mt < Mp / 8; ++mt) {
+            const int r = mt * 8 + g;
+            const long o0 = c0 * gs + r, o1 = c1 * gs + r;
+            const bool v0 = r < M && c0 < nblocks && (limit < 0 || o0 < limit);
+            const bool v1 = r < M && c1 < nblocks && (limit < 0 || o1 < limit);
+            const double a0 = v0 ? acc[o0] : 0.0, a1 = v1 ? acc[o1] : 0.0;
+            double d0 = 0.0, d1 = 0.0;
+            const double* wr = Ws + r * kpitch<NP>() + t;
+#pragma unroll
+            for (int kk = 0; kk < NP / 4; ++kk) dmma_m8n8k4(d0, d1, wr[4 * kk], bv[kk]);
+            if (v0) Y[o0] = a0 + d0;
+            if (v1) Y[o1] = a1 + d1;
         }
-        __syncthreads();
     }
 }
 
 template <int NP>
 size_t state_smem(int Mp)
 {
-    return ((size_t)Mp * kpitch<NP>() + 8 * (size_t)kpitch<NP>() + 8 * (size_t)(Mp + 4)) * sizeof(double);
+    return (size_t)Mp * kpitch<NP>() * sizeof(double);
 }
 
 template <int NP>
@@ -94,7 +92,8 @@ bool state_t(const double* W, long ld, int M, const double* X, const double* acc
     int per_sm = 0;
     PARODE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_state_out<NP>, kThreads, smem));
     const long tiles = (nblocks + 7) / 8;
-    const unsigned grid = (unsigned)std::max<long>(1, std::min<long>(tiles, (long)sms * std::max(per_sm, 1)));
+    const unsigned grid =
+        (unsigned)std::max<long>(1, std::min<long>((tiles + kWarps - 1) / kWarps, (long)sms * std::max(per_sm, 1)));
     k_state_out<NP><<<grid, kThreads, smem, s>>>(W, ld, M, Mp, X, acc, Y, gs, nblocks, limit);
     PARODE_CUDA(cudaGetLastError());
     return true;

@@ -381,8 +381,22 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
             r[1].fault_withhold = 0;
             const long start[2] = {0, resp_tc_tiles(r[0])};
             const long tiles = start[1] + resp_tc_tiles(r[1]);
-            tcCtas_ = (int)std::min<long>(sms_, tiles);
-            const std::vector<long> ranges = resp_tc_ranges({r[0], r[1]}, tcCtas_);
+            std::vector<long> ranges;
+            // with two or more carry levels the output windows run beside the
+            // carry's small upper-level launches (on the SMs those leave
+            // free), the aggregates alone before it; else both in one launch
+            tc_overlap_ = chunk_carry_levels(nblocks_) >= 2 && sms_ >= 64;
+            if (tc_overlap_) {
+                const long c1 = (nblocks_ + 15) / 16, upper = ((c1 + 15) / 16 + 7) / 8;
+                tcCtas_ = (int)std::min<long>(sms_, start[1]);
+                tcCtasW_ = (int)std::min<long>(sms_ - std::min<long>(upper, sms_ / 2), resp_tc_tiles(r[1]));
+                ranges = resp_tc_ranges({r[0]}, tcCtas_);
+                const std::vector<long> rw = resp_tc_ranges({r[1]}, tcCtasW_);
+                ranges.insert(ranges.end(), rw.begin(), rw.end());
+            } else {
+                tcCtas_ = (int)std::min<long>(sms_, tiles);
+                ranges = resp_tc_ranges({r[0], r[1]}, tcCtas_);
+            }
             double* d = nullptr;
             alloc(&d, (long)((2 * sizeof(LevelArgs) + 7) / 8));
             dTc_ = reinterpret_cast<LevelArgs*>(d);
@@ -444,6 +458,8 @@ Plan::~Plan()
     if (stream_) cudaStreamSynchronize(stream_);
     if (side_) cudaStreamSynchronize(side_);
     for (cudaEvent_t e : events_) cudaEventDestroy(e);
+    for (cudaEvent_t e : side_ev_)
+        if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : fork_)
         if (e) cudaEventDestroy(e);
     if (done_) cudaEventDestroy(done_);
@@ -483,6 +499,16 @@ void Plan::mark(const char* stage, cudaStream_t s)
     PARODE_CUDA(cudaEventRecord(events_[k], s));
 }
 
+void Plan::side_span(int end)
+{
+    // the output-window launch on the side stream, timed apart from the
+    // stages of the main stream
+    if (!profiling_) return;
+    if (!side_ev_[end]) PARODE_CUDA(cudaEventCreate(&side_ev_[end]));
+    PARODE_CUDA(cudaEventRecord(side_ev_[end], side_));
+    side_marked_ = end == 1;
+}
+
 std::vector<std::pair<std::string, float>> Plan::stage_times()
 {
     std::vector<std::pair<std::string, float>> out;
@@ -492,6 +518,12 @@ std::vector<std::pair<std::string, float>> Plan::stage_times()
         float ms = 0.f;
         PARODE_CUDA(cudaEventElapsedTime(&ms, events_[k - 1], events_[k]));
         out.emplace_back(marks_[k], ms);
+    }
+    if (side_marked_) {
+        float ms = 0.f;
+        PARODE_CUDA(cudaEventSynchronize(side_ev_[1]));
+        PARODE_CUDA(cudaEventElapsedTime(&ms, side_ev_[0], side_ev_[1]));
+        out.emplace_back("windows (side stream)", ms);
     }
     return out;
 }
@@ -673,10 +705,10 @@ void Plan::execute_general(double* Y, cudaStream_t s)
     last_y_ = Y;
 }
 
-int Plan::carry(cudaStream_t s)
+int Plan::carry(cudaStream_t s, cudaEvent_t after_first)
 {
     // the exclusive scan of the block aggregates (kernels_carry.cu)
-    return launch_chunk_carry(Np_, dG_, nblocks_, dPow_, shape_.R, dX0_, dWork_, s);
+    return launch_chunk_carry(Np_, dG_, nblocks_, dPow_, shape_.R, dX0_, dWork_, s, after_first);
 }
 
 void Plan::execute_response(double* Y, cudaStream_t s)
@@ -688,6 +720,7 @@ void Plan::execute_response(double* Y, cudaStream_t s)
     // P_1..P_levels was formed with W when the plan was made.
     int launches = 0;
     marks_.clear();
+    side_marked_ = false;
     mark("start", s);
     fill_inputs(s);
     ++launches;
@@ -697,11 +730,28 @@ void Plan::execute_response(double* Y, cudaStream_t s)
     if (br_tc_) {
         // mixed: aggregates and output windows (tensor cores) -> carry ->
         // y = windows + C Phi^j X_b (FP64)
-        launch_resp_tc(dResp_, dTcStart_, 2, dTcCta_, tcCtas_, dStatus_, one_pass_, s);
-        ++launches;
-        mark("aggregates+windows", s);
-        launches += carry(s);
-        mark("carry", s);
+        if (tc_overlap_) {
+            // aggregates -> carry, the output windows on the side stream from
+            // the end of the carry's level-0 up-sweep (kernels.h)
+            launch_resp_tc(dResp_, dTcStart_, 1, dTcCta_, tcCtas_, dStatus_, one_pass_, s);
+            ++launches;
+            mark("aggregates", s);
+            launches += carry(s, fork_[2]);
+            PARODE_CUDA(cudaStreamWaitEvent(side_, fork_[2], 0));
+            side_span(0);
+            launch_resp_tc(dResp_ + 1, dTcStart_, 1, dTcCta_ + tcCtas_ + 1, tcCtasW_, dStatus_, one_pass_, side_);
+            side_span(1);
+            ++launches;
+            PARODE_CUDA(cudaEventRecord(fork_[3], side_));
+            PARODE_CUDA(cudaStreamWaitEvent(s, fork_[3], 0));
+            mark("carry+windows", s);
+        } else {
+            launch_resp_tc(dResp_, dTcStart_, 2, dTcCta_, tcCtas_, dStatus_, one_pass_, s);
+            ++launches;
+            mark("aggregates+windows", s);
+            launches += carry(s);
+            mark("carry", s);
+        }
         // y = windows + (C Phi^j) X_b: W's state columns stay in shared
         // memory (kernels_state.cu); the general tiled GEMM where they do not fit
         if (!launch_state_out(Np_, dW_ + brKpad_, ld, shape_.B * p_, dG_, dY_ + ybase * p_, Y + ybase * p_,

@@ -97,7 +97,8 @@ private:
     void execute_blocked(double* Y, cudaStream_t s);
     void execute_response(double* Y, cudaStream_t s);
     void execute_general(double* Y, cudaStream_t s);
-    int carry(cudaStream_t s);
+    int carry(cudaStream_t s, cudaEvent_t after_first = nullptr);
+    void side_span(int end);
     void fill_inputs(cudaStream_t s);
 
     int device_ = 0;
@@ -140,6 +141,8 @@ private:
     long* dTcStart_ = nullptr;  // device: their first tiles
     long* dTcCta_ = nullptr;    // device: tile ranges of the persistent CTAs
     int tcCtas_ = 0;
+    int tcCtasW_ = 0;           // CTAs of the output-window launch beside the carry
+    bool tc_overlap_ = false;  // the windows run beside the carry (tcCtas_ then the aggregates' CTAs)
     int* dStatus_ = nullptr;
     bool one_pass_ = false;  // single-pass TF32 response GEMMs (hi*hi only)
     cudaStream_t side_ = nullptr;
@@ -150,6 +153,8 @@ private:
     bool profiling_ = false;
     std::vector<cudaEvent_t> events_;
     std::vector<std::string> marks_;
+    cudaEvent_t side_ev_[2] = {nullptr, nullptr};  // span of the side-stream window launch
+    bool side_marked_ = false;
 };
 
 }  // namespace parode
