@@ -257,13 +257,30 @@ def _cheap_sample(cases, k):
     return small[: k // 2] + large[: k - k // 2]
 
 
-def measure_batched(pb, wl, torch, dev, reps=3, tune_classes=0):
-    """The batched form: 4096 independent systems (cfg4) in one batch, FP64 and mixed."""
-    cases = wl.cfg4()
+def _over_ranks(torch, dev, world, value, op="max"):
+    """value reduced over the ranks (max or sum); itself on one rank."""
+    if world == 1:
+        return value
+    import torch.distributed as dist
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def measure_batched(pb, wl, torch, dev, reps=3, tune_classes=0, rank=0, world=1):
+    """The batched form: 4096 independent systems (cfg4) in one batch, FP64 and
+    mixed; on N ranks each solves its cost-balanced shard of the systems
+    (parode_b200.multi.shard, no data-path collective) and the time is the
+    slowest rank's."""
+    from parode_b200 import multi
+
+    cases_all = wl.cfg4()
+    cases = [cases_all[i] for i in multi.shard(cases_all, rank, world, multi.system_cost)]
     specs = [_spec(pb, c) for c in cases]
     check = _cheap_sample(cases, 8)
     out = {"workload": "cfg4: 4096 systems, n log-uniform [4,96], T log-uniform [2^10,2^16], RK4/ABM 50/50",
-           "state_steps": None}
+           "state_steps": None, "ranks": world, "systems_on_rank0": len(cases)}
     stream = torch.cuda.Stream(device=dev)
     y64 = {}
     for name, prec in (("fp64", pb.FP64), ("mixed", pb.MIXED)):
@@ -288,8 +305,11 @@ def measure_batched(pb, wl, torch, dev, reps=3, tune_classes=0):
                 y64[i] = y
             else:
                 worst = max(worst or 0.0, rel_err(y, y64[i]))
-        out["state_steps"] = b.state_steps
-        out[name] = {"ms": ms, "value": b.state_steps / (ms / 1e3), "unit": UNIT, "launches": b.launch_count,
+        ms = _over_ranks(torch, dev, world, ms)
+        work = _over_ranks(torch, dev, world, b.state_steps, "sum")
+        setup_s = _over_ranks(torch, dev, world, setup_s)
+        out["state_steps"] = work
+        out[name] = {"ms": ms, "value": work / (ms / 1e3), "unit": UNIT, "launches": b.launch_count,
                      "setup_s": setup_s}
         if worst is not None:
             out[name].update(rel_err_vs_fp64_sampled=worst, sampled_systems=len(check))
@@ -310,8 +330,9 @@ def measure_batched(pb, wl, torch, dev, reps=3, tune_classes=0):
             e.record(stream)
             e.synchronize()
             ts.append(s.elapsed_time(e))
-        ms = statistics.median(ts)
-        out["mixed_tuned"] = {"ms": ms, "value": b.state_steps / (ms / 1e3), "unit": UNIT, "launches": b.launch_count,
+        ms = _over_ranks(torch, dev, world, statistics.median(ts))
+        out["mixed_tuned"] = {"ms": ms, "value": out["state_steps"] / (ms / 1e3), "unit": UNIT,
+                              "launches": b.launch_count,
                               "classes_tuned": len(tuned), "share_of_work_tuned": sum(w for _, w in tuned),
                               "gain_over_untuned": out["mixed"]["ms"] / ms}
         b.close()
@@ -410,15 +431,21 @@ def measure_cfg3(pb, wl, torch, reps=3):
     return out
 
 
-def measure_serving(pb, wl, torch, count=64, rates=(500.0, 2000.0, 8000.0)):
+def measure_serving(pb, wl, torch, count=64, rates=(500.0, 2000.0, 8000.0), dev=None, rank=0, world=1):
     """The serving loop on cfg5-shaped requests (Poisson arrivals), mixed form,
-    beside one offline batch of the same requests."""
+    beside one offline batch of the same requests.  On N ranks each serves its
+    share of every request stream (round robin in arrival order) with its own
+    server; latencies are the worst rank's percentiles, throughput the summed
+    work over the longest span."""
+    from parode_b200 import multi
+
     out = {"workload": f"cfg5: {count} requests per rate, n log-uniform [8,256], T log-uniform [1e3,1e6], "
                        f"RK4/ABM 50/50, Poisson arrivals", "budget_bytes": 150e9, "precision": "mixed",
            "rates": {}}
     reqs_all = {}
     for rate in rates:
         reqs = wl.cfg5(count, rate)
+        reqs = [reqs[i] for i in multi.shard(reqs, rank, world)]
         reqs_all[rate] = reqs
         server = pb.Server(precision=pb.MIXED, hbm_budget_bytes=150e9, max_batch=32, max_inflight=8)
         specs = [(arr, c, _spec(pb, c)) for arr, c in reqs]
@@ -434,10 +461,13 @@ def measure_serving(pb, wl, torch, count=64, rates=(500.0, 2000.0, 8000.0)):
             server.wait(rid, timeout_s=600)
         st = server.stats()
         server.close()
-        out["rates"][str(int(rate))] = {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
-                                        "value": st["state_steps"] / st["span_s"] if st["span_s"] else None,
-                                        "unit": UNIT, "batches": int(st["batches"]),
-                                        "peak_gb": st["peak_bytes"] / 1e9, "span_s": st["span_s"]}
+        red = {k: _over_ranks(torch, dev, world, st[k]) for k in ("p50_ms", "p99_ms", "mean_ms", "span_s", "peak_bytes")}
+        work = _over_ranks(torch, dev, world, st["state_steps"], "sum")
+        batches = _over_ranks(torch, dev, world, st["batches"], "sum")
+        out["rates"][str(int(rate))] = {"p50_ms": red["p50_ms"], "p99_ms": red["p99_ms"], "mean_ms": red["mean_ms"],
+                                        "value": work / red["span_s"] if red["span_s"] else None,
+                                        "unit": UNIT, "batches": int(batches),
+                                        "peak_gb": red["peak_bytes"] / 1e9, "span_s": red["span_s"]}
     # offline: all requests of the middle rate in one batch (set-up excluded and included)
     reqs = reqs_all[rates[len(rates) // 2]]
     t0 = time.perf_counter()
@@ -451,8 +481,10 @@ def measure_serving(pb, wl, torch, count=64, rates=(500.0, 2000.0, 8000.0)):
     b.execute(stream.cuda_stream)
     e.record(stream)
     e.synchronize()
-    ms = s.elapsed_time(e)
-    out["offline"] = {"value": b.state_steps / (ms / 1e3), "value_with_setup": b.state_steps / (ms / 1e3 + setup),
+    ms = _over_ranks(torch, dev, world, s.elapsed_time(e))
+    setup = _over_ranks(torch, dev, world, setup)
+    work = _over_ranks(torch, dev, world, b.state_steps, "sum")
+    out["offline"] = {"value": work / (ms / 1e3), "value_with_setup": work / (ms / 1e3 + setup),
                       "unit": UNIT, "ms": ms, "setup_s": setup}
     b.close()
     mid = out["rates"][str(int(rates[len(rates) // 2]))]
@@ -626,10 +658,12 @@ def run_ours(args):
     cfg1 = measure_cfg1(pb, wl, torch) if world == 1 and not args.no_extra else None
 
     batched = serving = cfg3 = None
-    if world == 1 and not args.no_extra:
-        batched = measure_batched(pb, wl, torch, dev, tune_classes=0 if args.no_tune else 16)
-        cfg3 = measure_cfg3(pb, wl, torch)
-        serving = measure_serving(pb, wl, torch, count=args.serve_requests)
+    if not args.no_extra:
+        # independent systems shard across the ranks (no data-path collective)
+        batched = measure_batched(pb, wl, torch, dev, tune_classes=0 if args.no_tune else 16, rank=rank, world=world)
+        if world == 1:
+            cfg3 = measure_cfg3(pb, wl, torch)
+        serving = measure_serving(pb, wl, torch, count=args.serve_requests, dev=dev, rank=rank, world=world)
 
     if rank == 0:
         peaks, peaks_kind = measured_peaks()

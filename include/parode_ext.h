@@ -125,6 +125,34 @@ void ParODE_PlanDestroy(ParODE_Plan* plan);
 void ParODE_PlanSetProfiling(ParODE_Plan* plan, int enable, int nErr[]);
 int ParODE_PlanStageTimes(ParODE_Plan* plan, float* ms, int cap, char* names, int names_cap, int nErr[]);
 
+/* ---- time partition of one solve across devices --------------------------
+ * The reference splits one solve's horizon over its devices in proportion to
+ * their compute units (Sources/RungeKutta4thOrder.cpp:96-125), up-sweeps each
+ * device's part, carries the parts' totals across devices on the host and
+ * down-sweeps (Sources/GPUFixedStepIterative.cpp:296-337).  Here shard
+ * `shard` of `shards` is one plan on one device (one process per GPU):
+ *   PlanShardUp    its inputs, block aggregates and the first k levels of
+ *                  the chunked carry from a zero state, leaving info[2]
+ *                  chunk aggregates of info[3] doubles in dTop (device);
+ *   (the caller all-gathers every shard's dTop in shard order: NCCL or any
+ *    device copy; equal devices take equal shares of the horizon)
+ *   PlanShardDown  the scan of the gathered items seeded with the initial
+ *                  state (every shard computes it, it is small), its own
+ *                  down-sweep and outputs into yDev (NumOutputs rows: the
+ *                  first 3 rows of an ABM solve are its start-up rows on
+ *                  shard 0 only, then the shard's steps).
+ * Block-response path only (scan dimension <= 64, inputs present).  info:
+ * [0] first scan step of the shard, [1] its scan steps, [2] items per shard,
+ * [3] doubles per item, [4] shards.  PlanExecute is refused on a shard plan;
+ * PlanGetOutput returns the shard's slice of the horizon's time vector. */
+ParODE_Plan* ParODE_PlanCreateShard(const double* A, const double* B, const double* C, const double* D,
+                                    int nInputs, int nStates, int nOutputs, int ZeroB, int ZeroC, int ZeroD,
+                                    int uIndex, double tStart, double tEnd, double tStep, const double* x0,
+                                    int solver, int precision, int shard, int shards, int nErr[]);
+void ParODE_PlanShardInfo(const ParODE_Plan* plan, long long info[5]);
+void ParODE_PlanShardUp(ParODE_Plan* plan, double* dTop, void* stream, int nErr[]);
+void ParODE_PlanShardDown(ParODE_Plan* plan, const double* dGathered, double* yDev, void* stream, int nErr[]);
+
 /* ---- batches: many independent systems solved together -----------------
  * One call set-up for nSystems systems (per-system arrays of the
  * SimulateODE_d arguments; B, C, D may be NULL arrays when every system has

@@ -108,6 +108,14 @@ def _load():
     L.ParODE_PlanSetProfiling.argtypes = [C.c_void_p, C.c_int, ip]
     L.ParODE_PlanStageTimes.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_int, C.c_char_p, C.c_int, ip]
     L.ParODE_PlanStageTimes.restype = C.c_int
+    L.ParODE_PlanCreateShard.argtypes = [dp, dp, dp, dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                         C.c_int, C.c_double, C.c_double, C.c_double, dp, C.c_int, C.c_int,
+                                         C.c_int, C.c_int, ip]
+    L.ParODE_PlanCreateShard.restype = C.c_void_p
+    L.ParODE_PlanShardInfo.argtypes = [C.c_void_p, C.POINTER(C.c_longlong)]
+    L.ParODE_PlanShardInfo.restype = None
+    L.ParODE_PlanShardUp.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, ip]
+    L.ParODE_PlanShardDown.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, ip]
     pp = C.POINTER(C.c_void_p)
     L.ParODE_BatchCreate.argtypes = [C.c_int, pp, pp, pp, pp, ip, ip, ip, ip, ip, ip, ip, dp, dp, dp, pp, ip,
                                      C.c_int, ip]
@@ -355,18 +363,47 @@ def simulate_f32(A, B, Cm, D, x0, u_index: int, t0: float, t_end: float, h: floa
 
 
 class Plan:
-    """Device-resident solve (ParODE_PlanCreate / Execute / GetOutput)."""
+    """Device-resident solve (ParODE_PlanCreate / Execute / GetOutput).
+
+    With shards > 1 the plan is time shard `shard` of the solve
+    (ParODE_PlanCreateShard): it runs through shard_up / shard_down instead of
+    execute (parode_b200.multi.solve_time_partitioned drives them)."""
 
     def __init__(self, A, B, Cm, D, x0, u_index: int, t0: float, t_end: float, h: float, solver: int = RK4,
-                 precision: int = FP64):
+                 precision: int = FP64, shard: int = 0, shards: int = 1):
         A, B, Cm, D, x0, n, m, p = _sys_arrays(A, B, Cm, D, x0)
         e = C.c_int(0)
-        self._h = lib.ParODE_PlanCreate(_dp(A), _dp(B), _dp(Cm), _dp(D), m, n, p, int(B is None), int(Cm is None),
-                                        int(D is None), u_index, t0, t_end, h, _dp(x0), solver, precision,
-                                        C.byref(e))
-        _check(e, "ParODE_PlanCreate")
+        if shards > 1 or shard != 0:
+            self._h = lib.ParODE_PlanCreateShard(_dp(A), _dp(B), _dp(Cm), _dp(D), m, n, p, int(B is None),
+                                                 int(Cm is None), int(D is None), u_index, t0, t_end, h, _dp(x0),
+                                                 solver, precision, shard, shards, C.byref(e))
+            _check(e, "ParODE_PlanCreateShard")
+        else:
+            self._h = lib.ParODE_PlanCreate(_dp(A), _dp(B), _dp(Cm), _dp(D), m, n, p, int(B is None),
+                                            int(Cm is None), int(D is None), u_index, t0, t_end, h, _dp(x0), solver,
+                                            precision, C.byref(e))
+            _check(e, "ParODE_PlanCreate")
         self.num_outputs = int(lib.ParODE_PlanNumOutputs(self._h))
         self.channels = int(lib.ParODE_PlanNumOutputChannels(self._h))
+
+    @property
+    def shard_info(self):
+        """(first scan step, scan steps, items per shard, doubles per item, shards)
+        of a time-shard plan."""
+        info = (C.c_longlong * 5)()
+        lib.ParODE_PlanShardInfo(self._h, info)
+        return tuple(int(v) for v in info)
+
+    def shard_up(self, top_dev_ptr: int, stream: int = 0) -> None:
+        e = C.c_int(0)
+        lib.ParODE_PlanShardUp(self._h, C.c_void_p(top_dev_ptr), C.c_void_p(stream or None), C.byref(e))
+        _check(e, "ParODE_PlanShardUp")
+
+    def shard_down(self, gathered_dev_ptr: int, y_dev_ptr: int = 0, stream: int = 0) -> None:
+        e = C.c_int(0)
+        lib.ParODE_PlanShardDown(self._h, C.c_void_p(gathered_dev_ptr), C.c_void_p(y_dev_ptr or None),
+                                 C.c_void_p(stream or None), C.byref(e))
+        _check(e, "ParODE_PlanShardDown")
 
     def execute(self, y_dev_ptr: int = 0, stream: int = 0) -> None:
         e = C.c_int(0)

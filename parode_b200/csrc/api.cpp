@@ -542,6 +542,60 @@ ParODE_Plan* ParODE_PlanCreate(const double* A, const double* B, const double* C
     return out;
 }
 
+ParODE_Plan* ParODE_PlanCreateShard(const double* A, const double* B, const double* C, const double* D, int nInputs,
+                                    int nStates, int nOutputs, int ZeroB, int ZeroC, int ZeroD, int uIndex,
+                                    double tStart, double tEnd, double tStep, const double* x0, int solver,
+                                    int precision, int shard, int shards, int nErr[])
+{
+    Library& L = lib();
+    std::lock_guard<std::recursive_mutex> g(L.mu);
+    ParODE_Plan* out = nullptr;
+    int rc = guarded([&] {
+        int dev = current_device_locked(L);
+        if (precision != PARODE_PRECISION_FP64 && precision != PARODE_PRECISION_MIXED &&
+            precision != PARODE_PRECISION_TF32)
+            throw Error(kInvalidArgument, "unknown precision");
+        if (shards < 1 || shard < 0 || shard >= shards) throw Error(kInvalidArgument, "shard index out of range");
+        SystemDesc s = make_system<double>(A, B, C, D, nInputs, nStates, nOutputs, ZeroB, ZeroC, ZeroD, x0);
+        PlanOptions opt;
+        opt.precision = precision;
+        opt.path = kPathBlockedResponse;  // the partition runs on the block-response leaf
+        opt.input_double = true;
+        opt.executions = (double)L.executions;
+        opt.shard = shard;
+        opt.shards = shards;
+        auto h = std::make_unique<ParODE_Plan>();
+        h->plan = std::make_unique<Plan>(dev, s, &L.inputs, uIndex, solver, tStart, tEnd, tStep, opt);
+        out = h.release();
+    });
+    if (nErr) nErr[0] = rc;
+    return out;
+}
+
+void ParODE_PlanShardInfo(const ParODE_Plan* plan, long long info[5])
+{
+    for (int k = 0; k < 5; ++k) info[k] = 0;
+    if (plan && plan->plan) plan->plan->shard_info(info);
+}
+
+void ParODE_PlanShardUp(ParODE_Plan* plan, double* dTop, void* stream, int nErr[])
+{
+    int rc = guarded([&] {
+        if (!plan || !plan->plan || !dTop) throw Error(kInvalidArgument, "null plan or buffer");
+        plan->plan->shard_up(dTop, (cudaStream_t)stream);
+    });
+    if (nErr) nErr[0] = rc;
+}
+
+void ParODE_PlanShardDown(ParODE_Plan* plan, const double* dGathered, double* yDev, void* stream, int nErr[])
+{
+    int rc = guarded([&] {
+        if (!plan || !plan->plan || !dGathered) throw Error(kInvalidArgument, "null plan or buffer");
+        plan->plan->shard_down(dGathered, yDev, (cudaStream_t)stream);
+    });
+    if (nErr) nErr[0] = rc;
+}
+
 void ParODE_PlanExecute(ParODE_Plan* plan, double* yDev, void* stream, int nErr[])
 {
     int rc = guarded([&] {

@@ -333,26 +333,33 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
     });
     phase("discretise", false);
     // ABM start-up: nine inputs at t0 + j h/2 (sinusoids on the host; user
-    // functions through their compiled kernel); the four states into x0, the
-    // outputs 0..2 into their slot
+    // functions through their compiled kernel, sampled first on this thread);
+    // the four states into x0, the outputs 0..2 into their slot (threads over
+    // systems)
+    std::vector<std::vector<double>> U9s(N);
     for (int i = 0; i < N; ++i) {
         Sys& q = sys_[i];
         if (q.solver != kABM) continue;
         const SystemDesc& s = specs[i].sys;
-        std::vector<double> U9((size_t)9 * std::max(s.m, 1), 0.0);
-        if (q.mu > 0) {
-            if (q.input->kind == InputEntry::kSinusoid) {
-                for (int j = 0; j < 9; ++j)
-                    for (int c = 0; c < q.mu; ++c) U9[(size_t)j * q.mu + c] = sinusoid_host(q.input, c, q.t0 + j * 0.5 * q.h);
-            } else {
-                double* dU9 = nullptr;
-                PARODE_CUDA(cudaMalloc(&dU9, sizeof(double) * 9 * q.mu));
-                inputs_->fill(q.input, device_, dU9, q.mu, q.t0, 0.5 * q.h, 9, opt_.input_double, nullptr);
-                cudaError_t e = cudaMemcpy(U9.data(), dU9, sizeof(double) * 9 * q.mu, cudaMemcpyDeviceToHost);
-                cudaFree(dU9);
-                PARODE_CUDA(e);
-            }
+        std::vector<double>& U9 = U9s[i];
+        U9.assign((size_t)9 * std::max(s.m, 1), 0.0);
+        if (q.mu > 0 && q.input->kind != InputEntry::kSinusoid) {
+            double* dU9 = nullptr;
+            PARODE_CUDA(cudaMalloc(&dU9, sizeof(double) * 9 * q.mu));
+            inputs_->fill(q.input, device_, dU9, q.mu, q.t0, 0.5 * q.h, 9, opt_.input_double, nullptr);
+            cudaError_t e = cudaMemcpy(U9.data(), dU9, sizeof(double) * 9 * q.mu, cudaMemcpyDeviceToHost);
+            cudaFree(dU9);
+            PARODE_CUDA(e);
         }
+    }
+    parallel_for(N, [&](int i) {
+        Sys& q = sys_[i];
+        if (q.solver != kABM) return;
+        const SystemDesc& s = specs[i].sys;
+        std::vector<double>& U9 = U9s[i];
+        if (q.mu > 0 && q.input->kind == InputEntry::kSinusoid)
+            for (int j = 0; j < 9; ++j)
+                for (int c = 0; c < q.mu; ++c) U9[(size_t)j * q.mu + c] = sinusoid_host(q.input, c, q.t0 + j * 0.5 * q.h);
         SystemDesc s0 = s;
         if (s0.zeroB) s0.m = 0;
         double* x0 = slot(off[i].x0);
@@ -374,7 +381,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
                 ypre[(size_t)k * q.p + o] = v;
             }
         }
-    }
+    });
     phase("abm-start-up", false);
     const size_t const_end = L.bytes;
     // work buffers (offsets only; not staged); per-kind totals for the log
@@ -580,6 +587,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         b.Cexts = reinterpret_cast<const double* const*>(base + jput(cexts.data(), sizeof(double*) * cexts.size()));
         b.X0s = reinterpret_cast<const double* const*>(base + jput(x0s.data(), sizeof(double*) * x0s.size()));
     }
+    phase("jobs/buckets", false);
     // input samples
     {
         std::vector<SampleJob> sj;
@@ -789,6 +797,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             }
             add_level(ls_power_, ents, -1);  // the power table stays FP64
         }
+        phase("jobs/power-levels", false);
         for (int l = 0; l < Lmax; ++l) {
             std::vector<std::pair<int, LevelArgs>> ents;
             for (int i : lv) {
@@ -835,6 +844,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             }
             add_level(ls_down_, ents, l);
         }
+        phase("jobs/scan-levels", false);
         // response GEMMs (FP64 tiled DMMA): the block aggregates into scan
         // slots 0 .. Tp - 1 (zeros past the last block), then the outputs from
         // [sample window; X_b], X_b = the scanned state in slot b - 1

@@ -87,7 +87,8 @@ __device__ __forceinline__ double sample_time(double base, double dt, long j)
 // sample.
 template <int L, int KT, class Out>
 __device__ __forceinline__ void sinusoid_run_terms(const double* a, const double* f, const double* phi, int i,
-                                                   double base, double dt, long j0, int n, const Out& out)
+                                                   double base, double dt, long j0, int n, const Out& out,
+                                                   long joff)
 {
     const double two_pi = 6.283185307179586476925286766559;
     double w[KT], ph[KT], amp[KT], prev[KT], s[KT], c[KT], dl[KT], sdl[KT], cdl[KT];
@@ -97,7 +98,7 @@ __device__ __forceinline__ void sinusoid_run_terms(const double* a, const double
         w[q] = __dmul_rn(two_pi, f[i * KT + q]);
         ph[q] = phi[i * KT + q];
         amp[q] = a[i * KT + q];
-        prev[q] = __dadd_rn(__dmul_rn(w[q], sample_time(base, dt, j0)), ph[q]);
+        prev[q] = __dadd_rn(__dmul_rn(w[q], sample_time(base, dt, joff + j0)), ph[q]);
         sincos(prev[q], &s[q], &c[q]);
         dl[q] = __dmul_rn(w[q], dt);
         sincos(dl[q], &sdl[q], &cdl[q]);
@@ -105,7 +106,7 @@ __device__ __forceinline__ void sinusoid_run_terms(const double* a, const double
     }
     if (n > 0) out(0, v);
     for (int j = 1; j < n; ++j) {
-        const double t = sample_time(base, dt, j0 + j);
+        const double t = sample_time(base, dt, joff + j0 + j);
         v = 0.0;
 #pragma unroll
         for (int q = 0; q < KT; ++q) {
@@ -128,23 +129,26 @@ __device__ __forceinline__ void sinusoid_run_terms(const double* a, const double
 }
 
 // KMAX (1..4): the largest term count given its own chains; a kernel's
-// registers follow the largest variant it contains.
+// registers follow the largest variant it contains.  Sample j of the run is
+// written at out(j) and taken at the time of sample joff + j0 + j (joff: the
+// index of the buffer's first sample on the whole horizon).
 template <int L, int KMAX, class Out>
 __device__ __forceinline__ void sinusoid_run(const double* a, const double* f, const double* phi, int K, int i,
-                                             double base, double dt, long j0, long count, const Out& out)
+                                             double base, double dt, long j0, long count, const Out& out,
+                                             long joff = 0)
 {
     const long rest = count - j0;
     const int n = rest < L ? (int)rest : L;
     if (K == 1) {
-        sinusoid_run_terms<L, 1>(a, f, phi, i, base, dt, j0, n, out);
+        sinusoid_run_terms<L, 1>(a, f, phi, i, base, dt, j0, n, out, joff);
     } else if (KMAX >= 2 && K == 2) {
-        sinusoid_run_terms<L, (KMAX >= 2 ? 2 : 1)>(a, f, phi, i, base, dt, j0, n, out);
+        sinusoid_run_terms<L, (KMAX >= 2 ? 2 : 1)>(a, f, phi, i, base, dt, j0, n, out, joff);
     } else if (KMAX >= 3 && K == 3) {
-        sinusoid_run_terms<L, (KMAX >= 3 ? 3 : 1)>(a, f, phi, i, base, dt, j0, n, out);
+        sinusoid_run_terms<L, (KMAX >= 3 ? 3 : 1)>(a, f, phi, i, base, dt, j0, n, out, joff);
     } else if (KMAX >= 4 && K == 4) {
-        sinusoid_run_terms<L, (KMAX >= 4 ? 4 : 1)>(a, f, phi, i, base, dt, j0, n, out);
+        sinusoid_run_terms<L, (KMAX >= 4 ? 4 : 1)>(a, f, phi, i, base, dt, j0, n, out, joff);
     } else {
-        for (int j = 0; j < n; ++j) out(j, sinusoid_value(a, f, phi, K, i, sample_time(base, dt, j0 + j)));
+        for (int j = 0; j < n; ++j) out(j, sinusoid_value(a, f, phi, K, i, sample_time(base, dt, joff + j0 + j)));
     }
 }
 

@@ -17,13 +17,14 @@ namespace {
 // Kernels/u.cl:6-11 (one value per (sample, input)), with the sample time
 // formed in FP64 before the conversion to fType.
 const char* kUKernelTail = R"(
-extern "C" __global__ void parode_u_samples(double* U, int m, double base, double dt, long long count)
+extern "C" __global__ void parode_u_samples(double* U, int m, double base, double dt, long long count,
+                                            long long joff)
 {
     long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= count * (long long)m) return;
     long long j = e / m;
     int i = (int)(e - j * m);
-    double t = __dadd_rn(base, __dmul_rn(dt, (double)j));
+    double t = __dadd_rn(base, __dmul_rn(dt, (double)(joff + j)));
     U[e] = (double)UFunc((fType)t, i);
 }
 )";
@@ -134,7 +135,7 @@ InputEntry* InputRegistry::get(int idx)
 }
 
 void InputRegistry::fill(InputEntry* e, int device, double* U, int m, double base, double dt, long count,
-                         bool double_type, cudaStream_t s)
+                         bool double_type, cudaStream_t s, long joff)
 {
     if (m <= 0 || count <= 0) return;
     if (e->kind == InputEntry::kSinusoid) {
@@ -143,31 +144,31 @@ void InputRegistry::fill(InputEntry* e, int device, double* U, int m, double bas
         const double* d = sinusoid_device(e, device);
         // the kernel indexes parameters as i*K + k for i < m, so a sinusoid
         // input wider than the system is read from its first m channels
-        launch_sinusoid_samples(U, m, e->K, d, d + q, d + 2 * q, base, dt, count, s);
+        launch_sinusoid_samples(U, m, e->K, d, d + q, d + 2 * q, base, dt, count, s, joff);
         return;
     }
     int v = double_type ? 1 : 0;
     if (!e->kern[v]) compile(e, v);
-    long long cnt = count;
-    void* args[] = {&U, &m, &base, &dt, &cnt};
+    long long cnt = count, off = joff;
+    void* args[] = {&U, &m, &base, &dt, &cnt, &off};
     long total = count * m;
     unsigned grid = (unsigned)((total + 255) / 256);
     PARODE_CUDA(cudaLaunchKernel((const void*)e->kern[v], dim3(grid), dim3(256), args, 0, s));
 }
 
 void InputRegistry::fill_planes(InputEntry* e, int device, float* hi, float* lo, double* scratch, int m, double base,
-                                double dt, long count, bool double_type, cudaStream_t s)
+                                double dt, long count, bool double_type, cudaStream_t s, long joff)
 {
     if (m <= 0 || count <= 0) return;
     if (e->kind == InputEntry::kSinusoid) {
         if (e->m < m) throw Error(kInvalidInput, "sinusoid input has fewer channels than the system");
         const long q = (long)e->m * e->K;
         const double* d = sinusoid_device(e, device);
-        launch_sinusoid_planes(hi, lo, m, e->K, d, d + q, d + 2 * q, base, dt, count, s);
+        launch_sinusoid_planes(hi, lo, m, e->K, d, d + q, d + 2 * q, base, dt, count, s, joff);
         return;
     }
     if (!scratch) throw Error(kInvalidArgument, "a user input function needs FP64 scratch for its samples");
-    fill(e, device, scratch, m, base, dt, count, double_type, s);
+    fill(e, device, scratch, m, base, dt, count, double_type, s, joff);
     launch_split_planes(scratch, hi, lo, count * m, s);
 }
 

@@ -39,15 +39,17 @@ public:
     void clear();
     int size() const { return (int)entries_.size(); }
 
-    // U[j*m + i] = u_i(base + dt*j) for j < count, i < m, enqueued on `s`.
-    // `double_type` selects the fType = double variant of a user function.
+    // U[j*m + i] = u_i(base + dt*(joff + j)) for j < count, i < m, enqueued
+    // on `s` (joff: the first sample's index on the whole horizon, for a time
+    // shard).  `double_type` selects the fType = double variant of a user
+    // function.
     void fill(InputEntry* e, int device, double* U, int m, double base, double dt, long count, bool double_type,
-              cudaStream_t s);
-    // The same samples as TF32 hi / lo planes (hi[j*m + i], lo[j*m + i]): the
-    // sinusoid input writes them directly; a user function fills `scratch`
-    // (count*m doubles) first.
+              cudaStream_t s, long joff = 0);
+    // The same samples as TF32 hi / lo planes (hi[j*m + i], lo[j*m + i]; lo
+    // may be null): the sinusoid input writes them directly; a user function
+    // fills `scratch` (count*m doubles) first.
     void fill_planes(InputEntry* e, int device, float* hi, float* lo, double* scratch, int m, double base,
-                     double dt, long count, bool double_type, cudaStream_t s);
+                     double dt, long count, bool double_type, cudaStream_t s, long joff = 0);
     // Device copy of a sinusoid input's parameters: a | f | phi, m*K each.
     const double* sinusoid_device(InputEntry* e, int device);
 

@@ -158,14 +158,25 @@ int response_log2_block(int solver, int NP, int n, int m, int p, long nScan, dou
 // Q = P_{l0} (P: power table, level l at l NP^2).  Chunks of 16 per level;
 // level h uses P_{l0 + 4h}, so the table must reach level
 // l0 + 4 chunk_carry_levels(count).  work: chunk_carry_scratch(count) NP
-// doubles.  after_first (optional) is recorded on s once the level-0 up-sweep
-// is issued (at once when there is none): from there on the carry's launches
-// are small, and work beside it can take the other SMs.  Returns the launches
-// made.
+// doubles.  Returns the launches made.
 int chunk_carry_levels(long count);
 long chunk_carry_scratch(long count);
 int launch_chunk_carry(int NP, double* items, long count, const double* P, int l0, const double* X0, double* work,
-                       cudaStream_t s, cudaEvent_t after_first = nullptr);
+                       cudaStream_t s);
+// The same scan in its two halves, for a scan whose top level is done
+// elsewhere (the time partition of one solve across devices): the up-sweep
+// leaves the chunk aggregates of level h in arr[h] (h = `levels`, or while
+// more than 16 items remain when levels < 0); once arr[h] holds the states
+// entering its items, the down-sweep rewrites every lower level (items end as
+// the states entering them).
+struct ChunkLevels {
+    double* arr[16] = {};
+    long cnt[16] = {};
+    int h = 0;
+};
+int launch_chunk_up(int NP, double* items, long count, const double* P, int l0, double* work, int levels,
+                    ChunkLevels* L, cudaStream_t s);
+int launch_chunk_down(int NP, const ChunkLevels& L, const double* P, int l0, cudaStream_t s);
 
 // Columns of a level that can reach an output.  Column g combines the
 // segments [g 2d, g 2d + d) and [g 2d + d, g 2d + 2d) of the time axis; when
@@ -179,12 +190,12 @@ inline long sweep_columns(long nScan, long Tp, long d)
 
 // U[j*m + i] = sum_k a sin(2 pi f t_j + phi), t_j = base + dt*j, j < count.
 void launch_sinusoid_samples(double* U, int m, int K, const double* a, const double* f, const double* phi,
-                             double base, double dt, long count, cudaStream_t s);
+                             double base, double dt, long count, cudaStream_t s, long joff = 0);
 
 // The same samples written as TF32 hi / lo planes (hi = TF32(x),
 // lo = TF32(x - hi), x = float(u)), the tensor-core GEMMs' operand form.
 void launch_sinusoid_planes(float* hi, float* lo, int m, int K, const double* a, const double* f, const double* phi,
-                            double base, double dt, long count, cudaStream_t s);
+                            double base, double dt, long count, cudaStream_t s, long joff = 0);
 // FP64 samples into those planes (n values).  lo may be null in both (hi only).
 void launch_split_planes(const double* U, float* hi, float* lo, long n, cudaStream_t s);
 

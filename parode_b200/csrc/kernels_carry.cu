@@ -238,42 +238,61 @@ __global__ void __launch_bounds__(kThreads) k_chunk_down(double* __restrict__ it
 
 // ---------------------------------------------------------------------------
 template <int NP>
-int chunk_carry_t(double* items, long count, const double* P, int l0, const double* X0, double* work, cudaStream_t s,
-                  cudaEvent_t after_first)
+int chunk_up_t(double* items, long count, const double* P, int l0, double* work, int levels, ChunkLevels* L,
+               cudaStream_t s)
 {
     const long mat = (long)NP * NP;
-    double* arr[16];
-    long cnt[16];
+    L->arr[0] = items;
+    L->cnt[0] = count;
     int h = 0;
-    arr[0] = items;
-    cnt[0] = count;
     double* w = work;
     int launches = 0;
-    while (cnt[h] > kChunk) {
+    while (levels < 0 ? L->cnt[h] > kChunk : h < levels) {
         if (h + 1 >= 16) throw Error(kInvalidArgument, "chunk carry: too many levels");
-        const long nc = (cnt[h] + kChunk - 1) / kChunk;
+        const long nc = (L->cnt[h] + kChunk - 1) / kChunk;
         const unsigned grid = (unsigned)((nc + kCols - 1) / kCols);
-        k_chunk_up<NP><<<grid, kThreads, 0, s>>>(arr[h], cnt[h], P + (long)(l0 + 4 * h) * mat, w);
+        k_chunk_up<NP><<<grid, kThreads, 0, s>>>(L->arr[h], L->cnt[h], P + (long)(l0 + 4 * h) * mat, w);
         PARODE_CUDA(cudaGetLastError());
-        if (h == 0 && after_first) PARODE_CUDA(cudaEventRecord(after_first, s));
         ++launches;
-        arr[h + 1] = w;
-        cnt[h + 1] = nc;
+        L->arr[h + 1] = w;
+        L->cnt[h + 1] = nc;
         w += nc * NP;
         ++h;
     }
-    if (h == 0 && after_first) PARODE_CUDA(cudaEventRecord(after_first, s));
-    // top: one chunk of the remaining items, entered with the initial state
-    k_chunk_down<NP><<<1, kThreads, 0, s>>>(arr[h], cnt[h], P + (long)(l0 + 4 * h) * mat, X0, (int)cnt[h]);
-    PARODE_CUDA(cudaGetLastError());
-    ++launches;
-    for (int k = h - 1; k >= 0; --k) {
-        const long nc = (cnt[k] + kChunk - 1) / kChunk;
+    L->h = h;
+    return launches;
+}
+
+template <int NP>
+int chunk_down_t(const ChunkLevels& L, const double* P, int l0, cudaStream_t s)
+{
+    const long mat = (long)NP * NP;
+    for (int k = L.h - 1; k >= 0; --k) {
+        const long nc = (L.cnt[k] + kChunk - 1) / kChunk;
         const unsigned grid = (unsigned)((nc + kCols - 1) / kCols);
-        k_chunk_down<NP><<<grid, kThreads, 0, s>>>(arr[k], cnt[k], P + (long)(l0 + 4 * k) * mat, arr[k + 1], kChunk);
+        k_chunk_down<NP><<<grid, kThreads, 0, s>>>(L.arr[k], L.cnt[k], P + (long)(l0 + 4 * k) * mat, L.arr[k + 1],
+                                                   kChunk);
         PARODE_CUDA(cudaGetLastError());
-        ++launches;
     }
+    return L.h;
+}
+
+template <int NP>
+int chunk_top_t(double* items, long count, const double* Q, const double* X0, cudaStream_t s)
+{
+    // one chunk of at most 16 items, entered with X0
+    k_chunk_down<NP><<<1, kThreads, 0, s>>>(items, count, Q, X0, (int)count);
+    PARODE_CUDA(cudaGetLastError());
+    return 1;
+}
+
+template <int NP>
+int chunk_carry_t(double* items, long count, const double* P, int l0, const double* X0, double* work, cudaStream_t s)
+{
+    ChunkLevels L;
+    int launches = chunk_up_t<NP>(items, count, P, l0, work, -1, &L, s);
+    launches += chunk_top_t<NP>(L.arr[L.h], L.cnt[L.h], P + (long)(l0 + 4 * L.h) * NP * NP, X0, s);
+    launches += chunk_down_t<NP>(L, P, l0, s);
     return launches;
 }
 
@@ -299,22 +318,47 @@ long chunk_carry_scratch(long count)
     return total;
 }
 
-int launch_chunk_carry(int NP, double* items, long count, const double* P, int l0, const double* X0, double* work,
-                       cudaStream_t s, cudaEvent_t after_first)
-{
-    if (count <= 0) {
-        if (after_first) PARODE_CUDA(cudaEventRecord(after_first, s));
-        return 0;
+#define PARODE_NP_SWITCH(NP, CALL)                                                             \
+    switch (NP) {                                                                              \
+    case 8: return CALL(8);                                                                    \
+    case 16: return CALL(16);                                                                  \
+    case 24: return CALL(24);                                                                  \
+    case 32: return CALL(32);                                                                  \
+    case 40: return CALL(40);                                                                  \
+    case 48: return CALL(48);                                                                  \
+    case 56: return CALL(56);                                                                  \
+    case 64: return CALL(64);                                                                  \
+    default: throw Error(kInvalidArgument, "chunk carry: NP must be a multiple of 8 up to 64"); \
     }
+
+int launch_chunk_up(int NP, double* items, long count, const double* P, int l0, double* work, int levels,
+                    ChunkLevels* L, cudaStream_t s)
+{
+#define PARODE_UP(K) chunk_up_t<K>(items, count, P, l0, work, levels, L, s)
+    PARODE_NP_SWITCH(NP, PARODE_UP)
+#undef PARODE_UP
+}
+
+int launch_chunk_down(int NP, const ChunkLevels& L, const double* P, int l0, cudaStream_t s)
+{
+#define PARODE_DOWN(K) chunk_down_t<K>(L, P, l0, s)
+    PARODE_NP_SWITCH(NP, PARODE_DOWN)
+#undef PARODE_DOWN
+}
+
+int launch_chunk_carry(int NP, double* items, long count, const double* P, int l0, const double* X0, double* work,
+                       cudaStream_t s)
+{
+    if (count <= 0) return 0;
     switch (NP) {
-    case 8: return chunk_carry_t<8>(items, count, P, l0, X0, work, s, after_first);
-    case 16: return chunk_carry_t<16>(items, count, P, l0, X0, work, s, after_first);
-    case 24: return chunk_carry_t<24>(items, count, P, l0, X0, work, s, after_first);
-    case 32: return chunk_carry_t<32>(items, count, P, l0, X0, work, s, after_first);
-    case 40: return chunk_carry_t<40>(items, count, P, l0, X0, work, s, after_first);
-    case 48: return chunk_carry_t<48>(items, count, P, l0, X0, work, s, after_first);
-    case 56: return chunk_carry_t<56>(items, count, P, l0, X0, work, s, after_first);
-    case 64: return chunk_carry_t<64>(items, count, P, l0, X0, work, s, after_first);
+    case 8: return chunk_carry_t<8>(items, count, P, l0, X0, work, s);
+    case 16: return chunk_carry_t<16>(items, count, P, l0, X0, work, s);
+    case 24: return chunk_carry_t<24>(items, count, P, l0, X0, work, s);
+    case 32: return chunk_carry_t<32>(items, count, P, l0, X0, work, s);
+    case 40: return chunk_carry_t<40>(items, count, P, l0, X0, work, s);
+    case 48: return chunk_carry_t<48>(items, count, P, l0, X0, work, s);
+    case 56: return chunk_carry_t<56>(items, count, P, l0, X0, work, s);
+    case 64: return chunk_carry_t<64>(items, count, P, l0, X0, work, s);
     default: throw Error(kInvalidArgument, "chunk carry: NP must be a multiple of 8 up to 64");
     }
 }

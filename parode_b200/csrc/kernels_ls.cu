@@ -341,7 +341,7 @@ __global__ void k_swap_grouped(const LevelArgs* __restrict__ args)
 // One thread per (run of kSampleRun samples, channel); channels fastest.
 template <int KMAX>
 __global__ void k_sinusoid_samples(double* U, int m, int K, const double* a, const double* f, const double* phi,
-                                   double base, double dt, long count)
+                                   double base, double dt, long count, long joff)
 {
     const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
     const long runs = (count + kSampleRun - 1) / kSampleRun;
@@ -349,13 +349,13 @@ __global__ void k_sinusoid_samples(double* U, int m, int K, const double* a, con
     const long r = e / m;
     const int i = (int)(e - r * m);
     const long j0 = r * kSampleRun;
-    sinusoid_run<kSampleRun, KMAX>(a, f, phi, K, i, base, dt, j0, count, SampleOut64{U + j0 * m + i, m});
+    sinusoid_run<kSampleRun, KMAX>(a, f, phi, K, i, base, dt, j0, count, SampleOut64{U + j0 * m + i, m}, joff);
 }
 
 // The same samples as TF32 hi / lo planes (the tensor-core GEMMs' operands).
 template <int KMAX>
 __global__ void k_sinusoid_planes(float* hi, float* lo, int m, int K, const double* a, const double* f,
-                                  const double* phi, double base, double dt, long count)
+                                  const double* phi, double base, double dt, long count, long joff)
 {
     const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
     const long runs = (count + kSampleRun - 1) / kSampleRun;
@@ -364,7 +364,7 @@ __global__ void k_sinusoid_planes(float* hi, float* lo, int m, int K, const doub
     const int i = (int)(e - r * m);
     const long j0 = r * kSampleRun;
     sinusoid_run<kSampleRun, KMAX>(a, f, phi, K, i, base, dt, j0, count,
-                                   SampleOutSplit{hi + j0 * m + i, lo + j0 * m + i, m});
+                                   SampleOutSplit{hi + j0 * m + i, lo ? lo + j0 * m + i : nullptr, m}, joff);
 }
 
 // FP64 samples (any input function) into TF32 hi / lo planes.
@@ -616,31 +616,31 @@ void launch_affine_level(const LevelArgs& a, cudaStream_t s)
 }
 
 void launch_sinusoid_samples(double* U, int m, int K, const double* a, const double* f, const double* phi,
-                             double base, double dt, long count, cudaStream_t s)
+                             double base, double dt, long count, cudaStream_t s, long joff)
 {
     if (count <= 0 || m <= 0) return;
     const long total = (count + kSampleRun - 1) / kSampleRun * m;
     const unsigned g = (unsigned)blocks_for(total, 256);
     switch (sample_kmax(K)) {
-    case 1: k_sinusoid_samples<1><<<g, 256, 0, s>>>(U, m, K, a, f, phi, base, dt, count); break;
-    case 2: k_sinusoid_samples<2><<<g, 256, 0, s>>>(U, m, K, a, f, phi, base, dt, count); break;
-    case 3: k_sinusoid_samples<3><<<g, 256, 0, s>>>(U, m, K, a, f, phi, base, dt, count); break;
-    default: k_sinusoid_samples<4><<<g, 256, 0, s>>>(U, m, K, a, f, phi, base, dt, count); break;
+    case 1: k_sinusoid_samples<1><<<g, 256, 0, s>>>(U, m, K, a, f, phi, base, dt, count, joff); break;
+    case 2: k_sinusoid_samples<2><<<g, 256, 0, s>>>(U, m, K, a, f, phi, base, dt, count, joff); break;
+    case 3: k_sinusoid_samples<3><<<g, 256, 0, s>>>(U, m, K, a, f, phi, base, dt, count, joff); break;
+    default: k_sinusoid_samples<4><<<g, 256, 0, s>>>(U, m, K, a, f, phi, base, dt, count, joff); break;
     }
     PARODE_CUDA(cudaGetLastError());
 }
 
 void launch_sinusoid_planes(float* hi, float* lo, int m, int K, const double* a, const double* f, const double* phi,
-                            double base, double dt, long count, cudaStream_t s)
+                            double base, double dt, long count, cudaStream_t s, long joff)
 {
     if (count <= 0 || m <= 0) return;
     const long total = (count + kSampleRun - 1) / kSampleRun * m;
     const unsigned g = (unsigned)blocks_for(total, 256);
     switch (sample_kmax(K)) {
-    case 1: k_sinusoid_planes<1><<<g, 256, 0, s>>>(hi, lo, m, K, a, f, phi, base, dt, count); break;
-    case 2: k_sinusoid_planes<2><<<g, 256, 0, s>>>(hi, lo, m, K, a, f, phi, base, dt, count); break;
-    case 3: k_sinusoid_planes<3><<<g, 256, 0, s>>>(hi, lo, m, K, a, f, phi, base, dt, count); break;
-    default: k_sinusoid_planes<4><<<g, 256, 0, s>>>(hi, lo, m, K, a, f, phi, base, dt, count); break;
+    case 1: k_sinusoid_planes<1><<<g, 256, 0, s>>>(hi, lo, m, K, a, f, phi, base, dt, count, joff); break;
+    case 2: k_sinusoid_planes<2><<<g, 256, 0, s>>>(hi, lo, m, K, a, f, phi, base, dt, count, joff); break;
+    case 3: k_sinusoid_planes<3><<<g, 256, 0, s>>>(hi, lo, m, K, a, f, phi, base, dt, count, joff); break;
+    default: k_sinusoid_planes<4><<<g, 256, 0, s>>>(hi, lo, m, K, a, f, phi, base, dt, count, joff); break;
     }
     PARODE_CUDA(cudaGetLastError());
 }

@@ -40,6 +40,8 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
     if (Np_ > 1024) throw Error(kInvalidSystem, "scan dimension above 1024 is not supported");
     if (opt.path == kPathGeneral && Ns_ > 64)
         throw Error(kInvalidArgument, "the general scan supports scan dimensions up to 64");
+    if ((opt.shards > 1 || opt.shard != 0) && (Ns_ > 64 || opt.path == kPathGeneral || opt.path == kPathLevel))
+        throw Error(kInvalidArgument, "a time shard runs on the block-response path (scan dimension <= 64, inputs)");
     if (Ns_ > 64 && opt.path != kPathBlocked && opt.path != kPathBlockedSweep) {
         // scan dimensions above 64: the batch engine's one-system form (the
         // response leaf or the level-synchronous scan, tensor-core levels in
@@ -162,6 +164,7 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
         if (opt.path == kPathBlockedResponse && !br_)
             throw Error(kInvalidArgument, "the response leaf needs inputs");
     }
+    if (opt.shards > 1 || opt.shard != 0) setup_shard(opt);
     PARODE_CUDA(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_));
 
     PARODE_CUDA(cudaSetDevice(device_));
@@ -203,7 +206,13 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
         }
     } else {
         alloc(&dG_, nblocks_ * (long)Np_);
-        alloc(&dWork_, std::max(blocked_items_scratch(shape_, nblocks_), chunk_carry_scratch(nblocks_) + 1) * (long)Np_);
+        alloc(&dWork_, std::max(blocked_items_scratch(shape_, nblocks_), chunk_carry_scratch(nblocks_) + 1 + shard_k_) *
+                           (long)Np_);
+        if (shards_ > 1) {
+            // the gathered top items of every shard, then the scratch of their scan
+            const long items = (long)shards_ * shard_c_;
+            alloc(&dTop_, (items + chunk_carry_scratch(items) + 1) * (long)Np_);
+        }
         alloc(&dCP_, (long)shape_.B * p_ * Np_);
         alloc(&dCext_, (long)p_ * Np_);
         // output rows of the scan state: C at the state block (the last n of
@@ -225,12 +234,14 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
         nU_ = 2 * nScan_ + 1;
         u_base_ = t0;
         u_dt_ = 0.5 * h;
+        u_joff_ = 2 * shard_begin_;
     } else {
         // ABM scan inputs on the grid (t0 + 3h) - 3h + j h
         // (reference Sources/AdamsMoulton.cpp:426-432 with FP64 time)
         nU_ = nScan_ + 4;
         u_base_ = (t0 + 3.0 * h) - 3.0 * h;
         u_dt_ = h;
+        u_joff_ = shard_begin_;
     }
     if (mu_ > 0 && !gen_) {
         // the response leaf reads whole windows: the last block's window runs
@@ -381,22 +392,11 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
             r[1].fault_withhold = 0;
             const long start[2] = {0, resp_tc_tiles(r[0])};
             const long tiles = start[1] + resp_tc_tiles(r[1]);
-            std::vector<long> ranges;
-            // with two or more carry levels the output windows run beside the
-            // carry's small upper-level launches (on the SMs those leave
-            // free), the aggregates alone before it; else both in one launch
-            tc_overlap_ = chunk_carry_levels(nblocks_) >= 2 && sms_ >= 64;
-            if (tc_overlap_) {
-                const long c1 = (nblocks_ + 15) / 16, upper = ((c1 + 15) / 16 + 7) / 8;
-                tcCtas_ = (int)std::min<long>(sms_, start[1]);
-                tcCtasW_ = (int)std::min<long>(sms_ - std::min<long>(upper, sms_ / 2), resp_tc_tiles(r[1]));
-                ranges = resp_tc_ranges({r[0]}, tcCtas_);
-                const std::vector<long> rw = resp_tc_ranges({r[1]}, tcCtasW_);
-                ranges.insert(ranges.end(), rw.begin(), rw.end());
-            } else {
-                tcCtas_ = (int)std::min<long>(sms_, tiles);
-                ranges = resp_tc_ranges({r[0], r[1]}, tcCtas_);
-            }
+            // both GEMMs in one persistent launch (the output windows beside
+            // the carry on a second stream slowed the latency-bound carry
+            // launches more than they saved)
+            tcCtas_ = (int)std::min<long>(sms_, tiles);
+            const std::vector<long> ranges = resp_tc_ranges({r[0], r[1]}, tcCtas_);
             double* d = nullptr;
             alloc(&d, (long)((2 * sizeof(LevelArgs) + 7) / 8));
             dTc_ = reinterpret_cast<LevelArgs*>(d);
@@ -458,8 +458,6 @@ Plan::~Plan()
     if (stream_) cudaStreamSynchronize(stream_);
     if (side_) cudaStreamSynchronize(side_);
     for (cudaEvent_t e : events_) cudaEventDestroy(e);
-    for (cudaEvent_t e : side_ev_)
-        if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : fork_)
         if (e) cudaEventDestroy(e);
     if (done_) cudaEventDestroy(done_);
@@ -499,16 +497,6 @@ void Plan::mark(const char* stage, cudaStream_t s)
     PARODE_CUDA(cudaEventRecord(events_[k], s));
 }
 
-void Plan::side_span(int end)
-{
-    // the output-window launch on the side stream, timed apart from the
-    // stages of the main stream
-    if (!profiling_) return;
-    if (!side_ev_[end]) PARODE_CUDA(cudaEventCreate(&side_ev_[end]));
-    PARODE_CUDA(cudaEventRecord(side_ev_[end], side_));
-    side_marked_ = end == 1;
-}
-
 std::vector<std::pair<std::string, float>> Plan::stage_times()
 {
     std::vector<std::pair<std::string, float>> out;
@@ -519,24 +507,20 @@ std::vector<std::pair<std::string, float>> Plan::stage_times()
         PARODE_CUDA(cudaEventElapsedTime(&ms, events_[k - 1], events_[k]));
         out.emplace_back(marks_[k], ms);
     }
-    if (side_marked_) {
-        float ms = 0.f;
-        PARODE_CUDA(cudaEventSynchronize(side_ev_[1]));
-        PARODE_CUDA(cudaEventElapsedTime(&ms, side_ev_[0], side_ev_[1]));
-        out.emplace_back("windows (side stream)", ms);
-    }
     return out;
 }
 
 void Plan::fill_inputs(cudaStream_t s)
 {
     if (mu_ <= 0) return;
-    if (dUh_) inputs_->fill_planes(input_, device_, dUh_, dUl_, dU_, mu_, u_base_, u_dt_, nU_, opt_.input_double, s);
-    else inputs_->fill(input_, device_, dU_, mu_, u_base_, u_dt_, nU_, opt_.input_double, s);
+    if (dUh_)
+        inputs_->fill_planes(input_, device_, dUh_, dUl_, dU_, mu_, u_base_, u_dt_, nU_, opt_.input_double, s, u_joff_);
+    else inputs_->fill(input_, device_, dU_, mu_, u_base_, u_dt_, nU_, opt_.input_double, s, u_joff_);
 }
 
 void Plan::execute(double* y, cudaStream_t s)
 {
+    if (shards_ > 1) throw Error(kInvalidArgument, "a time-shard plan runs through its up and down phases");
     PARODE_CUDA(cudaSetDevice(device_));
     if (!s) s = stream_;
     execute_body(y, s);
@@ -705,82 +689,16 @@ void Plan::execute_general(double* Y, cudaStream_t s)
     last_y_ = Y;
 }
 
-int Plan::carry(cudaStream_t s, cudaEvent_t after_first)
+int Plan::carry(cudaStream_t s)
 {
     // the exclusive scan of the block aggregates (kernels_carry.cu)
-    return launch_chunk_carry(Np_, dG_, nblocks_, dPow_, shape_.R, dX0_, dWork_, s, after_first);
+    return launch_chunk_carry(Np_, dG_, nblocks_, dPow_, shape_.R, dX0_, dWork_, s);
 }
 
-void Plan::execute_response(double* Y, cudaStream_t s)
+LevelArgs Plan::response_agg_args() const
 {
-    // leaf = W x [sample window; initial state] per block (kernels_br.cu):
-    // aggregates first (the state columns are not used), then the carry, then
-    // the outputs with the carried block states, written straight into y
-    // (rows (j, o) of block b are contiguous there).  The power table
-    // P_1..P_levels was formed with W when the plan was made.
-    int launches = 0;
-    marks_.clear();
-    side_marked_ = false;
-    mark("start", s);
-    fill_inputs(s);
-    ++launches;
-    mark("inputs", s);
-    const int ybase = solver_ == kRK4 ? 0 : 3;
+    // FP64 aggregates G = W_agg [sample window] per block (tiled DMMA GEMM)
     const long ld = brKpad_ + Np_;
-    if (br_tc_) {
-        // mixed: aggregates and output windows (tensor cores) -> carry ->
-        // y = windows + C Phi^j X_b (FP64)
-        if (tc_overlap_) {
-            // aggregates -> carry, the output windows on the side stream from
-            // the end of the carry's level-0 up-sweep (kernels.h)
-            launch_resp_tc(dResp_, dTcStart_, 1, dTcCta_, tcCtas_, dStatus_, one_pass_, s);
-            ++launches;
-            mark("aggregates", s);
-            launches += carry(s, fork_[2]);
-            PARODE_CUDA(cudaStreamWaitEvent(side_, fork_[2], 0));
-            side_span(0);
-            launch_resp_tc(dResp_ + 1, dTcStart_, 1, dTcCta_ + tcCtas_ + 1, tcCtasW_, dStatus_, one_pass_, side_);
-            side_span(1);
-            ++launches;
-            PARODE_CUDA(cudaEventRecord(fork_[3], side_));
-            PARODE_CUDA(cudaStreamWaitEvent(s, fork_[3], 0));
-            mark("carry+windows", s);
-        } else {
-            launch_resp_tc(dResp_, dTcStart_, 2, dTcCta_, tcCtas_, dStatus_, one_pass_, s);
-            ++launches;
-            mark("aggregates+windows", s);
-            launches += carry(s);
-            mark("carry", s);
-        }
-        // y = windows + (C Phi^j) X_b: W's state columns stay in shared
-        // memory (kernels_state.cu); the general tiled GEMM where they do not fit
-        if (!launch_state_out(Np_, dW_ + brKpad_, ld, shape_.B * p_, dG_, dY_ + ybase * p_, Y + ybase * p_,
-                              (long)shape_.B * p_, nblocks_, nScan_ * p_, sms_, s)) {
-            LevelArgs x;
-            x.P = dW_ + brKpad_;
-            x.ldp = ld;
-            x.Np = Np_;
-            x.M = shape_.B * p_;
-            x.K = Np_;
-            x.ncols = nblocks_;
-            x.src = dG_;
-            x.src_gs = Np_;
-            x.src_ks = 1;
-            x.acc = dY_ + ybase * p_;
-            x.acc_gs = (long)shape_.B * p_;
-            x.dst = Y + ybase * p_;
-            x.dst_gs = (long)shape_.B * p_;
-            x.dst_limit = nScan_ * p_;
-            launch_gemm_tiled(x, s);
-        }
-        ++launches;
-        if (solver_ == kABM)
-            PARODE_CUDA(cudaMemcpyAsync(Y, dYpre_, sizeof(double) * 3 * p_, cudaMemcpyDeviceToDevice, s));
-        mark("outputs", s);
-        launches_ = launches;
-        last_y_ = Y;
-        return;
-    }
     LevelArgs g;
     g.P = dW_ + (long)shape_.B * p_ * ld;
     g.ldp = ld;
@@ -794,12 +712,16 @@ void Plan::execute_response(double* Y, cudaStream_t s)
     g.dst = dG_;
     g.dst_gs = Np_;
     g.dst_is = 1;
-    launch_gemm_tiled(g, s);
-    ++launches;
-    mark("aggregates", s);
-    launches += carry(s);
-    mark("carry", s);
-    LevelArgs h = g;
+    return g;
+}
+
+LevelArgs Plan::response_out_args(double* Y) const
+{
+    // FP64 outputs y = W_out [sample window ; X_b] per block, written into y
+    // (rows (j, o) of block b are contiguous there)
+    const long ld = brKpad_ + Np_;
+    const int ybase = solver_ == kRK4 ? 0 : 3;
+    LevelArgs h = response_agg_args();
     h.P = dW_;
     h.M = shape_.B * p_;
     h.K = (int)ld;
@@ -809,13 +731,173 @@ void Plan::execute_response(double* Y, cudaStream_t s)
     h.dst = Y + ybase * p_;
     h.dst_gs = (long)shape_.B * p_;
     h.dst_limit = nScan_ * p_;
-    launch_gemm_tiled(h, s);
+    return h;
+}
+
+void Plan::state_part(double* Y, cudaStream_t s)
+{
+    // mixed: y = windows + (C Phi^j) X_b, W's state columns resident in shared
+    // memory (kernels_state.cu); the general tiled GEMM where they do not fit
+    const int ybase = solver_ == kRK4 ? 0 : 3;
+    const long ld = brKpad_ + Np_;
+    if (launch_state_out(Np_, dW_ + brKpad_, ld, shape_.B * p_, dG_, dY_ + ybase * p_, Y + ybase * p_,
+                         (long)shape_.B * p_, nblocks_, nScan_ * p_, sms_, s))
+        return;
+    LevelArgs x;
+    x.P = dW_ + brKpad_;
+    x.ldp = ld;
+    x.Np = Np_;
+    x.M = shape_.B * p_;
+    x.K = Np_;
+    x.ncols = nblocks_;
+    x.src = dG_;
+    x.src_gs = Np_;
+    x.src_ks = 1;
+    x.acc = dY_ + ybase * p_;
+    x.acc_gs = (long)shape_.B * p_;
+    x.dst = Y + ybase * p_;
+    x.dst_gs = (long)shape_.B * p_;
+    x.dst_limit = nScan_ * p_;
+    launch_gemm_tiled(x, s);
+}
+
+void Plan::execute_response(double* Y, cudaStream_t s)
+{
+    // leaf = W x [sample window; initial state] per block (kernels_br.cu):
+    // aggregates first (the state columns are not used), then the carry, then
+    // the outputs with the carried block states, written straight into y
+    // (rows (j, o) of block b are contiguous there).  The power table
+    // P_1..P_levels was formed with W when the plan was made.
+    int launches = 0;
+    marks_.clear();
+    mark("start", s);
+    fill_inputs(s);
+    ++launches;
+    mark("inputs", s);
+    if (br_tc_) {
+        // mixed: aggregates and output windows (tensor cores) -> carry ->
+        // y = windows + C Phi^j X_b (FP64)
+        launch_resp_tc(dResp_, dTcStart_, 2, dTcCta_, tcCtas_, dStatus_, one_pass_, s);
+        ++launches;
+        mark("aggregates+windows", s);
+        launches += carry(s);
+        mark("carry", s);
+        state_part(Y, s);
+        ++launches;
+        if (solver_ == kABM)
+            PARODE_CUDA(cudaMemcpyAsync(Y, dYpre_, sizeof(double) * 3 * p_, cudaMemcpyDeviceToDevice, s));
+        mark("outputs", s);
+        launches_ = launches;
+        last_y_ = Y;
+        return;
+    }
+    launch_gemm_tiled(response_agg_args(), s);
+    ++launches;
+    mark("aggregates", s);
+    launches += carry(s);
+    mark("carry", s);
+    launch_gemm_tiled(response_out_args(Y), s);
     ++launches;
     if (solver_ == kABM)
         PARODE_CUDA(cudaMemcpyAsync(Y, dYpre_, sizeof(double) * 3 * p_, cudaMemcpyDeviceToDevice, s));
     mark("outputs", s);
     launches_ = launches;
     last_y_ = Y;
+}
+
+void Plan::setup_shard(const PlanOptions& opt)
+{
+    // Time shard `shard` of `shards` (the reference's multi-device split of
+    // the horizon, Sources/RungeKutta4thOrder.cpp:96-125, with its carry
+    // between devices, Sources/GPUFixedStepIterative.cpp:296-337): every
+    // shard but the last holds S = c 16^k whole blocks, so the chunked
+    // carry's first k levels stay inside a shard and the shards' level-k
+    // chunk aggregates (c per shard) line up as one sequence; that sequence
+    // is scanned by every shard (it is small) after an all-gather, and each
+    // shard down-sweeps its own levels from its items' prefixes.
+    if (opt.shards < 1 || opt.shard < 0 || opt.shard >= opt.shards)
+        throw Error(kInvalidArgument, "shard index out of range");
+    if (!br_ || batch_)
+        throw Error(kInvalidArgument, "a time shard runs on the block-response path (scan dimension <= 64, inputs)");
+    const long B = shape_.B;
+    const long nbG = (nScan_ + B - 1) / B;
+    const long per = (nbG + opt.shards - 1) / opt.shards;
+    int k = 0;
+    long p16 = 1;  // 16^k, with c = per / 16^k in [16, 256) once per >= 256
+    while (p16 * 256 <= per) {
+        p16 *= 16;
+        ++k;
+    }
+    const long c = (per + p16 - 1) / p16;
+    const long Sb = p16 * c;
+    const long b0 = (long)opt.shard * Sb;
+    if (b0 >= nbG) throw Error(kInvalidArgument, "more shards than the horizon's blocks fill");
+    shard_ = opt.shard;
+    shards_ = opt.shards;
+    shard_k_ = k;
+    shard_c_ = (int)c;
+    shard_begin_ = b0 * B;
+    nScanGlobal_ = nScan_;
+    nScan_ = std::min(Sb * B, nScan_ - shard_begin_);
+    nOut_ = nScan_ + (solver_ == kABM ? 3 : 0);
+    nblocks_ = (nScan_ + B - 1) / B;
+    // the power table reaches the top scan's levels: P_{R + 4 (k + h)}
+    levels_ = shape_.R + 4 * (k + chunk_carry_levels((long)shards_ * c)) + 1;
+}
+
+void Plan::shard_info(long long info[5]) const
+{
+    info[0] = shard_begin_;
+    info[1] = nScan_;
+    info[2] = shard_c_;
+    info[3] = Np_;
+    info[4] = shards_;
+}
+
+void Plan::shard_up(double* dTop, cudaStream_t s)
+{
+    if (shards_ < 1 || !dTop_) throw Error(kInvalidArgument, "not a time-shard plan");
+    PARODE_CUDA(cudaSetDevice(device_));
+    if (!s) s = stream_;
+    fill_inputs(s);
+    if (br_tc_) launch_resp_tc(dResp_, dTcStart_, 2, dTcCta_, tcCtas_, dStatus_, one_pass_, s);
+    else launch_gemm_tiled(response_agg_args(), s);
+    // the first k chunk levels, from a zero state: the shard's level-k chunk
+    // aggregates (fewer than c in a short last shard: zeros after them)
+    launch_chunk_up(Np_, dG_, nblocks_, dPow_, shape_.R, dWork_, shard_k_, &shard_levels_, s);
+    const ChunkLevels& L = shard_levels_;
+    PARODE_CUDA(cudaMemsetAsync(dTop, 0, sizeof(double) * (size_t)shard_c_ * Np_, s));
+    PARODE_CUDA(cudaMemcpyAsync(dTop, L.arr[L.h], sizeof(double) * (size_t)L.cnt[L.h] * Np_, cudaMemcpyDeviceToDevice,
+                                s));
+    shard_up_done_ = true;
+}
+
+void Plan::shard_down(const double* dGathered, double* Y, cudaStream_t s)
+{
+    if (!shard_up_done_) throw Error(kInvalidArgument, "shard_down before shard_up");
+    PARODE_CUDA(cudaSetDevice(device_));
+    if (!s) s = stream_;
+    if (!Y) Y = dY_;
+    const long items = (long)shards_ * shard_c_;
+    // every shard scans the gathered sequence (exclusive, seeded with the
+    // initial state) and keeps the prefixes of its own items
+    PARODE_CUDA(cudaMemcpyAsync(dTop_, dGathered, sizeof(double) * (size_t)items * Np_, cudaMemcpyDeviceToDevice, s));
+    launch_chunk_carry(Np_, dTop_, items, dPow_, shape_.R + 4 * shard_k_, dX0_, dTop_ + items * Np_, s);
+    ChunkLevels L = shard_levels_;
+    const double* mine = dTop_ + (long)shard_ * shard_c_ * Np_;
+    if (L.h == 0) {
+        PARODE_CUDA(cudaMemcpyAsync(dG_, mine, sizeof(double) * (size_t)L.cnt[0] * Np_, cudaMemcpyDeviceToDevice, s));
+    } else {
+        L.arr[L.h] = const_cast<double*>(mine);
+        launch_chunk_down(Np_, L, dPow_, shape_.R, s);
+    }
+    if (br_tc_) state_part(Y, s);
+    else launch_gemm_tiled(response_out_args(Y), s);
+    if (solver_ == kABM && shard_ == 0)
+        PARODE_CUDA(cudaMemcpyAsync(Y, dYpre_, sizeof(double) * 3 * p_, cudaMemcpyDeviceToDevice, s));
+    PARODE_CUDA(cudaEventRecord(done_, s));
+    last_y_ = Y;
+    shard_up_done_ = false;
 }
 
 void Plan::execute_blocked(double* Y, cudaStream_t s)
@@ -919,7 +1001,19 @@ void Plan::get_output(double* t, double* y)
     if (y)
         PARODE_CUDA(cudaMemcpyAsync(y, last_y_ ? last_y_ : dY_, sizeof(double) * nOut_ * p_, cudaMemcpyDeviceToHost,
                                     stream_));
-    if (t) time_vector(solver_, t0_, tEnd_, h_, t);
+    if (t && shards_ > 1) {
+        // the shard's slice of the horizon's time vector (its first ybase rows
+        // are the start-up rows' times, as on shard 0)
+        long ns = 0;
+        const long nt = parode::num_outputs(solver_, t0_, tEnd_, h_, &ns);
+        std::vector<double> tg((size_t)std::max(nt, 1L));
+        time_vector(solver_, t0_, tEnd_, h_, tg.data());
+        const long ybase = nt - ns;
+        for (long i = 0; i < ybase; ++i) t[i] = tg[(size_t)i];
+        for (long j = 0; j < nScan_; ++j) t[ybase + j] = tg[(size_t)(ybase + shard_begin_ + j)];
+    } else if (t) {
+        time_vector(solver_, t0_, tEnd_, h_, t);
+    }
     PARODE_CUDA(cudaStreamSynchronize(stream_));
     int status = 0;
     PARODE_CUDA(cudaMemcpy(&status, dStatus_, sizeof(int), cudaMemcpyDeviceToHost));

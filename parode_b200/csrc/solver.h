@@ -50,6 +50,9 @@ struct PlanOptions {
     // block-response leaf: log2 of the block length (0: the tuned value of
     // the system's class, else the cost model's / the shape's default)
     int force_log2_block = 0;
+    // time partition of the solve across devices (setup_shard): this plan is
+    // shard `shard` of `shards` (shards > 1)
+    int shard = 0, shards = 1;
 };
 
 class Plan {
@@ -85,6 +88,17 @@ public:
     void response_shape(long long info[4]) const;
     int precision_used() const { return precision_used_; }
 
+    // Time shard (PlanOptions::shards > 1; block-response path only).  The
+    // plan covers the scan steps [info[0], info[0] + info[1]) of the horizon;
+    // its outputs are num_outputs() rows whose first ybase (3 for ABM, else
+    // 0) are the start-up rows on shard 0 only, the rest the shard's steps.
+    // shard_up writes info[2] items of info[3] doubles (the shard's chunk
+    // aggregates) to dTop; once every shard's items are gathered in shard
+    // order (info[4] x info[2] items), shard_down finishes the solve into y.
+    void shard_info(long long info[5]) const;
+    void shard_up(double* dTop, cudaStream_t s);
+    void shard_down(const double* dGathered, double* y, cudaStream_t s);
+
     // Optional stage timing with CUDA events on the execution stream.
     void set_profiling(bool on);
     // Stage names and milliseconds of the last profiled execute (synchronises).
@@ -97,8 +111,11 @@ private:
     void execute_blocked(double* Y, cudaStream_t s);
     void execute_response(double* Y, cudaStream_t s);
     void execute_general(double* Y, cudaStream_t s);
-    int carry(cudaStream_t s, cudaEvent_t after_first = nullptr);
-    void side_span(int end);
+    int carry(cudaStream_t s);
+    LevelArgs response_agg_args() const;
+    LevelArgs response_out_args(double* Y) const;
+    void state_part(double* Y, cudaStream_t s);
+    void setup_shard(const PlanOptions& opt);
     void fill_inputs(cudaStream_t s);
 
     int device_ = 0;
@@ -141,8 +158,6 @@ private:
     long* dTcStart_ = nullptr;  // device: their first tiles
     long* dTcCta_ = nullptr;    // device: tile ranges of the persistent CTAs
     int tcCtas_ = 0;
-    int tcCtasW_ = 0;           // CTAs of the output-window launch beside the carry
-    bool tc_overlap_ = false;  // the windows run beside the carry (tcCtas_ then the aggregates' CTAs)
     int* dStatus_ = nullptr;
     bool one_pass_ = false;  // single-pass TF32 response GEMMs (hi*hi only)
     cudaStream_t side_ = nullptr;
@@ -153,8 +168,13 @@ private:
     bool profiling_ = false;
     std::vector<cudaEvent_t> events_;
     std::vector<std::string> marks_;
-    cudaEvent_t side_ev_[2] = {nullptr, nullptr};  // span of the side-stream window launch
-    bool side_marked_ = false;
+    // time shard (setup_shard)
+    int shard_ = 0, shards_ = 1, shard_k_ = 0, shard_c_ = 0;
+    long shard_begin_ = 0, nScanGlobal_ = 0;
+    long u_joff_ = 0;           // index of the first input sample on the whole horizon
+    double* dTop_ = nullptr;    // gathered top items + their scan's scratch
+    ChunkLevels shard_levels_;  // the up-sweep's levels, reused by the down-sweep
+    bool shard_up_done_ = false;
 };
 
 }  // namespace parode
