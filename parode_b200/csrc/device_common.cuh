@@ -128,6 +128,57 @@ __device__ __forceinline__ void sinusoid_run_terms(const double* a, const double
     }
 }
 
+// The plain rotation: each term from sincos at the run's first sample, then
+// rotated by sincos of the nominal step w dt, with no correction for the
+// rounding of the sample times.  Against the rounded arguments the phase
+// drifts by at most w ulp(t) plus ~64 roundings over a run (about 1e-13 of
+// the amplitude at the benchmark's times): for the TF32 sample planes, whose
+// own rounding is 2^-22, not for the FP64 samples.  5 FP64 operations per
+// term and sample instead of ~14.
+template <int L, int KT, class Out>
+__device__ __forceinline__ void sinusoid_rot_terms(const double* a, const double* f, const double* phi, int i,
+                                                   double base, double dt, long j0, int n, const Out& out, long joff)
+{
+    const double two_pi = 6.283185307179586476925286766559;
+    double amp[KT], s[KT], c[KT], sdl[KT], cdl[KT];
+    double v = 0.0;
+    const double t0 = sample_time(base, dt, joff + j0);
+#pragma unroll
+    for (int q = 0; q < KT; ++q) {
+        const double w = __dmul_rn(two_pi, f[i * KT + q]);
+        amp[q] = a[i * KT + q];
+        sincos(__dadd_rn(__dmul_rn(w, t0), phi[i * KT + q]), &s[q], &c[q]);
+        sincos(__dmul_rn(w, dt), &sdl[q], &cdl[q]);
+        v = fma(amp[q], s[q], v);
+    }
+    if (n > 0) out(0, v);
+    for (int j = 1; j < n; ++j) {
+        v = 0.0;
+#pragma unroll
+        for (int q = 0; q < KT; ++q) {
+            const double sn = fma(s[q], cdl[q], c[q] * sdl[q]);
+            c[q] = fma(c[q], cdl[q], -(s[q] * sdl[q]));
+            s[q] = sn;
+            v = fma(amp[q], s[q], v);
+        }
+        out(j, v);
+    }
+}
+
+template <int L, int KMAX, class Out>
+__device__ __forceinline__ void sinusoid_rot(const double* a, const double* f, const double* phi, int K, int i,
+                                             double base, double dt, long j0, long count, const Out& out, long joff)
+{
+    const long rest = count - j0;
+    const int n = rest < L ? (int)rest : L;
+    if (K == 1) sinusoid_rot_terms<L, 1>(a, f, phi, i, base, dt, j0, n, out, joff);
+    else if (KMAX >= 2 && K == 2) sinusoid_rot_terms<L, (KMAX >= 2 ? 2 : 1)>(a, f, phi, i, base, dt, j0, n, out, joff);
+    else if (KMAX >= 3 && K == 3) sinusoid_rot_terms<L, (KMAX >= 3 ? 3 : 1)>(a, f, phi, i, base, dt, j0, n, out, joff);
+    else if (KMAX >= 4 && K == 4) sinusoid_rot_terms<L, (KMAX >= 4 ? 4 : 1)>(a, f, phi, i, base, dt, j0, n, out, joff);
+    else
+        for (int j = 0; j < n; ++j) out(j, sinusoid_value(a, f, phi, K, i, sample_time(base, dt, joff + j0 + j)));
+}
+
 // KMAX (1..4): the largest term count given its own chains; a kernel's
 // registers follow the largest variant it contains.  Sample j of the run is
 // written at out(j) and taken at the time of sample joff + j0 + j (joff: the

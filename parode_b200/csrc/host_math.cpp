@@ -9,7 +9,13 @@ namespace parode {
 
 namespace {
 
-// Z (r x c) = X (r x k) * Y (k x c), row-major.
+// Z (r x c) = X (r x k) * Y (k x c), row-major.  The inner loop runs over
+// contiguous columns, so it vectorises; each element still accumulates in
+// the order q = 0, 1, ..., so every clone gives the same bits (no FMA
+// contraction: this file is built with -ffp-contract=off).
+#if defined(__GNUC__) && !defined(__clang__) && defined(__x86_64__) && !defined(__CUDACC__)
+__attribute__((target_clones("avx2", "default")))
+#endif
 void gemm(int r, int k, int c, const double* X, const double* Y, double* Z)
 {
     for (int i = 0; i < r; ++i) {

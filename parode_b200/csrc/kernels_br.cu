@@ -28,7 +28,7 @@ namespace parode {
 
 namespace {
 
-constexpr int kCols = 32;       // window columns per CTA
+constexpr int kCols = 8;        // window columns per CTA (a cfg2 W: 41 CTAs)
 constexpr int kThreads = 256;
 
 // z (NP x kCols, row-major in shared memory): z <- Phi z + S_j, and the
@@ -64,7 +64,12 @@ __global__ void __launch_bounds__(kThreads) k_block_response(const ResponseArgs*
             if (col >= ld) continue;
             double v = 0.0;
             if (col < a.K || col >= a.Kpad) {
-                for (int r = 0; r < NP; ++r) v = fma(sC[o * NP + r], z[r * kCols + c], v);
+                // four independent partial sums (NP is a multiple of 8)
+                double v4[4] = {0.0, 0.0, 0.0, 0.0};
+                for (int r = 0; r < NP; r += 4)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) v4[q] = fma(sC[o * NP + r + q], z[(r + q) * kCols + c], v4[q]);
+                v = (v4[0] + v4[1]) + (v4[2] + v4[3]);
                 if (col < a.K && !a.zeroD && m > 0 && col / m == su) v += a.D[(long)o * m + col % m];
             }
             a.Wm[(long)(j * p + o) * ld + col] = v;
@@ -72,8 +77,11 @@ __global__ void __launch_bounds__(kThreads) k_block_response(const ResponseArgs*
         // z_{j+1} = Phi z_j + S_j, S_j = the forcing of step j on the window
         for (int e = threadIdx.x; e < NP * kCols; e += kThreads) {
             const int r = e / kCols, c = e - r * kCols, col = c0 + c;
-            double v = 0.0;
-            for (int k = 0; k < NP; ++k) v = fma(sPhi[r * NP + k], z[k * kCols + c], v);
+            double v4[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int k = 0; k < NP; k += 4)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) v4[q] = fma(sPhi[r * NP + k + q], z[(k + q) * kCols + c], v4[q]);
+            double v = (v4[0] + v4[1]) + (v4[2] + v4[3]);
             if (!a.zeroB && m > 0 && col < a.K && r >= coff && r < coff + n) {
                 const int s = col / m, i = col - s * m;
                 const int w = rk4 ? s - 2 * j : s - j;  // window slot of sample s at step j

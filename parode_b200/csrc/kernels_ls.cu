@@ -352,7 +352,8 @@ __global__ void k_sinusoid_samples(double* U, int m, int K, const double* a, con
     sinusoid_run<kSampleRun, KMAX>(a, f, phi, K, i, base, dt, j0, count, SampleOut64{U + j0 * m + i, m}, joff);
 }
 
-// The same samples as TF32 hi / lo planes (the tensor-core GEMMs' operands).
+// The same samples as TF32 hi / lo planes (the tensor-core GEMMs' operands),
+// by the plain rotation (sinusoid_rot: the planes' own rounding is 2^-22).
 template <int KMAX>
 __global__ void k_sinusoid_planes(float* hi, float* lo, int m, int K, const double* a, const double* f,
                                   const double* phi, double base, double dt, long count, long joff)
@@ -363,7 +364,7 @@ __global__ void k_sinusoid_planes(float* hi, float* lo, int m, int K, const doub
     const long r = e / m;
     const int i = (int)(e - r * m);
     const long j0 = r * kSampleRun;
-    sinusoid_run<kSampleRun, KMAX>(a, f, phi, K, i, base, dt, j0, count,
+    sinusoid_rot<kSampleRun, KMAX>(a, f, phi, K, i, base, dt, j0, count,
                                    SampleOutSplit{hi + j0 * m + i, lo ? lo + j0 * m + i : nullptr, m}, joff);
 }
 
