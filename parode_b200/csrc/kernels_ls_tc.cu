@@ -255,6 +255,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
         Cursor c;
         c.init(args, start, nent, t0, t1);
         long j = 0;  // slice counter
+        int pst = 0;  // its ring stage and the parity of that stage's use
+        uint32_t pph = 0;
         for (long t = t0; t < t1 && !*abort; ++t) {
             const long lt = c.seek(t);
             const LevelArgs& a = c.a;
@@ -273,9 +275,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
                 }
             }
             for (int s = 0; s < nk && !*abort; ++s, ++j) {
-                const int st = (int)(j % kS);
-                const long use = j / kS;
-                if (use >= 1 && !role_wait(&empty[st], (uint32_t)((use - 1) & 1), abort, status)) break;
+                // ring position as counters (no per-slice division by kS)
+                if (j >= kS && !role_wait(&empty[pst], pph ^ 1u, abort, status)) break;
+                const int st = pst;
                 unsigned char* stg = sm + st * kStage;
                 // A: one 16 KB bulk copy; B: one 2D tensor load of 64 vectors x
                 // 16 K (FP64; x = 16 s, a multiple of 16 bytes; the tails beyond
@@ -297,6 +299,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
                     tma_load_2d(stg + kOffRaw, a.src_map, sr * kBK, (int)n0, &full[st]);
                 }
                 __syncwarp();
+                if (++pst == kS) {
+                    pst = 0;
+                    pph ^= 1u;
+                }
             }
         }
     } else if (warp == 1) {
@@ -304,7 +310,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
         if (lane == 0) {
             Cursor c;
             c.init(args, start, nent, t0, t1);
-            long j = 0, u = 0, tt = 0;  // slice, drain-unit and tile counters
+            long u = 0, tt = 0;  // drain-unit and tile counters
+            int mst = 0;         // ring stage of the next slice and its fill parity
+            uint32_t mph = 0;
             constexpr uint32_t SBO = kBK * 32;
             constexpr uint32_t idesc = make_idesc(kBM, kBN);
             bool ok = true;
@@ -322,7 +330,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
                     ok = false;
                     break;
                 }
-                for (int s = 0; s < nk; ++s, ++j) {
+                for (int s = 0; s < nk; ++s) {
                     if (s % kDrain == 0) {
                         // a new drain unit: wait until the epilogue has read this accumulator
                         ab = (int)(u % kAcc);
@@ -334,10 +342,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
                         fence_after_sync();
                         d = tbase + (uint32_t)(ab * kBN);
                     }
-                    const int st = (int)(j % kS);
+                    const int st = mst;
                     // A landed (bulk copy) and B converted
-                    if (!role_wait(&full[st], (uint32_t)((j / kS) & 1), abort, status) ||
-                        !role_wait(&conv[st], (uint32_t)((j / kS) & 1), abort, status)) {
+                    if (!role_wait(&full[st], mph, abort, status) || !role_wait(&conv[st], mph, abort, status)) {
                         ok = false;
                         break;
                     }
@@ -359,6 +366,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
                             mma_tf32(q == 0 ? d : dc, A[q] + (uint64_t)(k * 16), B[q] + (uint64_t)(k * 16), idesc,
                                      ((q == 0 && s % kDrain == 0) || (q == 1 && s == 0)) && k == 0 ? 0u : 1u);
                     mma_commit(&empty[st]);
+                    if (++mst == kS) {
+                        mst = 0;
+                        mph ^= 1u;
+                    }
                     if (s % kDrain == kDrain - 1 || s == nk - 1) {
                         mma_commit(&acc_full[ab]);
                         ++u;
@@ -372,7 +383,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
         const int ct = threadIdx.x - 64;
         Cursor c;
         c.init(args, start, nent, t0, t1);
-        long j = 0;
+        int cst = 0;  // ring stage of the next slice and its fill parity
+        uint32_t cph = 0;
         for (long t = t0; t < t1 && !*abort; ++t) {
             const long lt = c.seek(t);
             const LevelArgs& a = c.a;
@@ -380,9 +392,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
             long n0;
             tile_coords(a, lt, mi, m0, n0, nk);
             bool ok = true;
-            for (int s = 0; s < nk; ++s, ++j) {
-                const int st = (int)(j % kS);
-                if (!role_wait(&full[st], (uint32_t)((j / kS) & 1), abort, status)) {
+            for (int s = 0; s < nk; ++s) {
+                const int st = cst;
+                if (!role_wait(&full[st], cph, abort, status)) {
                     ok = false;
                     break;
                 }
@@ -412,6 +424,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_level_tc(const LevelArgs* __res
                 fence_async_smem();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&conv[st]);
+                if (++cst == kS) {
+                    cst = 0;
+                    cph ^= 1u;
+                }
             }
             if (!ok) break;
         }

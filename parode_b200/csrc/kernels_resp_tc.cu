@@ -203,7 +203,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_resp_tc(const RespArgs* __restr
         // ---------------- producer ----------------
         Cursor c;
         c.init(args, start, nent, t0, t1);
-        long j = 0;
+        // ring position of the next slice: stage st in its use of parity ph
+        // (kept as counters: a division by the six stages per slice cost the
+        // single issuing threads more than the tensor work of a slice)
+        int st = 0;
+        uint32_t ph = 0;
+        long slices = 0;
         for (long t = t0; t < t1 && !*abort; ++t) {
             const long lt = c.seek(t);
             const RespArgs& a = c.a();
@@ -212,13 +217,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_resp_tc(const RespArgs* __restr
             tile_coords(a, lt, mi, m0, n0, nk);
             const int rowsv = a.rows - m0 < kBM ? a.rows - m0 : kBM;
             const uint32_t abytes = (uint32_t)((rowsv + 7) / 8) * (uint32_t)(kBK * 32);
-            for (int s = 0; s < nk && !*abort; ++s, ++j) {
-                const int st = (int)(j % kS);
-                const long use = j / kS;
-                if (use >= 1 && !role_wait(&empty[st], (uint32_t)((use - 1) & 1), abort, status)) break;
+            for (int s = 0; s < nk && !*abort; ++s) {
+                if (slices >= kS && !role_wait(&empty[st], ph ^ 1u, abort, status)) break;
                 unsigned char* stg = sm + st * kStage;
                 // test hook: CTA 0 issues nothing for its first slice
-                const bool withhold = a.fault_withhold && blockIdx.x == 0 && j == 0;
+                const bool withhold = a.fault_withhold && blockIdx.x == 0 && slices == 0;
                 if (lane == 0 && !withhold) {
                     const int sr = s;
                     const unsigned char* ab =
@@ -233,6 +236,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_resp_tc(const RespArgs* __restr
                     }
                 }
                 __syncwarp();
+                ++slices;
+                if (++st == kS) {
+                    st = 0;
+                    ph ^= 1u;
+                }
             }
         }
     } else if (warp == 1) {
@@ -240,7 +248,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_resp_tc(const RespArgs* __restr
         if (lane == 0) {
             Cursor c;
             c.init(args, start, nent, t0, t1);
-            long j = 0, u = 0, tt = 0;
+            long u = 0, tt = 0;
+            int st = 0;  // ring stage of the next slice and the parity of its fill
+            uint32_t ph = 0;
             constexpr uint32_t SBO = kBK * 32;
             constexpr uint32_t idesc = make_idesc(kBM, kBN);
             bool ok = true;
@@ -257,7 +267,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_resp_tc(const RespArgs* __restr
                     ok = false;
                     break;
                 }
-                for (int s = 0; s < nk; ++s, ++j) {
+                for (int s = 0; s < nk; ++s) {
                     if (s % kDrain == 0) {
                         ab = (int)(u % kAcc);
                         const long ause = u / kAcc;
@@ -268,8 +278,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_resp_tc(const RespArgs* __restr
                         fence_after_sync();
                         d = tbase + (uint32_t)(ab * kBN);
                     }
-                    const int st = (int)(j % kS);
-                    if (!role_wait(&full[st], (uint32_t)((j / kS) & 1), abort, status)) {
+                    if (!role_wait(&full[st], ph, abort, status)) {
                         ok = false;
                         break;
                     }
@@ -287,6 +296,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_resp_tc(const RespArgs* __restr
                             mma_tf32(q == 0 ? d : dc, A[q] + (uint64_t)(k * 16), B[q] + (uint64_t)(k * 2), idesc,
                                      ((q == 0 && s % kDrain == 0) || (q == 1 && s == 0)) && k == 0 ? 0u : 1u);
                     mma_commit(&empty[st]);
+                    if (++st == kS) {
+                        st = 0;
+                        ph ^= 1u;
+                    }
                     if (s % kDrain == kDrain - 1 || s == nk - 1) {
                         mma_commit(&acc_full[ab]);
                         ++u;
