@@ -497,6 +497,7 @@ void ParODE_SimulateODE_d(const double* A, const double* B, const double* C, con
         opt.path = L.path;
         opt.input_double = true;
         opt.fault_withhold = L.fault_withhold;
+        opt.log = L.log != 0;
         Plan plan(dev, s, &L.inputs, uIndex, solver, tStart, tEnd, tStep, opt);
         // the host time vector is built on a helper thread while the plan
         // is set up, solved and its outputs copied
@@ -534,6 +535,7 @@ ParODE_Plan* ParODE_PlanCreate(const double* A, const double* B, const double* C
         opt.input_double = true;
         opt.executions = (double)L.executions;
         opt.fault_withhold = L.fault_withhold;
+        opt.log = L.log != 0;
         auto h = std::make_unique<ParODE_Plan>();
         h->plan = std::make_unique<Plan>(dev, s, &L.inputs, uIndex, solver, tStart, tEnd, tStep, opt);
         out = h.release();

@@ -8,9 +8,82 @@
 #include "tuner.h"
 
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
 #include <cstring>
+#include <mutex>
+#include <string>
 
 namespace parode {
+
+namespace {
+
+// Streams and events of finished plans, kept per device for the next plan
+// (creating two streams and five events cost ~0.1 ms of every one-shot
+// SimulateODE call).  Returned idle: the plan synchronises them first.
+struct HandlePool {
+    std::mutex mu;
+    std::vector<std::pair<int, cudaStream_t>> streams;
+    std::vector<std::pair<int, cudaEvent_t>> events;
+};
+
+HandlePool& handles()
+{
+    static HandlePool* p = new HandlePool();
+    return *p;
+}
+
+cudaStream_t take_stream(int dev)
+{
+    {
+        HandlePool& h = handles();
+        std::lock_guard<std::mutex> g(h.mu);
+        for (size_t k = 0; k < h.streams.size(); ++k)
+            if (h.streams[k].first == dev) {
+                cudaStream_t s = h.streams[k].second;
+                h.streams[k] = h.streams.back();
+                h.streams.pop_back();
+                return s;
+            }
+    }
+    cudaStream_t s = nullptr;
+    PARODE_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    return s;
+}
+
+cudaEvent_t take_event(int dev)
+{
+    {
+        HandlePool& h = handles();
+        std::lock_guard<std::mutex> g(h.mu);
+        for (size_t k = 0; k < h.events.size(); ++k)
+            if (h.events[k].first == dev) {
+                cudaEvent_t e = h.events[k].second;
+                h.events[k] = h.events.back();
+                h.events.pop_back();
+                return e;
+            }
+    }
+    cudaEvent_t e = nullptr;
+    PARODE_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    return e;
+}
+
+void give_stream(int dev, cudaStream_t s)
+{
+    HandlePool& h = handles();
+    std::lock_guard<std::mutex> g(h.mu);
+    h.streams.emplace_back(dev, s);
+}
+
+void give_event(int dev, cudaEvent_t e)
+{
+    HandlePool& h = handles();
+    std::lock_guard<std::mutex> g(h.mu);
+    h.events.emplace_back(dev, e);
+}
+
+}  // namespace
 
 Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex, int solver, double t0,
            double tEnd, double h, const PlanOptions& opt)
@@ -166,13 +239,27 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
     }
     if (opt.shards > 1 || opt.shard != 0) setup_shard(opt);
     PARODE_CUDA(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_));
+    // set-up phase times on stderr with PARODE_OPT_LOG (device phases then
+    // wait for the device)
+    auto clock0 = std::chrono::steady_clock::now();
+    std::string phases;
+    auto phase = [&](const char* name, bool device) {
+        if (!opt.log) return;
+        if (device && stream_) PARODE_CUDA(cudaStreamSynchronize(stream_));
+        const auto now = std::chrono::steady_clock::now();
+        char b[64];
+        std::snprintf(b, sizeof b, " %s %.3f ms", name, std::chrono::duration<double, std::milli>(now - clock0).count());
+        phases += b;
+        clock0 = now;
+    };
 
     PARODE_CUDA(cudaSetDevice(device_));
-    PARODE_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
-    PARODE_CUDA(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
-    for (auto& e : fork_) PARODE_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    PARODE_CUDA(cudaEventCreateWithFlags(&done_, cudaEventDisableTiming));
+    stream_ = take_stream(device_);
+    side_ = take_stream(device_);
+    for (auto& e : fork_) e = take_event(device_);
+    done_ = take_event(device_);
 
+    phase("streams", false);
     // ---- host FP64 discretisation --------------------------------------
     const int n = sys.n, mB = sys.zeroB ? 0 : sys.m;
     const int W = solver == kRK4 ? 3 : 5;
@@ -185,6 +272,7 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
     for (int r = 0; r < Ns_; ++r)
         std::memcpy(&PhiP[(size_t)r * Np_], &Phi[(size_t)r * Ns_], sizeof(double) * Ns_);
 
+    phase("discretise", false);
     // ---- device buffers ---------------------------------------------------
     long npow = std::max(levels_, 1);
     alloc(&dPow_, npow * (long)Np_ * Np_);
@@ -253,21 +341,24 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
         const bool planes = br_tc_;
         if (!planes || input_->kind != InputEntry::kSinusoid) {
             alloc(&dU_, nU_ * (long)mu_ + pad);
-            if (pad) PARODE_CUDA(cudaMemsetAsync(dU_, 0, sizeof(double) * (size_t)(nU_ * mu_ + pad), stream_));
+            // every execute writes all nU x mu samples: only the padding is zeroed
+            if (pad) PARODE_CUDA(cudaMemsetAsync(dU_ + nU_ * mu_, 0, sizeof(double) * (size_t)pad, stream_));
         }
         if (planes) {
             const long nf = nU_ * (long)mu_ + pad + 16;
             double* d = nullptr;
             alloc(&d, (nf + 1) / 2);
             dUh_ = reinterpret_cast<float*>(d);
-            PARODE_CUDA(cudaMemsetAsync(dUh_, 0, sizeof(float) * (size_t)nf, stream_));
+            const size_t used = (size_t)nU_ * mu_;  // rewritten by every execute
+            PARODE_CUDA(cudaMemsetAsync(dUh_ + used, 0, sizeof(float) * ((size_t)nf - used), stream_));
             if (!one_pass_) {  // the single-pass form reads no lo plane
                 alloc(&d, (nf + 1) / 2);
                 dUl_ = reinterpret_cast<float*>(d);
-                PARODE_CUDA(cudaMemsetAsync(dUl_, 0, sizeof(float) * (size_t)nf, stream_));
+                PARODE_CUDA(cudaMemsetAsync(dUl_ + used, 0, sizeof(float) * ((size_t)nf - used), stream_));
             }
         }
     }
+    phase("buffers", true);
     PARODE_CUDA(cudaMemcpyAsync(dPow_, PhiP.data(), sizeof(double) * PhiP.size(), cudaMemcpyHostToDevice, stream_));
     PARODE_CUDA(cudaMemcpyAsync(dBbar_, Bbar.data(), sizeof(double) * Bbar.size(), cudaMemcpyHostToDevice, stream_));
     if (!sys.zeroC)
@@ -319,6 +410,7 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
                                     stream_));
     }
     PARODE_CUDA(cudaMemcpyAsync(dX0_, X0.data(), sizeof(double) * Np_, cudaMemcpyHostToDevice, stream_));
+    phase("copies+start-up", true);
     if (br_) {
         // block response matrix from Phi (power-table level 0), Bbar, Cext, D
         alloc(&dW_, (long)(shape_.B * p_ + Np_) * (brKpad_ + Np_));
@@ -343,9 +435,11 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
         alloc(&dra, (long)((sizeof(ResponseArgs) + 7) / 8));
         PARODE_CUDA(cudaMemcpyAsync(dra, &ra, sizeof(ra), cudaMemcpyHostToDevice, stream_));
         launch_block_response(reinterpret_cast<const ResponseArgs*>(dra), 1, Np_, p_, brKpad_, stream_);
+        phase("W", true);
         // the carry's powers P_1 .. P_levels (Phi^(2^l)) depend on Phi alone:
         // formed once here, like W
         launch_blocked_tables(shape_, dPow_, 1, levels_, nullptr, nullptr, p_, stream_);
+        phase("tables", true);
         if (br_tc_) {
             // the two tensor-core GEMMs over the sample windows: aggregates
             // into G, output windows into the plan's y buffer (the FP64 state
@@ -412,9 +506,12 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
             PARODE_CUDA(cudaMemcpyAsync(dTcCta_, ranges.data(), sizeof(long) * ranges.size(), cudaMemcpyHostToDevice,
                                         stream_));
             launch_level_split(dTc_, 2, (long)std::max(sa, sw) / 8, stream_);
+            phase("tensor-core set-up", true);
         }
     }
     PARODE_CUDA(cudaStreamSynchronize(stream_));
+    phase("sync", false);
+    if (opt.log) std::fprintf(stderr, "ParODE plan set-up (n=%d T=%ld path=%d):%s\n", sys.n, nScan_, path(), phases.c_str());
     // keep a plan's worth of freed memory in the pool, so that the next plan
     // of this size (the next SimulateODE call) maps nothing new
     {
@@ -443,26 +540,25 @@ Plan::~Plan()
     // the buffers return to the device's stream-ordered pool once the last
     // execute (on whatever stream) and the plan's own work are done
     if (stream_ && done_) cudaStreamWaitEvent(stream_, done_, 0);
-    if (stream_ && side_) {
-        cudaEvent_t e = nullptr;
-        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess) {
-            cudaEventRecord(e, side_);
-            cudaStreamWaitEvent(stream_, e, 0);
-            cudaEventDestroy(e);
-        }
+    if (stream_ && side_ && fork_[0]) {
+        cudaEventRecord(fork_[0], side_);
+        cudaStreamWaitEvent(stream_, fork_[0], 0);
     }
     for (double* p : bufs_) {
         if (stream_) cudaFreeAsync(p, stream_);
         else cudaFree(p);
     }
-    if (stream_) cudaStreamSynchronize(stream_);
-    if (side_) cudaStreamSynchronize(side_);
+    const bool ok_s = !stream_ || cudaStreamSynchronize(stream_) == cudaSuccess;
+    const bool ok_d = !side_ || cudaStreamSynchronize(side_) == cudaSuccess;
     for (cudaEvent_t e : events_) cudaEventDestroy(e);
+    // idle streams and events go back to the pool for the next plan (handles
+    // of a failed context are destroyed instead)
+    const bool reuse = ok_s && ok_d;
     for (cudaEvent_t e : fork_)
-        if (e) cudaEventDestroy(e);
-    if (done_) cudaEventDestroy(done_);
-    if (side_) cudaStreamDestroy(side_);
-    if (stream_) cudaStreamDestroy(stream_);
+        if (e) reuse ? give_event(device_, e) : (void)cudaEventDestroy(e);
+    if (done_) reuse ? give_event(device_, done_) : (void)cudaEventDestroy(done_);
+    if (side_) reuse ? give_stream(device_, side_) : (void)cudaStreamDestroy(side_);
+    if (stream_) reuse ? give_stream(device_, stream_) : (void)cudaStreamDestroy(stream_);
 }
 
 void Plan::alloc(double** p, long n)
