@@ -74,14 +74,12 @@ __device__ __forceinline__ void load_g(const double* __restrict__ items, long co
 
 // acc += Q X on the tile (X in shared memory, row pitch kLd).  The K
 // products go to kSplit independent partial sums, so the dependent MMA chain
-// (the step's latency) is NP / 4 / kSplit long.  A dependent DMMA costs about
-// 200 cycles here: launches of few CTAs (latency-bound) take KS = 16 chains,
-// the wide level-0 launches (throughput-bound) 4.
-template <int NP, int KS>
+// (the step's latency) is NP / 4 / kSplit long.
+template <int NP>
 __device__ __forceinline__ void step_mma(const double* X, const double (&qa)[NP / 4], double (&acc)[kNT][2],
                                          const Roles<NP>& r)
 {
-    constexpr int kSplit = NP / 4 < KS ? NP / 4 : KS;
+    constexpr int kSplit = NP / 4 < 4 ? NP / 4 : 4;
     double part[kSplit][kNT][2];
 #pragma unroll
     for (int q = 0; q < kSplit; ++q)
@@ -98,12 +96,10 @@ __device__ __forceinline__ void step_mma(const double* X, const double (&qa)[NP 
     for (int u = 0; u < kNT; ++u)
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
-            // pairwise sum of the partials (a tree, not a chain)
+            double v = acc[u][e];
 #pragma unroll
-            for (int w = 1; w < kSplit; w *= 2)
-#pragma unroll
-                for (int q = 0; q + w < kSplit; q += 2 * w) part[q][u][e] += part[q + w][u][e];
-            acc[u][e] += part[0][u][e];
+            for (int q = 0; q < kSplit; ++q) v += part[q][u][e];
+            acc[u][e] = v;
         }
 }
 
@@ -138,7 +134,7 @@ __device__ __forceinline__ void store_tile(double* X, const double (&acc)[kNT][2
 // next[c] = sum_{j<16} Q^(15-j) items[16 c + j] (items past count are zero;
 // the last chunk's aggregate is never read by the scan).  Xs: 2 NP x kLd
 // doubles of shared memory.  Every thread of the CTA takes part.
-template <int NP, int KS>
+template <int NP>
 __device__ __forceinline__ void chunk_up_tile(const double* __restrict__ items, long count,
                                               const double* __restrict__ Q, double* __restrict__ next, long tile,
                                               double* Xs0, double* Xs1)
@@ -160,7 +156,7 @@ __device__ __forceinline__ void chunk_up_tile(const double* __restrict__ items, 
 #pragma unroll
             for (int u = 0; u < kNT; ++u) acc[u][0] = pre[u][0], acc[u][1] = pre[u][1];
             if (j + 1 < kChunk) load_g<NP>(items, count, c0, kChunk, j + 1, r, pre);
-            step_mma<NP, KS>(Xs[cur], qa, acc, r);
+            step_mma<NP>(Xs[cur], qa, acc, r);
             store_tile<NP>(Xs[cur ^ 1], acc, r);
         }
         __syncthreads();
@@ -173,12 +169,12 @@ __device__ __forceinline__ void chunk_up_tile(const double* __restrict__ items, 
     __syncthreads();  // Xs is reused by the CTA's next tile
 }
 
-template <int NP, int KS>
+template <int NP>
 __global__ void __launch_bounds__(kThreads) k_chunk_up(const double* __restrict__ items, long count,
                                                         const double* __restrict__ Q, double* __restrict__ next)
 {
     __shared__ double Xs[2][NP * kLd];
-    chunk_up_tile<NP, KS>(items, count, Q, next, blockIdx.x, Xs[0], Xs[1]);
+    chunk_up_tile<NP>(items, count, Q, next, blockIdx.x, Xs[0], Xs[1]);
 }
 
 // Chunk rewrite of one tile: from the chunk's carried-in state
@@ -186,7 +182,7 @@ __global__ void __launch_bounds__(kThreads) k_chunk_up(const double* __restrict_
 // then Q x + item, ...).  Each lane reads item j + 1 (its D-fragment
 // positions) before it writes the state into the same positions, so slots
 // need no barrier.
-template <int NP, int KS>
+template <int NP>
 __device__ __forceinline__ void chunk_down_tile(double* __restrict__ items, long count,
                                                 const double* __restrict__ Q, const double* __restrict__ carries,
                                                 int F, long tile, double* Xs0, double* Xs1)
@@ -221,7 +217,7 @@ __device__ __forceinline__ void chunk_down_tile(double* __restrict__ items, long
 #pragma unroll
             for (int u = 0; u < kNT; ++u) acc[u][0] = pre[u][0], acc[u][1] = pre[u][1];
             load_g<NP>(items, count, c0, F, j + 1, r, pre);
-            step_mma<NP, KS>(Xs[cur], qa, acc, r);
+            step_mma<NP>(Xs[cur], qa, acc, r);
             store_tile<NP>(Xs[cur ^ 1], acc, r);
             store_g<NP>(items, count, c0, F, j + 1, r, acc);
         }
@@ -231,17 +227,14 @@ __device__ __forceinline__ void chunk_down_tile(double* __restrict__ items, long
     __syncthreads();  // Xs is reused by the CTA's next tile
 }
 
-template <int NP, int KS>
+template <int NP>
 __global__ void __launch_bounds__(kThreads) k_chunk_down(double* __restrict__ items, long count,
                                                           const double* __restrict__ Q,
                                                           const double* __restrict__ carries, int F)
 {
     __shared__ double Xs[2][NP * kLd];
-    chunk_down_tile<NP, KS>(items, count, Q, carries, F, blockIdx.x, Xs[0], Xs[1]);
+    chunk_down_tile<NP>(items, count, Q, carries, F, blockIdx.x, Xs[0], Xs[1]);
 }
-
-// launches of at most this many CTAs are latency-bound: more DMMA chains
-constexpr unsigned kFewCtas = 64;
 
 // ---------------------------------------------------------------------------
 template <int NP>
@@ -258,10 +251,7 @@ int chunk_up_t(double* items, long count, const double* P, int l0, double* work,
         if (h + 1 >= 16) throw Error(kInvalidArgument, "chunk carry: too many levels");
         const long nc = (L->cnt[h] + kChunk - 1) / kChunk;
         const unsigned grid = (unsigned)((nc + kCols - 1) / kCols);
-        if (grid <= kFewCtas)
-            k_chunk_up<NP, 16><<<grid, kThreads, 0, s>>>(L->arr[h], L->cnt[h], P + (long)(l0 + 4 * h) * mat, w);
-        else
-            k_chunk_up<NP, 4><<<grid, kThreads, 0, s>>>(L->arr[h], L->cnt[h], P + (long)(l0 + 4 * h) * mat, w);
+        k_chunk_up<NP><<<grid, kThreads, 0, s>>>(L->arr[h], L->cnt[h], P + (long)(l0 + 4 * h) * mat, w);
         PARODE_CUDA(cudaGetLastError());
         ++launches;
         L->arr[h + 1] = w;
@@ -280,12 +270,8 @@ int chunk_down_t(const ChunkLevels& L, const double* P, int l0, cudaStream_t s)
     for (int k = L.h - 1; k >= 0; --k) {
         const long nc = (L.cnt[k] + kChunk - 1) / kChunk;
         const unsigned grid = (unsigned)((nc + kCols - 1) / kCols);
-        if (grid <= kFewCtas)
-            k_chunk_down<NP, 16><<<grid, kThreads, 0, s>>>(L.arr[k], L.cnt[k], P + (long)(l0 + 4 * k) * mat,
-                                                           L.arr[k + 1], kChunk);
-        else
-            k_chunk_down<NP, 4><<<grid, kThreads, 0, s>>>(L.arr[k], L.cnt[k], P + (long)(l0 + 4 * k) * mat,
-                                                          L.arr[k + 1], kChunk);
+        k_chunk_down<NP><<<grid, kThreads, 0, s>>>(L.arr[k], L.cnt[k], P + (long)(l0 + 4 * k) * mat, L.arr[k + 1],
+                                                   kChunk);
         PARODE_CUDA(cudaGetLastError());
     }
     return L.h;
@@ -295,7 +281,7 @@ template <int NP>
 int chunk_top_t(double* items, long count, const double* Q, const double* X0, cudaStream_t s)
 {
     // one chunk of at most 16 items, entered with X0
-    k_chunk_down<NP, 16><<<1, kThreads, 0, s>>>(items, count, Q, X0, (int)count);
+    k_chunk_down<NP><<<1, kThreads, 0, s>>>(items, count, Q, X0, (int)count);
     PARODE_CUDA(cudaGetLastError());
     return 1;
 }
