@@ -1180,7 +1180,9 @@ void BatchPlan::build_responses()
 BatchPlan::~BatchPlan()
 {
     cudaSetDevice(device_);
+    if (last_stream_ && last_stream_ != stream_) cudaStreamSynchronize(last_stream_);
     if (stream_) cudaStreamSynchronize(stream_);
+    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
     for (auto f : forks_)
         if (f) {
             cudaStreamSynchronize(f);
@@ -1206,6 +1208,50 @@ void BatchPlan::execute(cudaStream_t s)
     if (!s) s = stream_;
     if (s != stream_) PARODE_CUDA(cudaStreamWaitEvent(s, ready_, 0));
     last_stream_ = s;
+    // a batch executed again replays its launch list as one CUDA graph
+    // (captured at the second execute): one host launch per execute
+    if (graph_state_ == 1) graph_state_ = capture_graph() ? 2 : -1;
+    if (graph_state_ == 2) {
+        PARODE_CUDA(cudaGraphLaunch(graph_exec_, s));
+        return;
+    }
+    enqueue(s);
+    if (graph_state_ == 0) graph_state_ = 1;
+}
+
+bool BatchPlan::capture_graph()
+{
+    // on the batch's own stream (never the legacy stream); a failure of any
+    // step leaves the batch executing launch by launch
+    if (cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    bool ok = true;
+    try {
+        enqueue(stream_);
+    } catch (...) {
+        ok = false;
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(stream_, &g);
+    if (!ok || e != cudaSuccess || !g) {
+        cudaGetLastError();
+        if (g) cudaGraphDestroy(g);
+        return false;
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&graph_exec_, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) {
+        cudaGetLastError();
+        graph_exec_ = nullptr;
+        return false;
+    }
+    return true;
+}
+
+void BatchPlan::enqueue(cudaStream_t s)
+{
     int launches = 0;
     // inputs for everything first
     if (nSampleJobs_ > 0) {

@@ -136,6 +136,12 @@ private:
     int sms_ = 148;
     int* dStatus_ = nullptr;  // set by a device wait that gave up
     cudaStream_t last_stream_ = nullptr;
+    // the launch list as a CUDA graph (execute): 0 no execute yet, 1 one eager
+    // execute, 2 graph instantiated, -1 capture failed (eager from then on)
+    int graph_state_ = 0;
+    cudaGraphExec_t graph_exec_ = nullptr;
+    void enqueue(cudaStream_t s);
+    bool capture_graph();
     cudaStream_t stream_ = nullptr;
     std::vector<cudaStream_t> forks_;
     std::vector<cudaEvent_t> events_;

@@ -7,12 +7,12 @@
 // the steps of a block, with the states those steps reach from X[b].
 //
 // FP64 on the DMMA tensor cores.  Ws is small (M x NP) and stays in shared
-// memory for the CTA's whole run.  Each warp works alone on tiles of 8
+// memory for the CTA's whole run.  Each warp works alone on tiles of 16
 // blocks: their states as DMMA B fragments in registers (read once from X),
-// then for every 8-row slice of W (m8n8k4, K = NP, as four independent partial
-// sums: a dependent DMMA costs ~200 cycles) the slice's window part is loaded
-// ahead of the product and y written straight to global memory (8 rows of a
-// block are 64 consecutive bytes).  No block-wide barrier after the staging
+// then for every 8-row slice of W (m8n8k4, K = NP; each A fragment feeds the
+// two 8-block halves) the slice's window part is loaded ahead of the product
+// and y written straight to global memory (8 rows of a block are 64
+// consecutive bytes).  No block-wide barrier after the staging
 // of W, so the warps' loads and products overlap freely.  HBM traffic per
 // block: NP states read, M doubles of the window part read, M of y written.
 #include "common.h"
@@ -48,42 +48,43 @@ __global__ void __launch_bounds__(kThreads) k_state_out(const double* __restrict
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int g = lane >> 2, t = lane & 3;
-    // a dependent DMMA costs ~200 cycles: each product runs as kChains
-    // independent partial sums of NP / 4 / kChains steps
-    constexpr int kChains = NP / 4 < 4 ? NP / 4 : 4;
-    const long tiles = (nblocks + 7) / 8;
+    // a warp takes 16 blocks at a time (two 8-block halves): every A fragment
+    // read from shared memory feeds two products
+    const long tiles = (nblocks + 15) / 16;
     for (long tile = (long)blockIdx.x * kWarps + warp; tile < tiles; tile += (long)gridDim.x * kWarps) {
-        const long b0 = tile * 8;
-        double bv[NP / 4];
-        {
-            const long bb = b0 + g;
+        const long b0 = tile * 16;
+        double bv[2][NP / 4];
 #pragma unroll
-            for (int kk = 0; kk < NP / 4; ++kk) bv[kk] = bb < nblocks ? X[bb * NP + 4 * kk + t] : 0.0;
+        for (int hf = 0; hf < 2; ++hf) {
+            const long bb = b0 + 8 * hf + g;
+#pragma unroll
+            for (int kk = 0; kk < NP / 4; ++kk) bv[hf][kk] = bb < nblocks ? X[bb * NP + 4 * kk + t] : 0.0;
         }
-        // this lane's two blocks (D fragment columns 2t, 2t + 1)
-        const long c0 = b0 + 2 * t, c1 = c0 + 1;
 #pragma unroll 2
         for (int mt = 0; mt < Mp / 8; ++mt) {
             const int r = mt * 8 + g;
-            const long o0 = c0 * gs + r, o1 = c1 * gs + r;
-            const bool v0 = r < M && c0 < nblocks && (limit < 0 || o0 < limit);
-            const bool v1 = r < M && c1 < nblocks && (limit < 0 || o1 < limit);
-            const double a0 = v0 ? acc[o0] : 0.0, a1 = v1 ? acc[o1] : 0.0;
-            double d[kChains][2];
+            // this lane's four blocks: D fragment columns 2t, 2t + 1 of each half
+            long o[4];
+            bool v[4];
+            double a[4];
 #pragma unroll
-            for (int q = 0; q < kChains; ++q) d[q][0] = d[q][1] = 0.0;
+            for (int q = 0; q < 4; ++q) {
+                const long c = b0 + 8 * (q >> 1) + 2 * t + (q & 1);
+                o[q] = c * gs + r;
+                v[q] = r < M && c < nblocks && (limit < 0 || o[q] < limit);
+                a[q] = v[q] ? acc[o[q]] : 0.0;
+            }
+            double d[4] = {0.0, 0.0, 0.0, 0.0};
             const double* wr = Ws + r * kpitch<NP>() + t;
 #pragma unroll
-            for (int kk = 0; kk < NP / 4; ++kk) dmma_m8n8k4(d[kk % kChains][0], d[kk % kChains][1], wr[4 * kk], bv[kk]);
+            for (int kk = 0; kk < NP / 4; ++kk) {
+                const double w = wr[4 * kk];
+                dmma_m8n8k4(d[0], d[1], w, bv[0][kk]);
+                dmma_m8n8k4(d[2], d[3], w, bv[1][kk]);
+            }
 #pragma unroll
-            for (int w = 1; w < kChains; w *= 2)
-#pragma unroll
-                for (int q = 0; q + w < kChains; q += 2 * w) {
-                    d[q][0] += d[q + w][0];
-                    d[q][1] += d[q + w][1];
-                }
-            if (v0) Y[o0] = a0 + d[0][0];
-            if (v1) Y[o1] = a1 + d[0][1];
+            for (int q = 0; q < 4; ++q)
+                if (v[q]) Y[o[q]] = a[q] + d[q];
         }
     }
 }
@@ -104,7 +105,7 @@ bool state_t(const double* W, long ld, int M, const double* X, const double* acc
     PARODE_CUDA(cudaFuncSetAttribute(k_state_out<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     PARODE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_state_out<NP>, kThreads, smem));
-    const long tiles = (nblocks + 7) / 8;
+    const long tiles = (nblocks + 15) / 16;
     const unsigned grid =
         (unsigned)std::max<long>(1, std::min<long>((tiles + kWarps - 1) / kWarps, (long)sms * std::max(per_sm, 1)));
     k_state_out<NP><<<grid, kThreads, smem, s>>>(W, ld, M, Mp, X, acc, Y, gs, nblocks, limit);

@@ -549,6 +549,7 @@ Plan::~Plan()
         else cudaFree(p);
     }
     const bool ok_s = !stream_ || cudaStreamSynchronize(stream_) == cudaSuccess;
+    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
     const bool ok_d = !side_ || cudaStreamSynchronize(side_) == cudaSuccess;
     for (cudaEvent_t e : events_) cudaEventDestroy(e);
     // idle streams and events go back to the pool for the next plan (handles
@@ -619,8 +620,58 @@ void Plan::execute(double* y, cudaStream_t s)
     if (shards_ > 1) throw Error(kInvalidArgument, "a time-shard plan runs through its up and down phases");
     PARODE_CUDA(cudaSetDevice(device_));
     if (!s) s = stream_;
+    // a plan executed again into the same output buffer replays its launch
+    // list as one CUDA graph (captured at the second such execute; stage
+    // profiling and the one-system batch form run launch by launch)
+    if (!profiling_ && !batch_ && graph_state_ >= 0) {
+        if (graph_state_ == 0 || y != graph_y_) {
+            if (graph_exec_) {
+                cudaGraphExecDestroy(graph_exec_);
+                graph_exec_ = nullptr;
+            }
+            graph_state_ = 1;
+            graph_y_ = y;
+        } else if (graph_state_ == 1) {
+            graph_state_ = capture_graph(y) ? 2 : -1;
+        }
+        if (graph_state_ == 2) {
+            PARODE_CUDA(cudaGraphLaunch(graph_exec_, s));
+            last_y_ = y ? y : dY_;
+            PARODE_CUDA(cudaEventRecord(done_, s));
+            return;
+        }
+    }
     execute_body(y, s);
     PARODE_CUDA(cudaEventRecord(done_, s));
+}
+
+bool Plan::capture_graph(double* y)
+{
+    if (cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    bool ok = true;
+    try {
+        execute_body(y, stream_);
+    } catch (...) {
+        ok = false;
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(stream_, &g);
+    if (!ok || e != cudaSuccess || !g) {
+        cudaGetLastError();
+        if (g) cudaGraphDestroy(g);
+        return false;
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&graph_exec_, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) {
+        cudaGetLastError();
+        graph_exec_ = nullptr;
+        return false;
+    }
+    return true;
 }
 
 const double* Plan::device_output() const { return batch_ ? batch_->device_output(0) : dY_; }

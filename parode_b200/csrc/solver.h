@@ -175,6 +175,12 @@ private:
     double* dTop_ = nullptr;    // gathered top items + their scan's scratch
     ChunkLevels shard_levels_;  // the up-sweep's levels, reused by the down-sweep
     bool shard_up_done_ = false;
+    // the launch list as a CUDA graph (execute): 0 none, 1 executed once into
+    // graph_y_, 2 graph ready for graph_y_, -1 capture failed
+    int graph_state_ = 0;
+    double* graph_y_ = nullptr;
+    cudaGraphExec_t graph_exec_ = nullptr;
+    bool capture_graph(double* y);
 };
 
 }  // namespace parode
