@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--min-warmup-s", type=float, default=0.5, help="least warm-up time under load (clock sampling)")
     ap.add_argument("--no-extra", action="store_true", help="skip the batched (4096 systems) and serving runs")
+    ap.add_argument("--time-partition", action="store_true",
+                    help="with N > 1 GPUs also time one cfg2 solve split by time over the ranks "
+                         "(parode_b200.multi.solve_time_partitioned: one all-gather per solve)")
     ap.add_argument("--serve-requests", type=int, default=256)
     ap.add_argument("--no-tune", action="store_true", help="time with the untuned block length of the response leaf")
     ap.add_argument("--ref-T", type=int, default=1 << 20,
@@ -506,6 +509,45 @@ def measure_serving(pb, wl, torch, count=64, rates=(500.0, 1000.0, 2000.0, 8000.
     return out
 
 
+def measure_time_partition(pb, torch, dev, case, u, precision, steps):
+    """One cfg2 solve split by time over all ranks (strong scaling of a single
+    system): each rank's shard plan, its up phase, one NCCL all-gather of the
+    shards' chunk aggregates, its down phase; the slowest rank's time."""
+    import torch.distributed as dist
+
+    rank, world = dist.get_rank(), dist.get_world_size()
+    plan = pb.Plan(case.A, case.B, case.C, case.D, case.x0, u, case.t0, case.t_end, case.h, solver=case.solver,
+                   precision=precision, shard=rank, shards=world)
+    _, steps_local, c, np_, _ = plan.shard_info
+    top = torch.zeros(c * np_, dtype=torch.float64, device=dev)
+    gathered = torch.empty(world * c * np_, dtype=torch.float64, device=dev)
+    y = torch.empty((plan.num_outputs, plan.channels), dtype=torch.float64, device=dev)
+    s = torch.cuda.current_stream(dev)
+
+    def solve():
+        plan.shard_up(top.data_ptr(), s.cuda_stream)
+        dist.all_gather_into_tensor(gathered, top)
+        plan.shard_down(gathered.data_ptr(), y.data_ptr(), s.cuda_stream)
+
+    for _ in range(3):
+        solve()
+    torch.cuda.synchronize()
+    dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(steps):
+        solve()
+    e1.record(s)
+    torch.cuda.synchronize()
+    ms = torch.tensor([e0.elapsed_time(e1) / steps], dtype=torch.float64, device=dev)
+    dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    plan.close()
+    ms = float(ms.item())
+    return {"workload": "cfg2 split by time over the ranks", "ms_per_solve": ms, "ranks": world,
+            "steps_on_rank0": steps_local, "value": case.n * case.T / (ms / 1e3), "unit": UNIT,
+            "scaling": "strong"}
+
+
 def run_ours(args):
     import torch
 
@@ -667,6 +709,8 @@ def run_ours(args):
                          note="parts timed separately with host clocks (synchronised); the e2e call overlaps the "
                               "host time vector with plan creation, the solve and the copy")
     cfg1 = measure_cfg1(pb, wl, torch) if world == 1 and not args.no_extra else None
+    tpart = measure_time_partition(pb, torch, dev, case, u, precision, args.steps) \
+        if (world > 1 and args.time_partition) else None
 
     batched = serving = cfg3 = None
     if not args.no_extra:
@@ -747,6 +791,7 @@ def run_ours(args):
             "batched": batched,
             "serving": serving,
             "abm_n128": cfg3,
+            "time_partitioned": tpart,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
