@@ -103,6 +103,25 @@ def reference_sample(T_sample):
     return case, run
 
 
+def cpu_batched_sample(wl):
+    """The batched workload's CPU baseline: every 8th cfg4 system (512 of 4096)
+    by the FP64 affine recurrence (the oracle's O1), OpenMP across systems on
+    all host threads."""
+    from oracle import oracle
+
+    sample = wl.cfg4()[::8]
+    jobs = [(oracle.System(c.A, c.B, c.C, c.D, c.x0), oracle.Input.sinusoid(c.u.a, c.u.f, c.u.phi), c.solver, c.t0,
+             c.t_end, c.h) for c in sample]
+    t0 = time.perf_counter()
+    ys = oracle.simulate_affine_many(jobs)
+    dt = time.perf_counter() - t0
+    work = float(sum(c.n * y.shape[0] for c, y in zip(sample, ys)))
+    cores = int(oracle.lib().po_threads())
+    return {"value": work / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"512 of the 4096 cfg4 systems (every 8th, {work:.3g} state*steps), FP64 affine recurrence, "
+                      f"OpenMP across systems, {dt:.1f} s on {cores} host threads"}
+
+
 def run_reference(args):
     rank, _, world = dist_env()
     if rank != 0:
@@ -762,6 +781,8 @@ def run_ours(args):
             cpu = {"value": c2.n * T_cpu / dt, "unit": UNIT, "cores": 1, "kind": "port",
                    "sample": f"the reference's CPU path (its tests' sequential FP32 RK4 loop, restated in C) on the "
                              f"full cfg2 horizon, {T_cpu} steps in {dt:.1f} s on 1 host core"}
+            if not args.no_extra:
+                cpu["batched"] = cpu_batched_sample(wl)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": main["ms_per_step"], "higher_is_better": True,

@@ -87,3 +87,26 @@ def test_shard_needs_the_response_path(pb):
     u = pb.register_sinusoid(c.u.a, c.u.f, c.u.phi)
     with pytest.raises(pb.ParODEError):
         pb.Plan(c.A, c.B, c.C, c.D, c.x0, u, c.t0, c.t_end, c.h, solver=0, shard=0, shards=2)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_time_partition_with_a_user_input_function(pb, precision):
+    """An NVRTC-compiled UFunc: every shard samples it at the whole horizon's
+    sample times (the sample index offset), so the split equals the unsplit
+    solve bit for bit."""
+    src = ("fType UFunc(fType t, int nInputIndex) {\n"
+           "    return sin(3.0 * t + nInputIndex) + 0.5 * cos(7.0 * t);\n"
+           "}\n")
+    u = pb.register_input(src)
+    c = wl.small(8400, 0, 16, 2, 2, 40000, h=1e-3)
+    y, _ = multi.emulate_time_partition(pb, c.A, c.B, c.C, c.D, c.x0, u, c.t0, c.t_end, c.h, 3, solver=0,
+                                        precision=precision)
+    pb.set_option(pb.OPT_PATH, pb.PATH_BLOCKED_RESPONSE)
+    try:
+        whole = pb.Plan(c.A, c.B, c.C, c.D, c.x0, u, c.t0, c.t_end, c.h, solver=0, precision=precision)
+    finally:
+        pb.set_option(pb.OPT_PATH, 0)
+    whole.execute()
+    _, y_whole = whole.output()
+    whole.close()
+    assert np.array_equal(y, y_whole)
