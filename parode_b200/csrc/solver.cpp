@@ -25,6 +25,7 @@ struct HandlePool {
     std::mutex mu;
     std::vector<std::pair<int, cudaStream_t>> streams;
     std::vector<std::pair<int, cudaEvent_t>> events;
+    std::vector<char*> pinned;
 };
 
 HandlePool& handles()
@@ -83,11 +84,56 @@ void give_event(int dev, cudaEvent_t e)
     h.events.emplace_back(dev, e);
 }
 
+// Pinned host blocks for a plan's small set-up copies (W's arguments, Phi,
+// B, C, D, the initial state, tensor maps): from pageable memory each copy
+// waits for its staging, from pinned memory it is queued at once.  A plan
+// holds one block until its set-up has synchronised.
+constexpr size_t kPinBlock = (size_t)512 << 10;
+
+char* take_pinned()
+{
+    {
+        HandlePool& h = handles();
+        std::lock_guard<std::mutex> g(h.mu);
+        if (!h.pinned.empty()) {
+            char* p = h.pinned.back();
+            h.pinned.pop_back();
+            return p;
+        }
+    }
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, kPinBlock, cudaHostAllocPortable) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;  // the copies then go from pageable memory
+    }
+    return static_cast<char*>(p);
+}
+
+void give_pinned(char* p)
+{
+    HandlePool& h = handles();
+    std::lock_guard<std::mutex> g(h.mu);
+    h.pinned.push_back(p);
+}
+
 }  // namespace
 
 Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex, int solver, double t0,
            double tEnd, double h, const PlanOptions& opt)
     : device_(device), sys_(sys), inputs_(inputs), opt_(opt), solver_(solver), t0_(t0), tEnd_(tEnd), h_(h)
+{
+    // a failed set-up returns what it took (buffers, streams, events, the
+    // pinned block) before the error leaves
+    try {
+        build(device, sys, inputs, uIndex, solver, t0, tEnd, h, opt);
+    } catch (...) {
+        release();
+        throw;
+    }
+}
+
+void Plan::build(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex, int solver, double t0,
+                 double tEnd, double h, const PlanOptions& opt)
 {
     if (solver != kRK4 && solver != kABM) throw Error(kInvalidSolverType, "unknown solver type");
     if (sys.n <= 0) throw Error(kInvalidSystem, "the system has no states");
@@ -314,8 +360,7 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
                 else if (sys.zeroD) v = (o == c) ? 1.0 : 0.0;
                 Cext[(size_t)o * Np_ + xoff + c] = v;
             }
-        PARODE_CUDA(cudaMemcpyAsync(dCext_, Cext.data(), sizeof(double) * Cext.size(), cudaMemcpyHostToDevice,
-                                    stream_));
+        h2d(dCext_, Cext.data(), sizeof(double) * Cext.size());
     }
     alloc(&dY_, nOut_ * (long)p_);
     if (solver == kRK4) {
@@ -359,14 +404,12 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
         }
     }
     phase("buffers", true);
-    PARODE_CUDA(cudaMemcpyAsync(dPow_, PhiP.data(), sizeof(double) * PhiP.size(), cudaMemcpyHostToDevice, stream_));
-    PARODE_CUDA(cudaMemcpyAsync(dBbar_, Bbar.data(), sizeof(double) * Bbar.size(), cudaMemcpyHostToDevice, stream_));
+    h2d(dPow_, PhiP.data(), sizeof(double) * PhiP.size());
+    h2d(dBbar_, Bbar.data(), sizeof(double) * Bbar.size());
     if (!sys.zeroC)
-        PARODE_CUDA(cudaMemcpyAsync(dC_, sys.C.data(), sizeof(double) * (size_t)p_ * n, cudaMemcpyHostToDevice,
-                                    stream_));
+        h2d(dC_, sys.C.data(), sizeof(double) * (size_t)p_ * n);
     if (!sys.zeroD)
-        PARODE_CUDA(cudaMemcpyAsync(dD_, sys.D.data(), sizeof(double) * (size_t)p_ * sys.m,
-                                    cudaMemcpyHostToDevice, stream_));
+        h2d(dD_, sys.D.data(), sizeof(double) * (size_t)p_ * sys.m);
 
     // ---- initial scan state -------------------------------------------------
     if (solver == kRK4) {
@@ -406,10 +449,9 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
             }
         }
         alloc(&dYpre_, 3L * p_);
-        PARODE_CUDA(cudaMemcpyAsync(dYpre_, ypre_.data(), sizeof(double) * ypre_.size(), cudaMemcpyHostToDevice,
-                                    stream_));
+        h2d(dYpre_, ypre_.data(), sizeof(double) * ypre_.size());
     }
-    PARODE_CUDA(cudaMemcpyAsync(dX0_, X0.data(), sizeof(double) * Np_, cudaMemcpyHostToDevice, stream_));
+    h2d(dX0_, X0.data(), sizeof(double) * Np_);
     phase("copies+start-up", true);
     if (br_) {
         // block response matrix from Phi (power-table level 0), Bbar, Cext, D
@@ -433,7 +475,7 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
         ra.NPstate = Np_;
         double* dra = nullptr;
         alloc(&dra, (long)((sizeof(ResponseArgs) + 7) / 8));
-        PARODE_CUDA(cudaMemcpyAsync(dra, &ra, sizeof(ra), cudaMemcpyHostToDevice, stream_));
+        h2d(dra, &ra, sizeof(ra));
         launch_block_response(reinterpret_cast<const ResponseArgs*>(dra), 1, Np_, p_, brKpad_, stream_);
         phase("W", true);
         // the carry's powers P_1 .. P_levels (Phi^(2^l)) depend on Phi alone:
@@ -467,7 +509,7 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
             alloc(&maps, 32);
             unsigned char host_maps[256];
             resp_encode_plane_maps(dUh_, dUl_, nblocks_, brK_, stride, host_maps);
-            PARODE_CUDA(cudaMemcpyAsync(maps, host_maps, 256, cudaMemcpyHostToDevice, stream_));
+            h2d(maps, host_maps, 256);
             RespArgs r[2];
             r[0].Ps = a.Ps;
             r[0].rows = Np_;
@@ -500,16 +542,19 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
             dTcStart_ = reinterpret_cast<long*>(d);
             alloc(&d, (long)ranges.size());
             dTcCta_ = reinterpret_cast<long*>(d);
-            PARODE_CUDA(cudaMemcpyAsync(dTc_, e, sizeof(e), cudaMemcpyHostToDevice, stream_));
-            PARODE_CUDA(cudaMemcpyAsync(dResp_, r, sizeof(r), cudaMemcpyHostToDevice, stream_));
-            PARODE_CUDA(cudaMemcpyAsync(dTcStart_, start, sizeof(start), cudaMemcpyHostToDevice, stream_));
-            PARODE_CUDA(cudaMemcpyAsync(dTcCta_, ranges.data(), sizeof(long) * ranges.size(), cudaMemcpyHostToDevice,
-                                        stream_));
+            h2d(dTc_, e, sizeof(e));
+            h2d(dResp_, r, sizeof(r));
+            h2d(dTcStart_, start, sizeof(start));
+            h2d(dTcCta_, ranges.data(), sizeof(long) * ranges.size());
             launch_level_split(dTc_, 2, (long)std::max(sa, sw) / 8, stream_);
             phase("tensor-core set-up", true);
         }
     }
     PARODE_CUDA(cudaStreamSynchronize(stream_));
+    if (pin_) {  // the set-up copies are done: the block goes back to the pool
+        give_pinned(pin_);
+        pin_ = nullptr;
+    }
     phase("sync", false);
     if (opt.log) std::fprintf(stderr, "ParODE plan set-up (n=%d T=%ld path=%d):%s\n", sys.n, nScan_, path(), phases.c_str());
     // keep a plan's worth of freed memory in the pool, so that the next plan
@@ -526,7 +571,9 @@ Plan::Plan(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex,
     }
 }
 
-Plan::~Plan()
+Plan::~Plan() { release(); }
+
+void Plan::release() noexcept
 {
     cudaSetDevice(device_);
     if (batch_) {
@@ -549,6 +596,7 @@ Plan::~Plan()
         else cudaFree(p);
     }
     const bool ok_s = !stream_ || cudaStreamSynchronize(stream_) == cudaSuccess;
+    if (pin_ && ok_s) give_pinned(pin_);
     if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
     const bool ok_d = !side_ || cudaStreamSynchronize(side_) == cudaSuccess;
     for (cudaEvent_t e : events_) cudaEventDestroy(e);
@@ -560,6 +608,31 @@ Plan::~Plan()
     if (done_) reuse ? give_event(device_, done_) : (void)cudaEventDestroy(done_);
     if (side_) reuse ? give_stream(device_, side_) : (void)cudaStreamDestroy(side_);
     if (stream_) reuse ? give_stream(device_, stream_) : (void)cudaStreamDestroy(stream_);
+    // idempotent
+    bufs_.clear();
+    events_.clear();
+    for (auto& e : fork_) e = nullptr;
+    done_ = nullptr;
+    side_ = stream_ = nullptr;
+    pin_ = nullptr;
+    graph_exec_ = nullptr;
+}
+
+void Plan::h2d(void* dst, const void* src, size_t bytes)
+{
+    // through the plan's pinned block while it has room, else from pageable memory
+    if (!pin_ && !pin_tried_) {
+        pin_ = take_pinned();
+        pin_tried_ = true;
+    }
+    const size_t at = (pin_used_ + 15) & ~(size_t)15;
+    if (pin_ && at + bytes <= kPinBlock) {
+        std::memcpy(pin_ + at, src, bytes);
+        PARODE_CUDA(cudaMemcpyAsync(dst, pin_ + at, bytes, cudaMemcpyHostToDevice, stream_));
+        pin_used_ = at + bytes;
+        return;
+    }
+    PARODE_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_));
 }
 
 void Plan::alloc(double** p, long n)

@@ -105,7 +105,11 @@ public:
     std::vector<std::pair<std::string, float>> stage_times();
 
 private:
+    void build(int device, const SystemDesc& sys, InputRegistry* inputs, int uIndex, int solver, double t0,
+               double tEnd, double h, const PlanOptions& opt);
+    void release() noexcept;
     void alloc(double** p, long n);
+    void h2d(void* dst, const void* src, size_t bytes);
     void mark(const char* stage, cudaStream_t s);
     void execute_body(double* y, cudaStream_t s);
     void execute_blocked(double* Y, cudaStream_t s);
@@ -175,6 +179,9 @@ private:
     double* dTop_ = nullptr;    // gathered top items + their scan's scratch
     ChunkLevels shard_levels_;  // the up-sweep's levels, reused by the down-sweep
     bool shard_up_done_ = false;
+    char* pin_ = nullptr;  // pinned staging of the set-up copies (h2d)
+    size_t pin_used_ = 0;
+    bool pin_tried_ = false;
     // the launch list as a CUDA graph (execute): 0 none, 1 executed once into
     // graph_y_, 2 graph ready for graph_y_, -1 capture failed
     int graph_state_ = 0;
