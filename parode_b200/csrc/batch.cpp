@@ -219,15 +219,84 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
     }
 
     phase("classify", false);
-    // ---- constant region: layout first, then the host FP64 discretisation
-    // (threads over systems) writes straight into its staged slots.  Phi is
-    // kept compact (RK4: n x n; ABM: its last block row, n x 4n, the rows
-    // above being the exact shift) and expanded into the padded power table's
-    // level 0 on the device: an ABM Phi is 16 n^2, its dense part 4 n^2
+    // ---- discretisation on the device (kernels_disc.cu): A and B go up,
+    // the compact Phi (RK4: n x n; ABM: its last block row, n x 4n, the rows
+    // above being the exact shift; expanded into the padded power table's
+    // level 0 later), Bbar (and its transpose for the level-synchronous
+    // systems) stay in the batch's discretisation buffer, and each system's
+    // distance ||Phi - R|| comes back (it sizes the tensor-core levels of the
+    // layout below).  The same bits as the host restatement.
+    PARODE_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    struct DiscOff {
+        size_t A, B, phi, bbar, bbarT, work;
+    };
+    std::vector<DiscOff> doff(N);
+    {
+        Layout D;
+        for (int i = 0; i < N; ++i) {  // staged inputs first
+            const SystemDesc& s = specs[i].sys;
+            const int mB = s.zeroB ? 0 : s.m;
+            doff[i].A = D.take(sizeof(double) * (size_t)sys_[i].n * sys_[i].n);
+            doff[i].B = mB ? D.take(sizeof(double) * (size_t)sys_[i].n * mB) : 0;
+        }
+        const size_t jobs_at = D.take(sizeof(DiscJob) * (size_t)N);
+        const size_t staged = D.bytes;
+        const size_t delta_at = D.take(sizeof(double) * (size_t)N);
+        for (int i = 0; i < N; ++i) {
+            const SystemDesc& s = specs[i].sys;
+            const Sys& q = sys_[i];
+            const int mB = s.zeroB ? 0 : s.m;
+            doff[i].phi = D.take(sizeof(double) * (size_t)q.n * q.Ns);
+            doff[i].bbar = D.take(sizeof(double) * (size_t)q.n * q.W * std::max(mB, 1));
+            doff[i].bbarT = (!q.blocked && !q.resp) ? D.take(sizeof(double) * (size_t)std::max(q.W * mB, 1) * q.n) : 0;
+            doff[i].work = D.take(sizeof(double) * (size_t)discretise_work_doubles(q.n, mB));
+        }
+        if (fault_alloc_now()) throw Error(kNotEnoughResources, "batch discretisation buffer (injected)");
+        cudaError_t e = cudaMallocAsync(&disc_, std::max<size_t>(D.bytes, 8), stream_);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            disc_ = nullptr;
+            throw Error(kNotEnoughResources, "batch discretisation buffer allocation failed");
+        }
+        char* db = static_cast<char*>(disc_);
+        std::unique_ptr<char[]> hsp(new char[std::max<size_t>(staged, 1)]);  // gaps are copied, never read
+        char* hs_data = hsp.get();
+        std::vector<DiscJob> jobs(N);
+        parallel_for(N, [&](int i) {
+            const SystemDesc& s = specs[i].sys;
+            const Sys& q = sys_[i];
+            const int mB = s.zeroB ? 0 : s.m;
+            std::memcpy(hs_data + doff[i].A, s.A.data(), sizeof(double) * (size_t)q.n * q.n);
+            if (mB) std::memcpy(hs_data + doff[i].B, s.B.data(), sizeof(double) * (size_t)q.n * mB);
+            DiscJob& j = jobs[i];
+            j.A = reinterpret_cast<const double*>(db + doff[i].A);
+            j.B = mB ? reinterpret_cast<const double*>(db + doff[i].B) : nullptr;
+            j.phi = reinterpret_cast<double*>(db + doff[i].phi);
+            j.bbar = reinterpret_cast<double*>(db + doff[i].bbar);
+            j.bbarT = doff[i].bbarT ? reinterpret_cast<double*>(db + doff[i].bbarT) : nullptr;
+            j.work = reinterpret_cast<double*>(db + doff[i].work);
+            j.delta = reinterpret_cast<double*>(db + delta_at) + i;
+            j.n = q.n;
+            j.m = mB;
+            j.solver = q.solver;
+            j.h = q.h;
+        });
+        std::memcpy(hs_data + jobs_at, jobs.data(), sizeof(DiscJob) * (size_t)N);
+        PARODE_CUDA(cudaMemcpyAsync(db, hs_data, staged, cudaMemcpyHostToDevice, stream_));
+        launch_discretise_batch(reinterpret_cast<const DiscJob*>(db + jobs_at), N, stream_);
+        std::vector<double> deltas((size_t)N);
+        PARODE_CUDA(cudaMemcpyAsync(deltas.data(), db + delta_at, sizeof(double) * (size_t)N, cudaMemcpyDeviceToHost,
+                                    stream_));
+        PARODE_CUDA(cudaStreamSynchronize(stream_));
+        for (int i = 0; i < N; ++i) sys_[i].delta = deltas[(size_t)i];
+    }
+    phase("discretise (device)", false);
+    // ---- constant region: layout first, then the host set-up (threads over
+    // systems) writes straight into its staged slots
     Layout L;
     struct Off {
-        size_t phi0, bbar, c, d, cext, x0, sin, ypre;
-        size_t bbarT, cT, dT;  // level-synchronous systems: transposed copies (coalesced per-row kernels)
+        size_t c, d, cext, x0, sin, ypre;
+        size_t cT, dT;  // level-synchronous systems: transposed copies (coalesced per-row kernels)
         size_t P, U, Y, V, G, CP, Ps, W, Psa, Psw;
     };
     std::vector<Off> off(N);
@@ -235,9 +304,6 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         const SystemDesc& s = specs[i].sys;
         Sys& q = sys_[i];
         Off& o = off[i];
-        const int mB = s.zeroB ? 0 : s.m;
-        o.phi0 = L.take(sizeof(double) * (size_t)q.n * q.Ns);
-        o.bbar = L.take(sizeof(double) * (size_t)q.n * q.W * std::max(mB, 1));
         o.c = L.take(sizeof(double) * (s.zeroC ? 1 : (size_t)q.p * q.n));
         o.d = L.take(sizeof(double) * (s.zeroD ? 1 : (size_t)q.p * s.m));
         o.x0 = L.take(sizeof(double) * (size_t)q.Np);
@@ -248,9 +314,8 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             o.sin = L.take(sizeof(double) * 3 * q.input->a.size());
         }
         o.ypre = q.solver == kABM ? L.take(sizeof(double) * 3 * (size_t)q.p) : 0;
-        o.bbarT = o.cT = o.dT = 0;
+        o.cT = o.dT = 0;
         if (!q.blocked && !q.resp) {
-            o.bbarT = L.take(sizeof(double) * (size_t)std::max(q.W * mB, 1) * q.n);
             o.cT = L.take(sizeof(double) * (size_t)q.n * q.p);
             o.dT = L.take(sizeof(double) * (size_t)std::max(s.m, 1) * q.p);
         }
@@ -263,28 +328,6 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         const SystemDesc& s = specs[i].sys;
         Sys& q = sys_[i];
         const Off& o = off[i];
-        const int mB = s.zeroB ? 0 : s.m;
-        double* phi = slot(o.phi0);
-        double* bbar = slot(o.bbar);
-        const size_t nb = (size_t)q.n * q.W * std::max(mB, 1);
-        std::fill(bbar, bbar + nb, 0.0);
-        if (q.solver == kRK4)
-            discretise_rk4(q.n, mB, s.A.data(), mB ? s.B.data() : nullptr, q.h, phi, bbar);
-        else
-            discretise_abm_last(q.n, mB, s.A.data(), mB ? s.B.data() : nullptr, q.h, phi, bbar);
-        // distance of Phi from its exact 0/1 part (I for RK4; for ABM the
-        // companion shift, whose rows above the last block are exact, the
-        // last row block reading itself): the max row sum of |Phi - R| over
-        // the stored rows
-        const int d0 = q.solver == kRK4 ? 0 : 3 * q.n;
-        double dmax = 0.0;
-        for (int r = 0; r < q.n; ++r) {
-            const int rc = d0 + r;
-            double sum = 0.0;
-            for (int c = 0; c < q.Ns; ++c) sum += std::fabs(phi[(size_t)r * q.Ns + c] - (c == rc ? 1.0 : 0.0));
-            dmax = std::max(dmax, sum);
-        }
-        q.delta = dmax;
         if (s.zeroC) slot(o.c)[0] = 0.0;
         else std::memcpy(slot(o.c), s.C.data(), sizeof(double) * (size_t)q.p * q.n);
         if (s.zeroD) slot(o.d)[0] = 0.0;
@@ -314,11 +357,6 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             std::memcpy(prm + 2 * na, e->phi.data(), sizeof(double) * na);
         }
         if (!q.blocked && !q.resp) {
-            const int Wm = q.W * mB;
-            double* bt = slot(o.bbarT);
-            std::fill(bt, bt + (size_t)std::max(Wm, 1) * q.n, 0.0);
-            for (int r = 0; r < q.n; ++r)
-                for (int c = 0; c < Wm; ++c) bt[(size_t)c * q.n + r] = bbar[(size_t)r * Wm + c];
             double* ct = slot(o.cT);
             double* dt = slot(o.dT);
             std::fill(ct, ct + (size_t)q.n * q.p, 0.0);
@@ -331,7 +369,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
                     for (int c = 0; c < s.m; ++c) dt[(size_t)c * q.p + r] = s.D[(size_t)r * s.m + c];
         }
     });
-    phase("discretise", false);
+    phase("host constants", false);
     // ABM start-up: nine inputs at t0 + j h/2 (sinusoids on the host; user
     // functions through their compiled kernel, sampled first on this thread);
     // the four states into x0, the outputs 0..2 into their slot (threads over
@@ -476,7 +514,6 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
     {
         // stream-ordered: creating or destroying a batch does not synchronise
         // the device, so batches can come and go while others run
-        PARODE_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
         if (fault_alloc_now()) throw Error(kNotEnoughResources, "batch arena allocation failed (injected)");
         cudaError_t e = cudaMallocAsync(&arena_, arena_bytes_, stream_);
         if (e != cudaSuccess) {
@@ -491,7 +528,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         Sys& q = sys_[i];
         const Off& o = off[i];
         q.P = dp(o.P);
-        q.Bbar = dp(o.bbar);
+        q.Bbar = reinterpret_cast<double*>(static_cast<char*>(disc_) + doff[i].bbar);
         q.C = dp(o.c);
         q.D = dp(o.d);
         q.X0 = dp(o.x0);
@@ -645,7 +682,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             f.n = q.n;
             f.m = q.zeroB ? 0 : q.m;
             f.solver = q.solver;
-            f.BbarT = dp(off[i].bbarT);
+            f.BbarT = reinterpret_cast<double*>(static_cast<char*>(disc_) + doff[i].bbarT);
             f.U = q.U;
             f.T = q.nScan;
             f.Tp = q.Tp;
@@ -998,7 +1035,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         const Sys& q = sys_[i];
         PhiJob pj;
         pj.dst = q.P;
-        pj.src = dp(off[i].phi0);
+        pj.src = reinterpret_cast<double*>(static_cast<char*>(disc_) + doff[i].phi);
         pj.n = q.n;
         pj.Np = q.Np;
         pj.solver = q.solver;
@@ -1183,6 +1220,7 @@ BatchPlan::~BatchPlan()
     if (last_stream_ && last_stream_ != stream_) cudaStreamSynchronize(last_stream_);
     if (stream_) cudaStreamSynchronize(stream_);
     if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    if (disc_) cudaFreeAsync(disc_, stream_ ? stream_ : cudaStreamPerThread);
     for (auto f : forks_)
         if (f) {
             cudaStreamSynchronize(f);

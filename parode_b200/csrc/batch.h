@@ -139,6 +139,7 @@ private:
     // the launch list as a CUDA graph (execute): 0 no execute yet, 1 one eager
     // execute, 2 graph instantiated, -1 capture failed (eager from then on)
     int graph_state_ = 0;
+    void* disc_ = nullptr;  // A, B, the compact Phi, Bbar (and transposes) of every system
     cudaGraphExec_t graph_exec_ = nullptr;
     void enqueue(cudaStream_t s);
     bool capture_graph();

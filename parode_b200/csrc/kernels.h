@@ -199,6 +199,26 @@ void launch_sinusoid_planes(float* hi, float* lo, int m, int K, const double* a,
 // FP64 samples into those planes (n values).  lo may be null in both (hi only).
 void launch_split_planes(const double* U, float* hi, float* lo, long n, cudaStream_t s);
 
+// The batch's discretisation on the device (kernels_disc.cu): one job per
+// system, A (n x n) and B (n x m, m = 0 without B) in, the compact Phi (RK4
+// n x n; ABM the last block row, n x 4n), Bbar (n x W max(m, 1), W = 3 / 5)
+// and, when bbarT is set, its transpose out, with ||Phi - R||_inf into
+// *delta; work: discretise_work_doubles(n, m) doubles.  The same bits as the
+// host restatement (host_math.cpp).
+struct DiscJob {
+    const double* A = nullptr;
+    const double* B = nullptr;
+    double* phi = nullptr;
+    double* bbar = nullptr;
+    double* bbarT = nullptr;
+    double* work = nullptr;
+    double* delta = nullptr;
+    int n = 0, m = 0, solver = 0;
+    double h = 0.0;
+};
+long discretise_work_doubles(int n, int m);
+void launch_discretise_batch(const DiscJob* jobs, int njobs, cudaStream_t s);
+
 // Scan-vector initialisation with the forcing term Gamma_k (zero padding
 // for k >= T and for the components the solver leaves empty).
 void launch_forcing(double* V, int Np, int n, int m, int solver, const double* Bbar, const double* U, long T,
