@@ -724,44 +724,45 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         nSeed_ = (int)cj.size();
         // grouped level launches: for each level, entries grouped by tiling config
         // one persistent tensor-core launch over the entries' tiles
-        auto make_tc = [&](std::vector<LevelArgs>& tc) {
-            // TMA tensor maps of the entries' source columns (128 bytes each)
-            std::vector<unsigned char> maps(tc.size() * 128);
-            for (size_t k = 0; k < tc.size(); ++k) level_encode_src_map(tc[k], &maps[k * 128]);
-            const size_t moff = jput(maps.data(), maps.size());
-            for (size_t k = 0; k < tc.size(); ++k) tc[k].src_map = base + moff + k * 128;
-            GroupedLaunch gl;
-            gl.cfg.id = kTcConfig;
+        // A level's launches in two steps: prepare (grouping by tiling
+        // configuration, tile prefix sums, tensor maps; no shared state, so
+        // the levels are prepared on all host threads) and emit (their arrays
+        // appended to the staged job tables, in launch order)
+        struct PreparedGroup {
+            LevelConfig cfg;
+            std::vector<LevelArgs> stored, swaps;
             std::vector<long> start;
-            long tiles = 0;
-            for (const LevelArgs& a : tc) {
-                start.push_back(tiles);
-                tiles += level_tc_tiles(a);
-            }
-            gl.nent = (int)tc.size();
-            gl.tiles = tiles;
-            gl.args = reinterpret_cast<LevelArgs*>(base + jput(tc.data(), sizeof(LevelArgs) * tc.size()));
-            gl.start = reinterpret_cast<long*>(base + jput(start.data(), sizeof(long) * start.size()));
-            // one persistent CTA per SM, tile ranges balanced by work
-            gl.ctas = (int)std::min<long>(sms_, tiles);
-            std::vector<long> r = level_tc_ranges(tc, gl.ctas);
-            gl.cta = reinterpret_cast<long*>(base + jput(r.data(), sizeof(long) * r.size()));
-            return gl;
+            long tiles = 0, swap_elems = 0;
+            size_t smem = 0;
         };
-        auto add_level = [&](std::vector<GroupedLaunch>& out, const std::vector<std::pair<int, LevelArgs>>& ents,
-                             int l) {
+        struct PreparedLevel {
+            std::vector<PreparedGroup> groups;
+            std::vector<LevelArgs> tc;
+            std::vector<unsigned char> maps;
+            std::vector<long> tc_start, tc_ranges;
+            long tc_tiles = 0;
+            int tc_ctas = 0;
+        };
+        auto prepare_tc = [&](PreparedLevel& P) {
+            // TMA tensor maps of the entries' source columns (128 bytes each)
+            P.maps.resize(P.tc.size() * 128);
+            for (size_t k = 0; k < P.tc.size(); ++k) level_encode_src_map(P.tc[k], &P.maps[k * 128]);
+            for (const LevelArgs& a : P.tc) {
+                P.tc_start.push_back(P.tc_tiles);
+                P.tc_tiles += level_tc_tiles(a);
+            }
+            // one persistent CTA per SM, tile ranges balanced by work
+            P.tc_ctas = (int)std::min<long>(sms_, P.tc_tiles);
+            P.tc_ranges = level_tc_ranges(P.tc, P.tc_ctas);
+        };
+        auto prepare = [&](const std::vector<std::pair<int, LevelArgs>>& ents, int l) {
             // group by (config id, CW); entries keep the original form for the
             // swap of a tiled down-sweep and the stored form for the contraction
-            struct Group {
-                std::pair<int, int> key;
-                LevelConfig cfg;
-                std::vector<LevelArgs> stored, swaps;
-            };
-            std::vector<Group> groups;
+            PreparedLevel P;
+            std::vector<std::pair<int, int>> keys;
             // mixed form: levels below the top four of a system run on the
             // tensor cores (3xTF32); the top four, where high powers of Phi
             // amplify rounding, stay FP64
-            std::vector<LevelArgs> tc;
             for (const auto& e : ents) {
                 if (e.second.ncols <= 0) continue;
                 const Sys& q = sys_[e.first];
@@ -774,113 +775,140 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
                     t.rn = q.solver == kRK4 ? 0 : q.n;
                     t.rsh = std::min(1 << std::min(k, 2), 3);
                     t.Ps = q.Ps + (size_t)l * (level_split_bytes(q.Np) / sizeof(float));
-                    tc.push_back(t);
+                    P.tc.push_back(t);
                     continue;
                 }
                 LevelConfig c = level_config(e.second);
                 std::pair<int, int> key(c.id, c.CW);
-                auto it = std::find_if(groups.begin(), groups.end(), [&](const Group& g) { return g.key == key; });
-                if (it == groups.end()) {
-                    groups.push_back(Group{key, c, {}, {}});
-                    it = groups.end() - 1;
+                size_t g = 0;
+                while (g < keys.size() && keys[g] != key) ++g;
+                if (g == keys.size()) {
+                    keys.push_back(key);
+                    P.groups.emplace_back();
+                    P.groups.back().cfg = c;
                 }
-                it->stored.push_back(level_grouped_args(e.second));
-                if (c.id >= 5 && e.second.cpy) it->swaps.push_back(e.second);
+                PreparedGroup& G = P.groups[g];
+                G.stored.push_back(level_grouped_args(e.second));
+                if (c.id >= 5 && e.second.cpy) G.swaps.push_back(e.second);
             }
-            for (auto& g : groups) {
-                GroupedLaunch gl;
-                gl.cfg = g.cfg;
-                std::vector<long> start;
-                long tiles = 0;
-                size_t smem = 0;
-                for (const LevelArgs& a : g.stored) {
+            for (PreparedGroup& G : P.groups) {
+                for (const LevelArgs& a : G.stored) {
                     LevelConfig c = level_config(a);
-                    start.push_back(tiles);
-                    tiles += level_tiles(c, a);
-                    smem = std::max(smem, c.smem);
+                    G.start.push_back(G.tiles);
+                    G.tiles += level_tiles(c, a);
+                    G.smem = std::max(G.smem, c.smem);
                 }
-                gl.nent = (int)g.stored.size();
-                gl.tiles = tiles;
-                gl.smem = smem;
-                gl.args = reinterpret_cast<LevelArgs*>(base + jput(g.stored.data(), sizeof(LevelArgs) * g.stored.size()));
-                gl.start = reinterpret_cast<long*>(base + jput(start.data(), sizeof(long) * start.size()));
-                if (!g.swaps.empty()) {
-                    for (const LevelArgs& a : g.swaps) gl.swap_elems = std::max(gl.swap_elems, a.ncols * (long)a.Np);
-                    gl.nswap = (int)g.swaps.size();
-                    gl.swaps = reinterpret_cast<LevelArgs*>(base + jput(g.swaps.data(), sizeof(LevelArgs) * g.swaps.size()));
+                for (const LevelArgs& a : G.swaps) G.swap_elems = std::max(G.swap_elems, a.ncols * (long)a.Np);
+            }
+            if (!P.tc.empty()) prepare_tc(P);
+            return P;
+        };
+        auto emit_tc = [&](PreparedLevel& P) {
+            const size_t moff = jput(P.maps.data(), P.maps.size());
+            for (size_t k = 0; k < P.tc.size(); ++k) P.tc[k].src_map = base + moff + k * 128;
+            GroupedLaunch gl;
+            gl.cfg.id = kTcConfig;
+            gl.nent = (int)P.tc.size();
+            gl.tiles = P.tc_tiles;
+            gl.args = reinterpret_cast<LevelArgs*>(base + jput(P.tc.data(), sizeof(LevelArgs) * P.tc.size()));
+            gl.start = reinterpret_cast<long*>(base + jput(P.tc_start.data(), sizeof(long) * P.tc_start.size()));
+            gl.ctas = P.tc_ctas;
+            gl.cta = reinterpret_cast<long*>(base + jput(P.tc_ranges.data(), sizeof(long) * P.tc_ranges.size()));
+            return gl;
+        };
+        auto emit = [&](std::vector<GroupedLaunch>& out, PreparedLevel& P) {
+            for (PreparedGroup& G : P.groups) {
+                GroupedLaunch gl;
+                gl.cfg = G.cfg;
+                gl.nent = (int)G.stored.size();
+                gl.tiles = G.tiles;
+                gl.smem = G.smem;
+                gl.args = reinterpret_cast<LevelArgs*>(base + jput(G.stored.data(), sizeof(LevelArgs) * G.stored.size()));
+                gl.start = reinterpret_cast<long*>(base + jput(G.start.data(), sizeof(long) * G.start.size()));
+                if (!G.swaps.empty()) {
+                    gl.swap_elems = G.swap_elems;
+                    gl.nswap = (int)G.swaps.size();
+                    gl.swaps = reinterpret_cast<LevelArgs*>(base + jput(G.swaps.data(), sizeof(LevelArgs) * G.swaps.size()));
                 }
                 out.push_back(gl);
             }
-            if (!tc.empty()) out.push_back(make_tc(tc));
+            if (!P.tc.empty()) out.push_back(emit_tc(P));
         };
-        for (int l = 1; l < Pmax; ++l) {
+        auto add_level = [&](std::vector<GroupedLaunch>& out, const std::vector<std::pair<int, LevelArgs>>& ents,
+                             int l) {
+            PreparedLevel P = prepare(ents, l);
+            emit(out, P);
+        };
+        auto make_tc = [&](std::vector<LevelArgs>& tc) {
+            PreparedLevel P;
+            P.tc = tc;
+            prepare_tc(P);
+            return emit_tc(P);
+        };
+        // the levels of every system: power table, up-sweep, down-sweep, in
+        // launch order
+        struct LevelTask {
+            std::vector<GroupedLaunch>* out;
+            int l, tc_level;
+            int kind;  // 0 power table, 1 up-sweep, 2 down-sweep
+            PreparedLevel P;
+        };
+        std::vector<LevelTask> tasks;
+        for (int l = 1; l < Pmax; ++l) tasks.push_back(LevelTask{&ls_power_, l, -1, 0, {}});  // the power table stays FP64
+        for (int l = 0; l < Lmax; ++l) tasks.push_back(LevelTask{&ls_up_, l, l, 1, {}});
+        for (int l = Lmax - 1; l >= 0; --l) tasks.push_back(LevelTask{&ls_down_, l, l, 2, {}});
+        parallel_for((int)tasks.size(), [&](int t) {
+            LevelTask& T = tasks[t];
+            const int l = T.l;
             std::vector<std::pair<int, LevelArgs>> ents;
             for (int i : lv) {
                 const Sys& q = sys_[i];
-                if (l >= q.pow_levels) continue;
                 const long Np = q.Np;
                 LevelArgs a;
-                a.P = q.P + (long)(l - 1) * Np * Np;
-                a.ldp = Np;
-                a.Np = q.Np;
-                a.ncols = Np;
-                a.src = a.P;
-                a.src_gs = 1;
-                a.src_ks = Np;
-                a.dst = q.P + (long)l * Np * Np;
-                a.dst_gs = 1;
-                a.dst_is = Np;
+                if (T.kind == 0) {
+                    if (l >= q.pow_levels) continue;
+                    a.P = q.P + (long)(l - 1) * Np * Np;
+                    a.ldp = Np;
+                    a.Np = q.Np;
+                    a.ncols = Np;
+                    a.src = a.P;
+                    a.src_gs = 1;
+                    a.src_ks = Np;
+                    a.dst = q.P + (long)l * Np * Np;
+                    a.dst_gs = 1;
+                    a.dst_is = Np;
+                } else {
+                    if (l >= q.levels) continue;
+                    const long d = 1L << l;
+                    const long items = q.resp ? q.nblocks : q.nScan;
+                    a.P = q.P + (long)(q.lev0 + l) * Np * Np;
+                    a.ldp = Np;
+                    a.Np = q.Np;
+                    a.ncols = sweep_columns(items, q.Tp, d);
+                    if (T.kind == 1) {
+                        a.src = q.V + d * Np;
+                        a.src_gs = 2 * d * Np;
+                        a.acc = q.V + 2 * d * Np;
+                        a.acc_gs = 2 * d * Np;
+                        a.dst = q.V + 2 * d * Np;
+                        a.dst_gs = 2 * d * Np;
+                    } else {
+                        // in place: node prefix in slot g 2d - 1, right half's prefix
+                        // replaces the left half's aggregate in slot g 2d + d - 1
+                        a.src = q.V;
+                        a.src_gs = 2 * d * Np;
+                        a.acc = q.V + d * Np;
+                        a.acc_gs = 2 * d * Np;
+                        a.dst = q.V + d * Np;
+                        a.dst_gs = 2 * d * Np;
+                    }
+                }
                 ents.push_back({i, a});
             }
-            add_level(ls_power_, ents, -1);  // the power table stays FP64
-        }
-        phase("jobs/power-levels", false);
-        for (int l = 0; l < Lmax; ++l) {
-            std::vector<std::pair<int, LevelArgs>> ents;
-            for (int i : lv) {
-                const Sys& q = sys_[i];
-                if (l >= q.levels) continue;
-                const long Np = q.Np, d = 1L << l;
-                const long items = q.resp ? q.nblocks : q.nScan;
-                LevelArgs a;
-                a.P = q.P + (long)(q.lev0 + l) * Np * Np;
-                a.ldp = Np;
-                a.Np = q.Np;
-                a.ncols = sweep_columns(items, q.Tp, d);
-                a.src = q.V + d * Np;
-                a.src_gs = 2 * d * Np;
-                a.acc = q.V + 2 * d * Np;
-                a.acc_gs = 2 * d * Np;
-                a.dst = q.V + 2 * d * Np;
-                a.dst_gs = 2 * d * Np;
-                ents.push_back({i, a});
-            }
-            add_level(ls_up_, ents, l);
-        }
-        for (int l = Lmax - 1; l >= 0; --l) {
-            std::vector<std::pair<int, LevelArgs>> ents;
-            for (int i : lv) {
-                const Sys& q = sys_[i];
-                if (l >= q.levels) continue;
-                const long Np = q.Np, d = 1L << l;
-                const long items = q.resp ? q.nblocks : q.nScan;
-                LevelArgs a;
-                a.P = q.P + (long)(q.lev0 + l) * Np * Np;
-                a.ldp = Np;
-                a.Np = q.Np;
-                a.ncols = sweep_columns(items, q.Tp, d);
-                // in place: node prefix in slot g 2d - 1, right half's prefix
-                // replaces the left half's aggregate in slot g 2d + d - 1
-                a.src = q.V;
-                a.src_gs = 2 * d * Np;
-                a.acc = q.V + d * Np;
-                a.acc_gs = 2 * d * Np;
-                a.dst = q.V + d * Np;
-                a.dst_gs = 2 * d * Np;
-                ents.push_back({i, a});
-            }
-            add_level(ls_down_, ents, l);
-        }
+            T.P = prepare(ents, T.tc_level);
+        });
+        phase("jobs/levels prepared", false);
+        for (LevelTask& T : tasks) emit(*T.out, T.P);
         phase("jobs/scan-levels", false);
         // response GEMMs (FP64 tiled DMMA): the block aggregates into scan
         // slots 0 .. Tp - 1 (zeros past the last block), then the outputs from
