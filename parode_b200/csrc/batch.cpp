@@ -858,6 +858,8 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         for (int l = 0; l < Lmax; ++l) tasks.push_back(LevelTask{&ls_up_, l, l, 1, {}});
         for (int l = Lmax - 1; l >= 0; --l) tasks.push_back(LevelTask{&ls_down_, l, l, 2, {}});
         parallel_for((int)tasks.size(), [&](int t) {
+            // the tensor-map encoder needs the device's context current on this thread
+            PARODE_CUDA(cudaSetDevice(device_));
             LevelTask& T = tasks[t];
             const int l = T.l;
             std::vector<std::pair<int, LevelArgs>> ents;
