@@ -557,11 +557,13 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
     // ---- job arrays (staged after the work region) ----------------------------
     Layout J;
     J.bytes = work_end;
-    std::vector<char> jstage;
+    // sized by the reservation (uninitialised: the alignment gaps are copied,
+    // never read); a job array past it is an error below
+    std::unique_ptr<char[]> jstage(new char[std::max<size_t>(arena_bytes_ - work_end, 1)]);
     auto jput = [&](const void* src, size_t n) {
         size_t at = J.take(n);
-        if (jstage.size() < J.bytes - work_end) jstage.resize(J.bytes - work_end, 0);
-        std::memcpy(jstage.data() + (at - work_end), src, n);
+        if (J.bytes > arena_bytes_) throw Error(kDeviceError, "batch job arrays overflow the arena reservation");
+        std::memcpy(jstage.get() + (at - work_end), src, n);
         return at;
     };
     std::vector<CopyJob> setup_copies;
@@ -743,10 +745,20 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             long tc_tiles = 0;
             int tc_ctas = 0;
         };
-        auto prepare_tc = [&](PreparedLevel& P) {
+        auto prepare_tc = [&](PreparedLevel& P, bool threads) {
             // TMA tensor maps of the entries' source columns (128 bytes each)
             P.maps.resize(P.tc.size() * 128);
-            for (size_t k = 0; k < P.tc.size(); ++k) level_encode_src_map(P.tc[k], &P.maps[k * 128]);
+            if (threads && P.tc.size() >= 1024) {
+                const int chunks = 32;
+                const size_t per = (P.tc.size() + chunks - 1) / chunks;
+                parallel_for(chunks, [&](int ck) {
+                    PARODE_CUDA(cudaSetDevice(device_));  // the encoder needs the device's context
+                    for (size_t k = ck * per; k < std::min(P.tc.size(), (size_t)(ck + 1) * per); ++k)
+                        level_encode_src_map(P.tc[k], &P.maps[k * 128]);
+                });
+            } else {
+                for (size_t k = 0; k < P.tc.size(); ++k) level_encode_src_map(P.tc[k], &P.maps[k * 128]);
+            }
             for (const LevelArgs& a : P.tc) {
                 P.tc_start.push_back(P.tc_tiles);
                 P.tc_tiles += level_tc_tiles(a);
@@ -800,7 +812,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
                 }
                 for (const LevelArgs& a : G.swaps) G.swap_elems = std::max(G.swap_elems, a.ncols * (long)a.Np);
             }
-            if (!P.tc.empty()) prepare_tc(P);
+            if (!P.tc.empty()) prepare_tc(P, false);  // the levels already run on all threads
             return P;
         };
         auto emit_tc = [&](PreparedLevel& P) {
@@ -842,7 +854,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         auto make_tc = [&](std::vector<LevelArgs>& tc) {
             PreparedLevel P;
             P.tc = tc;
-            prepare_tc(P);
+            prepare_tc(P, true);
             return emit_tc(P);
         };
         // the levels of every system: power table, up-sweep, down-sweep, in
@@ -1095,7 +1107,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
     // work buffers start zeroed (the response windows' sample padding relies on it)
     if (!rs_.empty()) PARODE_CUDA(cudaMemsetAsync(base + const_end, 0, work_end - const_end, stream_));
     PARODE_CUDA(cudaMemcpyAsync(base, stage.get(), const_end, cudaMemcpyHostToDevice, stream_));
-    PARODE_CUDA(cudaMemcpyAsync(base + work_end, jstage.data(), jstage.size(), cudaMemcpyHostToDevice, stream_));
+    PARODE_CUDA(cudaMemcpyAsync(base + work_end, jstage.get(), J.bytes - work_end, cudaMemcpyHostToDevice, stream_));
     for (size_t k = 0; k < setup_copies.size(); k += 65535)
         launch_copy_batch(dSetup + k, (int)std::min<size_t>(65535, setup_copies.size() - k), max_copy, stream_);
     for (size_t k = 0; k < phi_jobs.size(); k += 65535)
@@ -1121,7 +1133,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
     PARODE_CUDA(cudaEventCreateWithFlags(&ready_, cudaEventDisableTiming));
     PARODE_CUDA(cudaEventRecord(ready_, stream_));
     host_stage_ = std::move(stage);
-    host_keep_.push_back(std::move(jstage));
+    host_jobs_ = std::move(jstage);
     phase("splits", true);
     if (opt.log)
         std::fprintf(stderr,

@@ -152,6 +152,7 @@ private:
     // that the constructor returns without waiting for the device
     std::vector<std::vector<char>> host_keep_;
     std::unique_ptr<char[]> host_stage_;  // the staged constant region
+    std::unique_ptr<char[]> host_jobs_;   // the staged job arrays
     InputRegistry* inputs_ = nullptr;
     PlanOptions opt_;
     std::vector<Sys> sys_;
