@@ -6,6 +6,8 @@
 #include "common.h"
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -65,6 +67,64 @@ void parallel_for(int n, F&& f)
 }
 
 }  // namespace
+
+// Pinned host blocks for the batches' staged uploads (discretisation inputs,
+// constants, job tables), kept for the next batch: from pinned memory the
+// uploads are plain DMA and the staging writes meet no first-touch page
+// faults.  Blocks are powers of two from 1 MiB; a failed pinning falls back to
+// pageable memory.
+namespace {
+
+struct PinnedBlocks {
+    std::mutex mu;
+    std::multimap<size_t, char*> free;
+};
+
+PinnedBlocks& pinned_blocks()
+{
+    static PinnedBlocks* p = new PinnedBlocks();
+    return *p;
+}
+
+}  // namespace
+
+HostStage::HostStage(size_t bytes)
+{
+    bytes = std::max<size_t>(bytes, 1);
+    {
+        PinnedBlocks& b = pinned_blocks();
+        std::lock_guard<std::mutex> g(b.mu);
+        auto it = b.free.lower_bound(bytes);
+        if (it != b.free.end() && it->first <= 4 * bytes) {
+            cap_ = it->first;
+            p_ = it->second;
+            b.free.erase(it);
+            pinned_ = true;
+            return;
+        }
+    }
+    size_t cap = (size_t)1 << 20;
+    while (cap < bytes) cap <<= 1;
+    void* q = nullptr;
+    if (cudaHostAlloc(&q, cap, cudaHostAllocPortable) == cudaSuccess) {
+        p_ = static_cast<char*>(q);
+        cap_ = cap;
+        pinned_ = true;
+        return;
+    }
+    cudaGetLastError();
+    owned_.reset(new char[bytes]);
+    p_ = owned_.get();
+    cap_ = bytes;
+}
+
+HostStage::~HostStage()
+{
+    if (!pinned_ || !p_) return;
+    PinnedBlocks& b = pinned_blocks();
+    std::lock_guard<std::mutex> g(b.mu);
+    b.free.emplace(cap_, p_);
+}
 
 BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* inputs, const PlanOptions& opt)
     : device_(device), inputs_(inputs), opt_(opt)
@@ -259,8 +319,8 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             throw Error(kNotEnoughResources, "batch discretisation buffer allocation failed");
         }
         char* db = static_cast<char*>(disc_);
-        std::unique_ptr<char[]> hsp(new char[std::max<size_t>(staged, 1)]);  // gaps are copied, never read
-        char* hs_data = hsp.get();
+        HostStage hsp(staged);  // gaps are copied, never read; released after the synchronise below
+        char* hs_data = hsp.data();
         std::vector<DiscJob> jobs(N);
         parallel_for(N, [&](int i) {
             const SystemDesc& s = specs[i].sys;
@@ -322,8 +382,8 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
     }
     // uninitialised: every slot is written below (the alignment gaps are
     // copied but never read)
-    std::unique_ptr<char[]> stage(new char[std::max<size_t>(L.bytes, 1)]);
-    auto slot = [&](size_t o) { return reinterpret_cast<double*>(stage.get() + o); };
+    auto stage = std::make_unique<HostStage>(L.bytes);
+    auto slot = [&](size_t o) { return reinterpret_cast<double*>(stage->data() + o); };
     parallel_for(N, [&](int i) {
         const SystemDesc& s = specs[i].sys;
         Sys& q = sys_[i];
@@ -559,11 +619,11 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
     J.bytes = work_end;
     // sized by the reservation (uninitialised: the alignment gaps are copied,
     // never read); a job array past it is an error below
-    std::unique_ptr<char[]> jstage(new char[std::max<size_t>(arena_bytes_ - work_end, 1)]);
+    auto jstage = std::make_unique<HostStage>(arena_bytes_ - work_end);
     auto jput = [&](const void* src, size_t n) {
         size_t at = J.take(n);
         if (J.bytes > arena_bytes_) throw Error(kDeviceError, "batch job arrays overflow the arena reservation");
-        std::memcpy(jstage.get() + (at - work_end), src, n);
+        std::memcpy(jstage->data() + (at - work_end), src, n);
         return at;
     };
     std::vector<CopyJob> setup_copies;
@@ -1104,10 +1164,13 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
 
     phase("jobs", false);
     // ---- upload and set-up launches ------------------------------------------
+    // from here on the device reads the staged blocks: a failure waits for the
+    // stream before the blocks go back to the pool
+    try {
     // work buffers start zeroed (the response windows' sample padding relies on it)
     if (!rs_.empty()) PARODE_CUDA(cudaMemsetAsync(base + const_end, 0, work_end - const_end, stream_));
-    PARODE_CUDA(cudaMemcpyAsync(base, stage.get(), const_end, cudaMemcpyHostToDevice, stream_));
-    PARODE_CUDA(cudaMemcpyAsync(base + work_end, jstage.get(), J.bytes - work_end, cudaMemcpyHostToDevice, stream_));
+    PARODE_CUDA(cudaMemcpyAsync(base, stage->data(), const_end, cudaMemcpyHostToDevice, stream_));
+    PARODE_CUDA(cudaMemcpyAsync(base + work_end, jstage->data(), J.bytes - work_end, cudaMemcpyHostToDevice, stream_));
     for (size_t k = 0; k < setup_copies.size(); k += 65535)
         launch_copy_batch(dSetup + k, (int)std::min<size_t>(65535, setup_copies.size() - k), max_copy, stream_);
     for (size_t k = 0; k < phi_jobs.size(); k += 65535)
@@ -1135,6 +1198,10 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
     host_stage_ = std::move(stage);
     host_jobs_ = std::move(jstage);
     phase("splits", true);
+    } catch (...) {
+        if (stream_) cudaStreamSynchronize(stream_);
+        throw;
+    }
     if (opt.log)
         std::fprintf(stderr,
                      "ParODE batch set-up (%d systems, %zu response, %zu level, %zu buckets, %.2f GB: tables+scan %.2f, "

@@ -40,6 +40,23 @@ struct BatchSpec {
     InputEntry* input = nullptr;
 };
 
+// Host staging of a batch's uploads: a pooled pinned block (kept for the next
+// batch when this one is done), or pageable memory when pinning fails.
+class HostStage {
+public:
+    explicit HostStage(size_t bytes);
+    ~HostStage();
+    HostStage(const HostStage&) = delete;
+    HostStage& operator=(const HostStage&) = delete;
+    char* data() { return p_; }
+
+private:
+    char* p_ = nullptr;
+    size_t cap_ = 0;
+    bool pinned_ = false;
+    std::unique_ptr<char[]> owned_;
+};
+
 class BatchPlan {
 public:
     BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* inputs, const PlanOptions& opt);
@@ -151,8 +168,8 @@ private:
     // host images of the set-up copies, kept until the plan is destroyed so
     // that the constructor returns without waiting for the device
     std::vector<std::vector<char>> host_keep_;
-    std::unique_ptr<char[]> host_stage_;  // the staged constant region
-    std::unique_ptr<char[]> host_jobs_;   // the staged job arrays
+    std::unique_ptr<HostStage> host_stage_;  // the staged constant region
+    std::unique_ptr<HostStage> host_jobs_;   // the staged job arrays
     InputRegistry* inputs_ = nullptr;
     PlanOptions opt_;
     std::vector<Sys> sys_;
