@@ -44,6 +44,18 @@ extern "C" {
                                       ParODE_BatchCreate is expected to run; the block-response leaf picks
                                       its block size against the FP64 build of its tables spread over that
                                       many solves (SimulateODE and the server always use 1) */
+#define PARODE_OPT_POOL_KEEP    7  /* >= 0 bytes (default 0): freed device memory that each selected device's
+                                      stream-ordered pool keeps mapped (its release threshold), so that a
+                                      later plan or batch of a similar size skips mapping fresh memory; needs
+                                      ParODE_Init / InitWithGPUs first (-2 before).  A server sets its own
+                                      device's threshold to its HBM budget. */
+#define PARODE_OPT_DISCRETISE   8  /* where a batch (or a server's batch) discretises its systems:
+                                      PARODE_DISCRETISE_AUTO (default: small batches on the host threads, with
+                                      no device round trip; large ones on the device), _HOST or _DEVICE.  Both
+                                      sides take every operation in the same order: the same bits. */
+#define PARODE_DISCRETISE_AUTO   0
+#define PARODE_DISCRETISE_HOST   1
+#define PARODE_DISCRETISE_DEVICE 2
 
 /* Test hooks, host side only (nothing faults on the device):
  *   PARODE_OPT_FAULT_ALLOC   k >= 0: the k-th device allocation of a solve,

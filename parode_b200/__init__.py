@@ -39,6 +39,11 @@ OPT_LOG = 3
 OPT_EXECUTIONS = 4
 OPT_FAULT_ALLOC = 5      # test hook: the k-th device allocation from now fails (-1: off)
 OPT_FAULT_WITHHOLD = 6   # test hook: the mixed response kernel withholds one arrive (bounded waits give up)
+OPT_POOL_KEEP = 7        # bytes of freed device memory the stream-ordered pool keeps mapped for later plans
+OPT_DISCRETISE = 8       # where batches discretise: DISCRETISE_AUTO (by cost), _HOST or _DEVICE (same bits)
+DISCRETISE_AUTO = 0
+DISCRETISE_HOST = 1
+DISCRETISE_DEVICE = 2
 
 PATH_AUTO = 0
 PATH_LEVEL = 1

@@ -66,6 +66,8 @@ struct Library {
     int log = 0;
     long long executions = 1;  // PARODE_OPT_EXECUTIONS: plans and batches
     int fault_withhold = 0;    // PARODE_OPT_FAULT_WITHHOLD (test hook)
+    long long pool_keep = 0;   // PARODE_OPT_POOL_KEEP: last value set (the driver's default pool keeps 0)
+    int discretise = 0;        // PARODE_OPT_DISCRETISE (batches and servers)
     std::vector<int> tune_inputs;  // sinusoid inputs of the tuner's synthetic systems, by input count
     cudaEvent_t t_start = nullptr, t_stop = nullptr;
     bool timer_running = false;
@@ -435,6 +437,31 @@ void ParODE_SetOption(int option, long long value, int nErr[])
         else g_fault_alloc.store(value);
         break;
     case PARODE_OPT_FAULT_WITHHOLD: L.fault_withhold = value != 0; break;
+    case PARODE_OPT_POOL_KEEP:
+        if (value < 0) {
+            rc = kInvalidArgument;
+        } else if (L.state != kFull || L.selected.empty()) {
+            rc = kNotInitialized;
+        } else {
+            // the release threshold of each selected device's stream-ordered
+            // pool, from which plans and batches take their device memory
+            uint64_t keep = (uint64_t)value;
+            for (int d : L.selected) {
+                cudaMemPool_t pool = nullptr;
+                if (cudaDeviceGetDefaultMemPool(&pool, d) != cudaSuccess ||
+                    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) {
+                    cudaGetLastError();
+                    rc = kDeviceError;
+                }
+            }
+            if (rc == kOK) L.pool_keep = value;
+        }
+        break;
+    case PARODE_OPT_DISCRETISE:
+        if (value != PARODE_DISCRETISE_AUTO && value != PARODE_DISCRETISE_HOST && value != PARODE_DISCRETISE_DEVICE)
+            rc = kInvalidArgument;
+        else L.discretise = (int)value;
+        break;
     default: rc = kInvalidArgument;
     }
     if (nErr) nErr[0] = rc;
@@ -452,6 +479,8 @@ long long ParODE_GetOption(int option, int nErr[])
     case PARODE_OPT_EXECUTIONS: return L.executions;
     case PARODE_OPT_FAULT_ALLOC: return g_fault_alloc.load();
     case PARODE_OPT_FAULT_WITHHOLD: return L.fault_withhold;
+    case PARODE_OPT_POOL_KEEP: return L.pool_keep;
+    case PARODE_OPT_DISCRETISE: return L.discretise;
     default:
         if (nErr) nErr[0] = kInvalidArgument;
         return -1;
@@ -706,6 +735,7 @@ ParODE_Batch* ParODE_BatchCreate(int nSystems, const double* const A[], const do
         opt.input_double = true;
         opt.log = L.log != 0;
         opt.executions = (double)L.executions;
+        opt.discretise = L.discretise;
         auto h = std::make_unique<ParODE_Batch>();
         h->batch = std::make_unique<BatchPlan>(dev, std::move(specs), &L.inputs, opt);
         out = h.release();
@@ -796,6 +826,7 @@ ParODE_Server* ParODE_ServerCreate(int precision, double hbmBudgetBytes, int max
         if (maxBatch > 0) o.max_batch = maxBatch;
         if (maxInflight > 0) o.max_inflight = maxInflight;
         o.log = L.log;
+        o.discretise = L.discretise;
         auto h = std::make_unique<ParODE_Server>();
         h->server = std::make_unique<Server>(dev, &L.inputs, &L.mu, o);
         out = h.release();

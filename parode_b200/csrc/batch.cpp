@@ -46,6 +46,12 @@ double sinusoid_host(const InputEntry* e, int i, double t)
     return v;
 }
 
+// A batch discretises on the host threads when no system takes more than
+// kHostDiscMaxSystem multiply-adds (RK4 n <= 69, ABM n <= 100: about a
+// millisecond on one core) and the batch no more than kHostDiscMaxBatch.
+constexpr double kHostDiscMaxSystem = 1e6;
+constexpr double kHostDiscMaxBatch = 8e6;
+
 template <class F>
 void parallel_for(int n, F&& f)
 {
@@ -66,18 +72,50 @@ void parallel_for(int n, F&& f)
         if (e) std::rethrow_exception(e);
 }
 
+// The discretisation of one system on the host, as the device kernel writes
+// it (kernels_disc.cu): the compact Phi, Bbar zero-filled to n x W max(m, 1),
+// its transpose when asked, and ||Phi - R||_inf over the stored rows (each
+// row summed in order), every operation in the kernel's order.
+double discretise_host(int solver, int n, int Ns, int W, double h, const SystemDesc& s, double* phi, double* bbar,
+                       double* bbarT)
+{
+    const int mB = s.zeroB ? 0 : s.m, Wm = W * mB;
+    std::fill(bbar, bbar + (size_t)n * W * std::max(mB, 1), 0.0);
+    if (solver == kRK4) discretise_rk4(n, mB, s.A.data(), mB ? s.B.data() : nullptr, h, phi, bbar);
+    else discretise_abm_last(n, mB, s.A.data(), mB ? s.B.data() : nullptr, h, phi, bbar);
+    if (bbarT) {
+        std::fill(bbarT, bbarT + (size_t)std::max(Wm, 1) * n, 0.0);
+        for (int r = 0; r < n; ++r)
+            for (int c = 0; c < Wm; ++c) bbarT[(size_t)c * n + r] = bbar[(size_t)r * Wm + c];
+    }
+    const int d0 = solver == kRK4 ? 0 : 3 * n;
+    double dmax = 0.0;
+    for (int r = 0; r < n; ++r) {
+        double sum = 0.0;
+        for (int c = 0; c < Ns; ++c) sum += std::fabs(phi[(size_t)r * Ns + c] + -(c == d0 + r ? 1.0 : 0.0));
+        dmax = std::max(dmax, sum);
+    }
+    return dmax;
+}
+
 }  // namespace
 
-// Pinned host blocks for the batches' staged uploads (discretisation inputs,
-// constants, job tables), kept for the next batch: from pinned memory the
-// uploads are plain DMA and the staging writes meet no first-touch page
-// faults.  Blocks are powers of two from 1 MiB; a failed pinning falls back to
-// pageable memory.
+// Pinned host blocks for the batches' staged uploads (discretisation
+// results or inputs, constants, job tables, response-table arguments), kept
+// for the next batch.  From pinned memory an upload is an asynchronous DMA;
+// from pageable memory the runtime first waits for the stream's earlier work,
+// which would hold a batch's set-up behind its own (and, in a server, other
+// batches') kernels.  Blocks come in power-of-two classes from 64 KiB and go
+// back to their class; pinning new memory is slow (and serialises the
+// driver), so a server pins a few blocks of the small classes when it starts.
+// A failed pinning falls back to pageable memory.
 namespace {
+
+constexpr int kStageMinLog = 16;
 
 struct PinnedBlocks {
     std::mutex mu;
-    std::multimap<size_t, char*> free;
+    std::vector<std::vector<char*>> free = std::vector<std::vector<char*>>(48);
 };
 
 PinnedBlocks& pinned_blocks()
@@ -86,34 +124,38 @@ PinnedBlocks& pinned_blocks()
     return *p;
 }
 
+int stage_class(size_t bytes)
+{
+    int c = kStageMinLog;
+    while (((size_t)1 << c) < bytes) ++c;
+    return c;
+}
+
 }  // namespace
 
 HostStage::HostStage(size_t bytes)
 {
-    bytes = std::max<size_t>(bytes, 1);
+    const int c = stage_class(std::max<size_t>(bytes, 1));
     {
         PinnedBlocks& b = pinned_blocks();
         std::lock_guard<std::mutex> g(b.mu);
-        auto it = b.free.lower_bound(bytes);
-        if (it != b.free.end() && it->first <= 4 * bytes) {
-            cap_ = it->first;
-            p_ = it->second;
-            b.free.erase(it);
+        if (!b.free[c].empty()) {
+            p_ = b.free[c].back();
+            b.free[c].pop_back();
+            cap_ = (size_t)1 << c;
             pinned_ = true;
             return;
         }
     }
-    size_t cap = (size_t)1 << 20;
-    while (cap < bytes) cap <<= 1;
     void* q = nullptr;
-    if (cudaHostAlloc(&q, cap, cudaHostAllocPortable) == cudaSuccess) {
+    if (cudaHostAlloc(&q, (size_t)1 << c, cudaHostAllocPortable) == cudaSuccess) {
         p_ = static_cast<char*>(q);
-        cap_ = cap;
+        cap_ = (size_t)1 << c;
         pinned_ = true;
         return;
     }
     cudaGetLastError();
-    owned_.reset(new char[bytes]);
+    owned_.reset(new char[std::max<size_t>(bytes, 1)]);
     p_ = owned_.get();
     cap_ = bytes;
 }
@@ -123,11 +165,44 @@ HostStage::~HostStage()
     if (!pinned_ || !p_) return;
     PinnedBlocks& b = pinned_blocks();
     std::lock_guard<std::mutex> g(b.mu);
-    b.free.emplace(cap_, p_);
+    b.free[stage_class(cap_)].push_back(p_);
+}
+
+void HostStage::prewarm(int blocks, int max_log2)
+{
+    for (int c = kStageMinLog; c <= max_log2; ++c) {
+        int have = 0;
+        {
+            PinnedBlocks& b = pinned_blocks();
+            std::lock_guard<std::mutex> g(b.mu);
+            have = (int)b.free[c].size();
+        }
+        for (int k = have; k < blocks; ++k) {
+            void* q = nullptr;
+            if (cudaHostAlloc(&q, (size_t)1 << c, cudaHostAllocPortable) != cudaSuccess) {
+                cudaGetLastError();
+                return;
+            }
+            PinnedBlocks& b = pinned_blocks();
+            std::lock_guard<std::mutex> g(b.mu);
+            b.free[c].push_back(static_cast<char*>(q));
+        }
+    }
 }
 
 BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* inputs, const PlanOptions& opt)
     : device_(device), inputs_(inputs), opt_(opt)
+{
+    // a failed set-up gives back what it took (no destructor runs for it)
+    try {
+        build(std::move(specs), inputs, opt);
+    } catch (...) {
+        release();
+        throw;
+    }
+}
+
+void BatchPlan::build(std::vector<BatchSpec> specs, InputRegistry* inputs, const PlanOptions& opt)
 {
     if (specs.empty()) throw Error(kInvalidArgument, "empty batch");
     if (specs.size() > 65535) throw Error(kInvalidArgument, "at most 65535 systems per batch");
@@ -279,19 +354,77 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
     }
 
     phase("classify", false);
-    // ---- discretisation on the device (kernels_disc.cu): A and B go up,
-    // the compact Phi (RK4: n x n; ABM: its last block row, n x 4n, the rows
-    // above being the exact shift; expanded into the padded power table's
-    // level 0 later), Bbar (and its transpose for the level-synchronous
-    // systems) stay in the batch's discretisation buffer, and each system's
-    // distance ||Phi - R|| comes back (it sizes the tensor-core levels of the
-    // layout below).  The same bits as the host restatement.
+    // ---- discretisation: the compact Phi (RK4: n x n; ABM: its last block
+    // row, n x 4n, the rows above being the exact shift; expanded into the
+    // padded power table's level 0 later), Bbar (and its transpose for the
+    // level-synchronous systems) into the batch's discretisation buffer, and
+    // each system's distance ||Phi - R|| (it sizes the tensor-core levels of
+    // the layout below).  Host and device take every operation in the same
+    // order (host_math.cpp, kernels_disc.cu): the same bits either way.  A
+    // batch of small systems runs it on the host threads, with no device round
+    // trip (a server sets batches up while others run); a large one on the
+    // device.
     PARODE_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     struct DiscOff {
         size_t A, B, phi, bbar, bbarT, work;
     };
     std::vector<DiscOff> doff(N);
-    {
+    double disc_total = 0.0, disc_max = 0.0;  // multiply-adds of the discretisation GEMMs
+    for (int i = 0; i < N; ++i) {
+        const Sys& q = sys_[i];
+        const double n = q.n, mB = specs[i].sys.zeroB ? 0 : q.m;
+        const double c = q.solver == kRK4 ? 3.0 * n * n * (n + mB) : n * n * (n + mB);
+        disc_total += c;
+        disc_max = std::max(disc_max, c);
+    }
+    const bool disc_host = opt.discretise == kDiscHost || (opt.discretise == kDiscAuto &&
+                                                            disc_max <= kHostDiscMaxSystem &&
+                                                            disc_total <= kHostDiscMaxBatch);
+    if (disc_host) {
+        Layout D;
+        for (int i = 0; i < N; ++i) {
+            const Sys& q = sys_[i];
+            const int mB = specs[i].sys.zeroB ? 0 : q.m;
+            doff[i].phi = D.take(sizeof(double) * (size_t)q.n * q.Ns);
+            doff[i].bbar = D.take(sizeof(double) * (size_t)q.n * q.W * std::max(mB, 1));
+            doff[i].bbarT = (!q.blocked && !q.resp) ? D.take(sizeof(double) * (size_t)std::max(q.W * mB, 1) * q.n) : 0;
+        }
+        if (fault_alloc_now()) throw Error(kNotEnoughResources, "batch discretisation buffer (injected)");
+        cudaError_t e = cudaMallocAsync(&disc_, std::max<size_t>(D.bytes, 8), stream_);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            disc_ = nullptr;
+            throw Error(kNotEnoughResources, "batch discretisation buffer allocation failed");
+        }
+        host_disc_ = std::make_unique<HostStage>(D.bytes);  // kept with the plan: the copy is asynchronous
+        char* hd = host_disc_->data();
+        parallel_for(N, [&](int i) {
+            const Sys& q = sys_[i];
+            sys_[i].delta = discretise_host(q.solver, q.n, q.Ns, q.W, q.h, specs[i].sys,
+                                            reinterpret_cast<double*>(hd + doff[i].phi),
+                                            reinterpret_cast<double*>(hd + doff[i].bbar),
+                                            doff[i].bbarT ? reinterpret_cast<double*>(hd + doff[i].bbarT) : nullptr);
+        });
+        PARODE_CUDA(cudaMemcpyAsync(disc_, hd, D.bytes, cudaMemcpyHostToDevice, stream_));
+    } else {
+        // A and B go up, the kernel fills the buffer and the distances come
+        // back.  The set-up waits for it, so it runs on a stream of the
+        // greatest priority: a batch set up while others execute is not
+        // queued behind their kernels.
+        cudaStream_t dstream = nullptr;
+        {
+            int least = 0, greatest = 0;
+            PARODE_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+            PARODE_CUDA(cudaStreamCreateWithPriority(&dstream, cudaStreamNonBlocking, greatest));
+        }
+        struct StreamGuard {
+            cudaStream_t s;
+            ~StreamGuard()
+            {
+                cudaStreamSynchronize(s);
+                cudaStreamDestroy(s);
+            }
+        } dguard{dstream};
         Layout D;
         for (int i = 0; i < N; ++i) {  // staged inputs first
             const SystemDesc& s = specs[i].sys;
@@ -300,6 +433,16 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             doff[i].B = mB ? D.take(sizeof(double) * (size_t)sys_[i].n * mB) : 0;
         }
         const size_t jobs_at = D.take(sizeof(DiscJob) * (size_t)N);
+        // the product tiles of the three stages (32 x 32 outputs each)
+        long ntiles[3] = {0, 0, 0};
+        for (int i = 0; i < N; ++i) {
+            const Sys& q = sys_[i];
+            const int mB = specs[i].sys.zeroB ? 0 : q.m;
+            const long tn = (q.n + 31) / 32, tm = mB > 0 ? (mB + 31) / 32 : 0;
+            for (int st = 0; st < (q.solver == kRK4 ? 3 : 1); ++st) ntiles[st] += tn * tn + tn * tm;
+        }
+        size_t tiles_at[3];
+        for (int st = 0; st < 3; ++st) tiles_at[st] = D.take(sizeof(DiscTile) * (size_t)std::max<long>(ntiles[st], 1));
         const size_t staged = D.bytes;
         const size_t delta_at = D.take(sizeof(double) * (size_t)N);
         for (int i = 0; i < N; ++i) {
@@ -312,7 +455,7 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             doff[i].work = D.take(sizeof(double) * (size_t)discretise_work_doubles(q.n, mB));
         }
         if (fault_alloc_now()) throw Error(kNotEnoughResources, "batch discretisation buffer (injected)");
-        cudaError_t e = cudaMallocAsync(&disc_, std::max<size_t>(D.bytes, 8), stream_);
+        cudaError_t e = cudaMallocAsync(&disc_, std::max<size_t>(D.bytes, 8), dstream);
         if (e != cudaSuccess) {
             cudaGetLastError();
             disc_ = nullptr;
@@ -342,15 +485,24 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
             j.h = q.h;
         });
         std::memcpy(hs_data + jobs_at, jobs.data(), sizeof(DiscJob) * (size_t)N);
-        PARODE_CUDA(cudaMemcpyAsync(db, hs_data, staged, cudaMemcpyHostToDevice, stream_));
-        launch_discretise_batch(reinterpret_cast<const DiscJob*>(db + jobs_at), N, stream_);
+        const DiscTile* dtiles[3];
+        for (int st = 0; st < 3; ++st) {
+            std::vector<DiscTile> tl;
+            tl.reserve((size_t)ntiles[st]);
+            for (int i = 0; i < N; ++i) discretise_tiles(jobs[i], st, tl);
+            if ((long)tl.size() != ntiles[st]) throw Error(kDeviceError, "discretisation tiles: count mismatch");
+            std::memcpy(hs_data + tiles_at[st], tl.data(), sizeof(DiscTile) * tl.size());
+            dtiles[st] = reinterpret_cast<const DiscTile*>(db + tiles_at[st]);
+        }
+        PARODE_CUDA(cudaMemcpyAsync(db, hs_data, staged, cudaMemcpyHostToDevice, dstream));
+        launch_discretise_batch(reinterpret_cast<const DiscJob*>(db + jobs_at), N, dtiles, ntiles, sms_, dstream);
         std::vector<double> deltas((size_t)N);
         PARODE_CUDA(cudaMemcpyAsync(deltas.data(), db + delta_at, sizeof(double) * (size_t)N, cudaMemcpyDeviceToHost,
-                                    stream_));
-        PARODE_CUDA(cudaStreamSynchronize(stream_));
+                                    dstream));
+        PARODE_CUDA(cudaStreamSynchronize(dstream));
         for (int i = 0; i < N; ++i) sys_[i].delta = deltas[(size_t)i];
-    }
-    phase("discretise (device)", false);
+        }
+    phase(disc_host ? "discretise (host)" : "discretise (device)", false);
     // ---- constant region: layout first, then the host set-up (threads over
     // systems) writes straight into its staged slots
     Layout L;
@@ -444,10 +596,9 @@ BatchPlan::BatchPlan(int device, std::vector<BatchSpec> specs, InputRegistry* in
         if (q.mu > 0 && q.input->kind != InputEntry::kSinusoid) {
             double* dU9 = nullptr;
             PARODE_CUDA(cudaMalloc(&dU9, sizeof(double) * 9 * q.mu));
+            std::unique_ptr<double, decltype(&cudaFree)> keep(dU9, &cudaFree);
             inputs_->fill(q.input, device_, dU9, q.mu, q.t0, 0.5 * q.h, 9, opt_.input_double, nullptr);
-            cudaError_t e = cudaMemcpy(U9.data(), dU9, sizeof(double) * 9 * q.mu, cudaMemcpyDeviceToHost);
-            cudaFree(dU9);
-            PARODE_CUDA(e);
+            PARODE_CUDA(cudaMemcpy(U9.data(), dU9, sizeof(double) * 9 * q.mu, cudaMemcpyDeviceToHost));
         }
     }
     parallel_for(N, [&](int i) {
@@ -1255,6 +1406,11 @@ void BatchPlan::build_responses()
         const size_t meta = align_up(sizeof(ResponseArgs) * nent) + 2 * align_up(sizeof(long) * nent) +
                             (size_t)(maxR + 1) * (align_up(2 * sizeof(LevelArgs) * nent) + align_up(2 * sizeof(long) * nent));
         PARODE_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&buf), ws + meta, stream_));
+        struct Workspace {  // freed after the stream's uses, also when a step below fails
+            char* p;
+            cudaStream_t s;
+            ~Workspace() { cudaFreeAsync(p, s); }
+        } wsguard{buf, stream_};
         for (ResponseArgs& a : ra) {
             const size_t off = reinterpret_cast<size_t>(a.CPt);
             response_workspace_carve(a, reinterpret_cast<double*>(buf + off));
@@ -1267,12 +1423,13 @@ void BatchPlan::build_responses()
             ictas += response_init_ctas(ra[e]);
             fctas += response_fill_ctas(ra[e]);
         }
-        // host image of the meta region
-        std::vector<char> img(meta, 0);
+        // host image of the meta region (pinned: the copy does not wait for
+        // the power tables launched before it); gaps are copied, never read
+        auto img = std::make_unique<HostStage>(meta);
         size_t at = 0;
         auto put = [&](const void* src, size_t n) {
             const size_t o = at;
-            std::memcpy(img.data() + o, src, n);
+            std::memcpy(img->data() + o, src, n);
             at = align_up(at + std::max<size_t>(n, 1));
             return buf + ws + o;
         };
@@ -1313,33 +1470,48 @@ void BatchPlan::build_responses()
             st.start = reinterpret_cast<const long*>(put(start.data(), sizeof(long) * start.size()));
             steps.push_back(st);
         }
-        PARODE_CUDA(cudaMemcpyAsync(buf + ws, img.data(), meta, cudaMemcpyHostToDevice, stream_));
+        PARODE_CUDA(cudaMemcpyAsync(buf + ws, img->data(), meta, cudaMemcpyHostToDevice, stream_));
         launch_response_init(dArgs, dIs, nent, ictas, stream_);
         for (const Step& st : steps)
             launch_affine_level_grouped(st.cfg, st.args, st.start, st.nent, st.tiles, st.cfg.smem, stream_);
         launch_response_fill(dArgs, dFs, nent, fctas, stream_);
-        PARODE_CUDA(cudaFreeAsync(buf, stream_));
         host_keep_.push_back(std::move(img));  // the copy may read it until it runs
     }
 }
 
-BatchPlan::~BatchPlan()
+BatchPlan::~BatchPlan() { release(); }
+
+void BatchPlan::release()
 {
     cudaSetDevice(device_);
     if (last_stream_ && last_stream_ != stream_) cudaStreamSynchronize(last_stream_);
     if (stream_) cudaStreamSynchronize(stream_);
+    last_stream_ = nullptr;
     if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
-    if (disc_) cudaFreeAsync(disc_, stream_ ? stream_ : cudaStreamPerThread);
-    for (auto f : forks_)
+    graph_exec_ = nullptr;
+    cudaStream_t fs = stream_ ? stream_ : cudaStreamPerThread;
+    if (disc_) cudaFreeAsync(disc_, fs);
+    disc_ = nullptr;
+    for (auto& f : forks_)
         if (f) {
             cudaStreamSynchronize(f);
             cudaStreamDestroy(f);
+            f = nullptr;
         }
-    for (auto e : events_)
-        if (e) cudaEventDestroy(e);
+    for (auto& e : events_)
+        if (e) {
+            cudaEventDestroy(e);
+            e = nullptr;
+        }
     if (ready_) cudaEventDestroy(ready_);
-    if (arena_) cudaFreeAsync(arena_, stream_ ? stream_ : cudaStreamPerThread);
-    if (stream_) cudaStreamDestroy(stream_);
+    ready_ = nullptr;
+    if (arena_) cudaFreeAsync(arena_, fs);
+    arena_ = nullptr;
+    if (stream_) {
+        cudaStreamSynchronize(stream_);
+        cudaStreamDestroy(stream_);
+    }
+    stream_ = nullptr;
 }
 
 double BatchPlan::state_steps() const

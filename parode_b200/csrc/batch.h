@@ -46,6 +46,9 @@ class HostStage {
 public:
     explicit HostStage(size_t bytes);
     ~HostStage();
+    // pins `blocks` free blocks of every class up to 2^max_log2 bytes ahead
+    // of use (a server's start)
+    static void prewarm(int blocks, int max_log2);
     HostStage(const HostStage&) = delete;
     HostStage& operator=(const HostStage&) = delete;
     char* data() { return p_; }
@@ -147,6 +150,8 @@ private:
     };
 
     void launch_grouped(const GroupedLaunch& g, cudaStream_t s);
+    void build(std::vector<BatchSpec> specs, InputRegistry* inputs, const PlanOptions& opt);
+    void release();  // idempotent: what the plan holds on the device goes back
     void build_responses();
 
     int device_ = 0;
@@ -167,7 +172,8 @@ private:
     cudaEvent_t ready_ = nullptr;
     // host images of the set-up copies, kept until the plan is destroyed so
     // that the constructor returns without waiting for the device
-    std::vector<std::vector<char>> host_keep_;
+    std::vector<std::unique_ptr<HostStage>> host_keep_;
+    std::unique_ptr<HostStage> host_disc_;   // the host discretisation's results (small batches)
     std::unique_ptr<HostStage> host_stage_;  // the staged constant region
     std::unique_ptr<HostStage> host_jobs_;   // the staged job arrays
     InputRegistry* inputs_ = nullptr;

@@ -204,7 +204,9 @@ void launch_split_planes(const double* U, float* hi, float* lo, long n, cudaStre
 // n x n; ABM the last block row, n x 4n), Bbar (n x W max(m, 1), W = 3 / 5)
 // and, when bbarT is set, its transpose out, with ||Phi - R||_inf into
 // *delta; work: discretise_work_doubles(n, m) doubles.  The same bits as the
-// host restatement (host_math.cpp).
+// host restatement (host_math.cpp).  The products run first, as 32 x 32
+// output tiles in three dependency stages (discretise_tiles lists a job's
+// tiles of one stage, with the job's device pointers).
 struct DiscJob {
     const double* A = nullptr;
     const double* B = nullptr;
@@ -216,8 +218,17 @@ struct DiscJob {
     int n = 0, m = 0, solver = 0;
     double h = 0.0;
 };
+struct DiscTile {
+    const double* X = nullptr;
+    const double* Y = nullptr;
+    double* Z = nullptr;
+    int r = 0, k = 0, c = 0, i0 = 0, j0 = 0;
+};
 long discretise_work_doubles(int n, int m);
-void launch_discretise_batch(const DiscJob* jobs, int njobs, cudaStream_t s);
+void discretise_tiles(const DiscJob& j, int stage, std::vector<DiscTile>& out);
+// tiles[st] / ntiles[st]: device arrays of the stages' tiles
+void launch_discretise_batch(const DiscJob* jobs, int njobs, const DiscTile* const tiles[3], const long ntiles[3],
+                             int sms, cudaStream_t s);
 
 // Scan-vector initialisation with the forcing term Gamma_k (zero padding
 // for k >= T and for the components the solver leaves empty).

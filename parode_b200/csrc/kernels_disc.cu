@@ -4,12 +4,17 @@
 // and ||Phi - R||_inf over the stored rows (R the exact 0/1 part: I for RK4,
 // the companion shift for ABM).
 //
-// One CTA per system.  Every product and sum is taken in the order of the
-// host restatement (host_math.cpp: discretise_rk4, discretise_abm_last; its
-// GEMM accumulates each element over the inner index in order, built without
-// FMA contraction): explicit __dmul_rn / __dadd_rn keep the device from
-// contracting, so the device gives the host's bits and the batch's layout
-// (which the distance to R sizes) is the same either way.
+// The matrix products (A^2, A^3, A^4 and A B, A^2 B, A^3 B; ABM needs A^2 and
+// A B) run as grouped GEMMs over 32 x 32 output tiles of every system, one
+// launch per dependency stage, so a large system spreads over many SMs; one
+// CTA per system then forms Phi, Bbar, the transpose and the distance.  Every
+// product and sum is taken in the order of the host restatement (host_math.cpp:
+// discretise_rk4, discretise_abm_last; its GEMM accumulates each element over
+// the inner index in order, built without FMA contraction): explicit
+// __dmul_rn / __dadd_rn keep the device from contracting, and a tile's sum
+// runs over the inner index in order from zero, so the device gives the host's
+// bits and the batch's layout (which the distance to R sizes) is the same
+// either way.
 #include "common.h"
 #include "kernels.h"
 
@@ -19,45 +24,80 @@ namespace parode {
 
 namespace {
 
-constexpr int kThreads = 256;
-
-// Z (r x c) = X (r x k) Y (k x c), row-major, every element summed over the
-// inner index in order; the CTA's threads split the elements.
-__device__ void gemm_cta(int r, int k, int c, const double* __restrict__ X, const double* __restrict__ Y,
-                         double* __restrict__ Z)
-{
-    for (int e = threadIdx.x; e < r * c; e += kThreads) {
-        const int i = e / c, j = e - i * c;
-        double s = 0.0;
-        for (int q = 0; q < k; ++q) s = __dadd_rn(s, __dmul_rn(X[(long)i * k + q], Y[(long)q * c + j]));
-        Z[e] = s;
-    }
-    __syncthreads();
-}
+constexpr int kThreads = 128;
+constexpr int kTile = 32;       // output tile edge and inner-index chunk
+constexpr int kPitch = kTile + 1;
 
 __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
 
-__global__ void __launch_bounds__(kThreads) k_discretise_batch(const DiscJob* __restrict__ jobs)
+// Grouped tile GEMM: thread (ty, tx) owns rows ty + 16 v (v < 2) and columns
+// tx + 8 u (u < 4) of its tile, eight independent in-order sums.
+__global__ void __launch_bounds__(kThreads) k_disc_gemm(const DiscTile* __restrict__ tiles, long ntiles)
+{
+    __shared__ double Xs[kTile * kPitch];  // [row][inner]
+    __shared__ double Ys[kTile * kPitch];  // [inner][col]
+    const int tx = threadIdx.x & 7, ty = threadIdx.x >> 3;
+    for (long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const DiscTile tl = tiles[t];
+        double s[2][4];
+#pragma unroll
+        for (int v = 0; v < 2; ++v)
+#pragma unroll
+            for (int u = 0; u < 4; ++u) s[v][u] = 0.0;
+        for (int kc = 0; kc < tl.k; kc += kTile) {
+            const int kn = min(kTile, tl.k - kc);
+            for (int e = threadIdx.x; e < kTile * kTile; e += kThreads) {
+                const int a = e >> 5, b = e & 31;
+                const int xi = tl.i0 + a, yj = tl.j0 + b;
+                Xs[a * kPitch + b] = (xi < tl.r && b < kn) ? tl.X[(long)xi * tl.k + kc + b] : 0.0;
+                Ys[a * kPitch + b] = (a < kn && yj < tl.c) ? tl.Y[(long)(kc + a) * tl.c + yj] : 0.0;
+            }
+            __syncthreads();
+            // only the chunk's real inner indices: no padded products join a sum
+            for (int q = 0; q < kn; ++q) {
+                double x[2], y[4];
+#pragma unroll
+                for (int v = 0; v < 2; ++v) x[v] = Xs[(ty + 16 * v) * kPitch + q];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) y[u] = Ys[q * kPitch + tx + 8 * u];
+#pragma unroll
+                for (int v = 0; v < 2; ++v)
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) s[v][u] = add(s[v][u], mul(x[v], y[u]));
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int v = 0; v < 2; ++v)
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int i = tl.i0 + ty + 16 * v, j = tl.j0 + tx + 8 * u;
+                if (i < tl.r && j < tl.c) tl.Z[(long)i * tl.c + j] = s[v][u];
+            }
+    }
+}
+
+// Per system: Phi, Bbar (and its transpose) from the products, then the
+// distance to R.
+__global__ void __launch_bounds__(kThreads) k_discretise_finish(const DiscJob* __restrict__ jobs)
 {
     const DiscJob jb = jobs[blockIdx.x];
     const int n = jb.n, m = jb.m, N = jb.solver == 0 ? n : 4 * n;
     const double h = jb.h, h2 = mul(h, h);
     const double* A = jb.A;
     const double* B = jb.B;
-    double* A2 = jb.work;                  // n x n
-    double* A3 = A2 + (long)n * n;         // n x n (RK4)
-    double* A4 = A3 + (long)n * n;         // n x n (RK4)
-    double* AB = A4 + (long)n * n;         // n x m
-    double* A2B = AB + (long)n * std::max(m, 1);
-    double* A3B = A2B + (long)n * std::max(m, 1);
+    const double* A2 = jb.work;
+    const double* A3 = A2 + (long)n * n;
+    const double* A4 = A3 + (long)n * n;
+    const double* AB = A4 + (long)n * n;
+    const double* A2B = AB + (long)n * max(m, 1);
+    const double* A3B = A2B + (long)n * max(m, 1);
     const int W = jb.solver == 0 ? 3 : 5;
     // Bbar starts at zero (the slots a system without B never fills)
-    for (int e = threadIdx.x; e < n * W * std::max(m, 1); e += kThreads) jb.bbar[e] = 0.0;
-    gemm_cta(n, n, n, A, A, A2);
+    for (int e = threadIdx.x; e < n * W * max(m, 1); e += kThreads) jb.bbar[e] = 0.0;
+    __syncthreads();
     if (jb.solver == 0) {
-        gemm_cta(n, n, n, A2, A, A3);
-        gemm_cta(n, n, n, A, A3, A4);
         const double h3 = mul(mul(h, h), h), h4 = mul(mul(mul(h, h), h), h);
         const double c2 = mul(0.5, h2), c3 = mul(1.0 / 6.0, h3), c4 = mul(1.0 / 24.0, h4);
         for (int q = threadIdx.x; q < n * n; q += kThreads) {
@@ -68,9 +108,6 @@ __global__ void __launch_bounds__(kThreads) k_discretise_batch(const DiscJob* __
             jb.phi[q] = add(v, mul(c4, A4[q]));
         }
         if (m > 0) {
-            gemm_cta(n, n, m, A, B, AB);
-            gemm_cta(n, n, m, A2, B, A2B);
-            gemm_cta(n, n, m, A3, B, A3B);
             const double b1 = mul(0.5, h3), b2 = mul(0.25, h4), b3 = mul(4.0, h), b4 = mul(2.0, h2);
             const double sixth = 1.0 / 6.0, b5 = mul(sixth, h);
             for (int q = threadIdx.x; q < n * m; q += kThreads) {
@@ -96,7 +133,6 @@ __global__ void __launch_bounds__(kThreads) k_discretise_batch(const DiscJob* __
             last[3 * n + c] = add(add(r == c ? 1.0 : 0.0, mul(k28, A[q])), mul(k495, A2[q]));
         }
         if (m > 0) {
-            gemm_cta(n, n, m, A, B, AB);
             const double kb1 = h / 24.0, kb19 = 19.0 * h / 24.0, kb9 = 9.0 * h / 24.0;
             for (int q = threadIdx.x; q < n * m; q += kThreads) {
                 const int r = q / m, c = q - r * m;
@@ -113,7 +149,7 @@ __global__ void __launch_bounds__(kThreads) k_discretise_batch(const DiscJob* __
     // Bbar transposed (level-synchronous systems' coalesced forcing kernel)
     if (jb.bbarT) {
         const int Wm = W * m;
-        for (int e = threadIdx.x; e < std::max(Wm, 1) * n; e += kThreads) jb.bbarT[e] = 0.0;
+        for (int e = threadIdx.x; e < max(Wm, 1) * n; e += kThreads) jb.bbarT[e] = 0.0;
         __syncthreads();
         for (int e = threadIdx.x; e < n * Wm; e += kThreads) {
             const int r = e / Wm, c = e - r * Wm;
@@ -127,26 +163,71 @@ __global__ void __launch_bounds__(kThreads) k_discretise_batch(const DiscJob* __
     for (int r = threadIdx.x; r < n; r += kThreads) {
         double sum = 0.0;
         for (int c = 0; c < N; ++c) sum = add(sum, fabs(add(jb.phi[(long)r * N + c], -(c == d0 + r ? 1.0 : 0.0))));
-        dmax = std::max(dmax, sum);
+        dmax = fmax(dmax, sum);
     }
     rowmax[threadIdx.x] = dmax;
     __syncthreads();
     if (threadIdx.x == 0) {
         double v = 0.0;
-        for (int t = 0; t < kThreads; ++t) v = std::max(v, rowmax[t]);
+        for (int t = 0; t < kThreads; ++t) v = fmax(v, rowmax[t]);
         *jb.delta = v;
     }
+}
+
+void push_tiles(const double* X, const double* Y, double* Z, int r, int k, int c, std::vector<DiscTile>& out)
+{
+    for (int i0 = 0; i0 < r; i0 += kTile)
+        for (int j0 = 0; j0 < c; j0 += kTile) {
+            DiscTile t;
+            t.X = X;
+            t.Y = Y;
+            t.Z = Z;
+            t.r = r;
+            t.k = k;
+            t.c = c;
+            t.i0 = i0;
+            t.j0 = j0;
+            out.push_back(t);
+        }
 }
 
 }  // namespace
 
 long discretise_work_doubles(int n, int m) { return 3L * n * n + 3L * n * std::max(m, 1); }
 
-void launch_discretise_batch(const DiscJob* jobs, int njobs, cudaStream_t s)
+void discretise_tiles(const DiscJob& j, int stage, std::vector<DiscTile>& out)
 {
+    const int n = j.n, m = j.m;
+    double* A2 = j.work;
+    double* A3 = A2 + (long)n * n;
+    double* A4 = A3 + (long)n * n;
+    double* AB = A4 + (long)n * n;
+    double* A2B = AB + (long)n * std::max(m, 1);
+    double* A3B = A2B + (long)n * std::max(m, 1);
+    if (stage == 0) {
+        push_tiles(j.A, j.A, A2, n, n, n, out);
+        if (m > 0) push_tiles(j.A, j.B, AB, n, n, m, out);
+    } else if (j.solver == 0 && stage == 1) {
+        push_tiles(A2, j.A, A3, n, n, n, out);
+        if (m > 0) push_tiles(A2, j.B, A2B, n, n, m, out);
+    } else if (j.solver == 0 && stage == 2) {
+        push_tiles(j.A, A3, A4, n, n, n, out);
+        if (m > 0) push_tiles(A3, j.B, A3B, n, n, m, out);
+    }
+}
+
+void launch_discretise_batch(const DiscJob* jobs, int njobs, const DiscTile* const tiles[3], const long ntiles[3],
+                             int sms, cudaStream_t s)
+{
+    for (int st = 0; st < 3; ++st) {
+        if (ntiles[st] <= 0) continue;
+        const long grid = std::min<long>(ntiles[st], (long)std::max(sms, 1) * 8);
+        k_disc_gemm<<<(unsigned)grid, kThreads, 0, s>>>(tiles[st], ntiles[st]);
+        PARODE_CUDA(cudaGetLastError());
+    }
     for (int k = 0; k < njobs; k += 65535) {
         const int cnt = std::min(65535, njobs - k);
-        k_discretise_batch<<<(unsigned)cnt, kThreads, 0, s>>>(jobs + k);
+        k_discretise_finish<<<(unsigned)cnt, kThreads, 0, s>>>(jobs + k);
         PARODE_CUDA(cudaGetLastError());
     }
 }

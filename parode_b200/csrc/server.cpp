@@ -94,6 +94,9 @@ Server::Server(int device, InputRegistry* inputs, std::recursive_mutex* inputs_m
             cudaStreamDestroy(st);
         }
     }
+    // pinned staging blocks for the batches' uploads (64 KiB .. 4 MiB, eight
+    // of each), so that small batches do not pin memory on the request path
+    HostStage::prewarm(8, 22);
     for (int k = 0; k < std::max(1, opt_.setup_threads); ++k) workers_.emplace_back([this] { worker(); });
     PARODE_CUDA(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
     for (int k = 0; k < 2; ++k) retirers_.emplace_back([this] { retirer(); });
@@ -299,6 +302,7 @@ void Server::worker()
             po.precision = opt_.precision;
             po.input_double = true;
             po.log = opt_.log >= 2;
+            po.discretise = opt_.discretise;
             if (resolved) {
                 f.plan = std::make_unique<BatchPlan>(device_, std::move(specs), inputs_, po);
             } else {

@@ -36,6 +36,7 @@ struct ServerOptions {
     int max_inflight = 8;       // batches on the device (or being set up) at once
     int setup_threads = 4;      // host threads building batches concurrently
     int log = 0;                // 1: each batch's timeline on stderr; 2: also its set-up phases (which wait on the device)
+    int discretise = 0;         // where batches discretise (PlanOptions::discretise)
     // device memory mapped into the stream-ordered pool at creation (at most
     // the budget and half the free memory)
     size_t prewarm_bytes = (size_t)32 << 30;

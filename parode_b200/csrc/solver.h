@@ -53,7 +53,13 @@ struct PlanOptions {
     // time partition of the solve across devices (setup_shard): this plan is
     // shard `shard` of `shards` (shards > 1)
     int shard = 0, shards = 1;
+    // where a batch discretises its systems (DiscretiseAt)
+    int discretise = 0;
 };
+
+// Batch discretisation: by its cost (small batches on the host threads,
+// large ones on the device), or forced to one side.  Both give the same bits.
+enum DiscretiseAt { kDiscAuto = 0, kDiscHost = 1, kDiscDevice = 2 };
 
 class Plan {
 public:

@@ -98,6 +98,29 @@ def test_fault_injection_options_round_trip():
     pb.set_option(pb.OPT_FAULT_WITHHOLD, 0)
 
 
+def test_pool_keep_option():
+    """A negative byte count is refused; the value reads back as last set."""
+    import parode_b200 as pb
+
+    keep = pb.get_option(pb.OPT_POOL_KEEP)
+    assert keep >= 0
+    with pytest.raises(pb.ParODEError):
+        pb.set_option(pb.OPT_POOL_KEEP, -1)
+    assert pb.get_option(pb.OPT_POOL_KEEP) == keep
+
+
+def test_discretise_option_round_trip():
+    import parode_b200 as pb
+
+    assert pb.get_option(pb.OPT_DISCRETISE) == pb.DISCRETISE_AUTO
+    pb.set_option(pb.OPT_DISCRETISE, pb.DISCRETISE_HOST)
+    assert pb.get_option(pb.OPT_DISCRETISE) == pb.DISCRETISE_HOST
+    with pytest.raises(pb.ParODEError):
+        pb.set_option(pb.OPT_DISCRETISE, 3)
+    assert pb.get_option(pb.OPT_DISCRETISE) == pb.DISCRETISE_HOST
+    pb.set_option(pb.OPT_DISCRETISE, pb.DISCRETISE_AUTO)
+
+
 def test_tuning_file_round_trip(tmp_path):
     """Entries of one GPU survive save and load; other GPUs' lines are skipped."""
     import parode_b200 as pb

@@ -177,3 +177,46 @@ def test_batch_rejects_bad_system(pb):
     bad["solver"] = 7
     with pytest.raises(pb.ParODEError):
         pb.Batch([_spec(pb, c), bad])
+
+
+def test_pool_keep_reuses_memory_bit_for_bit(pb):
+    """With the stream-ordered pool keeping freed memory, a batch set up again
+    on the memory of the first gives the same outputs bit for bit."""
+    cases = _mix_cases()
+    specs = [_spec(pb, c, B, Cm, D) for c, B, Cm, D in cases]
+    pb.set_option(pb.OPT_POOL_KEEP, 1 << 30)
+    try:
+        assert pb.get_option(pb.OPT_POOL_KEEP) == 1 << 30
+        outs = []
+        for _ in range(2):
+            b = pb.Batch(specs, precision=pb.MIXED)
+            b.execute()
+            outs.append([b.output(i)[1] for i in range(len(cases))])
+            b.close()
+    finally:
+        pb.set_option(pb.OPT_POOL_KEEP, 0)
+    for i in range(len(cases)):
+        assert np.array_equal(outs[0][i], outs[1][i]), i
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_host_and_device_discretisation_agree_bit_for_bit(pb, precision):
+    """The batch's discretisation on the host threads and on the device take
+    every operation in the same order: Phi, Bbar, their distance to the exact
+    part (which sizes the mixed form's levels) and so every output agree bit
+    for bit, over RK4 and ABM, blocked, response and level-synchronous
+    systems and absent matrices."""
+    cases = _mix_cases()
+    specs = [_spec(pb, c, B, Cm, D) for c, B, Cm, D in cases]
+    outs = {}
+    try:
+        for where in (pb.DISCRETISE_HOST, pb.DISCRETISE_DEVICE):
+            pb.set_option(pb.OPT_DISCRETISE, where)
+            b = pb.Batch(specs, precision=precision)
+            b.execute()
+            outs[where] = [b.output(i)[1] for i in range(len(cases))]
+            b.close()
+    finally:
+        pb.set_option(pb.OPT_DISCRETISE, pb.DISCRETISE_AUTO)
+    for i in range(len(cases)):
+        assert np.array_equal(outs[pb.DISCRETISE_HOST][i], outs[pb.DISCRETISE_DEVICE][i]), i
