@@ -3,8 +3,38 @@
 
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <utility>
+
+#include "common.h"
 
 namespace parode {
+
+// Programmatic dependent launch (a kernel launched by launch_dependent may
+// start while the kernel before it in the stream finishes): grid_dep_wait()
+// returns once the grids it depends on have completed and their memory is
+// visible (at once for a kernel launched the ordinary way); every read of
+// their results, and every write, comes after it.  grid_dep_trigger() lets
+// the dependent grid's CTAs be scheduled once every CTA of this grid has
+// called it (or exited), so the dependents' own prologue (loads of data no
+// kernel in flight writes) overlaps this grid's work.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
+template <typename... K, typename... A>
+void launch_dependent(void (*kernel)(K...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, A&&... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    PARODE_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...));
+}
 
 // D(8x8) += A(8x4, row) * B(4x8, col), FP64 tensor-core MMA.
 // Fragments (PTX ISA, mma.m8n8k4 .f64): lane = 4*g + t with g = lane>>2,

@@ -156,13 +156,16 @@ int response_log2_block(int solver, int NP, int n, int m, int p, long nScan, dou
 // Exclusive scan of block aggregates for NP <= 64 (a multiple of 8),
 // kernels_carry.cu: items[b] <- X_b with X_0 = X0, X_{b+1} = Q X_b + items[b],
 // Q = P_{l0} (P: power table, level l at l NP^2).  Chunks of 16 per level;
-// level h uses P_{l0 + 4h}, so the table must reach level
-// l0 + 4 chunk_carry_levels(count).  work: chunk_carry_scratch(count) NP
-// doubles.  Returns the launches made.
+// level h uses P_{l0 + 4h} .. P_{l0 + 4h + 3}, so the table must hold
+// l0 + chunk_carry_table_levels(count) levels.  h0: the global index of the
+// call's first chunk level (0 for a whole scan; a time-partitioned solve's top
+// scan starts higher), which picks each level's form.  work:
+// chunk_carry_scratch(count) NP doubles.  Returns the launches made.
 int chunk_carry_levels(long count);
+int chunk_carry_table_levels(long count);
 long chunk_carry_scratch(long count);
-int launch_chunk_carry(int NP, double* items, long count, const double* P, int l0, const double* X0, double* work,
-                       cudaStream_t s);
+int launch_chunk_carry(int NP, double* items, long count, const double* P, int l0, int h0, const double* X0,
+                       double* work, cudaStream_t s);
 // The same scan in its two halves, for a scan whose top level is done
 // elsewhere (the time partition of one solve across devices): the up-sweep
 // leaves the chunk aggregates of level h in arr[h] (h = `levels`, or while

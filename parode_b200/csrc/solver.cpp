@@ -243,8 +243,8 @@ void Plan::build(int device, const SystemDesc& sys, InputRegistry* inputs, int u
                 brK_ = Kb;
                 brKpad_ = (Kb + 1) & ~1;
                 nblocks_ = (nScan_ + shape_.B - 1) / shape_.B;
-                // the chunked carry over blocks reads P_R .. P_{R + 4 h}
-                levels_ = shape_.R + 4 * chunk_carry_levels(nblocks_) + 1;
+                // the chunked carry over blocks reads P_R .. P_{R + 4 h + 3}
+                levels_ = shape_.R + chunk_carry_table_levels(nblocks_);
             }
         }
         // otherwise the mixed form runs the in-block sweeps on the tensor
@@ -912,7 +912,7 @@ void Plan::execute_general(double* Y, cudaStream_t s)
 int Plan::carry(cudaStream_t s)
 {
     // the exclusive scan of the block aggregates (kernels_carry.cu)
-    return launch_chunk_carry(Np_, dG_, nblocks_, dPow_, shape_.R, dX0_, dWork_, s);
+    return launch_chunk_carry(Np_, dG_, nblocks_, dPow_, shape_.R, 0, dX0_, dWork_, s);
 }
 
 LevelArgs Plan::response_agg_args() const
@@ -1061,8 +1061,8 @@ void Plan::setup_shard(const PlanOptions& opt)
     nScan_ = std::min(Sb * B, nScan_ - shard_begin_);
     nOut_ = nScan_ + (solver_ == kABM ? 3 : 0);
     nblocks_ = (nScan_ + B - 1) / B;
-    // the power table reaches the top scan's levels: P_{R + 4 (k + h)}
-    levels_ = shape_.R + 4 * (k + chunk_carry_levels((long)shards_ * c)) + 1;
+    // the power table reaches the top scan's levels: P_{R + 4 (k + h) + 3}
+    levels_ = shape_.R + 4 * k + chunk_carry_table_levels((long)shards_ * c);
 }
 
 void Plan::shard_info(long long info[5]) const
@@ -1102,7 +1102,7 @@ void Plan::shard_down(const double* dGathered, double* Y, cudaStream_t s)
     // every shard scans the gathered sequence (exclusive, seeded with the
     // initial state) and keeps the prefixes of its own items
     PARODE_CUDA(cudaMemcpyAsync(dTop_, dGathered, sizeof(double) * (size_t)items * Np_, cudaMemcpyDeviceToDevice, s));
-    launch_chunk_carry(Np_, dTop_, items, dPow_, shape_.R + 4 * shard_k_, dX0_, dTop_ + items * Np_, s);
+    launch_chunk_carry(Np_, dTop_, items, dPow_, shape_.R + 4 * shard_k_, shard_k_, dX0_, dTop_ + items * Np_, s);
     ChunkLevels L = shard_levels_;
     const double* mine = dTop_ + (long)shard_ * shard_c_ * Np_;
     if (L.h == 0) {
