@@ -358,6 +358,7 @@ template <int KMAX>
 __global__ void k_sinusoid_planes(float* hi, float* lo, int m, int K, const double* a, const double* f,
                                   const double* phi, double base, double dt, long count, long joff)
 {
+    grid_dep_trigger();  // the response GEMMs may set up meanwhile (they wait for these samples)
     const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
     const long runs = (count + kSampleRun - 1) / kSampleRun;
     if (e >= runs * m) return;

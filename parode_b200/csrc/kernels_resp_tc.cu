@@ -33,6 +33,7 @@
 // only hi*hi: a third of the tensor work and half of the operand traffic,
 // with the TF32 rounding of both operands (about 2^-11 relative) left in.
 #include "common.h"
+#include "device_common.cuh"
 #include "kernels.h"
 #include "tc05.cuh"
 
@@ -196,6 +197,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_resp_tc(const RespArgs* __restr
     fence_before_sync();
     __syncthreads();
     fence_after_sync();
+    // launched as a dependent of the sample kernel: the set-up above overlaps
+    // its tail, the samples are read (and the outputs written) after this
+    grid_dep_wait();
     const uint32_t tbase = *slot;
     const long t0 = cta[blockIdx.x], t1 = cta[blockIdx.x + 1];
 
@@ -444,12 +448,11 @@ void launch_resp_tc(const RespArgs* dArgs, const long* dStart, int nent, const l
     if (nent <= 0 || ctas <= 0) return;
     if (one_pass) {
         PARODE_CUDA(cudaFuncSetAttribute(k_resp_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));
-        k_resp_tc<true><<<(unsigned)ctas, kThreads, kSmem, s>>>(dArgs, dStart, nent, dCta, status);
+        launch_dependent(k_resp_tc<true>, (unsigned)ctas, kThreads, kSmem, s, dArgs, dStart, nent, dCta, status);
     } else {
         PARODE_CUDA(cudaFuncSetAttribute(k_resp_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));
-        k_resp_tc<false><<<(unsigned)ctas, kThreads, kSmem, s>>>(dArgs, dStart, nent, dCta, status);
+        launch_dependent(k_resp_tc<false>, (unsigned)ctas, kThreads, kSmem, s, dArgs, dStart, nent, dCta, status);
     }
-    PARODE_CUDA(cudaGetLastError());
 }
 
 }  // namespace parode

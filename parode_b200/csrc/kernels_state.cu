@@ -46,6 +46,9 @@ __global__ void __launch_bounds__(kThreads) k_state_out(const double* __restrict
         Ws[r * kpitch<NP>() + k] = r < M ? W[(long)r * ld + k] : 0.0;
     }
     __syncthreads();
+    // launched as a dependent of the carry's last kernel: W (formed with the
+    // plan) is staged while it finishes; the states and windows after this
+    grid_dep_wait();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int g = lane >> 2, t = lane & 3;
     // a warp takes 16 blocks at a time (two 8-block halves): every A fragment
@@ -108,8 +111,7 @@ bool state_t(const double* W, long ld, int M, const double* X, const double* acc
     const long tiles = (nblocks + 15) / 16;
     const unsigned grid =
         (unsigned)std::max<long>(1, std::min<long>((tiles + kWarps - 1) / kWarps, (long)sms * std::max(per_sm, 1)));
-    k_state_out<NP><<<grid, kThreads, smem, s>>>(W, ld, M, Mp, X, acc, Y, gs, nblocks, limit);
-    PARODE_CUDA(cudaGetLastError());
+    launch_dependent(k_state_out<NP>, grid, kThreads, smem, s, W, ld, M, Mp, X, acc, Y, gs, nblocks, limit);
     return true;
 }
 
