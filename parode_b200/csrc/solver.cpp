@@ -306,63 +306,60 @@ void Plan::build(int device, const SystemDesc& sys, InputRegistry* inputs, int u
     done_ = take_event(device_);
 
     phase("streams", false);
-    // ---- host FP64 discretisation --------------------------------------
     const int n = sys.n, mB = sys.zeroB ? 0 : sys.m;
     const int W = solver == kRK4 ? 3 : 5;
-    std::vector<double> Phi((size_t)Ns_ * Ns_), Bbar((size_t)n * W * std::max(mB, 1), 0.0);
-    if (solver == kRK4)
-        discretise_rk4(n, mB, sys.A.data(), mB ? sys.B.data() : nullptr, h, Phi.data(), Bbar.data());
-    else
-        discretise_abm(n, mB, sys.A.data(), mB ? sys.B.data() : nullptr, h, Phi.data(), Bbar.data());
-    std::vector<double> PhiP((size_t)Np_ * Np_, 0.0), X0((size_t)Np_, 0.0);
-    for (int r = 0; r < Ns_; ++r)
-        std::memcpy(&PhiP[(size_t)r * Np_], &Phi[(size_t)r * Ns_], sizeof(double) * Ns_);
-
-    phase("discretise", false);
-    // ---- device buffers ---------------------------------------------------
+    std::vector<double> X0((size_t)Np_, 0.0);
+    // ---- device buffers: one block from the stream-ordered pool, carved
+    // (each cudaMallocAsync costs a few microseconds even from a warm pool)
+    std::vector<std::pair<double**, long>> want;
+    double* st = nullptr;
     long npow = std::max(levels_, 1);
-    alloc(&dPow_, npow * (long)Np_ * Np_);
-    alloc(&dBbar_, (long)Bbar.size());
-    alloc(&dC_, std::max<long>(1, (long)p_ * n));
-    alloc(&dD_, std::max<long>(1, (long)p_ * std::max(sys.m, 1)));
-    alloc(&dX0_, Np_);
+    want.emplace_back(&dPow_, npow * (long)Np_ * Np_);
+    want.emplace_back(&dBbar_, (long)n * W * std::max(mB, 1));
+    // the discretisation's inputs and work (kernels_disc.cu: the host
+    // restatement's operation order, so the same bits as host_math.cpp)
+    double *dDA = nullptr, *dDB = nullptr, *dPhiC = nullptr, *dDWork = nullptr, *dDelta = nullptr;
+    double *dDJob = nullptr, *dPhiJob = nullptr;
+    double* dTiles[3] = {nullptr, nullptr, nullptr};
+    long ntiles[3] = {0, 0, 0};
     {
-        double* st = nullptr;
-        alloc(&st, 1);
-        dStatus_ = reinterpret_cast<int*>(st);
-        PARODE_CUDA(cudaMemsetAsync(st, 0, sizeof(double), stream_));
+        const long tn = (n + 31) / 32, tm = mB > 0 ? (mB + 31) / 32 : 0;
+        for (int st = 0; st < (solver == kRK4 ? 3 : 1); ++st) ntiles[st] = tn * tn + tn * tm;
+        const auto words = [](size_t bytes) { return (long)((bytes + 7) / 8); };
+        want.emplace_back(&dDA, (long)n * n);
+        if (mB) want.emplace_back(&dDB, (long)n * mB);
+        want.emplace_back(&dPhiC, (long)n * Ns_);
+        want.emplace_back(&dDWork, discretise_work_doubles(n, mB));
+        want.emplace_back(&dDelta, 1);
+        want.emplace_back(&dDJob, words(sizeof(DiscJob)));
+        want.emplace_back(&dPhiJob, words(sizeof(PhiJob)));
+        for (int st = 0; st < 3; ++st)
+            if (ntiles[st]) want.emplace_back(&dTiles[st], words(sizeof(DiscTile) * (size_t)ntiles[st]));
     }
+    want.emplace_back(&dC_, std::max<long>(1, (long)p_ * n));
+    want.emplace_back(&dD_, std::max<long>(1, (long)p_ * std::max(sys.m, 1)));
+    want.emplace_back(&dX0_, Np_);
+    want.emplace_back(&st, 1);
     if (path_ == kPathLevel || path_ == kPathGeneral) {
-        alloc(&dV_, (Tp_ + 1) * (long)Np_);  // a leading slot holds the initial state
+        want.emplace_back(&dV_, (Tp_ + 1) * (long)Np_);  // a leading slot holds the initial state
         if (path_ == kPathGeneral) {
-            alloc(&dMs_, nScan_ * (long)Np_ * Np_);
-            alloc(&dXs_, nScan_ * (long)Np_);
+            want.emplace_back(&dMs_, nScan_ * (long)Np_ * Np_);
+            want.emplace_back(&dXs_, nScan_ * (long)Np_);
         }
     } else {
-        alloc(&dG_, nblocks_ * (long)Np_);
-        alloc(&dWork_, std::max(blocked_items_scratch(shape_, nblocks_), chunk_carry_scratch(nblocks_) + 1 + shard_k_) *
-                           (long)Np_);
+        want.emplace_back(&dG_, nblocks_ * (long)Np_);
+        want.emplace_back(&dWork_, std::max(blocked_items_scratch(shape_, nblocks_),
+                                            chunk_carry_scratch(nblocks_) + 1 + shard_k_) *
+                                       (long)Np_);
         if (shards_ > 1) {
             // the gathered top items of every shard, then the scratch of their scan
             const long items = (long)shards_ * shard_c_;
-            alloc(&dTop_, (items + chunk_carry_scratch(items) + 1) * (long)Np_);
+            want.emplace_back(&dTop_, (items + chunk_carry_scratch(items) + 1) * (long)Np_);
         }
-        alloc(&dCP_, (long)shape_.B * p_ * Np_);
-        alloc(&dCext_, (long)p_ * Np_);
-        // output rows of the scan state: C at the state block (the last n of
-        // the ABM companion state), or the state itself when C and D are absent
-        std::vector<double> Cext((size_t)p_ * Np_, 0.0);
-        const int xoff = solver == kRK4 ? 0 : 3 * n;
-        for (int o = 0; o < p_; ++o)
-            for (int c = 0; c < n; ++c) {
-                double v = 0.0;
-                if (!sys.zeroC) v = sys.C[(size_t)o * n + c];
-                else if (sys.zeroD) v = (o == c) ? 1.0 : 0.0;
-                Cext[(size_t)o * Np_ + xoff + c] = v;
-            }
-        h2d(dCext_, Cext.data(), sizeof(double) * Cext.size());
+        want.emplace_back(&dCP_, (long)shape_.B * p_ * Np_);
+        want.emplace_back(&dCext_, (long)p_ * Np_);
     }
-    alloc(&dY_, nOut_ * (long)p_);
+    want.emplace_back(&dY_, nOut_ * (long)p_);
     if (solver == kRK4) {
         nU_ = 2 * nScan_ + 1;
         u_base_ = t0;
@@ -376,36 +373,95 @@ void Plan::build(int device, const SystemDesc& sys, InputRegistry* inputs, int u
         u_dt_ = h;
         u_joff_ = shard_begin_;
     }
+    // the response leaf reads whole windows: the last block's window runs
+    // past the samples into a zero padding
+    const long pad = (mu_ > 0 && !gen_ && br_) ? (2L * shape_.B + 8) * mu_ + 2 : 0;
+    // the mixed response GEMMs read the samples as TF32 planes (their TMA
+    // boxes run up to 15 samples past a window); FP64 samples are then only
+    // the scratch a user input function fills before the split
+    const bool planes = mu_ > 0 && !gen_ && br_tc_;
+    const long nf = nU_ * (long)mu_ + pad + 16;
+    double* dh = nullptr;
+    double* dl = nullptr;
     if (mu_ > 0 && !gen_) {
-        // the response leaf reads whole windows: the last block's window runs
-        // past the samples into a zero padding
-        const long pad = br_ ? (2L * shape_.B + 8) * mu_ + 2 : 0;
-        // the mixed response GEMMs read the samples as TF32 planes (their TMA
-        // boxes run up to 15 samples past a window); FP64 samples are then
-        // only the scratch a user input function fills before the split
-        const bool planes = br_tc_;
-        if (!planes || input_->kind != InputEntry::kSinusoid) {
-            alloc(&dU_, nU_ * (long)mu_ + pad);
-            // every execute writes all nU x mu samples: only the padding is zeroed
-            if (pad) PARODE_CUDA(cudaMemsetAsync(dU_ + nU_ * mu_, 0, sizeof(double) * (size_t)pad, stream_));
-        }
+        if (!planes || input_->kind != InputEntry::kSinusoid) want.emplace_back(&dU_, nU_ * (long)mu_ + pad);
         if (planes) {
-            const long nf = nU_ * (long)mu_ + pad + 16;
-            double* d = nullptr;
-            alloc(&d, (nf + 1) / 2);
-            dUh_ = reinterpret_cast<float*>(d);
-            const size_t used = (size_t)nU_ * mu_;  // rewritten by every execute
-            PARODE_CUDA(cudaMemsetAsync(dUh_ + used, 0, sizeof(float) * ((size_t)nf - used), stream_));
-            if (!one_pass_) {  // the single-pass form reads no lo plane
-                alloc(&d, (nf + 1) / 2);
-                dUl_ = reinterpret_cast<float*>(d);
-                PARODE_CUDA(cudaMemsetAsync(dUl_ + used, 0, sizeof(float) * ((size_t)nf - used), stream_));
-            }
+            want.emplace_back(&dh, (nf + 1) / 2);
+            if (!one_pass_) want.emplace_back(&dl, (nf + 1) / 2);  // the single-pass form reads no lo plane
         }
     }
-    phase("buffers", true);
-    h2d(dPow_, PhiP.data(), sizeof(double) * PhiP.size());
-    h2d(dBbar_, Bbar.data(), sizeof(double) * Bbar.size());
+    carve(want);
+    phase("allocate", false);
+    dStatus_ = reinterpret_cast<int*>(st);
+    PARODE_CUDA(cudaMemsetAsync(st, 0, sizeof(double), stream_));
+    if (!(path_ == kPathLevel || path_ == kPathGeneral)) {
+        // output rows of the scan state: C at the state block (the last n of
+        // the ABM companion state), or the state itself when C and D are absent
+        std::vector<double> Cext((size_t)p_ * Np_, 0.0);
+        const int xoff = solver == kRK4 ? 0 : 3 * n;
+        for (int o = 0; o < p_; ++o)
+            for (int c = 0; c < n; ++c) {
+                double v = 0.0;
+                if (!sys.zeroC) v = sys.C[(size_t)o * n + c];
+                else if (sys.zeroD) v = (o == c) ? 1.0 : 0.0;
+                Cext[(size_t)o * Np_ + xoff + c] = v;
+            }
+        h2d(dCext_, Cext.data(), sizeof(double) * Cext.size());
+    }
+    phase("output rows", false);
+    if (mu_ > 0 && !gen_) {
+        // every execute writes all nU x mu samples: only the padding is zeroed
+        if (dU_ && pad) PARODE_CUDA(cudaMemsetAsync(dU_ + nU_ * mu_, 0, sizeof(double) * (size_t)pad, stream_));
+        const size_t used = (size_t)nU_ * mu_;  // rewritten by every execute
+        if (dh) {
+            dUh_ = reinterpret_cast<float*>(dh);
+            PARODE_CUDA(cudaMemsetAsync(dUh_ + used, 0, sizeof(float) * ((size_t)nf - used), stream_));
+        }
+        if (dl) {
+            dUl_ = reinterpret_cast<float*>(dl);
+            PARODE_CUDA(cudaMemsetAsync(dUl_ + used, 0, sizeof(float) * ((size_t)nf - used), stream_));
+        }
+    }
+    phase("padding", true);
+    // ---- discretisation on the device: A and B up, Phi's compact form and
+    // Bbar from the tiled products, Phi expanded into the power table's
+    // level 0 (zero padded; ABM: the shift rows above the last block row)
+    {
+        DiscJob j;
+        j.A = dDA;
+        j.B = mB ? dDB : nullptr;
+        j.phi = dPhiC;
+        j.bbar = dBbar_;
+        j.work = dDWork;
+        j.delta = dDelta;
+        j.n = n;
+        j.m = mB;
+        j.solver = solver;
+        j.h = h;
+        h2d(dDA, sys.A.data(), sizeof(double) * (size_t)n * n);
+        if (mB) h2d(dDB, sys.B.data(), sizeof(double) * (size_t)n * mB);
+        h2d(dDJob, &j, sizeof j);
+        const DiscTile* dt[3] = {nullptr, nullptr, nullptr};
+        for (int st = 0; st < 3; ++st) {
+            if (!ntiles[st]) continue;
+            std::vector<DiscTile> tl;
+            tl.reserve((size_t)ntiles[st]);
+            discretise_tiles(j, st, tl);
+            if ((long)tl.size() != ntiles[st]) throw Error(kDeviceError, "discretisation tiles: count mismatch");
+            h2d(dTiles[st], tl.data(), sizeof(DiscTile) * tl.size());
+            dt[st] = reinterpret_cast<const DiscTile*>(dTiles[st]);
+        }
+        launch_discretise_batch(reinterpret_cast<const DiscJob*>(dDJob), 1, dt, ntiles, sms_, stream_);
+        PhiJob pj;
+        pj.dst = dPow_;
+        pj.src = dPhiC;
+        pj.n = n;
+        pj.Np = Np_;
+        pj.solver = solver;
+        h2d(dPhiJob, &pj, sizeof pj);
+        launch_phi_batch(reinterpret_cast<const PhiJob*>(dPhiJob), 1, (long)Np_ * Np_, stream_);
+    }
+    phase("discretise (device)", true);
     if (!sys.zeroC)
         h2d(dC_, sys.C.data(), sizeof(double) * (size_t)p_ * n);
     if (!sys.zeroD)
@@ -558,16 +614,19 @@ void Plan::build(int device, const SystemDesc& sys, InputRegistry* inputs, int u
     phase("sync", false);
     if (opt.log) std::fprintf(stderr, "ParODE plan set-up (n=%d T=%ld path=%d):%s\n", sys.n, nScan_, path(), phases.c_str());
     // keep a plan's worth of freed memory in the pool, so that the next plan
-    // of this size (the next SimulateODE call) maps nothing new
+    // of this size (the next SimulateODE call) maps nothing new.  The pool's
+    // reserved memory runs above the plan's bytes (its mapping granularity,
+    // the stream and handle pools' neighbours), and a threshold of exactly
+    // the plan's bytes let it release the large block between calls (a 250 MB
+    // block re-mapped per cfg2 call: 3 ms instead of 7 us): twice the plan
+    // plus 256 MiB of slack
     {
         cudaMemPool_t pool = nullptr;
         PARODE_CUDA(cudaDeviceGetDefaultMemPool(&pool, device_));
         uint64_t keep = 0;
         PARODE_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
-        if (keep < (uint64_t)bytes_) {
-            keep = (uint64_t)bytes_;
-            PARODE_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
-        }
+        uint64_t want = 2 * (uint64_t)bytes_ + ((uint64_t)256 << 20);
+        if (keep < want) PARODE_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &want));
     }
 }
 
@@ -650,6 +709,20 @@ void Plan::alloc(double** p, long n)
     }
     bufs_.push_back(*p);
     bytes_ += bytes;
+}
+
+void Plan::carve(const std::vector<std::pair<double**, long>>& want)
+{
+    // 256-byte aligned parts of one block (TMA and bulk copies need 16)
+    size_t total = 0;
+    for (const auto& w : want) total += (sizeof(double) * (size_t)std::max<long>(w.second, 1) + 255) & ~(size_t)255;
+    double* base = nullptr;
+    alloc(&base, (long)(total / sizeof(double)));
+    char* at = reinterpret_cast<char*>(base);
+    for (const auto& w : want) {
+        *w.first = reinterpret_cast<double*>(at);
+        at += (sizeof(double) * (size_t)std::max<long>(w.second, 1) + 255) & ~(size_t)255;
+    }
 }
 
 void Plan::set_profiling(bool on) { profiling_ = on; }

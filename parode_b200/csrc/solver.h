@@ -115,6 +115,7 @@ private:
                double tEnd, double h, const PlanOptions& opt);
     void release() noexcept;
     void alloc(double** p, long n);
+    void carve(const std::vector<std::pair<double**, long>>& want);  // one allocation, parts assigned
     void h2d(void* dst, const void* src, size_t bytes);
     void mark(const char* stage, cudaStream_t s);
     void execute_body(double* y, cudaStream_t s);
