@@ -309,6 +309,7 @@ void Plan::build(int device, const SystemDesc& sys, InputRegistry* inputs, int u
     const int n = sys.n, mB = sys.zeroB ? 0 : sys.m;
     const int W = solver == kRK4 ? 3 : 5;
     std::vector<double> X0((size_t)Np_, 0.0);
+    bool tables_forked = false;  // the power table is built on side_ (joined before the final synchronise)
     // ---- device buffers: one block from the stream-ordered pool, carved
     // (each cudaMallocAsync costs a few microseconds even from a warm pool)
     std::vector<std::pair<double**, long>> want;
@@ -510,6 +511,13 @@ void Plan::build(int device, const SystemDesc& sys, InputRegistry* inputs, int u
     h2d(dX0_, X0.data(), sizeof(double) * Np_);
     phase("copies+start-up", true);
     if (br_) {
+        // the carry's powers P_1 .. P_levels (Phi^(2^l)) depend on Phi alone:
+        // formed once here, on the side stream beside W (both only read level 0)
+        PARODE_CUDA(cudaEventRecord(fork_[0], stream_));
+        PARODE_CUDA(cudaStreamWaitEvent(side_, fork_[0], 0));
+        launch_blocked_tables(shape_, dPow_, 1, levels_, nullptr, nullptr, p_, side_);
+        PARODE_CUDA(cudaEventRecord(fork_[1], side_));
+        tables_forked = true;
         // block response matrix from Phi (power-table level 0), Bbar, Cext, D
         alloc(&dW_, (long)(shape_.B * p_ + Np_) * (brKpad_ + Np_));
         ResponseArgs ra;
@@ -534,10 +542,6 @@ void Plan::build(int device, const SystemDesc& sys, InputRegistry* inputs, int u
         h2d(dra, &ra, sizeof(ra));
         launch_block_response(reinterpret_cast<const ResponseArgs*>(dra), 1, Np_, p_, brKpad_, stream_);
         phase("W", true);
-        // the carry's powers P_1 .. P_levels (Phi^(2^l)) depend on Phi alone:
-        // formed once here, like W
-        launch_blocked_tables(shape_, dPow_, 1, levels_, nullptr, nullptr, p_, stream_);
-        phase("tables", true);
         if (br_tc_) {
             // the two tensor-core GEMMs over the sample windows: aggregates
             // into G, output windows into the plan's y buffer (the FP64 state
@@ -606,6 +610,7 @@ void Plan::build(int device, const SystemDesc& sys, InputRegistry* inputs, int u
             phase("tensor-core set-up", true);
         }
     }
+    if (tables_forked) PARODE_CUDA(cudaStreamWaitEvent(stream_, fork_[1], 0));
     PARODE_CUDA(cudaStreamSynchronize(stream_));
     if (pin_) {  // the set-up copies are done: the block goes back to the pool
         give_pinned(pin_);
