@@ -680,36 +680,61 @@ def run_ours(args):
         del y_single
     value = world * case.n * case.T / (main["ms_per_step"] / 1e3)
 
-    # e2e: the C-ABI call with host buffers (plan set-up, H2D, solve, D2H of y
-    # into pinned host arrays the caller keeps across calls)
-    e2e = None
-    if not args.no_e2e:
-        e2e_ms = []
-        T_out = pb.num_outputs(case.solver, case.t0, case.t_end, case.h)
-        t_host = torch.empty(T_out, dtype=torch.float64, pin_memory=True).numpy()
-        y_host = torch.empty((T_out, case.p), dtype=torch.float64, pin_memory=True).numpy()
+    # e2e: the reference's C-ABI call with host buffers (plan set-up, H2D,
+    # solve, D2H of y into host arrays the caller keeps across calls, pinned):
+    # SimulateODE with its float arrays (fType), the precision mode set by
+    # PARODE_OPT_PRECISION; beside it the FP64 extension ParODE_SimulateODE_d
+    def time_calls(call):
+        ms = []
         # 1 warm-up + 7 timed calls; the median, since the host side (page
         # cache, other processes on the host cores) adds outliers of 10-600 ms
         for it in range(1 + 7):
             torch.cuda.synchronize()
             s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             s.record()
-            pb.simulate(case.A, case.B, case.C, case.D, case.x0, u, case.t0, case.t_end, case.h, solver=case.solver,
-                        precision=precision, t_out=t_host, y_out=y_host)
+            call()
             e.record()
             e.synchronize()
             if it > 0:
-                e2e_ms.append(s.elapsed_time(e))
-        e2e_t = torch.tensor([statistics.median(e2e_ms)], dtype=torch.float64, device=dev)
+                ms.append(s.elapsed_time(e))
+        t_ = torch.tensor([statistics.median(ms)], dtype=torch.float64, device=dev)
         if world > 1:
-            torch.distributed.all_reduce(e2e_t, op=torch.distributed.ReduceOp.MAX)
-        h2d = 8 * (case.A.size + case.B.size + case.C.size + case.D.size + case.x0.size + 3 * case.u.a.size)
-        d2h = 8 * case.T * case.p
-        e2e = {"value": world * case.n * case.T / (float(e2e_t.item()) / 1e3), "unit": UNIT,
-               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "ms_per_step": float(e2e_t.item()),
-               "statistic": f"median of {len(e2e_ms)} calls", "mean_ms": statistics.mean(e2e_ms),
-               "max_ms": max(e2e_ms),
-               "call": "ParODE_SimulateODE_d (host arrays in, y out into pinned host memory reused across calls)"}
+            torch.distributed.all_reduce(t_, op=torch.distributed.ReduceOp.MAX)
+        return float(t_.item()), ms
+
+    e2e = None
+    e2e_f64 = None
+    if not args.no_e2e:
+        T_out = pb.num_outputs(case.solver, case.t0, case.t_end, case.h)
+        t32 = torch.empty(T_out, dtype=torch.float32, pin_memory=True).numpy()
+        y32 = torch.empty((T_out, case.p), dtype=torch.float32, pin_memory=True).numpy()
+        prev = pb.get_option(pb.OPT_PRECISION)
+        pb.set_option(pb.OPT_PRECISION, precision)
+        try:
+            def call32():
+                _, _, err = pb.simulate_f32(case.A, case.B, case.C, case.D, case.x0, u, case.t0, case.t_end, case.h,
+                                            solver=case.solver, t_out=t32, y_out=y32)
+                if err != 0:
+                    raise RuntimeError(f"SimulateODE error {err}")
+            med, ms = time_calls(call32)
+        finally:
+            pb.set_option(pb.OPT_PRECISION, prev)
+        h2d = 4 * (case.A.size + case.B.size + case.C.size + case.D.size + case.x0.size) + 8 * 3 * case.u.a.size
+        d2h = 4 * case.T * case.p
+        e2e = {"value": world * case.n * case.T / (med / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "ms_per_step": med,
+               "statistic": f"median of {len(ms)} calls", "mean_ms": statistics.mean(ms), "max_ms": max(ms),
+               "call": "SimulateODE, the reference's C ABI (float arrays in, t and y out into pinned host memory "
+                       "reused across calls; y rounded to float on the device), precision mode mixed"}
+        t64 = torch.empty(T_out, dtype=torch.float64, pin_memory=True).numpy()
+        y64 = torch.empty((T_out, case.p), dtype=torch.float64, pin_memory=True).numpy()
+        med, ms = time_calls(lambda: pb.simulate(case.A, case.B, case.C, case.D, case.x0, u, case.t0, case.t_end,
+                                                 case.h, solver=case.solver, precision=precision, t_out=t64, y_out=y64))
+        e2e_f64 = {"value": world * case.n * case.T / (med / 1e3), "unit": UNIT, "ms_per_step": med,
+                   "h2d_bytes_per_step": int(8 * (case.A.size + case.B.size + case.C.size + case.D.size +
+                                                  case.x0.size + 3 * case.u.a.size)),
+                   "d2h_bytes_per_step": int(2 * d2h), "statistic": f"median of {len(ms)} calls",
+                   "call": "ParODE_SimulateODE_d (double arrays in, y out into pinned host memory reused across calls)"}
 
     # the e2e call's parts, each timed on its own: plan creation (host
     # discretisation, W and power tables on the device), the solve, the copy
@@ -822,6 +847,7 @@ def run_ours(args):
             "peaks_source": peaks_kind,
             "tuner": tuner,
             "e2e_split": e2e_split,
+            "e2e_f64": e2e_f64,
             "cfg1": cfg1,
             "batched": batched,
             "serving": serving,

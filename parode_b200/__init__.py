@@ -342,8 +342,12 @@ def tune_clear() -> None:
     lib.ParODE_TuneClear()
 
 
-def simulate_f32(A, B, Cm, D, x0, u_index: int, t0: float, t_end: float, h: float, solver: int = RK4):
-    """The reference C ABI SimulateODE (float arrays).  Returns (t, y, err)."""
+def simulate_f32(A, B, Cm, D, x0, u_index: int, t0: float, t_end: float, h: float, solver: int = RK4, t_out=None,
+                 y_out=None):
+    """The reference C ABI SimulateODE (float arrays; the precision mode is
+    PARODE_OPT_PRECISION's).  Returns (t, y, err).  t_out / y_out: optional
+    caller-owned float32 arrays of T and (T, outputs) elements (C-contiguous;
+    pinned host memory makes the copy-out fastest), filled in place."""
     A32 = np.ascontiguousarray(A, dtype=np.float32)
     n = A32.shape[0]
     zB, zC, zD = int(B is None or np.size(B) == 0), int(Cm is None or np.size(Cm) == 0), int(D is None or np.size(D) == 0)
@@ -354,8 +358,11 @@ def simulate_f32(A, B, Cm, D, x0, u_index: int, t0: float, t_end: float, h: floa
     m = B32.shape[1] if not zB else (D32.shape[1] if not zD else 0)
     p = C32.shape[0] if not zC else (D32.shape[0] if not zD else n)
     T = max(num_outputs(solver, t0, t_end, h), 1)
-    t = np.zeros(T, dtype=np.float32)
-    y = np.zeros((T, p), dtype=np.float32)
+    t = np.zeros(T, dtype=np.float32) if t_out is None else t_out
+    y = np.zeros((T, p), dtype=np.float32) if y_out is None else y_out
+    for a_, shape in ((t, (T,)), (y, (T, p))):
+        if a_.dtype != np.float32 or a_.shape != shape or not a_.flags.c_contiguous:
+            raise ValueError("simulate_f32: t_out / y_out must be C-contiguous float32 arrays of the output shape")
     fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
     args_i = [C.c_int(v) for v in (m, n, p, zB, zC, zD, u_index)]
     ts, te, hs = C.c_double(t0), C.c_double(t_end), C.c_double(h)

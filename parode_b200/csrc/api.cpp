@@ -333,19 +333,22 @@ void SimulateODE(fType A[], fType B[], fType C[], fType D[], int* nInputs, int* 
         opt.input_double = false;  // UFunc(fType t, ...) with fType = float, as the reference ABI
         Plan plan(dev, s, &L.inputs, *uIndex, *solver, *tStart, *tEnd, *tStep, opt);
         long T = plan.num_outputs();
-        int p = plan.channels();
-        std::vector<double> t((size_t)T), y((size_t)T * p);
+        // fType is float: y is rounded on the device and copied straight into
+        // xVect, and the time vector is written as float on a helper thread
+        static_assert(sizeof(fType) == sizeof(float), "the reference ABI's fType is float");
         HelperThread tv;
         const int sv = *solver;
         const double t0 = *tStart, t1 = *tEnd, h = *tStep;
-        if (tVect) tv.run([&t, sv, t0, t1, h] { time_vector(sv, t0, t1, h, t.data()); });
+        float* tOut = reinterpret_cast<float*>(tVect);
+        if (tVect) tv.run([tOut, sv, t0, t1, h] { time_vector_f(sv, t0, t1, h, tOut); });
         plan.execute(nullptr, nullptr);
-        plan.get_output(nullptr, y.data());
+        try {
+            plan.get_output_f32(nullptr, reinterpret_cast<float*>(xVect));
+        } catch (...) {
+            tv.join();
+            throw;
+        }
         tv.join();
-        if (tVect)
-            for (long k = 0; k < T; ++k) tVect[k] = (fType)t[(size_t)k];
-        if (xVect)
-            for (long q = 0; q < T * p; ++q) xVect[q] = (fType)y[(size_t)q];
         if (nSteps) nSteps[0] = (int)T;
         if (L.log)
             std::fprintf(stderr, "ParODE: SimulateODE solver=%d n=%d T=%ld path=%d launches=%d\n", *solver, s.n, T,

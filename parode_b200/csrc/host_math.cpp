@@ -61,7 +61,11 @@ inline double time_link(double prev, double h) { return (double)(float)(prev + h
 
 }  // namespace
 
-void time_chain(double* tv, long count, double h)
+// The chain in either storage type (every element is a float value, so the
+// float form stores the same numbers; each link is checked in double on the
+// stored values, so the speculation stays exact).
+template <class T>
+void time_chain_t(T* tv, long count, double h)
 {
     // The chain tv[i+1] = time_link(tv[i]) is one dependent float round trip
     // per element (~5 ms for 2^20).  Within a binade of the float values it
@@ -79,36 +83,42 @@ void time_chain(double* tv, long count, double h)
         const double v = tv[s];
         const double d = time_link(v, h) - v;
         const long e = std::min(count - 1, s + kBlock);
-        for (long j = s + 1; j <= e; ++j) tv[j] = v + (double)(j - s) * d;
+        for (long j = s + 1; j <= e; ++j) tv[j] = (T)(v + (double)(j - s) * d);
         int ok = 1;
-        for (long j = s; j < e; ++j) ok &= (time_link(tv[j], h) == tv[j + 1]) ? 1 : 0;
+        for (long j = s; j < e; ++j) ok &= (time_link((double)tv[j], h) == (double)tv[j + 1]) ? 1 : 0;
         if (ok) {
             s = e;
             continue;
         }
         long j = s;
-        while (time_link(tv[j], h) == tv[j + 1]) ++j;
-        tv[j + 1] = time_link(tv[j], h);
+        while (time_link((double)tv[j], h) == (double)tv[j + 1]) ++j;
+        tv[j + 1] = (T)time_link((double)tv[j], h);
         long next = j + 1;
         if (j - s < kEarly) {
             const long stop = std::min(count - 1, next + kStretch);
-            for (; next < stop; ++next) tv[next + 1] = time_link(tv[next], h);
+            for (; next < stop; ++next) tv[next + 1] = (T)time_link((double)tv[next], h);
         }
         s = next;
     }
 }
 
-void time_vector(int solver, double t0, double tEnd, double h, double* tv)
+void time_chain(double* tv, long count, double h) { time_chain_t<double>(tv, count, h); }
+
+template <class T>
+void time_vector_t(int solver, double t0, double tEnd, double h, T* tv)
 {
     long ns = 0;
     long nt = num_outputs(solver, t0, tEnd, h, &ns);
     if (nt <= 0) return;
     long pre = nt - ns;
     double ts = (solver == 1) ? t0 + 3.0 * h : t0;
-    for (long i = 0; i < pre; ++i) tv[i] = (double)(float)(ts - (double)(pre - i) * h);
-    tv[pre] = (double)(float)ts;
-    time_chain(tv + pre, ns, h);
+    for (long i = 0; i < pre; ++i) tv[i] = (T)(float)(ts - (double)(pre - i) * h);
+    tv[pre] = (T)(float)ts;
+    time_chain_t<T>(tv + pre, ns, h);
 }
+
+void time_vector(int solver, double t0, double tEnd, double h, double* tv) { time_vector_t<double>(solver, t0, tEnd, h, tv); }
+void time_vector_f(int solver, double t0, double tEnd, double h, float* tv) { time_vector_t<float>(solver, t0, tEnd, h, tv); }
 
 void discretise_rk4(int n, int m, const double* A, const double* B, double h, double* Phi, double* Bbar)
 {

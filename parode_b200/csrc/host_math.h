@@ -27,6 +27,8 @@ void time_chain(double* tv, long count, double h);
 // Time vector with the reference's float accumulation
 // (Sources/GPUFixedStepIterative.cpp:141-146); written as double.
 void time_vector(int solver, double t0, double tEnd, double h, double* tv);
+// The same values stored as float (the reference C ABI's fType arrays).
+void time_vector_f(int solver, double t0, double tEnd, double h, float* tv);
 
 // One-step affine map.  Phi is Ns x Ns (Ns = n or 4n), Bbar is n x W*m
 // (W = 3 for RK4, 5 for ABM), both row-major FP64.

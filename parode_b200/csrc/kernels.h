@@ -201,6 +201,8 @@ void launch_sinusoid_planes(float* hi, float* lo, int m, int K, const double* a,
                             double base, double dt, long count, cudaStream_t s, long joff = 0);
 // FP64 samples into those planes (n values).  lo may be null in both (hi only).
 void launch_split_planes(const double* U, float* hi, float* lo, long n, cudaStream_t s);
+// dst[i] = (float)src[i], i < n
+void launch_to_float(const double* src, float* dst, long n, cudaStream_t s);
 
 // The batch's discretisation on the device (kernels_disc.cu): one job per
 // system, A (n x n) and B (n x m, m = 0 without B) in, the compact Phi (RK4

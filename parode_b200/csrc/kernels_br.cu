@@ -20,6 +20,7 @@
 // W is built once per plan in FP64 by running the block recurrence on the
 // basis of the window and state columns.
 #include "common.h"
+#include "device_common.cuh"
 #include "kernels.h"
 
 #include <algorithm>
@@ -100,6 +101,110 @@ __global__ void __launch_bounds__(kThreads) k_block_response(const ResponseArgs*
         const int r = e / kCols, c = e - r * kCols, col = c0 + c;
         if (col < ld) a.Wm[(long)(B * p + r) * ld + col] = (col < a.K || col >= a.Kpad) ? z[e] : 0.0;
     }
+}
+
+// The same recurrence for one system with NP <= 64 (a multiple of 8), its
+// product Phi z on the FP64 tensor cores: warp w (< NP / 8) holds Phi's rows
+// 8w .. 8w + 7 as DMMA A fragments in registers and forms those rows of
+// z_{j+1} for the CTA's 8 columns (m8n8k4 over K = NP, four partial chains),
+// the forcing S_j as the accumulators' start; z sits in shared memory with a
+// 12-double row pitch (conflict-free B fragments).  The output rows stay as
+// above.
+template <int NP>
+__global__ void __launch_bounds__(kThreads) k_block_response_mma(const ResponseArgs* __restrict__ args)
+{
+    extern __shared__ double sm[];
+    constexpr int ZP = kCols + 4, MT = NP / 8, KS = NP / 4 < 4 ? NP / 4 : 4;
+    const ResponseArgs a = args[blockIdx.y];
+    const int B = a.B, p = a.p, m = a.m, n = a.n;
+    const int c0 = blockIdx.x * kCols;
+    const int ld = a.Kpad + a.NPstate;
+    if (c0 >= ld) return;
+    const bool rk4 = a.solver == 0;
+    const int W = rk4 ? 3 : 5;
+    const int coff = rk4 ? 0 : 3 * n;
+    double* z = sm;             // NP x ZP
+    double* zn = z + NP * ZP;   // NP x ZP
+    double* sC = zn + NP * ZP;  // p x NP
+    for (int e = threadIdx.x; e < p * NP; e += kThreads) sC[e] = a.Cext[e];
+    // z_0: zero on the window columns, the identity on the state columns
+    for (int e = threadIdx.x; e < NP * ZP; e += kThreads) {
+        const int r = e / ZP, cc = e - r * ZP, col = c0 + cc;
+        z[e] = (cc < kCols && col >= a.Kpad && col - a.Kpad == r) ? 1.0 : 0.0;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+    double qa[NP / 4];
+    if (warp < MT)
+#pragma unroll
+        for (int kk = 0; kk < NP / 4; ++kk) qa[kk] = a.Phi[(warp * 8 + g) * NP + 4 * kk + t];
+    __syncthreads();
+    for (int j = 0; j < B; ++j) {
+        // outputs of step j: Cext z_j + D u_j (u_j: sample 2j for RK4, j + 3 for ABM)
+        const int su = rk4 ? 2 * j : j + 3;
+        for (int e = threadIdx.x; e < p * kCols; e += kThreads) {
+            const int o = e / kCols, c = e - o * kCols, col = c0 + c;
+            if (col >= ld) continue;
+            double v = 0.0;
+            if (col < a.K || col >= a.Kpad) {
+                double v4[4] = {0.0, 0.0, 0.0, 0.0};
+                for (int r = 0; r < NP; r += 4)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) v4[q] = fma(sC[o * NP + r + q], z[(r + q) * ZP + c], v4[q]);
+                v = (v4[0] + v4[1]) + (v4[2] + v4[3]);
+                if (col < a.K && !a.zeroD && m > 0 && col / m == su) v += a.D[(long)o * m + col % m];
+            }
+            a.Wm[(long)(j * p + o) * ld + col] = v;
+        }
+        // z_{j+1} = Phi z_j + S_j, S_j = the forcing of step j on the window
+        if (warp < MT) {
+            const int r = warp * 8 + g;
+            double acc[2];
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int col = c0 + 2 * t + e;
+                double sv = 0.0;
+                if (!a.zeroB && m > 0 && col < a.K && r >= coff && r < coff + n) {
+                    const int sidx = col / m, i = col - sidx * m;
+                    const int w = rk4 ? sidx - 2 * j : sidx - j;  // window slot of sample sidx at step j
+                    if (w >= 0 && w < W) sv = a.Bbar[(long)(r - coff) * W * m + w * m + i];
+                }
+                acc[e] = sv;
+            }
+            double part[KS][2];
+#pragma unroll
+            for (int q = 0; q < KS; ++q) part[q][0] = part[q][1] = 0.0;
+#pragma unroll
+            for (int kk = 0; kk < NP / 4; ++kk)
+                dmma_m8n8k4(part[kk % KS][0], part[kk % KS][1], qa[kk], z[(4 * kk + t) * ZP + g]);
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                double v = acc[e];
+#pragma unroll
+                for (int q = 0; q < KS; ++q) v += part[q][e];
+                zn[r * ZP + 2 * t + e] = v;
+            }
+        }
+        __syncthreads();
+        double* tz = z;
+        z = zn;
+        zn = tz;
+    }
+    // aggregate rows: z_B
+    for (int e = threadIdx.x; e < NP * kCols; e += kThreads) {
+        const int r = e / kCols, c = e - r * kCols, col = c0 + c;
+        if (col < ld) a.Wm[(long)(B * p + r) * ld + col] = (col < a.K || col >= a.Kpad) ? z[r * ZP + c] : 0.0;
+    }
+}
+
+template <int NP>
+void block_response_mma_t(const ResponseArgs* dArgs, int max_p, int max_kpad, cudaStream_t s)
+{
+    const size_t smem = (2 * (size_t)NP * (kCols + 4) + (size_t)max_p * NP) * sizeof(double);
+    if (smem > 220 * 1024) throw Error(kInvalidArgument, "block response: shared memory");
+    PARODE_CUDA(cudaFuncSetAttribute(k_block_response_mma<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid((unsigned)((max_kpad + NP + kCols - 1) / kCols), 1);
+    k_block_response_mma<NP><<<grid, kThreads, smem, s>>>(dArgs);
+    PARODE_CUDA(cudaGetLastError());
 }
 
 // ---------------------------------------------------------------------------
@@ -378,6 +483,19 @@ int response_log2_block(int solver, int NP, int n, int m, int p, long nScan, dou
 void launch_block_response(const ResponseArgs* dArgs, int nsys, int max_np, int max_p, int max_kpad, cudaStream_t s)
 {
     if (nsys <= 0 || max_kpad <= 0) return;
+    if (nsys == 1) {  // one system: its NP is max_np
+        switch (max_np) {
+        case 8: return block_response_mma_t<8>(dArgs, max_p, max_kpad, s);
+        case 16: return block_response_mma_t<16>(dArgs, max_p, max_kpad, s);
+        case 24: return block_response_mma_t<24>(dArgs, max_p, max_kpad, s);
+        case 32: return block_response_mma_t<32>(dArgs, max_p, max_kpad, s);
+        case 40: return block_response_mma_t<40>(dArgs, max_p, max_kpad, s);
+        case 48: return block_response_mma_t<48>(dArgs, max_p, max_kpad, s);
+        case 56: return block_response_mma_t<56>(dArgs, max_p, max_kpad, s);
+        case 64: return block_response_mma_t<64>(dArgs, max_p, max_kpad, s);
+        default: break;
+        }
+    }
     const size_t smem = ((size_t)max_np * max_np + 2 * (size_t)max_np * kCols + (size_t)max_p * max_np) * sizeof(double);
     if (smem > 220 * 1024) throw Error(kInvalidArgument, "block response: shared memory");
     PARODE_CUDA(cudaFuncSetAttribute(k_block_response, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

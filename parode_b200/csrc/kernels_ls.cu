@@ -647,6 +647,22 @@ void launch_sinusoid_planes(float* hi, float* lo, int m, int K, const double* a,
     PARODE_CUDA(cudaGetLastError());
 }
 
+// y rounded to float (the reference C ABI's output arrays), two per thread
+__global__ void k_to_float(const double* __restrict__ src, float* __restrict__ dst, long n)
+{
+    for (long i = 2 * ((long)blockIdx.x * blockDim.x + threadIdx.x); i < n; i += 2L * gridDim.x * blockDim.x) {
+        dst[i] = (float)src[i];
+        if (i + 1 < n) dst[i + 1] = (float)src[i + 1];
+    }
+}
+
+void launch_to_float(const double* src, float* dst, long n, cudaStream_t s)
+{
+    if (n <= 0) return;
+    k_to_float<<<(unsigned)std::min<long>((n / 2 + 255) / 256 + 1, 148L * 16), 256, 0, s>>>(src, dst, n);
+    PARODE_CUDA(cudaGetLastError());
+}
+
 void launch_split_planes(const double* U, float* hi, float* lo, long n, cudaStream_t s)
 {
     if (n <= 0) return;

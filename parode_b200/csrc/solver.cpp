@@ -1282,6 +1282,39 @@ void Plan::execute_blocked(double* Y, cudaStream_t s)
     last_y_ = Y;
 }
 
+void Plan::get_output_f32(float* t, float* y)
+{
+    PARODE_CUDA(cudaSetDevice(device_));
+    if (batch_ || shards_ > 1) {
+        // through the FP64 copy
+        std::vector<double> td(t ? (size_t)nOut_ : 0), yd(y ? (size_t)nOut_ * p_ : 0);
+        get_output(t ? td.data() : nullptr, y ? yd.data() : nullptr);
+        for (size_t k = 0; k < td.size(); ++k) t[k] = (float)td[k];
+        for (size_t k = 0; k < yd.size(); ++k) y[k] = (float)yd[k];
+        return;
+    }
+    // y rounded to float on the device, then half the bytes cross the link;
+    // the host writes the float time vector meanwhile
+    PARODE_CUDA(cudaStreamWaitEvent(stream_, done_, 0));
+    float* dF = nullptr;
+    const long ny = nOut_ * (long)p_;
+    if (y) {
+        if (fault_alloc_now()) throw Error(kNotEnoughResources, "device allocation failed (injected)");
+        if (cudaMallocAsync((void**)&dF, sizeof(float) * (size_t)std::max<long>(ny, 1), stream_) != cudaSuccess) {
+            cudaGetLastError();
+            throw Error(kNotEnoughResources, "device allocation failed");
+        }
+        launch_to_float(last_y_ ? last_y_ : dY_, dF, ny, stream_);
+        PARODE_CUDA(cudaMemcpyAsync(y, dF, sizeof(float) * (size_t)ny, cudaMemcpyDeviceToHost, stream_));
+        PARODE_CUDA(cudaFreeAsync(dF, stream_));
+    }
+    if (t) time_vector_f(solver_, t0_, tEnd_, h_, t);
+    PARODE_CUDA(cudaStreamSynchronize(stream_));
+    int status = 0;
+    PARODE_CUDA(cudaMemcpy(&status, dStatus_, sizeof(int), cudaMemcpyDeviceToHost));
+    if (status != 0) throw Error(kDeviceError, "a device-side wait gave up (tensor-core completion not observed)");
+}
+
 void Plan::get_output(double* t, double* y)
 {
     PARODE_CUDA(cudaSetDevice(device_));

@@ -74,6 +74,7 @@ public:
     void execute(double* y, cudaStream_t s);
     // Synchronise and copy the last result (and the time vector) to the host.
     void get_output(double* t, double* y);
+    void get_output_f32(float* t, float* y);  // the same values rounded to float (y on the device)
 
     long num_outputs() const { return nOut_; }
     long scan_steps() const { return nScan_; }
