@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <thread>
 
 namespace parode {
 
@@ -102,6 +103,69 @@ void time_chain_t(T* tv, long count, double h)
     }
 }
 
+// The same chain on several host threads, every element still exactly the
+// chain's.  Within a float binade [2^e, 2^(e+1)) the link adds a constant
+// (the step rounded to the binade's spacing; an exact tie would alternate),
+// so a walk over the binades -- a few dozen links -- predicts the value at any
+// index.  Each thread fills its slice from the predicted start by the checked
+// speculation above; then the first link into every slice is checked in order
+// and a slice whose start was mispredicted is filled again from the true one.
+// Negative times (whose spacing shrinks towards zero) run on one thread.
+template <class T>
+void time_chain_par(T* tv, long count, double h)
+{
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int P = (int)std::min<unsigned>(std::max(1u, hw / 2), 8u);
+    if (count < (1L << 16) || P <= 1 || !((double)tv[0] >= 0.0)) return time_chain_t<T>(tv, count, h);
+    // binade runs: from index s the values are v + k d while below hi
+    struct Run {
+        long s;
+        double v, d;
+    };
+    std::vector<Run> runs;
+    long s = 0;
+    double v = tv[0];
+    while (s < count - 1 && runs.size() < 4096) {
+        const double d = time_link(v, h) - v;
+        runs.push_back({s, v, d});
+        if (!(d > 0.0)) break;  // a step below the spacing: the chain stalls
+        long k = 1;
+        if (v > 0.0) {
+            int e = 0;
+            std::frexp(v, &e);
+            const double hi = std::ldexp(1.0, e);  // v in [hi / 2, hi)
+            k = std::max(1L, (long)((hi - v) / d));
+            while (k > 1 && v + (double)k * d >= hi) --k;
+            while (v + (double)(k + 1) * d < hi) ++k;
+        }
+        if (s + k >= count - 1) break;
+        s += k + 1;
+        v = time_link(v + (double)k * d, h);
+    }
+    auto predict = [&](long i) {
+        const Run* r = &runs[0];
+        for (const Run& q : runs)
+            if (q.s <= i) r = &q;
+        return r->v + (double)(i - r->s) * r->d;
+    };
+    std::vector<long> a(P + 1);
+    for (int t = 0; t <= P; ++t) a[t] = count * t / P;
+    std::vector<std::thread> th;
+    for (int t = 1; t < P; ++t)
+        th.emplace_back([&, t] {
+            tv[a[t]] = (T)predict(a[t]);
+            time_chain_t<T>(tv + a[t], a[t + 1] - a[t], h);
+        });
+    time_chain_t<T>(tv, a[1], h);
+    for (auto& x : th) x.join();
+    for (int t = 1; t < P; ++t) {
+        const T want = (T)time_link((double)tv[a[t] - 1], h);
+        if (tv[a[t]] == want) continue;
+        tv[a[t]] = want;
+        time_chain_t<T>(tv + a[t], a[t + 1] - a[t], h);
+    }
+}
+
 void time_chain(double* tv, long count, double h) { time_chain_t<double>(tv, count, h); }
 
 template <class T>
@@ -114,7 +178,7 @@ void time_vector_t(int solver, double t0, double tEnd, double h, T* tv)
     double ts = (solver == 1) ? t0 + 3.0 * h : t0;
     for (long i = 0; i < pre; ++i) tv[i] = (T)(float)(ts - (double)(pre - i) * h);
     tv[pre] = (T)(float)ts;
-    time_chain_t<T>(tv + pre, ns, h);
+    time_chain_par<T>(tv + pre, ns, h);
 }
 
 void time_vector(int solver, double t0, double tEnd, double h, double* tv) { time_vector_t<double>(solver, t0, tEnd, h, tv); }
