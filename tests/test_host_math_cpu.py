@@ -178,3 +178,58 @@ def test_time_vector_is_the_reference_accumulation(tmp_path):
     out = subprocess.run([str(exe)], capture_output=True, text=True)
     assert out.returncode == 0, out.stdout[-2000:]
     assert "bad 0" in out.stdout
+
+
+TIME_DRIVER = r"""
+#include "host_math.h"
+#include <cstdio>
+#include <vector>
+using namespace parode;
+int main()
+{
+    // (solver, t0, h, steps): one thread and several, ties of the float
+    // rounding (h = 1.5 2^-12), a negative start, late starts, a tiny step
+    struct C { int solver; double t0, h; long steps; };
+    const C cs[] = {{0, 0.0, 1e-4, 1L << 20}, {1, 0.0, 1e-3, 300000}, {0, 0.5, 3e-5, 1500000},
+                    {0, 0.0, 1.5 / 4096.0, 400000}, {0, -2.0, 1e-4, 300000}, {0, 1000.0, 1e-3, 300000},
+                    {0, 0.0, 1e-7, 300000}, {1, 3.0, 0.1, 70000}, {0, 0.25, 1e-3, 1000}};
+    for (const C& c : cs) {
+        const double t1 = c.t0 + (double)(c.steps - 1) * c.h;
+        long ns = 0;
+        const long T = num_outputs(c.solver, c.t0, t1, c.h, &ns);
+        std::vector<double> td((size_t)T), ref((size_t)T);
+        std::vector<float> tf((size_t)T);
+        time_vector(c.solver, c.t0, t1, c.h, td.data());
+        time_vector_f(c.solver, c.t0, t1, c.h, tf.data());
+        // the plain sequential chain
+        const long pre = T - ns;
+        const double ts = c.solver == 1 ? c.t0 + 3.0 * c.h : c.t0;
+        for (long i = 0; i < pre; ++i) ref[i] = (double)(float)(ts - (double)(pre - i) * c.h);
+        ref[pre] = (double)(float)ts;
+        for (long i = pre; i + 1 < T; ++i) ref[i + 1] = (double)(float)(ref[i] + c.h);
+        long bad = 0;
+        for (long i = 0; i < T; ++i) bad += (td[i] != ref[i]) + ((double)tf[i] != ref[i]);
+        std::printf("%ld %ld\n", T, bad);
+    }
+    return 0;
+}
+"""
+
+
+def test_time_vector_is_the_sequential_float_chain(tmp_path):
+    """time_vector / time_vector_f (speculated, and split over host threads
+    from binade-predicted slice starts) equal the plain link-by-link float
+    chain element for element."""
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("g++ not available")
+    drv = tmp_path / "tv.cpp"
+    drv.write_text(TIME_DRIVER)
+    exe = tmp_path / "tv"
+    subprocess.run([gxx, "-O2", "-std=c++17", "-ffp-contract=off", "-pthread", "-I", CSRC, str(drv),
+                    os.path.join(CSRC, "host_math.cpp"), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    rows = [tuple(int(v) for v in line.split()) for line in out.strip().splitlines()]
+    assert len(rows) == 9
+    for T, bad in rows:
+        assert T > 0 and bad == 0, (T, bad)
