@@ -180,7 +180,7 @@ def test_time_vector_is_the_reference_accumulation(tmp_path):
     assert "bad 0" in out.stdout
 
 
-TIME_DRIVER = r"""
+CHAIN_DRIVER = r"""
 #include "host_math.h"
 #include <cstdio>
 #include <vector>
@@ -224,7 +224,7 @@ def test_time_vector_is_the_sequential_float_chain(tmp_path):
     if gxx is None:
         pytest.skip("g++ not available")
     drv = tmp_path / "tv.cpp"
-    drv.write_text(TIME_DRIVER)
+    drv.write_text(CHAIN_DRIVER)
     exe = tmp_path / "tv"
     subprocess.run([gxx, "-O2", "-std=c++17", "-ffp-contract=off", "-pthread", "-I", CSRC, str(drv),
                     os.path.join(CSRC, "host_math.cpp"), "-o", str(exe)], check=True)
