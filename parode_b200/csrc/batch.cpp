@@ -55,6 +55,10 @@ constexpr double kHostDiscMaxBatch = 8e6;
 template <class F>
 void parallel_for(int n, F&& f)
 {
+    if (n <= 1) {  // one item: no thread to start (a server's small batches)
+        if (n == 1) f(0);
+        return;
+    }
     int nt = (int)std::min<unsigned>(std::max(1u, std::thread::hardware_concurrency()), 32u);
     nt = std::min(nt, std::max(1, n));
     std::vector<std::thread> th;
@@ -1080,7 +1084,15 @@ void BatchPlan::build(std::vector<BatchSpec> specs, InputRegistry* inputs, const
         for (int l = 1; l < Pmax; ++l) tasks.push_back(LevelTask{&ls_power_, l, -1, 0, {}});  // the power table stays FP64
         for (int l = 0; l < Lmax; ++l) tasks.push_back(LevelTask{&ls_up_, l, l, 1, {}});
         for (int l = Lmax - 1; l >= 0; --l) tasks.push_back(LevelTask{&ls_down_, l, l, 2, {}});
-        parallel_for((int)tasks.size(), [&](int t) {
+        // few systems: the levels are prepared inline (starting a thread per
+        // level costs more than their work)
+        auto over_tasks = [&](auto&& body) {
+            if (lv.size() < 32)
+                for (int t = 0; t < (int)tasks.size(); ++t) body(t);
+            else
+                parallel_for((int)tasks.size(), body);
+        };
+        over_tasks([&](int t) {
             // the tensor-map encoder needs the device's context current on this thread
             PARODE_CUDA(cudaSetDevice(device_));
             LevelTask& T = tasks[t];
