@@ -208,7 +208,7 @@ void launch_to_float(const double* src, float* dst, long n, cudaStream_t s);
 // system, A (n x n) and B (n x m, m = 0 without B) in, the compact Phi (RK4
 // n x n; ABM the last block row, n x 4n), Bbar (n x W max(m, 1), W = 3 / 5)
 // and, when bbarT is set, its transpose out, with ||Phi - R||_inf into
-// *delta; work: discretise_work_doubles(n, m) doubles.  The same bits as the
+// *delta when delta is set; work: discretise_work_doubles(n, m) doubles.  The same bits as the
 // host restatement (host_math.cpp).  The products run first, as 32 x 32
 // output tiles in three dependency stages (discretise_tiles lists a job's
 // tiles of one stage, with the job's device pointers).

@@ -156,7 +156,9 @@ __global__ void __launch_bounds__(kThreads) k_discretise_finish(const DiscJob* _
             jb.bbarT[(long)c * n + r] = jb.bbar[e];
         }
     }
-    // ||Phi - R||_inf over the stored rows (each row summed in order)
+    // ||Phi - R||_inf over the stored rows (each row summed in order), when
+    // asked for (a batch sizes its layout with it; a single plan does not)
+    if (!jb.delta) return;
     __shared__ double rowmax[kThreads];
     const int d0 = jb.solver == 0 ? 0 : 3 * n;
     double dmax = 0.0;

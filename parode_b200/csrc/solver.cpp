@@ -319,7 +319,7 @@ void Plan::build(int device, const SystemDesc& sys, InputRegistry* inputs, int u
     want.emplace_back(&dBbar_, (long)n * W * std::max(mB, 1));
     // the discretisation's inputs and work (kernels_disc.cu: the host
     // restatement's operation order, so the same bits as host_math.cpp)
-    double *dDA = nullptr, *dDB = nullptr, *dPhiC = nullptr, *dDWork = nullptr, *dDelta = nullptr;
+    double *dDA = nullptr, *dDB = nullptr, *dPhiC = nullptr, *dDWork = nullptr;
     double *dDJob = nullptr, *dPhiJob = nullptr;
     double* dTiles[3] = {nullptr, nullptr, nullptr};
     long ntiles[3] = {0, 0, 0};
@@ -331,7 +331,6 @@ void Plan::build(int device, const SystemDesc& sys, InputRegistry* inputs, int u
         if (mB) want.emplace_back(&dDB, (long)n * mB);
         want.emplace_back(&dPhiC, (long)n * Ns_);
         want.emplace_back(&dDWork, discretise_work_doubles(n, mB));
-        want.emplace_back(&dDelta, 1);
         want.emplace_back(&dDJob, words(sizeof(DiscJob)));
         want.emplace_back(&dPhiJob, words(sizeof(PhiJob)));
         for (int st = 0; st < 3; ++st)
@@ -434,7 +433,7 @@ void Plan::build(int device, const SystemDesc& sys, InputRegistry* inputs, int u
         j.phi = dPhiC;
         j.bbar = dBbar_;
         j.work = dDWork;
-        j.delta = dDelta;
+        j.delta = nullptr;  // the distance to the exact part sizes batch layouts only
         j.n = n;
         j.m = mB;
         j.solver = solver;
