@@ -488,20 +488,31 @@ class Batch:
     def __init__(self, systems, precision: int = FP64):
         N = len(systems)
         keep = []
-        arrs = {k: (C.c_void_p * N)() for k in ("A", "B", "C", "D", "x0")}
-        ints = {k: (C.c_int * N)() for k in ("m", "n", "p", "zB", "zC", "zD", "u", "solver")}
-        dbl = {k: (C.c_double * N)() for k in ("t0", "t1", "h")}
-        for i, s in enumerate(systems):
+        cols = {k: [] for k in ("A", "B", "C", "D", "x0", "m", "n", "p", "zB", "zC", "zD", "u", "solver", "t0", "t1",
+                                "h")}
+        for s in systems:
             A, B, Cm, D, x0, n, m, p = _sys_arrays(s["A"], s.get("B"), s.get("C"), s.get("D"), s["x0"])
             for k, v in (("A", A), ("B", B), ("C", Cm), ("D", D), ("x0", x0)):
                 if v is not None:
                     keep.append(v)
-                    arrs[k][i] = v.ctypes.data
-            ints["m"][i], ints["n"][i], ints["p"][i] = m, n, p
-            ints["zB"][i], ints["zC"][i], ints["zD"][i] = int(B is None), int(Cm is None), int(D is None)
-            ints["u"][i] = int(s.get("u", 0))
-            ints["solver"][i] = int(s.get("solver", RK4))
-            dbl["t0"][i], dbl["t1"][i], dbl["h"][i] = s["t0"], s["t_end"], s["h"]
+                    cols[k].append(v.ctypes.data)
+                else:
+                    cols[k].append(None)
+            cols["m"].append(m)
+            cols["n"].append(n)
+            cols["p"].append(p)
+            cols["zB"].append(int(B is None))
+            cols["zC"].append(int(Cm is None))
+            cols["zD"].append(int(D is None))
+            cols["u"].append(int(s.get("u", 0)))
+            cols["solver"].append(int(s.get("solver", RK4)))
+            cols["t0"].append(s["t0"])
+            cols["t1"].append(s["t_end"])
+            cols["h"].append(s["h"])
+        # the argument arrays built in bulk (one ctypes construction each)
+        arrs = {k: (C.c_void_p * N)(*cols[k]) for k in ("A", "B", "C", "D", "x0")}
+        ints = {k: (C.c_int * N)(*cols[k]) for k in ("m", "n", "p", "zB", "zC", "zD", "u", "solver")}
+        dbl = {k: (C.c_double * N)(*cols[k]) for k in ("t0", "t1", "h")}
         e = C.c_int(0)
         ip = lambda a: C.cast(a, C.POINTER(C.c_int))
         dpp = lambda a: C.cast(a, C.POINTER(C.c_double))
@@ -512,8 +523,21 @@ class Batch:
                                          vp(arrs["x0"]), ip(ints["solver"]), precision, C.byref(e))
         _check(e, "ParODE_BatchCreate")
         self.size = N
-        self.num_outputs = [int(lib.ParODE_BatchNumOutputs(self._h, i)) for i in range(N)]
-        self.channels = [int(lib.ParODE_BatchNumOutputChannels(self._h, i)) for i in range(N)]
+        self._shapes = None  # (outputs, channels) per system, read on first use
+
+    def _shape_lists(self):
+        if self._shapes is None:
+            self._shapes = ([int(lib.ParODE_BatchNumOutputs(self._h, i)) for i in range(self.size)],
+                            [int(lib.ParODE_BatchNumOutputChannels(self._h, i)) for i in range(self.size)])
+        return self._shapes
+
+    @property
+    def num_outputs(self):
+        return self._shape_lists()[0]
+
+    @property
+    def channels(self):
+        return self._shape_lists()[1]
 
     def execute(self, stream: int = 0) -> None:
         e = C.c_int(0)
