@@ -262,7 +262,24 @@ def register_sinusoid(a, f, phi) -> int:
     return idx.value
 
 
+def _f64(a):
+    """a as a C-contiguous float64 array (itself when it already is one)."""
+    if type(a) is np.ndarray and a.dtype == np.float64 and a.flags.c_contiguous:
+        return a
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
 def _sys_arrays(A, B, Cm, D, x0):
+    if (type(A) is np.ndarray and type(x0) is np.ndarray and A.ndim == 2 and A.dtype == np.float64 and
+            A.flags.c_contiguous and x0.dtype == np.float64 and x0.flags.c_contiguous):
+        # already C-contiguous float64 (a batch of thousands passes here)
+        B = None if B is None or np.size(B) == 0 else _f64(B)
+        Cm = None if Cm is None or np.size(Cm) == 0 else _f64(Cm)
+        D = None if D is None or np.size(D) == 0 else _f64(D)
+        n = A.shape[0]
+        m = B.shape[1] if B is not None else (D.shape[1] if D is not None else 0)
+        p = Cm.shape[0] if Cm is not None else (D.shape[0] if D is not None else 0)
+        return A, B, Cm, D, x0, n, m, p
     A = np.ascontiguousarray(A, dtype=np.float64)
     n = A.shape[0]
     B = None if B is None or np.size(B) == 0 else np.ascontiguousarray(B, dtype=np.float64)
