@@ -384,6 +384,22 @@ void BatchPlan::build(std::vector<BatchSpec> specs, InputRegistry* inputs, const
     const bool disc_host = opt.discretise == kDiscHost || (opt.discretise == kDiscAuto &&
                                                             disc_max <= kHostDiscMaxSystem &&
                                                             disc_total <= kHostDiscMaxBatch);
+    // the device discretisation runs while the host sets up the constants and
+    // the ABM start-up; its distances are read just before the layout needs
+    // them (its stream, staged inputs and pinned readback live until then; the
+    // guard waits for the stream before they go, also when a step fails)
+    cudaStream_t dstream = nullptr;
+    std::unique_ptr<HostStage> dstage, ddelta;
+    struct StreamGuard {
+        cudaStream_t* s;
+        ~StreamGuard()
+        {
+            if (*s) {
+                cudaStreamSynchronize(*s);
+                cudaStreamDestroy(*s);
+            }
+        }
+    } dguard{&dstream};
     if (disc_host) {
         Layout D;
         for (int i = 0; i < N; ++i) {
@@ -415,20 +431,11 @@ void BatchPlan::build(std::vector<BatchSpec> specs, InputRegistry* inputs, const
         // back.  The set-up waits for it, so it runs on a stream of the
         // greatest priority: a batch set up while others execute is not
         // queued behind their kernels.
-        cudaStream_t dstream = nullptr;
         {
             int least = 0, greatest = 0;
             PARODE_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
             PARODE_CUDA(cudaStreamCreateWithPriority(&dstream, cudaStreamNonBlocking, greatest));
         }
-        struct StreamGuard {
-            cudaStream_t s;
-            ~StreamGuard()
-            {
-                cudaStreamSynchronize(s);
-                cudaStreamDestroy(s);
-            }
-        } dguard{dstream};
         Layout D;
         for (int i = 0; i < N; ++i) {  // staged inputs first
             const SystemDesc& s = specs[i].sys;
@@ -466,8 +473,8 @@ void BatchPlan::build(std::vector<BatchSpec> specs, InputRegistry* inputs, const
             throw Error(kNotEnoughResources, "batch discretisation buffer allocation failed");
         }
         char* db = static_cast<char*>(disc_);
-        HostStage hsp(staged);  // gaps are copied, never read; released after the synchronise below
-        char* hs_data = hsp.data();
+        dstage = std::make_unique<HostStage>(staged);  // gaps are copied, never read
+        char* hs_data = dstage->data();
         std::vector<DiscJob> jobs(N);
         parallel_for(N, [&](int i) {
             const SystemDesc& s = specs[i].sys;
@@ -500,11 +507,9 @@ void BatchPlan::build(std::vector<BatchSpec> specs, InputRegistry* inputs, const
         }
         PARODE_CUDA(cudaMemcpyAsync(db, hs_data, staged, cudaMemcpyHostToDevice, dstream));
         launch_discretise_batch(reinterpret_cast<const DiscJob*>(db + jobs_at), N, dtiles, ntiles, sms_, dstream);
-        std::vector<double> deltas((size_t)N);
-        PARODE_CUDA(cudaMemcpyAsync(deltas.data(), db + delta_at, sizeof(double) * (size_t)N, cudaMemcpyDeviceToHost,
+        ddelta = std::make_unique<HostStage>(sizeof(double) * (size_t)N);
+        PARODE_CUDA(cudaMemcpyAsync(ddelta->data(), db + delta_at, sizeof(double) * (size_t)N, cudaMemcpyDeviceToHost,
                                     dstream));
-        PARODE_CUDA(cudaStreamSynchronize(dstream));
-        for (int i = 0; i < N; ++i) sys_[i].delta = deltas[(size_t)i];
         }
     phase(disc_host ? "discretise (host)" : "discretise (device)", false);
     // ---- constant region: layout first, then the host set-up (threads over
@@ -636,6 +641,12 @@ void BatchPlan::build(std::vector<BatchSpec> specs, InputRegistry* inputs, const
         }
     });
     phase("abm-start-up", false);
+    if (dstream) {
+        PARODE_CUDA(cudaStreamSynchronize(dstream));
+        const double* dl = reinterpret_cast<const double*>(ddelta->data());
+        for (int i = 0; i < N; ++i) sys_[i].delta = dl[i];
+        phase("distances", false);
+    }
     const size_t const_end = L.bytes;
     // work buffers (offsets only; not staged); per-kind totals for the log
     size_t kind_bytes[5] = {0, 0, 0, 0, 0};  // power tables + scan vectors, W, W split, samples, outputs
