@@ -334,16 +334,16 @@ void SimulateODE(fType A[], fType B[], fType C[], fType D[], int* nInputs, int* 
         Plan plan(dev, s, &L.inputs, *uIndex, *solver, *tStart, *tEnd, *tStep, opt);
         long T = plan.num_outputs();
         // fType is float: y is rounded on the device and copied straight into
-        // xVect, and the time vector is written as float on a helper thread
+        // xVect range by range while the later ranges are formed, and the time
+        // vector is written as float on a helper thread
         static_assert(sizeof(fType) == sizeof(float), "the reference ABI's fType is float");
         HelperThread tv;
         const int sv = *solver;
         const double t0 = *tStart, t1 = *tEnd, h = *tStep;
         float* tOut = reinterpret_cast<float*>(tVect);
         if (tVect) tv.run([tOut, sv, t0, t1, h] { time_vector_f(sv, t0, t1, h, tOut); });
-        plan.execute(nullptr, nullptr);
         try {
-            plan.get_output_f32(nullptr, reinterpret_cast<float*>(xVect));
+            plan.solve_to_host(nullptr, reinterpret_cast<float*>(xVect));
         } catch (...) {
             tv.join();
             throw;
@@ -535,8 +535,12 @@ void ParODE_SimulateODE_d(const double* A, const double* B, const double* C, con
         // is set up, solved and its outputs copied
         HelperThread tv;
         if (tVect) tv.run([=] { time_vector(solver, tStart, tEnd, tStep, tVect); });
-        plan.execute(nullptr, nullptr);
-        plan.get_output(nullptr, yVect);
+        try {
+            plan.solve_to_host(yVect, nullptr);
+        } catch (...) {
+            tv.join();
+            throw;
+        }
         tv.join();
         if (nSteps) nSteps[0] = plan.num_outputs();
     });

@@ -1031,14 +1031,18 @@ LevelArgs Plan::response_out_args(double* Y) const
     return h;
 }
 
-void Plan::state_part(double* Y, cudaStream_t s)
+void Plan::state_part(double* Y, long c0, long c1, cudaStream_t s)
 {
-    // mixed: y = windows + (C Phi^j) X_b, W's state columns resident in shared
-    // memory (kernels_state.cu); the general tiled GEMM where they do not fit
+    // mixed: y = windows + (C Phi^j) X_b over blocks [c0, c1), W's state
+    // columns resident in shared memory (kernels_state.cu); the general tiled
+    // GEMM where they do not fit.  A block's result does not depend on the
+    // range it is formed in.
     const int ybase = solver_ == kRK4 ? 0 : 3;
     const long ld = brKpad_ + Np_;
-    if (launch_state_out(Np_, dW_ + brKpad_, ld, shape_.B * p_, dG_, dY_ + ybase * p_, Y + ybase * p_,
-                         (long)shape_.B * p_, nblocks_, nScan_ * p_, sms_, s))
+    const long gs = (long)shape_.B * p_;
+    const long off = ybase * p_ + c0 * gs;
+    if (launch_state_out(Np_, dW_ + brKpad_, ld, shape_.B * p_, dG_ + c0 * Np_, dY_ + off, Y + off, gs, c1 - c0,
+                         nScan_ * p_ - c0 * gs, sms_, s))
         return;
     LevelArgs x;
     x.P = dW_ + brKpad_;
@@ -1046,25 +1050,23 @@ void Plan::state_part(double* Y, cudaStream_t s)
     x.Np = Np_;
     x.M = shape_.B * p_;
     x.K = Np_;
-    x.ncols = nblocks_;
-    x.src = dG_;
+    x.ncols = c1 - c0;
+    x.src = dG_ + c0 * Np_;
     x.src_gs = Np_;
     x.src_ks = 1;
-    x.acc = dY_ + ybase * p_;
-    x.acc_gs = (long)shape_.B * p_;
-    x.dst = Y + ybase * p_;
-    x.dst_gs = (long)shape_.B * p_;
-    x.dst_limit = nScan_ * p_;
+    x.acc = dY_ + off;
+    x.acc_gs = gs;
+    x.dst = Y + off;
+    x.dst_gs = gs;
+    x.dst_limit = nScan_ * p_ - c0 * gs;
     launch_gemm_tiled(x, s);
 }
 
-void Plan::execute_response(double* Y, cudaStream_t s)
+int Plan::response_head(cudaStream_t s)
 {
     // leaf = W x [sample window; initial state] per block (kernels_br.cu):
-    // aggregates first (the state columns are not used), then the carry, then
-    // the outputs with the carried block states, written straight into y
-    // (rows (j, o) of block b are contiguous there).  The power table
-    // P_1..P_levels was formed with W when the plan was made.
+    // aggregates first (the state columns are not used), then the carry.  The
+    // power table P_1..P_levels was formed with W when the plan was made.
     int launches = 0;
     marks_.clear();
     mark("start", s);
@@ -1072,34 +1074,111 @@ void Plan::execute_response(double* Y, cudaStream_t s)
     ++launches;
     mark("inputs", s);
     if (br_tc_) {
-        // mixed: aggregates and output windows (tensor cores) -> carry ->
-        // y = windows + C Phi^j X_b (FP64)
+        // mixed: aggregates and output windows on the tensor cores
         launch_resp_tc(dResp_, dTcStart_, 2, dTcCta_, tcCtas_, dStatus_, one_pass_, s);
         ++launches;
         mark("aggregates+windows", s);
-        launches += carry(s);
-        mark("carry", s);
-        state_part(Y, s);
+    } else {
+        launch_gemm_tiled(response_agg_args(), s);
         ++launches;
-        if (solver_ == kABM)
-            PARODE_CUDA(cudaMemcpyAsync(Y, dYpre_, sizeof(double) * 3 * p_, cudaMemcpyDeviceToDevice, s));
-        mark("outputs", s);
-        launches_ = launches;
-        last_y_ = Y;
-        return;
+        mark("aggregates", s);
     }
-    launch_gemm_tiled(response_agg_args(), s);
-    ++launches;
-    mark("aggregates", s);
     launches += carry(s);
     mark("carry", s);
-    launch_gemm_tiled(response_out_args(Y), s);
+    return launches;
+}
+
+void Plan::response_outputs(double* Y, long c0, long c1, cudaStream_t s)
+{
+    // the outputs of blocks [c0, c1) with their carried states, written
+    // straight into y (rows (j, o) of block b are contiguous there)
+    if (br_tc_) {
+        state_part(Y, c0, c1, s);  // y = windows + C Phi^j X_b (FP64)
+        return;
+    }
+    LevelArgs h = response_out_args(Y);
+    h.src += c0 * h.src_gs;
+    h.src2 += c0 * h.src2_gs;
+    h.dst += c0 * h.dst_gs;
+    h.dst_limit -= c0 * h.dst_gs;
+    h.ncols = c1 - c0;
+    launch_gemm_tiled(h, s);
+}
+
+void Plan::execute_response(double* Y, cudaStream_t s)
+{
+    int launches = response_head(s);
+    response_outputs(Y, 0, nblocks_, s);
     ++launches;
     if (solver_ == kABM)
         PARODE_CUDA(cudaMemcpyAsync(Y, dYpre_, sizeof(double) * 3 * p_, cudaMemcpyDeviceToDevice, s));
     mark("outputs", s);
     launches_ = launches;
     last_y_ = Y;
+}
+
+void Plan::solve_to_host(double* yd, float* yf)
+{
+    void* y = yf ? (void*)yf : (void*)yd;
+    if (!y || batch_ || shards_ > 1 || path_ != kPathBlocked || !br_ || profiling_ || nblocks_ < 8) {
+        execute(nullptr, nullptr);
+        if (yf)
+            get_output_f32(nullptr, yf);
+        else
+            get_output(nullptr, yd);
+        return;
+    }
+    PARODE_CUDA(cudaSetDevice(device_));
+    cudaStream_t s = stream_;
+    int launches = response_head(s);
+    float* dF = nullptr;
+    const long total = nOut_ * (long)p_;
+    if (yf) {
+        if (fault_alloc_now()) throw Error(kNotEnoughResources, "device allocation failed (injected)");
+        if (cudaMallocAsync((void**)&dF, sizeof(float) * (size_t)std::max<long>(total, 1), s) != cudaSuccess) {
+            cudaGetLastError();
+            throw Error(kNotEnoughResources, "device allocation failed");
+        }
+    }
+    // block ranges: an eighth first (its copy starts soonest), then two
+    // quarters and the rest; range k's rows of y are [r[k], r[k + 1]) (the
+    // first also holds the ABM start-up rows, the last the ragged tail)
+    const long gs = (long)shape_.B * p_, base = (solver_ == kRK4 ? 0 : 3) * (long)p_;
+    const long cut[5] = {0, nblocks_ / 8, 3 * nblocks_ / 8, 5 * nblocks_ / 8, nblocks_};
+    long r[5] = {0, 0, 0, 0, total};
+    for (int k = 1; k < 4; ++k) r[k] = std::min(total, base + cut[k] * gs);
+    for (int k = 0; k < 4; ++k) {
+        response_outputs(dY_, cut[k], cut[k + 1], s);
+        ++launches;
+        if (k == 0 && solver_ == kABM)
+            PARODE_CUDA(cudaMemcpyAsync(dY_, dYpre_, sizeof(double) * 3 * p_, cudaMemcpyDeviceToDevice, s));
+        if (dF) {
+            launch_to_float(dY_ + r[k], dF + r[k], r[k + 1] - r[k], s);
+            ++launches;
+        }
+        PARODE_CUDA(cudaEventRecord(fork_[k], s));
+    }
+    // the copies on the side stream, each after its range (issued after all
+    // the ranges, so a pageable destination that blocks the host per copy
+    // does not hold back the device's work)
+    const size_t es = dF ? sizeof(float) : sizeof(double);
+    for (int k = 0; k < 4; ++k) {
+        if (r[k + 1] <= r[k]) continue;
+        PARODE_CUDA(cudaStreamWaitEvent(side_, fork_[k], 0));
+        const void* src = dF ? (const void*)(dF + r[k]) : (const void*)(dY_ + r[k]);
+        PARODE_CUDA(cudaMemcpyAsync((char*)y + es * (size_t)r[k], src, es * (size_t)(r[k + 1] - r[k]),
+                                    cudaMemcpyDeviceToHost, side_));
+    }
+    PARODE_CUDA(cudaEventRecord(fork_[0], side_));
+    PARODE_CUDA(cudaStreamWaitEvent(s, fork_[0], 0));
+    if (dF) PARODE_CUDA(cudaFreeAsync(dF, s));
+    PARODE_CUDA(cudaEventRecord(done_, s));
+    launches_ = launches;
+    last_y_ = dY_;
+    PARODE_CUDA(cudaStreamSynchronize(s));
+    int status = 0;
+    PARODE_CUDA(cudaMemcpy(&status, dStatus_, sizeof(int), cudaMemcpyDeviceToHost));
+    if (status != 0) throw Error(kDeviceError, "a device-side wait gave up (tensor-core completion not observed)");
 }
 
 void Plan::setup_shard(const PlanOptions& opt)
@@ -1188,8 +1267,7 @@ void Plan::shard_down(const double* dGathered, double* Y, cudaStream_t s)
         L.arr[L.h] = const_cast<double*>(mine);
         launch_chunk_down(Np_, L, dPow_, shape_.R, s);
     }
-    if (br_tc_) state_part(Y, s);
-    else launch_gemm_tiled(response_out_args(Y), s);
+    response_outputs(Y, 0, nblocks_, s);
     if (solver_ == kABM && shard_ == 0)
         PARODE_CUDA(cudaMemcpyAsync(Y, dYpre_, sizeof(double) * 3 * p_, cudaMemcpyDeviceToDevice, s));
     PARODE_CUDA(cudaEventRecord(done_, s));

@@ -75,6 +75,12 @@ public:
     // Synchronise and copy the last result (and the time vector) to the host.
     void get_output(double* t, double* y);
     void get_output_f32(float* t, float* y);  // the same values rounded to float (y on the device)
+    // One-shot execute with y copied to the host (yd as double, or yf rounded
+    // to float on the device; at most one non-null): on the block-response
+    // path the output stage runs over four block ranges and each range's rows
+    // are copied out on the side stream while the later ranges are formed.
+    // The same bits as execute followed by get_output / get_output_f32.
+    void solve_to_host(double* yd, float* yf);
 
     long num_outputs() const { return nOut_; }
     long scan_steps() const { return nScan_; }
@@ -126,7 +132,9 @@ private:
     int carry(cudaStream_t s);
     LevelArgs response_agg_args() const;
     LevelArgs response_out_args(double* Y) const;
-    void state_part(double* Y, cudaStream_t s);
+    int response_head(cudaStream_t s);  // inputs, aggregates, carry; returns the launches
+    void response_outputs(double* Y, long c0, long c1, cudaStream_t s);  // blocks [c0, c1)
+    void state_part(double* Y, long c0, long c1, cudaStream_t s);
     void setup_shard(const PlanOptions& opt);
     void fill_inputs(cudaStream_t s);
 
