@@ -726,7 +726,8 @@ def run_ours(args):
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "ms_per_step": med,
                "statistic": f"median of {len(ms)} calls", "mean_ms": statistics.mean(ms), "max_ms": max(ms),
                "call": "SimulateODE, the reference's C ABI (float arrays in, t and y out into pinned host memory "
-                       "reused across calls; y rounded to float on the device), precision mode mixed"}
+                       "reused across calls; y rounded to float on the device and copied out in four block ranges, "
+                       "each while the later ones are formed), precision mode mixed"}
         t64 = torch.empty(T_out, dtype=torch.float64, pin_memory=True).numpy()
         y64 = torch.empty((T_out, case.p), dtype=torch.float64, pin_memory=True).numpy()
         med, ms = time_calls(lambda: pb.simulate(case.A, case.B, case.C, case.D, case.x0, u, case.t0, case.t_end,
@@ -735,7 +736,8 @@ def run_ours(args):
                    "h2d_bytes_per_step": int(8 * (case.A.size + case.B.size + case.C.size + case.D.size +
                                                   case.x0.size + 3 * case.u.a.size)),
                    "d2h_bytes_per_step": int(2 * d2h), "statistic": f"median of {len(ms)} calls",
-                   "call": "ParODE_SimulateODE_d (double arrays in, y out into pinned host memory reused across calls)"}
+                   "call": "ParODE_SimulateODE_d (double arrays in, y out into pinned host memory reused across calls, "
+                           "in four block ranges as above)"}
 
     # the e2e call's parts, each timed on its own: plan creation (host
     # discretisation, W and power tables on the device), the solve, the copy
@@ -765,8 +767,9 @@ def run_ours(args):
                 parts["copy_ms"].append((t3 - t2) * 1e3)
         med = {k: statistics.median(v) for k, v in parts.items()}
         e2e_split = dict(med, d2h_gbs=8.0 * case.T * case.p / (med["copy_ms"] / 1e3) / 1e9,
-                         note="parts timed separately with host clocks (synchronised); the e2e call overlaps the "
-                              "host time vector with plan creation, the solve and the copy")
+                         note="parts timed separately with host clocks (synchronised), the copy as one piece after "
+                              "the solve; the e2e call overlaps the host time vector with plan creation, the solve "
+                              "and the copy, and each output range's copy with the forming of the later ranges")
     cfg1 = measure_cfg1(pb, wl, torch) if world == 1 and not args.no_extra else None
     tpart = measure_time_partition(pb, torch, dev, case, u, precision, args.steps) \
         if (world > 1 and args.time_partition) else None
