@@ -331,6 +331,7 @@ void SimulateODE(fType A[], fType B[], fType C[], fType D[], int* nInputs, int* 
         opt.precision = L.precision;
         opt.path = L.path;
         opt.input_double = false;  // UFunc(fType t, ...) with fType = float, as the reference ABI
+        opt.one_shot = true;
         Plan plan(dev, s, &L.inputs, *uIndex, *solver, *tStart, *tEnd, *tStep, opt);
         long T = plan.num_outputs();
         // fType is float: y is rounded on the device and copied straight into
@@ -530,6 +531,7 @@ void ParODE_SimulateODE_d(const double* A, const double* B, const double* C, con
         opt.input_double = true;
         opt.fault_withhold = L.fault_withhold;
         opt.log = L.log != 0;
+        opt.one_shot = true;
         Plan plan(dev, s, &L.inputs, uIndex, solver, tStart, tEnd, tStep, opt);
         // the host time vector is built on a helper thread while the plan
         // is set up, solved and its outputs copied

@@ -610,11 +610,13 @@ void Plan::build(int device, const SystemDesc& sys, InputRegistry* inputs, int u
         }
     }
     if (tables_forked) PARODE_CUDA(cudaStreamWaitEvent(stream_, fork_[1], 0));
-    PARODE_CUDA(cudaStreamSynchronize(stream_));
-    if (pin_) {  // the set-up copies are done: the block goes back to the pool
-        give_pinned(pin_);
-        pin_ = nullptr;
-    }
+    if (!opt.one_shot || shards_ > 1) {
+        PARODE_CUDA(cudaStreamSynchronize(stream_));
+        if (pin_) {  // the set-up copies are done: the block goes back to the pool
+            give_pinned(pin_);
+            pin_ = nullptr;
+        }
+    }  // else the pinned block stays with the plan until release() has synchronised
     phase("sync", false);
     if (opt.log) std::fprintf(stderr, "ParODE plan set-up (n=%d T=%ld path=%d):%s\n", sys.n, nScan_, path(), phases.c_str());
     // keep a plan's worth of freed memory in the pool, so that the next plan

@@ -55,6 +55,10 @@ struct PlanOptions {
     int shard = 0, shards = 1;
     // where a batch discretises its systems (DiscretiseAt)
     int discretise = 0;
+    // solved once, right after creation, on the plan's own stream (the
+    // one-shot SimulateODE calls): creation returns without waiting for its
+    // device work, which the solve queues behind and whose synchronise ends both
+    bool one_shot = false;
 };
 
 // Batch discretisation: by its cost (small batches on the host threads,
