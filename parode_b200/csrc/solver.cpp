@@ -609,8 +609,13 @@ void Plan::build(int device, const SystemDesc& sys, InputRegistry* inputs, int u
             phase("tensor-core set-up", true);
         }
     }
-    if (tables_forked) PARODE_CUDA(cudaStreamWaitEvent(stream_, fork_[1], 0));
-    if (!opt.one_shot || shards_ > 1) {
+    // a one-shot response plan joins the power table's stream just before the
+    // carry, its first user: the solve's samples and response GEMMs run
+    // beside the table's squarings
+    const bool one_shot = opt.one_shot && shards_ == 1;
+    if (tables_forked && one_shot && br_) tables_pending_ = true;
+    else if (tables_forked) PARODE_CUDA(cudaStreamWaitEvent(stream_, fork_[1], 0));
+    if (!one_shot) {
         PARODE_CUDA(cudaStreamSynchronize(stream_));
         if (pin_) {  // the set-up copies are done: the block goes back to the pool
             give_pinned(pin_);
@@ -1084,6 +1089,10 @@ int Plan::response_head(cudaStream_t s)
         launch_gemm_tiled(response_agg_args(), s);
         ++launches;
         mark("aggregates", s);
+    }
+    if (tables_pending_) {
+        PARODE_CUDA(cudaStreamWaitEvent(s, fork_[1], 0));
+        tables_pending_ = false;
     }
     launches += carry(s);
     mark("carry", s);

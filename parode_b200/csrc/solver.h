@@ -199,6 +199,7 @@ private:
     double* dTop_ = nullptr;    // gathered top items + their scan's scratch
     ChunkLevels shard_levels_;  // the up-sweep's levels, reused by the down-sweep
     bool shard_up_done_ = false;
+    bool tables_pending_ = false;  // one-shot response plan: the power table's stream joins before the carry
     char* pin_ = nullptr;  // pinned staging of the set-up copies (h2d)
     size_t pin_used_ = 0;
     bool pin_tried_ = false;
