@@ -231,9 +231,10 @@ struct DiscTile {
 };
 long discretise_work_doubles(int n, int m);
 void discretise_tiles(const DiscJob& j, int stage, std::vector<DiscTile>& out);
-// tiles[st] / ntiles[st]: device arrays of the stages' tiles
+// tiles[st] / ntiles[st]: device arrays of the stages' tiles.  parts > 1
+// CTAs share each system's finish (jobs without bbarT and delta only).
 void launch_discretise_batch(const DiscJob* jobs, int njobs, const DiscTile* const tiles[3], const long ntiles[3],
-                             int sms, cudaStream_t s);
+                             int sms, cudaStream_t s, int parts = 1);
 
 // Scan-vector initialisation with the forcing term Gamma_k (zero padding
 // for k >= T and for the components the solver leaves empty).

@@ -79,11 +79,13 @@ __global__ void __launch_bounds__(kThreads) k_disc_gemm(const DiscTile* __restri
 }
 
 // Per system: Phi, Bbar (and its transpose) from the products, then the
-// distance to R.
+// distance to R.  gridDim.y CTAs share a system's elementwise part (only for
+// jobs without a transpose or a distance, which read all of it).
 __global__ void __launch_bounds__(kThreads) k_discretise_finish(const DiscJob* __restrict__ jobs)
 {
     const DiscJob jb = jobs[blockIdx.x];
     const int n = jb.n, m = jb.m, N = jb.solver == 0 ? n : 4 * n;
+    const int tid = blockIdx.y * kThreads + threadIdx.x, nthr = gridDim.y * kThreads;
     const double h = jb.h, h2 = mul(h, h);
     const double* A = jb.A;
     const double* B = jb.B;
@@ -94,13 +96,13 @@ __global__ void __launch_bounds__(kThreads) k_discretise_finish(const DiscJob* _
     const double* A2B = AB + (long)n * max(m, 1);
     const double* A3B = A2B + (long)n * max(m, 1);
     const int W = jb.solver == 0 ? 3 : 5;
-    // Bbar starts at zero (the slots a system without B never fills)
-    for (int e = threadIdx.x; e < n * W * max(m, 1); e += kThreads) jb.bbar[e] = 0.0;
-    __syncthreads();
+    // a system without B has a zero Bbar; with B every slot is written below
+    if (m == 0)
+        for (int e = tid; e < n * W; e += nthr) jb.bbar[e] = 0.0;
     if (jb.solver == 0) {
         const double h3 = mul(mul(h, h), h), h4 = mul(mul(mul(h, h), h), h);
         const double c2 = mul(0.5, h2), c3 = mul(1.0 / 6.0, h3), c4 = mul(1.0 / 24.0, h4);
-        for (int q = threadIdx.x; q < n * n; q += kThreads) {
+        for (int q = tid; q < n * n; q += nthr) {
             const int i = q / n, j = q - i * n;
             double v = add(i == j ? 1.0 : 0.0, mul(h, A[q]));
             v = add(v, mul(c2, A2[q]));
@@ -110,7 +112,7 @@ __global__ void __launch_bounds__(kThreads) k_discretise_finish(const DiscJob* _
         if (m > 0) {
             const double b1 = mul(0.5, h3), b2 = mul(0.25, h4), b3 = mul(4.0, h), b4 = mul(2.0, h2);
             const double sixth = 1.0 / 6.0, b5 = mul(sixth, h);
-            for (int q = threadIdx.x; q < n * m; q += kThreads) {
+            for (int q = tid; q < n * m; q += nthr) {
                 const int i = q / m, j = q - i * m;
                 double* row = jb.bbar + (long)i * 3 * m;
                 const double u = add(add(add(mul(h, B[q]), mul(h2, AB[q])), mul(b1, A2B[q])), mul(b2, A3B[q]));
@@ -124,7 +126,7 @@ __global__ void __launch_bounds__(kThreads) k_discretise_finish(const DiscJob* _
         const double k81 = -81.0 * h2 / 576.0, k333 = 333.0 * h2 / 576.0, k531 = -531.0 * h2 / 576.0,
                      k495 = 495.0 * h2 / 576.0;
         const double k1 = 1.0 * h / 24.0, k5 = -5.0 * h / 24.0, k28 = 28.0 * h / 24.0;
-        for (int q = threadIdx.x; q < n * n; q += kThreads) {
+        for (int q = tid; q < n * n; q += nthr) {
             const int r = q / n, c = q - r * n;
             double* last = jb.phi + (long)r * N;
             last[c] = mul(k81, A2[q]);
@@ -134,7 +136,7 @@ __global__ void __launch_bounds__(kThreads) k_discretise_finish(const DiscJob* _
         }
         if (m > 0) {
             const double kb1 = h / 24.0, kb19 = 19.0 * h / 24.0, kb9 = 9.0 * h / 24.0;
-            for (int q = threadIdx.x; q < n * m; q += kThreads) {
+            for (int q = tid; q < n * m; q += nthr) {
                 const int r = q / m, c = q - r * m;
                 double* row = jb.bbar + (long)r * 5 * m;
                 row[c] = mul(k81, AB[q]);
@@ -219,7 +221,7 @@ void discretise_tiles(const DiscJob& j, int stage, std::vector<DiscTile>& out)
 }
 
 void launch_discretise_batch(const DiscJob* jobs, int njobs, const DiscTile* const tiles[3], const long ntiles[3],
-                             int sms, cudaStream_t s)
+                             int sms, cudaStream_t s, int parts)
 {
     for (int st = 0; st < 3; ++st) {
         if (ntiles[st] <= 0) continue;
@@ -229,7 +231,7 @@ void launch_discretise_batch(const DiscJob* jobs, int njobs, const DiscTile* con
     }
     for (int k = 0; k < njobs; k += 65535) {
         const int cnt = std::min(65535, njobs - k);
-        k_discretise_finish<<<(unsigned)cnt, kThreads, 0, s>>>(jobs + k);
+        k_discretise_finish<<<dim3((unsigned)cnt, (unsigned)std::max(parts, 1)), kThreads, 0, s>>>(jobs + k);
         PARODE_CUDA(cudaGetLastError());
     }
 }

@@ -451,7 +451,9 @@ void Plan::build(int device, const SystemDesc& sys, InputRegistry* inputs, int u
             h2d(dTiles[st], tl.data(), sizeof(DiscTile) * tl.size());
             dt[st] = reinterpret_cast<const DiscTile*>(dTiles[st]);
         }
-        launch_discretise_batch(reinterpret_cast<const DiscJob*>(dDJob), 1, dt, ntiles, sms_, stream_);
+        // no transpose, no distance: the finish's elements spread over CTAs
+        const int parts = std::max(1, std::min(32, (n * n + 255) / 256));
+        launch_discretise_batch(reinterpret_cast<const DiscJob*>(dDJob), 1, dt, ntiles, sms_, stream_, parts);
         PhiJob pj;
         pj.dst = dPow_;
         pj.src = dPhiC;
